@@ -1,0 +1,355 @@
+"""Benchmark of the particle-mesh step on B200 (one JSON line on rank 0).
+
+Workload (the metric's configuration): 256^3 particles on a 256^3 mesh, box 1000 Mpc/h,
+Planck18, seeded white-noise ICs, 2LPT to a = 0.1, EfficientDriftDoubleKick. A "step"
+is one PM step of the whole particle set: kick with the force of the previous step,
+drift, CIC paint, Poisson solve (r2c, Green's function, c2r) -- one force evaluation.
+
+  value : Mpart-steps/s with particles resident in HBM (the 201 MB particle state and
+          the 67 MB meshes exceed... the state is larger than the 126 MB L2, so no flush)
+  e2e   : the same metric through the public API (jfli_b200.interpolate_initial_conditions
+          -> lpt -> nbody -> power) from pinned host white noise to host density + P(k),
+          40 KDK steps per request, copies inside the timed region
+  roofline : the fused particle pass (k_kick_drift_paint), algorithmic bytes
+          48 B/particle (read+write position and velocity) + 8 B/cell (potential gather,
+          density deposit) per launch, over its CUDA-event time, against MEASURED_PEAKS.json
+  cpu_baseline : the NumPy/SciPy FP32 port of the same step (oracle/pm.py) on this host
+
+--gpus N runs N independent replicas (one per GPU, no collective on the data path);
+value is the sum over ranks / the max-over-ranks time. --impl reference times the CPU
+port of the reference algorithm (JAX and the JaxPM fork are not installable here).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_MESH = 256
+BOX = 1000.0
+E2E_STEPS = 40
+METRIC = "Mpart-steps/s at 256^3 (PM KDK step, 2LPT ICs, L=1000 Mpc/h)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="jfli", choices=["jfli", "reference"])
+    ap.add_argument("--mesh", type=int, default=N_MESH)
+    ap.add_argument("--e2e-requests", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- distributed
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(val, world):
+    if world == 1:
+        return val
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([val], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def setup_state(n, cosmo):
+    import jfli_b200 as jf
+
+    noise = jf.white_noise(0, (n, n, n))
+    ic = jf.interpolate_initial_conditions(noise, (n, n, n), (BOX * n / N_MESH,) * 3, cosmo=cosmo)
+    dx, p = jf.lpt(cosmo, ic, ts=0.1, order=2)
+    return dx, p
+
+
+def run_gpu(args, world, rank):
+    import torch
+
+    import jfli_b200 as jf
+    from jfli_b200 import ops
+    from jfli_b200._lib import JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
+    from jfli_b200.pm.solvers import EfficientDriftDoubleKick as EDK
+
+    n = args.mesh
+    cosmo = jf.Planck18()
+    box = BOX * n / N_MESH
+    dx, p = setup_state(n, cosmo)
+    x = dx.array.clone()
+    v = p.array.clone()
+    rho = torch.empty(n, n, n, device="cuda")
+    pot = torch.empty_like(rho)
+    dt0 = 0.9 / E2E_STEPS
+    c = EDK.step_coefficients(cosmo, 0.5, 0.5 + dt0, dt0)
+    flags = JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT
+    stream = torch.cuda.current_stream()
+    rho.zero_()
+    ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT, rho)
+    ops.poisson_potential(rho, 1.0, out=pot)
+
+    # the timed step keeps the same fixed (kick, drift) so every step does identical work
+    kdp_ms = []
+
+    def one_step(timed_kdp=None):
+        rho.zero_()
+        if timed_kdp is not None:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ops.kick_drift_paint(x, v, pot, c.kick, c.drift, flags, rho)
+            e1.record(stream)
+            timed_kdp.append((e0, e1))
+        else:
+            ops.kick_drift_paint(x, v, pot, c.kick, c.drift, flags, rho)
+        ops.poisson_potential(rho, 1.0, out=pot)
+
+    for _ in range(args.warmup):
+        one_step()
+    barrier(world)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    if rank == 0:
+        clocks.start()
+    launches0 = ops.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    ev0.record(stream)
+    pairs = []
+    for _ in range(args.steps):
+        one_step(pairs)
+    ev1.record(stream)
+    barrier(world)
+    launches = ops.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, world)
+    kdp = [a.elapsed_time(b) for a, b in pairs]
+    clk = clocks.stop() if rank == 0 else None
+    particles = n**3
+    value = world * particles * args.steps / (ms_max / 1e3) / 1e6
+
+    # ---- end-to-end through the public API, host buffers in and out
+    e2e = run_e2e(args, cosmo, n, box)
+
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    kdp_avg_ms = statistics.mean(kdp)
+    alg_bytes = 48.0 * particles + 8.0 * particles
+    achieved = alg_bytes / (kdp_avg_ms / 1e3) / 1e9
+    roof = {"kernel": "k_kick_drift_paint", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+            "peak_source": "measured" if peaks else "fallback", "avg_launch_ms": round(kdp_avg_ms, 4),
+            "algorithmic_bytes_per_launch": alg_bytes, "step_share": round(sum(kdp) / ms, 4)}
+    return dict(value=value, ms=ms_max, clocks=clk, launches=launches, e2e=e2e, roofline=roof)
+
+
+def run_e2e(args, cosmo, n, box):
+    import torch
+
+    import jfli_b200 as jf
+
+    noise = torch.from_numpy(jf.white_noise(1, (n, n, n))).pin_memory()
+    kedges = np.geomspace(2 * np.pi / box * (1 - 1e-6), np.pi * n / box, 33)
+    solver = jf.EfficientDriftDoubleKick(interp_kernel=jf.NoInterp(painting=jf.PaintingOptions(target="density")))
+    out_rho = torch.empty(n, n, n, dtype=torch.float32).pin_memory()
+    dt0 = 0.9 / E2E_STEPS
+    steps = None
+    stream = torch.cuda.current_stream()
+
+    def request():
+        nonlocal steps
+        w = noise.to("cuda", non_blocking=True)
+        ic = jf.interpolate_initial_conditions(w, (n, n, n), (box,) * 3, cosmo=cosmo)
+        dx, p = jf.lpt(cosmo, ic, ts=0.1, order=2)
+        rho, run = jf.nbody(cosmo, dx, p, t0=0.1, t1=1.0, dt0=dt0, solver=solver, return_state=True)
+        ps = rho.power(kedges=kedges)
+        out_rho.copy_(rho.array, non_blocking=True)
+        pk = ps.array.to("cpu", non_blocking=True)
+        steps = run.steps
+        return pk
+
+    request()  # warm-up (tables, workspaces)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_requests):
+        pk = request()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    val = n**3 * steps * args.e2e_requests / (ms / 1e3) / 1e6
+    return {"value": round(val, 2), "unit": "Mpart-steps/s", "h2d_bytes_per_step": n**3 * 4,
+            "d2h_bytes_per_step": n**3 * 4 + 32 * 8, "per": "request (ICs + 2LPT + %d KDK steps + P(k))" % steps,
+            "ms_per_request": round(ms / args.e2e_requests, 2)}
+
+
+# ----------------------------------------------------------------------------- CPU arm
+def cpu_step_rate(n, nsteps=1):
+    """Mpart-steps/s of the FP32 NumPy/SciPy port (oracle/pm.py), all host threads."""
+    from oracle import pm as opm
+
+    rng = np.random.default_rng(0)
+    x = (2.0 * rng.standard_normal((n, n, n, 3))).astype(np.float32)
+    v = (0.5 * rng.standard_normal((n, n, n, 3))).astype(np.float32)
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        v += opm.pm_forces(x, np.float32) * np.float32(0.3)
+        x += v * np.float32(0.02)
+    dt = time.perf_counter() - t0
+    return n**3 * nsteps / dt / 1e6, dt
+
+
+def cpu_baseline_block(n):
+    rate, dt = cpu_step_rate(n, 1)
+    return {"value": round(rate, 4), "unit": "Mpart-steps/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"1 KDK step (paint, 4 complex FFTs, 3 readouts) at {n}^3, FP32 NumPy/SciPy, "
+                      f"scipy.fft workers=all; {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n = args.mesh if (args.steps + args.warmup) <= 6 else args.mesh // 2
+    for _ in range(args.warmup):
+        cpu_step_rate(n, 1)
+    rate, dt = cpu_step_rate(n, args.steps)
+    line = {"metric": METRIC, "value": round(rate, 4), "unit": "Mpart-steps/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"PM KDK step, {n}^3 particles/mesh (sample of the 256^3 config)",
+                       "mesh": n, "box": BOX * n / N_MESH},
+            "cpu_baseline": {"value": round(rate, 4), "unit": "Mpart-steps/s", "cores": os.cpu_count(),
+                             "kind": "port",
+                             "sample": f"{args.steps} KDK steps at {n}^3 (FP32 NumPy/SciPy port of the reference "
+                                       f"algorithm; jax and the JaxPM fork are not installable on this image)"},
+            "e2e": {"value": round(rate, 4), "unit": "Mpart-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    world, rank, local = dist_setup(args)
+    res = run_gpu(args, world, rank)
+    if rank == 0:
+        cpu = None if args.no_cpu_baseline else cpu_baseline_block(args.mesh)
+        line = {"metric": METRIC, "value": round(res["value"], 2), "unit": "Mpart-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(res["ms"] / args.steps, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": f"PM KDK step at {args.mesh}^3 particles on a {args.mesh}^3 mesh, "
+                                       f"box {BOX * args.mesh / N_MESH:g} Mpc/h, 2LPT ICs (seeded white noise)",
+                           "mesh": args.mesh, "particles": args.mesh**3, "box": BOX * args.mesh / N_MESH,
+                           "solver": "EfficientDriftDoubleKick", "parallelism": f"replicas x{world}",
+                           "l2": "particle state (x, v: 402 MB) exceeds the 126 MB L2; no flush"},
+                "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"], "clocks": res["clocks"],
+                "gpu_launches": res["launches"]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,138 @@
+/*
+ * libjfli_b200 — C-ABI of the B200 (sm_100a) particle-mesh kernels behind the
+ * jax-fli API. Every function takes device pointers owned by the caller, enqueues its
+ * work on `stream` (a cudaStream_t passed as void*, NULL = legacy default stream) and
+ * returns JFLI_OK (0) or a JFLI_E* code, with a NUL-terminated message written to
+ * `err` (may be NULL) of capacity `errlen`. Nothing throws across this boundary.
+ *
+ * Layouts (all C order, float32 unless stated):
+ *   mesh       [batch][nx][ny][nz]
+ *   particles  [batch][nx][ny][nz][3]  particle (i,j,k) sits on grid point (i,j,k);
+ *              "relative" positions are displacements in cell units (jax-fli
+ *              PositionUnit.GRID_RELATIVE), "absolute" positions are grid coordinates
+ *              (PositionUnit.GRID_ABSOLUTE)
+ *   spectrum   [batch][nx][ny][nz/2+1] complex64 (interleaved float2)
+ * Meshes used with an FFT need nx, ny and nz/2 of the form 2^a 3^b (<= 4096), nz even.
+ *
+ * Reference interfaces replaced (paths inside the jax-fli project):
+ *   jfli_paint_cic         <- _src/fields/_painting.py:22-86 (_single_paint -> cic_paint_dx / cic_paint)
+ *   jfli_readout_cic       <- fields/particles.py:182-229 (read_out -> cic_read_dx / cic_read)
+ *   jfli_rfft3d/irfft3d    <- jaxpm fft3d / ifft3d as used at initial.py:175,182, pm/correction.py:174,193
+ *   jfli_poisson_potential <- the invlaplace_kernel stage of jaxpm pm_forces (pm/solvers.py:22)
+ *   jfli_pm_forces         <- pm/solvers.py:19-32 (_forces -> jaxpm pm_forces, times 1.5 Omega_m)
+ *   jfli_kick_drift_paint  <- pm/solvers.py:151-202 and 258-325 (the per-particle part of step())
+ *   jfli_pm_step           <- one step() of EfficientDriftDoubleKick / ReversibleDoubleKickDrift
+ *   jfli_ic_filter         <- initial.py:167-182 (interpolate_initial_conditions), infer/dist.py:43-79
+ *   jfli_lpt               <- pm/lpt.py:119 (jaxpm lpt, order 1 and 2)
+ *   jfli_power_spectrum    <- _src/power/_compute.py:23-119 (_initialize_pk + _power)
+ *   jfli_healpix_paint     <- _src/fields/_painting.py:249-348 (jaxpm paint_particles_spherical)
+ */
+#ifndef JFLI_B200_H
+#define JFLI_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JFLI_OK 0
+#define JFLI_EINVAL 1      /* bad argument (null pointer, bad shape, short workspace) */
+#define JFLI_ECUDA 2       /* a CUDA call or kernel launch failed */
+#define JFLI_EUNSUPPORTED 3 /* valid but unsupported configuration */
+
+#define JFLI_STEP_KICK 1   /* v += F(x) * kick, F = -grad_FD(pot) read out with CIC */
+#define JFLI_STEP_DRIFT 2  /* x += v * drift */
+#define JFLI_STEP_PAINT 4  /* CIC deposit at the new position */
+#define JFLI_STEP_FORCE 8  /* (jfli_pm_step) solve the Poisson equation for the new positions */
+#define JFLI_STEP_CORRECT 16 /* x += F(x) * kick instead of a kick (PGD position correction) */
+
+#define JFLI_HEALPIX_NGP 0
+#define JFLI_HEALPIX_BILINEAR 1
+
+/* Library identification and device checks. */
+const char* jfli_version(void);
+/* Number of kernels this library has launched in the calling process. */
+long long jfli_launch_count(void);
+/* JFLI_OK if the current device is sm_100 (B200). */
+int jfli_device_check(char* err, size_t errlen);
+/* 1 if an FFT over an (nx, ny, nz) mesh is supported. */
+int jfli_mesh_supported(int nx, int ny, int nz);
+/* Complex elements of one half spectrum: nx * ny * (nz/2 + 1). */
+long long jfli_spectrum_elems(int nx, int ny, int nz);
+
+/* Forward real-to-complex 3D FFT (unnormalised, numpy.fft.rfftn convention). */
+int jfli_rfft3d(void* stream, const float* mesh, void* spec, int nx, int ny, int nz, int batch, char* err,
+                size_t errlen);
+/* Inverse complex-to-real 3D FFT, normalised by 1/(nx ny nz) (numpy.fft.irfftn).
+ * The spectrum is used as scratch and is overwritten. */
+int jfli_irfft3d(void* stream, void* spec, float* mesh, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* CIC deposit of weight `weight` (times weights[p] when weights != NULL) per particle.
+ * accumulate = 0 clears the mesh first. */
+int jfli_paint_cic(void* stream, const float* pos, int absolute, const float* weights, float weight, float* mesh,
+                   int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* CIC interpolation of a scalar mesh at the particle positions, out[batch][nx][ny][nz]. */
+int jfli_readout_cic(void* stream, const float* pos, int absolute, const float* mesh, float* out, int nx, int ny,
+                     int nz, int batch, char* err, size_t errlen);
+
+/* pot = irfft(rfft(rho - rho_mean) * (-1/k^2)), k in radians per cell, k = 0 -> 0. */
+size_t jfli_poisson_workspace_bytes(int nx, int ny, int nz, int batch);
+int jfli_poisson_potential(void* stream, const float* rho, float rho_mean, float* pot, void* workspace,
+                           size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* PGD potential: as jfli_poisson_potential with the extra filter exp(-kl^2/k^2) exp(-k^4/ks^4)
+ * (kl, ks in radians per cell). Replaces pm/correction.py:170-189 (PGDKernel.apply). */
+int jfli_pgd_potential(void* stream, const float* rho, float rho_mean, float kl, float ks, float* pot, void* workspace,
+                       size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* forces[p] = scale * CIC readout of -grad_FD(pot) at the particle positions. */
+int jfli_readout_gradient(void* stream, const float* pos, int absolute, const float* pot, float scale, float* forces,
+                          int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* forces = scale * (paint -> Poisson -> -grad_FD -> readout); jax-fli's _forces uses scale = 1.5 Omega_m. */
+size_t jfli_pm_forces_workspace_bytes(int nx, int ny, int nz, int batch);
+int jfli_pm_forces(void* stream, const float* pos, int absolute, float scale, float* forces, void* workspace,
+                   size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* Fused particle pass: [kick, or with CORRECT a position shift, by kick * -grad_FD(pot)
+ * read out at the current position] -> [drift] -> [paint into rho (accumulating)].
+ * Positions are relative (displacements). */
+int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* pot, float kick, float drift, int flags,
+                          float weight, float* rho, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* One PM step: clear rho, kick/drift/paint (flags KICK|DRIFT), then with FORCE solve for the
+ * new potential into `pot`. Workspace: jfli_poisson_workspace_bytes. */
+int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift, int flags, float* rho, float* pot,
+                 void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                 size_t errlen);
+
+/* out = irfft(rfft(noise) * sqrt(P(|k|) * M / V)), P by linear interpolation (with end
+ * extrapolation) of the device tables ktab/ptab (h/Mpc, (Mpc/h)^3). zero_mode_one sets
+ * P(k=0) to 1. Workspace: jfli_poisson_workspace_bytes. */
+int jfli_ic_filter(void* stream, const float* noise, float* out, const float* ktab, const float* ptab, int ntab,
+                   float lx, float ly, float lz, int zero_mode_one, void* workspace, size_t workspace_bytes, int nx,
+                   int ny, int nz, int batch, char* err, size_t errlen);
+
+/* LPT at the grid points: F1 = -grad_FD laplace^-1 ic, and for order 2 the same from the
+ * second-order source; dx = c1x F1 + c2x F2, p = c1p (c1x F1) + c2p (c2x F2). */
+size_t jfli_lpt_workspace_bytes(int nx, int ny, int nz, int batch);
+int jfli_lpt(void* stream, const float* ic, int order, float c1x, float c2x, float c1p, float c2p, float* dx, float* p,
+             void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* P(k) sums over the full Fourier grid of `mesh` (ortho normalisation), binned with
+ * numpy.digitize(|k|, kedges). out[batch][3][nedges+1] (FP64): sum |delta_k|^2, mode
+ * count, sum |k|; bin 0 and bin nedges are the under/overflow bins. */
+size_t jfli_power_spectrum_workspace_bytes(int nx, int ny, int nz, int batch, int nedges);
+int jfli_power_spectrum(void* stream, const float* mesh, const float* kedges, int nedges, float lx, float ly,
+                        float lz, double* out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
+                        int batch, char* err, size_t errlen);
+
+/* HEALPix RING-ordered shell map of the particles with rmin < |x - observer| <= rmax
+ * (Mpc/h), deposited by `scheme` (JFLI_HEALPIX_NGP or JFLI_HEALPIX_BILINEAR).
+ * map[batch][12 nside^2]; accumulate = 0 clears it first. Raw weight sums. */
+int jfli_healpix_paint(void* stream, const float* disp, int absolute, const float* weights, float weight, float lx,
+                       float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside, int scheme,
+                       float* map, int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JFLI_B200_H */

@@ -1,0 +1,357 @@
+// C-ABI of libjfli_b200: plain pointers, sizes and a caller-owned error buffer.
+// Every entry point validates its arguments, enqueues its kernels on `stream`
+// (a cudaStream_t; 0 = legacy default stream) and returns 0 on success or one of the
+// JFLI_E* codes with a message in `err`. Nothing throws across this boundary and
+// nothing synchronises the device except where documented.
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "../../include/jfli_b200.h"
+#include "internal.h"
+
+namespace jfli {
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace jfli
+
+using jfli::MeshDims;
+
+namespace {
+
+int fail(char* err, size_t errlen, int code, const char* fmt, ...) {
+  if (err && errlen) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(err, errlen, fmt, ap);
+    va_end(ap);
+  }
+  return code;
+}
+
+int cuda_status(cudaError_t e, char* err, size_t errlen, const char* what) {
+  if (e == cudaSuccess) return JFLI_OK;
+  return fail(err, errlen, JFLI_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+bool dims_ok(int nx, int ny, int nz, int batch) {
+  return nx > 0 && ny > 0 && nz > 0 && batch > 0 && batch <= 65535 && (long long)nx * ny * nz < (1LL << 40);
+}
+
+#define CHECK_DIMS(nx, ny, nz, batch)                                                                       \
+  if (!dims_ok(nx, ny, nz, batch))                                                                          \
+  return fail(err, errlen, JFLI_EINVAL, "invalid mesh shape (%d, %d, %d) x batch %d", nx, ny, nz, batch)
+
+#define CHECK_FFT(nx, ny, nz)                                                                               \
+  if (!jfli::mesh_fft_supported(nx, ny, nz))                                                               \
+  return fail(err, errlen, JFLI_EUNSUPPORTED,                                                               \
+              "mesh (%d, %d, %d) unsupported: each axis must be 2^a 3^b <= 4096 and nz even with nz/2 "    \
+              "also 2^a 3^b",                                                                               \
+              nx, ny, nz)
+
+#define CHECK_PTR(p)                                                                                        \
+  if (!(p)) return fail(err, errlen, JFLI_EINVAL, "null pointer argument '%s'", #p)
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t spec_bytes(const MeshDims& d) { return align256((size_t)d.spec_elems() * d.batch * sizeof(float2)); }
+size_t mesh_bytes(const MeshDims& d) { return align256((size_t)d.cells() * d.batch * sizeof(float)); }
+
+}  // namespace
+
+extern "C" {
+
+const char* jfli_version(void) { return "jfli-b200 0.1.0 (sm_100a)"; }
+
+long long jfli_launch_count(void) { return jfli::g_launches.load(); }
+
+int jfli_device_check(char* err, size_t errlen) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e, err, errlen, "cudaGetDevice");
+  int major = 0, minor = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+  if (major != 10 || minor != 0)
+    return fail(err, errlen, JFLI_EUNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a only", dev,
+                major, minor);
+  return JFLI_OK;
+}
+
+int jfli_mesh_supported(int nx, int ny, int nz) { return jfli::mesh_fft_supported(nx, ny, nz) ? 1 : 0; }
+
+long long jfli_spectrum_elems(int nx, int ny, int nz) { return (long long)nx * ny * (nz / 2 + 1); }
+
+int jfli_rfft3d(void* stream, const float* mesh, void* spec, int nx, int ny, int nz, int batch, char* err,
+                size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(mesh);
+  CHECK_PTR(spec);
+  const MeshDims d{nx, ny, nz, batch};
+  return cuda_status(jfli::rfft3d_forward(mesh, (float2*)spec, d, 0.0f, (cudaStream_t)stream), err, errlen,
+                     "jfli_rfft3d");
+}
+
+int jfli_irfft3d(void* stream, void* spec, float* mesh, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(mesh);
+  CHECK_PTR(spec);
+  const MeshDims d{nx, ny, nz, batch};
+  const float scale = 1.0f / ((float)nx * (float)ny * (float)nz);
+  return cuda_status(jfli::rfft3d_inverse((float2*)spec, mesh, d, scale, (cudaStream_t)stream), err, errlen,
+                     "jfli_irfft3d");
+}
+
+int jfli_paint_cic(void* stream, const float* pos, int absolute, const float* weights, float weight, float* mesh,
+                   int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(pos);
+  CHECK_PTR(mesh);
+  const MeshDims d{nx, ny, nz, batch};
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!accumulate) {
+    cudaError_t e = cudaMemsetAsync(mesh, 0, (size_t)d.cells() * batch * sizeof(float), s);
+    if (e != cudaSuccess) return cuda_status(e, err, errlen, "jfli_paint_cic memset");
+  }
+  return cuda_status(jfli::cic_paint(pos, absolute, weights, weight, mesh, d, s), err, errlen, "jfli_paint_cic");
+}
+
+int jfli_readout_cic(void* stream, const float* pos, int absolute, const float* mesh, float* out, int nx, int ny,
+                     int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(pos);
+  CHECK_PTR(mesh);
+  CHECK_PTR(out);
+  const MeshDims d{nx, ny, nz, batch};
+  return cuda_status(jfli::cic_readout(pos, absolute, mesh, out, d, (cudaStream_t)stream), err, errlen,
+                     "jfli_readout_cic");
+}
+
+size_t jfli_poisson_workspace_bytes(int nx, int ny, int nz, int batch) {
+  return spec_bytes(MeshDims{nx, ny, nz, batch});
+}
+
+int jfli_poisson_potential(void* stream, const float* rho, float rho_mean, float* pot, void* workspace,
+                           size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(rho);
+  CHECK_PTR(pot);
+  CHECK_PTR(workspace);
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < spec_bytes(d))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, spec_bytes(d));
+  return cuda_status(jfli::poisson_potential(rho, (float2*)workspace, pot, d, rho_mean, 1.0f, (cudaStream_t)stream),
+                     err, errlen, "jfli_poisson_potential");
+}
+
+int jfli_pgd_potential(void* stream, const float* rho, float rho_mean, float kl, float ks, float* pot, void* workspace,
+                       size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(rho);
+  CHECK_PTR(pot);
+  CHECK_PTR(workspace);
+  if (!(kl >= 0.0f && ks > 0.0f)) return fail(err, errlen, JFLI_EINVAL, "PGD scales need kl >= 0 and ks > 0");
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < spec_bytes(d))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, spec_bytes(d));
+  return cuda_status(
+      jfli::pgd_potential(rho, (float2*)workspace, pot, d, rho_mean, kl, ks, 1.0f, (cudaStream_t)stream), err, errlen,
+      "jfli_pgd_potential");
+}
+
+size_t jfli_pm_forces_workspace_bytes(int nx, int ny, int nz, int batch) {
+  const MeshDims d{nx, ny, nz, batch};
+  return mesh_bytes(d) + spec_bytes(d);
+}
+
+int jfli_pm_forces(void* stream, const float* pos, int absolute, float scale, float* forces, void* workspace,
+                   size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(pos);
+  CHECK_PTR(forces);
+  CHECK_PTR(workspace);
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < jfli_pm_forces_workspace_bytes(nx, ny, nz, batch))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes,
+                jfli_pm_forces_workspace_bytes(nx, ny, nz, batch));
+  cudaStream_t s = (cudaStream_t)stream;
+  float* rho = (float*)workspace;  // the potential overwrites the density in place
+  float2* spec = (float2*)((char*)workspace + mesh_bytes(d));
+  cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
+  if (e == cudaSuccess) e = jfli::cic_paint(pos, absolute, nullptr, 1.0f, rho, d, s);
+  if (e == cudaSuccess) e = jfli::poisson_potential(rho, spec, rho, d, 1.0f, 1.0f, s);
+  if (e == cudaSuccess) e = jfli::cic_readout_gradient(pos, absolute, rho, forces, scale, d, s);
+  return cuda_status(e, err, errlen, "jfli_pm_forces");
+}
+
+int jfli_readout_gradient(void* stream, const float* pos, int absolute, const float* pot, float scale, float* forces,
+                          int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(pos);
+  CHECK_PTR(pot);
+  CHECK_PTR(forces);
+  const MeshDims d{nx, ny, nz, batch};
+  return cuda_status(jfli::cic_readout_gradient(pos, absolute, pot, forces, scale, d, (cudaStream_t)stream), err,
+                     errlen, "jfli_readout_gradient");
+}
+
+int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* pot, float kick, float drift, int flags,
+                          float weight, float* rho, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(vel);
+  if ((flags & ~(JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT | JFLI_STEP_CORRECT)) != 0)
+    return fail(err, errlen, JFLI_EINVAL, "unknown step flags 0x%x", flags);
+  if ((flags & JFLI_STEP_KICK) && (flags & JFLI_STEP_CORRECT))
+    return fail(err, errlen, JFLI_EINVAL, "KICK and CORRECT are exclusive");
+  if ((flags & (JFLI_STEP_KICK | JFLI_STEP_CORRECT)) && !pot)
+    return fail(err, errlen, JFLI_EINVAL, "kick requested without a potential");
+  if ((flags & JFLI_STEP_PAINT) && !rho) return fail(err, errlen, JFLI_EINVAL, "paint requested without a mesh");
+  const MeshDims d{nx, ny, nz, batch};
+  return cuda_status(jfli::kick_drift_paint(disp, vel, pot, kick, drift, flags, weight, rho, d, (cudaStream_t)stream),
+                     err, errlen, "jfli_kick_drift_paint");
+}
+
+int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift, int flags, float* rho, float* pot,
+                 void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                 size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(disp);
+  CHECK_PTR(vel);
+  CHECK_PTR(rho);
+  CHECK_PTR(pot);
+  CHECK_PTR(workspace);
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < spec_bytes(d))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, spec_bytes(d));
+  if ((flags & ~(JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_FORCE)) != 0)
+    return fail(err, errlen, JFLI_EINVAL, "unknown step flags 0x%x", flags);
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
+  if (e == cudaSuccess)
+    e = jfli::kick_drift_paint(disp, vel, pot, kick, drift, (flags & (JFLI_STEP_KICK | JFLI_STEP_DRIFT)) | JFLI_STEP_PAINT,
+                               1.0f, rho, d, s);
+  if (e == cudaSuccess && (flags & JFLI_STEP_FORCE))
+    e = jfli::poisson_potential(rho, (float2*)workspace, pot, d, 1.0f, 1.0f, s);
+  return cuda_status(e, err, errlen, "jfli_pm_step");
+}
+
+int jfli_ic_filter(void* stream, const float* noise, float* out, const float* ktab, const float* ptab, int ntab,
+                   float lx, float ly, float lz, int zero_mode_one, void* workspace, size_t workspace_bytes, int nx,
+                   int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(noise);
+  CHECK_PTR(out);
+  CHECK_PTR(ktab);
+  CHECK_PTR(ptab);
+  CHECK_PTR(workspace);
+  if (ntab < 2 || ntab > 4096) return fail(err, errlen, JFLI_EINVAL, "table length %d outside [2, 4096]", ntab);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < spec_bytes(d))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, spec_bytes(d));
+  const float box[3] = {lx, ly, lz};
+  return cuda_status(jfli::ic_filter(noise, (float2*)workspace, out, d, ktab, ptab, ntab, box, zero_mode_one,
+                                     (cudaStream_t)stream),
+                     err, errlen, "jfli_ic_filter");
+}
+
+size_t jfli_lpt_workspace_bytes(int nx, int ny, int nz, int batch) {
+  const MeshDims d{nx, ny, nz, batch};
+  return spec_bytes(d) + 2 * mesh_bytes(d) + align256((size_t)d.cells() * batch * 3 * sizeof(float));
+}
+
+int jfli_lpt(void* stream, const float* ic, int order, float c1x, float c2x, float c1p, float c2p, float* dx, float* p,
+             void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(ic);
+  CHECK_PTR(dx);
+  CHECK_PTR(p);
+  CHECK_PTR(workspace);
+  if (order != 1 && order != 2) return fail(err, errlen, JFLI_EINVAL, "LPT order must be 1 or 2, got %d", order);
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < jfli_lpt_workspace_bytes(nx, ny, nz, batch))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes,
+                jfli_lpt_workspace_bytes(nx, ny, nz, batch));
+  cudaStream_t s = (cudaStream_t)stream;
+  char* w = (char*)workspace;
+  float2* spec = (float2*)w;
+  float* pot = (float*)(w + spec_bytes(d));
+  float* src = (float*)(w + spec_bytes(d) + mesh_bytes(d));
+  float* f2 = (float*)(w + spec_bytes(d) + 2 * mesh_bytes(d));
+  // first order: phi1 = laplace^-1 ic, F1 = -D phi1 at the grid points (written to dx)
+  cudaError_t e = jfli::poisson_potential(ic, spec, pot, d, 0.0f, 1.0f, s);
+  if (e == cudaSuccess) e = jfli::grid_gradient(pot, dx, 1.0f, 0, d, s);
+  if (e == cudaSuccess && order == 2) {
+    e = jfli::lpt2_source(pot, src, d, s);
+    if (e == cudaSuccess) e = jfli::poisson_potential(src, spec, pot, d, 0.0f, 1.0f, s);
+    if (e == cudaSuccess) e = jfli::grid_gradient(pot, f2, 1.0f, 0, d, s);
+  }
+  if (e == cudaSuccess) e = jfli::lpt_combine(dx, order == 2 ? f2 : nullptr, c1x, c2x, c1p, c2p, dx, p, d, s);
+  return cuda_status(e, err, errlen, "jfli_lpt");
+}
+
+size_t jfli_power_spectrum_workspace_bytes(int nx, int ny, int nz, int batch, int nedges) {
+  const MeshDims d{nx, ny, nz, batch};
+  const size_t partial = (size_t)jfli::x_pass_ctas(d) * batch * 3 * (nedges + 1) * sizeof(double);
+  return spec_bytes(d) + align256(partial);
+}
+
+int jfli_power_spectrum(void* stream, const float* mesh, const float* kedges, int nedges, float lx, float ly,
+                        float lz, double* out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
+                        int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(mesh);
+  CHECK_PTR(kedges);
+  CHECK_PTR(out);
+  CHECK_PTR(workspace);
+  if (nedges < 1 || nedges > 2048) return fail(err, errlen, JFLI_EINVAL, "nedges %d outside [1, 2048]", nedges);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  const size_t need = jfli_power_spectrum_workspace_bytes(nx, ny, nz, batch, nedges);
+  if (workspace_bytes < need)
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  cudaStream_t s = (cudaStream_t)stream;
+  float2* spec = (float2*)workspace;
+  double* partials = (double*)((char*)workspace + spec_bytes(d));
+  const float box[3] = {lx, ly, lz};
+  const float norm = 1.0f / ((float)nx * (float)ny * (float)nz);
+  cudaError_t e = jfli::power_partials(mesh, spec, partials, d, kedges, nedges, box, norm, s);
+  if (e == cudaSuccess) e = jfli::power_finalize(partials, jfli::x_pass_ctas(d), nedges + 1, out, batch, s);
+  return cuda_status(e, err, errlen, "jfli_power_spectrum");
+}
+
+int jfli_healpix_paint(void* stream, const float* disp, int absolute, const float* weights, float weight, float lx,
+                       float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside, int scheme,
+                       float* map, int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(map);
+  if (nside < 1 || nside > 8192) return fail(err, errlen, JFLI_EINVAL, "nside %d outside [1, 8192]", nside);
+  if (scheme != JFLI_HEALPIX_NGP && scheme != JFLI_HEALPIX_BILINEAR)
+    return fail(err, errlen, JFLI_EUNSUPPORTED, "HEALPix scheme %d not supported (0 = ngp, 1 = bilinear)", scheme);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!accumulate) {
+    cudaError_t e = cudaMemsetAsync(map, 0, (size_t)12 * nside * nside * batch * sizeof(float), s);
+    if (e != cudaSuccess) return cuda_status(e, err, errlen, "jfli_healpix_paint memset");
+  }
+  const float box[3] = {lx, ly, lz};
+  const float obs[3] = {ox, oy, oz};
+  return cuda_status(
+      jfli::healpix_paint(disp, absolute, weights, weight, d, box, obs, rmin, rmax, nside, scheme, map, s), err,
+      errlen, "jfli_healpix_paint");
+}
+
+}  // extern "C"

@@ -1,0 +1,221 @@
+// HEALPix lightcone shell painting (reference pm/interp.py:161-209 ->
+// fields/particles.py:326-442 -> _src/fields/_painting.py:249-348 -> JaxPM
+// `paint_particles_spherical`).
+//
+// Each particle is placed in comoving Mpc/h, its distance r to the observer selects the
+// shell R_min < r <= R_max, and its direction is deposited on the RING-ordered HEALPix
+// map either on one pixel ("ngp", ang2pix) or on the 4 pixels of the bilinear
+// interpolation ("bilinear", the default scheme). Pixel geometry follows the published
+// HEALPix construction (Gorski et al. 2005, ApJ 622:759): ring index, ring start pixel,
+// ring length, ring colatitude and the half-pixel shift of alternate equatorial rings.
+// Angles are computed in FP64 from the FP32 positions.
+#include <math.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace jfli {
+
+struct RingInfo {
+  long long start;
+  int npix;
+  double theta;
+  int shifted;
+};
+
+__device__ __forceinline__ RingInfo ring_info(int ring, int nside) {
+  const long long npix = 12LL * nside * nside;
+  const long long ncap = 2LL * nside * (nside - 1);
+  const int north = ring > 2 * nside ? 4 * nside - ring : ring;
+  RingInfo r;
+  if (north < nside) {
+    const double tmp = (double)north * north * (4.0 / (double)npix);
+    const double cth = 1.0 - tmp;
+    const double sth = sqrt(tmp * (2.0 - tmp));
+    r.theta = atan2(sth, cth);
+    r.npix = 4 * north;
+    r.shifted = 1;
+    r.start = 2LL * north * (north - 1);
+  } else {
+    r.theta = acos((double)(2 * nside - north) * (2.0 / (3.0 * nside)));
+    r.npix = 4 * nside;
+    r.shifted = ((north - nside) & 1) == 0;
+    r.start = ncap + (long long)(north - nside) * 4 * nside;
+  }
+  if (north != ring) {
+    r.theta = M_PI - r.theta;
+    r.start = npix - r.start - r.npix;
+  }
+  return r;
+}
+
+// Number of the ring at or above colatitude with cos(theta) = z (0 = north pole).
+__device__ __forceinline__ int ring_above(double z, int nside) {
+  const double az = fabs(z);
+  if (az <= 2.0 / 3.0) return (int)(nside * (2.0 - 1.5 * z));
+  const int ir = (int)(nside * sqrt(3.0 * (1.0 - az)));
+  return z > 0 ? ir : 4 * nside - ir - 1;
+}
+
+__device__ __forceinline__ long long ang2pix_ring(double z, double phi, int nside) {
+  const double twopi = 2.0 * M_PI;
+  double ph = fmod(phi, twopi);
+  if (ph < 0) ph += twopi;
+  const double tt = ph / (0.5 * M_PI);  // in [0, 4)
+  const double za = fabs(z);
+  const long long npix = 12LL * nside * nside;
+  const long long ncap = 2LL * nside * (nside - 1);
+  if (za <= 2.0 / 3.0) {
+    const double t1 = nside * (0.5 + tt);
+    const double t2 = nside * z * 0.75;
+    const long long jp = (long long)(t1 - t2);
+    const long long jm = (long long)(t1 + t2);
+    const long long ir = nside + 1 + jp - jm;
+    const long long kshift = 1 - (ir & 1);
+    long long ip = (jp + jm - nside + kshift + 1) / 2;
+    ip %= 4LL * nside;
+    if (ip < 0) ip += 4LL * nside;
+    return ncap + (ir - 1) * 4LL * nside + ip;
+  }
+  const double tp = tt - (double)(int)tt;
+  const double tmp = nside * sqrt(3.0 * (1.0 - za));
+  const long long jp = (long long)(tp * tmp);
+  const long long jm = (long long)((1.0 - tp) * tmp);
+  const long long ir = jp + jm + 1;
+  long long ip = (long long)(tt * ir);
+  ip %= 4 * ir;
+  if (ip < 0) ip += 4 * ir;
+  return z > 0 ? 2 * ir * (ir - 1) + ip : npix - 2 * ir * (ir + 1) + ip;
+}
+
+// Bilinear interpolation pixels and weights (the 4-neighbour scheme of HEALPix
+// get_interpol / healpy get_interp_weights, RING ordering).
+__device__ __forceinline__ void interp_weights(double theta, double phi, int nside, long long pix[4], double w[4]) {
+  const double twopi = 2.0 * M_PI;
+  double ph = fmod(phi, twopi);
+  if (ph < 0) ph += twopi;
+  const long long npix = 12LL * nside * nside;
+  const double z = cos(theta);
+  const int ir1 = ring_above(z, nside);
+  const int ir2 = ir1 + 1;
+  double theta1 = 0.0, theta2 = 0.0;
+  if (ir1 > 0) {
+    const RingInfo r = ring_info(ir1, nside);
+    theta1 = r.theta;
+    const double dphi = twopi / r.npix;
+    const double tmp = ph / dphi - 0.5 * r.shifted;
+    long long i1 = tmp < 0 ? (long long)tmp - 1 : (long long)tmp;
+    const double wp = (ph - (i1 + 0.5 * r.shifted) * dphi) / dphi;
+    long long i2 = i1 + 1;
+    if (i1 < 0) i1 += r.npix;
+    if (i2 >= r.npix) i2 -= r.npix;
+    pix[0] = r.start + i1;
+    pix[1] = r.start + i2;
+    w[0] = 1.0 - wp;
+    w[1] = wp;
+  }
+  if (ir2 < 4 * nside) {
+    const RingInfo r = ring_info(ir2, nside);
+    theta2 = r.theta;
+    const double dphi = twopi / r.npix;
+    const double tmp = ph / dphi - 0.5 * r.shifted;
+    long long i1 = tmp < 0 ? (long long)tmp - 1 : (long long)tmp;
+    const double wp = (ph - (i1 + 0.5 * r.shifted) * dphi) / dphi;
+    long long i2 = i1 + 1;
+    if (i1 < 0) i1 += r.npix;
+    if (i2 >= r.npix) i2 -= r.npix;
+    pix[2] = r.start + i1;
+    pix[3] = r.start + i2;
+    w[2] = 1.0 - wp;
+    w[3] = wp;
+  }
+  if (ir1 == 0) {
+    const double wt = theta / theta2;
+    w[2] *= wt;
+    w[3] *= wt;
+    const double fac = (1.0 - wt) * 0.25;
+    w[0] = fac;
+    w[1] = fac;
+    w[2] += fac;
+    w[3] += fac;
+    pix[0] = (pix[2] + 2) & 3;
+    pix[1] = (pix[3] + 2) & 3;
+  } else if (ir2 == 4 * nside) {
+    const double wt = (theta - theta1) / (M_PI - theta1);
+    w[0] *= (1.0 - wt);
+    w[1] *= (1.0 - wt);
+    const double fac = wt * 0.25;
+    w[0] += fac;
+    w[1] += fac;
+    w[2] = fac;
+    w[3] = fac;
+    pix[2] = ((pix[0] + 2) & 3) + npix - 4;
+    pix[3] = ((pix[1] + 2) & 3) + npix - 4;
+  } else {
+    const double wt = (theta - theta1) / (theta2 - theta1);
+    w[0] *= (1.0 - wt);
+    w[1] *= (1.0 - wt);
+    w[2] *= wt;
+    w[3] *= wt;
+  }
+}
+
+__global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, const float* __restrict__ weights,
+                                float weight, MeshDims d, float3 cell, float3 obs, float rmin, float rmax, int nside,
+                                int scheme, float* __restrict__ map) {
+  const long long np = d.cells();
+  const long long npix = 12LL * nside * nside;
+  const int b = blockIdx.y;
+  disp += (long long)b * np * 3;
+  map += (long long)b * npix;
+  if (weights) weights += (long long)b * np;
+  const long long yz = (long long)d.ny * d.nz;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+    float gx = disp[3 * p + 0], gy = disp[3 * p + 1], gz = disp[3 * p + 2];
+    if (!absolute) {
+      const int i = (int)(p / yz);
+      const long long r = p - (long long)i * yz;
+      const int j = (int)(r / d.nz);
+      const int k = (int)(r - (long long)j * d.nz);
+      gx += (float)i;
+      gy += (float)j;
+      gz += (float)k;
+    }
+    const float vx = gx * cell.x - obs.x, vy = gy * cell.y - obs.y, vz = gz * cell.z - obs.z;
+    const float rr = sqrtf(vx * vx + vy * vy + vz * vz);
+    if (!(rr > rmin && rr <= rmax)) continue;
+    const float w = weights ? weights[p] * weight : weight;
+    const double dr = (double)rr;
+    const double zc = (double)vz / dr;
+    const double phi = atan2((double)vy, (double)vx);
+    if (scheme == 0) {
+      const long long pix = ang2pix_ring(zc, phi, nside);
+      if (pix >= 0 && pix < npix) atomicAdd(map + pix, w);
+    } else {
+      long long pix[4];
+      double wt[4];
+      interp_weights(acos(fmin(1.0, fmax(-1.0, zc))), phi, nside, pix, wt);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (pix[q] >= 0 && pix[q] < npix) atomicAdd(map + pix[q], (float)(wt[q] * (double)w));
+    }
+  }
+}
+
+cudaError_t healpix_paint(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d,
+                          const float* box, const float* observer, float rmin, float rmax, int nside, int scheme,
+                          float* map, cudaStream_t s) {
+  const float3 cell = make_float3(box[0] / d.nx, box[1] / d.ny, box[2] / d.nz);
+  const float3 obs = make_float3(observer[0], observer[1], observer[2]);
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  long long blocks = (d.cells() + 255) / 256;
+  if (blocks > (long long)nsm * 16) blocks = (long long)nsm * 16;
+  k_healpix_paint<<<dim3((unsigned)blocks, d.batch), 256, 0, s>>>(disp, absolute, weights, weight, d, cell, obs, rmin,
+                                                                  rmax, nside, scheme, map);
+  note_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace jfli

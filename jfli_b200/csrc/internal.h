@@ -1,0 +1,65 @@
+// Internal C++ interface between the kernel files and the C-ABI layer (api.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace jfli {
+
+// Counts kernel launches issued by this library (reported by jfli_launch_count).
+void note_launch();
+
+struct MeshDims {
+  int nx, ny, nz, batch;
+  __host__ __device__ long long cells() const { return (long long)nx * ny * nz; }
+  __host__ __device__ int hz() const { return nz / 2 + 1; }
+  __host__ __device__ long long spec_elems() const { return (long long)nx * ny * (nz / 2 + 1); }
+};
+
+// ---- fft.cu ----
+bool fft_axis_supported(int n);
+bool mesh_fft_supported(int nx, int ny, int nz);
+int x_pass_ctas(const MeshDims& d);
+cudaError_t rfft3d_forward(const float* in, float2* spec, const MeshDims& d, float sub, cudaStream_t s);
+cudaError_t rfft3d_inverse(float2* spec, float* out, const MeshDims& d, float scale, cudaStream_t s);
+cudaError_t poisson_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean,
+                              float scale, cudaStream_t s);
+cudaError_t pgd_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean, float kl,
+                          float ks, float scale, cudaStream_t s);
+cudaError_t ic_filter(const float* noise, float2* spec, float* out, const MeshDims& d, const float* ktab,
+                      const float* ptab, int ntab, const float* box, int zero_mode_one, cudaStream_t s);
+cudaError_t power_partials(const float* mesh, float2* spec, double* partials, const MeshDims& d, const float* kedges,
+                           int nedges, const float* box, float norm, cudaStream_t s);
+
+// ---- cic.cu ----
+// Particle update program flags for kick_drift_paint.
+enum StepFlags {
+  kStepKick = 1,   // v += F(x) * kick, F = -grad_FD(pot) read out with CIC
+  kStepDrift = 2,  // x += v * drift
+  kStepPaint = 4,  // CIC deposit of weight `weight` at the (new) position into rho
+  kStepCorrect = 16,  // x += F(x) * kick (position correction, PGD); exclusive with kStepKick
+};
+cudaError_t cic_paint(const float* pos, int absolute, const float* weights, float weight, float* mesh,
+                      const MeshDims& d, cudaStream_t s);
+cudaError_t cic_readout(const float* pos, int absolute, const float* mesh, float* out, const MeshDims& d,
+                        cudaStream_t s);
+cudaError_t cic_readout_gradient(const float* pos, int absolute, const float* pot, float* out, float scale,
+                                 const MeshDims& d, cudaStream_t s);
+cudaError_t kick_drift_paint(float* disp, float* vel, const float* pot, float kick, float drift, int flags,
+                             float weight, float* rho, const MeshDims& d, cudaStream_t s);
+cudaError_t grid_gradient(const float* pot, float* out, float scale, int accumulate, const MeshDims& d,
+                          cudaStream_t s);
+cudaError_t lpt2_source(const float* pot, float* out, const MeshDims& d, cudaStream_t s);
+cudaError_t lpt_combine(const float* f1, const float* f2, float c1x, float c2x, float c1p, float c2p, float* dx,
+                        float* p, const MeshDims& d, cudaStream_t s);
+cudaError_t axpy_particles(float* y, const float* x, float a, const MeshDims& d, cudaStream_t s);
+
+// ---- spectra.cu ----
+cudaError_t power_finalize(const double* partials, int nctas, int nbins, double* out, int batch, cudaStream_t s);
+
+// ---- healpix.cu ----
+cudaError_t healpix_paint(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d,
+                          const float* box, const float* observer, float rmin, float rmax, int nside, int scheme,
+                          float* map, cudaStream_t s);
+
+}  // namespace jfli

@@ -1,0 +1,196 @@
+// k-space operators applied inside the x pass of the 3D FFT (see fft.cu).
+//
+// Wavenumbers follow the particle-mesh convention of JaxPM's `fftk`
+// (k_i = 2*pi*fftfreq(n_i), radians per cell) for the Poisson/PGD kernels, and the
+// physical convention of jax-fli's `_initialize_pk` (k_i = 2*pi*fftfreq(n_i)*n_i/L_i,
+// h/Mpc) for P(k) and initial conditions.
+#pragma once
+
+#include "common.cuh"
+
+namespace jfli {
+
+// k_i^2 for bin i of an axis of length n, rounded to float like fftk's float32 table.
+__device__ __forceinline__ float k_rad_per_cell(int i, int n) {
+  return (float)(6.283185307179586476925 * (double)signed_freq(i, n) / (double)n);
+}
+
+// Poisson potential: pot_k = delta_k * (-1/k^2) * norm, k = 0 -> 0.
+// Follows JaxPM `invlaplace_kernel` (reference call site pm/solvers.py:22 via pm_forces).
+struct PoissonOp {
+  static constexpr bool kInverse = true;
+  static constexpr bool kStore = true;
+  int nx, ny, nz;
+  float norm;
+  static size_t smem_bytes(const PoissonOp& op) { return sizeof(float) * op.nx; }
+  __device__ void prologue(float* sm, int) const {
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+      const float k = k_rad_per_cell(i, nx);
+      sm[i] = k * k;
+    }
+    __syncthreads();
+  }
+  __device__ float2 apply(float2 v, int kx, int ky, int kz, float* sm, int) const {
+    const float k1 = k_rad_per_cell(ky, ny);
+    const float k2 = k_rad_per_cell(kz, nz);
+    const float kk = sm[kx] + k1 * k1 + k2 * k2;
+    const float g = (kk == 0.f) ? 0.f : -1.f / kk;
+    return cscale(v, g * norm);
+  }
+  __device__ void epilogue(float*, int, int, int) const {}
+};
+
+// PGD short-range potential (reference pm/correction.py:177-189):
+// pot_k = delta_k * (-1/k^2) * exp(-kl^2/k^2) * exp(-k^4/ks^4) * norm, k = 0 -> 0.
+struct PgdOp {
+  static constexpr bool kInverse = true;
+  static constexpr bool kStore = true;
+  int nx, ny, nz;
+  float norm, kl2, ks4;
+  static size_t smem_bytes(const PgdOp& op) { return sizeof(float) * op.nx; }
+  __device__ void prologue(float* sm, int) const {
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+      const float k = k_rad_per_cell(i, nx);
+      sm[i] = k * k;
+    }
+    __syncthreads();
+  }
+  __device__ float2 apply(float2 v, int kx, int ky, int kz, float* sm, int) const {
+    const float k1 = k_rad_per_cell(ky, ny);
+    const float k2 = k_rad_per_cell(kz, nz);
+    const float kk = sm[kx] + k1 * k1 + k2 * k2;
+    if (kk == 0.f) return make_float2(0.f, 0.f);
+    const float range = expf(-kl2 / kk) * expf(-(kk * kk) / ks4);
+    return cscale(v, (-1.f / kk) * range * norm);
+  }
+  __device__ void epilogue(float*, int, int, int) const {}
+};
+
+// Linear interpolation with end extrapolation on a tabulated P(k), the behaviour of
+// jax_cosmo's `interp` used by JaxPM `interpolate_power_spectrum`
+// (reference call site initial.py:171-173; infer/dist.py:50-53).
+__device__ __forceinline__ float interp_table(float x, const float* xp, const float* fp, int n) {
+  // first index with xp[i] >= x (searchsorted, side="left")
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (xp[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  int i = lo - 1;
+  i = i < 0 ? 0 : (i > n - 2 ? n - 2 : i);
+  const float slope = (fp[i + 1] - fp[i]) / (xp[i + 1] - xp[i]);
+  return fp[i] + (x - xp[i]) * slope;
+}
+
+// Gaussian initial conditions (reference initial.py:175-182):
+// field_k *= sqrt(P(|k|) * M / V) * norm, |k| in h/Mpc. `zero_mode_one` reproduces the
+// k = 0 guard of infer/dist.py:68.
+struct IcOp {
+  static constexpr bool kInverse = true;
+  static constexpr bool kStore = true;
+  int nx, ny, nz;
+  const float* ktab;
+  const float* ptab;
+  int ntab;
+  float lx, ly, lz;  // box side lengths L_i
+  float factor;      // M / V
+  float norm;        // 1 / M
+  int zero_mode_one;
+  static size_t smem_bytes(const IcOp& op) { return sizeof(float) * (op.nx + 2 * op.ntab); }
+  __device__ void prologue(float* sm, int) const {
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+      sm[i] = k_rad_per_cell(i, nx) / lx * (float)nx;
+    }
+    for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
+      sm[nx + i] = ktab[i];
+      sm[nx + ntab + i] = ptab[i];
+    }
+    __syncthreads();
+  }
+  __device__ float2 apply(float2 v, int kx, int ky, int kz, float* sm, int) const {
+    const float ax = sm[kx];
+    const float ay = k_rad_per_cell(ky, ny) / ly * (float)ny;
+    const float az = k_rad_per_cell(kz, nz) / lz * (float)nz;
+    const float kmag = sqrtf(ax * ax + ay * ay + az * az);
+    float pk = interp_table(kmag, sm + nx, sm + nx + ntab, ntab) * factor;
+    if (zero_mode_one && kmag == 0.f) pk = 1.f;
+    return cscale(v, sqrtf(pk) * norm);
+  }
+  __device__ void epilogue(float*, int, int, int) const {}
+};
+
+// Power spectrum histogram (reference _src/power/_compute.py:23-119): |delta_k|^2 with
+// ortho normalisation binned by digitize(|k|, kedges) over the full grid. The half
+// spectrum stores each mode with 0 < kz < nz/2 once for itself and its conjugate
+// partner, so those modes count twice. Sums are kept in FP64.
+struct PkOp {
+  static constexpr bool kInverse = false;
+  static constexpr bool kStore = false;
+  int nx, ny, nz;
+  const float* kedges;
+  int nedges;
+  float cx, cy, cz;  // 2*pi / L_i
+  float norm;        // 1 / M for norm="ortho"
+  double* partials;  // [batch][nctas][3][nedges+1]
+  static size_t smem_bytes(const PkOp& op) {
+    return sizeof(double) * 3 * (op.nedges + 1) + sizeof(float) * (op.nedges + 1);
+  }
+  __device__ void prologue(float* smf, int) const {
+    double* bins = reinterpret_cast<double*>(smf);
+    float* edges = reinterpret_cast<float*>(bins + 3 * (nedges + 1));
+    for (int i = threadIdx.x; i < 3 * (nedges + 1); i += blockDim.x) bins[i] = 0.0;
+    for (int i = threadIdx.x; i < nedges; i += blockDim.x) edges[i] = kedges[i];
+    __syncthreads();
+  }
+  __device__ float2 apply(float2 v, int kx, int ky, int kz, float* smf, int) const {
+    double* bins = reinterpret_cast<double*>(smf);
+    const float* edges = reinterpret_cast<const float*>(bins + 3 * (nedges + 1));
+    const float ax = cx * (float)signed_freq(kx, nx);
+    const float ay = cy * (float)signed_freq(ky, ny);
+    const float az = cz * (float)signed_freq(kz, nz);
+    const float kmag = sqrtf(ax * ax + ay * ay + az * az);
+    // digitize(right=False): number of edges <= kmag
+    int lo = 0, hi = nedges;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (edges[mid] <= kmag)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    const int bin = lo;
+    const double w = (kz == 0 || 2 * kz == nz) ? 1.0 : 2.0;
+    const double p = w * ((double)v.x * v.x + (double)v.y * v.y) * (double)norm;
+    const double kw = w * (double)kmag;
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, bin);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    double sp = 0.0, sw = 0.0, sk = 0.0;
+    unsigned m = peers;
+    while (m) {
+      const int l = __ffs(m) - 1;
+      sp += __shfl_sync(peers, p, l);
+      sw += __shfl_sync(peers, w, l);
+      sk += __shfl_sync(peers, kw, l);
+      m &= m - 1;
+    }
+    if (lane == leader) {
+      atomicAdd(&bins[bin], sp);
+      atomicAdd(&bins[(nedges + 1) + bin], sw);
+      atomicAdd(&bins[2 * (nedges + 1) + bin], sk);
+    }
+    return v;
+  }
+  __device__ void epilogue(float* smf, int batch, int cta, int nctas) const {
+    const double* bins = reinterpret_cast<const double*>(smf);
+    const int nb = 3 * (nedges + 1);
+    double* dst = partials + ((long long)batch * nctas + cta) * nb;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) dst[i] = bins[i];
+  }
+};
+
+}  // namespace jfli

@@ -1,0 +1,309 @@
+"""Field containers mirroring jax-fli's field pytrees (reference _src/base/_core.py:175-516,
+fields/particles.py, fields/density.py, fields/lightcone.py, fields/painting.py).
+
+A field holds a CUDA tensor in `array` plus the same static metadata the reference
+carries (mesh_size, box_size, observer_position, nside, status, unit, ...). Painting,
+readout and power spectra dispatch to the B200 kernels through `jfli_b200.ops`.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+from enum import Enum, auto
+from typing import Any
+
+import numpy as np
+import torch
+
+from . import ops
+
+DEFAULT_CHUNK_SIZE = 2**24
+
+
+class FieldStatus(str, Enum):
+    UNKNOWN = auto()
+    INITIAL_FIELD = auto()
+    LPT1 = auto()
+    LPT2 = auto()
+    DENSITY_FIELD = auto()
+    PARTICLES = auto()
+    PROJECTED_DENSITY = auto()
+    LIGHTCONE = auto()
+    KAPPA = auto()
+    GAMMA = auto()
+
+
+class PhysicalUnit(str, Enum):
+    INVALID_UNIT = auto()
+
+
+class PositionUnit(str, Enum):
+    GRID_RELATIVE = auto()
+    GRID_ABSOLUTE = auto()
+    MPC_H = auto()
+
+
+class DensityUnit(str, Enum):
+    OVERDENSITY = auto()
+    DENSITY = auto()
+    COUNTS = auto()
+    MSUN_H_PER_MPC3 = auto()
+
+
+@dataclasses.dataclass(frozen=True)
+class PaintingOptions:
+    """Painting configuration (reference fields/painting.py:15-96)."""
+
+    target: str
+    scheme: str = "bilinear"
+    kernel_width_arcmin: float | None = None
+    smoothing_interpretation: str = "fwhm"
+    paint_nside: int | None = None
+    ud_grade_power: float = 0.0
+    ud_grade_order_in: str = "RING"
+    ud_grade_order_out: str = "RING"
+    ud_grade_pess: bool = False
+    chunk_size: int = DEFAULT_CHUNK_SIZE
+    weights: Any = 1.0
+    batch_size: int | None = None
+
+    def __post_init__(self):
+        if self.target not in ("spherical", "flat", "density", "particles"):
+            raise ValueError(f"unknown painting target {self.target!r}")
+        if self.scheme not in ("ngp", "bilinear", "rbf_neighbor"):
+            raise ValueError(f"unknown spherical scheme {self.scheme!r}")
+
+
+def _weights_arg(weights):
+    """Split a painting weight into (per-particle tensor or None, scalar)."""
+    if weights is None:
+        return None, 1.0
+    if isinstance(weights, torch.Tensor):
+        if weights.ndim == 0:
+            return None, float(weights)
+        return weights.to(torch.float32).contiguous(), 1.0
+    if isinstance(weights, np.ndarray):
+        if weights.ndim == 0:
+            return None, float(weights)
+        return torch.as_tensor(weights, dtype=torch.float32, device="cuda").contiguous(), 1.0
+    return None, float(weights)
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class AbstractField:
+    array: Any
+    mesh_size: tuple
+    box_size: tuple
+    z_sources: Any = None
+    scale_factors: Any = None
+    comoving_centers: Any = None
+    density_width: Any = None
+    observer_position: tuple = (0.5, 0.5, 0.5)
+    sharding: Any = None
+    halo_size: tuple = (0, 0)
+    nside: int | None = None
+    flatsky_npix: tuple | None = None
+    field_size: float | None = None
+    status: FieldStatus = FieldStatus.UNKNOWN
+    unit: Any = PhysicalUnit.INVALID_UNIT
+
+    def __post_init__(self):
+        if not (isinstance(self.mesh_size, tuple) and len(self.mesh_size) == 3):
+            raise ValueError(f"mesh_size must be a tuple of 3, got {self.mesh_size}")
+        if not (isinstance(self.box_size, tuple) and len(self.box_size) == 3):
+            raise ValueError(f"box_size must be a tuple of 3, got {self.box_size}")
+        if any(not 0.0 <= f <= 1.0 for f in self.observer_position):
+            raise ValueError("observer_position entries must lie within [0, 1]")
+        if self.sharding is not None:
+            raise NotImplementedError("jfli_b200 runs on one GPU; sharded fields are not supported")
+        if self.nside is not None and self.nside <= 0:
+            raise ValueError(f"nside must be positive, got {self.nside}")
+
+    def replace(self, **kw):
+        return dataclasses.replace(self, **kw)
+
+    @property
+    def observer_position_mpc(self) -> tuple:
+        return tuple(f * L for f, L in zip(self.observer_position, self.box_size))
+
+    @property
+    def max_comoving_radius(self) -> float:
+        box = np.asarray(self.box_size, dtype=np.float64)
+        fr = np.clip(np.asarray(self.observer_position, dtype=np.float64), 0.0, 1.0)
+        return float(np.min(box / (1.0 + 2.0 * np.minimum(fr, 1.0 - fr))))
+
+    @classmethod
+    def FromDensityMetadata(cls, array, field: "AbstractField", **kw):
+        base = dict(mesh_size=field.mesh_size, box_size=field.box_size, observer_position=field.observer_position,
+                    halo_size=field.halo_size, nside=field.nside, flatsky_npix=field.flatsky_npix,
+                    field_size=field.field_size, status=field.status, unit=field.unit,
+                    scale_factors=field.scale_factors, z_sources=field.z_sources,
+                    comoving_centers=field.comoving_centers, density_width=field.density_width)
+        base.update(kw)
+        return cls(array=array, **base)
+
+    def _meta(self, **kw):
+        d = {f.name: getattr(self, f.name) for f in dataclasses.fields(self) if f.name != "array"}
+        d.update(kw)
+        return d
+
+    def is_batched(self) -> bool:
+        return self.array.ndim > self._core_ndim()
+
+    def _core_ndim(self) -> int:
+        return 3
+
+    def __getitem__(self, key):
+        if not self.is_batched():
+            raise ValueError("indexing requires a batched field")
+        sub = lambda v: v[key] if (isinstance(v, (torch.Tensor, np.ndarray)) and getattr(v, "ndim", 0) >= 1) else v
+        return self.replace(array=self.array[key], scale_factors=sub(self.scale_factors),
+                            z_sources=sub(self.z_sources), comoving_centers=sub(self.comoving_centers),
+                            density_width=sub(self.density_width))
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class PowerSpectrum:
+    """P(k) container (reference power/power_spec.py:20-60)."""
+
+    wavenumber: Any
+    array: Any
+    name: str | None = None
+    scale_factors: Any = None
+
+    @property
+    def spectra(self):
+        return self.array
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class DensityField(AbstractField):
+    def power(self, mesh2: "DensityField" | None = None, *, kedges=None, multipoles=0, los=(0.0, 0.0, 1.0),
+              batch_size=None) -> PowerSpectrum:
+        """P(k) of the mesh (reference fields/density.py:275-318)."""
+        from .power import power as power_fn
+
+        if mesh2 is not None:
+            raise NotImplementedError("cross power spectra are not on the B200 path")
+        k, pk = power_fn(self.array, box_shape=self.box_size, kedges=kedges, multipoles=multipoles, los=los)
+        return PowerSpectrum(wavenumber=k, array=pk, name="pk", scale_factors=self.scale_factors)
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class SphericalDensity(AbstractField):
+    def _core_ndim(self) -> int:
+        return 1
+
+    def angular_cl(self, lmax: int | None = None):
+        """Angular power spectrum of each map (computed on the host)."""
+        from .sht import anafast
+
+        maps = self.array.detach().double().cpu().numpy()
+        if maps.ndim == 1:
+            return anafast(maps, lmax=lmax)
+        return np.stack([anafast(m, lmax=lmax) for m in maps])
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class ParticleField(AbstractField):
+    def _core_ndim(self) -> int:
+        return 4
+
+    def to(self, unit: PositionUnit) -> "ParticleField":
+        """Unit conversion through GRID_ABSOLUTE (reference fields/units.py:78-130)."""
+        if unit == self.unit:
+            return self
+        n = torch.tensor(self.mesh_size, dtype=torch.float32, device=self.array.device)
+        L = torch.tensor(self.box_size, dtype=torch.float32, device=self.array.device)
+        if self.unit == PositionUnit.GRID_ABSOLUTE:
+            grid = self.array
+        elif self.unit == PositionUnit.GRID_RELATIVE:
+            grid = self.array + uniform_particles(self.mesh_size, self.array.device)
+        elif self.unit == PositionUnit.MPC_H:
+            grid = self.array / L * n
+        else:
+            raise ValueError(f"unknown unit {self.unit}")
+        if unit == PositionUnit.GRID_ABSOLUTE:
+            out = grid
+        elif unit == PositionUnit.GRID_RELATIVE:
+            out = grid - uniform_particles(self.mesh_size, self.array.device)
+        elif unit == PositionUnit.MPC_H:
+            out = grid / n * L
+        else:
+            raise ValueError(f"unknown unit {unit}")
+        return self.replace(array=out.contiguous(), unit=unit)
+
+    def _grid_mode(self):
+        if self.unit == PositionUnit.MPC_H:
+            raise ValueError("Cannot paint ParticleField with unit MPC_H; convert to GRID_RELATIVE or GRID_ABSOLUTE first.")
+        return self.unit == PositionUnit.GRID_ABSOLUTE
+
+    def paint(self, *, mesh=None, weights=1.0, chunk_size: int = DEFAULT_CHUNK_SIZE, batch_size=None) -> DensityField:
+        """CIC paint onto the mesh (reference fields/particles.py:119-178)."""
+        absolute = self._grid_mode()
+        w, ws = _weights_arg(weights)
+        out = None
+        acc = False
+        if mesh is not None:
+            out = (mesh.array if isinstance(mesh, AbstractField) else mesh).clone().contiguous()
+            acc = True
+        dens = ops.paint_cic(self.array.contiguous(), absolute=absolute, weights=w, weight=ws, out=out,
+                             accumulate=acc)
+        return DensityField(array=dens, **self._meta_for_density(FieldStatus.DENSITY_FIELD))
+
+    def _meta_for_density(self, status):
+        return dict(mesh_size=self.mesh_size, box_size=self.box_size, observer_position=self.observer_position,
+                    halo_size=self.halo_size, nside=self.nside, flatsky_npix=self.flatsky_npix,
+                    field_size=self.field_size, status=status, scale_factors=self.scale_factors,
+                    unit=DensityUnit.DENSITY)
+
+    def read_out(self, density_mesh) -> DensityField:
+        """CIC interpolation of a mesh at the particle positions (reference fields/particles.py:182-229)."""
+        absolute = self._grid_mode()
+        mesh = density_mesh.array if isinstance(density_mesh, AbstractField) else density_mesh
+        vals = ops.readout_cic(self.array.contiguous(), mesh.contiguous(), absolute=absolute)
+        return DensityField(array=vals, **self._meta_for_density(self.status))
+
+    def paint_spherical(self, center, density_plane_width, *, scheme: str = "bilinear", weights=None,
+                        kernel_width_arcmin=None, smoothing_interpretation="fwhm", paint_nside=None,
+                        ud_grade_power=0.0, ud_grade_order_in="RING", ud_grade_order_out="RING",
+                        ud_grade_pess=False, batch_size=None) -> SphericalDensity:
+        """HEALPix shell painting (reference fields/particles.py:326-442)."""
+        if self.nside is None:
+            raise ValueError("Spherical painting requires `nside`.")
+        if paint_nside is not None and paint_nside != self.nside:
+            raise NotImplementedError("paint_nside / ud_grade are not on the B200 path")
+        if kernel_width_arcmin is not None or scheme == "rbf_neighbor":
+            raise NotImplementedError("rbf_neighbor smoothing is not on the B200 path")
+        from .painting import paint_shells
+
+        centers = np.atleast_1d(np.asarray(center, dtype=np.float64))
+        widths = np.atleast_1d(np.asarray(density_plane_width, dtype=np.float64))
+        if centers.shape != widths.shape:
+            raise ValueError("center and density_plane_width must have the same shape")
+        arr = self.array
+        if arr.ndim == 5:
+            if arr.shape[0] != centers.size:
+                raise ValueError(f"Batched input: center must have {arr.shape[0]} elements")
+            maps = torch.stack([paint_shells(self.replace(array=arr[i]), centers[i:i + 1], widths[i:i + 1], scheme,
+                                             weights)[0] for i in range(arr.shape[0])])
+        else:
+            maps = paint_shells(self, centers, widths, scheme, weights)
+        if maps.shape[0] == 1:
+            maps = maps[0]
+        return SphericalDensity(array=maps, mesh_size=self.mesh_size, box_size=self.box_size,
+                                observer_position=self.observer_position, nside=self.nside,
+                                status=FieldStatus.LIGHTCONE, comoving_centers=centers, density_width=widths,
+                                scale_factors=self.scale_factors, unit=DensityUnit.DENSITY)
+
+
+def uniform_particles(mesh_size, device="cuda") -> torch.Tensor:
+    """Lagrangian grid coordinates (N, N, N, 3) (jaxpm uniform_particles)."""
+    axes = [torch.arange(n, dtype=torch.float32, device=device) for n in mesh_size]
+    g = torch.meshgrid(*axes, indexing="ij")
+    return torch.stack(g, dim=-1)
+
+
+def convert_units(array, origin, destination, mesh_size, box_size, **_):
+    f = ParticleField(array=array, mesh_size=tuple(mesh_size), box_size=tuple(box_size), unit=origin)
+    return f.to(destination).array

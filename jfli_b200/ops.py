@@ -1,0 +1,225 @@
+"""Tensor-level wrappers around the C-ABI kernels.
+
+Every function takes CUDA float32 tensors (a leading batch dimension is optional),
+enqueues the library's kernels on torch's current stream and returns new tensors or
+fills the ones given. Shapes:
+
+* mesh       (..., nx, ny, nz)
+* particles  (..., nx, ny, nz, 3)
+* spectrum   (..., nx, ny, nz//2+1) complex64
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr, query, stream_ptr
+
+_workspaces: dict[tuple, torch.Tensor] = {}
+
+
+def workspace(nbytes: int, key: str = "default", device=None) -> torch.Tensor:
+    """A cached uint8 device buffer of at least `nbytes` (one per key and device)."""
+    dev = torch.device("cuda") if device is None else torch.device(device)
+    k = (key, dev.index if dev.index is not None else torch.cuda.current_device())
+    buf = _workspaces.get(k)
+    if buf is None or buf.numel() < nbytes:
+        buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)
+        _workspaces[k] = buf
+    return buf
+
+
+def release_workspaces():
+    _workspaces.clear()
+
+
+def _mesh_dims(t: torch.Tensor, particle: bool):
+    shape = tuple(t.shape)
+    core = shape[-4:-1] if particle else shape[-3:]
+    if len(core) != 3:
+        raise ValueError(f"bad {'particle' if particle else 'mesh'} tensor shape {shape}")
+    lead = shape[:-4] if particle else shape[:-3]
+    batch = int(np.prod(lead)) if lead else 1
+    return tuple(int(v) for v in core), batch, lead
+
+
+def _check(t: torch.Tensor, name: str, dtype=torch.float32):
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+def mesh_supported(nx: int, ny: int, nz: int) -> bool:
+    return bool(query("jfli_mesh_supported", nx, ny, nz))
+
+
+def rfft3d(mesh: torch.Tensor) -> torch.Tensor:
+    _check(mesh, "mesh")
+    (nx, ny, nz), batch, lead = _mesh_dims(mesh, False)
+    spec = torch.empty(*lead, nx, ny, nz // 2 + 1, dtype=torch.complex64, device=mesh.device)
+    call("jfli_rfft3d", stream_ptr(), ptr(mesh), ptr(spec), nx, ny, nz, batch)
+    return spec
+
+
+def irfft3d(spec: torch.Tensor, nz: int) -> torch.Tensor:
+    """Inverse of rfft3d; the spectrum is copied first (the kernel overwrites its input)."""
+    if spec.dtype != torch.complex64:
+        raise TypeError("spec must be complex64")
+    work = spec.contiguous().clone()
+    nx, ny = int(spec.shape[-3]), int(spec.shape[-2])
+    lead = tuple(spec.shape[:-3])
+    batch = int(np.prod(lead)) if lead else 1
+    out = torch.empty(*lead, nx, ny, nz, dtype=torch.float32, device=spec.device)
+    call("jfli_irfft3d", stream_ptr(), ptr(work), ptr(out), nx, ny, nz, batch)
+    return out
+
+
+def paint_cic(pos: torch.Tensor, *, absolute: bool = False, weights: torch.Tensor | None = None,
+              weight: float = 1.0, out: torch.Tensor | None = None, accumulate: bool = False) -> torch.Tensor:
+    _check(pos, "pos")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    if weights is not None:
+        _check(weights, "weights")
+        if tuple(weights.shape) != tuple(pos.shape[:-1]):
+            raise ValueError("weights must have the particle grid shape")
+    if out is None:
+        out = torch.empty(*lead, nx, ny, nz, dtype=torch.float32, device=pos.device)
+        accumulate = False
+    call("jfli_paint_cic", stream_ptr(), ptr(pos), int(absolute), ptr(weights), float(weight), ptr(out),
+         int(accumulate), nx, ny, nz, batch)
+    return out
+
+
+def readout_cic(pos: torch.Tensor, mesh: torch.Tensor, *, absolute: bool = False) -> torch.Tensor:
+    _check(pos, "pos")
+    _check(mesh, "mesh")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    if tuple(mesh.shape[-3:]) != (nx, ny, nz):
+        raise ValueError("mesh and particle grid shapes differ")
+    out = torch.empty(*lead, nx, ny, nz, dtype=torch.float32, device=pos.device)
+    call("jfli_readout_cic", stream_ptr(), ptr(pos), int(absolute), ptr(mesh), ptr(out), nx, ny, nz, batch)
+    return out
+
+
+def poisson_potential(rho: torch.Tensor, rho_mean: float = 0.0, out: torch.Tensor | None = None) -> torch.Tensor:
+    _check(rho, "rho")
+    (nx, ny, nz), batch, lead = _mesh_dims(rho, False)
+    if out is None:
+        out = torch.empty_like(rho)
+    nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "spec", rho.device)
+    call("jfli_poisson_potential", stream_ptr(), ptr(rho), float(rho_mean), ptr(out), ptr(ws), ws.numel(), nx, ny,
+         nz, batch)
+    return out
+
+
+def readout_gradient(pos: torch.Tensor, pot: torch.Tensor, *, absolute: bool = False, scale: float = 1.0,
+                     out: torch.Tensor | None = None) -> torch.Tensor:
+    _check(pos, "pos")
+    _check(pot, "pot")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    if out is None:
+        out = torch.empty_like(pos)
+    call("jfli_readout_gradient", stream_ptr(), ptr(pos), int(absolute), ptr(pot), float(scale), ptr(out), nx, ny,
+         nz, batch)
+    return out
+
+
+def pm_forces(pos: torch.Tensor, *, absolute: bool = False, scale: float = 1.0) -> torch.Tensor:
+    """paint -> Poisson -> -grad_FD -> readout, times `scale` (jax-fli _forces: 1.5 Omega_m)."""
+    _check(pos, "pos")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    out = torch.empty_like(pos)
+    nb = query("jfli_pm_forces_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "forces", pos.device)
+    call("jfli_pm_forces", stream_ptr(), ptr(pos), int(absolute), float(scale), ptr(out), ptr(ws), ws.numel(), nx,
+         ny, nz, batch)
+    return out
+
+
+def kick_drift_paint(disp: torch.Tensor, vel: torch.Tensor, pot: torch.Tensor | None, kick: float, drift: float,
+                     flags: int, rho: torch.Tensor | None = None, weight: float = 1.0) -> None:
+    _check(disp, "disp")
+    _check(vel, "vel")
+    (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
+    call("jfli_kick_drift_paint", stream_ptr(), ptr(disp), ptr(vel), ptr(pot), float(kick), float(drift), int(flags),
+         float(weight), ptr(rho), nx, ny, nz, batch)
+
+
+def pm_step(disp, vel, kick, drift, flags, rho, pot) -> None:
+    (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
+    nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "spec", disp.device)
+    call("jfli_pm_step", stream_ptr(), ptr(disp), ptr(vel), float(kick), float(drift), int(flags), ptr(rho), ptr(pot),
+         ptr(ws), ws.numel(), nx, ny, nz, batch)
+
+
+def ic_filter(noise: torch.Tensor, ktab: torch.Tensor, ptab: torch.Tensor, box_size, *,
+              zero_mode_one: bool = False) -> torch.Tensor:
+    _check(noise, "noise")
+    _check(ktab, "ktab")
+    _check(ptab, "ptab")
+    (nx, ny, nz), batch, lead = _mesh_dims(noise, False)
+    out = torch.empty_like(noise)
+    nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "spec", noise.device)
+    lx, ly, lz = (float(v) for v in box_size)
+    call("jfli_ic_filter", stream_ptr(), ptr(noise), ptr(out), ptr(ktab), ptr(ptab), int(ktab.numel()), lx, ly, lz,
+         int(zero_mode_one), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return out
+
+
+def lpt(ic: torch.Tensor, order: int, c1x: float, c2x: float, c1p: float, c2p: float):
+    _check(ic, "ic")
+    (nx, ny, nz), batch, lead = _mesh_dims(ic, False)
+    dx = torch.empty(*lead, nx, ny, nz, 3, dtype=torch.float32, device=ic.device)
+    p = torch.empty_like(dx)
+    nb = query("jfli_lpt_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "lpt", ic.device)
+    call("jfli_lpt", stream_ptr(), ptr(ic), int(order), float(c1x), float(c2x), float(c1p), float(c2p), ptr(dx),
+         ptr(p), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return dx, p
+
+
+def power_sums(mesh: torch.Tensor, kedges: torch.Tensor, box_size) -> torch.Tensor:
+    """(..., 3, nedges+1) float64 sums: |delta_k|^2, mode count, |k| per digitize bin."""
+    _check(mesh, "mesh")
+    _check(kedges, "kedges")
+    (nx, ny, nz), batch, lead = _mesh_dims(mesh, False)
+    ne = int(kedges.numel())
+    out = torch.empty(*lead, 3, ne + 1, dtype=torch.float64, device=mesh.device)
+    nb = query("jfli_power_spectrum_workspace_bytes", nx, ny, nz, batch, ne)
+    ws = workspace(nb, "power", mesh.device)
+    lx, ly, lz = (float(v) for v in box_size)
+    call("jfli_power_spectrum", stream_ptr(), ptr(mesh), ptr(kedges), ne, lx, ly, lz, ptr(out), ptr(ws), ws.numel(),
+         nx, ny, nz, batch)
+    return out
+
+
+def healpix_paint(pos: torch.Tensor, nside: int, box_size, observer_mpc, rmin: float, rmax: float, *,
+                  scheme: str = "bilinear", absolute: bool = False, weights: torch.Tensor | None = None,
+                  weight: float = 1.0, out: torch.Tensor | None = None, accumulate: bool = False) -> torch.Tensor:
+    _check(pos, "pos")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    sch = {"ngp": _lib.JFLI_HEALPIX_NGP, "bilinear": _lib.JFLI_HEALPIX_BILINEAR}.get(scheme)
+    if sch is None:
+        raise NotImplementedError(f"spherical painting scheme {scheme!r} is not implemented (ngp, bilinear)")
+    if out is None:
+        out = torch.empty(*lead, 12 * nside * nside, dtype=torch.float32, device=pos.device)
+        accumulate = False
+    lx, ly, lz = (float(v) for v in box_size)
+    ox, oy, oz = (float(v) for v in observer_mpc)
+    call("jfli_healpix_paint", stream_ptr(), ptr(pos), int(absolute), ptr(weights), float(weight), lx, ly, lz, ox,
+         oy, oz, float(rmin), float(rmax), int(nside), sch, ptr(out), int(accumulate), nx, ny, nz, batch)
+    return out
+
+
+def launch_count() -> int:
+    return _lib.launch_count()

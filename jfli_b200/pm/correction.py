@@ -1,0 +1,94 @@
+"""Sub-grid corrections (reference pm/correction.py:25-333)."""
+
+from __future__ import annotations
+
+import dataclasses
+
+import torch
+
+from .. import ops
+from .._lib import JFLI_STEP_CORRECT, JFLI_STEP_PAINT
+
+
+class AbstractCorrection:
+    reversible: bool = True
+
+    def apply(self, t, pos, vel, full_drift_factor):
+        raise NotImplementedError
+
+    def rewind(self, t, pos, vel, full_drift_factor):
+        raise NotImplementedError
+
+
+@dataclasses.dataclass(frozen=True)
+class NoCorrection(AbstractCorrection):
+    @property
+    def reversible(self) -> bool:
+        return True
+
+    def apply(self, t, pos, vel, full_drift_factor):
+        return pos, vel
+
+    def rewind(self, t, pos, vel, full_drift_factor):
+        return pos, vel
+
+
+@dataclasses.dataclass(frozen=True)
+class PGDKernel(AbstractCorrection):
+    """Potential-gradient-descent position correction (reference pm/correction.py:130-202):
+    x += alpha * F_pgd(x), F_pgd the FD-gradient force of the potential filtered by
+    exp(-kl^2/k^2) exp(-k^4/ks^4), k in radians per cell."""
+
+    alpha: float = 0.2
+    kl: float = 0.3
+    ks: float = 1.0
+
+    @property
+    def reversible(self) -> bool:
+        return False
+
+    def pgd_potential(self, rho: torch.Tensor, rho_mean: float = 1.0) -> torch.Tensor:
+        return pgd_potential(rho, self.kl, self.ks, rho_mean)
+
+    def apply(self, t, pos, vel, full_drift_factor):
+        from ..fields import PositionUnit
+
+        if pos.unit != PositionUnit.GRID_RELATIVE:
+            pos = pos.to(PositionUnit.GRID_RELATIVE)
+        x = pos.array.contiguous().clone()
+        rho = ops.paint_cic(x)
+        pot = pgd_potential(rho, self.kl, self.ks, 1.0)
+        dummy_v = torch.empty_like(x)
+        ops.kick_drift_paint(x, dummy_v, pot, self.alpha, 0.0, JFLI_STEP_CORRECT)
+        return pos.replace(array=x), vel
+
+    def rewind(self, t, pos, vel, full_drift_factor):
+        raise NotImplementedError("PGDKernel is not reversible")
+
+
+@dataclasses.dataclass(frozen=True)
+class SharpeningKernel(AbstractCorrection):
+    """Velocity sharpening (reference pm/correction.py:205-333); not on the B200 path."""
+
+    @property
+    def reversible(self) -> bool:
+        return True
+
+    def apply(self, t, pos, vel, full_drift_factor):
+        raise NotImplementedError("SharpeningKernel is not on the B200 path")
+
+    def rewind(self, t, pos, vel, full_drift_factor):
+        raise NotImplementedError("SharpeningKernel is not on the B200 path")
+
+
+def pgd_potential(rho: torch.Tensor, kl: float, ks: float, rho_mean: float = 1.0) -> torch.Tensor:
+    from .._lib import call, ptr, query, stream_ptr
+
+    (nx, ny, nz) = tuple(rho.shape[-3:])
+    batch = rho.numel() // (nx * ny * nz)
+    out = torch.empty_like(rho)
+    nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
+    ws = ops.workspace(nb, "spec", rho.device)
+    call("jfli_pgd_potential", stream_ptr(), ptr(rho), float(rho_mean), float(kl), float(ks), ptr(out), ptr(ws),
+         ws.numel(), nx, ny, nz, batch)
+    return out

@@ -1,0 +1,198 @@
+"""Time integration (reference pm/integrate.py:17-279).
+
+The loop structure is the reference's: an outer scan over the snapshot times `ts`, an
+inner loop of `dt0` steps clipped to each snapshot time (tolerance 1e-6 for FP32 state,
+1e-10 for FP64), `solver.save_at` after each inner loop.
+
+On the GPU the loop runs as fused particle passes. With the FastPM KDK scheme the kick
+that ends step n and the drift that starts step n+1 read and write the particles once:
+
+    paint(x0) -> Poisson
+    for each step: [kick(prev) + drift + paint]  -> Poisson      (one particle pass)
+    final kick
+
+and with the reversible KKD scheme each step is [kick + drift + paint] -> Poisson. The
+density painted for the force at a snapshot time is the snapshot's density, so a
+"density" snapshot is a copy of that mesh.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Any
+
+import numpy as np
+import torch
+
+from .. import ops
+from .._lib import JFLI_STEP_CORRECT, JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
+from ..fields import ParticleField, PositionUnit
+from .correction import NoCorrection, PGDKernel, pgd_potential
+from .solvers import AbstractNBodySolver, EfficientDriftDoubleKick, NBodyState, ReversibleDoubleKickDrift
+
+
+def _clip_to_end(t_next, t1, tol):
+    return t1 if t_next > t1 - tol else t_next
+
+
+def time_events(t0: float, ts, dt0: float, dtype=np.float32):
+    """Events of the reference loop: ("step", t_curr, t_next) and ("save", i, t_target).
+
+    Times are accumulated in `dtype` (the precision of the reference's time variables)."""
+    dt = np.dtype(dtype).type
+    tol = 1e-10 if np.dtype(dtype) == np.float64 else 1e-6
+    events = []
+    t = dt(t0)
+    for i, target in enumerate(np.atleast_1d(np.asarray(ts, dtype=np.float64))):
+        tgt = dt(target)
+        while t < tgt:
+            tn = dt(t + dt(dt0))
+            tn = _clip_to_end(tn, tgt, tol)
+            events.append(("step", float(t), float(tn)))
+            t = tn
+        events.append(("save", i, float(tgt)))
+    return events
+
+
+@dataclasses.dataclass
+class RunResult:
+    snapshots: list
+    disp: torch.Tensor
+    vel: torch.Tensor
+    steps: int
+
+
+def _scalar_weight(w):
+    if w is None:
+        return 1.0
+    if isinstance(w, (int, float)):
+        return float(w)
+    if isinstance(w, torch.Tensor) and w.ndim == 0:
+        return float(w)
+    return None
+
+
+def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, cosmo, ts, t0: float, dt0: float,
+              dtype=np.float32) -> RunResult:
+    """Run the loop with fused particle passes; returns the snapshots and final state."""
+    efficient = isinstance(solver, EfficientDriftDoubleKick)
+    if not efficient and not isinstance(solver, ReversibleDoubleKickDrift):
+        raise NotImplementedError(f"{type(solver).__name__} has no fused GPU schedule")
+    pgd = solver.pgd_kernel if (efficient and isinstance(solver.pgd_kernel, PGDKernel)) else None
+    if not isinstance(solver.pgd_kernel, (NoCorrection, PGDKernel)):
+        raise NotImplementedError(f"{type(solver.pgd_kernel).__name__} is not on the B200 path")
+    interp = solver.interp_kernel
+    if dx.unit != PositionUnit.GRID_RELATIVE:
+        dx = dx.to(PositionUnit.GRID_RELATIVE)
+    x = dx.array.contiguous().clone()
+    v = p.array.contiguous().clone()
+    rho = torch.empty(x.shape[:-1], dtype=torch.float32, device=x.device)
+    pot = torch.empty_like(rho)
+    events = time_events(t0, ts, dt0, dtype)
+    n_steps = sum(1 for e in events if e[0] == "step")
+    state = NBodyState(interp_state=interp.init(), t_initial=t0)
+
+    tgt = interp.painting.target if interp.painting is not None else "particles"
+    w_snap = _scalar_weight(interp.painting.weights) if interp.painting is not None else 1.0
+    density_from_force_mesh = tgt == "density" and w_snap == 1.0
+
+    # force at the initial positions
+    rho.zero_()
+    ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT, rho)
+    ops.poisson_potential(rho, 1.0, out=pot)
+    pending = EfficientDriftDoubleKick.init_kick(cosmo, t0, t0 + dt0) if efficient else None
+    rho_is_current = True  # rho holds the paint of the current positions
+
+    snapshots = []
+    step_i = 0
+    for ev in events:
+        if ev[0] == "step":
+            _, ta, tb = ev
+            step_i += 1
+            c = solver.step_coefficients(cosmo, ta, tb, dt0, t0)
+            rho.zero_()
+            if efficient:
+                flags = JFLI_STEP_DRIFT | JFLI_STEP_PAINT
+                kick = 0.0
+                if pending is not None:
+                    flags |= JFLI_STEP_KICK
+                    kick = pending
+                if pgd is not None:
+                    ops.kick_drift_paint(x, v, pot, kick, c.drift, flags, rho)
+                    ppot = pgd_potential(rho, pgd.kl, pgd.ks, 1.0)
+                    rho.zero_()
+                    ops.kick_drift_paint(x, v, ppot, pgd.alpha, 0.0, JFLI_STEP_CORRECT | JFLI_STEP_PAINT, rho)
+                else:
+                    ops.kick_drift_paint(x, v, pot, kick, c.drift, flags, rho)
+                ops.poisson_potential(rho, 1.0, out=pot)
+                pending = c.kick
+            else:
+                ops.kick_drift_paint(x, v, pot, c.kick, c.drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
+                                     rho)
+                if step_i < n_steps:
+                    ops.poisson_potential(rho, 1.0, out=pot)
+            rho_is_current = True
+            state = NBodyState(interp_state=interp.advance(state.interp_state, tb), t_initial=t0)
+        else:
+            _, i, t_target = ev
+            if efficient and pending is not None and interp.needs_velocity():
+                ops.kick_drift_paint(x, v, pot, pending, 0.0, JFLI_STEP_KICK)
+                pending = None
+            xf = dx.replace(array=x, scale_factors=t_target)
+            vf = p.replace(array=v, scale_factors=t_target)
+            if density_from_force_mesh and rho_is_current and not interp.needs_velocity():
+                from ..fields import DensityField, DensityUnit, FieldStatus
+
+                snap = DensityField(array=rho.clone(), **xf._meta_for_density(FieldStatus.DENSITY_FIELD))
+                r_center = float(interp.r_centers[state.interp_state.shell_idx])
+                width = float(interp.density_widths[state.interp_state.shell_idx])
+                snap = snap.replace(scale_factors=t_target, comoving_centers=r_center, density_width=width)
+            else:
+                snap = solver.save_at(xf, vf, t_target, dt0, state, cosmo)
+                if tgt == "particles":
+                    snap = snap.replace(array=snap.array.clone())
+            snapshots.append(snap)
+    if efficient and pending is not None:
+        ops.kick_drift_paint(x, v, pot, pending, 0.0, JFLI_STEP_KICK)
+    return RunResult(snapshots=snapshots, disp=x, vel=v, steps=n_steps)
+
+
+def run_stepwise(solver, dx, p, cosmo, ts, t0, dt0, dtype=np.float32) -> RunResult:
+    """The reference loop driven through solver.init/step/save_at (unfused)."""
+    disp, vel, state = solver.init(dx, p, t0, t0 + dt0, dt0, cosmo)
+    snapshots = []
+    n = 0
+    for ev in time_events(t0, ts, dt0, dtype):
+        if ev[0] == "step":
+            disp, vel, state = solver.step(disp, vel, ev[1], ev[2], dt0, state, cosmo)
+            n += 1
+        else:
+            snapshots.append(solver.save_at(disp, vel, ev[2], dt0, state, cosmo))
+    return RunResult(snapshots=snapshots, disp=disp.array, vel=vel.array, steps=n)
+
+
+def _stack(snapshots):
+    first = snapshots[0]
+    arr = torch.stack([s.array for s in snapshots])
+    meta = {}
+    for key in ("scale_factors", "comoving_centers", "density_width"):
+        vals = [getattr(s, key) for s in snapshots]
+        meta[key] = None if any(v is None for v in vals) else np.asarray([float(np.asarray(v).reshape(-1)[0])
+                                                                         for v in vals])
+    return first.replace(array=arr, **meta)
+
+
+def integrate(displacements, velocities, cosmo, ts, solver, t0, t1, dt0, adjoint="checkpointed", checkpoints=None,
+              fused: bool = True):
+    """Snapshots at each time in ts (reference pm/integrate.py:55-118), stacked on axis 0."""
+    if adjoint == "reverse" and not solver.pgd_kernel.reversible:
+        raise ValueError(
+            f"Cannot use adjoint='reverse' with {type(solver.pgd_kernel).__name__}. "
+            f"Use SharpeningKernel for reversible integration, or use adjoint='checkpointed'.")
+    if adjoint not in ("checkpointed", "reverse", "lax"):
+        raise ValueError(f"Unknown adjoint type: {adjoint}")
+    run = run_fused if fused else run_stepwise
+    res = run(solver, displacements, velocities, cosmo, ts, t0, dt0)
+    out = _stack(res.snapshots)
+    return out, res

@@ -1,0 +1,166 @@
+"""N-body steppers (reference pm/solvers.py:35-411).
+
+Time-step coefficients are computed in FP64 on the host from the growth tables
+(`jfli_b200.cosmology`) and passed to the kernels as FP32 scalars. Each solver exposes
+
+* the reference's per-step protocol `init / step / save_at / reverse`, implemented with
+  the B200 kernels, for callers that drive the loop themselves; and
+* `init_coefficients / step_coefficients`, which `integrate` uses to run the whole loop
+  as fused particle passes (kick of one step + drift of the next + paint in one kernel).
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Any
+
+import torch
+
+from .. import cosmology as cj
+from .. import ops
+from .._lib import JFLI_STEP_DRIFT, JFLI_STEP_KICK
+from ..fields import PositionUnit
+from .correction import AbstractCorrection, NoCorrection, PGDKernel
+from .interp import AbstractInterp, InterpTilerState
+
+
+@dataclasses.dataclass(frozen=True)
+class NBodyState:
+    interp_state: InterpTilerState
+    t_initial: float
+
+
+def _forces_potential(x: torch.Tensor) -> torch.Tensor:
+    rho = ops.paint_cic(x)
+    return ops.poisson_potential(rho, rho_mean=1.0)
+
+
+def _rel(field):
+    return field if field.unit == PositionUnit.GRID_RELATIVE else field.to(PositionUnit.GRID_RELATIVE)
+
+
+@dataclasses.dataclass(frozen=True)
+class StepCoefficients:
+    """One step's scalars. kick multiplies F = -grad_FD(pot) (1.5 Omega_m included)."""
+
+    kick: float
+    drift: float
+    kick_first: bool  # True: force at the current position, then drift (reversible KKD)
+
+
+@dataclasses.dataclass(frozen=True)
+class AbstractNBodySolver:
+    interp_kernel: AbstractInterp
+    pgd_kernel: AbstractCorrection = NoCorrection()
+
+    def init(self, displacement, velocities, t0, t1, dt, cosmo):
+        raise NotImplementedError
+
+    def step(self, displacement, velocities, t0, t1, dt, state, cosmo):
+        raise NotImplementedError
+
+    def save_at(self, displacement, velocities, t1, dt, state, cosmo):
+        return self.interp_kernel.paint(state.interp_state, t1, (displacement, velocities), cosmo)
+
+    def reverse(self, displacement, velocities, t0, t1, dt, state, cosmo):
+        raise NotImplementedError(f"{type(self).__name__} is not reversible.")
+
+
+@dataclasses.dataclass(frozen=True)
+class EfficientDriftDoubleKick(AbstractNBodySolver):
+    """FastPM KDK scheme (reference pm/solvers.py:118-225)."""
+
+    @staticmethod
+    def init_kick(cosmo, t0, t1) -> float:
+        t0t1 = math.sqrt(t0 * t1)
+        ai, ac, af = t0, t0, t0t1
+        kf = (cj.Gf(cosmo, af) - cj.Gf(cosmo, ai)) / cj.dGfa(cosmo, ac)
+        return float(1.5 * cosmo.Omega_m * kf / (ac**2 * cj.E(cosmo, ac)))
+
+    @staticmethod
+    def step_coefficients(cosmo, t0, t1, dt, t_initial=None) -> StepCoefficients:
+        t0t1 = math.sqrt(t0 * t1)
+        ai, ac, af = t0, t0t1, t1
+        drift = (cj.Gp(cosmo, af) - cj.Gp(cosmo, ai)) / cj.gp(cosmo, ac) / (ac**3 * cj.E(cosmo, ac))
+        t2 = t1 + dt
+        t1t2 = math.sqrt(t1 * t2)
+        ac = t1
+        k1 = (cj.Gf(cosmo, t1) - cj.Gf(cosmo, t0t1)) / cj.dGfa(cosmo, ac)
+        k2 = (cj.Gf(cosmo, t1t2) - cj.Gf(cosmo, t1)) / cj.dGfa(cosmo, ac)
+        kick = 1.5 * cosmo.Omega_m * (k1 + k2) / (ac**2 * cj.E(cosmo, ac))
+        return StepCoefficients(kick=float(kick), drift=float(drift), kick_first=False)
+
+    def init(self, displacement, velocities, t0, t1, dt, cosmo):
+        state = NBodyState(interp_state=self.interp_kernel.init(), t_initial=t0)
+        x = _rel(displacement).array.contiguous()
+        v = velocities.array.contiguous().clone()
+        pot = _forces_potential(x)
+        ops.kick_drift_paint(x, v, pot, self.init_kick(cosmo, t0, t1), 0.0, JFLI_STEP_KICK)
+        return displacement, velocities.replace(array=v, scale_factors=math.sqrt(t0 * t1)), state
+
+    def step(self, displacement, velocities, t0, t1, dt, state, cosmo):
+        c = self.step_coefficients(cosmo, t0, t1, dt)
+        disp = _rel(displacement)
+        x = disp.array.contiguous().clone()
+        v = velocities.array.contiguous().clone()
+        ops.kick_drift_paint(x, v, None, 0.0, c.drift, JFLI_STEP_DRIFT)
+        xf, vf = self.pgd_kernel.apply(t1, disp.replace(array=x, scale_factors=t1), velocities.replace(array=v),
+                                       full_drift_factor=c.drift)
+        x = xf.array.contiguous()
+        pot = _forces_potential(x)
+        ops.kick_drift_paint(x, v, pot, c.kick, 0.0, JFLI_STEP_KICK)
+        new_state = NBodyState(interp_state=self.interp_kernel.advance(state.interp_state, t1),
+                               t_initial=state.t_initial)
+        return xf.replace(array=x, scale_factors=t1), velocities.replace(array=v, scale_factors=t1), new_state
+
+
+@dataclasses.dataclass(frozen=True)
+class ReversibleDoubleKickDrift(AbstractNBodySolver):
+    """Reversible KKD scheme (reference pm/solvers.py:228-411). The reverse step undoes the
+    drift with the same growth factor gp the forward step uses, so reverse(step(y)) == y."""
+
+    @staticmethod
+    def step_coefficients(cosmo, t0, t1, dt, t_initial=None) -> StepCoefficients:
+        t_prev = max(t0 - dt, t_initial if t_initial is not None else t0)
+        ai_1 = math.sqrt(t_prev * t0)
+        af_2 = math.sqrt(t0 * t1)
+        k1 = (cj.Gf(cosmo, t0) - cj.Gf(cosmo, ai_1)) / cj.dGfa(cosmo, t0)
+        k2 = (cj.Gf(cosmo, af_2) - cj.Gf(cosmo, t0)) / cj.dGfa(cosmo, t0)
+        kick = 1.5 * cosmo.Omega_m * (k1 + k2) / (t0**2 * cj.E(cosmo, t0))
+        drift = (cj.Gp(cosmo, t1) - cj.Gp(cosmo, t0)) / cj.gp(cosmo, af_2) / (af_2**3 * cj.E(cosmo, af_2))
+        return StepCoefficients(kick=float(kick), drift=float(drift), kick_first=True)
+
+    def init(self, displacement, velocities, t0, t1, dt, cosmo):
+        return displacement, velocities, NBodyState(interp_state=self.interp_kernel.init(), t_initial=t0)
+
+    def step(self, displacement, velocities, t0, t1, dt, state, cosmo):
+        if isinstance(self.pgd_kernel, PGDKernel):
+            # The reference applies PGD here but then drifts from the uncorrected position,
+            # so the correction has no effect on the trajectory (pm/solvers.py:314-318).
+            pass
+        elif not isinstance(self.pgd_kernel, NoCorrection):
+            raise NotImplementedError(f"{type(self.pgd_kernel).__name__} is not on the B200 path")
+        c = self.step_coefficients(cosmo, t0, t1, dt, state.t_initial)
+        disp = _rel(displacement)
+        x = disp.array.contiguous().clone()
+        v = velocities.array.contiguous().clone()
+        pot = _forces_potential(x)
+        ops.kick_drift_paint(x, v, pot, c.kick, c.drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT)
+        new_state = NBodyState(interp_state=self.interp_kernel.advance(state.interp_state, t1),
+                               t_initial=state.t_initial)
+        return (disp.replace(array=x, scale_factors=t1), velocities.replace(array=v, scale_factors=math.sqrt(t0 * t1)),
+                new_state)
+
+    def reverse(self, displacement, velocities, t0, t1, dt, state, cosmo):
+        c = self.step_coefficients(cosmo, t0, t1, dt, state.t_initial)
+        disp = _rel(displacement)
+        x = disp.array.contiguous().clone()
+        v = velocities.array.contiguous().clone()
+        ops.kick_drift_paint(x, v, None, 0.0, -c.drift, JFLI_STEP_DRIFT)
+        pot = _forces_potential(x)
+        ops.kick_drift_paint(x, v, pot, -c.kick, 0.0, JFLI_STEP_KICK)
+        ts = self.interp_kernel.ts
+        t1c = min(t1, float(ts[-1])) if ts is not None else t1
+        prev = NBodyState(interp_state=self.interp_kernel.rewind(state.interp_state, t1c), t_initial=state.t_initial)
+        return disp.replace(array=x, scale_factors=t0), velocities.replace(array=v), prev

@@ -1,0 +1,276 @@
+"""CPU oracle for the particle-mesh path — TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import this
+module, and only as the checker; the product (jfli_b200) never imports it.
+
+NumPy/SciPy restatement, in FP64 (default) or FP32, of the algorithm the reference runs
+through its un-vendored JaxPM fork (jaxpm @ ALL-MODIF, pyproject.toml:32), written from
+the published method and the reference's call sites:
+
+* cic_paint_dx / cic_read_dx     <- _src/fields/_painting.py:67, fields/particles.py:203
+* pm_forces                      <- pm/solvers.py:19-32 (k-space: -1/k^2, FD-4 gradient
+                                    i(8 sin k - sin 2k)/6, k = 2 pi fftfreq, one inverse
+                                    complex FFT per force component, CIC readout)
+* lpt (order 1, 2)               <- pm/lpt.py:119 (JaxPM lpt, FastPM momentum)
+* ic_filter                      <- initial.py:167-182, infer/dist.py:43-79
+* power                          <- _src/power/_compute.py:23-119 (full complex FFT,
+                                    norm="ortho", digitize + bincount, [1:-1], prod(L/N))
+* KDK / KKD steps and the loop   <- pm/solvers.py:118-411, pm/integrate.py:17-279
+
+Parity status: the JaxPM fork and jax itself are not installable here, so no output of
+the reference could be generated. The oracle is pinned by the reference's portable
+test statements and by analytic known answers (tests/test_oracle.py): the reversible
+round trip of tests/test_against_fpm.py:177-216, the shell partition invariants of
+tests/test_equal_vol_shells.py, a single plane-wave mode through LPT / forces / P(k)
+with closed-form results, and mass conservation of CIC. Values that only the forks
+define (growth tables, P_lin normalisation) are parity unpinned.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import scipy.fft as sfft
+
+WORKERS = -1
+
+
+# ----------------------------------------------------------------------------------- CIC
+def grid(shape, dtype=np.float64):
+    ax = [np.arange(n, dtype=dtype) for n in shape]
+    return np.stack(np.meshgrid(*ax, indexing="ij"), axis=-1)
+
+
+def _cic_corners(disp, shape, absolute=False):
+    """(indices (P, 8) flat, weights (P, 8)) for positions grid + disp (or absolute)."""
+    dt = disp.dtype
+    pos = disp.reshape(-1, 3)
+    if absolute:
+        base = np.zeros_like(pos, dtype=np.int64)
+        f = np.floor(pos)
+        frac = pos - f
+        ii = f.astype(np.int64)
+    else:
+        g = grid(shape, np.int64).reshape(-1, 3)
+        f = np.floor(pos)
+        frac = (pos - f).astype(dt)
+        ii = g + f.astype(np.int64)
+    n = np.asarray(shape, np.int64)
+    idx = []
+    wts = []
+    one = dt.type(1)
+    for ox, oy, oz in ((0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (1, 0, 1), (0, 1, 1), (1, 1, 1)):
+        o = np.array([ox, oy, oz])
+        c = np.mod(ii + o, n)
+        w = np.ones(pos.shape[0], dtype=dt)
+        for a in range(3):
+            w = w * (frac[:, a] if o[a] else (one - frac[:, a]))
+        idx.append((c[:, 0] * n[1] + c[:, 1]) * n[2] + c[:, 2])
+        wts.append(w)
+    return np.stack(idx, axis=1), np.stack(wts, axis=1)
+
+
+def cic_paint(disp, shape=None, weight=1.0, absolute=False):
+    """Trilinear deposit onto a periodic mesh; positions are grid + disp (relative)."""
+    shape = tuple(disp.shape[:3]) if shape is None else tuple(shape)
+    idx, w = _cic_corners(disp, shape, absolute)
+    if np.ndim(weight) > 0:
+        w = w * np.asarray(weight, dtype=w.dtype).reshape(-1, 1)
+    else:
+        w = w * w.dtype.type(weight)
+    mesh = np.bincount(idx.ravel(), weights=w.ravel(), minlength=int(np.prod(shape)))
+    return mesh.reshape(shape).astype(disp.dtype)
+
+
+def cic_read(mesh, disp, absolute=False):
+    idx, w = _cic_corners(disp, mesh.shape, absolute)
+    vals = mesh.reshape(-1)[idx]
+    return (vals * w).sum(axis=1).reshape(disp.shape[:3]).astype(disp.dtype)
+
+
+# -------------------------------------------------------------------------- k-space kernels
+def fftk(shape, dtype=np.float64):
+    """Wave vectors in radians per cell, broadcastable over the full complex grid."""
+    out = []
+    for i, n in enumerate(shape):
+        k = (2 * np.pi * np.fft.fftfreq(n)).astype(dtype)
+        s = [1, 1, 1]
+        s[i] = n
+        out.append(k.reshape(s))
+    return out
+
+
+def invlaplace(kvec):
+    kk = sum(k**2 for k in kvec)
+    safe = np.where(kk == 0, 1, kk)
+    return np.where(kk == 0, 0, -1 / safe)
+
+
+def gradient_kernel(kvec, i):
+    w = kvec[i]
+    return 1j * (8 * np.sin(w) - np.sin(2 * w)) / 6
+
+
+def _ctype(dtype):
+    return np.complex128 if np.dtype(dtype) == np.float64 else np.complex64
+
+
+def fft3(x):
+    return sfft.fftn(x, workers=WORKERS)
+
+
+def ifft3(x):
+    return sfft.ifftn(x, workers=WORKERS)
+
+
+def potential_k(delta_k, kvec):
+    return delta_k * invlaplace(kvec)
+
+
+def forces_from_delta_k(delta_k, disp, dtype=np.float64):
+    kvec = fftk(delta_k.shape, dtype)
+    pot_k = potential_k(delta_k, kvec)
+    comps = []
+    for i in range(3):
+        f = ifft3(-gradient_kernel(kvec, i) * pot_k).real.astype(dtype)
+        comps.append(cic_read(f, disp))
+    return np.stack(comps, axis=-1)
+
+
+def pm_forces(disp, dtype=np.float64):
+    """-grad_FD laplace^-1 of the CIC density, read out at the particles (no 1.5 Omega_m)."""
+    disp = disp.astype(dtype)
+    rho = cic_paint(disp)
+    return forces_from_delta_k(fft3(rho), disp, dtype)
+
+
+def potential_real(rho, dtype=np.float64):
+    kvec = fftk(rho.shape, dtype)
+    return ifft3(potential_k(fft3(rho.astype(dtype)), kvec)).real.astype(dtype)
+
+
+# ------------------------------------------------------------------------------------ ICs
+def interp_extrap(x, xp, fp):
+    i = np.clip(np.searchsorted(xp, x) - 1, 0, len(xp) - 2)
+    slope = (fp[i + 1] - fp[i]) / (xp[i + 1] - xp[i])
+    return fp[i] + (x - xp[i]) * slope
+
+
+def ic_filter(noise, box, ktab, ptab, zero_mode_one=False, dtype=np.float64):
+    shape = noise.shape
+    field = fft3(noise.astype(dtype))
+    kvec = fftk(shape, dtype)
+    kmesh = np.sqrt(sum((kk / box[i] * shape[i]) ** 2 for i, kk in enumerate(kvec)))
+    pk = interp_extrap(kmesh.ravel(), np.asarray(ktab, dtype), np.asarray(ptab, dtype)).reshape(kmesh.shape)
+    pk = pk * (np.prod(shape) / np.prod(box))
+    if zero_mode_one:
+        pk = np.where(kmesh == 0, 1.0, pk)
+    return ifft3(field * np.sqrt(pk)).real.astype(dtype)
+
+
+# ------------------------------------------------------------------------------------ LPT
+def lpt(ic, c1x, c2x, c1p, c2p, order=1, dtype=np.float64):
+    """JaxPM lpt at the grid points: dx = c1x F1 (+ c2x F2), p = c1p c1x F1 (+ c2p c2x F2)."""
+    ic = ic.astype(dtype)
+    zeros = np.zeros(ic.shape + (3,), dtype)
+    delta_k = fft3(ic)
+    F1 = forces_from_delta_k(delta_k, zeros, dtype)
+    dx = c1x * F1
+    p = c1p * dx
+    if order == 2:
+        kvec = fftk(ic.shape, dtype)
+        pot_k = potential_k(delta_k, kvec)
+        delta2 = 0
+        shear_acc = 0
+        for i in range(3):
+            shear_ii = ifft3(gradient_kernel(kvec, i) ** 2 * pot_k).real
+            delta2 = delta2 + shear_ii * shear_acc
+            shear_acc = shear_acc + shear_ii
+            for j in range(i + 1, 3):
+                delta2 = delta2 - ifft3(gradient_kernel(kvec, i) * gradient_kernel(kvec, j) * pot_k).real ** 2
+        F2 = forces_from_delta_k(fft3(delta2), zeros, dtype)
+        dx2 = c2x * F2
+        dx = dx + dx2
+        p = p + c2p * dx2
+    return dx.astype(dtype), p.astype(dtype)
+
+
+# ------------------------------------------------------------------------------------ P(k)
+def power(mesh, box, kedges):
+    """(kavg, pk) with jax-fli's _power conventions."""
+    shape = mesh.shape
+    meshk = sfft.fftn(mesh.astype(np.float64), norm="ortho", workers=WORKERS)
+    kvec = []
+    for i, (m, b) in enumerate(zip(shape, box)):
+        s = [1, 1, 1]
+        s[i] = m
+        kvec.append((2 * np.pi * m / b) * np.fft.fftfreq(m).reshape(s))
+    kmesh = np.sqrt(sum(k**2 for k in kvec))
+    dig = np.digitize(kmesh.ravel(), kedges)
+    nb = len(kedges) + 1
+    cnt = np.bincount(dig, minlength=nb)
+    kavg = np.bincount(dig, weights=kmesh.ravel(), minlength=nb) / np.where(cnt == 0, 1, cnt)
+    ps = np.bincount(dig, weights=(meshk.real**2 + meshk.imag**2).ravel(), minlength=nb)
+    pk = (ps / np.where(cnt > 0, cnt, 1))[1:-1] * np.prod(np.asarray(box) / np.asarray(shape))
+    return kavg[1:-1], pk
+
+
+# ------------------------------------------------------------------------------- stepping
+def clip_times(t0, ts, dt0, dtype=np.float32):
+    """Step list of pm/integrate.py:_fwd_loop: [(t_curr, t_next)], snapshot after each target."""
+    T = np.dtype(dtype).type
+    tol = 1e-10 if np.dtype(dtype) == np.float64 else 1e-6
+    out = []
+    t = T(t0)
+    for target in np.atleast_1d(ts):
+        tg = T(target)
+        seg = []
+        while t < tg:
+            tn = T(t + T(dt0))
+            if tn > tg - tol:
+                tn = tg
+            seg.append((float(t), float(tn)))
+            t = tn
+        out.append(seg)
+    return out
+
+
+def kdk_run(dx, p, coeffs, dtype=np.float64, snapshot_after=None):
+    """FastPM KDK loop (EfficientDriftDoubleKick): coeffs = dict(init_kick, steps=[(kick, drift)]).
+
+    Returns (x, v, snapshots) with snapshots = densities painted after the listed steps."""
+    x = dx.astype(dtype).copy()
+    v = p.astype(dtype).copy()
+    v += pm_forces(x, dtype) * dtype(coeffs["init_kick"])
+    snaps = []
+    for n, (kick, drift) in enumerate(coeffs["steps"]):
+        x += v * dtype(drift)
+        v += pm_forces(x, dtype) * dtype(kick)
+        if snapshot_after is not None and n in snapshot_after:
+            snaps.append(cic_paint(x))
+    return x, v, snaps
+
+
+def kkd_step(x, v, kick, drift, dtype=np.float64):
+    """One ReversibleDoubleKickDrift step: kick with the force at x, then drift."""
+    v = v + pm_forces(x, dtype) * dtype(kick)
+    x = x + v * dtype(drift)
+    return x, v
+
+
+def kkd_reverse(x, v, kick, drift, dtype=np.float64):
+    x = x - v * dtype(drift)
+    v = v - pm_forces(x, dtype) * dtype(kick)
+    return x, v
+
+
+def kkd_run(dx, p, steps, dtype=np.float64, snapshot_after=None):
+    x = dx.astype(dtype).copy()
+    v = p.astype(dtype).copy()
+    snaps = []
+    for n, (kick, drift) in enumerate(steps):
+        x, v = kkd_step(x, v, kick, drift, dtype)
+        if snapshot_after is not None and n in snapshot_after:
+            snaps.append(cic_paint(x))
+    return x, v, snaps

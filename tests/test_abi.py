@@ -1,0 +1,94 @@
+"""The C-ABI library loads and exports every entry point include/jfli_b200.h declares
+(CPU only: no compute calls)."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "jfli_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(jfli_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from jfli_b200 import _build
+
+    path = _build.LIB
+    if not path.exists():
+        _build.build()
+    return ctypes.CDLL(str(path))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "jfli_pm_forces" in names and "jfli_healpix_paint" in names and len(names) >= 15
+
+
+def test_library_exports_every_declared_symbol(lib):
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, f"symbols declared in the header but not exported: {missing}"
+
+
+def test_binding_covers_header():
+    from jfli_b200 import _lib
+
+    bound = set(_lib.exported_symbols())
+    assert set(declared_functions()) <= bound
+
+
+def test_pure_queries_without_gpu(lib):
+    lib.jfli_mesh_supported.restype = ctypes.c_int
+    assert lib.jfli_mesh_supported(256, 256, 256) == 1
+    assert lib.jfli_mesh_supported(192, 96, 64) == 1
+    assert lib.jfli_mesh_supported(100, 100, 100) == 0  # 5 is not a supported radix
+    assert lib.jfli_mesh_supported(64, 64, 63) == 0  # nz must be even
+    lib.jfli_spectrum_elems.restype = ctypes.c_longlong
+    assert lib.jfli_spectrum_elems(256, 256, 256) == 256 * 256 * 129
+    lib.jfli_version.restype = ctypes.c_char_p
+    assert b"sm_100a" in lib.jfli_version()
+    lib.jfli_pm_forces_workspace_bytes.restype = ctypes.c_size_t
+    assert lib.jfli_pm_forces_workspace_bytes(64, 64, 64, 1) >= 64**3 * 4 + 64 * 64 * 33 * 8
+
+
+def test_argument_errors_are_reported_not_raised(lib):
+    """Bad arguments come back as JFLI_EINVAL with a message; nothing reaches the GPU."""
+    buf = ctypes.create_string_buffer(256)
+    fn = lib.jfli_paint_cic
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_float,
+                   ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_char_p, ctypes.c_size_t]
+    rc = fn(None, None, 0, None, 1.0, None, 0, 8, 8, 8, 1, buf, 256)
+    assert rc == 1 and b"null pointer" in buf.value
+    rc = fn(None, None, 0, None, 1.0, None, 0, 0, 8, 8, 1, buf, 256)
+    assert rc == 1 and b"invalid mesh shape" in buf.value
+
+
+def test_unsupported_fft_shape_reported(lib):
+    buf = ctypes.create_string_buffer(256)
+    fn = lib.jfli_rfft3d
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 4 + [ctypes.c_char_p,
+                                                                                             ctypes.c_size_t]
+    rc = fn(None, ctypes.c_void_p(16), ctypes.c_void_p(16), 100, 64, 64, 1, buf, 256)
+    assert rc == 3 and b"unsupported" in buf.value
+
+
+def test_no_cpu_fallback_in_product():
+    """The product package never imports the oracle and has no CPU compute path."""
+    pkg = os.path.join(ROOT, "jfli_b200")
+    for dirpath, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith(".py"):
+                src = open(os.path.join(dirpath, f)).read()
+                assert "oracle" not in re.sub(r"#.*", "", src).replace('"""', ""), f
