@@ -148,10 +148,12 @@ struct PkOp {
   __device__ float2 apply(float2 v, int kx, int ky, int kz, float* smf, int) const {
     double* bins = reinterpret_cast<double*>(smf);
     const float* edges = reinterpret_cast<const float*>(bins + 3 * (nedges + 1));
-    const float ax = cx * (float)signed_freq(kx, nx);
-    const float ay = cy * (float)signed_freq(ky, ny);
-    const float az = cz * (float)signed_freq(kz, nz);
-    const float kmag = sqrtf(ax * ax + ay * ay + az * az);
+    // |k| with the rounding of the reference's float32 grid: no FMA contraction, sum in
+    // x, y, z order, correctly rounded sqrt (decides the bin of modes on an edge)
+    const float ax = __fmul_rn(cx, (float)signed_freq(kx, nx));
+    const float ay = __fmul_rn(cy, (float)signed_freq(ky, ny));
+    const float az = __fmul_rn(cz, (float)signed_freq(kz, nz));
+    const float kmag = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az)));
     // digitize(right=False): number of edges <= kmag
     int lo = 0, hi = nedges;
     while (lo < hi) {

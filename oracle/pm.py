@@ -197,16 +197,19 @@ def lpt(ic, c1x, c2x, c1p, c2p, order=1, dtype=np.float64):
 
 
 # ------------------------------------------------------------------------------------ P(k)
-def power(mesh, box, kedges):
-    """(kavg, pk) with jax-fli's _power conventions."""
+def power(mesh, box, kedges, kdtype=np.float64):
+    """(kavg, pk) with jax-fli's _power conventions. `kdtype` is the precision of the
+    |k| grid and of the bin edges used by digitize (float32 in the reference's default
+    FP32 mode, which decides the bin of modes that sit exactly on an edge)."""
     shape = mesh.shape
     meshk = sfft.fftn(mesh.astype(np.float64), norm="ortho", workers=WORKERS)
     kvec = []
     for i, (m, b) in enumerate(zip(shape, box)):
         s = [1, 1, 1]
         s[i] = m
-        kvec.append((2 * np.pi * m / b) * np.fft.fftfreq(m).reshape(s))
-    kmesh = np.sqrt(sum(k**2 for k in kvec))
+        kvec.append(kdtype(2 * np.pi * m / b) * np.fft.fftfreq(m).astype(kdtype).reshape(s))
+    kmesh = np.sqrt(sum(k * k for k in kvec)).astype(kdtype)
+    kedges = np.asarray(kedges).astype(kdtype)
     dig = np.digitize(kmesh.ravel(), kedges)
     nb = len(kedges) + 1
     cnt = np.bincount(dig, minlength=nb)

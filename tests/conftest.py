@@ -30,6 +30,10 @@ def cosmo():
 
 
 def rel_l2(a, b):
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
+    """||a - b|| / ||b|| over all elements (complex-aware)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    dt = np.complex128 if (np.iscomplexobj(a) or np.iscomplexobj(b)) else np.float64
+    a = a.astype(dt)
+    b = b.astype(dt)
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
