@@ -50,6 +50,11 @@ bool dims_ok(int nx, int ny, int nz, int batch) {
               "also 2^a 3^b",                                                                               \
               nx, ny, nz)
 
+#define CHECK_STENCIL(nx, ny, nz)                                                                           \
+  if ((nx) < 4 || (ny) < 4 || (nz) < 4)                                                                     \
+  return fail(err, errlen, JFLI_EUNSUPPORTED, "the finite-difference force needs every axis >= 4 cells, got (%d, %d, %d)", \
+              nx, ny, nz)
+
 #define CHECK_PTR(p)                                                                                        \
   if (!(p)) return fail(err, errlen, JFLI_EINVAL, "null pointer argument '%s'", #p)
 
@@ -172,6 +177,7 @@ size_t jfli_pm_forces_workspace_bytes(int nx, int ny, int nz, int batch) {
 int jfli_pm_forces(void* stream, const float* pos, int absolute, float scale, float* forces, void* workspace,
                    size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
   CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
   CHECK_FFT(nx, ny, nz);
   CHECK_PTR(pos);
   CHECK_PTR(forces);
@@ -193,6 +199,7 @@ int jfli_pm_forces(void* stream, const float* pos, int absolute, float scale, fl
 int jfli_readout_gradient(void* stream, const float* pos, int absolute, const float* pot, float scale, float* forces,
                           int nx, int ny, int nz, int batch, char* err, size_t errlen) {
   CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
   CHECK_PTR(pos);
   CHECK_PTR(pot);
   CHECK_PTR(forces);
@@ -213,6 +220,7 @@ int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* po
   if ((flags & (JFLI_STEP_KICK | JFLI_STEP_CORRECT)) && !pot)
     return fail(err, errlen, JFLI_EINVAL, "kick requested without a potential");
   if ((flags & JFLI_STEP_PAINT) && !rho) return fail(err, errlen, JFLI_EINVAL, "paint requested without a mesh");
+  if (flags & (JFLI_STEP_KICK | JFLI_STEP_CORRECT)) CHECK_STENCIL(nx, ny, nz);
   const MeshDims d{nx, ny, nz, batch};
   return cuda_status(jfli::kick_drift_paint(disp, vel, pot, kick, drift, flags, weight, rho, d, (cudaStream_t)stream),
                      err, errlen, "jfli_kick_drift_paint");
@@ -222,6 +230,7 @@ int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift,
                  void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
                  size_t errlen) {
   CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
   CHECK_FFT(nx, ny, nz);
   CHECK_PTR(disp);
   CHECK_PTR(vel);
@@ -272,6 +281,7 @@ size_t jfli_lpt_workspace_bytes(int nx, int ny, int nz, int batch) {
 int jfli_lpt(void* stream, const float* ic, int order, float c1x, float c2x, float c1p, float c2p, float* dx, float* p,
              void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
   CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
   CHECK_FFT(nx, ny, nz);
   CHECK_PTR(ic);
   CHECK_PTR(dx);

@@ -23,81 +23,101 @@ struct Cic1 {
   float w0, w1;
 };
 
-// Relative mode: grid index g plus displacement d.
-__device__ __forceinline__ Cic1 cic_rel(int g, float d, int n) {
+// Particle grid with fast index decomposition; cells < 2^31 so offsets are 32-bit.
+struct PGrid {
+  int nx, ny, nz, yz;
+  unsigned np;
+  FastDiv dyz, dz;
+};
+
+static PGrid make_pgrid(const MeshDims& d) {
+  PGrid g;
+  g.nx = d.nx;
+  g.ny = d.ny;
+  g.nz = d.nz;
+  g.yz = d.ny * d.nz;
+  g.np = (unsigned)d.cells();
+  g.dyz = FastDiv::make((unsigned)g.yz);
+  g.dz = FastDiv::make((unsigned)d.nz);
+  return g;
+}
+
+__device__ __forceinline__ void particle_ijk(const PGrid& g, unsigned p, int& i, int& j, int& k) {
+  const unsigned ii = g.dyz.div(p);
+  const unsigned r = p - ii * (unsigned)g.yz;
+  const unsigned jj = g.dz.div(r);
+  i = (int)ii;
+  j = (int)jj;
+  k = (int)(r - jj * (unsigned)g.nz);
+}
+
+// Relative mode: grid index g plus displacement d (integer part split off first).
+__device__ __forceinline__ Cic1 cic_rel(int gidx, float d, int n) {
   const float f = floorf(d);
-  const float t = d - f;
   Cic1 c;
-  c.w0 = 1.0f - t;
-  c.w1 = t;
-  c.i0 = wrap_index(g + (int)f, n);
-  c.i1 = (c.i0 + 1 == n) ? 0 : c.i0 + 1;
+  c.w1 = d - f;
+  c.w0 = 1.0f - c.w1;
+  int i = gidx + (int)f;
+  if ((unsigned)i >= (unsigned)n) i = wrap_index(i, n);
+  c.i0 = i;
+  c.i1 = (i + 1 == n) ? 0 : i + 1;
   return c;
 }
 
 // Absolute mode: position in grid units.
 __device__ __forceinline__ Cic1 cic_abs(float p, int n) {
   const float f = floorf(p);
-  const float t = p - f;
   Cic1 c;
-  c.w0 = 1.0f - t;
-  c.w1 = t;
-  c.i0 = wrap_index((int)f, n);
-  c.i1 = (c.i0 + 1 == n) ? 0 : c.i0 + 1;
+  c.w1 = p - f;
+  c.w0 = 1.0f - c.w1;
+  int i = (int)f;
+  if ((unsigned)i >= (unsigned)n) i = wrap_index(i, n);
+  c.i0 = i;
+  c.i1 = (i + 1 == n) ? 0 : i + 1;
   return c;
 }
 
-__device__ __forceinline__ void particle_grid(long long p, int ny, int nz, int& i, int& j, int& k) {
-  const long long yz = (long long)ny * nz;
-  i = (int)(p / yz);
-  const long long r = p - (long long)i * yz;
-  j = (int)(r / nz);
-  k = (int)(r - (long long)j * nz);
-}
-
-__device__ __forceinline__ void cic_setup(const float* pos3, long long p, int absolute, const MeshDims& d, Cic1& cx,
+__device__ __forceinline__ void cic_setup(const float* pos3, unsigned p, int absolute, const PGrid& g, Cic1& cx,
                                           Cic1& cy, Cic1& cz) {
   const float px = pos3[0], py = pos3[1], pz = pos3[2];
   if (absolute) {
-    cx = cic_abs(px, d.nx);
-    cy = cic_abs(py, d.ny);
-    cz = cic_abs(pz, d.nz);
+    cx = cic_abs(px, g.nx);
+    cy = cic_abs(py, g.ny);
+    cz = cic_abs(pz, g.nz);
   } else {
     int i, j, k;
-    particle_grid(p, d.ny, d.nz, i, j, k);
-    cx = cic_rel(i, px, d.nx);
-    cy = cic_rel(j, py, d.ny);
-    cz = cic_rel(k, pz, d.nz);
+    particle_ijk(g, p, i, j, k);
+    cx = cic_rel(i, px, g.nx);
+    cy = cic_rel(j, py, g.ny);
+    cz = cic_rel(k, pz, g.nz);
   }
 }
 
-__device__ __forceinline__ long long cell(const MeshDims& d, int x, int y, int z) {
-  return ((long long)x * d.ny + y) * d.nz + z;
-}
-
-__device__ __forceinline__ void deposit(float* mesh, const MeshDims& d, const Cic1& cx, const Cic1& cy,
-                                        const Cic1& cz, float w) {
-  const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
-  const int ix[2] = {cx.i0, cx.i1}, iy[2] = {cy.i0, cy.i1}, iz[2] = {cz.i0, cz.i1};
+__device__ __forceinline__ void deposit(float* mesh, const PGrid& g, const Cic1& cx, const Cic1& cy, const Cic1& cz,
+                                        float w) {
+  const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
+  const float wx[2] = {cx.w0 * w, cx.w1 * w}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
-    for (int b = 0; b < 2; ++b)
+    for (int b = 0; b < 2; ++b) {
+      const float wab = wx[a] * wy[b];
 #pragma unroll
-      for (int c = 0; c < 2; ++c) atomicAdd(mesh + cell(d, ix[a], iy[b], iz[c]), wx[a] * wy[b] * wz[c] * w);
+      for (int c = 0; c < 2; ++c) atomicAdd(mesh + (xo[a] + yo[b] + zo[c]), wab * wz[c]);
+    }
 }
 
-__device__ __forceinline__ float gather(const float* __restrict__ mesh, const MeshDims& d, const Cic1& cx,
+__device__ __forceinline__ float gather(const float* __restrict__ mesh, const PGrid& g, const Cic1& cx,
                                         const Cic1& cy, const Cic1& cz) {
+  const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
   const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
-  const int ix[2] = {cx.i0, cx.i1}, iy[2] = {cy.i0, cy.i1}, iz[2] = {cz.i0, cz.i1};
   float acc = 0.f;
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int b = 0; b < 2; ++b)
 #pragma unroll
-      for (int c = 0; c < 2; ++c) acc += mesh[cell(d, ix[a], iy[b], iz[c])] * (wx[a] * wy[b] * wz[c]);
+      for (int c = 0; c < 2; ++c) acc += __ldg(mesh + (xo[a] + yo[b] + zo[c])) * (wx[a] * wy[b] * wz[c]);
   return acc;
 }
 
@@ -109,14 +129,16 @@ __device__ __forceinline__ void fd_pair(const float* v, float& g0, float& g1) {
 }
 
 // F = -grad_FD(pot) read out with CIC weights at one particle (56 distinct loads).
-__device__ __forceinline__ void gather_force(const float* __restrict__ pot, const MeshDims& d, const Cic1& cx,
+// Needs every axis >= 4 cells (offsets -2..+3 wrap at most once).
+__device__ __forceinline__ void gather_force(const float* __restrict__ pot, const PGrid& g, const Cic1& cx,
                                              const Cic1& cy, const Cic1& cz, float& fx, float& fy, float& fz) {
-  const int x[6] = {wrap_index(cx.i0 - 2, d.nx), wrap_index(cx.i0 - 1, d.nx), cx.i0, cx.i1,
-                    wrap_index(cx.i0 + 2, d.nx), wrap_index(cx.i0 + 3, d.nx)};
-  const int y[6] = {wrap_index(cy.i0 - 2, d.ny), wrap_index(cy.i0 - 1, d.ny), cy.i0, cy.i1,
-                    wrap_index(cy.i0 + 2, d.ny), wrap_index(cy.i0 + 3, d.ny)};
-  const int z[6] = {wrap_index(cz.i0 - 2, d.nz), wrap_index(cz.i0 - 1, d.nz), cz.i0, cz.i1,
-                    wrap_index(cz.i0 + 2, d.nz), wrap_index(cz.i0 + 3, d.nz)};
+  int x[6], y[6], z[6];
+#pragma unroll
+  for (int s = 0; s < 6; ++s) {
+    x[s] = wrap1(cx.i0 + s - 2, g.nx) * g.yz;
+    y[s] = wrap1(cy.i0 + s - 2, g.ny) * g.nz;
+    z[s] = wrap1(cz.i0 + s - 2, g.nz);
+  }
   const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
   float c[2][2][2];
 #pragma unroll
@@ -124,19 +146,20 @@ __device__ __forceinline__ void gather_force(const float* __restrict__ pot, cons
 #pragma unroll
     for (int b = 0; b < 2; ++b)
 #pragma unroll
-      for (int e = 0; e < 2; ++e) c[a][b][e] = __ldg(pot + cell(d, x[2 + a], y[2 + b], z[2 + e]));
+      for (int e = 0; e < 2; ++e) c[a][b][e] = __ldg(pot + (x[2 + a] + y[2 + b] + z[2 + e]));
   float gx = 0.f, gy = 0.f, gz = 0.f;
 #pragma unroll
   for (int b = 0; b < 2; ++b)
 #pragma unroll
     for (int e = 0; e < 2; ++e) {  // x lines
+      const int o = y[2 + b] + z[2 + e];
       float v[6];
-      v[0] = __ldg(pot + cell(d, x[0], y[2 + b], z[2 + e]));
-      v[1] = __ldg(pot + cell(d, x[1], y[2 + b], z[2 + e]));
+      v[0] = __ldg(pot + (x[0] + o));
+      v[1] = __ldg(pot + (x[1] + o));
       v[2] = c[0][b][e];
       v[3] = c[1][b][e];
-      v[4] = __ldg(pot + cell(d, x[4], y[2 + b], z[2 + e]));
-      v[5] = __ldg(pot + cell(d, x[5], y[2 + b], z[2 + e]));
+      v[4] = __ldg(pot + (x[4] + o));
+      v[5] = __ldg(pot + (x[5] + o));
       float g0, g1;
       fd_pair(v, g0, g1);
       gx += wy[b] * wz[e] * (wx[0] * g0 + wx[1] * g1);
@@ -145,13 +168,14 @@ __device__ __forceinline__ void gather_force(const float* __restrict__ pot, cons
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int e = 0; e < 2; ++e) {  // y lines
+      const int o = x[2 + a] + z[2 + e];
       float v[6];
-      v[0] = __ldg(pot + cell(d, x[2 + a], y[0], z[2 + e]));
-      v[1] = __ldg(pot + cell(d, x[2 + a], y[1], z[2 + e]));
+      v[0] = __ldg(pot + (y[0] + o));
+      v[1] = __ldg(pot + (y[1] + o));
       v[2] = c[a][0][e];
       v[3] = c[a][1][e];
-      v[4] = __ldg(pot + cell(d, x[2 + a], y[4], z[2 + e]));
-      v[5] = __ldg(pot + cell(d, x[2 + a], y[5], z[2 + e]));
+      v[4] = __ldg(pot + (y[4] + o));
+      v[5] = __ldg(pot + (y[5] + o));
       float g0, g1;
       fd_pair(v, g0, g1);
       gy += wx[a] * wz[e] * (wy[0] * g0 + wy[1] * g1);
@@ -160,13 +184,14 @@ __device__ __forceinline__ void gather_force(const float* __restrict__ pot, cons
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int b = 0; b < 2; ++b) {  // z lines
+      const int o = x[2 + a] + y[2 + b];
       float v[6];
-      v[0] = __ldg(pot + cell(d, x[2 + a], y[2 + b], z[0]));
-      v[1] = __ldg(pot + cell(d, x[2 + a], y[2 + b], z[1]));
+      v[0] = __ldg(pot + (z[0] + o));
+      v[1] = __ldg(pot + (z[1] + o));
       v[2] = c[a][b][0];
       v[3] = c[a][b][1];
-      v[4] = __ldg(pot + cell(d, x[2 + a], y[2 + b], z[4]));
-      v[5] = __ldg(pot + cell(d, x[2 + a], y[2 + b], z[5]));
+      v[4] = __ldg(pot + (z[4] + o));
+      v[5] = __ldg(pot + (z[5] + o));
       float g0, g1;
       fd_pair(v, g0, g1);
       gz += wx[a] * wy[b] * (wz[0] * g0 + wz[1] * g1);
@@ -178,46 +203,43 @@ __device__ __forceinline__ void gather_force(const float* __restrict__ pot, cons
 
 // ----------------------------------------------------------------------------------
 __global__ void k_paint(const float* __restrict__ pos, int absolute, const float* __restrict__ weights, float weight,
-                        float* __restrict__ mesh, MeshDims d) {
-  const long long np = d.cells();
-  const int b = blockIdx.y;
-  pos += (long long)b * np * 3;
-  mesh += (long long)b * np;
-  if (weights) weights += (long long)b * np;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+                        float* __restrict__ mesh, PGrid g) {
+  const long long b = blockIdx.y;
+  pos += b * g.np * 3;
+  mesh += b * g.np;
+  if (weights) weights += b * g.np;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     Cic1 cx, cy, cz;
-    cic_setup(pos + 3 * p, p, absolute, d, cx, cy, cz);
+    cic_setup(pos + 3ull * p, p, absolute, g, cx, cy, cz);
     const float w = weights ? weights[p] * weight : weight;
-    deposit(mesh, d, cx, cy, cz, w);
+    deposit(mesh, g, cx, cy, cz, w);
   }
 }
 
 __global__ void k_readout(const float* __restrict__ pos, int absolute, const float* __restrict__ mesh,
-                          float* __restrict__ out, MeshDims d) {
-  const long long np = d.cells();
-  const int b = blockIdx.y;
-  pos += (long long)b * np * 3;
-  mesh += (long long)b * np;
-  out += (long long)b * np;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+                          float* __restrict__ out, PGrid g) {
+  const long long b = blockIdx.y;
+  pos += b * g.np * 3;
+  mesh += b * g.np;
+  out += b * g.np;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     Cic1 cx, cy, cz;
-    cic_setup(pos + 3 * p, p, absolute, d, cx, cy, cz);
-    out[p] = gather(mesh, d, cx, cy, cz);
+    cic_setup(pos + 3ull * p, p, absolute, g, cx, cy, cz);
+    out[p] = gather(mesh, g, cx, cy, cz);
   }
 }
 
 __global__ void k_readout_gradient(const float* __restrict__ pos, int absolute, const float* __restrict__ pot,
-                                   float* __restrict__ out, float scale, MeshDims d) {
-  const long long np = d.cells();
-  const int b = blockIdx.y;
-  pos += (long long)b * np * 3;
-  pot += (long long)b * np;
-  out += (long long)b * np * 3;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+                                   float* __restrict__ out, float scale, PGrid g) {
+  const long long b = blockIdx.y;
+  pos += b * g.np * 3;
+  pot += b * g.np;
+  out += b * g.np * 3;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     Cic1 cx, cy, cz;
-    cic_setup(pos + 3 * p, p, absolute, d, cx, cy, cz);
+    cic_setup(pos + 3ull * p, p, absolute, g, cx, cy, cz);
     float fx, fy, fz;
-    gather_force(pot, d, cx, cy, cz, fx, fy, fz);
+    gather_force(pot, g, cx, cy, cz, fx, fy, fz);
     out[3 * p + 0] = fx * scale;
     out[3 * p + 1] = fy * scale;
     out[3 * p + 2] = fz * scale;
@@ -228,21 +250,20 @@ __global__ void k_readout_gradient(const float* __restrict__ pos, int absolute, 
 // current position) -> drift (with the kicked velocity) -> paint (at the new position).
 __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ pot,
                                    float kick, float drift, int flags, float weight, float* __restrict__ rho,
-                                   MeshDims d) {
-  const long long np = d.cells();
-  const int b = blockIdx.y;
-  disp += (long long)b * np * 3;
-  vel += (long long)b * np * 3;
-  if (pot) pot += (long long)b * np;
-  if (rho) rho += (long long)b * np;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+                                   PGrid g) {
+  const long long b = blockIdx.y;
+  disp += b * g.np * 3;
+  vel += b * g.np * 3;
+  if (pot) pot += b * g.np;
+  if (rho) rho += b * g.np;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
-    particle_grid(p, d.ny, d.nz, i, j, k);
+    particle_ijk(g, p, i, j, k);
     float x0 = disp[3 * p + 0], x1 = disp[3 * p + 1], x2 = disp[3 * p + 2];
     if (flags & (kStepKick | kStepCorrect)) {
-      const Cic1 cx = cic_rel(i, x0, d.nx), cy = cic_rel(j, x1, d.ny), cz = cic_rel(k, x2, d.nz);
+      const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
       float fx, fy, fz;
-      gather_force(pot, d, cx, cy, cz, fx, fy, fz);
+      gather_force(pot, g, cx, cy, cz, fx, fy, fz);
       if (flags & kStepKick) {
         vel[3 * p + 0] += fx * kick;
         vel[3 * p + 1] += fy * kick;
@@ -264,8 +285,8 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
       disp[3 * p + 2] = x2;
     }
     if (flags & kStepPaint) {
-      const Cic1 cx = cic_rel(i, x0, d.nx), cy = cic_rel(j, x1, d.ny), cz = cic_rel(k, x2, d.nz);
-      deposit(rho, d, cx, cy, cz, weight);
+      const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
+      deposit(rho, g, cx, cy, cz, weight);
     }
   }
 }
@@ -273,35 +294,35 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
 // F = scale * (-D pot) at every grid point (particles exactly on the grid), optionally
 // accumulated into `out` (AoS [..,3]).
 __global__ void k_grid_gradient(const float* __restrict__ pot, float* __restrict__ out, float scale, int accumulate,
-                                MeshDims d) {
-  const long long np = d.cells();
-  const int b = blockIdx.y;
-  pot += (long long)b * np;
-  out += (long long)b * np * 3;
+                                PGrid g) {
+  const long long b = blockIdx.y;
+  pot += b * g.np;
+  out += b * g.np * 3;
   const float s = 1.0f / 12.0f;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
-    particle_grid(p, d.ny, d.nz, i, j, k);
-    float g[3];
+    particle_ijk(g, p, i, j, k);
+    const int xo = i * g.yz, yo = j * g.nz;
+    float gr[3];
     {
-      const float a = pot[cell(d, wrap_index(i + 1, d.nx), j, k)], bm = pot[cell(d, wrap_index(i - 1, d.nx), j, k)];
-      const float c = pot[cell(d, wrap_index(i + 2, d.nx), j, k)], e = pot[cell(d, wrap_index(i - 2, d.nx), j, k)];
-      g[0] = -(8.0f * (a - bm) - (c - e)) * s;
+      const float a = pot[wrap1(i + 1, g.nx) * g.yz + yo + k], bm = pot[wrap1(i - 1, g.nx) * g.yz + yo + k];
+      const float c = pot[wrap1(i + 2, g.nx) * g.yz + yo + k], e = pot[wrap1(i - 2, g.nx) * g.yz + yo + k];
+      gr[0] = -(8.0f * (a - bm) - (c - e)) * s;
     }
     {
-      const float a = pot[cell(d, i, wrap_index(j + 1, d.ny), k)], bm = pot[cell(d, i, wrap_index(j - 1, d.ny), k)];
-      const float c = pot[cell(d, i, wrap_index(j + 2, d.ny), k)], e = pot[cell(d, i, wrap_index(j - 2, d.ny), k)];
-      g[1] = -(8.0f * (a - bm) - (c - e)) * s;
+      const float a = pot[xo + wrap1(j + 1, g.ny) * g.nz + k], bm = pot[xo + wrap1(j - 1, g.ny) * g.nz + k];
+      const float c = pot[xo + wrap1(j + 2, g.ny) * g.nz + k], e = pot[xo + wrap1(j - 2, g.ny) * g.nz + k];
+      gr[1] = -(8.0f * (a - bm) - (c - e)) * s;
     }
     {
-      const float a = pot[cell(d, i, j, wrap_index(k + 1, d.nz))], bm = pot[cell(d, i, j, wrap_index(k - 1, d.nz))];
-      const float c = pot[cell(d, i, j, wrap_index(k + 2, d.nz))], e = pot[cell(d, i, j, wrap_index(k - 2, d.nz))];
-      g[2] = -(8.0f * (a - bm) - (c - e)) * s;
+      const float a = pot[xo + yo + wrap1(k + 1, g.nz)], bm = pot[xo + yo + wrap1(k - 1, g.nz)];
+      const float c = pot[xo + yo + wrap1(k + 2, g.nz)], e = pot[xo + yo + wrap1(k - 2, g.nz)];
+      gr[2] = -(8.0f * (a - bm) - (c - e)) * s;
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float v = g[a] * scale;
-      out[3 * p + a] = accumulate ? out[3 * p + a] + v : v;
+      const float v = gr[a] * scale;
+      out[3ull * p + a] = accumulate ? out[3ull * p + a] + v : v;
     }
   }
 }
@@ -309,30 +330,30 @@ __global__ void k_grid_gradient(const float* __restrict__ pot, float* __restrict
 // Second-order LPT source from the first-order potential (JaxPM `lpt`, order 2):
 //   delta2 = sum_{i<j} phi_ii phi_jj - phi_ij^2,  phi_ij = D_i D_j phi,
 // with D the same 4-point finite difference (its square is the k-space product
-// gradient_kernel_i * gradient_kernel_j used by the reference).
+// gradient_kernel_i * gradient_kernel_j used by the reference). Needs axes >= 4 cells.
 __constant__ float c_d5[5] = {1.0f / 12.0f, -8.0f / 12.0f, 0.0f, 8.0f / 12.0f, -1.0f / 12.0f};
 
-__global__ void k_lpt2_source(const float* __restrict__ pot, float* __restrict__ out, MeshDims d) {
-  const long long np = d.cells();
-  const int b = blockIdx.y;
-  pot += (long long)b * np;
-  out += (long long)b * np;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    particle_grid(p, d.ny, d.nz, i, j, k);
+__global__ void k_lpt2_source(const float* __restrict__ pot, float* __restrict__ out, PGrid g) {
+  const long long b = blockIdx.y;
+  pot += b * g.np;
+  out += b * g.np;
+  const int n3[3] = {g.nx, g.ny, g.nz};
+  const int st[3] = {g.yz, g.nz, 1};
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    int c3[3];
+    particle_ijk(g, p, c3[0], c3[1], c3[2]);
+    const int base = c3[0] * g.yz + c3[1] * g.nz + c3[2];
     float h[3][3];
-    // diagonal: D_a D_a
+    // diagonal: D_a D_a, offsets -4..4 along axis a
     for (int a = 0; a < 3; ++a) {
+      const int rest = base - c3[a] * st[a];
       float acc = 0.f;
       for (int s = 0; s < 5; ++s) {
         if (s == 2) continue;
         for (int t = 0; t < 5; ++t) {
           if (t == 2) continue;
           const int off = (s - 2) + (t - 2);
-          const int ii = a == 0 ? wrap_index(i + off, d.nx) : i;
-          const int jj = a == 1 ? wrap_index(j + off, d.ny) : j;
-          const int kk = a == 2 ? wrap_index(k + off, d.nz) : k;
-          acc += c_d5[s] * c_d5[t] * pot[cell(d, ii, jj, kk)];
+          acc += c_d5[s] * c_d5[t] * pot[rest + wrap1(c3[a] + off, n3[a]) * st[a]];
         }
       }
       h[a][a] = acc;
@@ -340,16 +361,14 @@ __global__ void k_lpt2_source(const float* __restrict__ pot, float* __restrict__
     // off-diagonal: D_a D_b
     for (int a = 0; a < 3; ++a)
       for (int bb = a + 1; bb < 3; ++bb) {
+        const int rest = base - c3[a] * st[a] - c3[bb] * st[bb];
         float acc = 0.f;
         for (int s = 0; s < 5; ++s) {
           if (s == 2) continue;
+          const int oa = wrap1(c3[a] + s - 2, n3[a]) * st[a];
           for (int t = 0; t < 5; ++t) {
             if (t == 2) continue;
-            int o[3] = {0, 0, 0};
-            o[a] = s - 2;
-            o[bb] = t - 2;
-            acc += c_d5[s] * c_d5[t] *
-                   pot[cell(d, wrap_index(i + o[0], d.nx), wrap_index(j + o[1], d.ny), wrap_index(k + o[2], d.nz))];
+            acc += c_d5[s] * c_d5[t] * pot[rest + oa + wrap1(c3[bb] + t - 2, n3[bb]) * st[bb]];
           }
         }
         h[a][bb] = acc;
@@ -409,14 +428,14 @@ static dim3 particle_grid_dims(long long np, int batch, int threads, int per_sm)
 
 cudaError_t cic_paint(const float* pos, int absolute, const float* weights, float weight, float* mesh,
                       const MeshDims& d, cudaStream_t s) {
-  k_paint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pos, absolute, weights, weight, mesh, d);
+  k_paint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pos, absolute, weights, weight, mesh, make_pgrid(d));
   note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t cic_readout(const float* pos, int absolute, const float* mesh, float* out, const MeshDims& d,
                         cudaStream_t s) {
-  k_readout<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pos, absolute, mesh, out, d);
+  k_readout<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pos, absolute, mesh, out, make_pgrid(d));
   note_launch();
   return cudaGetLastError();
 }
@@ -424,7 +443,7 @@ cudaError_t cic_readout(const float* pos, int absolute, const float* mesh, float
 cudaError_t cic_readout_gradient(const float* pos, int absolute, const float* pot, float* out, float scale,
                                  const MeshDims& d, cudaStream_t s) {
   k_readout_gradient<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pos, absolute, pot, out, scale,
-                                                                                     d);
+                                                                                     make_pgrid(d));
   note_launch();
   return cudaGetLastError();
 }
@@ -432,20 +451,20 @@ cudaError_t cic_readout_gradient(const float* pos, int absolute, const float* po
 cudaError_t kick_drift_paint(float* disp, float* vel, const float* pot, float kick, float drift, int flags,
                              float weight, float* rho, const MeshDims& d, cudaStream_t s) {
   k_kick_drift_paint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(disp, vel, pot, kick, drift,
-                                                                                     flags, weight, rho, d);
+                                                                                     flags, weight, rho, make_pgrid(d));
   note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t grid_gradient(const float* pot, float* out, float scale, int accumulate, const MeshDims& d,
                           cudaStream_t s) {
-  k_grid_gradient<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, out, scale, accumulate, d);
+  k_grid_gradient<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, out, scale, accumulate, make_pgrid(d));
   note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t lpt2_source(const float* pot, float* out, const MeshDims& d, cudaStream_t s) {
-  k_lpt2_source<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, out, d);
+  k_lpt2_source<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, out, make_pgrid(d));
   note_launch();
   return cudaGetLastError();
 }

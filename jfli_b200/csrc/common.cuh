@@ -55,4 +55,36 @@ __device__ __forceinline__ int wrap_index(int i, int n) {
 // Signed frequency index of bin i for an axis of length n (numpy fftfreq * n).
 __device__ __forceinline__ int signed_freq(int i, int n) { return (i < (n + 1) / 2) ? i : i - n; }
 
+// Division of 32-bit unsigned numerators by a fixed divisor d with a multiply-high and
+// shifts (round-up magic number, Granlund & Montgomery 1994).
+struct FastDiv {
+  unsigned d, m, s;
+  static FastDiv make(unsigned d) {
+    FastDiv f;
+    f.d = d;
+    if (d <= 1) {
+      f.m = 0;
+      f.s = 0;
+      return f;
+    }
+    unsigned l = 0;
+    while ((1ull << l) < d) ++l;
+    f.m = (unsigned)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+    f.s = l;
+    return f;
+  }
+  __device__ __forceinline__ unsigned div(unsigned x) const {
+    if (d <= 1) return x;
+    const unsigned t = __umulhi(x, m);
+    return (t + ((x - t) >> 1)) >> (s - 1);
+  }
+};
+
+// Index of one periodic axis shifted by a small offset (|offset| <= n).
+__device__ __forceinline__ int wrap1(int v, int n) {
+  v += (v < 0) ? n : 0;
+  v -= (v >= n) ? n : 0;
+  return v;
+}
+
 }  // namespace jfli

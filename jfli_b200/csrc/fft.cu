@@ -12,9 +12,14 @@
 //   cols(y)^-1
 //   irfft_z  : read the half spectrum, write 4M B real
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 #include "common.cuh"
 #include "fft_engine.cuh"
+#include "fft_reg.cuh"
 #include "internal.h"
 #include "kspace_ops.cuh"
 
@@ -218,6 +223,257 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_x_op(float2* __restrict__ d
   }
 }
 
+// =================================================================================
+// Register-resident passes for the specialised lengths (fft_reg.cuh). Dynamic shared
+// memory: the w_N table, the stage exchange buffer, and (x pass) the operator's space.
+// =================================================================================
+__device__ __forceinline__ long long col_base(const ColGeom& g, int c) {
+  const int o = c / g.hz;
+  return (long long)o * g.outer_stride + (c - o * g.hz);
+}
+
+template <int N, int SIGN>
+__global__ void __launch_bounds__(ColCfg<N>::T) k_cols_reg(float2* __restrict__ data, ColGeom g,
+                                                           const float2* __restrict__ twg, long long bstride) {
+  constexpr int P = Split<N>::P, Q = Split<N>::Q, W = ColCfg<N>::W, T = ColCfg<N>::T;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* ybuf = sm + N;
+  data += (long long)blockIdx.y * bstride;
+  const int tid = threadIdx.x;
+  for (int m = tid; m < N; m += T) tw[m] = twg[m];
+  __syncthreads();
+  const int c0 = blockIdx.x * W;
+  for (int w = tid; w < W * P; w += T) {
+    const int c = w % W, t = w / W;
+    const int col = c0 + c;
+    float2 u[Q];
+    if (col < g.ncols) {
+      const float2* src = data + col_base(g, col) + (long long)t * g.stride;
+#pragma unroll
+      for (int m = 0; m < Q; ++m) u[m] = src[(long long)(P * m) * g.stride];
+    } else {
+#pragma unroll
+      for (int m = 0; m < Q; ++m) u[m] = make_float2(0.f, 0.f);
+    }
+    RegDFT<Q, SIGN, P>::run(u, tw);
+#pragma unroll
+    for (int kb = 0; kb < Q; ++kb)
+      ybuf[(kb * P + t) * W + c] = (kb == 0) ? u[0] : cmul(u[kb], twid<SIGN>(tw, t * kb));
+  }
+  __syncthreads();
+  const int c = tid % W, kb = tid / W;
+  float2 u[P];
+#pragma unroll
+  for (int t = 0; t < P; ++t) u[t] = ybuf[(kb * P + t) * W + c];
+  RegDFT<P, SIGN, Q>::run(u, tw);
+  const int col = c0 + c;
+  if (col < g.ncols) {
+    float2* dst = data + col_base(g, col) + (long long)kb * g.stride;
+#pragma unroll
+    for (int ka = 0; ka < P; ++ka) dst[(long long)(Q * ka) * g.stride] = u[ka];
+  }
+}
+
+template <int N, class Op>
+__global__ void __launch_bounds__(ColCfg<N>::T) k_x_op_reg(float2* __restrict__ data, ColGeom g,
+                                                           const float2* __restrict__ twg, Op op, long long bstride) {
+  constexpr int P = Split<N>::P, Q = Split<N>::Q, W = ColCfg<N>::W, T = ColCfg<N>::T;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* ybuf = sm + N;
+  float* opsm = reinterpret_cast<float*>(ybuf + N * W);
+  const int batch = blockIdx.y;
+  data += (long long)batch * bstride;
+  const int tid = threadIdx.x;
+  for (int m = tid; m < N; m += T) tw[m] = twg[m];
+  op.prologue(opsm, batch);  // ends with __syncthreads()
+  const int c0 = blockIdx.x * W;
+  // forward stage 1
+  for (int w = tid; w < W * P; w += T) {
+    const int c = w % W, t = w / W;
+    const int col = c0 + c;
+    float2 u[Q];
+    if (col < g.ncols) {
+      const float2* src = data + col + (long long)t * g.stride;
+#pragma unroll
+      for (int m = 0; m < Q; ++m) u[m] = src[(long long)(P * m) * g.stride];
+    } else {
+#pragma unroll
+      for (int m = 0; m < Q; ++m) u[m] = make_float2(0.f, 0.f);
+    }
+    RegDFT<Q, -1, P>::run(u, tw);
+#pragma unroll
+    for (int kb = 0; kb < Q; ++kb)
+      ybuf[(kb * P + t) * W + c] = (kb == 0) ? u[0] : cmul(u[kb], twid<-1>(tw, t * kb));
+  }
+  __syncthreads();
+  // forward stage 2: this thread holds X[kb + Q ka], ka < P
+  const int c = tid % W, kb = tid / W;
+  const int col = c0 + c;
+  float2 u[P];
+#pragma unroll
+  for (int t = 0; t < P; ++t) u[t] = ybuf[(kb * P + t) * W + c];
+  RegDFT<P, -1, Q>::run(u, tw);
+  if (col < g.ncols) {
+    const int ky = col / g.hz;
+    const int kz = col - ky * g.hz;
+#pragma unroll
+    for (int ka = 0; ka < P; ++ka) u[ka] = op.apply(u[ka], kb + Q * ka, ky, kz, opsm, batch);
+  }
+  __syncthreads();
+  op.epilogue(opsm, batch, blockIdx.x, gridDim.x);
+  if (Op::kInverse) {
+    // inverse stage 1': t' = kb holds x'[t' + Q m'] = u[m'], m' < P
+    RegDFT<P, 1, Q>::run(u, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < P; ++k1)
+      ybuf[(k1 * Q + kb) * W + c] = (k1 == 0) ? u[0] : cmul(u[k1], twid<1>(tw, kb * k1));
+    __syncthreads();
+    // inverse stage 2': items (c, k1), k1 < P
+    for (int w = tid; w < W * P; w += T) {
+      const int cc = w % W, k1 = w / W;
+      const int col2 = c0 + cc;
+      float2 v[Q];
+#pragma unroll
+      for (int t = 0; t < Q; ++t) v[t] = ybuf[(k1 * Q + t) * W + cc];
+      RegDFT<Q, 1, P>::run(v, tw);
+      if (col2 < g.ncols) {
+        float2* dst = data + col2 + (long long)k1 * g.stride;
+#pragma unroll
+        for (int k2 = 0; k2 < Q; ++k2) dst[(long long)(P * k2) * g.stride] = v[k2];
+      }
+    }
+  } else if (Op::kStore) {
+    if (col < g.ncols) {
+      float2* dst = data + col + (long long)kb * g.stride;
+#pragma unroll
+      for (int ka = 0; ka < P; ++ka) dst[(long long)(Q * ka) * g.stride] = u[ka];
+    }
+  }
+}
+
+// r2c along z, nh = nz/2 = N complex per row, R rows per CTA.
+template <int N>
+__global__ void __launch_bounds__(RowCfg<N>::T) k_rfft_z_reg(const float* __restrict__ in, float2* __restrict__ out,
+                                                             int nrows, float sub, const float2* __restrict__ twg,
+                                                             const float2* __restrict__ twg2, long long in_b,
+                                                             long long out_b) {
+  constexpr int P = Split<N>::P, Q = Split<N>::Q, R = RowCfg<N>::R, T = RowCfg<N>::T;
+  constexpr int S = P * (Q + 1);
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* tw2 = tw + N;        // N+1 entries: exp(-2 pi i k / (2N))
+  float2* ybuf = tw2 + N + 1;  // R*S; reused for the Z rows (stride N+1 <= S)
+  in += (long long)blockIdx.y * in_b;
+  out += (long long)blockIdx.y * out_b;
+  const int tid = threadIdx.x;
+  for (int m = tid; m < N; m += T) tw[m] = twg[m];
+  for (int m = tid; m <= N; m += T) tw2[m] = twg2[m];
+  __syncthreads();
+  const int row0 = blockIdx.x * R;
+  const float2* in2 = reinterpret_cast<const float2*>(in);
+  for (int w = tid; w < R * P; w += T) {
+    const int t = w % P, r = w / P;
+    const int row = row0 + r;
+    float2 u[Q];
+    if (row < nrows) {
+      const float2* src = in2 + (long long)row * N + t;
+#pragma unroll
+      for (int m = 0; m < Q; ++m) {
+        const float2 z = src[P * m];
+        u[m] = make_float2(z.x - sub, z.y - sub);
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < Q; ++m) u[m] = make_float2(0.f, 0.f);
+    }
+    RegDFT<Q, -1, P>::run(u, tw);
+#pragma unroll
+    for (int kb = 0; kb < Q; ++kb)
+      ybuf[r * S + t * (Q + 1) + kb] = (kb == 0) ? u[0] : cmul(u[kb], twid<-1>(tw, t * kb));
+  }
+  __syncthreads();
+  const int kb = tid % Q, r = tid / Q;
+  float2 u[P];
+#pragma unroll
+  for (int t = 0; t < P; ++t) u[t] = ybuf[r * S + t * (Q + 1) + kb];
+  RegDFT<P, -1, Q>::run(u, tw);
+  __syncthreads();
+#pragma unroll
+  for (int ka = 0; ka < P; ++ka) ybuf[r * (N + 1) + kb + Q * ka] = u[ka];
+  __syncthreads();
+  for (int w = tid; w < R * (N + 1); w += T) {
+    const int rr = w / (N + 1);
+    const int k = w - rr * (N + 1);
+    const int row = row0 + rr;
+    if (row >= nrows) continue;
+    const float2 zk = ybuf[rr * (N + 1) + (k == N ? 0 : k)];
+    const float2 zm = ybuf[rr * (N + 1) + (k == 0 ? 0 : N - k)];
+    const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);
+    const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+    out[(long long)row * (N + 1) + k] = cadd(e, cmul(tw2[k], o));
+  }
+}
+
+// c2r along z (unnormalised times `scale`).
+template <int N>
+__global__ void __launch_bounds__(RowCfg<N>::T) k_irfft_z_reg(const float2* __restrict__ in, float* __restrict__ out,
+                                                              int nrows, float scale, const float2* __restrict__ twg,
+                                                              const float2* __restrict__ twg2, long long in_b,
+                                                              long long out_b) {
+  constexpr int P = Split<N>::P, Q = Split<N>::Q, R = RowCfg<N>::R, T = RowCfg<N>::T;
+  constexpr int S = P * (Q + 1);
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* tw2 = tw + N;
+  float2* xbuf = tw2 + N + 1;   // R*(N+1)
+  float2* ybuf = xbuf + R * (N + 1);  // R*S
+  in += (long long)blockIdx.y * in_b;
+  out += (long long)blockIdx.y * out_b;
+  const int tid = threadIdx.x;
+  for (int m = tid; m < N; m += T) tw[m] = twg[m];
+  for (int m = tid; m <= N; m += T) tw2[m] = twg2[m];
+  const int row0 = blockIdx.x * R;
+  for (int w = tid; w < R * (N + 1); w += T) {
+    const int rr = w / (N + 1);
+    const int k = w - rr * (N + 1);
+    const int row = row0 + rr;
+    xbuf[w] = (row < nrows) ? in[(long long)row * (N + 1) + k] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  for (int w = tid; w < R * P; w += T) {
+    const int t = w % P, r = w / P;
+    float2 u[Q];
+#pragma unroll
+    for (int m = 0; m < Q; ++m) {
+      const int e = t + P * m;
+      const float2 xk = xbuf[r * (N + 1) + e];
+      const float2 xm = xbuf[r * (N + 1) + N - e];
+      const float2 ee = make_float2(xk.x + xm.x, xk.y - xm.y);
+      const float2 dd = cmul(make_float2(xk.x - xm.x, xk.y + xm.y), conjf2(tw2[e]));
+      u[m] = make_float2(ee.x - dd.y, ee.y + dd.x);
+    }
+    RegDFT<Q, 1, P>::run(u, tw);
+#pragma unroll
+    for (int kb = 0; kb < Q; ++kb)
+      ybuf[r * S + t * (Q + 1) + kb] = (kb == 0) ? u[0] : cmul(u[kb], twid<1>(tw, t * kb));
+  }
+  __syncthreads();
+  const int kb = tid % Q, r = tid / Q;
+  const int row = row0 + r;
+  float2 u[P];
+#pragma unroll
+  for (int t = 0; t < P; ++t) u[t] = ybuf[r * S + t * (Q + 1) + kb];
+  RegDFT<P, 1, Q>::run(u, tw);
+  if (row < nrows) {
+    float2* dst = reinterpret_cast<float2*>(out) + (long long)row * N + kb;
+#pragma unroll
+    for (int ka = 0; ka < P; ++ka) dst[Q * ka] = cscale(u[ka], scale);
+  }
+}
+
 // ---------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------
@@ -268,7 +524,124 @@ static int col_tile_width(int n) {
   return w < 1 ? 1 : pow2_floor(w);
 }
 
+// ---- twiddle tables w_n^m = exp(-2 pi i m / n), one per (device, n), built once on the host
+static std::mutex g_tw_mutex;
+static std::map<std::pair<int, int>, float2*> g_tw_tables;
+
+const float2* twiddle_table(int n) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_tw_mutex);
+  auto key = std::make_pair(dev, n);
+  auto it = g_tw_tables.find(key);
+  if (it != g_tw_tables.end()) return it->second;
+  std::vector<float2> h(n);
+  for (int m = 0; m < n; ++m) {
+    const double ang = 2.0 * M_PI * (double)m / (double)n;
+    h[m] = make_float2((float)std::cos(ang), (float)-std::sin(ang));
+  }
+  float2* d = nullptr;
+  if (cudaMalloc(&d, sizeof(float2) * n) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(d, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  g_tw_tables[key] = d;
+  return d;
+}
+
+#define JFLI_REG_SIZES(X) \
+  X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+
+static bool reg_size(int n) {
+  switch (n) {
+#define JFLI_CASE(N_) case N_:
+    JFLI_REG_SIZES(JFLI_CASE)
+#undef JFLI_CASE
+    return true;
+    default:
+      return false;
+  }
+}
+
+static int reg_col_w(int n) {
+  switch (n) {
+#define JFLI_CASE(N_) \
+  case N_:            \
+    return ColCfg<N_>::W;
+    JFLI_REG_SIZES(JFLI_CASE)
+#undef JFLI_CASE
+    default:
+      return 0;
+  }
+}
+
+template <int N>
+static cudaError_t rfft_z_reg(const float* in, float2* out, const MeshDims& d, float sub, cudaStream_t s) {
+  constexpr int R = RowCfg<N>::R, T = RowCfg<N>::T, P = Split<N>::P, Q = Split<N>::Q;
+  const float2* tw = twiddle_table(N);
+  const float2* tw2 = twiddle_table(2 * N);
+  if (!tw || !tw2) return cudaErrorMemoryAllocation;
+  const int nrows = d.nx * d.ny;
+  const size_t smem = ((size_t)N + N + 1 + (size_t)R * P * (Q + 1)) * sizeof(float2);
+  cudaFuncSetAttribute(k_rfft_z_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_rfft_z_reg<N><<<dim3((nrows + R - 1) / R, d.batch), T, smem, s>>>(in, out, nrows, sub, tw, tw2, d.cells(),
+                                                                       d.spec_elems());
+  note_launch();
+  return cudaGetLastError();
+}
+
+template <int N>
+static cudaError_t irfft_z_reg(const float2* in, float* out, const MeshDims& d, float scale, cudaStream_t s) {
+  constexpr int R = RowCfg<N>::R, T = RowCfg<N>::T, P = Split<N>::P, Q = Split<N>::Q;
+  const float2* tw = twiddle_table(N);
+  const float2* tw2 = twiddle_table(2 * N);
+  if (!tw || !tw2) return cudaErrorMemoryAllocation;
+  const int nrows = d.nx * d.ny;
+  const size_t smem = ((size_t)N + N + 1 + (size_t)R * (N + 1) + (size_t)R * P * (Q + 1)) * sizeof(float2);
+  cudaFuncSetAttribute(k_irfft_z_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_irfft_z_reg<N><<<dim3((nrows + R - 1) / R, d.batch), T, smem, s>>>(in, out, nrows, scale, tw, tw2,
+                                                                        d.spec_elems(), d.cells());
+  note_launch();
+  return cudaGetLastError();
+}
+
+template <int N, int SIGN>
+static cudaError_t cols_reg(float2* data, const ColGeom& g, long long bstride, int batch, cudaStream_t s) {
+  constexpr int W = ColCfg<N>::W, T = ColCfg<N>::T;
+  const float2* tw = twiddle_table(N);
+  if (!tw) return cudaErrorMemoryAllocation;
+  const size_t smem = ((size_t)N + (size_t)N * W) * sizeof(float2);
+  cudaFuncSetAttribute(k_cols_reg<N, SIGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_cols_reg<N, SIGN><<<dim3((g.ncols + W - 1) / W, batch), T, smem, s>>>(data, g, tw, bstride);
+  note_launch();
+  return cudaGetLastError();
+}
+
+template <int N, class Op>
+static cudaError_t x_op_reg(float2* data, const ColGeom& g, const Op& op, long long bstride, int batch,
+                            cudaStream_t s) {
+  constexpr int W = ColCfg<N>::W, T = ColCfg<N>::T;
+  const float2* tw = twiddle_table(N);
+  if (!tw) return cudaErrorMemoryAllocation;
+  const size_t smem = ((size_t)N + (size_t)N * W) * sizeof(float2) + Op::smem_bytes(op);
+  cudaFuncSetAttribute(k_x_op_reg<N, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_x_op_reg<N, Op><<<dim3((g.ncols + W - 1) / W, batch), T, smem, s>>>(data, g, tw, op, bstride);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// ---- generic (shared-memory Stockham) launchers for the remaining lengths
 static cudaError_t launch_rfft_z(const float* in, float2* out, const MeshDims& d, float sub, cudaStream_t s) {
+  switch (d.nz / 2) {
+#define JFLI_CASE(N_) \
+  case N_:            \
+    return rfft_z_reg<N_>(in, out, d, sub, s);
+    JFLI_REG_SIZES(JFLI_CASE)
+#undef JFLI_CASE
+    default:
+      break;
+  }
   FftPlan pl;
   make_fft_plan(d.nz / 2, &pl);
   const int nrows = d.nx * d.ny;
@@ -283,6 +656,15 @@ static cudaError_t launch_rfft_z(const float* in, float2* out, const MeshDims& d
 }
 
 static cudaError_t launch_irfft_z(const float2* in, float* out, const MeshDims& d, float scale, cudaStream_t s) {
+  switch (d.nz / 2) {
+#define JFLI_CASE(N_) \
+  case N_:            \
+    return irfft_z_reg<N_>(in, out, d, scale, s);
+    JFLI_REG_SIZES(JFLI_CASE)
+#undef JFLI_CASE
+    default:
+      break;
+  }
   FftPlan pl;
   make_fft_plan(d.nz / 2, &pl);
   const int nrows = d.nx * d.ny;
@@ -320,6 +702,15 @@ static ColGeom x_geom(const MeshDims& d) {
 
 template <int SIGN>
 static cudaError_t launch_cols(float2* data, const ColGeom& g, long long bstride, int batch, cudaStream_t s) {
+  switch (g.n) {
+#define JFLI_CASE(N_) \
+  case N_:            \
+    return cols_reg<N_, SIGN>(data, g, bstride, batch, s);
+    JFLI_REG_SIZES(JFLI_CASE)
+#undef JFLI_CASE
+    default:
+      break;
+  }
   FftPlan pl;
   make_fft_plan(g.n, &pl);
   const size_t smem = ((size_t)2 * g.n * g.w + g.n) * sizeof(float2);
@@ -333,6 +724,15 @@ static cudaError_t launch_cols(float2* data, const ColGeom& g, long long bstride
 template <class Op>
 static cudaError_t launch_x_op(float2* data, const MeshDims& d, const Op& op, cudaStream_t s) {
   const ColGeom g = x_geom(d);
+  switch (g.n) {
+#define JFLI_CASE(N_) \
+  case N_:            \
+    return x_op_reg<N_, Op>(data, g, op, d.spec_elems(), d.batch, s);
+    JFLI_REG_SIZES(JFLI_CASE)
+#undef JFLI_CASE
+    default:
+      break;
+  }
   FftPlan pl;
   make_fft_plan(g.n, &pl);
   const size_t smem = ((size_t)2 * g.n * g.w + g.n) * sizeof(float2) + Op::smem_bytes(op);
@@ -345,7 +745,8 @@ static cudaError_t launch_x_op(float2* data, const MeshDims& d, const Op& op, cu
 
 int x_pass_ctas(const MeshDims& d) {
   const ColGeom g = x_geom(d);
-  return (g.ncols + g.w - 1) / g.w;
+  const int w = reg_size(g.n) ? reg_col_w(g.n) : g.w;
+  return (g.ncols + w - 1) / w;
 }
 
 cudaError_t rfft3d_forward(const float* in, float2* spec, const MeshDims& d, float sub, cudaStream_t s) {

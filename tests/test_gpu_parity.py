@@ -213,7 +213,9 @@ def test_healpix_paint_matches_oracle(scheme, nside):
     else:
         p, w = oh.get_interp_weights(nside, th, ph)
         ref = np.bincount(p.ravel(), weights=w.ravel(), minlength=npix)
-        assert rel_l2(out, ref) < 1e-6
+        # bilinear weights move continuously with the FP32 position (the kernel may fuse
+        # multiply-adds), ~1e-7 rad over a pixel of 0.016 rad at nside 64
+        assert rel_l2(out, ref) < 2e-5
     assert abs(out.sum() - sel.sum()) < 1e-3 * max(sel.sum(), 1)
 
 
