@@ -425,11 +425,12 @@ __global__ void __launch_bounds__(RowCfg<N>::T) k_irfft_z_reg(const float2* __re
                                                               long long out_b) {
   constexpr int P = Split<N>::P, Q = Split<N>::Q, R = RowCfg<N>::R, T = RowCfg<N>::T;
   constexpr int S = P * (Q + 1);
+  constexpr int IT = (R * P + T - 1) / T;  // stage-1 items per thread
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* tw2 = tw + N;
-  float2* xbuf = tw2 + N + 1;   // R*(N+1)
-  float2* ybuf = xbuf + R * (N + 1);  // R*S
+  float2* xbuf = tw2 + N + 1;  // R*(N+1) input rows, then (aliased) the R*S exchange buffer
+  float2* ybuf = xbuf;
   in += (long long)blockIdx.y * in_b;
   out += (long long)blockIdx.y * out_b;
   const int tid = threadIdx.x;
@@ -443,9 +444,12 @@ __global__ void __launch_bounds__(RowCfg<N>::T) k_irfft_z_reg(const float2* __re
     xbuf[w] = (row < nrows) ? in[(long long)row * (N + 1) + k] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  for (int w = tid; w < R * P; w += T) {
+  float2 u1[IT][Q];
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int w = tid + it * T;
+    if (w >= R * P) continue;
     const int t = w % P, r = w / P;
-    float2 u[Q];
 #pragma unroll
     for (int m = 0; m < Q; ++m) {
       const int e = t + P * m;
@@ -453,12 +457,19 @@ __global__ void __launch_bounds__(RowCfg<N>::T) k_irfft_z_reg(const float2* __re
       const float2 xm = xbuf[r * (N + 1) + N - e];
       const float2 ee = make_float2(xk.x + xm.x, xk.y - xm.y);
       const float2 dd = cmul(make_float2(xk.x - xm.x, xk.y + xm.y), conjf2(tw2[e]));
-      u[m] = make_float2(ee.x - dd.y, ee.y + dd.x);
+      u1[it][m] = make_float2(ee.x - dd.y, ee.y + dd.x);
     }
-    RegDFT<Q, 1, P>::run(u, tw);
+    RegDFT<Q, 1, P>::run(u1[it], tw);
+  }
+  __syncthreads();  // every input row has been read; the exchange buffer may overwrite it
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int w = tid + it * T;
+    if (w >= R * P) continue;
+    const int t = w % P, r = w / P;
 #pragma unroll
     for (int kb = 0; kb < Q; ++kb)
-      ybuf[r * S + t * (Q + 1) + kb] = (kb == 0) ? u[0] : cmul(u[kb], twid<1>(tw, t * kb));
+      ybuf[r * S + t * (Q + 1) + kb] = (kb == 0) ? u1[it][0] : cmul(u1[it][kb], twid<1>(tw, t * kb));
   }
   __syncthreads();
   const int kb = tid % Q, r = tid / Q;
@@ -598,7 +609,8 @@ static cudaError_t irfft_z_reg(const float2* in, float* out, const MeshDims& d, 
   const float2* tw2 = twiddle_table(2 * N);
   if (!tw || !tw2) return cudaErrorMemoryAllocation;
   const int nrows = d.nx * d.ny;
-  const size_t smem = ((size_t)N + N + 1 + (size_t)R * (N + 1) + (size_t)R * P * (Q + 1)) * sizeof(float2);
+  const size_t rows_buf = (size_t)R * P * (Q + 1) > (size_t)R * (N + 1) ? (size_t)R * P * (Q + 1) : (size_t)R * (N + 1);
+  const size_t smem = ((size_t)N + N + 1 + rows_buf) * sizeof(float2);
   cudaFuncSetAttribute(k_irfft_z_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_irfft_z_reg<N><<<dim3((nrows + R - 1) / R, d.batch), T, smem, s>>>(in, out, nrows, scale, tw, tw2,
                                                                         d.spec_elems(), d.cells());

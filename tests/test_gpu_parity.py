@@ -240,6 +240,32 @@ def test_kick_drift_paint_matches_unfused(cosmo):
     assert rel_l2(host(rho), opm.cic_paint(rx)) < 1e-5
 
 
+@pytest.mark.parametrize("spread", [0.3, 6.0, 14.0])
+def test_kick_drift_paint_tiled_and_fallback_paths(spread):
+    """Small spreads run from the shared-memory tiles, large ones exceed the tile and take
+    the global path; both must match the oracle. Also a 40^3 mesh with partial bricks."""
+    from jfli_b200._lib import JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
+
+    for n in (32, 40):
+        rng = np.random.default_rng(int(spread * 10) + n)
+        x0 = rng.uniform(-spread, spread, (n, n, n, 3)).astype(np.float32)
+        v0 = rng.normal(0, 1.0, (n, n, n, 3)).astype(np.float32)
+        kick, drift = 0.25, 0.5
+        pot64 = opm.potential_real(1.0 + 0.3 * rng.normal(size=(n, n, n)))
+        x, v = dev(x0), dev(v0)
+        rho = torch.zeros(n, n, n, device="cuda")
+        ops.kick_drift_paint(x, v, dev(pot64), kick, drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT, rho)
+        kvec = opm.fftk((n, n, n))
+        pk = np.fft.fftn(pot64)
+        F = np.stack([opm.cic_read(-np.fft.ifftn(opm.gradient_kernel(kvec, i) * pk).real, x0.astype(np.float64))
+                      for i in range(3)], -1)
+        rv = v0 + kick * F
+        rx = x0 + drift * rv
+        assert rel_l2(host(v) - v0, rv - v0) < 1e-5
+        assert rel_l2(host(x), rx) < 1e-6
+        assert rel_l2(host(rho), opm.cic_paint(rx)) < 1e-5
+
+
 def _config1(cosmo, n=64, L=256.0, steps=10):
     noise = jf.white_noise(0, (n, n, n))
     ic = jf.interpolate_initial_conditions(noise, (n, n, n), (L, L, L), cosmo=cosmo)
