@@ -20,6 +20,7 @@
  *   jfli_rfft3d/irfft3d    <- jaxpm fft3d / ifft3d as used at initial.py:175,182, pm/correction.py:174,193
  *   jfli_poisson_potential <- the invlaplace_kernel stage of jaxpm pm_forces (pm/solvers.py:22)
  *   jfli_pm_forces         <- pm/solvers.py:19-32 (_forces -> jaxpm pm_forces, times 1.5 Omega_m)
+ *   jfli_force_mesh        <- the gradient_kernel stage of jaxpm pm_forces (pm/solvers.py:22)
  *   jfli_kick_drift_paint  <- pm/solvers.py:151-202 and 258-325 (the per-particle part of step())
  *   jfli_pm_step           <- one step() of EfficientDriftDoubleKick / ReversibleDoubleKickDrift
  *   jfli_ic_filter         <- initial.py:167-182 (interpolate_initial_conditions), infer/dist.py:43-79
@@ -41,7 +42,7 @@ extern "C" {
 #define JFLI_ECUDA 2       /* a CUDA call or kernel launch failed */
 #define JFLI_EUNSUPPORTED 3 /* valid but unsupported configuration */
 
-#define JFLI_STEP_KICK 1   /* v += F(x) * kick, F = -grad_FD(pot) read out with CIC */
+#define JFLI_STEP_KICK 1   /* v += F(x) * kick, F the CIC readout of the force meshes */
 #define JFLI_STEP_DRIFT 2  /* x += v * drift */
 #define JFLI_STEP_PAINT 4  /* CIC deposit at the new position */
 #define JFLI_STEP_FORCE 8  /* (jfli_pm_step) solve the Poisson equation for the new positions */
@@ -92,14 +93,21 @@ size_t jfli_pm_forces_workspace_bytes(int nx, int ny, int nz, int batch);
 int jfli_pm_forces(void* stream, const float* pos, int absolute, float scale, float* forces, void* workspace,
                    size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
 
-/* Fused particle pass: [kick, or with CORRECT a position shift, by kick * -grad_FD(pot)
- * read out at the current position] -> [drift] -> [paint into rho (accumulating)].
- * Positions are relative (displacements). */
-int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* pot, float kick, float drift, int flags,
-                          float weight, float* rho, int nx, int ny, int nz, int batch, char* err, size_t errlen);
-/* One PM step: clear rho, kick/drift/paint (flags KICK|DRIFT), then with FORCE solve for the
- * new potential into `pot`. Workspace: jfli_poisson_workspace_bytes. */
-int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift, int flags, float* rho, float* pot,
+/* Force meshes: force[a] = scale * (-D_a pot), SoA [batch][3][nx][ny][nz], D the 4-point
+ * finite difference whose Fourier eigenvalue is JaxPM's gradient_kernel. Its CIC readout is
+ * the force of jaxpm pm_forces (pm/solvers.py:19-32). */
+int jfli_force_mesh(void* stream, const float* pot, float scale, float* force, int nx, int ny, int nz, int batch,
+                    char* err, size_t errlen);
+/* Fused particle pass: [kick, or with CORRECT a position shift, by kick * the CIC readout
+ * of `force` (jfli_force_mesh layout) at the current position] -> [drift] -> [paint into
+ * rho (accumulating)]. Positions are relative (displacements). */
+int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* force, float kick, float drift,
+                          int flags, float weight, float* rho, int nx, int ny, int nz, int batch, char* err,
+                          size_t errlen);
+/* One PM step: clear rho, kick/drift/paint (flags KICK|DRIFT), then with FORCE solve the
+ * Poisson equation for the new positions and write the new force meshes into `force`. */
+size_t jfli_pm_step_workspace_bytes(int nx, int ny, int nz, int batch);
+int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift, int flags, float* rho, float* force,
                  void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
                  size_t errlen);
 

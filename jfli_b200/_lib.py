@@ -54,6 +54,8 @@ _SIGNATURES = {
     "jfli_readout_gradient": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_float, c_void_p, *_DIMS, *_ERR]),
     "jfli_pm_forces_workspace_bytes": (c_size_t, _DIMS),
     "jfli_pm_forces": (c_int, [c_void_p, c_void_p, c_int, c_float, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR]),
+    "jfli_force_mesh": (c_int, [c_void_p, c_void_p, c_float, c_void_p, *_DIMS, *_ERR]),
+    "jfli_pm_step_workspace_bytes": (c_size_t, _DIMS),
     "jfli_kick_drift_paint": (
         c_int,
         [c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_float, c_int, c_float, c_void_p, *_DIMS, *_ERR],

@@ -208,8 +208,19 @@ int jfli_readout_gradient(void* stream, const float* pos, int absolute, const fl
                      errlen, "jfli_readout_gradient");
 }
 
-int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* pot, float kick, float drift, int flags,
-                          float weight, float* rho, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+int jfli_force_mesh(void* stream, const float* pot, float scale, float* force, int nx, int ny, int nz, int batch,
+                    char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
+  CHECK_PTR(pot);
+  CHECK_PTR(force);
+  const MeshDims d{nx, ny, nz, batch};
+  return cuda_status(jfli::force_mesh(pot, force, scale, d, (cudaStream_t)stream), err, errlen, "jfli_force_mesh");
+}
+
+int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* force, float kick, float drift,
+                          int flags, float weight, float* rho, int nx, int ny, int nz, int batch, char* err,
+                          size_t errlen) {
   CHECK_DIMS(nx, ny, nz, batch);
   CHECK_PTR(disp);
   CHECK_PTR(vel);
@@ -217,16 +228,20 @@ int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* po
     return fail(err, errlen, JFLI_EINVAL, "unknown step flags 0x%x", flags);
   if ((flags & JFLI_STEP_KICK) && (flags & JFLI_STEP_CORRECT))
     return fail(err, errlen, JFLI_EINVAL, "KICK and CORRECT are exclusive");
-  if ((flags & (JFLI_STEP_KICK | JFLI_STEP_CORRECT)) && !pot)
-    return fail(err, errlen, JFLI_EINVAL, "kick requested without a potential");
+  if ((flags & (JFLI_STEP_KICK | JFLI_STEP_CORRECT)) && !force)
+    return fail(err, errlen, JFLI_EINVAL, "kick requested without a force mesh");
   if ((flags & JFLI_STEP_PAINT) && !rho) return fail(err, errlen, JFLI_EINVAL, "paint requested without a mesh");
-  if (flags & (JFLI_STEP_KICK | JFLI_STEP_CORRECT)) CHECK_STENCIL(nx, ny, nz);
   const MeshDims d{nx, ny, nz, batch};
-  return cuda_status(jfli::kick_drift_paint(disp, vel, pot, kick, drift, flags, weight, rho, d, (cudaStream_t)stream),
+  return cuda_status(jfli::kick_drift_paint(disp, vel, force, kick, drift, flags, weight, rho, d, (cudaStream_t)stream),
                      err, errlen, "jfli_kick_drift_paint");
 }
 
-int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift, int flags, float* rho, float* pot,
+size_t jfli_pm_step_workspace_bytes(int nx, int ny, int nz, int batch) {
+  const MeshDims d{nx, ny, nz, batch};
+  return spec_bytes(d) + mesh_bytes(d);
+}
+
+int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift, int flags, float* rho, float* force,
                  void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
                  size_t errlen) {
   CHECK_DIMS(nx, ny, nz, batch);
@@ -235,20 +250,23 @@ int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift,
   CHECK_PTR(disp);
   CHECK_PTR(vel);
   CHECK_PTR(rho);
-  CHECK_PTR(pot);
+  CHECK_PTR(force);
   CHECK_PTR(workspace);
   const MeshDims d{nx, ny, nz, batch};
-  if (workspace_bytes < spec_bytes(d))
-    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, spec_bytes(d));
+  const size_t need = jfli_pm_step_workspace_bytes(nx, ny, nz, batch);
+  if (workspace_bytes < need)
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, need);
   if ((flags & ~(JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_FORCE)) != 0)
     return fail(err, errlen, JFLI_EINVAL, "unknown step flags 0x%x", flags);
   cudaStream_t s = (cudaStream_t)stream;
+  float2* spec = (float2*)workspace;
+  float* pot = (float*)((char*)workspace + spec_bytes(d));
   cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
   if (e == cudaSuccess)
-    e = jfli::kick_drift_paint(disp, vel, pot, kick, drift, (flags & (JFLI_STEP_KICK | JFLI_STEP_DRIFT)) | JFLI_STEP_PAINT,
-                               1.0f, rho, d, s);
-  if (e == cudaSuccess && (flags & JFLI_STEP_FORCE))
-    e = jfli::poisson_potential(rho, (float2*)workspace, pot, d, 1.0f, 1.0f, s);
+    e = jfli::kick_drift_paint(disp, vel, force, kick, drift,
+                               (flags & (JFLI_STEP_KICK | JFLI_STEP_DRIFT)) | JFLI_STEP_PAINT, 1.0f, rho, d, s);
+  if (e == cudaSuccess && (flags & JFLI_STEP_FORCE)) e = jfli::poisson_potential(rho, spec, pot, d, 1.0f, 1.0f, s);
+  if (e == cudaSuccess && (flags & JFLI_STEP_FORCE)) e = jfli::force_mesh(pot, force, 1.0f, d, s);
   return cuda_status(e, err, errlen, "jfli_pm_step");
 }
 

@@ -246,15 +246,18 @@ __global__ void k_readout_gradient(const float* __restrict__ pos, int absolute, 
   }
 }
 
+__device__ __forceinline__ void gather_force_mesh(const float* __restrict__ F, const PGrid& g, const Cic1& cx,
+                                                  const Cic1& cy, const Cic1& cz, float& fx, float& fy, float& fz);
+
 // One fused particle pass of a PM step. Order inside: kick (with the force at the
 // current position) -> drift (with the kicked velocity) -> paint (at the new position).
-__global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ pot,
+__global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ force,
                                    float kick, float drift, int flags, float weight, float* __restrict__ rho,
                                    PGrid g) {
   const long long b = blockIdx.y;
   disp += b * g.np * 3;
   vel += b * g.np * 3;
-  if (pot) pot += b * g.np;
+  if (force) force += b * g.np * 3;
   if (rho) rho += b * g.np;
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
@@ -263,7 +266,7 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
     if (flags & (kStepKick | kStepCorrect)) {
       const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
       float fx, fy, fz;
-      gather_force(pot, g, cx, cy, cz, fx, fy, fz);
+      gather_force_mesh(force, g, cx, cy, cz, fx, fy, fz);
       if (flags & kStepKick) {
         vel[3 * p + 0] += fx * kick;
         vel[3 * p + 1] += fy * kick;
@@ -292,317 +295,59 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
 }
 
 // ----------------------------------------------------------------------------------
-// Brick-tiled particle pass. A CTA owns a Lagrangian brick of BX x BY x BZ particles.
-// Particles of a brick stay close together, so the cells they touch form a compact box
-// whose bounds the CTA reduces from the actual displacements:
-//   * the potential over [min cell - 2, max cell + 3] is staged in shared memory and the
-//     FD-gradient readout runs from there (56 shared loads per particle instead of 56
-//     scattered global loads);
-//   * the CIC deposit goes to a shared-memory tile over [min cell, max cell + 1] with
-//     shared atomics, then the tile is added to the mesh with one coalesced atomic per
-//     non-empty cell.
-// A brick whose box exceeds the tile capacity takes the global path for that phase.
+// Force mesh: F_a = scale * (-D_a pot) at every cell, SoA [3][nx][ny][nz]. The particle
+// pass then reads 8 CIC corners per component (24 loads) instead of the 56-point FD
+// stencil of the potential; the CIC readout of F equals the stencil readout of pot.
 // ----------------------------------------------------------------------------------
-namespace brick {
-constexpr int BX = 8, BY = 8, BZ = 32;
-constexpr int T = 256;
-constexpr int K = BX * BY * BZ / T;  // particles per thread
-constexpr int TILE = 24576;          // floats of shared memory per CTA (96 KB)
-}  // namespace brick
-
-// FD-gradient readout from a tile in local (unwrapped) coordinates; (cx, cy, cz) is
-// the low CIC corner, strides sx (x) and sy (y), z contiguous.
-__device__ __forceinline__ void gather_force_tile(const float* tile, int sx, int sy, int cx, int cy, int cz,
-                                                  const float* wx, const float* wy, const float* wz, float& fx,
-                                                  float& fy, float& fz) {
-  int x[6], y[6], z[6];
-#pragma unroll
-  for (int s = 0; s < 6; ++s) {
-    x[s] = (cx + s - 2) * sx;
-    y[s] = (cy + s - 2) * sy;
-    z[s] = cz + s - 2;
+__global__ void k_force_mesh(const float* __restrict__ pot, float* __restrict__ F, float scale, PGrid g) {
+  const long long b = blockIdx.y;
+  pot += b * g.np;
+  F += b * g.np * 3;
+  const float s = scale / 12.0f;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    int i, j, k;
+    particle_ijk(g, p, i, j, k);
+    const int xo = i * g.yz, yo = j * g.nz;
+    const float* r = pot + xo + yo;
+    const float fz = (8.0f * (__ldg(r + wrap1(k + 1, g.nz)) - __ldg(r + wrap1(k - 1, g.nz))) -
+                      (__ldg(r + wrap1(k + 2, g.nz)) - __ldg(r + wrap1(k - 2, g.nz))));
+    const float* cy = pot + xo + k;
+    const float fy = (8.0f * (__ldg(cy + wrap1(j + 1, g.ny) * g.nz) - __ldg(cy + wrap1(j - 1, g.ny) * g.nz)) -
+                      (__ldg(cy + wrap1(j + 2, g.ny) * g.nz) - __ldg(cy + wrap1(j - 2, g.ny) * g.nz)));
+    const float* cx = pot + yo + k;
+    const float fx = (8.0f * (__ldg(cx + wrap1(i + 1, g.nx) * g.yz) - __ldg(cx + wrap1(i - 1, g.nx) * g.yz)) -
+                      (__ldg(cx + wrap1(i + 2, g.nx) * g.yz) - __ldg(cx + wrap1(i - 2, g.nx) * g.yz)));
+    F[p] = -fx * s;
+    F[g.np + p] = -fy * s;
+    F[2ull * g.np + p] = -fz * s;
   }
-  float c[2][2][2];
-#pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int b = 0; b < 2; ++b)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) c[a][b][e] = tile[x[2 + a] + y[2 + b] + z[2 + e]];
-  float gx = 0.f, gy = 0.f, gz = 0.f;
-#pragma unroll
-  for (int b = 0; b < 2; ++b)
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int o = y[2 + b] + z[2 + e];
-      const float v[6] = {tile[x[0] + o], tile[x[1] + o], c[0][b][e], c[1][b][e], tile[x[4] + o], tile[x[5] + o]};
-      float g0, g1;
-      fd_pair(v, g0, g1);
-      gx += wy[b] * wz[e] * (wx[0] * g0 + wx[1] * g1);
-    }
-#pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int o = x[2 + a] + z[2 + e];
-      const float v[6] = {tile[y[0] + o], tile[y[1] + o], c[a][0][e], c[a][1][e], tile[y[4] + o], tile[y[5] + o]};
-      float g0, g1;
-      fd_pair(v, g0, g1);
-      gy += wx[a] * wz[e] * (wy[0] * g0 + wy[1] * g1);
-    }
+}
+
+// CIC readout of the three force meshes at one particle.
+__device__ __forceinline__ void gather_force_mesh(const float* __restrict__ F, const PGrid& g, const Cic1& cx,
+                                                  const Cic1& cy, const Cic1& cz, float& fx, float& fy, float& fz) {
+  const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
+  const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
+  const float* F1 = F + g.np;
+  const float* F2 = F + 2ull * g.np;
+  float ax = 0.f, ay = 0.f, az = 0.f;
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
-      const int o = x[2 + a] + y[2 + b];
-      const float v[6] = {tile[z[0] + o], tile[z[1] + o], c[a][b][0], c[a][b][1], tile[z[4] + o], tile[z[5] + o]};
-      float g0, g1;
-      fd_pair(v, g0, g1);
-      gz += wx[a] * wy[b] * (wz[0] * g0 + wz[1] * g1);
-    }
-  fx = -gx;
-  fy = -gy;
-  fz = -gz;
-}
-
-// Block-wide min (v[0..2]) and max (v[3..5]) of six ints; `red` holds 6 * (T/32) + 6 ints.
-__device__ __forceinline__ void block_minmax6(int* v, int* red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      const float wab = wx[a] * wy[b];
 #pragma unroll
-  for (int i = 0; i < 6; ++i) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const int o = __shfl_xor_sync(0xffffffffu, v[i], off);
-      v[i] = i < 3 ? min(v[i], o) : max(v[i], o);
-    }
-  }
-  if (lane == 0)
-#pragma unroll
-    for (int i = 0; i < 6; ++i) red[warp * 6 + i] = v[i];
-  __syncthreads();
-  if (threadIdx.x < 6) {
-    const int i = threadIdx.x;
-    int r = red[i];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = i < 3 ? min(r, red[w * 6 + i]) : max(r, red[w * 6 + i]);
-    red[(blockDim.x >> 5) * 6 + i] = r;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < 6; ++i) v[i] = red[(blockDim.x >> 5) * 6 + i];
-}
-
-__device__ __forceinline__ int wrap_any(int v, int n) {
-  v %= n;
-  return v < 0 ? v + n : v;
-}
-
-__global__ void __launch_bounds__(brick::T, 2)
-    k_kdp_brick(float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ pot, float kick,
-                float drift, int flags, float weight, float* __restrict__ rho, PGrid g, int nbx, int nby, int nbz) {
-  using namespace brick;
-  extern __shared__ float tile[];
-  __shared__ int red[6 * (T / 32) + 6];
-  const long long bofs = blockIdx.y;
-  disp += bofs * g.np * 3;
-  vel += bofs * g.np * 3;
-  if (pot) pot += bofs * g.np;
-  if (rho) rho += bofs * g.np;
-  const int bz = blockIdx.x % nbz;
-  const int brest = blockIdx.x / nbz;
-  const int by = brest % nby;
-  const int bx = brest / nby;
-  const int ox = bx * BX, oy = by * BY, oz = bz * BZ;
-  const bool need_v = (flags & (kStepKick | kStepDrift)) != 0;
-
-  float xr[K][3], vr[K][3];
-  bool valid[K];
-#pragma unroll
-  for (int q = 0; q < K; ++q) {
-    const int L = threadIdx.x + q * T;
-    const int gx = ox + L / (BY * BZ), gy = oy + (L / BZ) % BY, gz = oz + L % BZ;
-    valid[q] = gx < g.nx && gy < g.ny && gz < g.nz;
-    const long long p = ((long long)gx * g.ny + gy) * g.nz + gz;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      xr[q][a] = valid[q] ? disp[3 * p + a] : 0.f;
-      vr[q][a] = (valid[q] && need_v) ? vel[3 * p + a] : 0.f;
-    }
-  }
-
-  if (flags & (kStepKick | kStepCorrect)) {
-    int mm[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
-#pragma unroll
-    for (int q = 0; q < K; ++q) {
-      if (!valid[q]) continue;
-      const int L = threadIdx.x + q * T;
-      const int gg[3] = {ox + L / (BY * BZ), oy + (L / BZ) % BY, oz + L % BZ};
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const int c = gg[a] + (int)floorf(xr[q][a]);
-        mm[a] = min(mm[a], c);
-        mm[3 + a] = max(mm[3 + a], c);
+      for (int c = 0; c < 2; ++c) {
+        const int o = xo[a] + yo[b] + zo[c];
+        const float w = wab * wz[c];
+        ax += __ldg(F + o) * w;
+        ay += __ldg(F1 + o) * w;
+        az += __ldg(F2 + o) * w;
       }
     }
-    block_minmax6(mm, red);
-    const long long ex = (long long)mm[3] - mm[0] + 6, ey = (long long)mm[4] - mm[1] + 6,
-                    ez = (long long)mm[5] - mm[2] + 6;
-    const bool fits = ex > 0 && ey > 0 && ez > 0 && ex * ey * ez <= TILE;
-    if (fits) {
-      const int tx = mm[0] - 2, ty = mm[1] - 2, tz = mm[2] - 2;
-      const int iey = (int)ey, iez = (int)ez;
-      const int gz0 = wrap_any(tz, g.nz);
-      for (int r = threadIdx.x >> 5; r < (int)(ex * ey); r += T / 32) {
-        const int a = r / iey;
-        const int b = r - a * iey;
-        const int base = wrap_any(tx + a, g.nx) * g.yz + wrap_any(ty + b, g.ny) * g.nz;
-        for (int c = threadIdx.x & 31; c < iez; c += 32) {
-          int gzc = gz0 + c;
-          while (gzc >= g.nz) gzc -= g.nz;
-          tile[r * iez + c] = __ldg(pot + base + gzc);
-        }
-      }
-      __syncthreads();
-#pragma unroll
-      for (int q = 0; q < K; ++q) {
-        if (!valid[q]) continue;
-        const int L = threadIdx.x + q * T;
-        const int gg[3] = {ox + L / (BY * BZ), oy + (L / BZ) % BY, oz + L % BZ};
-        float w[3][2];
-        int cl[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const float f = floorf(xr[q][a]);
-          w[a][1] = xr[q][a] - f;
-          w[a][0] = 1.0f - w[a][1];
-          cl[a] = gg[a] + (int)f;
-        }
-        float fx, fy, fz;
-        gather_force_tile(tile, iey * iez, iez, cl[0] - tx, cl[1] - ty, cl[2] - tz, w[0], w[1], w[2], fx, fy, fz);
-        if (flags & kStepKick) {
-          vr[q][0] += fx * kick;
-          vr[q][1] += fy * kick;
-          vr[q][2] += fz * kick;
-        } else {
-          xr[q][0] += fx * kick;
-          xr[q][1] += fy * kick;
-          xr[q][2] += fz * kick;
-        }
-      }
-      __syncthreads();  // the tile is reused by the paint phase
-    } else {
-#pragma unroll
-      for (int q = 0; q < K; ++q) {
-        if (!valid[q]) continue;
-        const int L = threadIdx.x + q * T;
-        const int gx = ox + L / (BY * BZ), gy = oy + (L / BZ) % BY, gz = oz + L % BZ;
-        const Cic1 cx = cic_rel(gx, xr[q][0], g.nx), cy = cic_rel(gy, xr[q][1], g.ny), cz = cic_rel(gz, xr[q][2], g.nz);
-        float fx, fy, fz;
-        gather_force(pot, g, cx, cy, cz, fx, fy, fz);
-        if (flags & kStepKick) {
-          vr[q][0] += fx * kick;
-          vr[q][1] += fy * kick;
-          vr[q][2] += fz * kick;
-        } else {
-          xr[q][0] += fx * kick;
-          xr[q][1] += fy * kick;
-          xr[q][2] += fz * kick;
-        }
-      }
-    }
-  }
-
-  if (flags & kStepDrift) {
-#pragma unroll
-    for (int q = 0; q < K; ++q)
-#pragma unroll
-      for (int a = 0; a < 3; ++a) xr[q][a] += vr[q][a] * drift;
-  }
-
-#pragma unroll
-  for (int q = 0; q < K; ++q) {
-    if (!valid[q]) continue;
-    const int L = threadIdx.x + q * T;
-    const long long p = ((long long)(ox + L / (BY * BZ)) * g.ny + (oy + (L / BZ) % BY)) * g.nz + (oz + L % BZ);
-    if (flags & (kStepDrift | kStepCorrect))
-#pragma unroll
-      for (int a = 0; a < 3; ++a) disp[3 * p + a] = xr[q][a];
-    if (flags & kStepKick)
-#pragma unroll
-      for (int a = 0; a < 3; ++a) vel[3 * p + a] = vr[q][a];
-  }
-
-  if (flags & kStepPaint) {
-    int mm[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
-#pragma unroll
-    for (int q = 0; q < K; ++q) {
-      if (!valid[q]) continue;
-      const int L = threadIdx.x + q * T;
-      const int gg[3] = {ox + L / (BY * BZ), oy + (L / BZ) % BY, oz + L % BZ};
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const int c = gg[a] + (int)floorf(xr[q][a]);
-        mm[a] = min(mm[a], c);
-        mm[3 + a] = max(mm[3 + a], c);
-      }
-    }
-    block_minmax6(mm, red);
-    const long long ex = (long long)mm[3] - mm[0] + 2, ey = (long long)mm[4] - mm[1] + 2,
-                    ez = (long long)mm[5] - mm[2] + 2;
-    const bool fits = ex > 0 && ey > 0 && ez > 0 && ex * ey * ez <= TILE;
-    if (fits) {
-      const int vol = (int)(ex * ey * ez), iey = (int)ey, iez = (int)ez;
-      for (int i = threadIdx.x; i < vol; i += T) tile[i] = 0.f;
-      __syncthreads();
-#pragma unroll
-      for (int q = 0; q < K; ++q) {
-        if (!valid[q]) continue;
-        const int L = threadIdx.x + q * T;
-        const int gg[3] = {ox + L / (BY * BZ), oy + (L / BZ) % BY, oz + L % BZ};
-        float w[3][2];
-        int cl[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const float f = floorf(xr[q][a]);
-          w[a][1] = xr[q][a] - f;
-          w[a][0] = 1.0f - w[a][1];
-          cl[a] = gg[a] + (int)f - mm[a];
-        }
-        const int base = (cl[0] * iey + cl[1]) * iez + cl[2];
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-          for (int b = 0; b < 2; ++b) {
-            const float wab = w[0][a] * weight * w[1][b];
-#pragma unroll
-            for (int c = 0; c < 2; ++c) atomicAdd(tile + base + (a * iey + b) * iez + c, wab * w[2][c]);
-          }
-      }
-      __syncthreads();
-      const int gz0 = wrap_any(mm[2], g.nz);
-      for (int r = threadIdx.x >> 5; r < (int)(ex * ey); r += T / 32) {
-        const int a = r / iey;
-        const int b = r - a * iey;
-        float* row = rho + wrap_any(mm[0] + a, g.nx) * g.yz + wrap_any(mm[1] + b, g.ny) * g.nz;
-        for (int c = threadIdx.x & 31; c < iez; c += 32) {
-          const float val = tile[r * iez + c];
-          if (val != 0.f) {
-            int gzc = gz0 + c;
-            while (gzc >= g.nz) gzc -= g.nz;
-            atomicAdd(row + gzc, val);
-          }
-        }
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < K; ++q) {
-        if (!valid[q]) continue;
-        const int L = threadIdx.x + q * T;
-        const int gx = ox + L / (BY * BZ), gy = oy + (L / BZ) % BY, gz = oz + L % BZ;
-        const Cic1 cx = cic_rel(gx, xr[q][0], g.nx), cy = cic_rel(gy, xr[q][1], g.ny), cz = cic_rel(gz, xr[q][2], g.nz);
-        deposit(rho, g, cx, cy, cz, weight);
-      }
-    }
-  }
+  fx = ax;
+  fy = ay;
+  fz = az;
 }
 
 // F = scale * (-D pot) at every grid point (particles exactly on the grid), optionally
@@ -762,14 +507,16 @@ cudaError_t cic_readout_gradient(const float* pos, int absolute, const float* po
   return cudaGetLastError();
 }
 
-cudaError_t kick_drift_paint(float* disp, float* vel, const float* pot, float kick, float drift, int flags,
+cudaError_t kick_drift_paint(float* disp, float* vel, const float* force, float kick, float drift, int flags,
                              float weight, float* rho, const MeshDims& d, cudaStream_t s) {
-  const int nbx = (d.nx + brick::BX - 1) / brick::BX, nby = (d.ny + brick::BY - 1) / brick::BY,
-            nbz = (d.nz + brick::BZ - 1) / brick::BZ;
-  const size_t smem = sizeof(float) * brick::TILE;
-  cudaFuncSetAttribute(k_kdp_brick, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_kdp_brick<<<dim3(nbx * nby * nbz, d.batch), brick::T, smem, s>>>(disp, vel, pot, kick, drift, flags, weight, rho,
-                                                                     make_pgrid(d), nbx, nby, nbz);
+  k_kick_drift_paint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(disp, vel, force, kick, drift,
+                                                                                     flags, weight, rho, make_pgrid(d));
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t force_mesh(const float* pot, float* force, float scale, const MeshDims& d, cudaStream_t s) {
+  k_force_mesh<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, force, scale, make_pgrid(d));
   note_launch();
   return cudaGetLastError();
 }

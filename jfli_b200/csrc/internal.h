@@ -34,7 +34,7 @@ cudaError_t power_partials(const float* mesh, float2* spec, double* partials, co
 // ---- cic.cu ----
 // Particle update program flags for kick_drift_paint.
 enum StepFlags {
-  kStepKick = 1,   // v += F(x) * kick, F = -grad_FD(pot) read out with CIC
+  kStepKick = 1,   // v += F(x) * kick, F the CIC readout of the force meshes
   kStepDrift = 2,  // x += v * drift
   kStepPaint = 4,  // CIC deposit of weight `weight` at the (new) position into rho
   kStepCorrect = 16,  // x += F(x) * kick (position correction, PGD); exclusive with kStepKick
@@ -45,8 +45,9 @@ cudaError_t cic_readout(const float* pos, int absolute, const float* mesh, float
                         cudaStream_t s);
 cudaError_t cic_readout_gradient(const float* pos, int absolute, const float* pot, float* out, float scale,
                                  const MeshDims& d, cudaStream_t s);
-cudaError_t kick_drift_paint(float* disp, float* vel, const float* pot, float kick, float drift, int flags,
+cudaError_t kick_drift_paint(float* disp, float* vel, const float* force, float kick, float drift, int flags,
                              float weight, float* rho, const MeshDims& d, cudaStream_t s);
+cudaError_t force_mesh(const float* pot, float* force, float scale, const MeshDims& d, cudaStream_t s);
 cudaError_t grid_gradient(const float* pot, float* out, float scale, int accumulate, const MeshDims& d,
                           cudaStream_t s);
 cudaError_t lpt2_source(const float* pot, float* out, const MeshDims& d, cudaStream_t s);

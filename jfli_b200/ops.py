@@ -144,21 +144,43 @@ def pm_forces(pos: torch.Tensor, *, absolute: bool = False, scale: float = 1.0) 
     return out
 
 
-def kick_drift_paint(disp: torch.Tensor, vel: torch.Tensor, pot: torch.Tensor | None, kick: float, drift: float,
+def force_mesh(pot: torch.Tensor, scale: float = 1.0, out: torch.Tensor | None = None) -> torch.Tensor:
+    """(..., 3, nx, ny, nz) force meshes scale * (-D_a pot), D the 4-point finite difference."""
+    _check(pot, "pot")
+    (nx, ny, nz), batch, lead = _mesh_dims(pot, False)
+    if out is None:
+        out = torch.empty(*lead, 3, nx, ny, nz, dtype=torch.float32, device=pot.device)
+    call("jfli_force_mesh", stream_ptr(), ptr(pot), float(scale), ptr(out), nx, ny, nz, batch)
+    return out
+
+
+def poisson_force(rho: torch.Tensor, rho_mean: float = 1.0, out: torch.Tensor | None = None,
+                  pot: torch.Tensor | None = None) -> torch.Tensor:
+    """Force meshes of a density: Poisson solve, then the finite-difference gradient."""
+    pot = poisson_potential(rho, rho_mean, out=pot)
+    return force_mesh(pot, out=out)
+
+
+def kick_drift_paint(disp: torch.Tensor, vel: torch.Tensor, force: torch.Tensor | None, kick: float, drift: float,
                      flags: int, rho: torch.Tensor | None = None, weight: float = 1.0) -> None:
+    """In place: [kick (or CORRECT shift) with the CIC readout of `force`] -> [drift] -> [paint]."""
     _check(disp, "disp")
     _check(vel, "vel")
     (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
-    call("jfli_kick_drift_paint", stream_ptr(), ptr(disp), ptr(vel), ptr(pot), float(kick), float(drift), int(flags),
-         float(weight), ptr(rho), nx, ny, nz, batch)
+    if force is not None:
+        _check(force, "force")
+        if force.numel() != 3 * batch * nx * ny * nz:
+            raise ValueError("force must hold 3 meshes per particle grid")
+    call("jfli_kick_drift_paint", stream_ptr(), ptr(disp), ptr(vel), ptr(force), float(kick), float(drift),
+         int(flags), float(weight), ptr(rho), nx, ny, nz, batch)
 
 
-def pm_step(disp, vel, kick, drift, flags, rho, pot) -> None:
+def pm_step(disp, vel, kick, drift, flags, rho, force) -> None:
     (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
-    nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
-    ws = workspace(nb, "spec", disp.device)
-    call("jfli_pm_step", stream_ptr(), ptr(disp), ptr(vel), float(kick), float(drift), int(flags), ptr(rho), ptr(pot),
-         ptr(ws), ws.numel(), nx, ny, nz, batch)
+    nb = query("jfli_pm_step_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "pm_step", disp.device)
+    call("jfli_pm_step", stream_ptr(), ptr(disp), ptr(vel), float(kick), float(drift), int(flags), ptr(rho),
+         ptr(force), ptr(ws), ws.numel(), nx, ny, nz, batch)
 
 
 def ic_filter(noise: torch.Tensor, ktab: torch.Tensor, ptab: torch.Tensor, box_size, *,

@@ -57,9 +57,9 @@ class PGDKernel(AbstractCorrection):
             pos = pos.to(PositionUnit.GRID_RELATIVE)
         x = pos.array.contiguous().clone()
         rho = ops.paint_cic(x)
-        pot = pgd_potential(rho, self.kl, self.ks, 1.0)
+        force = ops.force_mesh(pgd_potential(rho, self.kl, self.ks, 1.0))
         dummy_v = torch.empty_like(x)
-        ops.kick_drift_paint(x, dummy_v, pot, self.alpha, 0.0, JFLI_STEP_CORRECT)
+        ops.kick_drift_paint(x, dummy_v, force, self.alpha, 0.0, JFLI_STEP_CORRECT)
         return pos.replace(array=x), vel
 
     def rewind(self, t, pos, vel, full_drift_factor):
@@ -81,12 +81,14 @@ class SharpeningKernel(AbstractCorrection):
         raise NotImplementedError("SharpeningKernel is not on the B200 path")
 
 
-def pgd_potential(rho: torch.Tensor, kl: float, ks: float, rho_mean: float = 1.0) -> torch.Tensor:
+def pgd_potential(rho: torch.Tensor, kl: float, ks: float, rho_mean: float = 1.0,
+                  out: torch.Tensor | None = None) -> torch.Tensor:
     from .._lib import call, ptr, query, stream_ptr
 
     (nx, ny, nz) = tuple(rho.shape[-3:])
     batch = rho.numel() // (nx * ny * nz)
-    out = torch.empty_like(rho)
+    if out is None:
+        out = torch.empty_like(rho)
     nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
     ws = ops.workspace(nb, "spec", rho.device)
     call("jfli_pgd_potential", stream_ptr(), ptr(rho), float(rho_mean), float(kl), float(ks), ptr(out), ptr(ws),

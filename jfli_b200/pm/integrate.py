@@ -89,6 +89,7 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
     v = p.array.contiguous().clone()
     rho = torch.empty(x.shape[:-1], dtype=torch.float32, device=x.device)
     pot = torch.empty_like(rho)
+    force = torch.empty((3,) + tuple(rho.shape), dtype=torch.float32, device=x.device)
     events = time_events(t0, ts, dt0, dtype)
     n_steps = sum(1 for e in events if e[0] == "step")
     state = NBodyState(interp_state=interp.init(), t_initial=t0)
@@ -100,7 +101,7 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
     # force at the initial positions
     rho.zero_()
     ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT, rho)
-    ops.poisson_potential(rho, 1.0, out=pot)
+    ops.poisson_force(rho, 1.0, out=force, pot=pot)
     pending = EfficientDriftDoubleKick.init_kick(cosmo, t0, t0 + dt0) if efficient else None
     rho_is_current = True  # rho holds the paint of the current positions
 
@@ -119,25 +120,26 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
                     flags |= JFLI_STEP_KICK
                     kick = pending
                 if pgd is not None:
-                    ops.kick_drift_paint(x, v, pot, kick, c.drift, flags, rho)
-                    ppot = pgd_potential(rho, pgd.kl, pgd.ks, 1.0)
+                    ops.kick_drift_paint(x, v, force, kick, c.drift, flags, rho)
+                    pgd_potential(rho, pgd.kl, pgd.ks, 1.0, out=pot)
+                    ops.force_mesh(pot, out=force)
                     rho.zero_()
-                    ops.kick_drift_paint(x, v, ppot, pgd.alpha, 0.0, JFLI_STEP_CORRECT | JFLI_STEP_PAINT, rho)
+                    ops.kick_drift_paint(x, v, force, pgd.alpha, 0.0, JFLI_STEP_CORRECT | JFLI_STEP_PAINT, rho)
                 else:
-                    ops.kick_drift_paint(x, v, pot, kick, c.drift, flags, rho)
-                ops.poisson_potential(rho, 1.0, out=pot)
+                    ops.kick_drift_paint(x, v, force, kick, c.drift, flags, rho)
+                ops.poisson_force(rho, 1.0, out=force, pot=pot)
                 pending = c.kick
             else:
-                ops.kick_drift_paint(x, v, pot, c.kick, c.drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
+                ops.kick_drift_paint(x, v, force, c.kick, c.drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
                                      rho)
                 if step_i < n_steps:
-                    ops.poisson_potential(rho, 1.0, out=pot)
+                    ops.poisson_force(rho, 1.0, out=force, pot=pot)
             rho_is_current = True
             state = NBodyState(interp_state=interp.advance(state.interp_state, tb), t_initial=t0)
         else:
             _, i, t_target = ev
             if efficient and pending is not None and interp.needs_velocity():
-                ops.kick_drift_paint(x, v, pot, pending, 0.0, JFLI_STEP_KICK)
+                ops.kick_drift_paint(x, v, force, pending, 0.0, JFLI_STEP_KICK)
                 pending = None
             xf = dx.replace(array=x, scale_factors=t_target)
             vf = p.replace(array=v, scale_factors=t_target)
@@ -154,7 +156,7 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
                     snap = snap.replace(array=snap.array.clone())
             snapshots.append(snap)
     if efficient and pending is not None:
-        ops.kick_drift_paint(x, v, pot, pending, 0.0, JFLI_STEP_KICK)
+        ops.kick_drift_paint(x, v, force, pending, 0.0, JFLI_STEP_KICK)
     return RunResult(snapshots=snapshots, disp=x, vel=v, steps=n_steps)
 
 

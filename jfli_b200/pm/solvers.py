@@ -31,9 +31,10 @@ class NBodyState:
     t_initial: float
 
 
-def _forces_potential(x: torch.Tensor) -> torch.Tensor:
+def _force_mesh(x: torch.Tensor) -> torch.Tensor:
+    """Force meshes (without 1.5 Omega_m) of the CIC density of relative positions x."""
     rho = ops.paint_cic(x)
-    return ops.poisson_potential(rho, rho_mean=1.0)
+    return ops.poisson_force(rho, rho_mean=1.0)
 
 
 def _rel(field):
@@ -95,8 +96,8 @@ class EfficientDriftDoubleKick(AbstractNBodySolver):
         state = NBodyState(interp_state=self.interp_kernel.init(), t_initial=t0)
         x = _rel(displacement).array.contiguous()
         v = velocities.array.contiguous().clone()
-        pot = _forces_potential(x)
-        ops.kick_drift_paint(x, v, pot, self.init_kick(cosmo, t0, t1), 0.0, JFLI_STEP_KICK)
+        force = _force_mesh(x)
+        ops.kick_drift_paint(x, v, force, self.init_kick(cosmo, t0, t1), 0.0, JFLI_STEP_KICK)
         return displacement, velocities.replace(array=v, scale_factors=math.sqrt(t0 * t1)), state
 
     def step(self, displacement, velocities, t0, t1, dt, state, cosmo):
@@ -108,8 +109,8 @@ class EfficientDriftDoubleKick(AbstractNBodySolver):
         xf, vf = self.pgd_kernel.apply(t1, disp.replace(array=x, scale_factors=t1), velocities.replace(array=v),
                                        full_drift_factor=c.drift)
         x = xf.array.contiguous()
-        pot = _forces_potential(x)
-        ops.kick_drift_paint(x, v, pot, c.kick, 0.0, JFLI_STEP_KICK)
+        force = _force_mesh(x)
+        ops.kick_drift_paint(x, v, force, c.kick, 0.0, JFLI_STEP_KICK)
         new_state = NBodyState(interp_state=self.interp_kernel.advance(state.interp_state, t1),
                                t_initial=state.t_initial)
         return xf.replace(array=x, scale_factors=t1), velocities.replace(array=v, scale_factors=t1), new_state
@@ -145,8 +146,8 @@ class ReversibleDoubleKickDrift(AbstractNBodySolver):
         disp = _rel(displacement)
         x = disp.array.contiguous().clone()
         v = velocities.array.contiguous().clone()
-        pot = _forces_potential(x)
-        ops.kick_drift_paint(x, v, pot, c.kick, c.drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT)
+        force = _force_mesh(x)
+        ops.kick_drift_paint(x, v, force, c.kick, c.drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT)
         new_state = NBodyState(interp_state=self.interp_kernel.advance(state.interp_state, t1),
                                t_initial=state.t_initial)
         return (disp.replace(array=x, scale_factors=t1), velocities.replace(array=v, scale_factors=math.sqrt(t0 * t1)),
@@ -158,8 +159,8 @@ class ReversibleDoubleKickDrift(AbstractNBodySolver):
         x = disp.array.contiguous().clone()
         v = velocities.array.contiguous().clone()
         ops.kick_drift_paint(x, v, None, 0.0, -c.drift, JFLI_STEP_DRIFT)
-        pot = _forces_potential(x)
-        ops.kick_drift_paint(x, v, pot, -c.kick, 0.0, JFLI_STEP_KICK)
+        force = _force_mesh(x)
+        ops.kick_drift_paint(x, v, force, -c.kick, 0.0, JFLI_STEP_KICK)
         ts = self.interp_kernel.ts
         t1c = min(t1, float(ts[-1])) if ts is not None else t1
         prev = NBodyState(interp_state=self.interp_kernel.rewind(state.interp_state, t1c), t_initial=state.t_initial)

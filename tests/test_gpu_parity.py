@@ -229,9 +229,9 @@ def test_kick_drift_paint_matches_unfused(cosmo):
     kick, drift = 0.37, 0.81
     # fused on the GPU
     x, v = dev(x0), dev(v0)
-    pot = ops.poisson_potential(ops.paint_cic(x), 1.0)
+    force = ops.poisson_force(ops.paint_cic(x), 1.0)
     rho = torch.zeros(n, n, n, device="cuda")
-    ops.kick_drift_paint(x, v, pot, kick, drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT, rho)
+    ops.kick_drift_paint(x, v, force, kick, drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT, rho)
     # oracle
     rv = v0.astype(np.float64) + kick * opm.pm_forces(x0.astype(np.float64))
     rx = x0.astype(np.float64) + drift * rv
@@ -241,9 +241,9 @@ def test_kick_drift_paint_matches_unfused(cosmo):
 
 
 @pytest.mark.parametrize("spread", [0.3, 6.0, 14.0])
-def test_kick_drift_paint_tiled_and_fallback_paths(spread):
-    """Small spreads run from the shared-memory tiles, large ones exceed the tile and take
-    the global path; both must match the oracle. Also a 40^3 mesh with partial bricks."""
+def test_kick_drift_paint_small_and_large_displacements(spread):
+    """Displacements from a fraction of a cell to many cells (periodic wrap of the CIC
+    corners and of the force meshes), on a power-of-two and a 40^3 mesh."""
     from jfli_b200._lib import JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
 
     for n in (32, 40):
@@ -254,7 +254,8 @@ def test_kick_drift_paint_tiled_and_fallback_paths(spread):
         pot64 = opm.potential_real(1.0 + 0.3 * rng.normal(size=(n, n, n)))
         x, v = dev(x0), dev(v0)
         rho = torch.zeros(n, n, n, device="cuda")
-        ops.kick_drift_paint(x, v, dev(pot64), kick, drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT, rho)
+        force = ops.force_mesh(dev(pot64))
+        ops.kick_drift_paint(x, v, force, kick, drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT, rho)
         kvec = opm.fftk((n, n, n))
         pk = np.fft.fftn(pot64)
         F = np.stack([opm.cic_read(-np.fft.ifftn(opm.gradient_kernel(kvec, i) * pk).real, x0.astype(np.float64))
