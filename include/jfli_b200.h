@@ -139,6 +139,23 @@ int jfli_healpix_paint(void* stream, const float* disp, int absolute, const floa
                        float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside, int scheme,
                        float* map, int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen);
 
+/* P(k) that allocates nothing. This entry point has no counterpart in the reference.
+ *
+ * Some callers cannot allocate device memory when they need P(k): a JAX/XLA custom-call
+ * handler in a process where XLA has already reserved most of the GPU memory for its own
+ * pool, or code that is being recorded into a CUDA graph, where cudaMalloc is not
+ * allowed. This variant takes the same inputs and writes the same out[batch][3][nedges+1]
+ * sums as jfli_power_spectrum, but needs no workspace: its scratch (the half spectrum and
+ * the histogram partials) is an 11 MiB array compiled into the library, which every GPU
+ * that loads the library holds until the process exits. That bounds the mesh: up to
+ * 128^3 cells (with up to 128 bin edges); larger requests return JFLI_EUNSUPPORTED.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress),
+ * so make that first call before any stream capture. Every call overwrites the array, so
+ * two calls that run on the GPU at the same time (other streams, other host threads)
+ * corrupt each other's results; serialise them. */
+int jfli_power_spectrum_noalloc(void* stream, const float* mesh, const float* kedges, int nedges, float lx, float ly,
+                                float lz, double* out, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

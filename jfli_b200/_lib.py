@@ -81,6 +81,10 @@ _SIGNATURES = {
         [c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_void_p, c_void_p, c_size_t, *_DIMS,
          *_ERR],
     ),
+    "jfli_power_spectrum_noalloc": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_void_p, *_DIMS, *_ERR],
+    ),
     "jfli_healpix_paint": (
         c_int,
         [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float, c_float,

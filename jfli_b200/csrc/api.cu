@@ -382,4 +382,40 @@ int jfli_healpix_paint(void* stream, const float* disp, int absolute, const floa
       errlen, "jfli_healpix_paint");
 }
 
+// P(k) for callers that cannot allocate device memory: the same sums as
+// jfli_power_spectrum, with the half spectrum and the histogram partials kept in a
+// fixed device array inside the library instead of a caller workspace. The array is
+// shared by all calls on a device and holds the previous call's data; calls that
+// overlap on the GPU (different streams, or host threads) race on it.
+int jfli_power_spectrum_noalloc(void* stream, const float* mesh, const float* kedges, int nedges, float lx, float ly,
+                                float lz, double* out, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(mesh);
+  CHECK_PTR(kedges);
+  CHECK_PTR(out);
+  if (nedges < 1 || nedges > 2048) return fail(err, errlen, JFLI_EINVAL, "nedges %d outside [1, 2048]", nedges);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  const size_t spec = spec_bytes(d);
+  const size_t partials = align256((size_t)jfli::noalloc_pk_ctas(d) * batch * 3 * (nedges + 1) * sizeof(double));
+  const size_t cap = jfli::noalloc_scratch_bytes();
+  if (spec + partials > cap)
+    return fail(err, errlen, JFLI_EUNSUPPORTED,
+                "mesh (%d, %d, %d) x batch %d with %d edges needs %zu bytes of scratch; the built-in scratch holds "
+                "%zu bytes (up to a 128^3 mesh); use jfli_power_spectrum with a workspace",
+                nx, ny, nz, batch, nedges, spec + partials, cap);
+  void* base = nullptr;
+  cudaError_t e = jfli::noalloc_scratch(&base);
+  if (e != cudaSuccess) return cuda_status(e, err, errlen, "jfli_power_spectrum_noalloc scratch address");
+  cudaStream_t s = (cudaStream_t)stream;
+  const float box[3] = {lx, ly, lz};
+  const float norm = 1.0f / ((float)nx * (float)ny * (float)nz);
+  float2* specp = (float2*)base;
+  double* part = (double*)((char*)base + spec);
+  e = jfli::power_partials_noalloc(mesh, specp, part, d, kedges, nedges, box, norm, s);
+  if (e == cudaSuccess) e = jfli::power_finalize(part, jfli::noalloc_pk_ctas(d), nedges + 1, out, batch, s);
+  return cuda_status(e, err, errlen, "jfli_power_spectrum_noalloc");
+}
+
 }  // extern "C"

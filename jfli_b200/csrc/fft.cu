@@ -852,4 +852,95 @@ cudaError_t power_partials(const float* mesh, float2* spec, double* partials, co
   return launch_x_op(spec, d, op, s);
 }
 
+// ---------------------------------------------------------------------------------
+// P(k) without any allocation, for callers that cannot allocate device memory.
+//
+// The half spectrum and the per-CTA histogram partials live in one file-scope device
+// array of kNoAllocScratchBytes. The transforms use the shared-memory Stockham kernels,
+// which build their twiddles in the kernel, so no twiddle table is created either.
+// ---------------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = 11u << 20;  // 11 MiB: a 128^3 spectrum plus its partials
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_ptr[kNoAllocMaxDevices];  // device -> address of g_noalloc_scratch on it
+
+// Device address of the scratch array on the current device. The first call on a device
+// looks it up with cudaGetSymbolAddress (with that device current); later calls reuse it.
+cudaError_t noalloc_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+
+size_t noalloc_scratch_bytes() { return kNoAllocScratchBytes; }
+
+int noalloc_pk_ctas(const MeshDims& d) {
+  const ColGeom g = x_geom(d);
+  return (g.ncols + g.w - 1) / g.w;
+}
+
+cudaError_t power_partials_noalloc(const float* mesh, float2* spec, double* partials, const MeshDims& d,
+                                   const float* kedges, int nedges, const float* box, float norm, cudaStream_t s) {
+  // r2c along z (Stockham, twiddles built in the kernel)
+  {
+    FftPlan pl;
+    make_fft_plan(d.nz / 2, &pl);
+    const int nrows = d.nx * d.ny;
+    const int rows = z_rows_per_cta(d.nz);
+    const int nh = d.nz / 2;
+    const size_t smem = ((size_t)2 * (nh + 1) * (rows + 1) + nh + nh + 1) * sizeof(float2);
+    cudaFuncSetAttribute(k_rfft_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_rfft_z<<<dim3((nrows + rows - 1) / rows, d.batch), kFftThreads, smem, s>>>(mesh, spec, nrows, d.nz, rows, pl,
+                                                                               0.0f, d.cells(), d.spec_elems());
+    note_launch();
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  // forward y
+  {
+    const ColGeom g = y_geom(d);
+    FftPlan pl;
+    make_fft_plan(g.n, &pl);
+    const size_t smem = ((size_t)2 * g.n * g.w + g.n) * sizeof(float2);
+    cudaFuncSetAttribute(k_fft_cols<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fft_cols<-1><<<dim3((g.ncols + g.w - 1) / g.w, d.batch), kFftThreads, smem, s>>>(spec, g, pl, d.spec_elems());
+    note_launch();
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  // forward x feeding the histogram
+  PkOp op;
+  op.nx = d.nx;
+  op.ny = d.ny;
+  op.nz = d.nz;
+  op.kedges = kedges;
+  op.nedges = nedges;
+  op.cx = (float)(2.0 * M_PI / (double)box[0]);
+  op.cy = (float)(2.0 * M_PI / (double)box[1]);
+  op.cz = (float)(2.0 * M_PI / (double)box[2]);
+  op.norm = norm;
+  op.partials = partials;
+  const ColGeom g = x_geom(d);
+  FftPlan pl;
+  make_fft_plan(g.n, &pl);
+  const size_t smem = ((size_t)2 * g.n * g.w + g.n) * sizeof(float2) + PkOp::smem_bytes(op);
+  cudaFuncSetAttribute(k_fft_x_op<PkOp>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_fft_x_op<PkOp><<<dim3((g.ncols + g.w - 1) / g.w, d.batch), kFftThreads, smem, s>>>(spec, g, pl, op,
+                                                                                     d.spec_elems());
+  note_launch();
+  return cudaGetLastError();
+}
+
 }  // namespace jfli

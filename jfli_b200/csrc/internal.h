@@ -55,6 +55,13 @@ cudaError_t lpt_combine(const float* f1, const float* f2, float c1x, float c2x, 
                         float* p, const MeshDims& d, cudaStream_t s);
 cudaError_t axpy_particles(float* y, const float* x, float a, const MeshDims& d, cudaStream_t s);
 
+// P(k) whose scratch is a file-scope device array (no allocation).
+cudaError_t noalloc_scratch(void** out);
+size_t noalloc_scratch_bytes();
+int noalloc_pk_ctas(const MeshDims& d);
+cudaError_t power_partials_noalloc(const float* mesh, float2* spec, double* partials, const MeshDims& d,
+                                   const float* kedges, int nedges, const float* box, float norm, cudaStream_t s);
+
 // ---- spectra.cu ----
 cudaError_t power_finalize(const double* partials, int nctas, int nbins, double* out, int batch, cudaStream_t s);
 
