@@ -112,43 +112,21 @@ class ClockSampler:
 
 # --------------------------------------------------------------------------- distributed
 def dist_setup(args):
-    import torch
+    from jfli_b200 import replicas
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    elif torch.cuda.is_available():
-        torch.cuda.set_device(0)
-    return world, rank, local
+    return replicas.init(backend="nccl")
 
 
 def barrier(world):
-    import torch
+    from jfli_b200 import replicas
 
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-    torch.cuda.synchronize()
+    replicas.barrier()
 
 
 def max_over_ranks(val, world):
-    if world == 1:
-        return val
-    import torch
-    import torch.distributed as dist
+    from jfli_b200 import replicas
 
-    t = torch.tensor([val], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(val)
 
 
 # ----------------------------------------------------------------------------- GPU arm
@@ -227,8 +205,7 @@ def run_gpu(args, world, rank):
         clocks.start()
         t_wait = time.time()
         while not clocks.lines and time.time() - t_wait < 3.0:  # first sample before timing
-            one_step()
-            torch.cuda.synchronize()
+            time.sleep(0.05)
     for _ in range(args.warmup):
         one_step()
     restart()  # the timed window starts at the first step of the schedule
@@ -379,9 +356,9 @@ def main():
                 "gpu_launches": res["launches"]}
         print(json.dumps(line), flush=True)
     if world > 1:
-        import torch.distributed as dist
+        from jfli_b200 import replicas
 
-        dist.destroy_process_group()
+        replicas.finalize()
 
 
 if __name__ == "__main__":
