@@ -323,6 +323,54 @@ __global__ void k_force_mesh(const float* __restrict__ pot, float* __restrict__ 
   }
 }
 
+// The same stencil for four consecutive z cells per thread (nz % 4 == 0): 11 aligned
+// 16-byte loads and 3 16-byte stores per 4 cells, row offsets and wraps shared.
+__global__ void k_force_mesh4(const float* __restrict__ pot, float* __restrict__ F, float scale, PGrid g) {
+  const long long b = blockIdx.y;
+  pot += b * g.np;
+  F += b * g.np * 3;
+  const float s = scale / 12.0f;
+  const unsigned nq = g.np >> 2;  // groups of 4 cells
+  const int nz4 = g.nz >> 2;
+  for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+    const unsigned row = q / (unsigned)nz4;  // i * ny + j
+    const int k0 = (int)(q - row * (unsigned)nz4) << 2;
+    const int i = (int)(row / (unsigned)g.ny);
+    const int j = (int)row - i * g.ny;
+    const int xo = i * g.yz, yo = j * g.nz;
+    const float4* r = reinterpret_cast<const float4*>(pot + xo + yo);
+    const float4 zm = __ldg(r + (wrap1(k0 - 4, g.nz) >> 2));
+    const float4 z0 = __ldg(r + (k0 >> 2));
+    const float4 zp = __ldg(r + (wrap1(k0 + 4, g.nz) >> 2));
+    const float w[12] = {zm.x, zm.y, zm.z, zm.w, z0.x, z0.y, z0.z, z0.w, zp.x, zp.y, zp.z, zp.w};
+    float fz[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) fz[t] = -(8.0f * (w[5 + t] - w[3 + t]) - (w[6 + t] - w[2 + t])) * s;
+    const float* cx = pot + yo + k0;
+    const float4 xp1 = __ldg(reinterpret_cast<const float4*>(cx + wrap1(i + 1, g.nx) * g.yz));
+    const float4 xm1 = __ldg(reinterpret_cast<const float4*>(cx + wrap1(i - 1, g.nx) * g.yz));
+    const float4 xp2 = __ldg(reinterpret_cast<const float4*>(cx + wrap1(i + 2, g.nx) * g.yz));
+    const float4 xm2 = __ldg(reinterpret_cast<const float4*>(cx + wrap1(i - 2, g.nx) * g.yz));
+    const float* cy = pot + xo + k0;
+    const float4 yp1 = __ldg(reinterpret_cast<const float4*>(cy + wrap1(j + 1, g.ny) * g.nz));
+    const float4 ym1 = __ldg(reinterpret_cast<const float4*>(cy + wrap1(j - 1, g.ny) * g.nz));
+    const float4 yp2 = __ldg(reinterpret_cast<const float4*>(cy + wrap1(j + 2, g.ny) * g.nz));
+    const float4 ym2 = __ldg(reinterpret_cast<const float4*>(cy + wrap1(j - 2, g.ny) * g.nz));
+    const float4 fx = make_float4(-(8.0f * (xp1.x - xm1.x) - (xp2.x - xm2.x)) * s,
+                                  -(8.0f * (xp1.y - xm1.y) - (xp2.y - xm2.y)) * s,
+                                  -(8.0f * (xp1.z - xm1.z) - (xp2.z - xm2.z)) * s,
+                                  -(8.0f * (xp1.w - xm1.w) - (xp2.w - xm2.w)) * s);
+    const float4 fy = make_float4(-(8.0f * (yp1.x - ym1.x) - (yp2.x - ym2.x)) * s,
+                                  -(8.0f * (yp1.y - ym1.y) - (yp2.y - ym2.y)) * s,
+                                  -(8.0f * (yp1.z - ym1.z) - (yp2.z - ym2.z)) * s,
+                                  -(8.0f * (yp1.w - ym1.w) - (yp2.w - ym2.w)) * s);
+    const unsigned c = (unsigned)(xo + yo + k0);
+    reinterpret_cast<float4*>(F + c)[0] = fx;
+    reinterpret_cast<float4*>(F + g.np + c)[0] = fy;
+    reinterpret_cast<float4*>(F + 2ull * g.np + c)[0] = make_float4(fz[0], fz[1], fz[2], fz[3]);
+  }
+}
+
 // CIC readout of the three force meshes at one particle.
 __device__ __forceinline__ void gather_force_mesh(const float* __restrict__ F, const PGrid& g, const Cic1& cx,
                                                   const Cic1& cy, const Cic1& cz, float& fx, float& fy, float& fz) {
@@ -516,7 +564,12 @@ cudaError_t kick_drift_paint(float* disp, float* vel, const float* force, float 
 }
 
 cudaError_t force_mesh(const float* pot, float* force, float scale, const MeshDims& d, cudaStream_t s) {
-  k_force_mesh<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, force, scale, make_pgrid(d));
+  const bool vec4 = d.nz % 4 == 0 && d.nz >= 8 && ((uintptr_t)pot % 16) == 0 && ((uintptr_t)force % 16) == 0;
+  if (vec4)
+    k_force_mesh4<<<particle_grid_dims(d.cells() / 4, d.batch, 256, 16), 256, 0, s>>>(pot, force, scale,
+                                                                                     make_pgrid(d));
+  else
+    k_force_mesh<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, force, scale, make_pgrid(d));
   note_launch();
   return cudaGetLastError();
 }

@@ -104,6 +104,17 @@ def test_pm_forces_matches_oracle(n, scale):
     assert rel_l2(f, ref) < 1e-5
 
 
+@pytest.mark.parametrize("shape", [(32, 32, 32), (16, 24, 36), (12, 20, 42), (8, 8, 4)])
+def test_force_mesh_matches_stencil(shape):
+    """Force meshes -D_a pot (vectorised path when nz % 4 == 0 and nz >= 8, scalar otherwise)."""
+    pot = np.random.default_rng(sum(shape)).normal(size=shape)
+    F = host(ops.force_mesh(dev(pot), scale=2.0))
+    for ax in range(3):
+        r = lambda s: np.roll(pot, -s, axis=ax)
+        ref = -2.0 * (8 * (r(1) - r(-1)) - (r(2) - r(-2))) / 12
+        np.testing.assert_allclose(F[ax], ref, rtol=1e-5, atol=1e-5)
+
+
 def test_readout_gradient_absolute_equals_relative():
     n = 32
     disp = lpt_disp(n, 3.0, seed=11).astype(np.float32)
