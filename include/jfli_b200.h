@@ -111,6 +111,16 @@ int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift,
                  void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
                  size_t errlen);
 
+/* One PM step over `batch` independent simulations of the same mesh size, each with its
+ * own schedule: slot b is kicked by kicks[b], drifted by drifts[b] with slot_flags[b]
+ * (JFLI_STEP_* bits; 0 leaves the slot untouched), painted, and gets new force meshes.
+ * kicks, drifts, slot_flags are device arrays of length batch, so the launches can be
+ * recorded once and replayed with new per-slot factors. Replaces a vmapped step() over a
+ * batch of forward-model evaluations (probabilistic_models/forward_model.py:24-79). */
+int jfli_pm_step_slots(void* stream, float* disp, float* vel, const float* kicks, const float* drifts,
+                       const int* slot_flags, float* rho, float* force, void* workspace, size_t workspace_bytes, int nx,
+                       int ny, int nz, int batch, char* err, size_t errlen);
+
 /* out = irfft(rfft(noise) * sqrt(P(|k|) * M / V)), P by linear interpolation (with end
  * extrapolation) of the device tables ktab/ptab (h/Mpc, (Mpc/h)^3). zero_mode_one sets
  * P(k=0) to 1. Workspace: jfli_poisson_workspace_bytes. */

@@ -64,6 +64,11 @@ _SIGNATURES = {
         c_int,
         [c_void_p, c_void_p, c_void_p, c_float, c_float, c_int, c_void_p, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
     ),
+    "jfli_pm_step_slots": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, *_DIMS,
+         *_ERR],
+    ),
     "jfli_ic_filter": (
         c_int,
         [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_int, c_void_p,

@@ -31,7 +31,7 @@ import functools
 import math
 
 import numpy as np
-from scipy.integrate import quad, solve_ivp
+from scipy.integrate import odeint
 
 RH = 2997.92458  # Hubble radius c/H0 in Mpc/h
 TCMB = 2.7255
@@ -135,7 +135,21 @@ class GrowthTable:
     d2g: np.ndarray  # d^2 (D1/D1(1)) / da^2
 
 
-@functools.lru_cache(maxsize=256)
+def _q_r_scalar(c: Cosmology, a: float):
+    """Coefficients of the growth ODE at one scale factor (plain floats, no arrays)."""
+    if c.wa == 0.0:
+        de = c.Omega_de * a ** (-3.0 * (1.0 + c.w0))
+    else:
+        de = c.Omega_de * a ** (-3.0 * (1.0 + c.w0 + c.wa) + 3.0 * c.wa * (a - 1.0) / math.log(a))
+    m = c.Omega_m / (a * a * a)
+    e2 = m + c.Omega_k / (a * a) + de
+    om = m / e2
+    ode = de / e2
+    wa = c.w0 + c.wa * (1.0 - a)
+    return (2.0 - 0.5 * (om + (1.0 + 3.0 * wa) * ode)) / a, 1.5 * om / (a * a)
+
+
+@functools.lru_cache(maxsize=1024)
 def growth_table(c: Cosmology, log10_amin: float = -3.0, steps: int = 128) -> GrowthTable:
     atab = np.logspace(log10_amin, 0.0, steps)
 
@@ -146,15 +160,15 @@ def growth_table(c: Cosmology, log10_amin: float = -3.0, steps: int = 128) -> Gr
         r = 1.5 * om / (a * a)
         return q, r
 
-    def rhs(a, y):
+    def rhs(y, a):
         g1, d1, g2, d2 = y
-        q, r = q_r(a)
+        q, r = _q_r_scalar(c, a)
         return [d1, -q * d1 + r * g1, d2, -q * d2 + r * g2 - r * g1 * g1]
 
     a0 = atab[0]
     y0 = [a0, 1.0, -3.0 / 7.0 * a0 * a0, -6.0 / 7.0 * a0]
-    sol = solve_ivp(rhs, (a0, 1.0), y0, t_eval=atab, method="DOP853", rtol=1e-12, atol=1e-15)
-    g1, d1, g2, d2 = sol.y
+    sol = odeint(rhs, y0, atab, rtol=1e-12, atol=1e-15)  # LSODA
+    g1, d1, g2, d2 = sol.T
     q, r = q_r(atab)
     dd1 = -q * d1 + r * g1
     gtab = g1 / g1[-1]
@@ -218,18 +232,22 @@ class DistanceTable:
     chi: np.ndarray
 
 
-@functools.lru_cache(maxsize=256)
+@functools.lru_cache(maxsize=1024)
 def distance_table(c: Cosmology, log10_amin: float = -3.0, steps: int = 256) -> DistanceTable:
     atab = np.logspace(log10_amin, 0.0, steps)
-    lna = np.log(atab)
-
-    def integrand(x):  # d chi / d ln a = a * (1 / (a^2 E)) = 1 / (a E)
-        a = math.exp(x)
-        return 1.0 / (a * float(E(c, a)))
-
-    chi = np.zeros_like(atab)
-    for i in range(steps - 2, -1, -1):
-        chi[i] = chi[i + 1] + quad(integrand, lna[i], lna[i + 1], epsabs=0, epsrel=1e-13)[0]
+    # d chi / d ln a = 1 / (a E): composite Simpson on 16 sub-intervals per table interval
+    sub = 16
+    x = np.linspace(np.log(atab[0]), 0.0, (steps - 1) * sub + 1)
+    a = np.exp(x)
+    f = 1.0 / (a * E(c, a))
+    h = x[1] - x[0]
+    seg = f[:-1].reshape(steps - 1, sub)
+    fe = np.append(f[sub::sub], [])  # right ends
+    # Simpson over each table interval: h/3 [f0 + 4 f_odd + 2 f_even + f_end]
+    odd = seg[:, 1::2].sum(axis=1)
+    even = seg[:, 2::2].sum(axis=1)
+    piece = h / 3.0 * (seg[:, 0] + 4.0 * odd + 2.0 * even + fe)
+    chi = np.concatenate([np.cumsum(piece[::-1])[::-1], [0.0]])
     return DistanceTable(a=atab, chi=RH * chi)
 
 
@@ -303,20 +321,24 @@ def eisenstein_hu_transfer(c: Cosmology, k):
     return fb * Tb + fc * Tc
 
 
-@functools.lru_cache(maxsize=256)
-def _sigma8_norm(c: Cosmology) -> float:
+@functools.lru_cache(maxsize=1024)
+def _sigma_r8_unnormalised(c: Cosmology) -> float:
+    """sigma^2(8 Mpc/h) of k^ns T(k)^2 (Simpson on a dense log-k grid; depends on
+    everything but sigma8, so sigma8 alone rescales without recomputation)."""
     R = 8.0
+    lnk = np.linspace(math.log(1e-5), math.log(1e3), 16385)
+    k = np.exp(lnk)
+    x = k * R
+    small = x < 1e-4
+    xs = np.where(small, 1.0, x)
+    wt = np.where(small, 1.0 - x * x / 10.0, 3.0 * (np.sin(xs) - xs * np.cos(xs)) / xs ** 3)
+    f = k ** 3 * k ** c.n_s * eisenstein_hu_transfer(c, k) ** 2 * wt * wt / (2.0 * math.pi ** 2)
+    h = lnk[1] - lnk[0]
+    return float(h / 3.0 * (f[0] + 4.0 * f[1:-1:2].sum() + 2.0 * f[2:-1:2].sum() + f[-1]))
 
-    def integrand(lnk):
-        k = math.exp(lnk)
-        x = k * R
-        wt = 3.0 * (math.sin(x) - x * math.cos(x)) / x ** 3 if x > 1e-4 else 1.0 - x * x / 10.0
-        pk = k ** c.n_s * float(eisenstein_hu_transfer(c, k)) ** 2
-        return k ** 3 * pk * wt * wt / (2.0 * math.pi ** 2)
 
-    edges = np.linspace(math.log(1e-5), math.log(1e3), 65)
-    s2 = sum(quad(integrand, edges[i], edges[i + 1], limit=200, epsrel=1e-11)[0] for i in range(64))
-    return c.sigma8 ** 2 / s2
+def _sigma8_norm(c: Cosmology) -> float:
+    return c.sigma8 ** 2 / _sigma_r8_unnormalised(c.replace(sigma8=1.0))
 
 
 def linear_matter_power(c: Cosmology, k, a=1.0):

@@ -270,6 +270,34 @@ int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift,
   return cuda_status(e, err, errlen, "jfli_pm_step");
 }
 
+int jfli_pm_step_slots(void* stream, float* disp, float* vel, const float* kicks, const float* drifts,
+                       const int* slot_flags, float* rho, float* force, void* workspace, size_t workspace_bytes, int nx,
+                       int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(disp);
+  CHECK_PTR(vel);
+  CHECK_PTR(kicks);
+  CHECK_PTR(drifts);
+  CHECK_PTR(slot_flags);
+  CHECK_PTR(rho);
+  CHECK_PTR(force);
+  CHECK_PTR(workspace);
+  const MeshDims d{nx, ny, nz, batch};
+  const size_t need = jfli_pm_step_workspace_bytes(nx, ny, nz, batch);
+  if (workspace_bytes < need)
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  cudaStream_t s = (cudaStream_t)stream;
+  float2* spec = (float2*)workspace;
+  float* pot = (float*)((char*)workspace + spec_bytes(d));
+  cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
+  if (e == cudaSuccess) e = jfli::kick_drift_paint_slots(disp, vel, force, kicks, drifts, slot_flags, 1.0f, rho, d, s);
+  if (e == cudaSuccess) e = jfli::poisson_potential(rho, spec, pot, d, 1.0f, 1.0f, s);
+  if (e == cudaSuccess) e = jfli::force_mesh(pot, force, 1.0f, d, s);
+  return cuda_status(e, err, errlen, "jfli_pm_step_slots");
+}
+
 int jfli_ic_filter(void* stream, const float* noise, float* out, const float* ktab, const float* ptab, int ntab,
                    float lx, float ly, float lz, int zero_mode_one, void* workspace, size_t workspace_bytes, int nx,
                    int ny, int nz, int batch, char* err, size_t errlen) {

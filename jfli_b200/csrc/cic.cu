@@ -251,10 +251,19 @@ __device__ __forceinline__ void gather_force_mesh(const float* __restrict__ F, c
 
 // One fused particle pass of a PM step. Order inside: kick (with the force at the
 // current position) -> drift (with the kicked velocity) -> paint (at the new position).
+// With per-slot arrays (kicks != nullptr) every batch entry b takes its own kick, drift
+// and flags from kicks[b], drifts[b], slot_flags[b]; flags 0 leaves the slot untouched.
 __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ force,
                                    float kick, float drift, int flags, float weight, float* __restrict__ rho,
-                                   PGrid g) {
+                                   PGrid g, const float* __restrict__ kicks, const float* __restrict__ drifts,
+                                   const int* __restrict__ slot_flags) {
   const long long b = blockIdx.y;
+  if (kicks) {
+    kick = kicks[b];
+    drift = drifts[b];
+    flags = slot_flags[b];
+    if (flags == 0) return;
+  }
   disp += b * g.np * 3;
   vel += b * g.np * 3;
   if (force) force += b * g.np * 3;
@@ -557,8 +566,17 @@ cudaError_t cic_readout_gradient(const float* pos, int absolute, const float* po
 
 cudaError_t kick_drift_paint(float* disp, float* vel, const float* force, float kick, float drift, int flags,
                              float weight, float* rho, const MeshDims& d, cudaStream_t s) {
-  k_kick_drift_paint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(disp, vel, force, kick, drift,
-                                                                                     flags, weight, rho, make_pgrid(d));
+  k_kick_drift_paint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(
+      disp, vel, force, kick, drift, flags, weight, rho, make_pgrid(d), nullptr, nullptr, nullptr);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t kick_drift_paint_slots(float* disp, float* vel, const float* force, const float* kicks,
+                                   const float* drifts, const int* slot_flags, float weight, float* rho,
+                                   const MeshDims& d, cudaStream_t s) {
+  k_kick_drift_paint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(
+      disp, vel, force, 0.f, 0.f, 0, weight, rho, make_pgrid(d), kicks, drifts, slot_flags);
   note_launch();
   return cudaGetLastError();
 }

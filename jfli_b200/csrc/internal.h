@@ -48,6 +48,9 @@ cudaError_t cic_readout_gradient(const float* pos, int absolute, const float* po
 cudaError_t kick_drift_paint(float* disp, float* vel, const float* force, float kick, float drift, int flags,
                              float weight, float* rho, const MeshDims& d, cudaStream_t s);
 cudaError_t force_mesh(const float* pot, float* force, float scale, const MeshDims& d, cudaStream_t s);
+cudaError_t kick_drift_paint_slots(float* disp, float* vel, const float* force, const float* kicks,
+                                   const float* drifts, const int* slot_flags, float weight, float* rho,
+                                   const MeshDims& d, cudaStream_t s);
 cudaError_t grid_gradient(const float* pot, float* out, float scale, int accumulate, const MeshDims& d,
                           cudaStream_t s);
 cudaError_t lpt2_source(const float* pot, float* out, const MeshDims& d, cudaStream_t s);

@@ -15,6 +15,7 @@ import dataclasses
 import math
 from typing import Any
 
+import numpy as np
 import torch
 
 from .. import cosmology as cj
@@ -91,6 +92,20 @@ class EfficientDriftDoubleKick(AbstractNBodySolver):
         k2 = (cj.Gf(cosmo, t1t2) - cj.Gf(cosmo, t1)) / cj.dGfa(cosmo, ac)
         kick = 1.5 * cosmo.Omega_m * (k1 + k2) / (ac**2 * cj.E(cosmo, ac))
         return StepCoefficients(kick=float(kick), drift=float(drift), kick_first=False)
+
+    @staticmethod
+    def schedule_arrays(cosmo, t0s, t1s, dt, t_initial=None):
+        """Vectorised step_coefficients over arrays of step boundaries -> (kicks, drifts)."""
+        t0s = np.asarray(t0s, np.float64)
+        t1s = np.asarray(t1s, np.float64)
+        t0t1 = np.sqrt(t0s * t1s)
+        drift = (cj.Gp(cosmo, t1s) - cj.Gp(cosmo, t0s)) / cj.gp(cosmo, t0t1) / (t0t1**3 * cj.E(cosmo, t0t1))
+        t1t2 = np.sqrt(t1s * (t1s + dt))
+        dg = cj.dGfa(cosmo, t1s)
+        k1 = (cj.Gf(cosmo, t1s) - cj.Gf(cosmo, t0t1)) / dg
+        k2 = (cj.Gf(cosmo, t1t2) - cj.Gf(cosmo, t1s)) / dg
+        kick = 1.5 * cosmo.Omega_m * (k1 + k2) / (t1s**2 * cj.E(cosmo, t1s))
+        return kick, drift
 
     def init(self, displacement, velocities, t0, t1, dt, cosmo):
         state = NBodyState(interp_state=self.interp_kernel.init(), t_initial=t0)
