@@ -18,6 +18,11 @@ schedule restarts from the initial conditions inside the timed region.
           read, density written) per launch, over its CUDA-event time, against
           MEASURED_PEAKS.json
   cpu_baseline : the NumPy/SciPy FP32 port of the same step (oracle/pm.py) on this host
+  serving : the request stream (512 Poisson arrivals over mesh 64/96/128/192, 10-40 KDK
+          steps, mixed cosmologies) through the continuous-batching engine
+          (jfli_b200.serving) and through the plain per-call path at the same offered
+          load: p50/p99 latency and Mpart-steps/s of each, the engine's capacity with all
+          requests queued at once, and 256^3 requests served two at a time vs one by one
 
 --gpus N runs N independent replicas (one per GPU, no collective on the data path);
 value is the sum over ranks / the max-over-ranks time. --impl reference times the CPU
@@ -44,7 +49,7 @@ sys.path.insert(0, ROOT)
 N_MESH = 256
 BOX = 1000.0
 E2E_STEPS = 40
-METRIC = "Mpart-steps/s at 256^3 (PM KDK step, 2LPT ICs, L=1000 Mpc/h)"
+METRIC = "Mpart-steps/s at 256\u00b3 served vs plain GPU @P(k) err<1e-4; p50/p99 latency"
 
 
 def parse():
@@ -56,6 +61,9 @@ def parse():
     ap.add_argument("--mesh", type=int, default=N_MESH)
     ap.add_argument("--e2e-requests", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=512)
+    ap.add_argument("--serve-rate", type=float, default=150.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-256", type=int, default=6, help="256^3 requests for the served-vs-plain pair")
     return ap.parse_args()
 
 
@@ -229,6 +237,7 @@ def run_gpu(args, world, rank):
 
     # ---- end-to-end through the public API, host buffers in and out
     e2e = run_e2e(args, cosmo, n, box)
+    serve = run_serving(args) if world == 1 else None
     # clocks are sampled every 200 ms from before the warm-up through the e2e requests
     clk = clocks.stop() if rank == 0 else None
 
@@ -242,7 +251,7 @@ def run_gpu(args, world, rank):
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
             "peak_source": "measured" if peaks else "fallback", "avg_launch_ms": round(kdp_avg_ms, 4),
             "algorithmic_bytes_per_launch": alg_bytes, "step_share": round(sum(kdp) / ms, 4)}
-    return dict(value=value, ms=ms_max, clocks=clk, launches=launches, e2e=e2e, roofline=roof)
+    return dict(value=value, ms=ms_max, clocks=clk, launches=launches, e2e=e2e, roofline=roof, serving=serve)
 
 
 def run_e2e(args, cosmo, n, box):
@@ -286,6 +295,64 @@ def run_e2e(args, cosmo, n, box):
     return {"value": round(val, 2), "unit": "Mpart-steps/s", "h2d_bytes_per_step": n**3 * 4,
             "d2h_bytes_per_step": n**3 * 4 + 32 * 8, "per": "request (ICs + 2LPT + %d KDK steps + P(k))" % steps,
             "ms_per_request": round(ms / args.e2e_requests, 2)}
+
+
+def run_serving(args):
+    """The request stream (Poisson arrivals; mesh 64/96/128/192; L = 4 Mpc/h per cell;
+    Omega_c ~ U[0.20, 0.35]; sigma8 ~ U[0.70, 0.90]; 10-40 KDK steps; seed = request id)
+    through the batched engine and through the plain per-call path at the same offered
+    load, plus 256^3 requests (40 steps, L = 1000 Mpc/h) served two at a time vs one by
+    one. Every request returns its P(k) (32 bins) to the host; densities stay on the device."""
+    import torch
+
+    from jfli_b200 import serving
+
+    if args.serve_requests <= 0:
+        return None
+    reqs = serving.poisson_stream(args.serve_requests, args.serve_rate, seed=0, grad_fraction=0.0)
+    eng = serving.Engine(sizes=(64, 96, 128, 192), hbm_budget_gb=24.0, max_slots=16, keep_density=False)
+    warm = serving.poisson_stream(16, 0.0, seed=1, grad_fraction=0.0)
+    for r in warm:
+        r.rid += 10**6
+    eng.run(warm, realtime=False)  # graphs, FFT tables, worker processes
+    serving.run_plain(warm[:4], realtime=False, keep_density=False)
+    torch.cuda.synchronize()
+    l0 = __import__("jfli_b200").ops.launch_count()
+    served = eng.run(reqs, realtime=True)
+    launches = __import__("jfli_b200").ops.launch_count() - l0
+    s_stats = serving.summarize(served, reqs)
+    burst = [dataclasses_replace(r, rid=r.rid + 2 * 10**6, arrival=0.0) for r in reqs]
+    s_cap = serving.summarize(eng.run(burst, realtime=False), burst)
+    eng.close()
+    plain = serving.run_plain(reqs, realtime=True, keep_density=False)
+    p_stats = serving.summarize(plain, reqs)
+    worst = max(serving.pk_max_rel(served[r.rid].pk, plain[r.rid].pk) for r in reqs)
+
+    out = {"stream": f"{len(reqs)} requests, Poisson arrivals at {args.serve_rate:g}/s, mesh U{{64,96,128,192}}, "
+                     f"10-40 KDK steps, no gradient requests (the adjoint is not on the batched path)",
+           "served": s_stats, "served_all_at_once": s_cap, "plain": p_stats,
+           "slots": eng.capacity(), "served_launches": launches,
+           "max_pk_rel_served_vs_plain": float(f"{worst:.3e}")}
+    if args.serve_256 > 0:
+        big = [serving.ForwardRequest(rid=3 * 10**6 + i, mesh=256, box=1000.0, omega_c=0.2607, sigma8=0.8102,
+                                      steps=40, seed=i) for i in range(args.serve_256)]
+        e256 = serving.Engine(sizes=(256,), hbm_budget_gb=2.0, max_slots=2, keep_density=False, workers=2)
+        e256.run(big[:2], realtime=False)
+        big2 = [dataclasses_replace(r, rid=r.rid + 100) for r in big]
+        s256 = serving.summarize(e256.run(big2, realtime=False), big2)
+        e256.close()
+        p256 = serving.summarize(serving.run_plain(big, realtime=False, keep_density=False), big)
+        out["at_256"] = {"requests": len(big), "served_mpart_steps_per_s": s256["mpart_steps_per_s"],
+                         "plain_mpart_steps_per_s": p256["mpart_steps_per_s"], "served_p50_ms": s256["p50_ms"],
+                         "plain_p50_ms": p256["p50_ms"], "slots": 2,
+                         "per": "request: ICs + 2LPT + 40 KDK steps + P(k) to host"}
+    return out
+
+
+def dataclasses_replace(obj, **kw):
+    import dataclasses
+
+    return dataclasses.replace(obj, **kw)
 
 
 # ----------------------------------------------------------------------------- CPU arm
@@ -359,7 +426,7 @@ def main():
                            "solver": "EfficientDriftDoubleKick", "parallelism": f"replicas x{world}",
                            "l2": "particle state (x, v: 402 MB) exceeds the 126 MB L2; no flush"},
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"], "clocks": res["clocks"],
-                "gpu_launches": res["launches"]}
+                "gpu_launches": res["launches"], "serving": res["serving"]}
         print(json.dumps(line), flush=True)
     if world > 1:
         from jfli_b200 import replicas

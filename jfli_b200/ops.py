@@ -198,11 +198,21 @@ def ic_filter(noise: torch.Tensor, ktab: torch.Tensor, ptab: torch.Tensor, box_s
     return out
 
 
-def lpt(ic: torch.Tensor, order: int, c1x: float, c2x: float, c1p: float, c2p: float):
+def lpt(ic: torch.Tensor, order: int, c1x: float, c2x: float, c1p: float, c2p: float,
+        dx: torch.Tensor | None = None, p: torch.Tensor | None = None):
+    """(displacement, momentum) particle grids; written into dx / p when given."""
     _check(ic, "ic")
     (nx, ny, nz), batch, lead = _mesh_dims(ic, False)
-    dx = torch.empty(*lead, nx, ny, nz, 3, dtype=torch.float32, device=ic.device)
-    p = torch.empty_like(dx)
+    shape = (*lead, nx, ny, nz, 3)
+    for name, t in (("dx", dx), ("p", p)):
+        if t is not None:
+            _check(t, name)
+            if tuple(t.shape) != shape:
+                raise ValueError(f"{name} must have shape {shape}")
+    if dx is None:
+        dx = torch.empty(shape, dtype=torch.float32, device=ic.device)
+    if p is None:
+        p = torch.empty(shape, dtype=torch.float32, device=ic.device)
     nb = query("jfli_lpt_workspace_bytes", nx, ny, nz, batch)
     ws = workspace(nb, "lpt", ic.device)
     call("jfli_lpt", stream_ptr(), ptr(ic), int(order), float(c1x), float(c2x), float(c1p), float(c2p), ptr(dx),

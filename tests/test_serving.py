@@ -1,0 +1,95 @@
+"""Continuous batching: each request's density and P(k) are the same served alone, served
+in a mix (admitted mid-stream into freed slots, batched with other cosmologies and step
+counts), and computed by the plain per-call path (lpt -> nbody -> power)."""
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+PK_TOL = 1e-4  # per bin, relative
+RHO_TOL = 1e-5  # relative L2 of the density
+
+
+def _stream():
+    from jfli_b200 import serving
+
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(9):
+        n = (64, 96)[i % 2]
+        reqs.append(serving.ForwardRequest(rid=i, mesh=n, box=4.0 * n, omega_c=float(rng.uniform(0.2, 0.35)),
+                                           sigma8=float(rng.uniform(0.7, 0.9)), steps=int(rng.integers(10, 15)),
+                                           seed=100 + i, arrival=0.0))
+    return reqs
+
+
+def _pk_rel(a, b):
+    """Max per-bin relative difference; bins with no modes (P = 0 in both) are equal."""
+    both_empty = (a == 0) & (b == 0)
+    return float(np.max(np.where(both_empty, 0.0, np.abs(a / np.where(b == 0, 1.0, b) - 1))))
+
+
+def _rel_l2(a, b):
+    a = a.double()
+    b = b.double()
+    return float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def runs():
+    from jfli_b200 import serving
+
+    reqs = _stream()
+    plain = serving.run_plain(reqs, realtime=False)
+    # 2 slots per size for 4-5 requests per size: later requests join while others run
+    eng = serving.Engine(sizes=(64, 96), max_slots=2, workers=2)
+    try:
+        mixed = eng.run(reqs, realtime=False)
+    finally:
+        eng.close()
+    alone = {}
+    for r in reqs[:2]:
+        e1 = serving.Engine(sizes=(r.mesh,), max_slots=1, workers=0, use_graph=False)
+        alone.update(e1.run([r], realtime=False))
+    return reqs, plain, mixed, alone
+
+
+def test_mix_matches_plain(runs):
+    reqs, plain, mixed, _ = runs
+    worst_pk = worst_rho = 0.0
+    for r in reqs:
+        a, b = mixed[r.rid], plain[r.rid]
+        assert a.steps == b.steps == r.steps
+        np.testing.assert_allclose(a.k, b.k, rtol=1e-6)
+        worst_pk = max(worst_pk, _pk_rel(a.pk, b.pk))
+        worst_rho = max(worst_rho, _rel_l2(a.density, b.density))
+    print(f"served vs plain: max P(k) rel {worst_pk:.2e}, max density rel L2 {worst_rho:.2e}")
+    assert worst_pk < PK_TOL
+    assert worst_rho < RHO_TOL
+
+
+def test_alone_matches_mix(runs):
+    reqs, _, mixed, alone = runs
+    for rid, a in alone.items():
+        m = mixed[rid]
+        assert _pk_rel(a.pk, m.pk) < PK_TOL
+        assert _rel_l2(a.density, m.density) < RHO_TOL
+
+
+def test_mix_overlaps_requests(runs):
+    """Later requests were admitted before earlier ones finished (continuous batching)."""
+    reqs, _, mixed, _ = runs
+    res = sorted(mixed.values(), key=lambda r: r.admitted)
+    overlaps = sum(1 for i in range(1, len(res)) if res[i].admitted < res[i - 1].done)
+    assert overlaps >= len(res) // 2
+
+
+def test_rejects_unknown_size():
+    from jfli_b200 import serving
+
+    eng = serving.Engine(sizes=(64,), max_slots=1, workers=0)
+    r = serving.ForwardRequest(rid=0, mesh=96, box=384.0, omega_c=0.25, sigma8=0.8, steps=10, seed=0)
+    with pytest.raises(ValueError):
+        eng.run([r], realtime=False)
