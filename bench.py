@@ -8,8 +8,8 @@ evaluation. The timed steps walk the real 40-step schedule from a = 0.1 to a = 1
 own kick/drift factors (the default --steps 40 is one whole simulation); past its end the
 schedule restarts from the initial conditions inside the timed region.
 
-  value : Mpart-steps/s with particles resident in HBM (the 201 MB particle state and
-          the 67 MB meshes exceed... the state is larger than the 126 MB L2, so no flush)
+  value : Mpart-steps/s with particles resident in HBM (positions and velocities are
+          402 MB, larger than the 126 MB L2, so no flush between steps)
   e2e   : the same metric through the public API (jfli_b200.interpolate_initial_conditions
           -> lpt -> nbody -> power) from pinned host white noise to host density + P(k),
           40 KDK steps per request, copies inside the timed region
@@ -248,10 +248,22 @@ def run_gpu(args, world, rank):
     alg_bytes = 48.0 * particles + 16.0 * particles  # x, v read+write; 3 force meshes read; density written
     achieved = alg_bytes / (kdp_avg_ms / 1e3) / 1e9
     roof = {"kernel": "k_kick_drift_paint", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": ncu_traffic(n),
             "peak_source": "measured" if peaks else "fallback", "avg_launch_ms": round(kdp_avg_ms, 4),
             "algorithmic_bytes_per_launch": alg_bytes, "step_share": round(sum(kdp) / ms, 4)}
     return dict(value=value, ms=ms_max, clocks=clk, launches=launches, e2e=e2e, roofline=roof, serving=serve)
+
+
+def ncu_traffic(n):
+    """DRAM bytes (read + write) per k_kick_drift_paint launch from the committed ncu
+    summary of this mesh size, or None when no capture exists for it."""
+    import re
+
+    path = os.path.join(ROOT, "profiles", f"k_kick_drift_paint_{n}_dram.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*(\d+)", open(path).read())
+    return int(m.group(1)) if m else None
 
 
 def run_e2e(args, cosmo, n, box):
