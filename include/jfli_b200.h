@@ -27,6 +27,15 @@
  *   jfli_lpt               <- pm/lpt.py:119 (jaxpm lpt, order 1 and 2)
  *   jfli_power_spectrum    <- _src/power/_compute.py:23-119 (_initialize_pk + _power)
  *   jfli_healpix_paint     <- _src/fields/_painting.py:249-348 (jaxpm paint_particles_spherical)
+ * Adjoints (the reverse-mode derivatives jax.grad takes through the same code, and the
+ * backward loop of the reversible adjoint, pm/integrate.py:147-535):
+ *   jfli_adjoint_unkick_paint, jfli_poisson_divergence, jfli_adjoint_position
+ *                          <- _integrate_bwd (pm/integrate.py:288-535): solver.reverse
+ *                             (pm/solvers.py:327-411) + VJP of ReversibleDoubleKickDrift.step
+ *                             (pm/solvers.py:258-325) through _forces (pm/solvers.py:19-32)
+ *   jfli_power_spectrum_adjoint <- VJP of _power (_src/power/_compute.py:68-119)
+ *   jfli_lpt_adjoint       <- VJP of jaxpm lpt (pm/lpt.py:119)
+ *   jfli_ic_filter_tangent <- derivative of initial.py:167-182 with respect to the P(k) table
  */
 #ifndef JFLI_B200_H
 #define JFLI_B200_H
@@ -148,6 +157,55 @@ int jfli_power_spectrum(void* stream, const float* mesh, const float* kedges, in
 int jfli_healpix_paint(void* stream, const float* disp, int absolute, const float* weights, float weight, float lx,
                        float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside, int scheme,
                        float* map, int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* ---- adjoints ------------------------------------------------------------------
+ * Reverse sweep of one reversible KKD step  v' = v + kick F(x);  x' = x + drift v'
+ * (F the CIC readout of the three force meshes), after the caller has un-drifted the
+ * positions (x = x' - drift v') and rebuilt the force meshes at x:
+ *   jfli_adjoint_unkick_paint: per particle u = lam_v + drift lam_x; v = v' - kick F(x);
+ *     lam_v = u; ubar_a = CIC paint of u_a (three meshes [batch][3][nx][ny][nz], cleared
+ *     first); partials[batch][nctas][2] = per-CTA sums of <u, F> (dL/dkick) and
+ *     <lam_x, v'> (dL/ddrift), nctas = jfli_adjoint_partials_count / (2 batch).
+ *   jfli_poisson_divergence: out = scale * P(sum_a D_a (alpha u_a + beta w_a)), P the
+ *     Poisson operator -1/k^2 (k = 0 -> 0), D_a the 4-point finite difference; u and w
+ *     are three meshes (aos = 0) or particle grids (aos = 1); w may be NULL. With
+ *     u = ubar it gives the density cotangent rho_bar of the force readout.
+ *   jfli_adjoint_position: lam_x += scale * grad_x R_x[rho_bar + sum_a u_a force_a] at
+ *     the relative positions disp (R the CIC readout; rho_bar or u/force may be NULL).
+ *     With scale = kick, u = lam_v it completes the step VJP; with force = NULL it is
+ *     the adjoint of the CIC paint. */
+size_t jfli_adjoint_partials_count(int nx, int ny, int nz, int batch);
+int jfli_adjoint_unkick_paint(void* stream, const float* disp, float* vel, const float* lam_x, float* lam_v,
+                              const float* force, float kick, float drift, float* ubar, double* partials,
+                              size_t partials_count, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+size_t jfli_poisson_divergence_workspace_bytes(int nx, int ny, int nz, int batch);
+int jfli_poisson_divergence(void* stream, const float* u, float alpha, const float* w, float beta, int aos, float scale,
+                            float* out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch,
+                            char* err, size_t errlen);
+int jfli_adjoint_position(void* stream, const float* disp, const float* u, const float* rho_bar, const float* force,
+                          float scale, float* lam_x, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* dL/dmesh of P(k): out = irfft(rfft(mesh) * weights[digitize(|k|, kedges)] / M), with
+ * weights[b] = 2 (dL/dP_b) prod(L/N) / count_b for the kept bins and 0 for bin 0 and
+ * bin nedges. Workspace: jfli_poisson_workspace_bytes. */
+int jfli_power_spectrum_adjoint(void* stream, const float* mesh, const float* kedges, const float* weights,
+                                int nedges, float lx, float ly, float lz, float* out, void* workspace,
+                                size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* dL/d ic of jfli_lpt given dL/ddx (lam_x) and dL/dp (lam_v). Workspace:
+ * jfli_lpt_adjoint_workspace_bytes. */
+size_t jfli_lpt_adjoint_workspace_bytes(int nx, int ny, int nz, int batch);
+int jfli_lpt_adjoint(void* stream, const float* ic, int order, float c1x, float c2x, float c1p, float c2p,
+                     const float* lam_x, const float* lam_v, float* out, void* workspace, size_t workspace_bytes,
+                     int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* Tangent of jfli_ic_filter along a change dptab of the P(k) table:
+ * out = irfft(rfft(noise) * interp(dptab) M/V / (2 sqrt(P M/V))), 0 where P <= 0.
+ * Workspace: jfli_poisson_workspace_bytes. */
+int jfli_ic_filter_tangent(void* stream, const float* noise, float* out, const float* ktab, const float* ptab,
+                           const float* dptab, int ntab, float lx, float ly, float lz, int zero_mode_one,
+                           void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                           size_t errlen);
 
 /* P(k) that allocates nothing. This entry point has no counterpart in the reference.
  *

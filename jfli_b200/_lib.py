@@ -90,6 +90,35 @@ _SIGNATURES = {
         c_int,
         [c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_void_p, *_DIMS, *_ERR],
     ),
+    "jfli_adjoint_partials_count": (c_size_t, _DIMS),
+    "jfli_adjoint_unkick_paint": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_float, c_void_p, c_void_p, c_size_t,
+         *_DIMS, *_ERR],
+    ),
+    "jfli_poisson_divergence_workspace_bytes": (c_size_t, _DIMS),
+    "jfli_poisson_divergence": (
+        c_int,
+        [c_void_p, c_void_p, c_float, c_void_p, c_float, c_int, c_float, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
+    ),
+    "jfli_adjoint_position": (
+        c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_void_p, *_DIMS, *_ERR]),
+    "jfli_power_spectrum_adjoint": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_void_p, c_void_p, c_size_t,
+         *_DIMS, *_ERR],
+    ),
+    "jfli_lpt_adjoint_workspace_bytes": (c_size_t, _DIMS),
+    "jfli_lpt_adjoint": (
+        c_int,
+        [c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_float, c_void_p, c_void_p, c_void_p, c_void_p,
+         c_size_t, *_DIMS, *_ERR],
+    ),
+    "jfli_ic_filter_tangent": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_int,
+         c_void_p, c_size_t, *_DIMS, *_ERR],
+    ),
     "jfli_healpix_paint": (
         c_int,
         [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float, c_float,

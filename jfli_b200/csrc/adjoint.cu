@@ -1,0 +1,223 @@
+// Adjoint (vector-Jacobian) kernels of the PM force step and the reversible KKD update.
+//
+// The force on a particle at x is F_a(x) = R_x[M_a], the CIC readout R of the force mesh
+// M_a = -D_a P (rho - mean), rho = sum_q W(x_q - .) the CIC density, P the Poisson
+// operator (-1/k^2, k = 0 -> 0) and D_a the 4-point finite difference. For a cotangent u
+// per particle the transpose J^T u of dF/dx has two parts:
+//   * readout: u . grad_x R_x[M] = grad_x R_x[sum_a u_a M_a]    (corners combined first)
+//   * density: grad_x R_x[rho_bar], rho_bar = sum_a (-D_a P)^T Ubar_a = P(div_FD Ubar),
+//     Ubar_a = CIC paint of the particles with weights u_a (D_a^T = -D_a, P^T = P).
+// The reversible step (reference pm/solvers.py:258-411, backward loop
+// pm/integrate.py:288-535) is  v' = v + k F(x);  x' = x + d v'.  Its reverse recomputes
+// x = x' - d v', F(x), v = v' - k F(x); its VJP is
+//   lambda_v_total = lambda_v' + d lambda_x',   dL/dd = <lambda_x', v'>,
+//   dL/dk = <lambda_v_total, F(x)>,   lambda_x = lambda_x' + k J^T lambda_v_total.
+#include "cic.cuh"
+#include "common.cuh"
+#include "internal.h"
+
+namespace jfli {
+
+constexpr int kAdjThreads = 256;
+constexpr int kAdjCtasPerSm = 8;
+
+// Block-wide sum of two doubles; thread 0 returns the result.
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+  __shared__ double sa[kAdjThreads / 32], sb[kAdjThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sa[w] = a;
+    sb[w] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = 0.0;
+    b = 0.0;
+    for (int i = 0; i < kAdjThreads / 32; ++i) {  // fixed order
+      a += sa[i];
+      b += sb[i];
+    }
+  }
+}
+
+// Reverse kick + first half of the VJP of one reversible step, at the un-drifted
+// positions x (relative displacements). Per particle:
+//   F = R_x[force];  <lambda_x, v'> -> partial[1];  u = lambda_v + drift * lambda_x;
+//   <u, F> -> partial[0];  v = v' - kick F;  lambda_v = u;  ubar_a += W * u_a.
+// partials holds 2 doubles per CTA and batch entry, summed in a fixed order later.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_unkick_paint(
+    const float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ lam_x,
+    float* __restrict__ lam_v, const float* __restrict__ force, float kick, float drift, float* __restrict__ ubar,
+    double* __restrict__ partials, PGrid g) {
+  const long long b = blockIdx.y;
+  disp += b * g.np * 3;
+  vel += b * g.np * 3;
+  lam_x += b * g.np * 3;
+  lam_v += b * g.np * 3;
+  force += b * g.np * 3;
+  ubar += b * g.np * 3;
+  double sk = 0.0, sd = 0.0;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    int i, j, k;
+    particle_ijk(g, p, i, j, k);
+    const Cic1 cx = cic_rel(i, disp[3 * p + 0], g.nx), cy = cic_rel(j, disp[3 * p + 1], g.ny),
+               cz = cic_rel(k, disp[3 * p + 2], g.nz);
+    float f[3];
+    gather_force_mesh(force, g, cx, cy, cz, f[0], f[1], f[2]);
+    float u[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float v = vel[3 * p + a];
+      const float lx = lam_x[3 * p + a];
+      sd += (double)lx * (double)v;
+      u[a] = lam_v[3 * p + a] + drift * lx;
+      sk += (double)u[a] * (double)f[a];
+      vel[3 * p + a] = v - f[a] * kick;
+      lam_v[3 * p + a] = u[a];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) deposit(ubar + (size_t)a * g.np, g, cx, cy, cz, u[a]);
+  }
+  block_sum2(sk, sd);
+  if (threadIdx.x == 0) {
+    double* dst = partials + 2 * (b * gridDim.x + blockIdx.x);
+    dst[0] = sk;
+    dst[1] = sd;
+  }
+}
+
+// out(c) = [accumulate ? out(c) : 0] + sum_a D_a (alpha u_a + beta w_a)(c), with
+// D_a f(c) = [8 (f(c+e_a) - f(c-e_a)) - (f(c+2e_a) - f(c-2e_a))] / 12. Component a of
+// cell c is at index c * cell_stride + a * comp_stride (SoA meshes: 1, cells; AoS
+// particle grids: 3, 1). w may be null.
+__global__ void k_div_fd(const float* __restrict__ u, float alpha, const float* __restrict__ w, float beta,
+                         long long cell_stride, long long comp_stride, int accumulate, float* __restrict__ out,
+                         PGrid g) {
+  const long long b = blockIdx.y;
+  u += b * g.np * 3;
+  if (w) w += b * g.np * 3;
+  out += b * g.np;
+  const float s = 1.0f / 12.0f;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    int c3[3];
+    particle_ijk(g, p, c3[0], c3[1], c3[2]);
+    const int n3[3] = {g.nx, g.ny, g.nz};
+    const int st[3] = {g.yz, g.nz, 1};
+    const int base = c3[0] * g.yz + c3[1] * g.nz + c3[2];
+    float acc = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int rest = base - c3[a] * st[a];
+      float v[4];
+      const int off[4] = {-2, -1, 1, 2};
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const long long q = (long long)(rest + wrap1(c3[a] + off[t], n3[a]) * st[a]);
+        float val = alpha * u[q * cell_stride + a * comp_stride];
+        if (w) val += beta * w[q * cell_stride + a * comp_stride];
+        v[t] = val;
+      }
+      acc += (8.0f * (v[2] - v[1]) - (v[3] - v[0])) * s;
+    }
+    out[p] = accumulate ? out[p] + acc : acc;
+  }
+}
+
+// lam_x += scale * grad_x R_x[h], h(corner) = rho_bar(corner) + sum_a u_a force_a(corner),
+// at relative positions disp. Either of rho_bar or (u, force) may be null. The gradient
+// of the trilinear weights is one-sided at cell faces, like the derivative of the
+// floor-based weights.
+__global__ void k_adj_position(const float* __restrict__ disp, const float* __restrict__ u,
+                               const float* __restrict__ rho_bar, const float* __restrict__ force, float scale,
+                               float* __restrict__ lam_x, PGrid g) {
+  const long long b = blockIdx.y;
+  disp += b * g.np * 3;
+  lam_x += b * g.np * 3;
+  if (u) u += b * g.np * 3;
+  if (force) force += b * g.np * 3;
+  if (rho_bar) rho_bar += b * g.np;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    int i, j, k;
+    particle_ijk(g, p, i, j, k);
+    const Cic1 cx = cic_rel(i, disp[3 * p + 0], g.nx), cy = cic_rel(j, disp[3 * p + 1], g.ny),
+               cz = cic_rel(k, disp[3 * p + 2], g.nz);
+    const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
+    float ua[3] = {0.f, 0.f, 0.f};
+    if (u && force) {
+      ua[0] = u[3 * p + 0];
+      ua[1] = u[3 * p + 1];
+      ua[2] = u[3 * p + 2];
+    }
+    float h[2][2][2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int o = xo[a] + yo[bb] + zo[c];
+          float v = rho_bar ? __ldg(rho_bar + o) : 0.f;
+          if (u && force)
+            v += ua[0] * __ldg(force + o) + ua[1] * __ldg(force + g.np + o) + ua[2] * __ldg(force + 2ull * g.np + o);
+          h[a][bb][c] = v;
+        }
+    const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
+    float gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+    for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) gx += wy[bb] * wz[c] * (h[1][bb][c] - h[0][bb][c]);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) gy += wx[a] * wz[c] * (h[a][1][c] - h[a][0][c]);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb) gz += wx[a] * wy[bb] * (h[a][bb][1] - h[a][bb][0]);
+    lam_x[3 * p + 0] += scale * gx;
+    lam_x[3 * p + 1] += scale * gy;
+    lam_x[3 * p + 2] += scale * gz;
+  }
+}
+
+// ----------------------------------------------------------------------------------
+static dim3 adj_grid(const MeshDims& d) { return particle_grid_dims(d.cells(), d.batch, kAdjThreads, kAdjCtasPerSm); }
+
+size_t adjoint_partials_count(const MeshDims& d) { return (size_t)2 * adj_grid(d).x * d.batch; }
+
+cudaError_t adjoint_unkick_paint(const float* disp, float* vel, const float* lam_x, float* lam_v, const float* force,
+                                 float kick, float drift, float* ubar, double* partials, const MeshDims& d,
+                                 cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(ubar, 0, sizeof(float) * 3 * (size_t)d.cells() * d.batch, s);
+  if (e != cudaSuccess) return e;
+  k_adj_unkick_paint<<<adj_grid(d), kAdjThreads, 0, s>>>(disp, vel, lam_x, lam_v, force, kick, drift, ubar, partials,
+                                                          make_pgrid(d));
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t divergence_fd(const float* u, float alpha, const float* w, float beta, int aos, int accumulate,
+                          float* out, const MeshDims& d, cudaStream_t s) {
+  const long long cell_stride = aos ? 3 : 1;
+  const long long comp_stride = aos ? 1 : d.cells();
+  k_div_fd<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(u, alpha, w, beta, cell_stride, comp_stride,
+                                                                          accumulate, out, make_pgrid(d));
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t adjoint_position(const float* disp, const float* u, const float* rho_bar, const float* force, float scale,
+                             float* lam_x, const MeshDims& d, cudaStream_t s) {
+  k_adj_position<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(disp, u, rho_bar, force, scale,
+                                                                                lam_x, make_pgrid(d));
+  note_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace jfli

@@ -446,4 +446,155 @@ int jfli_power_spectrum_noalloc(void* stream, const float* mesh, const float* ke
   return cuda_status(e, err, errlen, "jfli_power_spectrum_noalloc");
 }
 
+// ---- adjoints --------------------------------------------------------------------
+size_t jfli_adjoint_partials_count(int nx, int ny, int nz, int batch) {
+  return jfli::adjoint_partials_count(MeshDims{nx, ny, nz, batch});
+}
+
+int jfli_adjoint_unkick_paint(void* stream, const float* disp, float* vel, const float* lam_x, float* lam_v,
+                              const float* force, float kick, float drift, float* ubar, double* partials,
+                              size_t partials_count, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(vel);
+  CHECK_PTR(lam_x);
+  CHECK_PTR(lam_v);
+  CHECK_PTR(force);
+  CHECK_PTR(ubar);
+  CHECK_PTR(partials);
+  const MeshDims d{nx, ny, nz, batch};
+  const size_t need = jfli::adjoint_partials_count(d);
+  if (partials_count < need)
+    return fail(err, errlen, JFLI_EINVAL, "partials hold %zu doubles, need %zu", partials_count, need);
+  return cuda_status(jfli::adjoint_unkick_paint(disp, vel, lam_x, lam_v, force, kick, drift, ubar, partials, d,
+                                                (cudaStream_t)stream),
+                     err, errlen, "jfli_adjoint_unkick_paint");
+}
+
+size_t jfli_poisson_divergence_workspace_bytes(int nx, int ny, int nz, int batch) {
+  const MeshDims d{nx, ny, nz, batch};
+  return spec_bytes(d) + mesh_bytes(d);
+}
+
+int jfli_poisson_divergence(void* stream, const float* u, float alpha, const float* w, float beta, int aos, float scale,
+                            float* out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch,
+                            char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(u);
+  CHECK_PTR(out);
+  CHECK_PTR(workspace);
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < jfli_poisson_divergence_workspace_bytes(nx, ny, nz, batch))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes,
+                jfli_poisson_divergence_workspace_bytes(nx, ny, nz, batch));
+  cudaStream_t s = (cudaStream_t)stream;
+  float2* spec = (float2*)workspace;
+  float* div = (float*)((char*)workspace + spec_bytes(d));
+  cudaError_t e = jfli::divergence_fd(u, alpha, w, beta, aos ? 1 : 0, 0, div, d, s);
+  if (e == cudaSuccess) e = jfli::poisson_potential(div, spec, out, d, 0.0f, scale, s);
+  return cuda_status(e, err, errlen, "jfli_poisson_divergence");
+}
+
+int jfli_adjoint_position(void* stream, const float* disp, const float* u, const float* rho_bar, const float* force,
+                          float scale, float* lam_x, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(lam_x);
+  if ((u == nullptr) != (force == nullptr))
+    return fail(err, errlen, JFLI_EINVAL, "u and force must be given together");
+  if (rho_bar == nullptr && force == nullptr) return fail(err, errlen, JFLI_EINVAL, "nothing to read out");
+  const MeshDims d{nx, ny, nz, batch};
+  return cuda_status(jfli::adjoint_position(disp, u, rho_bar, force, scale, lam_x, d, (cudaStream_t)stream), err,
+                     errlen, "jfli_adjoint_position");
+}
+
+int jfli_power_spectrum_adjoint(void* stream, const float* mesh, const float* kedges, const float* weights,
+                                int nedges, float lx, float ly, float lz, float* out, void* workspace,
+                                size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(mesh);
+  CHECK_PTR(kedges);
+  CHECK_PTR(weights);
+  CHECK_PTR(out);
+  CHECK_PTR(workspace);
+  if (nedges < 1 || nedges > 2048) return fail(err, errlen, JFLI_EINVAL, "nedges %d outside [1, 2048]", nedges);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < spec_bytes(d))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, spec_bytes(d));
+  const float box[3] = {lx, ly, lz};
+  return cuda_status(jfli::power_adjoint(mesh, (float2*)workspace, out, d, kedges, weights, nedges, box,
+                                         (cudaStream_t)stream),
+                     err, errlen, "jfli_power_spectrum_adjoint");
+}
+
+size_t jfli_lpt_adjoint_workspace_bytes(int nx, int ny, int nz, int batch) {
+  const MeshDims d{nx, ny, nz, batch};
+  return spec_bytes(d) + 9 * mesh_bytes(d);
+}
+
+int jfli_lpt_adjoint(void* stream, const float* ic, int order, float c1x, float c2x, float c1p, float c2p,
+                     const float* lam_x, const float* lam_v, float* out, void* workspace, size_t workspace_bytes,
+                     int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(ic);
+  CHECK_PTR(lam_x);
+  CHECK_PTR(lam_v);
+  CHECK_PTR(out);
+  CHECK_PTR(workspace);
+  if (order != 1 && order != 2) return fail(err, errlen, JFLI_EINVAL, "LPT order must be 1 or 2, got %d", order);
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < jfli_lpt_adjoint_workspace_bytes(nx, ny, nz, batch))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes,
+                jfli_lpt_adjoint_workspace_bytes(nx, ny, nz, batch));
+  cudaStream_t s = (cudaStream_t)stream;
+  char* w = (char*)workspace;
+  float2* spec = (float2*)w;
+  float* phi1 = (float*)(w + spec_bytes(d));
+  float* sbar = (float*)(w + spec_bytes(d) + mesh_bytes(d));
+  float* acc = (float*)(w + spec_bytes(d) + 2 * mesh_bytes(d));
+  float* q = (float*)(w + spec_bytes(d) + 3 * mesh_bytes(d));
+  // dx = c1x F1 + c2x F2, p = c1p c1x F1 + c2p c2x F2 with F_i = -D P s_i (s_1 = ic,
+  // s_2 = delta2(P ic)); (-D P)^T = P div, so dL/ds_i = P div(ubar_i) with
+  // ubar_1 = c1x lam_x + c1p c1x lam_v, ubar_2 = c2x lam_x + c2p c2x lam_v.
+  cudaError_t e = jfli::divergence_fd(lam_x, c1x, lam_v, c1p * c1x, 1, 0, acc, d, s);
+  if (e == cudaSuccess && order == 2) {
+    e = jfli::poisson_potential(ic, spec, phi1, d, 0.0f, 1.0f, s);
+    if (e == cudaSuccess) e = jfli::divergence_fd(lam_x, c2x, lam_v, c2p * c2x, 1, 0, sbar, d, s);
+    if (e == cudaSuccess) e = jfli::poisson_potential(sbar, spec, sbar, d, 0.0f, 1.0f, s);
+    // dL/dphi1 accumulated into acc, then the common P: dL/dic = P(div ubar_1 + dL/dphi1)
+    if (e == cudaSuccess) e = jfli::lpt2_source_adjoint(phi1, sbar, q, acc, 1, d, s);
+  }
+  if (e == cudaSuccess) e = jfli::poisson_potential(acc, spec, out, d, 0.0f, 1.0f, s);
+  return cuda_status(e, err, errlen, "jfli_lpt_adjoint");
+}
+
+int jfli_ic_filter_tangent(void* stream, const float* noise, float* out, const float* ktab, const float* ptab,
+                           const float* dptab, int ntab, float lx, float ly, float lz, int zero_mode_one,
+                           void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                           size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(noise);
+  CHECK_PTR(out);
+  CHECK_PTR(ktab);
+  CHECK_PTR(ptab);
+  CHECK_PTR(dptab);
+  CHECK_PTR(workspace);
+  if (ntab < 2 || ntab > 4096) return fail(err, errlen, JFLI_EINVAL, "table length %d outside [2, 4096]", ntab);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < spec_bytes(d))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, spec_bytes(d));
+  const float box[3] = {lx, ly, lz};
+  return cuda_status(jfli::ic_filter(noise, (float2*)workspace, out, d, ktab, ptab, ntab, box, zero_mode_one,
+                                     (cudaStream_t)stream, dptab),
+                     err, errlen, "jfli_ic_filter_tangent");
+}
+
 }  // extern "C"

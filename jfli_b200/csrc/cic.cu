@@ -13,113 +13,11 @@
 // whose Fourier eigenvalue i (8 sin k - sin 2k) / 6 is JaxPM's `gradient_kernel`;
 // applying it in real space at the 8 CIC corners equals the k-space gradient followed
 // by an inverse FFT per component (reference pm/solvers.py:19-32 -> pm_forces).
+#include "cic.cuh"
 #include "common.cuh"
 #include "internal.h"
 
 namespace jfli {
-
-struct Cic1 {
-  int i0, i1;
-  float w0, w1;
-};
-
-// Particle grid with fast index decomposition; cells < 2^31 so offsets are 32-bit.
-struct PGrid {
-  int nx, ny, nz, yz;
-  unsigned np;
-  FastDiv dyz, dz;
-};
-
-static PGrid make_pgrid(const MeshDims& d) {
-  PGrid g;
-  g.nx = d.nx;
-  g.ny = d.ny;
-  g.nz = d.nz;
-  g.yz = d.ny * d.nz;
-  g.np = (unsigned)d.cells();
-  g.dyz = FastDiv::make((unsigned)g.yz);
-  g.dz = FastDiv::make((unsigned)d.nz);
-  return g;
-}
-
-__device__ __forceinline__ void particle_ijk(const PGrid& g, unsigned p, int& i, int& j, int& k) {
-  const unsigned ii = g.dyz.div(p);
-  const unsigned r = p - ii * (unsigned)g.yz;
-  const unsigned jj = g.dz.div(r);
-  i = (int)ii;
-  j = (int)jj;
-  k = (int)(r - jj * (unsigned)g.nz);
-}
-
-// Relative mode: grid index g plus displacement d (integer part split off first).
-__device__ __forceinline__ Cic1 cic_rel(int gidx, float d, int n) {
-  const float f = floorf(d);
-  Cic1 c;
-  c.w1 = d - f;
-  c.w0 = 1.0f - c.w1;
-  int i = gidx + (int)f;
-  if ((unsigned)i >= (unsigned)n) i = wrap_index(i, n);
-  c.i0 = i;
-  c.i1 = (i + 1 == n) ? 0 : i + 1;
-  return c;
-}
-
-// Absolute mode: position in grid units.
-__device__ __forceinline__ Cic1 cic_abs(float p, int n) {
-  const float f = floorf(p);
-  Cic1 c;
-  c.w1 = p - f;
-  c.w0 = 1.0f - c.w1;
-  int i = (int)f;
-  if ((unsigned)i >= (unsigned)n) i = wrap_index(i, n);
-  c.i0 = i;
-  c.i1 = (i + 1 == n) ? 0 : i + 1;
-  return c;
-}
-
-__device__ __forceinline__ void cic_setup(const float* pos3, unsigned p, int absolute, const PGrid& g, Cic1& cx,
-                                          Cic1& cy, Cic1& cz) {
-  const float px = pos3[0], py = pos3[1], pz = pos3[2];
-  if (absolute) {
-    cx = cic_abs(px, g.nx);
-    cy = cic_abs(py, g.ny);
-    cz = cic_abs(pz, g.nz);
-  } else {
-    int i, j, k;
-    particle_ijk(g, p, i, j, k);
-    cx = cic_rel(i, px, g.nx);
-    cy = cic_rel(j, py, g.ny);
-    cz = cic_rel(k, pz, g.nz);
-  }
-}
-
-__device__ __forceinline__ void deposit(float* mesh, const PGrid& g, const Cic1& cx, const Cic1& cy, const Cic1& cz,
-                                        float w) {
-  const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
-  const float wx[2] = {cx.w0 * w, cx.w1 * w}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
-#pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      const float wab = wx[a] * wy[b];
-#pragma unroll
-      for (int c = 0; c < 2; ++c) atomicAdd(mesh + (xo[a] + yo[b] + zo[c]), wab * wz[c]);
-    }
-}
-
-__device__ __forceinline__ float gather(const float* __restrict__ mesh, const PGrid& g, const Cic1& cx,
-                                        const Cic1& cy, const Cic1& cz) {
-  const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
-  const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
-  float acc = 0.f;
-#pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int b = 0; b < 2; ++b)
-#pragma unroll
-      for (int c = 0; c < 2; ++c) acc += __ldg(mesh + (xo[a] + yo[b] + zo[c])) * (wx[a] * wy[b] * wz[c]);
-  return acc;
-}
 
 // -F = D(pot) at both CIC corners of one line: values v[0..5] = pot at i0-2 .. i0+3.
 __device__ __forceinline__ void fd_pair(const float* v, float& g0, float& g1) {
@@ -245,9 +143,6 @@ __global__ void k_readout_gradient(const float* __restrict__ pos, int absolute, 
     out[3 * p + 2] = fz * scale;
   }
 }
-
-__device__ __forceinline__ void gather_force_mesh(const float* __restrict__ F, const PGrid& g, const Cic1& cx,
-                                                  const Cic1& cy, const Cic1& cz, float& fx, float& fy, float& fz);
 
 // One fused particle pass of a PM step. Order inside: kick (with the force at the
 // current position) -> drift (with the kicked velocity) -> paint (at the new position).
@@ -380,33 +275,6 @@ __global__ void k_force_mesh4(const float* __restrict__ pot, float* __restrict__
   }
 }
 
-// CIC readout of the three force meshes at one particle.
-__device__ __forceinline__ void gather_force_mesh(const float* __restrict__ F, const PGrid& g, const Cic1& cx,
-                                                  const Cic1& cy, const Cic1& cz, float& fx, float& fy, float& fz) {
-  const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
-  const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
-  const float* F1 = F + g.np;
-  const float* F2 = F + 2ull * g.np;
-  float ax = 0.f, ay = 0.f, az = 0.f;
-#pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      const float wab = wx[a] * wy[b];
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        const int o = xo[a] + yo[b] + zo[c];
-        const float w = wab * wz[c];
-        ax += __ldg(F + o) * w;
-        ay += __ldg(F1 + o) * w;
-        az += __ldg(F2 + o) * w;
-      }
-    }
-  fx = ax;
-  fy = ay;
-  fz = az;
-}
-
 // F = scale * (-D pot) at every grid point (particles exactly on the grid), optionally
 // accumulated into `out` (AoS [..,3]).
 __global__ void k_grid_gradient(const float* __restrict__ pot, float* __restrict__ out, float scale, int accumulate,
@@ -449,6 +317,37 @@ __global__ void k_grid_gradient(const float* __restrict__ pot, float* __restrict
 // gradient_kernel_i * gradient_kernel_j used by the reference). Needs axes >= 4 cells.
 __constant__ float c_d5[5] = {1.0f / 12.0f, -8.0f / 12.0f, 0.0f, 8.0f / 12.0f, -1.0f / 12.0f};
 
+// (D_a D_b f)(c) for the 4-point finite difference D (5-point stencil c_d5 per axis):
+// offsets -4..4 along a for a == b, a 4x4 cross for a != b. The stencil is symmetric
+// under (s, t) -> (-s, -t), so the operator is its own transpose.
+__device__ __forceinline__ float hess_component(const float* __restrict__ f, const int* c3, const int* n3,
+                                                const int* st, int base, int a, int bb) {
+  float acc = 0.f;
+  if (a == bb) {
+    const int rest = base - c3[a] * st[a];
+    for (int s = 0; s < 5; ++s) {
+      if (s == 2) continue;
+      for (int t = 0; t < 5; ++t) {
+        if (t == 2) continue;
+        const int off = (s - 2) + (t - 2);
+        acc += c_d5[s] * c_d5[t] * f[rest + wrap1(c3[a] + off, n3[a]) * st[a]];
+      }
+    }
+  } else {
+    const int rest = base - c3[a] * st[a] - c3[bb] * st[bb];
+    for (int s = 0; s < 5; ++s) {
+      if (s == 2) continue;
+      const int oa = wrap1(c3[a] + s - 2, n3[a]) * st[a];
+      for (int t = 0; t < 5; ++t) {
+        if (t == 2) continue;
+        acc += c_d5[s] * c_d5[t] * f[rest + oa + wrap1(c3[bb] + t - 2, n3[bb]) * st[bb]];
+      }
+    }
+  }
+  return acc;
+}
+
+// The 2LPT source itself (reference call site pm/lpt.py:119).
 __global__ void k_lpt2_source(const float* __restrict__ pot, float* __restrict__ out, PGrid g) {
   const long long b = blockIdx.y;
   pot += b * g.np;
@@ -460,35 +359,8 @@ __global__ void k_lpt2_source(const float* __restrict__ pot, float* __restrict__
     particle_ijk(g, p, c3[0], c3[1], c3[2]);
     const int base = c3[0] * g.yz + c3[1] * g.nz + c3[2];
     float h[3][3];
-    // diagonal: D_a D_a, offsets -4..4 along axis a
-    for (int a = 0; a < 3; ++a) {
-      const int rest = base - c3[a] * st[a];
-      float acc = 0.f;
-      for (int s = 0; s < 5; ++s) {
-        if (s == 2) continue;
-        for (int t = 0; t < 5; ++t) {
-          if (t == 2) continue;
-          const int off = (s - 2) + (t - 2);
-          acc += c_d5[s] * c_d5[t] * pot[rest + wrap1(c3[a] + off, n3[a]) * st[a]];
-        }
-      }
-      h[a][a] = acc;
-    }
-    // off-diagonal: D_a D_b
     for (int a = 0; a < 3; ++a)
-      for (int bb = a + 1; bb < 3; ++bb) {
-        const int rest = base - c3[a] * st[a] - c3[bb] * st[bb];
-        float acc = 0.f;
-        for (int s = 0; s < 5; ++s) {
-          if (s == 2) continue;
-          const int oa = wrap1(c3[a] + s - 2, n3[a]) * st[a];
-          for (int t = 0; t < 5; ++t) {
-            if (t == 2) continue;
-            acc += c_d5[s] * c_d5[t] * pot[rest + oa + wrap1(c3[bb] + t - 2, n3[bb]) * st[bb]];
-          }
-        }
-        h[a][bb] = acc;
-      }
+      for (int bb = a; bb < 3; ++bb) h[a][bb] = hess_component(pot, c3, n3, st, base, a, bb);
     // accumulate in the reference's loop order
     float delta2 = 0.f, acc_diag = 0.f;
     for (int a = 0; a < 3; ++a) {
@@ -497,6 +369,54 @@ __global__ void k_lpt2_source(const float* __restrict__ pot, float* __restrict__
       for (int bb = a + 1; bb < 3; ++bb) delta2 -= h[a][bb] * h[a][bb];
     }
     out[p] = delta2;
+  }
+}
+
+// Adjoint of the 2LPT source, first half: with s = dL/d delta2 at a cell,
+//   q_aa = s * sum_{b != a} phi_bb  (a = 0, 1, 2)   and   q_ab = -2 s phi_ab  (01, 02, 12),
+// written as six meshes [6][cells].
+__global__ void k_lpt2_source_adj_products(const float* __restrict__ pot, const float* __restrict__ sbar,
+                                           float* __restrict__ q, PGrid g) {
+  const long long b = blockIdx.y;
+  pot += b * g.np;
+  sbar += b * g.np;
+  q += b * g.np * 6;
+  const int n3[3] = {g.nx, g.ny, g.nz};
+  const int st[3] = {g.yz, g.nz, 1};
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    int c3[3];
+    particle_ijk(g, p, c3[0], c3[1], c3[2]);
+    const int base = c3[0] * g.yz + c3[1] * g.nz + c3[2];
+    float h[3][3];
+    for (int a = 0; a < 3; ++a)
+      for (int bb = a; bb < 3; ++bb) h[a][bb] = hess_component(pot, c3, n3, st, base, a, bb);
+    const float sv = sbar[p];
+    q[p] = sv * (h[1][1] + h[2][2]);
+    q[g.np + p] = sv * (h[0][0] + h[2][2]);
+    q[2ull * g.np + p] = sv * (h[0][0] + h[1][1]);
+    q[3ull * g.np + p] = -2.0f * sv * h[0][1];
+    q[4ull * g.np + p] = -2.0f * sv * h[0][2];
+    q[5ull * g.np + p] = -2.0f * sv * h[1][2];
+  }
+}
+
+// Second half: dL/d phi1 = sum_a D_a D_a q_aa + sum_{a<b} D_a D_b q_ab (each operator is
+// its own transpose), optionally accumulated into out.
+__global__ void k_lpt2_source_adj_apply(const float* __restrict__ q, float* __restrict__ out, int accumulate,
+                                        PGrid g) {
+  const long long b = blockIdx.y;
+  q += b * g.np * 6;
+  out += b * g.np;
+  const int n3[3] = {g.nx, g.ny, g.nz};
+  const int st[3] = {g.yz, g.nz, 1};
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    int c3[3];
+    particle_ijk(g, p, c3[0], c3[1], c3[2]);
+    const int base = c3[0] * g.yz + c3[1] * g.nz + c3[2];
+    float acc = 0.f;
+    for (int m = 0; m < 6; ++m) acc += hess_component(q + (size_t)m * g.np, c3, n3, st, base, pa[m], pb[m]);
+    out[p] = accumulate ? out[p] + acc : acc;
   }
 }
 
@@ -523,25 +443,6 @@ __global__ void k_axpy(float* __restrict__ y, const float* __restrict__ x, float
 }
 
 // ----------------------------------------------------------------------------------
-static int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
-  return n;
-}
-
-static dim3 particle_grid_dims(long long np, int batch, int threads, int per_sm) {
-  long long blocks = (np + threads - 1) / threads;
-  const long long cap = (long long)sm_count() * per_sm;
-  if (blocks > cap) blocks = cap;
-  if (blocks < 1) blocks = 1;
-  return dim3((unsigned)blocks, batch);
-}
-
 cudaError_t cic_paint(const float* pos, int absolute, const float* weights, float weight, float* mesh,
                       const MeshDims& d, cudaStream_t s) {
   k_paint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pos, absolute, weights, weight, mesh, make_pgrid(d));
@@ -601,6 +502,19 @@ cudaError_t grid_gradient(const float* pot, float* out, float scale, int accumul
 
 cudaError_t lpt2_source(const float* pot, float* out, const MeshDims& d, cudaStream_t s) {
   k_lpt2_source<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, out, make_pgrid(d));
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t lpt2_source_adjoint(const float* pot, const float* sbar, float* q, float* out, int accumulate,
+                                const MeshDims& d, cudaStream_t s) {
+  k_lpt2_source_adj_products<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, sbar, q,
+                                                                                            make_pgrid(d));
+  note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_lpt2_source_adj_apply<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(q, out, accumulate,
+                                                                                         make_pgrid(d));
   note_launch();
   return cudaGetLastError();
 }

@@ -815,8 +815,10 @@ cudaError_t pgd_potential(const float* rho, float2* spec, float* pot, const Mesh
 }
 
 cudaError_t ic_filter(const float* noise, float2* spec, float* out, const MeshDims& d, const float* ktab,
-                      const float* ptab, int ntab, const float* box, int zero_mode_one, cudaStream_t s) {
+                      const float* ptab, int ntab, const float* box, int zero_mode_one, cudaStream_t s,
+                      const float* dptab) {
   IcOp op;
+  op.dptab = dptab;
   op.nx = d.nx;
   op.ny = d.ny;
   op.nz = d.nz;
@@ -830,6 +832,22 @@ cudaError_t ic_filter(const float* noise, float2* spec, float* out, const MeshDi
   op.norm = 1.0f / ((float)d.nx * (float)d.ny * (float)d.nz);
   op.zero_mode_one = zero_mode_one;
   return filter_chain(noise, spec, out, d, 0.0f, op, s);
+}
+
+cudaError_t power_adjoint(const float* mesh, float2* spec, float* out, const MeshDims& d, const float* kedges,
+                          const float* weights, int nedges, const float* box, cudaStream_t s) {
+  PkAdjOp op;
+  op.nx = d.nx;
+  op.ny = d.ny;
+  op.nz = d.nz;
+  op.kedges = kedges;
+  op.weights = weights;
+  op.nedges = nedges;
+  op.cx = (float)(2.0 * M_PI / (double)box[0]);
+  op.cy = (float)(2.0 * M_PI / (double)box[1]);
+  op.cz = (float)(2.0 * M_PI / (double)box[2]);
+  op.norm = 1.0f / ((float)d.nx * (float)d.ny * (float)d.nz);
+  return filter_chain(mesh, spec, out, d, 0.0f, op, s);
 }
 
 cudaError_t power_partials(const float* mesh, float2* spec, double* partials, const MeshDims& d, const float* kedges,

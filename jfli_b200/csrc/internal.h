@@ -26,8 +26,12 @@ cudaError_t poisson_potential(const float* rho, float2* spec, float* pot, const 
                               float scale, cudaStream_t s);
 cudaError_t pgd_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean, float kl,
                           float ks, float scale, cudaStream_t s);
+// dptab != null: the tangent of the filter along a change dptab of the P(k) table.
 cudaError_t ic_filter(const float* noise, float2* spec, float* out, const MeshDims& d, const float* ktab,
-                      const float* ptab, int ntab, const float* box, int zero_mode_one, cudaStream_t s);
+                      const float* ptab, int ntab, const float* box, int zero_mode_one, cudaStream_t s,
+                      const float* dptab = nullptr);
+cudaError_t power_adjoint(const float* mesh, float2* spec, float* out, const MeshDims& d, const float* kedges,
+                          const float* weights, int nedges, const float* box, cudaStream_t s);
 cudaError_t power_partials(const float* mesh, float2* spec, double* partials, const MeshDims& d, const float* kedges,
                            int nedges, const float* box, float norm, cudaStream_t s);
 
@@ -57,6 +61,19 @@ cudaError_t lpt2_source(const float* pot, float* out, const MeshDims& d, cudaStr
 cudaError_t lpt_combine(const float* f1, const float* f2, float c1x, float c2x, float c1p, float c2p, float* dx,
                         float* p, const MeshDims& d, cudaStream_t s);
 cudaError_t axpy_particles(float* y, const float* x, float a, const MeshDims& d, cudaStream_t s);
+// q: six scratch meshes; out (+)= dL/dphi1 for sbar = dL/d delta2.
+cudaError_t lpt2_source_adjoint(const float* pot, const float* sbar, float* q, float* out, int accumulate,
+                                const MeshDims& d, cudaStream_t s);
+
+// ---- adjoint.cu ----
+size_t adjoint_partials_count(const MeshDims& d);
+cudaError_t adjoint_unkick_paint(const float* disp, float* vel, const float* lam_x, float* lam_v, const float* force,
+                                 float kick, float drift, float* ubar, double* partials, const MeshDims& d,
+                                 cudaStream_t s);
+cudaError_t divergence_fd(const float* u, float alpha, const float* w, float beta, int aos, int accumulate,
+                          float* out, const MeshDims& d, cudaStream_t s);
+cudaError_t adjoint_position(const float* disp, const float* u, const float* rho_bar, const float* force, float scale,
+                             float* lam_x, const MeshDims& d, cudaStream_t s);
 
 // P(k) whose scratch is a file-scope device array (no allocation).
 cudaError_t noalloc_scratch(void** out);

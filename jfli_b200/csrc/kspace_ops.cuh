@@ -99,7 +99,11 @@ struct IcOp {
   float factor;      // M / V
   float norm;        // 1 / M
   int zero_mode_one;
-  static size_t smem_bytes(const IcOp& op) { return sizeof(float) * (op.nx + 2 * op.ntab); }
+  // Tangent mode (dptab != null): the derivative of the multiplier along a change dptab
+  // of the table, interp(dptab) * factor / (2 sqrt(P)) (0 where P <= 0 and at the
+  // k = 0 guard), used for gradients with respect to the cosmology behind P(k).
+  const float* dptab = nullptr;
+  static size_t smem_bytes(const IcOp& op) { return sizeof(float) * (op.nx + 3 * op.ntab); }
   __device__ void prologue(float* sm, int) const {
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
       sm[i] = k_rad_per_cell(i, nx) / lx * (float)nx;
@@ -107,6 +111,7 @@ struct IcOp {
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
       sm[nx + i] = ktab[i];
       sm[nx + ntab + i] = ptab[i];
+      if (dptab) sm[nx + 2 * ntab + i] = dptab[i];
     }
     __syncthreads();
   }
@@ -116,6 +121,12 @@ struct IcOp {
     const float az = k_rad_per_cell(kz, nz) / lz * (float)nz;
     const float kmag = sqrtf(ax * ax + ay * ay + az * az);
     float pk = interp_table(kmag, sm + nx, sm + nx + ntab, ntab) * factor;
+    if (dptab) {
+      const float dpk = interp_table(kmag, sm + nx, sm + nx + 2 * ntab, ntab) * factor;
+      float m = pk > 0.f ? dpk / (2.0f * sqrtf(pk)) : 0.f;
+      if (zero_mode_one && kmag == 0.f) m = 0.f;
+      return cscale(v, m * norm);
+    }
     if (zero_mode_one && kmag == 0.f) pk = 1.f;
     return cscale(v, sqrtf(pk) * norm);
   }
@@ -193,6 +204,43 @@ struct PkOp {
     double* dst = partials + ((long long)batch * nctas + cta) * nb;
     for (int i = threadIdx.x; i < nb; i += blockDim.x) dst[i] = bins[i];
   }
+};
+
+// Adjoint of P(k) with respect to the mesh: mode k is scaled by weights[bin(k)] * norm,
+// bin(k) = digitize(|k|, kedges) with the same |k| rounding as PkOp, so that the inverse
+// transform gives dL/dmesh = sum over bins of dL/dP_b * dP_b/dmesh when
+// weights[b] = 2 * dL/dP_b * prod(L/N) / count_b (0 for the dropped under/overflow bins).
+struct PkAdjOp {
+  static constexpr bool kInverse = true;
+  static constexpr bool kStore = true;
+  int nx, ny, nz;
+  const float* kedges;
+  const float* weights;  // nedges + 1
+  int nedges;
+  float cx, cy, cz;  // 2*pi / L_i
+  float norm;        // 1 / M (inverse transform)
+  static size_t smem_bytes(const PkAdjOp& op) { return sizeof(float) * (2 * op.nedges + 1); }
+  __device__ void prologue(float* sm, int) const {
+    for (int i = threadIdx.x; i < nedges; i += blockDim.x) sm[i] = kedges[i];
+    for (int i = threadIdx.x; i <= nedges; i += blockDim.x) sm[nedges + i] = weights[i];
+    __syncthreads();
+  }
+  __device__ float2 apply(float2 v, int kx, int ky, int kz, float* sm, int) const {
+    const float ax = __fmul_rn(cx, (float)signed_freq(kx, nx));
+    const float ay = __fmul_rn(cy, (float)signed_freq(ky, ny));
+    const float az = __fmul_rn(cz, (float)signed_freq(kz, nz));
+    const float kmag = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az)));
+    int lo = 0, hi = nedges;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (sm[mid] <= kmag)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    return cscale(v, sm[nedges + lo] * norm);
+  }
+  __device__ void epilogue(float*, int, int, int) const {}
 };
 
 }  // namespace jfli

@@ -253,5 +253,107 @@ def healpix_paint(pos: torch.Tensor, nside: int, box_size, observer_mpc, rmin: f
     return out
 
 
+# ------------------------------------------------------------------------- adjoints
+def adjoint_unkick_paint(disp: torch.Tensor, vel: torch.Tensor, lam_x: torch.Tensor, lam_v: torch.Tensor,
+                         force: torch.Tensor, kick: float, drift: float, ubar: torch.Tensor | None = None):
+    """Reverse kick and first half of the VJP of one reversible step (in place on vel and
+    lam_v). Returns (ubar, (dL/dkick, dL/ddrift)) with ubar the (..., 3, nx, ny, nz) paint
+    of the new lam_v; the two scalars are FP64 sums in a fixed order (one tensor of 2)."""
+    for name, t in (("disp", disp), ("vel", vel), ("lam_x", lam_x), ("lam_v", lam_v), ("force", force)):
+        _check(t, name)
+    (nx, ny, nz), batch, lead = _mesh_dims(disp, True)
+    if ubar is None:
+        ubar = torch.empty(*lead, 3, nx, ny, nz, dtype=torch.float32, device=disp.device)
+    count = int(query("jfli_adjoint_partials_count", nx, ny, nz, batch))
+    partials = torch.empty(count, dtype=torch.float64, device=disp.device)
+    call("jfli_adjoint_unkick_paint", stream_ptr(), ptr(disp), ptr(vel), ptr(lam_x), ptr(lam_v), ptr(force),
+         float(kick), float(drift), ptr(ubar), ptr(partials), count, nx, ny, nz, batch)
+    return ubar, partials.view(batch, -1, 2).sum(dim=1).reshape(*lead, 2) if lead else partials.view(-1, 2).sum(0)
+
+
+def poisson_divergence(u: torch.Tensor, *, aos: bool, alpha: float = 1.0, w: torch.Tensor | None = None,
+                       beta: float = 0.0, scale: float = 1.0, out: torch.Tensor | None = None) -> torch.Tensor:
+    """scale * P(div_FD(alpha u + beta w)); u, w three meshes (..., 3, nx, ny, nz) or particle
+    grids (..., nx, ny, nz, 3) (aos=True)."""
+    _check(u, "u")
+    if w is not None:
+        _check(w, "w")
+        if w.shape != u.shape:
+            raise ValueError("u and w must have the same shape")
+    if aos:
+        (nx, ny, nz), batch, lead = _mesh_dims(u, True)
+    else:
+        if u.shape[-4] != 3:
+            raise ValueError("u must hold three meshes (..., 3, nx, ny, nz)")
+        nx, ny, nz = (int(v) for v in u.shape[-3:])
+        lead = tuple(u.shape[:-4])
+        batch = int(np.prod(lead)) if lead else 1
+    if out is None:
+        out = torch.empty(*lead, nx, ny, nz, dtype=torch.float32, device=u.device)
+    nb = query("jfli_poisson_divergence_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "div", u.device)
+    call("jfli_poisson_divergence", stream_ptr(), ptr(u), float(alpha), ptr(w), float(beta), int(aos), float(scale),
+         ptr(out), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return out
+
+
+def adjoint_position(disp: torch.Tensor, lam_x: torch.Tensor, *, rho_bar: torch.Tensor | None = None,
+                     u: torch.Tensor | None = None, force: torch.Tensor | None = None, scale: float = 1.0) -> None:
+    """lam_x += scale * grad_x R_x[rho_bar + sum_a u_a force_a] (in place)."""
+    _check(disp, "disp")
+    _check(lam_x, "lam_x")
+    (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
+    call("jfli_adjoint_position", stream_ptr(), ptr(disp), ptr(u), ptr(rho_bar), ptr(force), float(scale), ptr(lam_x),
+         nx, ny, nz, batch)
+
+
+def power_adjoint(mesh: torch.Tensor, kedges: torch.Tensor, weights: torch.Tensor, box_size) -> torch.Tensor:
+    """dL/dmesh of the P(k) sums for per-bin weights 2 dL/dP_b prod(L/N) / count_b."""
+    _check(mesh, "mesh")
+    _check(kedges, "kedges")
+    _check(weights, "weights")
+    (nx, ny, nz), batch, lead = _mesh_dims(mesh, False)
+    ne = int(kedges.numel())
+    if weights.numel() != ne + 1:
+        raise ValueError("weights must have nedges + 1 entries")
+    out = torch.empty_like(mesh)
+    nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "spec", mesh.device)
+    lx, ly, lz = (float(v) for v in box_size)
+    call("jfli_power_spectrum_adjoint", stream_ptr(), ptr(mesh), ptr(kedges), ptr(weights), ne, lx, ly, lz, ptr(out),
+         ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return out
+
+
+def lpt_adjoint(ic: torch.Tensor, order: int, c1x: float, c2x: float, c1p: float, c2p: float, lam_x: torch.Tensor,
+                lam_v: torch.Tensor) -> torch.Tensor:
+    """dL/d ic of lpt() given the cotangents of its displacement and momentum."""
+    _check(ic, "ic")
+    _check(lam_x, "lam_x")
+    _check(lam_v, "lam_v")
+    (nx, ny, nz), batch, lead = _mesh_dims(ic, False)
+    out = torch.empty_like(ic)
+    nb = query("jfli_lpt_adjoint_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "lpt_adj", ic.device)
+    call("jfli_lpt_adjoint", stream_ptr(), ptr(ic), int(order), float(c1x), float(c2x), float(c1p), float(c2p),
+         ptr(lam_x), ptr(lam_v), ptr(out), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return out
+
+
+def ic_filter_tangent(noise: torch.Tensor, ktab: torch.Tensor, ptab: torch.Tensor, dptab: torch.Tensor, box_size, *,
+                      zero_mode_one: bool = False) -> torch.Tensor:
+    """Derivative of ic_filter(noise) along a change dptab of the P(k) table."""
+    for name, t in (("noise", noise), ("ktab", ktab), ("ptab", ptab), ("dptab", dptab)):
+        _check(t, name)
+    (nx, ny, nz), batch, lead = _mesh_dims(noise, False)
+    out = torch.empty_like(noise)
+    nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "spec", noise.device)
+    lx, ly, lz = (float(v) for v in box_size)
+    call("jfli_ic_filter_tangent", stream_ptr(), ptr(noise), ptr(out), ptr(ktab), ptr(ptab), ptr(dptab),
+         int(ktab.numel()), lx, ly, lz, int(zero_mode_one), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return out
+
+
 def launch_count() -> int:
     return _lib.launch_count()

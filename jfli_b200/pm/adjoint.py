@@ -1,0 +1,301 @@
+"""Reverse-mode gradients of the forward model with the reversible adjoint.
+
+The reference differentiates `lpt -> nbody -> power` with jax.grad; with
+`adjoint="reverse"` its N-body part is a custom VJP (pm/integrate.py:147-535) whose
+backward loop steps the ReversibleDoubleKickDrift solver backwards (solver.reverse,
+pm/solvers.py:327-411) and pulls the cotangents through the VJP of each step, so the
+trajectory is recomputed instead of stored.
+
+Here every stage is a torch.autograd.Function whose backward runs the B200 adjoint
+kernels, so `torch.autograd.grad(loss, [noise, omega_c, sigma8])` plays the role of
+jax.grad:
+
+* `ICFilter`    white noise -> linear density (initial.py:167-182). The filter is a real
+                even Fourier multiplier, hence symmetric: its VJP is the filter itself.
+                Cosmology: d/dsigma8 exactly (delta is proportional to sigma8), d/dOmega_c
+                with the tangent kernel along dP_lin/dOmega_c.
+* `LPT`         linear density -> (dx, p) (pm/lpt.py:119), VJP by `jfli_lpt_adjoint`.
+* `ReversibleNBody`  (dx, p) -> final CIC density after the KKD steps. Backward: per step
+                un-drift + paint, force meshes at the previous positions, then
+                un-kick + adjoint paint, P(div), and the CIC-gradient gather
+                (`jfli_adjoint_*`); dL/dkick_n and dL/ddrift_n come out as FP64 sums.
+* `PowerSpectrum` density -> P(k) per bin (_src/power/_compute.py:68-119).
+
+Gradients with respect to the cosmology go through the FP64 host tables the kernels
+consume (kick/drift factors, LPT factors, the P_lin table): the adjoint gives dL/d(each
+scalar) and the host differentiates the scalars by central differences of the FP64
+tables (the growth ODE is solved to rtol 1e-12, so a step of 1e-5 gives ~1e-7 relative
+accuracy).
+
+One deliberate difference from the reference: its reverse step un-drifts with a factor
+built from dGfa while the forward step drifts with gp (pm/solvers.py:309 vs 364), so its
+backward loop linearises around slightly different positions than the forward pass
+visited. Here the reverse drift uses the forward factor, so reverse(step(y)) == y up to
+FP32 rounding and the gradient is the gradient of the forward model.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+import torch
+
+from .. import cosmology as cj
+from .. import ops
+from .._lib import JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
+from .integrate import time_events
+from .lpt import lpt_coefficients
+from .solvers import ReversibleDoubleKickDrift
+
+OMEGA_C_STEP = 1e-5
+
+
+# ----------------------------------------------------------------------------- host tables
+@dataclasses.dataclass
+class ForwardTables:
+    """FP64 host tables of one cosmology and their Omega_c derivatives."""
+
+    ktab: np.ndarray
+    ptab: np.ndarray
+    lpt: tuple  # (c1x, c2x, c1p, c2p)
+    kicks: np.ndarray
+    drifts: np.ndarray
+    dptab: np.ndarray | None = None
+    dlpt: np.ndarray | None = None
+    dkicks: np.ndarray | None = None
+    ddrifts: np.ndarray | None = None
+
+
+def kkd_schedule(cosmo, t0: float, t1: float, dt0: float):
+    """(kicks, drifts) of the ReversibleDoubleKickDrift steps from t0 to t1."""
+    ev = [(e[1], e[2]) for e in time_events(t0, [t1], dt0) if e[0] == "step"]
+    cs = [ReversibleDoubleKickDrift.step_coefficients(cosmo, a, b, dt0, t0) for a, b in ev]
+    return np.array([c.kick for c in cs]), np.array([c.drift for c in cs])
+
+
+def forward_tables(omega_c: float, sigma8: float, *, t0: float, t1: float, dt0: float, n_table: int = 128,
+                   derivatives: bool = True, **cosmo_kw) -> ForwardTables:
+    def build(oc):
+        c = cj.Planck18(Omega_c=float(oc), sigma8=float(sigma8), **cosmo_kw)
+        k, pk = cj.pk_table(c, n_table)
+        kicks, drifts = kkd_schedule(c, t0, t1, dt0)
+        return k, pk, np.asarray(lpt_coefficients(c, t0), np.float64), kicks, drifts
+
+    k, pk, lc, kicks, drifts = build(omega_c)
+    tab = ForwardTables(ktab=k, ptab=pk, lpt=tuple(float(v) for v in lc), kicks=kicks, drifts=drifts)
+    if derivatives:
+        h = OMEGA_C_STEP
+        _, pk_p, lc_p, k_p, d_p = build(omega_c + h)
+        _, pk_m, lc_m, k_m, d_m = build(omega_c - h)
+        tab.dptab = (pk_p - pk_m) / (2 * h)
+        tab.dlpt = (lc_p - lc_m) / (2 * h)
+        tab.dkicks = (k_p - k_m) / (2 * h)
+        tab.ddrifts = (d_p - d_m) / (2 * h)
+    return tab
+
+
+def _dev(a) -> torch.Tensor:
+    return torch.as_tensor(np.asarray(a, np.float32), device="cuda")
+
+
+def _dot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+    return torch.sum(a.double() * b.double())
+
+
+def _scalar(t) -> float:
+    return float(t.detach()) if isinstance(t, torch.Tensor) else float(t)
+
+
+def _like(value, param) -> torch.Tensor:
+    """A gradient value as a tensor with the dtype and device of the parameter."""
+    if isinstance(value, torch.Tensor):
+        value = float(value.detach().double())
+    return torch.as_tensor(value, dtype=param.dtype, device=param.device)
+
+
+# ----------------------------------------------------------------------------- functions
+class ICFilter(torch.autograd.Function):
+    """noise -> sqrt(P_lin(|k|) M / V) filtered field (FP32 kernels, FP64 tables)."""
+
+    @staticmethod
+    def forward(ctx, noise, omega_c, sigma8, tables: ForwardTables, box):
+        kt, pt = _dev(tables.ktab), _dev(tables.ptab)
+        delta = ops.ic_filter(noise.contiguous(), kt, pt, box)
+        ctx.tables, ctx.box = tables, box
+        ctx.sigma8 = _scalar(sigma8)
+        ctx.params = (omega_c, sigma8)
+        ctx.save_for_backward(noise, delta)
+        return delta
+
+    @staticmethod
+    def backward(ctx, gdelta):
+        noise, delta = ctx.saved_tensors
+        t = ctx.tables
+        g = gdelta.contiguous()
+        kt, pt = _dev(t.ktab), _dev(t.ptab)
+        gnoise = ops.ic_filter(g, kt, pt, ctx.box) if ctx.needs_input_grad[0] else None
+        gom = gs8 = None
+        if ctx.needs_input_grad[1]:
+            tang = ops.ic_filter_tangent(noise.contiguous(), kt, pt, _dev(t.dptab), ctx.box)
+            gom = _like(_dot(g, tang), ctx.params[0])
+        if ctx.needs_input_grad[2]:
+            gs8 = _like(_dot(g, delta) / ctx.sigma8, ctx.params[1])
+        return gnoise, gom, gs8, None, None
+
+
+class LPT(torch.autograd.Function):
+    """linear density -> (dx, p) at the grid points (order 1 or 2)."""
+
+    @staticmethod
+    def forward(ctx, ic, omega_c, order: int, tables: ForwardTables):
+        ic = ic.contiguous()
+        dx, p = ops.lpt(ic, order, *tables.lpt)
+        ctx.order, ctx.tables = order, tables
+        ctx.omega_c = omega_c
+        ctx.save_for_backward(ic)
+        return dx, p
+
+    @staticmethod
+    def backward(ctx, lam_x, lam_v):
+        (ic,) = ctx.saved_tensors
+        t = ctx.tables
+        c1x, c2x, c1p, c2p = t.lpt
+        lam_x = lam_x.contiguous()
+        lam_v = lam_v.contiguous()
+        gic = ops.lpt_adjoint(ic, ctx.order, c1x, c2x, c1p, c2p, lam_x, lam_v) if ctx.needs_input_grad[0] else None
+        gom = None
+        if ctx.needs_input_grad[1]:
+            f1 = ops.lpt(ic, 1, 1.0, 0.0, 0.0, 0.0)[0]
+            x1, v1 = _dot(lam_x, f1), _dot(lam_v, f1)
+            dc = [x1 + c1p * v1, 0.0, c1x * v1, 0.0]
+            if ctx.order == 2:
+                f2 = ops.lpt(ic, 2, 0.0, 1.0, 0.0, 0.0)[0]
+                x2, v2 = _dot(lam_x, f2), _dot(lam_v, f2)
+                dc[1] = x2 + c2p * v2
+                dc[3] = c2x * v2
+            gom = _like(sum(float(t.dlpt[i]) * dc[i] for i in range(4)), ctx.omega_c)
+        return gic, gom, None, None
+
+
+def kkd_forward(x: torch.Tensor, v: torch.Tensor, kicks, drifts, rho: torch.Tensor, force: torch.Tensor,
+                pot: torch.Tensor) -> None:
+    """The ReversibleDoubleKickDrift loop in place: per step kick with the force at the
+    current positions, drift, paint; rho ends as the CIC density of the final positions."""
+    rho.zero_()
+    ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT, rho)
+    ops.poisson_force(rho, 1.0, out=force, pot=pot)
+    n = len(kicks)
+    for i in range(n):
+        rho.zero_()
+        ops.kick_drift_paint(x, v, force, float(kicks[i]), float(drifts[i]),
+                             JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT, rho)
+        if i < n - 1:
+            ops.poisson_force(rho, 1.0, out=force, pot=pot)
+
+
+def kkd_reverse_adjoint(x: torch.Tensor, v: torch.Tensor, lam_x: torch.Tensor, lam_v: torch.Tensor, kicks, drifts):
+    """Backward sweep of kkd_forward, in place on (x, v, lam_x, lam_v): on return (x, v) is
+    the recomputed initial state and (lam_x, lam_v) the cotangent at it. Returns the FP64
+    (dL/dkick_n, dL/ddrift_n) arrays."""
+    shape = x.shape[:-1]
+    rho = torch.empty(shape, dtype=torch.float32, device=x.device)
+    pot = torch.empty_like(rho)
+    force = torch.empty((3,) + tuple(shape), dtype=torch.float32, device=x.device)
+    ubar = torch.empty_like(force)
+    rho_bar = torch.empty_like(rho)
+    n = len(kicks)
+    sens = torch.zeros(n, 2, dtype=torch.float64, device=x.device)
+    for i in reversed(range(n)):
+        k, d = float(kicks[i]), float(drifts[i])
+        rho.zero_()
+        ops.kick_drift_paint(x, v, None, 0.0, -d, JFLI_STEP_DRIFT | JFLI_STEP_PAINT, rho)
+        ops.poisson_force(rho, 1.0, out=force, pot=pot)
+        _, s = ops.adjoint_unkick_paint(x, v, lam_x, lam_v, force, k, d, ubar)
+        sens[i] = s
+        ops.poisson_divergence(ubar, aos=False, out=rho_bar)
+        ops.adjoint_position(x, lam_x, rho_bar=rho_bar, u=lam_v, force=force, scale=k)
+    return sens
+
+
+class ReversibleNBody(torch.autograd.Function):
+    """(dx, p) -> final CIC density of the ReversibleDoubleKickDrift loop."""
+
+    @staticmethod
+    def forward(ctx, dx, p, omega_c, tables: ForwardTables):
+        x = dx.detach().contiguous().clone()
+        v = p.detach().contiguous().clone()
+        shape = x.shape[:-1]
+        rho = torch.empty(shape, dtype=torch.float32, device=x.device)
+        pot = torch.empty_like(rho)
+        force = torch.empty((3,) + tuple(shape), dtype=torch.float32, device=x.device)
+        kkd_forward(x, v, tables.kicks, tables.drifts, rho, force, pot)
+        ctx.tables = tables
+        ctx.omega_c = omega_c
+        ctx.save_for_backward(x, v)
+        return rho
+
+    @staticmethod
+    def backward(ctx, grho):
+        x, v = ctx.saved_tensors
+        t = ctx.tables
+        x = x.clone()
+        v = v.clone()
+        lam_x = torch.zeros_like(x)
+        lam_v = torch.zeros_like(v)
+        ops.adjoint_position(x, lam_x, rho_bar=grho.contiguous())  # adjoint of the final paint
+        sens = kkd_reverse_adjoint(x, v, lam_x, lam_v, t.kicks, t.drifts)
+        gom = None
+        if ctx.needs_input_grad[2]:
+            sk, sd = sens[:, 0].cpu().numpy(), sens[:, 1].cpu().numpy()
+            gom = _like(float(np.dot(sk, t.dkicks) + np.dot(sd, t.ddrifts)), ctx.omega_c)
+        ctx.sensitivities = sens
+        return lam_x, lam_v, gom, None
+
+
+class PowerSpectrum(torch.autograd.Function):
+    """density -> P(k) in the kept bins (FP64), the jax-fli `power` estimator."""
+
+    @staticmethod
+    def forward(ctx, mesh, kedges: np.ndarray, box):
+        mesh = mesh.contiguous()
+        ke = _dev(kedges)
+        sums = ops.power_sums(mesh, ke, box)
+        cnt = sums[1]
+        vol = float(np.prod(np.asarray(box, np.float64) / np.asarray(mesh.shape[-3:], np.float64)))
+        norm = torch.where(cnt > 0, cnt, torch.ones_like(cnt))
+        pk = (sums[0] / norm)[1:-1] * vol
+        ctx.save_for_backward(mesh, ke, cnt)
+        ctx.vol, ctx.box = vol, box
+        return pk
+
+    @staticmethod
+    def backward(ctx, gpk):
+        mesh, ke, cnt = ctx.saved_tensors
+        w = torch.zeros(ke.numel() + 1, dtype=torch.float64, device=mesh.device)
+        c = cnt[1:-1]
+        w[1:-1] = torch.where(c > 0, 2.0 * gpk * ctx.vol / torch.where(c > 0, c, torch.ones_like(c)),
+                              torch.zeros_like(c))
+        return ops.power_adjoint(mesh, ke, w.float(), ctx.box), None, None
+
+
+# ----------------------------------------------------------------------------- model
+def forward_model_pk(noise: torch.Tensor, omega_c: torch.Tensor, sigma8: torch.Tensor, *, box, kedges, t0: float = 0.1,
+                     t1: float = 1.0, dt0: float, lpt_order: int = 2, tables: ForwardTables | None = None):
+    """P(k) of the final density of noise -> ICs -> LPT -> ReversibleDoubleKickDrift,
+    differentiable in noise, omega_c and sigma8 (0-d tensors) through the B200 adjoints."""
+    if tables is None:
+        tables = forward_tables(_scalar(omega_c), _scalar(sigma8), t0=t0, t1=t1, dt0=dt0,
+                                derivatives=bool(getattr(omega_c, "requires_grad", False)))
+    box = tuple(float(b) for b in box)
+    delta = ICFilter.apply(noise, omega_c, sigma8, tables, box)
+    dx, p = LPT.apply(delta, omega_c, lpt_order, tables)
+    rho = ReversibleNBody.apply(dx, p, omega_c, tables)
+    return PowerSpectrum.apply(rho, np.asarray(kedges, np.float64), box)
+
+
+def pk_log_loss(pk: torch.Tensor, pk_target: torch.Tensor) -> torch.Tensor:
+    """sum over bins of (log P - log P_target)^2; bins without modes are left out."""
+    mask = (pk_target > 0) & (pk.detach() > 0)
+    return torch.sum((torch.log(pk[mask]) - torch.log(pk_target[mask])) ** 2)

@@ -1,0 +1,274 @@
+"""Adjoint kernels and the reversible-adjoint gradient against finite differences.
+
+Small cases compare the CUDA adjoints (FP32) with central differences of the FP64 oracle
+(oracle/pm.py) along random directions; the 128^3 case (the differentiation
+configuration: ReversibleDoubleKickDrift, 20 steps from a = 0.1, box 500 Mpc/h, 2LPT,
+loss = sum over 32 bins of (log P - log P_target)^2) compares with central differences
+of the GPU forward model at eps = 1e-3."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import pm as opm
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    return torch.as_tensor(np.asarray(a, np.float32), device="cuda")
+
+
+def _kedges(n, box):
+    return np.geomspace(2 * np.pi / box * (1 - 1e-6), np.pi * n / box, 33)
+
+
+def _rel(a, b):
+    return abs(a - b) / max(abs(b), 1e-30)
+
+
+# --------------------------------------------------------------------------- KKD steps
+def test_kkd_step_vjp_matches_oracle_fd():
+    from jfli_b200.pm import adjoint as adj
+
+    n = 32
+    rng = np.random.default_rng(1)
+    x0 = (1.5 * rng.standard_normal((n, n, n, 3))).astype(np.float32)
+    v0 = (0.5 * rng.standard_normal((n, n, n, 3))).astype(np.float32)
+    kicks, drifts = np.array([0.3, 0.25, 0.35]), np.array([0.4, 0.5, 0.3])
+    a = rng.standard_normal(x0.shape)
+    b = rng.standard_normal(x0.shape)
+    r = rng.standard_normal(x0.shape)
+    s = rng.standard_normal(x0.shape)
+
+    x, v = _dev(x0), _dev(v0)
+    rho = torch.empty(n, n, n, device="cuda")
+    force = torch.empty(3, n, n, n, device="cuda")
+    pot = torch.empty_like(rho)
+    adj.kkd_forward(x, v, kicks, drifts, rho, force, pot)
+    lam_x, lam_v = _dev(a), _dev(b)
+    sens = adj.kkd_reverse_adjoint(x, v, lam_x, lam_v, kicks, drifts).cpu().numpy()
+    g_dir = float(np.sum(lam_x.cpu().numpy() * r) + np.sum(lam_v.cpu().numpy() * s))
+
+    def loss(xi, vi, ks=kicks, ds=drifts):
+        xf, vf, _ = opm.kkd_run(xi, vi, list(zip(ks, ds)), np.float64)
+        return float(np.sum(a * xf) + np.sum(b * vf))
+
+    eps = 1e-5
+    x64, v64 = x0.astype(np.float64), v0.astype(np.float64)
+    fd = (loss(x64 + eps * r, v64 + eps * s) - loss(x64 - eps * r, v64 - eps * s)) / (2 * eps)
+    print(f"direction: adjoint {g_dir:.8e} fd {fd:.8e}")
+    assert _rel(g_dir, fd) < 1e-4
+    for i in range(len(kicks)):
+        kp, km = kicks.copy(), kicks.copy()
+        kp[i] += eps
+        km[i] -= eps
+        fdk = (loss(x64, v64, ks=kp) - loss(x64, v64, ks=km)) / (2 * eps)
+        dp, dm = drifts.copy(), drifts.copy()
+        dp[i] += eps
+        dm[i] -= eps
+        fdd = (loss(x64, v64, ds=dp) - loss(x64, v64, ds=dm)) / (2 * eps)
+        print(f"step {i}: dkick {sens[i, 0]:.6e} vs {fdk:.6e}; ddrift {sens[i, 1]:.6e} vs {fdd:.6e}")
+        assert _rel(sens[i, 0], fdk) < 1e-4
+        assert _rel(sens[i, 1], fdd) < 1e-4
+
+
+def test_reverse_recovers_initial_state():
+    from jfli_b200.pm import adjoint as adj
+
+    n = 64
+    rng = np.random.default_rng(2)
+    x0 = _dev(1.0 * rng.standard_normal((n, n, n, 3)))
+    v0 = _dev(0.3 * rng.standard_normal((n, n, n, 3)))
+    kicks = np.linspace(0.2, 0.4, 10)
+    drifts = np.linspace(0.5, 0.2, 10)
+    x, v = x0.clone(), v0.clone()
+    rho = torch.empty(n, n, n, device="cuda")
+    force = torch.empty(3, n, n, n, device="cuda")
+    adj.kkd_forward(x, v, kicks, drifts, rho, force, torch.empty_like(rho))
+    moved = float((x - x0).abs().max())
+    adj.kkd_reverse_adjoint(x, v, torch.zeros_like(x), torch.zeros_like(v), kicks, drifts)
+    ex, ev = float((x - x0).abs().max()), float((v - v0).abs().max())
+    print(f"max displacement change {moved:.3f} cells; after reverse |dx| {ex:.2e}, |dv| {ev:.2e}")
+    assert moved > 0.5
+    assert ex < 1e-4 and ev < 1e-4
+
+
+# --------------------------------------------------------------------------- P(k), LPT, ICs
+def test_power_adjoint_matches_oracle_fd():
+    from jfli_b200.pm import adjoint as adj
+
+    n, box = 32, 128.0
+    rng = np.random.default_rng(3)
+    m0 = (1.0 + 0.3 * rng.standard_normal((n, n, n))).astype(np.float32)
+    ke = _kedges(n, box)
+    g = rng.standard_normal(len(ke) - 1)
+    r = rng.standard_normal(m0.shape)
+    mesh = _dev(m0).requires_grad_(True)
+    pk = adj.PowerSpectrum.apply(mesh, ke, (box,) * 3)
+    (pk * torch.as_tensor(g, device="cuda")).sum().backward()
+    g_dir = float(np.sum(mesh.grad.cpu().numpy() * r))
+
+    def loss(m):
+        return float(np.sum(g * opm.power(m, (box,) * 3, ke, kdtype=np.float32)[1]))
+
+    eps = 1e-3
+    fd = (loss(m0.astype(np.float64) + eps * r) - loss(m0.astype(np.float64) - eps * r)) / (2 * eps)
+    print(f"P(k) adjoint {g_dir:.8e} fd {fd:.8e}")
+    assert _rel(g_dir, fd) < 1e-4
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_lpt_adjoint_matches_oracle_fd(order):
+    from jfli_b200.pm import adjoint as adj
+
+    n = 32
+    rng = np.random.default_rng(4 + order)
+    ic0 = (0.5 * rng.standard_normal((n, n, n))).astype(np.float32)
+    coeffs = (1.3, -0.4, 2.1, 3.5)
+    tables = adj.ForwardTables(ktab=None, ptab=None, lpt=coeffs, kicks=None, drifts=None)
+    a = rng.standard_normal((n, n, n, 3))
+    b = rng.standard_normal((n, n, n, 3))
+    r = rng.standard_normal(ic0.shape)
+    ic = _dev(ic0).requires_grad_(True)
+    dx, p = adj.LPT.apply(ic, None, order, tables)
+    (torch.sum(dx * _dev(a)) + torch.sum(p * _dev(b))).backward()
+    g_dir = float(np.sum(ic.grad.cpu().numpy() * r))
+
+    def loss(f):
+        dxo, po = opm.lpt(f, *coeffs, order=order, dtype=np.float64)
+        return float(np.sum(a * dxo) + np.sum(b * po))
+
+    eps = 1e-3
+    f64 = ic0.astype(np.float64)
+    fd = (loss(f64 + eps * r) - loss(f64 - eps * r)) / (2 * eps)
+    print(f"LPT{order} adjoint {g_dir:.8e} fd {fd:.8e}")
+    assert _rel(g_dir, fd) < 1e-4
+
+
+def test_ic_filter_gradients_match_oracle_fd():
+    from jfli_b200.pm import adjoint as adj
+
+    n, box = 32, 128.0
+    rng = np.random.default_rng(7)
+    w0 = rng.standard_normal((n, n, n)).astype(np.float32)
+    a = rng.standard_normal((n, n, n))
+    r = rng.standard_normal((n, n, n))
+    oc, s8 = 0.27, 0.79
+    tab = adj.forward_tables(oc, s8, t0=0.1, t1=1.0, dt0=0.45)
+    w = _dev(w0).requires_grad_(True)
+    om = torch.tensor(oc, dtype=torch.float64, requires_grad=True)
+    sg = torch.tensor(s8, dtype=torch.float64, requires_grad=True)
+    delta = adj.ICFilter.apply(w, om, sg, tab, (box,) * 3)
+    torch.sum(delta * _dev(a)).backward()
+
+    def loss(wi, oci=oc, s8i=s8):
+        t = adj.forward_tables(oci, s8i, t0=0.1, t1=1.0, dt0=0.45, derivatives=False)
+        return float(np.sum(a * opm.ic_filter(wi, (box,) * 3, t.ktab, t.ptab, dtype=np.float64)))
+
+    w64 = w0.astype(np.float64)
+    fd_w = (loss(w64 + r) - loss(w64 - r)) / 2.0  # linear in w
+    g_w = float(np.sum(w.grad.cpu().numpy() * r))
+    h = 1e-4
+    fd_s8 = (loss(w64, s8i=s8 + h) - loss(w64, s8i=s8 - h)) / (2 * h)
+    fd_oc = (loss(w64, oci=oc + h) - loss(w64, oci=oc - h)) / (2 * h)
+    print(f"noise {g_w:.6e} vs {fd_w:.6e}; sigma8 {float(sg.grad):.6e} vs {fd_s8:.6e}; "
+          f"Omega_c {float(om.grad):.6e} vs {fd_oc:.6e}")
+    assert _rel(g_w, fd_w) < 1e-4
+    assert _rel(float(sg.grad), fd_s8) < 1e-4
+    assert _rel(float(om.grad), fd_oc) < 1e-3
+
+
+# --------------------------------------------------------------------------- whole chain
+def _oracle_loss(w, oc, s8, *, n, box, t0, dt0, order, kedges, pk_target):
+    from jfli_b200.pm import adjoint as adj
+
+    t = adj.forward_tables(oc, s8, t0=t0, t1=1.0, dt0=dt0, derivatives=False)
+    ic = opm.ic_filter(w, (box,) * 3, t.ktab, t.ptab, dtype=np.float64)
+    dx, p = opm.lpt(ic, *t.lpt, order=order, dtype=np.float64)
+    x, _, _ = opm.kkd_run(dx, p, list(zip(t.kicks, t.drifts)), np.float64)
+    pk = opm.power(opm.cic_paint(x), (box,) * 3, kedges, kdtype=np.float32)[1]
+    m = (pk_target > 0) & (pk > 0)
+    return float(np.sum((np.log(pk[m]) - np.log(pk_target[m])) ** 2))
+
+
+def test_full_chain_gradient_matches_oracle_fd():
+    from jfli_b200.pm import adjoint as adj
+
+    n, box, t0, dt0, order = 32, 128.0, 0.1, 0.225, 2
+    ke = _kedges(n, box)
+    rng = np.random.default_rng(8)
+    w0 = rng.standard_normal((n, n, n)).astype(np.float32)
+    wt = np.random.default_rng(9).standard_normal((n, n, n)).astype(np.float32)
+    oc, s8 = 0.2607, 0.8102
+    with torch.no_grad():
+        pk_t = adj.forward_model_pk(_dev(wt), torch.tensor(oc), torch.tensor(s8), box=(box,) * 3, kedges=ke, t0=t0,
+                                    dt0=dt0, lpt_order=order)
+    w = _dev(w0).requires_grad_(True)
+    om = torch.tensor(oc, dtype=torch.float64, requires_grad=True)
+    sg = torch.tensor(s8, dtype=torch.float64, requires_grad=True)
+    pk = adj.forward_model_pk(w, om, sg, box=(box,) * 3, kedges=ke, t0=t0, dt0=dt0, lpt_order=order)
+    loss = adj.pk_log_loss(pk, pk_t)
+    loss.backward()
+    r = rng.standard_normal((n, n, n))
+    g_w = float(np.sum(w.grad.cpu().numpy() * r))
+    kw = dict(n=n, box=box, t0=t0, dt0=dt0, order=order, kedges=ke, pk_target=pk_t.cpu().numpy())
+    w64 = w0.astype(np.float64)
+    L0 = _oracle_loss(w64, oc, s8, **kw)
+    e = 1e-4
+    fd_w = (_oracle_loss(w64 + e * r, oc, s8, **kw) - _oracle_loss(w64 - e * r, oc, s8, **kw)) / (2 * e)
+    fd_oc = (_oracle_loss(w64, oc + e, s8, **kw) - _oracle_loss(w64, oc - e, s8, **kw)) / (2 * e)
+    fd_s8 = (_oracle_loss(w64, oc, s8 + e, **kw) - _oracle_loss(w64, oc, s8 - e, **kw)) / (2 * e)
+    print(f"loss GPU {float(loss):.8e} oracle {L0:.8e}")
+    print(f"noise {g_w:.6e} vs {fd_w:.6e}; Omega_c {float(om.grad):.6e} vs {fd_oc:.6e}; "
+          f"sigma8 {float(sg.grad):.6e} vs {fd_s8:.6e}")
+    assert _rel(float(loss), L0) < 1e-3
+    assert _rel(g_w, fd_w) < 2e-3
+    assert _rel(float(om.grad), fd_oc) < 2e-3
+    assert _rel(float(sg.grad), fd_s8) < 2e-3
+
+
+def test_differentiation_config_128_matches_gpu_fd():
+    """128^3, box 500, 20 KKD steps from a = 0.1, 2LPT, 32-bin log-P loss against a
+    second seed; gradients vs central differences (eps = 1e-3) of the GPU forward."""
+    import time
+
+    from jfli_b200.pm import adjoint as adj
+
+    n, box, t0, order = 128, 500.0, 0.1, 2
+    dt0 = 0.9 / 20
+    ke = _kedges(n, box)
+    rng = np.random.default_rng(10)
+    w0 = _dev(rng.standard_normal((n, n, n)))
+    wt = _dev(np.random.default_rng(11).standard_normal((n, n, n)))
+    oc, s8 = 0.2607, 0.8102
+    kw = dict(box=(box,) * 3, kedges=ke, t0=t0, dt0=dt0, lpt_order=order)
+
+    def loss_at(w, o, s):
+        with torch.no_grad():
+            return float(adj.pk_log_loss(adj.forward_model_pk(w, torch.tensor(o), torch.tensor(s), **kw), pk_t))
+
+    with torch.no_grad():
+        pk_t = adj.forward_model_pk(wt, torch.tensor(oc), torch.tensor(s8), **kw)
+    for it in range(2):  # second iteration timed (tables and workspaces warm)
+        w = w0.clone().requires_grad_(True)
+        om = torch.tensor(oc, dtype=torch.float64, requires_grad=True)
+        sg = torch.tensor(s8, dtype=torch.float64, requires_grad=True)
+        torch.cuda.synchronize()
+        t_start = time.perf_counter()
+        loss = adj.pk_log_loss(adj.forward_model_pk(w, om, sg, **kw), pk_t)
+        loss.backward()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t_start
+    r = torch.randn(n, n, n, device="cuda", generator=torch.Generator(device="cuda").manual_seed(12))
+    g_w = float(torch.sum(w.grad.double() * r.double()))
+    e = 1e-3
+    fd_w = (loss_at(w0 + e * r, oc, s8) - loss_at(w0 - e * r, oc, s8)) / (2 * e)
+    fd_oc = (loss_at(w0, oc + e, s8) - loss_at(w0, oc - e, s8)) / (2 * e)
+    fd_s8 = (loss_at(w0, oc, s8 + e) - loss_at(w0, oc, s8 - e)) / (2 * e)
+    print(f"128^3 gradient iteration {wall * 1e3:.1f} ms; loss {float(loss):.6e}")
+    print(f"noise {g_w:.6e} vs {fd_w:.6e}; Omega_c {float(om.grad):.6e} vs {fd_oc:.6e}; "
+          f"sigma8 {float(sg.grad):.6e} vs {fd_s8:.6e}")
+    assert _rel(g_w, fd_w) < 1e-2
+    assert _rel(float(om.grad), fd_oc) < 1e-2
+    assert _rel(float(sg.grad), fd_s8) < 1e-2
