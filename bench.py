@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=512)
     ap.add_argument("--serve-rate", type=float, default=150.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serve-256", type=int, default=6, help="256^3 requests for the served-vs-plain pair")
+    ap.add_argument("--grad-iters", type=int, default=5, help="timed gradient iterations at 128^3")
     return ap.parse_args()
 
 
@@ -164,7 +165,7 @@ def run_gpu(args, world, rank):
     rho = torch.empty(n, n, n, device="cuda")
     pot = torch.empty_like(rho)
     force = torch.empty(3, n, n, n, device="cuda")
-    # the config-2 schedule: EfficientDriftDoubleKick, dt0 = 0.9/40 from a = 0.1 to a = 1
+    # the 40-step schedule of the 256^3 run: EfficientDriftDoubleKick, dt0 = 0.9/40 from a = 0.1 to a = 1
     from jfli_b200.pm.integrate import time_events
 
     dt0 = 0.9 / E2E_STEPS
@@ -238,6 +239,7 @@ def run_gpu(args, world, rank):
     # ---- end-to-end through the public API, host buffers in and out
     e2e = run_e2e(args, cosmo, n, box)
     serve = run_serving(args) if world == 1 else None
+    grad = run_gradient(args) if world == 1 else None
     # clocks are sampled every 200 ms from before the warm-up through the e2e requests
     clk = clocks.stop() if rank == 0 else None
 
@@ -251,7 +253,8 @@ def run_gpu(args, world, rank):
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": ncu_traffic(n),
             "peak_source": "measured" if peaks else "fallback", "avg_launch_ms": round(kdp_avg_ms, 4),
             "algorithmic_bytes_per_launch": alg_bytes, "step_share": round(sum(kdp) / ms, 4)}
-    return dict(value=value, ms=ms_max, clocks=clk, launches=launches, e2e=e2e, roofline=roof, serving=serve)
+    return dict(value=value, ms=ms_max, clocks=clk, launches=launches, e2e=e2e, roofline=roof, serving=serve,
+                gradient=grad)
 
 
 def ncu_traffic(n):
@@ -321,7 +324,7 @@ def run_serving(args):
 
     if args.serve_requests <= 0:
         return None
-    reqs = serving.poisson_stream(args.serve_requests, args.serve_rate, seed=0, grad_fraction=0.0)
+    reqs = serving.poisson_stream(args.serve_requests, args.serve_rate, seed=0, grad_fraction=0.25)
     eng = serving.Engine(sizes=(64, 96, 128, 192), hbm_budget_gb=24.0, max_slots=16, keep_density=False)
     warm = serving.poisson_stream(16, 0.0, seed=1, grad_fraction=0.0)
     for r in warm:
@@ -340,8 +343,10 @@ def run_serving(args):
     p_stats = serving.summarize(plain, reqs)
     worst = max(serving.pk_max_rel(served[r.rid].pk, plain[r.rid].pk) for r in reqs)
 
+    n_grad = sum(r.want_grad for r in reqs)
     out = {"stream": f"{len(reqs)} requests, Poisson arrivals at {args.serve_rate:g}/s, mesh U{{64,96,128,192}}, "
-                     f"10-40 KDK steps, no gradient requests (the adjoint is not on the batched path)",
+                     f"10-40 KDK steps; {n_grad} also ask for the gradient of the 32-bin log-P(k) loss (reversible "
+                     f"KKD adjoint, same mesh and step count) w.r.t. white noise, Omega_c and sigma8",
            "served": s_stats, "served_all_at_once": s_cap, "plain": p_stats,
            "slots": eng.capacity(), "served_launches": launches,
            "max_pk_rel_served_vs_plain": float(f"{worst:.3e}")}
@@ -359,6 +364,57 @@ def run_serving(args):
                          "plain_p50_ms": p256["p50_ms"], "slots": 2,
                          "per": "request: ICs + 2LPT + 40 KDK steps + P(k) to host"}
     return out
+
+
+def run_gradient(args):
+    """Wall time of one gradient iteration of the differentiation configuration: 128^3,
+    box 500 Mpc/h, 2LPT, ReversibleDoubleKickDrift 20 steps from a = 0.1, loss = sum over
+    32 bins of (log P - log P_target)^2, gradient w.r.t. the white noise, Omega_c, sigma8."""
+    import torch
+
+    from jfli_b200 import ops
+    from jfli_b200.pm import adjoint as adj
+
+    if args.grad_iters <= 0:
+        return None
+    n, box = 128, 500.0
+    ke = np.geomspace(2 * np.pi / box * (1 - 1e-6), np.pi * n / box, 33)
+    kw = dict(box=(box,) * 3, kedges=ke, t0=0.1, dt0=0.9 / 20, lpt_order=2)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    w0 = torch.randn(n, n, n, device="cuda", generator=g)
+    wt = torch.randn(n, n, n, device="cuda", generator=g)
+    tables = adj.forward_tables(0.2607, 0.8102, t0=0.1, t1=1.0, dt0=0.9 / 20)
+    with torch.no_grad():
+        pk_t = adj.forward_model_pk(wt, torch.tensor(0.2607), torch.tensor(0.8102), tables=tables, **kw)
+
+    def iteration():
+        w = w0.clone().requires_grad_(True)
+        om = torch.tensor(0.2607, dtype=torch.float64, requires_grad=True)
+        sg = torch.tensor(0.8102, dtype=torch.float64, requires_grad=True)
+        loss = adj.pk_log_loss(adj.forward_model_pk(w, om, sg, tables=tables, **kw), pk_t)
+        loss.backward()
+        return w.grad
+
+    for _ in range(2):
+        iteration()
+    torch.cuda.synchronize()
+    l0 = ops.launch_count()
+    times = []
+    for _ in range(args.grad_iters):
+        t = time.perf_counter()
+        iteration()
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t)
+    t_tab = time.perf_counter()
+    adj.forward_tables(0.2607, 0.8102, t0=0.1, t1=1.0, dt0=0.9 / 20)
+    t_tab = time.perf_counter() - t_tab
+    return {"workload": "128^3, box 500 Mpc/h, 2LPT, ReversibleDoubleKickDrift 20 steps, 32-bin log-P loss; "
+                        "d/d(white noise, Omega_c, sigma8)",
+            "ms_per_iteration": round(1e3 * statistics.median(times), 2), "iterations": args.grad_iters,
+            "launches_per_iteration": (ops.launch_count() - l0) // args.grad_iters,
+            "host_tables_ms": round(1e3 * t_tab, 1),
+            "note": "wall time, forward + backward on the device with the FP64 host tables precomputed; "
+                    "host_tables_ms is the per-cosmology table build (with Omega_c derivatives)"}
 
 
 def dataclasses_replace(obj, **kw):
@@ -438,7 +494,7 @@ def main():
                            "solver": "EfficientDriftDoubleKick", "parallelism": f"replicas x{world}",
                            "l2": "particle state (x, v: 402 MB) exceeds the 126 MB L2; no flush"},
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"], "clocks": res["clocks"],
-                "gpu_launches": res["launches"], "serving": res["serving"]}
+                "gpu_launches": res["launches"], "serving": res["serving"], "gradient": res["gradient"]}
         print(json.dumps(line), flush=True)
     if world > 1:
         from jfli_b200 import replicas

@@ -54,7 +54,13 @@ def interpolate_initial_conditions(initial_field, mesh_size, box_size, *, cosmo=
         halo_size = (halo_size, halo_size)
     w = _as_device(initial_field, mesh_size)
     kt, pt = _pk_tables(cosmo, pk_fn, n_table, mesh_size, box_size)
-    field = ops.ic_filter(w, kt, pt, box_size, zero_mode_one=zero_mode_one)
+    if torch.is_grad_enabled() and w.requires_grad and not zero_mode_one:
+        from .pm.adjoint import ForwardTables, ICFilter
+
+        tables = ForwardTables(ktab=kt, ptab=pt, lpt=None, kicks=None, drifts=None)
+        field = ICFilter.apply(w, None, None, tables, box_size)
+    else:
+        field = ops.ic_filter(w, kt, pt, box_size, zero_mode_one=zero_mode_one)
     return DensityField(array=field, mesh_size=mesh_size, box_size=box_size, observer_position=observer_position,
                         sharding=sharding, halo_size=tuple(halo_size), nside=nside, field_size=field_size,
                         flatsky_npix=flatsky_npix, scale_factors=0.0, status=FieldStatus.INITIAL_FIELD,

@@ -23,9 +23,11 @@ _workspaces: dict[tuple, torch.Tensor] = {}
 
 
 def workspace(nbytes: int, key: str = "default", device=None) -> torch.Tensor:
-    """A cached uint8 device buffer of at least `nbytes` (one per key and device)."""
+    """A cached uint8 device buffer of at least `nbytes`, one per key, device and current
+    stream, so that work enqueued on different streams never shares scratch space."""
     dev = torch.device("cuda") if device is None else torch.device(device)
-    k = (key, dev.index if dev.index is not None else torch.cuda.current_device())
+    idx = dev.index if dev.index is not None else torch.cuda.current_device()
+    k = (key, idx, torch.cuda.current_stream(idx).cuda_stream)
     buf = _workspaces.get(k)
     if buf is None or buf.numel() < nbytes:
         buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)

@@ -97,6 +97,8 @@ def forward_tables(omega_c: float, sigma8: float, *, t0: float, t1: float, dt0: 
 
 
 def _dev(a) -> torch.Tensor:
+    if isinstance(a, torch.Tensor):
+        return a.to(device="cuda", dtype=torch.float32).contiguous()
     return torch.as_tensor(np.asarray(a, np.float32), device="cuda")
 
 
@@ -104,7 +106,9 @@ def _dot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
     return torch.sum(a.double() * b.double())
 
 
-def _scalar(t) -> float:
+def _scalar(t) -> float | None:
+    if t is None:
+        return None
     return float(t.detach()) if isinstance(t, torch.Tensor) else float(t)
 
 

@@ -160,6 +160,41 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
     return RunResult(snapshots=snapshots, disp=x, vel=v, steps=n_steps)
 
 
+def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t0: float, dt0: float,
+                       dtype=np.float32) -> RunResult:
+    """The ReversibleDoubleKickDrift loop as one autograd node whose backward is the
+    reversible adjoint (pm/adjoint.py), for inputs that require gradients. The
+    reference's equivalent is nbody(..., adjoint="reverse") under jax.grad
+    (pm/integrate.py:147-535). Covers one density snapshot without a correction kernel."""
+    from .adjoint import ForwardTables, ReversibleNBody
+    from .interp import NoInterp
+
+    interp = solver.interp_kernel
+    tgt = interp.painting.target if interp.painting is not None else "particles"
+    ts_arr = np.atleast_1d(np.asarray(ts))
+    if not (isinstance(solver, ReversibleDoubleKickDrift) and isinstance(solver.pgd_kernel, NoCorrection)
+            and isinstance(interp, NoInterp) and tgt == "density" and ts_arr.size == 1
+            and _scalar_weight(interp.painting.weights) == 1.0):
+        raise NotImplementedError(
+            "gradients run through the reversible adjoint: ReversibleDoubleKickDrift with NoCorrection and a "
+            "NoInterp density snapshot at one time")
+    if dx.unit != PositionUnit.GRID_RELATIVE:
+        raise NotImplementedError("differentiable integration takes GRID_RELATIVE displacements")
+    steps = [(e[1], e[2]) for e in time_events(t0, ts, dt0, dtype) if e[0] == "step"]
+    cs = [solver.step_coefficients(cosmo, a, b, dt0, t0) for a, b in steps]
+    tables = ForwardTables(ktab=None, ptab=None, lpt=None, kicks=np.array([c.kick for c in cs]),
+                           drifts=np.array([c.drift for c in cs]))
+    rho = ReversibleNBody.apply(dx.array.contiguous(), p.array.contiguous(), None, tables)
+    from ..fields import DensityField, FieldStatus
+
+    t_target = float(ts_arr[0])
+    state = NBodyState(interp_state=interp.init(), t_initial=t0)
+    snap = DensityField(array=rho, **dx.replace(scale_factors=t_target)._meta_for_density(FieldStatus.DENSITY_FIELD))
+    snap = snap.replace(scale_factors=t_target, comoving_centers=float(interp.r_centers[state.interp_state.shell_idx]),
+                        density_width=float(interp.density_widths[state.interp_state.shell_idx]))
+    return RunResult(snapshots=[snap], disp=None, vel=None, steps=len(steps))
+
+
 def run_stepwise(solver, dx, p, cosmo, ts, t0, dt0, dtype=np.float32) -> RunResult:
     """The reference loop driven through solver.init/step/save_at (unfused)."""
     disp, vel, state = solver.init(dx, p, t0, t0 + dt0, dt0, cosmo)
@@ -194,7 +229,10 @@ def integrate(displacements, velocities, cosmo, ts, solver, t0, t1, dt0, adjoint
             f"Use SharpeningKernel for reversible integration, or use adjoint='checkpointed'.")
     if adjoint not in ("checkpointed", "reverse", "lax"):
         raise ValueError(f"Unknown adjoint type: {adjoint}")
-    run = run_fused if fused else run_stepwise
-    res = run(solver, displacements, velocities, cosmo, ts, t0, dt0)
+    if torch.is_grad_enabled() and (displacements.array.requires_grad or velocities.array.requires_grad):
+        res = run_differentiable(solver, displacements, velocities, cosmo, ts, t0, dt0)
+    else:
+        run = run_fused if fused else run_stepwise
+        res = run(solver, displacements, velocities, cosmo, ts, t0, dt0)
     out = _stack(res.snapshots)
     return out, res

@@ -95,7 +95,14 @@ def lpt(cosmo, initial_field: DensityField, *, ts=None, nb_shells=None, density_
             f"Painting target {painting.target} is incompatible with snapshot mode. Use 'particles' or 'density'.")
     a = float(np.asarray(ts_resolved).reshape(-1)[0])
     c1x, c2x, c1p, c2p = lpt_coefficients(cosmo, a)
-    dx, p = ops.lpt(initial_field.array.contiguous(), order, c1x, c2x, c1p, c2p)
+    ic = initial_field.array.contiguous()
+    if torch.is_grad_enabled() and ic.requires_grad:
+        from .adjoint import LPT, ForwardTables
+
+        tables = ForwardTables(ktab=None, ptab=None, lpt=(c1x, c2x, c1p, c2p), kicks=None, drifts=None)
+        dx, p = LPT.apply(ic, None, order, tables)
+    else:
+        dx, p = ops.lpt(ic, order, c1x, c2x, c1p, c2p)
     status = FieldStatus.LPT1 if order == 1 else FieldStatus.LPT2
     a_arr = np.atleast_1d(np.float64(a))
     meta = dict(status=status, scale_factors=a_arr, comoving_centers=cj.radial_comoving_distance(cosmo, a_arr),

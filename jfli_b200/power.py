@@ -56,5 +56,12 @@ def power(mesh, mesh2=None, *, box_shape, kedges=None, multipoles=0, los=(0.0, 0
     box_shape = tuple(float(v) for v in box_shape)
     if kedges is None:
         kedges = default_kedges(mesh_shape, box_shape)
+    if torch.is_grad_enabled() and mesh.requires_grad:
+        # differentiable path: the adjoint kernel gives dL/dmesh (pm/adjoint.py)
+        from .pm.adjoint import PowerSpectrum
+
+        with torch.no_grad():
+            kavg, _ = finalize(power_sums(mesh, box_shape, kedges), mesh_shape, box_shape)
+        return kavg, PowerSpectrum.apply(mesh, np.asarray(kedges, np.float64), box_shape)
     sums = power_sums(mesh, box_shape, kedges)
     return finalize(sums, mesh_shape, box_shape)

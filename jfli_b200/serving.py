@@ -62,6 +62,11 @@ class ForwardResult:
     arrival: float
     admitted: float = 0.0
     done: float = 0.0
+    # gradient requests: loss and gradients of the log-P(k) loss (reversible adjoint)
+    loss: float | None = None
+    grad_noise: torch.Tensor | None = None  # host copy, (mesh,)*3
+    grad_omega_c: float | None = None
+    grad_sigma8: float | None = None
 
     @property
     def latency(self) -> float:
@@ -85,10 +90,93 @@ def prepare(req: ForwardRequest) -> dict:
     dt0 = (1.0 - A_INIT) / req.steps
     ev = [(e[1], e[2]) for e in time_events(A_INIT, [1.0], dt0) if e[0] == "step"]
     kicks, drifts = EDK.schedule_arrays(c, [a for a, _ in ev], [b for _, b in ev], dt0)
-    return dict(rid=req.rid, ktab=k.astype(np.float32), ptab=pk.astype(np.float32),
-                lpt=lpt_coefficients(c, A_INIT), init_kick=EDK.init_kick(c, A_INIT, A_INIT + dt0),
-                kicks=np.asarray(kicks, np.float64), drifts=np.asarray(drifts, np.float64),
-                kedges=config_kedges(req.mesh, req.box).astype(np.float32))
+    out = dict(rid=req.rid, ktab=k.astype(np.float32), ptab=pk.astype(np.float32),
+               lpt=lpt_coefficients(c, A_INIT), init_kick=EDK.init_kick(c, A_INIT, A_INIT + dt0),
+               kicks=np.asarray(kicks, np.float64), drifts=np.asarray(drifts, np.float64),
+               kedges=config_kedges(req.mesh, req.box).astype(np.float32))
+    if req.want_grad:
+        from .pm.adjoint import forward_tables
+
+        out["grad_tables"] = forward_tables(req.omega_c, req.sigma8, t0=A_INIT, t1=1.0, dt0=dt0)
+    return out
+
+
+# Target spectrum of the gradient requests' loss: the fiducial cosmology, a second seed.
+TARGET_SEED = 1_000_003
+FIDUCIAL = (0.2607, 0.8102)
+
+
+def gradient_request(req: ForwardRequest, prep: dict, pk_target: torch.Tensor):
+    """Loss sum_b (log P_b - log P_target,b)^2 of the request's ReversibleDoubleKickDrift
+    run (its mesh, cosmology and step count) and its gradients with respect to the white
+    noise, Omega_c and sigma8 through the reversible adjoint. Enqueued on the current stream."""
+    from .pm.adjoint import forward_model_pk, pk_log_loss
+
+    w = device_white_noise(req.seed, req.mesh).requires_grad_(True)
+    om = torch.tensor(float(req.omega_c), dtype=torch.float64, requires_grad=True)
+    sg = torch.tensor(float(req.sigma8), dtype=torch.float64, requires_grad=True)
+    pk = forward_model_pk(w, om, sg, box=(req.box,) * 3, kedges=config_kedges(req.mesh, req.box), t0=A_INIT,
+                          dt0=(1.0 - A_INIT) / req.steps, tables=prep["grad_tables"])
+    loss = pk_log_loss(pk, pk_target)
+    loss.backward()
+    return loss.detach(), w.grad, om.grad, sg.grad
+
+
+def target_spectrum(n: int, box: float, steps: int = 20) -> torch.Tensor:
+    from .pm.adjoint import forward_model_pk
+
+    with torch.no_grad():
+        return forward_model_pk(device_white_noise(TARGET_SEED, n), torch.tensor(FIDUCIAL[0]),
+                                torch.tensor(FIDUCIAL[1]), box=(box,) * 3, kedges=config_kedges(n, box), t0=A_INIT,
+                                dt0=(1.0 - A_INIT) / steps)
+
+
+class GradientWorker:
+    """Runs gradient requests one at a time on its own CUDA stream from a host thread,
+    concurrently with the batched forward steps on the main stream."""
+
+    def __init__(self):
+        import queue
+        import threading
+
+        self.stream = torch.cuda.Stream()
+        self.inbox: "queue.Queue" = queue.Queue()
+        self.outbox: "queue.Queue" = queue.Queue()
+        self.targets: dict = {}
+        self.t0 = time.perf_counter()
+        self._thread = threading.Thread(target=self._loop, daemon=True)
+        self._thread.start()
+
+    def target(self, n: int, box: float) -> torch.Tensor:
+        key = (n, box)
+        if key not in self.targets:
+            with torch.cuda.stream(self.stream):
+                self.targets[key] = target_spectrum(n, box)
+            self.stream.synchronize()
+        return self.targets[key]
+
+    def submit(self, req, prep):
+        self.inbox.put((req, prep))
+
+    def _loop(self):
+        while True:
+            item = self.inbox.get()
+            if item is None:
+                return
+            req, prep = item
+            try:
+                with torch.cuda.stream(self.stream):
+                    loss, gw, gom, gs8 = gradient_request(req, prep, self.target(req.mesh, req.box))
+                    gw_h = torch.empty(gw.shape, dtype=torch.float32, pin_memory=True)
+                    gw_h.copy_(gw, non_blocking=True)
+                self.stream.synchronize()
+                self.outbox.put((req.rid, float(loss), gw_h, float(gom), float(gs8), time.perf_counter(), None))
+            except Exception as exc:  # reported to the caller through the outbox
+                self.outbox.put((req.rid, None, None, None, None, time.perf_counter(), exc))
+
+    def close(self):
+        self.inbox.put(None)
+        self._thread.join(timeout=60)
 
 
 def device_white_noise(seed: int, n: int, device="cuda") -> torch.Tensor:
@@ -281,6 +369,9 @@ class Engine:
         self._ready = False
         self.results: dict[int, ForwardResult] = {}
         self._inflight = []  # finished slots whose P(k) / density copies are still on the stream
+        self._grad = None
+        self._await_grad: dict[int, ForwardResult] = {}  # forward done, gradient pending
+        self._grad_done: dict[int, tuple] = {}  # gradient done, forward pending
 
     def capacity(self) -> dict:
         return {n: g.B for n, g in self.groups.items()}
@@ -301,6 +392,14 @@ class Engine:
         if self._pool is not None:
             self._pool.shutdown(wait=True, cancel_futures=True)
             self._pool = None
+        if self._grad is not None:
+            self._grad.close()
+            self._grad = None
+
+    def _gradient_worker(self) -> GradientWorker:
+        if self._grad is None:
+            self._grad = GradientWorker()
+        return self._grad
 
     def _finalize(self, g: SizeGroup, b: int):
         s = g.slots[b]
@@ -332,20 +431,38 @@ class Engine:
             res.pk = (s[0] / cnt)[1:-1] * vol
             res.k = (s[2] / cnt)[1:-1]
             res.done = now_fn()
-            self.results[res.rid] = res
+            if req.want_grad:
+                self._await_grad[res.rid] = res
+            else:
+                self.results[res.rid] = res
         self._inflight = keep
+        if self._grad is not None:
+            while not self._grad.outbox.empty():
+                rid, loss, gw, gom, gs8, t_done, exc = self._grad.outbox.get()
+                if exc is not None:
+                    raise RuntimeError(f"gradient request {rid} failed") from exc
+                self._grad_done[rid] = (loss, gw, gom, gs8, t_done - self._t0_abs)
+        for rid in [r for r in self._await_grad if r in self._grad_done]:
+            res = self._await_grad.pop(rid)
+            loss, gw, gom, gs8, t_done = self._grad_done.pop(rid)
+            res.loss, res.grad_noise, res.grad_omega_c, res.grad_sigma8 = loss, gw, gom, gs8
+            res.done = max(res.done, t_done)
+            self.results[rid] = res
 
     def run(self, requests, realtime: bool = True):
         """Serve `requests` (arrival times in seconds after the call); returns {rid: ForwardResult}."""
         for r in requests:
             if r.mesh not in self.groups:
                 raise ValueError(f"request {r.rid}: mesh {r.mesh} has no slot group (sizes {list(self.groups)})")
-            if r.want_grad:
-                raise NotImplementedError("gradient requests are not served by the batched engine")
         self.warmup()
         pool = self._pool
         reqs = sorted(requests, key=lambda r: r.arrival)
+        if any(r.want_grad for r in reqs):
+            gw = self._gradient_worker()
+            for key in sorted({(r.mesh, r.box) for r in reqs if r.want_grad}):
+                gw.target(*key)
         t0 = time.perf_counter()
+        self._t0_abs = t0
         now = lambda: time.perf_counter() - t0
         futures = {}
         waiting = deque()  # arrived, not yet in a slot (per-size FIFO order)
@@ -369,6 +486,8 @@ class Engine:
                 prep = f.result() if f is not None else prepare(r)
                 del futures[r.rid]
                 g.admit(r, prep, now())
+                if r.want_grad:
+                    self._grad.submit(r, prep)
             waiting = still
             ran = False
             for g in self.groups.values():
@@ -380,6 +499,8 @@ class Engine:
             if not ran:
                 if self._inflight:
                     self._inflight[0][0].synchronize()
+                elif self._await_grad:
+                    time.sleep(0.0005)
                 elif nxt < total and realtime and not waiting:
                     time.sleep(max(0.0, min(0.002, reqs[nxt].arrival - now())))
                 elif waiting:
@@ -395,6 +516,7 @@ def run_plain(requests, realtime: bool = True, keep_density: bool = True):
     t0 = time.perf_counter()
     now = lambda: time.perf_counter() - t0
     out = {}
+    targets = {}
     solver = jf.EfficientDriftDoubleKick(interp_kernel=jf.NoInterp(painting=jf.PaintingOptions(target="density")))
     for r in reqs:
         if realtime and r.arrival > now():
@@ -409,8 +531,16 @@ def run_plain(requests, realtime: bool = True, keep_density: bool = True):
         ps = rho.power(kedges=config_kedges(r.mesh, r.box))
         dens = rho.array.cpu() if keep_density else None
         pk = ps.array.cpu().numpy()
-        out[r.rid] = ForwardResult(rid=r.rid, density=dens, k=ps.wavenumber.cpu().numpy(), pk=pk, steps=run.steps,
-                                   arrival=r.arrival, admitted=start, done=now())
+        res = ForwardResult(rid=r.rid, density=dens, k=ps.wavenumber.cpu().numpy(), pk=pk, steps=run.steps,
+                            arrival=r.arrival, admitted=start)
+        if r.want_grad:
+            key = (r.mesh, r.box)
+            if key not in targets:
+                targets[key] = target_spectrum(*key)
+            loss, gw, gom, gs8 = gradient_request(r, prepare(r), targets[key])
+            res.loss, res.grad_noise, res.grad_omega_c, res.grad_sigma8 = float(loss), gw.cpu(), float(gom), float(gs8)
+        res.done = now()
+        out[r.rid] = res
     return out
 
 
@@ -444,4 +574,5 @@ def summarize(results: dict, requests) -> dict:
     end = max(res.done for res in results.values())
     return {"requests": len(requests), "p50_ms": round(float(np.percentile(lat, 50)), 2),
             "p99_ms": round(float(np.percentile(lat, 99)), 2), "makespan_s": round(end - start, 3),
+            "requests_per_s": round(len(requests) / (end - start), 1),
             "mpart_steps_per_s": round(work / (end - start) / 1e6, 1)}

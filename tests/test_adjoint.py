@@ -272,3 +272,37 @@ def test_differentiation_config_128_matches_gpu_fd():
     assert _rel(g_w, fd_w) < 1e-2
     assert _rel(float(om.grad), fd_oc) < 1e-2
     assert _rel(float(sg.grad), fd_s8) < 1e-2
+
+
+def test_public_api_gradient_equals_forward_model():
+    """interpolate_initial_conditions -> lpt -> nbody(ReversibleDoubleKickDrift) -> power
+    through the public API with a noise field that requires grad gives the same gradient
+    as forward_model_pk."""
+    import jfli_b200 as jf
+    from jfli_b200.pm import adjoint as adj
+
+    n, box, t0, dt0 = 32, 128.0, 0.1, 0.225
+    ke = _kedges(n, box)
+    rng = np.random.default_rng(13)
+    w0 = _dev(rng.standard_normal((n, n, n)))
+    with torch.no_grad():
+        pk_t = adj.forward_model_pk(_dev(rng.standard_normal((n, n, n))), torch.tensor(0.2607),
+                                    torch.tensor(0.8102), box=(box,) * 3, kedges=ke, t0=t0, dt0=dt0)
+    cosmo = jf.Planck18()
+    noise = w0.clone().requires_grad_(True)
+    ic = jf.interpolate_initial_conditions(noise, (n,) * 3, (box,) * 3, cosmo=cosmo)
+    dx, p = jf.lpt(cosmo, ic, ts=t0, order=2)
+    solver = jf.ReversibleDoubleKickDrift(interp_kernel=jf.NoInterp(painting=jf.PaintingOptions(target="density")))
+    rho = jf.nbody(cosmo, dx, p, t0=t0, t1=1.0, dt0=dt0, solver=solver)
+    _, pk = jf.power(rho.array, box_shape=(box,) * 3, kedges=ke)
+    loss = adj.pk_log_loss(pk, pk_t)
+    loss.backward()
+
+    w2 = w0.clone().requires_grad_(True)
+    loss2 = adj.pk_log_loss(adj.forward_model_pk(w2, torch.tensor(0.2607), torch.tensor(0.8102), box=(box,) * 3,
+                                                 kedges=ke, t0=t0, dt0=dt0), pk_t)
+    loss2.backward()
+    assert abs(float(loss) - float(loss2)) <= 1e-6 * abs(float(loss2))
+    err = float(torch.linalg.norm(noise.grad - w2.grad) / torch.linalg.norm(w2.grad))
+    print(f"public API vs forward_model_pk gradient rel L2 {err:.2e}")
+    assert err < 1e-5
