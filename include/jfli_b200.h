@@ -27,6 +27,8 @@
  *   jfli_lpt               <- pm/lpt.py:119 (jaxpm lpt, order 1 and 2)
  *   jfli_power_spectrum    <- _src/power/_compute.py:23-119 (_initialize_pk + _power)
  *   jfli_healpix_paint     <- _src/fields/_painting.py:249-348 (jaxpm paint_particles_spherical)
+ *   jfli_lightcone_drift   <- pm/interp.py:110-121 (_drift_to_time) as used by DriftInterp.paint
+ *                             (pm/interp.py:254-318)
  * Adjoints (the reverse-mode derivatives jax.grad takes through the same code, and the
  * backward loop of the reversible adjoint, pm/integrate.py:147-535):
  *   jfli_adjoint_unkick_paint, jfli_poisson_divergence, jfli_adjoint_position
@@ -157,6 +159,16 @@ int jfli_power_spectrum(void* stream, const float* mesh, const float* kedges, in
 int jfli_healpix_paint(void* stream, const float* disp, int absolute, const float* weights, float weight, float lx,
                        float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside, int scheme,
                        float* map, int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* Positions (Mpc/h) of the particles drifted to their light-cone crossing:
+ *   x = (grid index + disp) / N * L;  a_t = interp(|x - observer|; chi, a_chi);
+ *   x += v * (interp(a_t; ga, g) - gp_t) / interp(sqrt(t a_t); da, dgfa)
+ * with jax_cosmo's linear interpolation (end extrapolation) on ascending tables;
+ * gp_t = Gp(t). out has the particle layout. */
+int jfli_lightcone_drift(void* stream, const float* disp, const float* vel, float* out, float lx, float ly, float lz,
+                         float ox, float oy, float oz, float t, float gp_t, const float* chi, const float* a_chi,
+                         int n_chi, const float* ga, const float* g, int n_g, const float* da, const float* dgfa,
+                         int n_d, int nx, int ny, int nz, int batch, char* err, size_t errlen);
 
 /* ---- adjoints ------------------------------------------------------------------
  * Reverse sweep of one reversible KKD step  v' = v + kick F(x);  x' = x + drift v'

@@ -90,6 +90,11 @@ _SIGNATURES = {
         c_int,
         [c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_void_p, *_DIMS, *_ERR],
     ),
+    "jfli_lightcone_drift": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float, c_float,
+         c_float, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, *_DIMS, *_ERR],
+    ),
     "jfli_adjoint_partials_count": (c_size_t, _DIMS),
     "jfli_adjoint_unkick_paint": (
         c_int,

@@ -446,6 +446,30 @@ int jfli_power_spectrum_noalloc(void* stream, const float* mesh, const float* ke
   return cuda_status(e, err, errlen, "jfli_power_spectrum_noalloc");
 }
 
+int jfli_lightcone_drift(void* stream, const float* disp, const float* vel, float* out, float lx, float ly, float lz,
+                         float ox, float oy, float oz, float t, float gp_t, const float* chi, const float* a_chi,
+                         int n_chi, const float* ga, const float* g, int n_g, const float* da, const float* dgfa,
+                         int n_d, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(vel);
+  CHECK_PTR(out);
+  CHECK_PTR(chi);
+  CHECK_PTR(a_chi);
+  CHECK_PTR(ga);
+  CHECK_PTR(g);
+  CHECK_PTR(da);
+  CHECK_PTR(dgfa);
+  if (n_chi < 2 || n_g < 2 || n_d < 2) return fail(err, errlen, JFLI_EINVAL, "tables need at least 2 entries");
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  if (!(t > 0)) return fail(err, errlen, JFLI_EINVAL, "scale factor must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  const float box[3] = {lx, ly, lz}, obs[3] = {ox, oy, oz};
+  return cuda_status(jfli::lightcone_drift(disp, vel, out, box, obs, t, gp_t, chi, a_chi, n_chi, ga, g, n_g, da, dgfa,
+                                           n_d, d, (cudaStream_t)stream),
+                     err, errlen, "jfli_lightcone_drift");
+}
+
 // ---- adjoints --------------------------------------------------------------------
 size_t jfli_adjoint_partials_count(int nx, int ny, int nz, int batch) {
   return jfli::adjoint_partials_count(MeshDims{nx, ny, nz, batch});

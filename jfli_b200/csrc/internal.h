@@ -65,6 +65,12 @@ cudaError_t axpy_particles(float* y, const float* x, float a, const MeshDims& d,
 cudaError_t lpt2_source_adjoint(const float* pot, const float* sbar, float* q, float* out, int accumulate,
                                 const MeshDims& d, cudaStream_t s);
 
+// ---- lightcone.cu ----
+cudaError_t lightcone_drift(const float* disp, const float* vel, float* out, const float* box, const float* observer,
+                            float t, float gp_t, const float* chi, const float* a_chi, int n_chi, const float* ga,
+                            const float* gtab, int n_g, const float* da, const float* dgfa, int n_d, const MeshDims& d,
+                            cudaStream_t s);
+
 // ---- adjoint.cu ----
 size_t adjoint_partials_count(const MeshDims& d);
 cudaError_t adjoint_unkick_paint(const float* disp, float* vel, const float* lam_x, float* lam_v, const float* force,

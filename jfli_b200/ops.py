@@ -255,6 +255,47 @@ def healpix_paint(pos: torch.Tensor, nside: int, box_size, observer_mpc, rmin: f
     return out
 
 
+def drift_tables(cosmo, n_dense: int = 4096):
+    """Device FP32 copies of the FP64 host tables the light-cone drift interpolates:
+    (chi ascending, a at chi), (growth a, D1), (dense a, dGfa)."""
+    from . import cosmology as cj
+
+    dt = cj.distance_table(cosmo)
+    gt = cj.growth_table(cosmo)
+    da = np.logspace(-3.0, 0.0, n_dense)
+    tabs = (dt.chi[::-1], dt.a[::-1], gt.a, gt.g, da, cj.dGfa(cosmo, da))
+    return tuple(torch.as_tensor(np.ascontiguousarray(t, dtype=np.float32), device="cuda") for t in tabs)
+
+
+def lightcone_drift_array(disp: torch.Tensor, vel: torch.Tensor, t: float, cosmo, box_size, observer_mpc,
+                          tables=None) -> torch.Tensor:
+    """Drifted positions in Mpc/h of particles given as relative displacements."""
+    from . import cosmology as cj
+
+    _check(disp, "disp")
+    _check(vel, "vel")
+    (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
+    chi, a_chi, ga, g, da, dg = drift_tables(cosmo) if tables is None else tables
+    out = torch.empty_like(disp)
+    lx, ly, lz = (float(v) for v in box_size)
+    ox, oy, oz = (float(v) for v in observer_mpc)
+    gp_t = float(cj.Gp(cosmo, float(t)))
+    call("jfli_lightcone_drift", stream_ptr(), ptr(disp), ptr(vel), ptr(out), lx, ly, lz, ox, oy, oz, float(t), gp_t,
+         ptr(chi), ptr(a_chi), int(chi.numel()), ptr(ga), ptr(g), int(ga.numel()), ptr(da), ptr(dg), int(da.numel()),
+         nx, ny, nz, batch)
+    return out
+
+
+def lightcone_drift(dx, p, t: float, cosmo):
+    """ParticleField (MPC_H) of dx drifted to the light cone with the momenta p."""
+    from .fields import PositionUnit
+
+    rel = dx if dx.unit == PositionUnit.GRID_RELATIVE else dx.to(PositionUnit.GRID_RELATIVE)
+    arr = lightcone_drift_array(rel.array.contiguous(), p.array.contiguous(), t, cosmo, dx.box_size,
+                                dx.observer_position_mpc)
+    return dx.replace(array=arr, unit=PositionUnit.MPC_H)
+
+
 # ------------------------------------------------------------------------- adjoints
 def adjoint_unkick_paint(disp: torch.Tensor, vel: torch.Tensor, lam_x: torch.Tensor, lam_v: torch.Tensor,
                          force: torch.Tensor, kick: float, drift: float, ubar: torch.Tensor | None = None):

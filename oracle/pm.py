@@ -277,3 +277,19 @@ def kkd_run(dx, p, steps, dtype=np.float64, snapshot_after=None):
         if snapshot_after is not None and n in snapshot_after:
             snaps.append(cic_paint(x))
     return x, v, snaps
+
+
+# ------------------------------------------------------------------------ light cone
+def lightcone_drift(disp, vel, box, observer, t, a_of_chi, Gp, dGfa):
+    """Particles drifted to their light-cone crossing, in Mpc/h (reference
+    pm/interp.py:110-121 and 284-297): x = (grid + disp) / N * L, a_t = a_of_chi(|x - o|),
+    x += v (Gp(a_t) - Gp(t)) / dGfa(sqrt(t a_t)); the momentum array is added as stored.
+    The cosmology functions are passed in (FP64)."""
+    shape = disp.shape[:3]
+    n = np.asarray(shape, np.float64)
+    L = np.asarray(box, np.float64)
+    x = (grid(shape) + disp.astype(np.float64)) / n * L
+    r = np.linalg.norm(x - np.asarray(observer, np.float64), axis=-1)
+    at = a_of_chi(r)
+    drift = (Gp(at) - Gp(t)) / dGfa(np.sqrt(t * at))
+    return x + drift[..., None] * vel.astype(np.float64)
