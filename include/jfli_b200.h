@@ -29,6 +29,7 @@
  *   jfli_healpix_paint     <- _src/fields/_painting.py:249-348 (jaxpm paint_particles_spherical)
  *   jfli_lightcone_drift   <- pm/interp.py:110-121 (_drift_to_time) as used by DriftInterp.paint
  *                             (pm/interp.py:254-318)
+ *   jfli_born              <- _src/lensing/_born.py:29-130 (_born_core_impl, _born_spherical)
  * Adjoints (the reverse-mode derivatives jax.grad takes through the same code, and the
  * backward loop of the reversible adjoint, pm/integrate.py:147-535):
  *   jfli_adjoint_unkick_paint, jfli_poisson_divergence, jfli_adjoint_position
@@ -169,6 +170,15 @@ int jfli_lightcone_drift(void* stream, const float* disp, const float* vel, floa
                          float ox, float oy, float oz, float t, float gp_t, const float* chi, const float* a_chi,
                          int n_chi, const float* ga, const float* g, int n_g, const float* da, const float* dgfa,
                          int n_d, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* Born convergence of nplanes HEALPix shell maps [nplanes][npix]:
+ *   out[k][pix] = sum_p weights[k][p] (maps[p][pix] / mean_p - 1),  k < nsrc,
+ * mean_p the pixel mean of map p (FP64 sum; 0 -> FP32 eps). The weights carry the lensing
+ * efficiency, the plane factor and any n(z) quadrature. nplanes <= 256, nsrc <= 32.
+ * Workspace: jfli_born_workspace_bytes. */
+size_t jfli_born_workspace_bytes(int nplanes, long long npix);
+int jfli_born(void* stream, const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
+              float* out, void* workspace, size_t workspace_bytes, char* err, size_t errlen);
 
 /* ---- adjoints ------------------------------------------------------------------
  * Reverse sweep of one reversible KKD step  v' = v + kick F(x);  x' = x + drift v'

@@ -22,6 +22,7 @@ from .fields import (
     uniform_particles,
 )
 from .initial import gaussian_initial_conditions, interpolate_initial_conditions, white_noise
+from .lensing import RedshiftDistribution, born, smail_nz, tophat_nz
 from .pm import (
     AbstractNBodySolver,
     DriftInterp,

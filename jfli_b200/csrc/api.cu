@@ -470,6 +470,30 @@ int jfli_lightcone_drift(void* stream, const float* disp, const float* vel, floa
                      err, errlen, "jfli_lightcone_drift");
 }
 
+size_t jfli_born_workspace_bytes(int nplanes, long long npix) {
+  if (nplanes <= 0 || npix <= 0) return 0;
+  return align256(sizeof(double) * (size_t)nplanes * jfli::born_ctas(npix)) + align256(sizeof(float) * nplanes);
+}
+
+int jfli_born(void* stream, const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
+              float* out, void* workspace, size_t workspace_bytes, char* err, size_t errlen) {
+  CHECK_PTR(maps);
+  CHECK_PTR(weights);
+  CHECK_PTR(out);
+  CHECK_PTR(workspace);
+  if (nplanes < 1 || nplanes > 256) return fail(err, errlen, JFLI_EINVAL, "nplanes %d outside [1, 256]", nplanes);
+  if (nsrc < 1 || nsrc > 32) return fail(err, errlen, JFLI_EINVAL, "nsrc %d outside [1, 32]", nsrc);
+  if (npix < 1) return fail(err, errlen, JFLI_EINVAL, "npix must be positive");
+  const size_t need = jfli_born_workspace_bytes(nplanes, npix);
+  if (workspace_bytes < need)
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  double* partials = (double*)workspace;
+  float* mean = (float*)((char*)workspace + align256(sizeof(double) * (size_t)nplanes * jfli::born_ctas(npix)));
+  return cuda_status(
+      jfli::born_convergence(maps, nplanes, npix, weights, nsrc, out, partials, mean, (cudaStream_t)stream), err,
+      errlen, "jfli_born");
+}
+
 // ---- adjoints --------------------------------------------------------------------
 size_t jfli_adjoint_partials_count(int nx, int ny, int nz, int batch) {
   return jfli::adjoint_partials_count(MeshDims{nx, ny, nz, batch});

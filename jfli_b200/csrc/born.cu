@@ -1,0 +1,95 @@
+// Born convergence of spherical shell maps (reference _src/lensing/_born.py:29-130):
+//   delta_p(pix) = map_p(pix) / mean_p - 1                     (mean 0 -> FP32 eps)
+//   kappa_k(pix) = sum_p W[k][p] delta_p(pix)
+// W folds the lensing efficiency clip(1 - r_p / chi_s, 0, 1000), the plane factor
+// 3/2 Omega_m (H0/c)^2 dr r_p / a_p and, for n(z) sources, the Simpson weights of the
+// source integral (computed on the host in FP64). The per-plane means are FP64 sums over
+// the pixels, per-CTA partials reduced in a fixed order.
+#include "cic.cuh"
+#include "common.cuh"
+#include "internal.h"
+
+namespace jfli {
+
+constexpr int kBornThreads = 256;
+
+__global__ void __launch_bounds__(kBornThreads) k_plane_partials(const float* __restrict__ maps, long long npix,
+                                                                double* __restrict__ partials) {
+  const long long p = blockIdx.y;
+  const float* m = maps + p * npix;
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += (long long)gridDim.x * blockDim.x)
+    acc += (double)m[i];
+  __shared__ double sh[kBornThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kBornThreads / 32; ++w) s += sh[w];
+    partials[p * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// One thread per plane: mean = (sum of the partials in CTA order) / npix.
+__global__ void k_plane_means(const double* __restrict__ partials, int nctas, int nplanes, long long npix,
+                              float* __restrict__ mean) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nplanes) return;
+  double s = 0.0;
+  for (int c = 0; c < nctas; ++c) s += partials[(long long)p * nctas + c];
+  const float m = (float)(s / (double)npix);
+  mean[p] = (m == 0.f) ? 1.1920929e-07f : m;  // FP32 eps, as the reference's safe mean
+}
+
+__global__ void k_born_combine(const float* __restrict__ maps, int nplanes, long long npix,
+                               const float* __restrict__ mean, const float* __restrict__ w, int nsrc,
+                               float* __restrict__ out) {
+  extern __shared__ float sm[];  // mean[nplanes], w[nsrc][nplanes]
+  for (int i = threadIdx.x; i < nplanes; i += blockDim.x) sm[i] = mean[i];
+  for (int i = threadIdx.x; i < nsrc * nplanes; i += blockDim.x) sm[nplanes + i] = w[i];
+  __syncthreads();
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += (long long)gridDim.x * blockDim.x) {
+    float acc[8];
+    for (int k0 = 0; k0 < nsrc; k0 += 8) {
+      const int kn = (nsrc - k0) < 8 ? (nsrc - k0) : 8;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[k] = 0.f;
+      for (int p = 0; p < nplanes; ++p) {
+        const float d = maps[(long long)p * npix + i] / sm[p] - 1.0f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (k < kn) acc[k] += sm[nplanes + (k0 + k) * nplanes + p] * d;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (k < kn) out[(long long)(k0 + k) * npix + i] = acc[k];
+    }
+  }
+}
+
+int born_ctas(long long npix) {
+  long long b = (npix + kBornThreads - 1) / kBornThreads;
+  const long long cap = (long long)sm_count() * 4;
+  return (int)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+cudaError_t born_convergence(const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
+                             float* out, double* partials, float* mean, cudaStream_t s) {
+  const int nctas = born_ctas(npix);
+  k_plane_partials<<<dim3(nctas, nplanes), kBornThreads, 0, s>>>(maps, npix, partials);
+  note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_plane_means<<<(nplanes + 127) / 128, 128, 0, s>>>(partials, nctas, nplanes, npix, mean);
+  note_launch();
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t smem = sizeof(float) * (size_t)nplanes * (1 + nsrc);
+  k_born_combine<<<born_ctas(npix), kBornThreads, smem, s>>>(maps, nplanes, npix, mean, weights, nsrc, out);
+  note_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace jfli

@@ -71,6 +71,11 @@ cudaError_t lightcone_drift(const float* disp, const float* vel, float* out, con
                             const float* gtab, int n_g, const float* da, const float* dgfa, int n_d, const MeshDims& d,
                             cudaStream_t s);
 
+// ---- born.cu ----
+int born_ctas(long long npix);
+cudaError_t born_convergence(const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
+                             float* out, double* partials, float* mean, cudaStream_t s);
+
 // ---- adjoint.cu ----
 size_t adjoint_partials_count(const MeshDims& d);
 cudaError_t adjoint_unkick_paint(const float* disp, float* vel, const float* lam_x, float* lam_v, const float* force,

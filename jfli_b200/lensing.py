@@ -1,0 +1,144 @@
+"""Born convergence of a spherical light cone (reference lensing/born.py:14-89,
+_src/lensing/_born.py:16-130, _src/lensing/_metadata.py:17-43).
+
+The host builds, in FP64, the (sources x planes) weight matrix of the Born sum:
+  W[k][p] = 3/2 Omega_m (H0/c)^2 * dr * r_p / a_p * sum_z w_z n_k(z) clip(1 - r_p/chi(z), 0, 1000)
+for redshift distributions (Simpson weights w_z on n_integrate + 1 points from min_z to
+max_z, as the reference's _simps_weights), or with n_k(z) w_z replaced by a single source
+redshift z_k. The GPU kernel (`jfli_born`) then forms kappa_k = sum_p W[k][p] delta_p
+with delta_p = map_p / mean(map_p) - 1, reading every shell map once.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+import torch
+
+from . import cosmology as cj
+from ._lib import call, ptr, query, stream_ptr
+from .fields import FieldStatus, SphericalDensity
+
+H0_OVER_C = 100.0 / 299792.458  # h/Mpc (jax_cosmo.constants: H0 = 100 km/s/(Mpc/h), c in km/s)
+
+
+def simpson_weights(a: float, b: float, n: int) -> np.ndarray:
+    """Composite Simpson weights dx/3 [1, 4, 2, ..., 4, 1] on n subintervals."""
+    w = np.ones(n + 1)
+    w[1:-1:2] = 4.0
+    w[2:-2:2] = 2.0
+    return w * ((b - a) / n / 3.0)
+
+
+@dataclasses.dataclass(frozen=True)
+class RedshiftDistribution:
+    """n(z) normalised on [0, zmax] with Simpson's rule on 256 intervals, like
+    jax_cosmo.redshift.redshift_distribution (pz_fn(z, *params) / norm)."""
+
+    pz_fn: object
+    params: tuple = ()
+    zmax: float = 10.0
+
+    @property
+    def norm(self) -> float:
+        z = np.linspace(0.0, self.zmax, 257)
+        return float(np.sum(simpson_weights(0.0, self.zmax, 256) * self.pz_fn(z, *self.params)))
+
+    def __call__(self, z):
+        z = np.asarray(z, dtype=np.float64)
+        return self.pz_fn(z, *self.params) / self.norm
+
+
+def _tophat(z, zmin, zmax):
+    return np.where((z >= zmin) & (z <= zmax), 1.0, 0.0)
+
+
+def tophat_nz(zmin: float, zmax: float) -> RedshiftDistribution:
+    return RedshiftDistribution(_tophat, (float(zmin), float(zmax)), zmax=float(zmax))
+
+
+def _smail(z, a, b, z0):
+    return z**a * np.exp(-((z / z0) ** b))
+
+
+def smail_nz(a: float, b: float, z0: float, zmax: float = 10.0) -> RedshiftDistribution:
+    return RedshiftDistribution(_smail, (float(a), float(b), float(z0)), zmax=float(zmax))
+
+
+def _sources(nz_shear):
+    entries = list(nz_shear) if isinstance(nz_shear, (list, tuple)) else [nz_shear]
+    if not entries:
+        raise ValueError("nz_shear must contain at least one entry")
+    if callable(entries[0]):
+        if not all(callable(e) for e in entries):
+            raise ValueError("Cannot mix redshift distributions with scalar sources")
+        return "distribution", entries
+    z = np.atleast_1d(np.asarray(entries, dtype=np.float64).squeeze())
+    if z.ndim != 1:
+        raise ValueError("Scalar redshift sources must be 1D array-like")
+    return "redshift", z
+
+
+def born_weights(cosmo, scale_factors, max_radius: float, nz_shear, min_z=0.01, max_z=1.5, n_integrate=32):
+    """(W (K, P) FP64, z_eff (K,)) of the Born sum for the planes at `scale_factors`."""
+    a = np.atleast_1d(np.asarray(scale_factors, dtype=np.float64))
+    r = cj.radial_comoving_distance(cosmo, a)
+    dr = max_radius / a.size
+    base = 1.5 * cosmo.Omega_m * H0_OVER_C**2 * dr * r / a
+    kind, src = _sources(nz_shear)
+
+    def efficiency(z):
+        chi_s = cj.radial_comoving_distance(cosmo, 1.0 / (1.0 + np.asarray(z, np.float64)))
+        return np.clip(1.0 - r[None, :] / np.atleast_1d(chi_s)[:, None], 0.0, 1000.0)  # (nz, P)
+
+    if kind == "distribution":
+        zg = np.linspace(min_z, max_z, n_integrate + 1)
+        sw = simpson_weights(min_z, max_z, n_integrate)
+        eff = efficiency(zg)
+        nzw = np.stack([np.asarray(nz(zg), np.float64) for nz in src])  # (K, nz)
+        W = (nzw * sw[None, :]) @ eff * base[None, :]
+        z_eff = np.array([np.sum(sw * zg * nz(zg)) / np.sum(sw * nz(zg)) for nz in src])
+    else:
+        W = efficiency(src) * base[None, :]
+        z_eff = src
+    return W, z_eff
+
+
+def born_maps(maps: torch.Tensor, weights: np.ndarray) -> torch.Tensor:
+    """kappa (K, npix) = W @ (maps / mean - 1) on the GPU."""
+    if maps.dtype != torch.float32 or not maps.is_cuda:
+        raise TypeError("maps must be a float32 CUDA tensor")
+    maps = maps.contiguous()
+    if maps.ndim == 1:
+        maps = maps[None]
+    nplanes, npix = int(maps.shape[0]), int(maps.shape[1])
+    w = torch.as_tensor(np.ascontiguousarray(weights, dtype=np.float32), device=maps.device)
+    if tuple(w.shape) != (w.shape[0], nplanes):
+        raise ValueError("weights must be (sources, planes)")
+    out = torch.empty(w.shape[0], npix, dtype=torch.float32, device=maps.device)
+    nb = int(query("jfli_born_workspace_bytes", nplanes, npix))
+    from .ops import workspace
+
+    ws = workspace(nb, "born", maps.device)
+    call("jfli_born", stream_ptr(), ptr(maps), nplanes, npix, ptr(w), int(w.shape[0]), ptr(out), ptr(ws), ws.numel())
+    return out
+
+
+def born(cosmo, lightcone: SphericalDensity, nz_shear, min_z=0.01, max_z=1.5, n_integrate=32) -> SphericalDensity:
+    """Born convergence maps (K, npix) of a spherical light cone (status LIGHTCONE)."""
+    if nz_shear is None:
+        raise ValueError("nz_shear must be provided for lensing")
+    if lightcone.status != FieldStatus.LIGHTCONE:
+        raise ValueError(f"Expected lightcone with status=LIGHTCONE, got {lightcone.status}")
+    if not isinstance(lightcone, SphericalDensity):
+        raise NotImplementedError("flat-sky Born is not on the B200 path")
+    if lightcone.array.ndim != 2:
+        raise ValueError(f"Lightcone array must be 2D (spherical), got {lightcone.array.ndim}D")
+    W, z_eff = born_weights(cosmo, lightcone.scale_factors, lightcone.max_comoving_radius, nz_shear, min_z, max_z,
+                            n_integrate)
+    kappa = born_maps(lightcone.array, W)
+    a_src = 1.0 / (1.0 + z_eff)
+    return lightcone.replace(array=kappa, status=FieldStatus.KAPPA, z_sources=z_eff, scale_factors=a_src,
+                             comoving_centers=cj.radial_comoving_distance(cosmo, a_src),
+                             density_width=np.zeros_like(z_eff))

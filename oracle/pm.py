@@ -239,8 +239,25 @@ def clip_times(t0, ts, dt0, dtype=np.float32):
     return out
 
 
-def kdk_run(dx, p, coeffs, dtype=np.float64, snapshot_after=None):
+def pgd_correction(disp, alpha, kl, ks, dtype=np.float64):
+    """PGD position correction (reference pm/correction.py:157-202): paint, filter the
+    potential by exp(-kl^2/k^2) exp(-k^4/ks^4) (k in rad/cell, k = 0 -> 0), read out the
+    FD-gradient force and move x by alpha times it."""
+    disp = disp.astype(dtype)
+    kvec = fftk(disp.shape[:3], dtype)
+    kk = sum(k**2 for k in kvec)
+    safe = np.where(kk == 0, 1, kk)
+    rng = np.where(kk == 0, 0, np.exp(-(kl**2) / safe) * np.exp(-(kk**2) / ks**4))
+    pot_k = fft3(cic_paint(disp)) * invlaplace(kvec) * rng
+    f = np.stack([cic_read(ifft3(-gradient_kernel(kvec, i) * pot_k).real.astype(dtype), disp) for i in range(3)],
+                 axis=-1)
+    return disp + dtype(alpha) * f
+
+
+def kdk_run(dx, p, coeffs, dtype=np.float64, snapshot_after=None, pgd=None):
     """FastPM KDK loop (EfficientDriftDoubleKick): coeffs = dict(init_kick, steps=[(kick, drift)]).
+    pgd = (alpha, kl, ks) applies the PGD correction after each drift (reference
+    pm/solvers.py:165-178).
 
     Returns (x, v, snapshots) with snapshots = densities painted after the listed steps."""
     x = dx.astype(dtype).copy()
@@ -249,6 +266,8 @@ def kdk_run(dx, p, coeffs, dtype=np.float64, snapshot_after=None):
     snaps = []
     for n, (kick, drift) in enumerate(coeffs["steps"]):
         x += v * dtype(drift)
+        if pgd is not None:
+            x = pgd_correction(x, *pgd, dtype=dtype)
         v += pm_forces(x, dtype) * dtype(kick)
         if snapshot_after is not None and n in snapshot_after:
             snaps.append(cic_paint(x))

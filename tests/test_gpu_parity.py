@@ -376,3 +376,58 @@ def test_errors_surface_as_exceptions():
 
     with pytest.raises(JfliError):
         ops.rfft3d(torch.zeros(10, 10, 10, device="cuda"))  # 5 is not a supported radix
+
+
+# ------------------------------------------------------------------------------------ PGD
+def test_pgd_correction_matches_oracle():
+    """PGDKernel.apply (reference pm/correction.py:157-202) on one particle state."""
+    from jfli_b200.fields import ParticleField, PositionUnit
+
+    n = 32
+    disp = lpt_disp(n, 2.0, seed=11).astype(np.float32)
+    pos = ParticleField(array=dev(disp), mesh_size=(n, n, n), box_size=(128.0,) * 3, unit=PositionUnit.GRID_RELATIVE)
+    for alpha, kl, ks in ((0.3, 0.3, 1.0), (0.3, 1.5 * 128.0 / n / 100.0, 8.0 * 128.0 / n)):
+        out, _ = jf.PGDKernel(alpha=alpha, kl=kl, ks=ks).apply(0.5, pos, pos, 0.0)
+        ref = opm.pgd_correction(disp, alpha, kl, ks)
+        moved = rel_l2(ref, disp.astype(np.float64))
+        err = rel_l2(host(out.array) - disp, ref - disp)
+        print(f"alpha={alpha} kl={kl:.3g} ks={ks:.3g}: correction rel L2 {err:.2e} (|dx|/|x| = {moved:.2e})")
+        assert moved > 1e-6
+        assert err < 1e-5
+
+
+def test_nbody_pgd_matches_oracle(cosmo):
+    """64^3, L=256, 1LPT, EfficientDriftDoubleKick 10 steps with the PGD correction after
+    every drift (reference pm/solvers.py:165-178)."""
+    from jfli_b200 import cosmology as cj
+    from jfli_b200.pm.integrate import time_events
+    from jfli_b200.pm.lpt import lpt_coefficients
+    from jfli_b200.pm.solvers import EfficientDriftDoubleKick as EDK
+
+    n, L = 64, 256.0
+    alpha, kl, ks = 0.3, 0.3, 1.0
+    noise, dx, p, dt0 = _config1(cosmo, n, L)
+    solver = jf.EfficientDriftDoubleKick(interp_kernel=jf.NoInterp(painting=jf.PaintingOptions(target="density")),
+                                         pgd_kernel=jf.PGDKernel(alpha=alpha, kl=kl, ks=ks))
+    res = jf.nbody(cosmo, dx, p, t0=0.1, t1=1.0, dt0=dt0, solver=solver)
+    gpu = host(res.array)
+    k, pk = cj.pk_table(cosmo, 128)
+    ric = opm.ic_filter(noise.astype(np.float64), (L, L, L), k, pk)
+    c = lpt_coefficients(cosmo, 0.1)
+    steps = [(e[1], e[2]) for e in time_events(0.1, [1.0], dt0) if e[0] == "step"]
+    coeffs = dict(init_kick=EDK.init_kick(cosmo, 0.1, 0.1 + dt0),
+                  steps=[(EDK.step_coefficients(cosmo, a, b, dt0).kick, EDK.step_coefficients(cosmo, a, b, dt0).drift)
+                         for a, b in steps])
+    rdx, rp = opm.lpt(ric, *c, order=1)
+    _, _, snaps = opm.kdk_run(rdx, rp, coeffs, snapshot_after={len(steps) - 1}, pgd=(alpha, kl, ks))
+    _, _, plain = opm.kdk_run(rdx, rp, coeffs, snapshot_after={len(steps) - 1})
+    err = rel_l2(gpu, snaps[0])
+    effect = rel_l2(plain[0], snaps[0])
+    print(f"PGD run: density rel L2 vs oracle {err:.2e}; PGD changes the density by {effect:.2e}")
+    assert effect > 1e-3
+    assert err < 1e-4
+    kedges = np.geomspace(2 * np.pi / L * (1 - 1e-6), np.pi * n / L, 33)
+    pk_gpu = host(res.power(kedges=kedges).array)
+    _, pk_ref = opm.power(snaps[0], (L, L, L), kedges)
+    ok = pk_ref > 0
+    assert np.abs(pk_gpu[ok] / pk_ref[ok] - 1).max() < 1e-4
