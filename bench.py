@@ -164,7 +164,7 @@ def run_gpu(args, world, rank):
     v = p.array.clone()
     rho = torch.empty(n, n, n, device="cuda")
     pot = torch.empty_like(rho)
-    force = torch.empty(3, n, n, n, device="cuda")
+    force = torch.empty(n, n, n, 4, device="cuda")
     # the 40-step schedule of the 256^3 run: EfficientDriftDoubleKick, dt0 = 0.9/40 from a = 0.1 to a = 1
     from jfli_b200.pm.integrate import time_events
 
@@ -325,7 +325,7 @@ def run_serving(args):
     if args.serve_requests <= 0:
         return None
     reqs = serving.poisson_stream(args.serve_requests, args.serve_rate, seed=0, grad_fraction=0.25)
-    eng = serving.Engine(sizes=(64, 96, 128, 192), hbm_budget_gb=24.0, max_slots=16, keep_density=False)
+    eng = serving.Engine(sizes=(64, 96, 128, 192), hbm_budget_gb=32.0, max_slots=16, keep_density=False)
     warm = serving.poisson_stream(16, 0.0, seed=1, grad_fraction=0.0)
     for r in warm:
         r.rid += 10**6

@@ -105,7 +105,8 @@ size_t jfli_pm_forces_workspace_bytes(int nx, int ny, int nz, int batch);
 int jfli_pm_forces(void* stream, const float* pos, int absolute, float scale, float* forces, void* workspace,
                    size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
 
-/* Force meshes: force[a] = scale * (-D_a pot), SoA [batch][3][nx][ny][nz], D the 4-point
+/* Force meshes: force = scale * (-D pot), AoS float4 [batch][nx][ny][nz][4] =
+ * (Fx, Fy, Fz, 0) (16-byte aligned; one aligned load per CIC corner), D the 4-point
  * finite difference whose Fourier eigenvalue is JaxPM's gradient_kernel. Its CIC readout is
  * the force of jaxpm pm_forces (pm/solvers.py:19-32). */
 int jfli_force_mesh(void* stream, const float* pot, float scale, float* force, int nx, int ny, int nz, int batch,

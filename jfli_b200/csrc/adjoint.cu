@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_unkick_paint(
   vel += b * g.np * 3;
   lam_x += b * g.np * 3;
   lam_v += b * g.np * 3;
-  force += b * g.np * 3;
+  force += b * g.np * 4;
   ubar += b * g.np * 3;
   double sk = 0.0, sd = 0.0;
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
@@ -128,7 +128,8 @@ __global__ void k_div_fd(const float* __restrict__ u, float alpha, const float* 
   }
 }
 
-// lam_x += scale * grad_x R_x[h], h(corner) = rho_bar(corner) + sum_a u_a force_a(corner),
+// lam_x += scale * grad_x R_x[h], h(corner) = rho_bar(corner) + sum_a u_a force_a(corner)
+// (force AoS float4 per cell, as written by the force-mesh kernels),
 // at relative positions disp. Either of rho_bar or (u, force) may be null. The gradient
 // of the trilinear weights is one-sided at cell faces, like the derivative of the
 // floor-based weights.
@@ -139,7 +140,7 @@ __global__ void k_adj_position(const float* __restrict__ disp, const float* __re
   disp += b * g.np * 3;
   lam_x += b * g.np * 3;
   if (u) u += b * g.np * 3;
-  if (force) force += b * g.np * 3;
+  if (force) force += b * g.np * 4;
   if (rho_bar) rho_bar += b * g.np;
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
@@ -162,8 +163,10 @@ __global__ void k_adj_position(const float* __restrict__ disp, const float* __re
         for (int c = 0; c < 2; ++c) {
           const int o = xo[a] + yo[bb] + zo[c];
           float v = rho_bar ? __ldg(rho_bar + o) : 0.f;
-          if (u && force)
-            v += ua[0] * __ldg(force + o) + ua[1] * __ldg(force + g.np + o) + ua[2] * __ldg(force + 2ull * g.np + o);
+          if (u && force) {
+            const float4 f = __ldg(reinterpret_cast<const float4*>(force) + o);
+            v += ua[0] * f.x + ua[1] * f.y + ua[2] * f.z;
+          }
           h[a][bb][c] = v;
         }
     const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};

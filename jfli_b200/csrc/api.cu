@@ -4,6 +4,7 @@
 // JFLI_E* codes with a message in `err`. Nothing throws across this boundary and
 // nothing synchronises the device except where documented.
 #include <atomic>
+#include <cstdint>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -57,6 +58,9 @@ bool dims_ok(int nx, int ny, int nz, int batch) {
 
 #define CHECK_PTR(p)                                                                                        \
   if (!(p)) return fail(err, errlen, JFLI_EINVAL, "null pointer argument '%s'", #p)
+#define CHECK_ALIGN16(p)                                                                                  \
+  if (((uintptr_t)(p)) % 16 != 0)                                                                        \
+  return fail(err, errlen, JFLI_EINVAL, "%s must be 16-byte aligned (AoS float4 force mesh)", #p)
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -214,6 +218,7 @@ int jfli_force_mesh(void* stream, const float* pot, float scale, float* force, i
   CHECK_STENCIL(nx, ny, nz);
   CHECK_PTR(pot);
   CHECK_PTR(force);
+  CHECK_ALIGN16(force);
   const MeshDims d{nx, ny, nz, batch};
   return cuda_status(jfli::force_mesh(pot, force, scale, d, (cudaStream_t)stream), err, errlen, "jfli_force_mesh");
 }
@@ -230,6 +235,7 @@ int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* fo
     return fail(err, errlen, JFLI_EINVAL, "KICK and CORRECT are exclusive");
   if ((flags & (JFLI_STEP_KICK | JFLI_STEP_CORRECT)) && !force)
     return fail(err, errlen, JFLI_EINVAL, "kick requested without a force mesh");
+  if (force) CHECK_ALIGN16(force);
   if ((flags & JFLI_STEP_PAINT) && !rho) return fail(err, errlen, JFLI_EINVAL, "paint requested without a mesh");
   const MeshDims d{nx, ny, nz, batch};
   return cuda_status(jfli::kick_drift_paint(disp, vel, force, kick, drift, flags, weight, rho, d, (cudaStream_t)stream),
@@ -251,6 +257,7 @@ int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift,
   CHECK_PTR(vel);
   CHECK_PTR(rho);
   CHECK_PTR(force);
+  CHECK_ALIGN16(force);
   CHECK_PTR(workspace);
   const MeshDims d{nx, ny, nz, batch};
   const size_t need = jfli_pm_step_workspace_bytes(nx, ny, nz, batch);
@@ -283,6 +290,7 @@ int jfli_pm_step_slots(void* stream, float* disp, float* vel, const float* kicks
   CHECK_PTR(slot_flags);
   CHECK_PTR(rho);
   CHECK_PTR(force);
+  CHECK_ALIGN16(force);
   CHECK_PTR(workspace);
   const MeshDims d{nx, ny, nz, batch};
   const size_t need = jfli_pm_step_workspace_bytes(nx, ny, nz, batch);
@@ -508,6 +516,7 @@ int jfli_adjoint_unkick_paint(void* stream, const float* disp, float* vel, const
   CHECK_PTR(lam_x);
   CHECK_PTR(lam_v);
   CHECK_PTR(force);
+  CHECK_ALIGN16(force);
   CHECK_PTR(ubar);
   CHECK_PTR(partials);
   const MeshDims d{nx, ny, nz, batch};
@@ -552,6 +561,7 @@ int jfli_adjoint_position(void* stream, const float* disp, const float* u, const
   CHECK_PTR(lam_x);
   if ((u == nullptr) != (force == nullptr))
     return fail(err, errlen, JFLI_EINVAL, "u and force must be given together");
+  if (force) CHECK_ALIGN16(force);
   if (rho_bar == nullptr && force == nullptr) return fail(err, errlen, JFLI_EINVAL, "nothing to read out");
   const MeshDims d{nx, ny, nz, batch};
   return cuda_status(jfli::adjoint_position(disp, u, rho_bar, force, scale, lam_x, d, (cudaStream_t)stream), err,

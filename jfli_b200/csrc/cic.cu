@@ -110,7 +110,7 @@ __global__ void k_paint(const float* __restrict__ pos, int absolute, const float
     Cic1 cx, cy, cz;
     cic_setup(pos + 3ull * p, p, absolute, g, cx, cy, cz);
     const float w = weights ? weights[p] * weight : weight;
-    deposit(mesh, g, cx, cy, cz, w);
+    deposit_lane_merged(mesh, g, cx, cy, cz, w);
   }
 }
 
@@ -161,7 +161,7 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
   }
   disp += b * g.np * 3;
   vel += b * g.np * 3;
-  if (force) force += b * g.np * 3;
+  if (force) force += b * g.np * 4;
   if (rho) rho += b * g.np;
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
@@ -193,20 +193,21 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
     }
     if (flags & kStepPaint) {
       const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
-      deposit(rho, g, cx, cy, cz, weight);
+      deposit_lane_merged(rho, g, cx, cy, cz, weight);
     }
   }
 }
 
 // ----------------------------------------------------------------------------------
-// Force mesh: F_a = scale * (-D_a pot) at every cell, SoA [3][nx][ny][nz]. The particle
-// pass then reads 8 CIC corners per component (24 loads) instead of the 56-point FD
-// stencil of the potential; the CIC readout of F equals the stencil readout of pot.
+// Force mesh: F = scale * (-D pot) at every cell, AoS float4 [nx][ny][nz] = (Fx, Fy, Fz, 0).
+// The particle pass then reads one 16-byte value per CIC corner (8 loads) instead of the
+// 56-point FD stencil of the potential; the CIC readout of F equals the stencil readout
+// of pot. The fourth lane is padding that makes every corner a single aligned load.
 // ----------------------------------------------------------------------------------
 __global__ void k_force_mesh(const float* __restrict__ pot, float* __restrict__ F, float scale, PGrid g) {
   const long long b = blockIdx.y;
   pot += b * g.np;
-  F += b * g.np * 3;
+  F += b * g.np * 4;
   const float s = scale / 12.0f;
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
@@ -221,18 +222,16 @@ __global__ void k_force_mesh(const float* __restrict__ pot, float* __restrict__ 
     const float* cx = pot + yo + k;
     const float fx = (8.0f * (__ldg(cx + wrap1(i + 1, g.nx) * g.yz) - __ldg(cx + wrap1(i - 1, g.nx) * g.yz)) -
                       (__ldg(cx + wrap1(i + 2, g.nx) * g.yz) - __ldg(cx + wrap1(i - 2, g.nx) * g.yz)));
-    F[p] = -fx * s;
-    F[g.np + p] = -fy * s;
-    F[2ull * g.np + p] = -fz * s;
+    reinterpret_cast<float4*>(F)[p] = make_float4(-fx * s, -fy * s, -fz * s, 0.f);
   }
 }
 
 // The same stencil for four consecutive z cells per thread (nz % 4 == 0): 11 aligned
-// 16-byte loads and 3 16-byte stores per 4 cells, row offsets and wraps shared.
+// 16-byte loads and 4 16-byte stores per 4 cells, row offsets and wraps shared.
 __global__ void k_force_mesh4(const float* __restrict__ pot, float* __restrict__ F, float scale, PGrid g) {
   const long long b = blockIdx.y;
   pot += b * g.np;
-  F += b * g.np * 3;
+  F += b * g.np * 4;
   const float s = scale / 12.0f;
   const unsigned nq = g.np >> 2;  // groups of 4 cells
   const int nz4 = g.nz >> 2;
@@ -247,9 +246,6 @@ __global__ void k_force_mesh4(const float* __restrict__ pot, float* __restrict__
     const float4 z0 = __ldg(r + (k0 >> 2));
     const float4 zp = __ldg(r + (wrap1(k0 + 4, g.nz) >> 2));
     const float w[12] = {zm.x, zm.y, zm.z, zm.w, z0.x, z0.y, z0.z, z0.w, zp.x, zp.y, zp.z, zp.w};
-    float fz[4];
-#pragma unroll
-    for (int t = 0; t < 4; ++t) fz[t] = -(8.0f * (w[5 + t] - w[3 + t]) - (w[6 + t] - w[2 + t])) * s;
     const float* cx = pot + yo + k0;
     const float4 xp1 = __ldg(reinterpret_cast<const float4*>(cx + wrap1(i + 1, g.nx) * g.yz));
     const float4 xm1 = __ldg(reinterpret_cast<const float4*>(cx + wrap1(i - 1, g.nx) * g.yz));
@@ -260,18 +256,16 @@ __global__ void k_force_mesh4(const float* __restrict__ pot, float* __restrict__
     const float4 ym1 = __ldg(reinterpret_cast<const float4*>(cy + wrap1(j - 1, g.ny) * g.nz));
     const float4 yp2 = __ldg(reinterpret_cast<const float4*>(cy + wrap1(j + 2, g.ny) * g.nz));
     const float4 ym2 = __ldg(reinterpret_cast<const float4*>(cy + wrap1(j - 2, g.ny) * g.nz));
-    const float4 fx = make_float4(-(8.0f * (xp1.x - xm1.x) - (xp2.x - xm2.x)) * s,
-                                  -(8.0f * (xp1.y - xm1.y) - (xp2.y - xm2.y)) * s,
-                                  -(8.0f * (xp1.z - xm1.z) - (xp2.z - xm2.z)) * s,
-                                  -(8.0f * (xp1.w - xm1.w) - (xp2.w - xm2.w)) * s);
-    const float4 fy = make_float4(-(8.0f * (yp1.x - ym1.x) - (yp2.x - ym2.x)) * s,
-                                  -(8.0f * (yp1.y - ym1.y) - (yp2.y - ym2.y)) * s,
-                                  -(8.0f * (yp1.z - ym1.z) - (yp2.z - ym2.z)) * s,
-                                  -(8.0f * (yp1.w - ym1.w) - (yp2.w - ym2.w)) * s);
-    const unsigned c = (unsigned)(xo + yo + k0);
-    reinterpret_cast<float4*>(F + c)[0] = fx;
-    reinterpret_cast<float4*>(F + g.np + c)[0] = fy;
-    reinterpret_cast<float4*>(F + 2ull * g.np + c)[0] = make_float4(fz[0], fz[1], fz[2], fz[3]);
+    const float fx[4] = {xp1.x - xm1.x, xp1.y - xm1.y, xp1.z - xm1.z, xp1.w - xm1.w};
+    const float fx2[4] = {xp2.x - xm2.x, xp2.y - xm2.y, xp2.z - xm2.z, xp2.w - xm2.w};
+    const float fy[4] = {yp1.x - ym1.x, yp1.y - ym1.y, yp1.z - ym1.z, yp1.w - ym1.w};
+    const float fy2[4] = {yp2.x - ym2.x, yp2.y - ym2.y, yp2.z - ym2.z, yp2.w - ym2.w};
+    float4* out = reinterpret_cast<float4*>(F) + (xo + yo + k0);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const float gz = -(8.0f * (w[5 + t] - w[3 + t]) - (w[6 + t] - w[2 + t])) * s;
+      out[t] = make_float4(-(8.0f * fx[t] - fx2[t]) * s, -(8.0f * fy[t] - fy2[t]) * s, gz, 0.f);
+    }
   }
 }
 

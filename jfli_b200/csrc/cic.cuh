@@ -98,6 +98,41 @@ __device__ __forceinline__ void deposit(float* mesh, const PGrid& g, const Cic1&
     }
 }
 
+// CIC deposit for lanes that hold consecutive particles of one z row (the grid-stride
+// particle loops: lane L has particle p, lane L+1 particle p+1). When lane L's upper-z
+// corners are lane L+1's lower-z corners (same x and y cells, next z cell: neighbouring
+// particles that moved together), lane L hands its four upper-z weights to lane L+1 with
+// a shuffle and lane L+1 adds them to its own lower-z deposits, so that pair of cells
+// takes one atomic instead of two. The sums reaching each cell are the same as with
+// deposit(); only the FP32 addition order differs. The active lanes of a warp must be a
+// prefix of it, which holds for the grid-stride loops (the last iteration drops lanes
+// from the top).
+__device__ __forceinline__ void deposit_lane_merged(float* mesh, const PGrid& g, const Cic1& cx, const Cic1& cy,
+                                                    const Cic1& cz, float w) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int xy0 = cx.i0 * g.yz + cy.i0 * g.nz;
+  const int lo = xy0 + cz.i0;  // my lower-z corner at (x0, y0)
+  const int hi = xy0 + cz.i1;  // my upper-z corner at (x0, y0)
+  const int next_lo = __shfl_down_sync(mask, lo, 1);
+  const int prev_hi = __shfl_up_sync(mask, hi, 1);
+  const bool give = lane < 31 && ((mask >> (lane + 1)) & 1u) && next_lo == hi;
+  const bool take = lane > 0 && ((mask >> (lane - 1)) & 1u) && prev_hi == lo;
+  const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz};
+  const float wx[2] = {cx.w0 * w, cx.w1 * w}, wy[2] = {cy.w0, cy.w1};
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const float wab = wx[a] * wy[b];
+      const float up = wab * cz.w1;
+      const float recv = __shfl_up_sync(mask, up, 1);
+      const float low = wab * cz.w0 + (take ? recv : 0.f);
+      atomicAdd(mesh + (xo[a] + yo[b] + cz.i0), low);
+      if (!give) atomicAdd(mesh + (xo[a] + yo[b] + cz.i1), up);
+    }
+}
+
 __device__ __forceinline__ float gather(const float* __restrict__ mesh, const PGrid& g, const Cic1& cx,
                                         const Cic1& cy, const Cic1& cz) {
   const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
@@ -112,13 +147,13 @@ __device__ __forceinline__ float gather(const float* __restrict__ mesh, const PG
   return acc;
 }
 
-// CIC readout of the three force meshes at one particle.
+// CIC readout of the force mesh at one particle. The force mesh is AoS float4
+// [nx][ny][nz] = (Fx, Fy, Fz, 0): one 16-byte load per CIC corner.
 __device__ __forceinline__ void gather_force_mesh(const float* __restrict__ F, const PGrid& g, const Cic1& cx,
                                                   const Cic1& cy, const Cic1& cz, float& fx, float& fy, float& fz) {
+  const float4* F4 = reinterpret_cast<const float4*>(F);
   const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
   const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
-  const float* F1 = F + g.np;
-  const float* F2 = F + 2ull * g.np;
   float ax = 0.f, ay = 0.f, az = 0.f;
 #pragma unroll
   for (int a = 0; a < 2; ++a)
@@ -127,11 +162,11 @@ __device__ __forceinline__ void gather_force_mesh(const float* __restrict__ F, c
       const float wab = wx[a] * wy[b];
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
-        const int o = xo[a] + yo[b] + zo[c];
+        const float4 f = __ldg(F4 + (xo[a] + yo[b] + zo[c]));
         const float w = wab * wz[c];
-        ax += __ldg(F + o) * w;
-        ay += __ldg(F1 + o) * w;
-        az += __ldg(F2 + o) * w;
+        ax += f.x * w;
+        ay += f.y * w;
+        az += f.z * w;
       }
     }
   fx = ax;

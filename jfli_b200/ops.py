@@ -147,11 +147,14 @@ def pm_forces(pos: torch.Tensor, *, absolute: bool = False, scale: float = 1.0) 
 
 
 def force_mesh(pot: torch.Tensor, scale: float = 1.0, out: torch.Tensor | None = None) -> torch.Tensor:
-    """(..., 3, nx, ny, nz) force meshes scale * (-D_a pot), D the 4-point finite difference."""
+    """(..., nx, ny, nz, 4) force mesh scale * (-D pot) as (Fx, Fy, Fz, 0) per cell, D the
+    4-point finite difference."""
     _check(pot, "pot")
     (nx, ny, nz), batch, lead = _mesh_dims(pot, False)
     if out is None:
-        out = torch.empty(*lead, 3, nx, ny, nz, dtype=torch.float32, device=pot.device)
+        out = torch.empty(*lead, nx, ny, nz, 4, dtype=torch.float32, device=pot.device)
+    elif out.numel() != 4 * batch * nx * ny * nz:
+        raise ValueError("out must hold (nx, ny, nz, 4) per mesh")
     call("jfli_force_mesh", stream_ptr(), ptr(pot), float(scale), ptr(out), nx, ny, nz, batch)
     return out
 
@@ -171,8 +174,8 @@ def kick_drift_paint(disp: torch.Tensor, vel: torch.Tensor, force: torch.Tensor 
     (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
     if force is not None:
         _check(force, "force")
-        if force.numel() != 3 * batch * nx * ny * nz:
-            raise ValueError("force must hold 3 meshes per particle grid")
+        if force.numel() != 4 * batch * nx * ny * nz:
+            raise ValueError("force must hold an (nx, ny, nz, 4) force mesh per particle grid")
     call("jfli_kick_drift_paint", stream_ptr(), ptr(disp), ptr(vel), ptr(force), float(kick), float(drift),
          int(flags), float(weight), ptr(rho), nx, ny, nz, batch)
 

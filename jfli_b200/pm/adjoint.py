@@ -206,8 +206,8 @@ def kkd_reverse_adjoint(x: torch.Tensor, v: torch.Tensor, lam_x: torch.Tensor, l
     shape = x.shape[:-1]
     rho = torch.empty(shape, dtype=torch.float32, device=x.device)
     pot = torch.empty_like(rho)
-    force = torch.empty((3,) + tuple(shape), dtype=torch.float32, device=x.device)
-    ubar = torch.empty_like(force)
+    force = torch.empty(tuple(shape) + (4,), dtype=torch.float32, device=x.device)
+    ubar = torch.empty((3,) + tuple(shape), dtype=torch.float32, device=x.device)
     rho_bar = torch.empty_like(rho)
     n = len(kicks)
     sens = torch.zeros(n, 2, dtype=torch.float64, device=x.device)
@@ -233,7 +233,7 @@ class ReversibleNBody(torch.autograd.Function):
         shape = x.shape[:-1]
         rho = torch.empty(shape, dtype=torch.float32, device=x.device)
         pot = torch.empty_like(rho)
-        force = torch.empty((3,) + tuple(shape), dtype=torch.float32, device=x.device)
+        force = torch.empty(tuple(shape) + (4,), dtype=torch.float32, device=x.device)
         kkd_forward(x, v, tables.kicks, tables.drifts, rho, force, pot)
         ctx.tables = tables
         ctx.omega_c = omega_c

@@ -89,7 +89,7 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
     v = p.array.contiguous().clone()
     rho = torch.empty(x.shape[:-1], dtype=torch.float32, device=x.device)
     pot = torch.empty_like(rho)
-    force = torch.empty((3,) + tuple(rho.shape), dtype=torch.float32, device=x.device)
+    force = torch.empty(tuple(rho.shape) + (4,), dtype=torch.float32, device=x.device)
     events = time_events(t0, ts, dt0, dtype)
     n_steps = sum(1 for e in events if e[0] == "step")
     state = NBodyState(interp_state=interp.init(), t_initial=t0)

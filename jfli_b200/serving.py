@@ -235,7 +235,7 @@ class SizeGroup:
         self.x = torch.zeros(capacity, n, n, n, 3, device=dev)
         self.v = torch.zeros_like(self.x)
         self.rho = torch.zeros(capacity, n, n, n, device=dev)
-        self.force = torch.zeros(capacity, 3, n, n, n, device=dev)
+        self.force = torch.zeros(capacity, n, n, n, 4, device=dev)
         self.pot1 = torch.empty(n, n, n, device=dev)
         nb = _lib.query("jfli_pm_step_workspace_bytes", n, n, n, capacity)
         self.ws = torch.empty(nb, dtype=torch.uint8, device=dev)
@@ -253,8 +253,8 @@ class SizeGroup:
 
     @staticmethod
     def bytes_per_slot(n: int) -> int:
-        # x, v (24 B) + density (4) + force (12) + half spectrum and potential (~8 B per cell)
-        return int(48 * n**3 + 8 * n * n * (n // 2 + 1))
+        # x, v (24 B) + density (4) + force mesh (16) + half spectrum and potential (~8 B per cell)
+        return int(52 * n**3 + 8 * n * n * (n // 2 + 1))
 
     def has_room(self) -> bool:
         return len(self.slots) < self.B

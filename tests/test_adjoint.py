@@ -43,7 +43,7 @@ def test_kkd_step_vjp_matches_oracle_fd():
 
     x, v = _dev(x0), _dev(v0)
     rho = torch.empty(n, n, n, device="cuda")
-    force = torch.empty(3, n, n, n, device="cuda")
+    force = torch.empty(n, n, n, 4, device="cuda")
     pot = torch.empty_like(rho)
     adj.kkd_forward(x, v, kicks, drifts, rho, force, pot)
     lam_x, lam_v = _dev(a), _dev(b)
@@ -84,7 +84,7 @@ def test_reverse_recovers_initial_state():
     drifts = np.linspace(0.5, 0.2, 10)
     x, v = x0.clone(), v0.clone()
     rho = torch.empty(n, n, n, device="cuda")
-    force = torch.empty(3, n, n, n, device="cuda")
+    force = torch.empty(n, n, n, 4, device="cuda")
     adj.kkd_forward(x, v, kicks, drifts, rho, force, torch.empty_like(rho))
     moved = float((x - x0).abs().max())
     adj.kkd_reverse_adjoint(x, v, torch.zeros_like(x), torch.zeros_like(v), kicks, drifts)

@@ -112,7 +112,8 @@ def test_force_mesh_matches_stencil(shape):
     for ax in range(3):
         r = lambda s: np.roll(pot, -s, axis=ax)
         ref = -2.0 * (8 * (r(1) - r(-1)) - (r(2) - r(-2))) / 12
-        np.testing.assert_allclose(F[ax], ref, rtol=1e-5, atol=1e-5)
+        np.testing.assert_allclose(F[..., ax], ref, rtol=1e-5, atol=1e-5)
+    assert np.all(F[..., 3] == 0)
 
 
 def test_readout_gradient_absolute_equals_relative():

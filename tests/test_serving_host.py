@@ -49,8 +49,10 @@ def test_prepare_matches_stepwise_coefficients(steps):
 
 
 def test_slot_capacities_respect_budget():
-    caps = serving.slot_capacities((64, 96, 128, 192), 24.0, 16)
+    caps = serving.slot_capacities((64, 96, 128, 192), 32.0, 16)
     assert caps == {64: 16, 96: 16, 128: 16, 192: 16}
+    caps = serving.slot_capacities((64, 96, 128, 192), 24.0, 16)
+    assert caps[64] == 16 and all(c * serving.SizeGroup.bytes_per_slot(n) <= 6e9 for n, c in caps.items())
     small = serving.slot_capacities((64, 96, 128, 192), 2.0, 16)
     assert small[192] < small[128] <= small[96] <= small[64]
     for n, cap in small.items():
