@@ -13,6 +13,8 @@
  *              (PositionUnit.GRID_ABSOLUTE)
  *   spectrum   [batch][nx][ny][nz/2+1] complex64 (interleaved float2)
  * Meshes used with an FFT need nx, ny and nz/2 of the form 2^a 3^b (<= 4096), nz even.
+ * One mesh (one batch entry) holds at most (2^32 - 1) / 3 cells (about 1130^3): particle
+ * offsets are 32-bit. Larger shapes return JFLI_EINVAL.
  *
  * Reference interfaces replaced (paths inside the jax-fli project):
  *   jfli_paint_cic         <- _src/fields/_painting.py:22-86 (_single_paint -> cic_paint_dx / cic_paint)

@@ -36,8 +36,12 @@ int cuda_status(cudaError_t e, char* err, size_t errlen, const char* what) {
   return fail(err, errlen, JFLI_ECUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
+// Particle kernels address a particle's three components with 32-bit unsigned offsets
+// (3 p) and cells with 32-bit signed offsets, so one mesh holds at most (2^32 - 1) / 3
+// cells (about 1130^3); batches are separate meshes.
 bool dims_ok(int nx, int ny, int nz, int batch) {
-  return nx > 0 && ny > 0 && nz > 0 && batch > 0 && batch <= 65535 && (long long)nx * ny * nz < (1LL << 40);
+  return nx > 0 && ny > 0 && nz > 0 && batch > 0 && batch <= 65535 &&
+         (long long)nx * ny * nz <= 1431655765LL;
 }
 
 #define CHECK_DIMS(nx, ny, nz, batch)                                                                       \
