@@ -14,7 +14,7 @@ schedule restarts from the initial conditions inside the timed region.
           -> lpt -> nbody -> power) from pinned host white noise to host density + P(k),
           40 KDK steps per request, copies inside the timed region
   roofline : the fused particle pass (k_kick_drift_paint), algorithmic bytes
-          48 B/particle (read+write position and velocity) + 16 B/cell (three force meshes
+          48 B/particle (read+write position and velocity) + 20 B/cell (float4 force mesh
           read, density written) per launch, over its CUDA-event time, against
           MEASURED_PEAKS.json
   cpu_baseline : the NumPy/SciPy FP32 port of the same step (oracle/pm.py) on this host
@@ -250,7 +250,7 @@ def run_gpu(args, world, rank):
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     kdp_avg_ms = statistics.mean(kdp)
-    alg_bytes = 48.0 * particles + 16.0 * particles  # x, v read+write; 3 force meshes read; density written
+    alg_bytes = 68.0 * particles  # x, v read+write (48 B); float4 force mesh read (16 B); density written (4 B)
     achieved = alg_bytes / (kdp_avg_ms / 1e3) / 1e9
     roof = {"kernel": "k_kick_drift_paint", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": ncu_traffic(n),
