@@ -498,6 +498,12 @@ def run_lightcone(args):
                                           max_z=1.0)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t
+    from jfli_b200 import sht
+
+    t = time.perf_counter()
+    shell = res.shells.array[-1].double().cpu().numpy()
+    cl = sht.anafast(shell / shell.mean() - 1.0, lmax=3000)
+    t_cl = time.perf_counter() - t
     kap = res.kappa.array
     line = {"workload": f"light cone {n}^3, box {BOX:g} Mpc/h, 2LPT, KDK + PGD, 16 shells nside 1024, Born",
             "steps": res.steps, "wall_s": round(wall, 2), "timings_s": {k: round(v, 3) for k, v in res.timings.items()},
@@ -505,6 +511,8 @@ def run_lightcone(args):
             "peak_hbm_gb": round(torch.cuda.max_memory_allocated() / 1e9, 1),
             "kappa_rms": float(kap.double().pow(2).mean().sqrt()), "kappa_finite": bool(torch.isfinite(kap).all()),
             "shell_means": [round(float(v), 6) for v in res.shells.array.double().mean(dim=1)],
+            "cl_farthest_shell": {"lmax": 3000, "seconds": round(t_cl, 2), "finite": bool(np.isfinite(cl).all()),
+                                  "c_ell_100_1000_3000": [float(cl[100]), float(cl[1000]), float(cl[3000])]},
             "clocks": clocks.stop()}
     print(json.dumps(line), flush=True)
 

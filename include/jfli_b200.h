@@ -32,6 +32,8 @@
  *   jfli_lightcone_drift   <- pm/interp.py:110-121 (_drift_to_time) as used by DriftInterp.paint
  *                             (pm/interp.py:254-318)
  *   jfli_born              <- _src/lensing/_born.py:29-130 (_born_core_impl, _born_spherical)
+ *   jfli_sht_map2alm / jfli_sht_alm2map <- the Legendre stages of healpy.anafast behind
+ *                             SphericalDensity.angular_cl (_src/power/_compute.py:175-191)
  * Adjoints (the reverse-mode derivatives jax.grad takes through the same code, and the
  * backward loop of the reversible adjoint, pm/integrate.py:147-535):
  *   jfli_adjoint_unkick_paint, jfli_poisson_divergence, jfli_adjoint_position
@@ -182,6 +184,20 @@ int jfli_lightcone_drift(void* stream, const float* disp, const float* vel, floa
 size_t jfli_born_workspace_bytes(int nplanes, long long npix);
 int jfli_born(void* stream, const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
               float* out, void* workspace, size_t workspace_bytes, char* err, size_t errlen);
+
+/* Legendre stages of the spherical harmonic transform of a HEALPix RING map (FP64).
+ * F and G are [nrings][lmax + 1] complex (interleaved doubles): per ring r the Fourier
+ * coefficients of the ring along phi for m = 0..lmax, with the ring's e^{-i m phi_0}
+ * applied; z[r] = cos theta_r. alm is packed by m, a[m][l - m] at offset
+ * m (lmax + 1) - m (m - 1) / 2, (lmax + 1)(lmax + 2) / 2 complex values.
+ *   jfli_sht_map2alm: alm = weight * sum_r lambda_lm(theta_r) F[r][m]  (alm cleared first)
+ *   jfli_sht_alm2map: G[r][m] = sum_l alm[l][m] lambda_lm(theta_r)
+ * lambda_lm: orthonormal associated Legendre functions with the Condon-Shortley phase.
+ * lmax <= 8191, nrings <= 65535. */
+int jfli_sht_map2alm(void* stream, const double* F, const double* z, int nrings, int lmax, double weight,
+                     double* alm, char* err, size_t errlen);
+int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nrings, int lmax, double* G, char* err,
+                     size_t errlen);
 
 /* ---- adjoints ------------------------------------------------------------------
  * Reverse sweep of one reversible KKD step  v' = v + kick F(x);  x' = x + drift v'

@@ -506,6 +506,28 @@ int jfli_born(void* stream, const float* maps, int nplanes, long long npix, cons
       errlen, "jfli_born");
 }
 
+int jfli_sht_map2alm(void* stream, const double* F, const double* z, int nrings, int lmax, double weight,
+                     double* alm, char* err, size_t errlen) {
+  CHECK_PTR(F);
+  CHECK_PTR(z);
+  CHECK_PTR(alm);
+  if (nrings < 1 || nrings > 65535) return fail(err, errlen, JFLI_EINVAL, "nrings %d outside [1, 65535]", nrings);
+  if (lmax < 0 || lmax > 8191) return fail(err, errlen, JFLI_EINVAL, "lmax %d outside [0, 8191]", lmax);
+  return cuda_status(jfli::sht_analysis(F, z, nrings, lmax, weight, alm, (cudaStream_t)stream), err, errlen,
+                     "jfli_sht_map2alm");
+}
+
+int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nrings, int lmax, double* G, char* err,
+                     size_t errlen) {
+  CHECK_PTR(alm);
+  CHECK_PTR(z);
+  CHECK_PTR(G);
+  if (nrings < 1 || nrings > 65535) return fail(err, errlen, JFLI_EINVAL, "nrings %d outside [1, 65535]", nrings);
+  if (lmax < 0 || lmax > 8191) return fail(err, errlen, JFLI_EINVAL, "lmax %d outside [0, 8191]", lmax);
+  return cuda_status(jfli::sht_synthesis(alm, z, nrings, lmax, G, (cudaStream_t)stream), err, errlen,
+                     "jfli_sht_alm2map");
+}
+
 // ---- adjoints --------------------------------------------------------------------
 size_t jfli_adjoint_partials_count(int nx, int ny, int nz, int batch) {
   return jfli::adjoint_partials_count(MeshDims{nx, ny, nz, batch});

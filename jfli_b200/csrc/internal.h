@@ -76,6 +76,11 @@ int born_ctas(long long npix);
 cudaError_t born_convergence(const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
                              float* out, double* partials, float* mean, cudaStream_t s);
 
+// ---- sht.cu ----
+cudaError_t sht_analysis(const double* F, const double* z, int nrings, int lmax, double weight, double* alm,
+                         cudaStream_t s);
+cudaError_t sht_synthesis(const double* alm, const double* z, int nrings, int lmax, double* G, cudaStream_t s);
+
 // ---- adjoint.cu ----
 size_t adjoint_partials_count(const MeshDims& d);
 cudaError_t adjoint_unkick_paint(const float* disp, float* vel, const float* lam_x, float* lam_v, const float* force,

@@ -15,8 +15,11 @@ phase, built by the standard three-term recursion in l at fixed m; the starting 
 lambda_mm is formed in log space so that polar rings at large m underflow to zero
 instead of to NaN.
 
-This is not a GPU kernel (a GPU SHT is future work); it is the host step the reference
-also runs on the CPU.
+Two engines share the ring FFTs along phi, which run on the host (numpy):
+* "gpu" (default): the O(lmax^2 x rings) Legendre stages run in the library's FP64 kernels
+  (`jfli_sht_map2alm`, `jfli_sht_alm2map`; a_lm packed by m);
+* "host": the same recursion in numpy, kept as the restatement the GPU engine is tested
+  against and for maps small enough that the transfer is not worth it.
 """
 
 from __future__ import annotations
@@ -169,9 +172,98 @@ def alm2cl(alm: dict, lmax: int) -> np.ndarray:
     return cl
 
 
-def anafast(m: np.ndarray, lmax: int | None = None, iter: int = 3) -> np.ndarray:
+# ------------------------------------------------------------------------- GPU engine
+def _ring_synth(G: np.ndarray, nside: int, lmax: int) -> np.ndarray:
+    """Map from per-ring coefficients G[r][m] (inverse of _ring_ffts)."""
+    z, npr, phi0, start = ring_geometry(nside)
+    out = np.empty(12 * nside * nside)
+    mvec = np.arange(lmax + 1)
+    for r in range(z.size):
+        n = int(npr[r])
+        c = G[r] * np.exp(1j * mvec * phi0[r])
+        spec = np.zeros(n, dtype=np.complex128)
+        spec[0] += c[0].real
+        np.add.at(spec, mvec[1:] % n, c[1:])
+        vals = np.fft.ifft(spec) * n
+        out[start[r]:start[r] + n] = 2.0 * vals.real - c[0].real
+    return out
+
+
+class _GpuSht:
+    """Device tables of one (nside, lmax) and the two Legendre stages."""
+
+    def __init__(self, nside: int, lmax: int):
+        import torch
+
+        self.nside, self.lmax = nside, lmax
+        z, _, _, _ = ring_geometry(nside)
+        self.nrings = z.size
+        self.z = torch.as_tensor(z, dtype=torch.float64, device="cuda")
+        self.nalm = (lmax + 1) * (lmax + 2) // 2
+
+    def map2alm_once(self, m: np.ndarray) -> np.ndarray:
+        import torch
+
+        from ._lib import call, stream_ptr
+
+        F = torch.as_tensor(_ring_ffts(m, self.nside, self.lmax), device="cuda")
+        alm = torch.empty(self.nalm, dtype=torch.complex128, device="cuda")
+        call("jfli_sht_map2alm", stream_ptr(), F.data_ptr(), self.z.data_ptr(), self.nrings, self.lmax,
+             4.0 * math.pi / m.size, alm.data_ptr())
+        return alm.cpu().numpy()
+
+    def alm2map(self, alm: np.ndarray) -> np.ndarray:
+        import torch
+
+        from ._lib import call, stream_ptr
+
+        a = torch.as_tensor(np.ascontiguousarray(alm, dtype=np.complex128), device="cuda")
+        G = torch.empty(self.nrings, self.lmax + 1, dtype=torch.complex128, device="cuda")
+        call("jfli_sht_alm2map", stream_ptr(), a.data_ptr(), self.z.data_ptr(), self.nrings, self.lmax, G.data_ptr())
+        return _ring_synth(G.cpu().numpy(), self.nside, self.lmax)
+
+
+def packed_offsets(lmax: int) -> np.ndarray:
+    """Start of each m in the packed a_lm array (a[m][l - m])."""
+    m = np.arange(lmax + 2, dtype=np.int64)
+    return m * (lmax + 1) - m * (m - 1) // 2
+
+
+def map2alm_gpu(m: np.ndarray, lmax: int | None = None, iter: int = 3) -> np.ndarray:
+    """Packed a_lm (complex128, (lmax + 1)(lmax + 2) / 2) with the GPU Legendre stages."""
+    m = np.asarray(m, dtype=np.float64)
+    nside = int(round(math.sqrt(m.size / 12)))
+    if 12 * nside * nside != m.size:
+        raise ValueError("map size is not 12 nside^2")
+    lmax = 3 * nside - 1 if lmax is None else int(lmax)
+    eng = _GpuSht(nside, lmax)
+    alm = eng.map2alm_once(m)
+    for _ in range(iter):
+        alm = alm + eng.map2alm_once(m - eng.alm2map(alm))
+    return alm
+
+
+def packed_to_dict(alm: np.ndarray, lmax: int) -> dict:
+    off = packed_offsets(lmax)
+    return {mm: alm[off[mm]:off[mm + 1]] for mm in range(lmax + 1)}
+
+
+def alm2cl_packed(alm: np.ndarray, lmax: int) -> np.ndarray:
+    off = packed_offsets(lmax)
+    p = np.abs(alm) ** 2
+    cl = p[off[0]:off[1]].copy()
+    for mm in range(1, lmax + 1):
+        cl[mm:] += 2.0 * p[off[mm]:off[mm + 1]]
+    return cl / (2.0 * np.arange(lmax + 1) + 1.0)
+
+
+def anafast(m: np.ndarray, lmax: int | None = None, iter: int = 3, engine: str = "gpu") -> np.ndarray:
     """C_l, l = 0..lmax, of a RING-ordered HEALPix map (healpy.anafast defaults)."""
     m = np.asarray(m, dtype=np.float64)
     nside = int(round(math.sqrt(m.size / 12)))
     lmax = 3 * nside - 1 if lmax is None else int(lmax)
+    if engine == "gpu":
+        return alm2cl_packed(map2alm_gpu(m, lmax, iter), lmax)
+    if engine != "host":
+        raise ValueError(f"unknown engine {engine!r} (gpu, host)")
     return alm2cl(map2alm(m, lmax, iter), lmax)

@@ -101,11 +101,11 @@ def test_angular_cl_of_gpu_shell_matches_oracle_shell(cosmo):
     pos = (g + disp.astype(np.float64)) * (L / n)
     ref = oh.paint_shell(pos, obs, rmin, rmax, nside, "bilinear")
     lmax = 2 * nside
-    cg = sht.anafast(gpu / gpu.mean() - 1, lmax)
-    cr = sht.anafast(ref / ref.mean() - 1, lmax)
+    cg = sht.anafast(gpu / gpu.mean() - 1, lmax, engine="host")
+    cr = sht.anafast(ref / ref.mean() - 1, lmax, engine="host")
     rel = np.abs(cg[1:] / cr[1:] - 1).max()
     print(f"C_ell GPU shell vs oracle shell: max per-ell rel {rel:.2e}")
     assert rel < 1e-4
     dens = jf.SphericalDensity(array=torch.as_tensor(gpu, device="cuda"), mesh_size=(n,) * 3, box_size=(L,) * 3,
                                nside=nside)
-    np.testing.assert_allclose(dens.angular_cl(lmax=lmax), sht.anafast(gpu, lmax), rtol=1e-12)
+    np.testing.assert_allclose(dens.angular_cl(lmax=lmax), sht.anafast(gpu, lmax, engine="host"), rtol=1e-9)
