@@ -29,7 +29,8 @@ from .. import ops
 from .._lib import JFLI_STEP_CORRECT, JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
 from ..fields import ParticleField, PositionUnit
 from .correction import NoCorrection, PGDKernel, pgd_potential
-from .solvers import AbstractNBodySolver, EfficientDriftDoubleKick, NBodyState, ReversibleDoubleKickDrift
+from .solvers import (AbstractNBodySolver, EfficientDriftDoubleKick, NBodyState, ReversibleDoubleKickDrift,
+                      StepCoefficients)
 
 
 def _clip_to_end(t_next, t1, tol):
@@ -93,6 +94,15 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
     events = time_events(t0, ts, dt0, dtype)
     n_steps = sum(1 for e in events if e[0] == "step")
     state = NBodyState(interp_state=interp.init(), t_initial=t0)
+    # every step's FP64 factors up front (one vectorised evaluation of the growth tables),
+    # so that the host only enqueues kernels inside the loop
+    step_ts = [(e[1], e[2]) for e in events if e[0] == "step"]
+    if step_ts:
+        ta_all, tb_all = [a for a, _ in step_ts], [b for _, b in step_ts]
+        if efficient:
+            kicks_all, drifts_all = EfficientDriftDoubleKick.schedule_arrays(cosmo, ta_all, tb_all, dt0)
+        else:
+            kicks_all, drifts_all = ReversibleDoubleKickDrift.schedule_arrays(cosmo, ta_all, tb_all, dt0, t0)
 
     tgt = interp.painting.target if interp.painting is not None else "particles"
     w_snap = _scalar_weight(interp.painting.weights) if interp.painting is not None else 1.0
@@ -110,8 +120,8 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
     for ev in events:
         if ev[0] == "step":
             _, ta, tb = ev
+            c = StepCoefficients(kick=float(kicks_all[step_i]), drift=float(drifts_all[step_i]), kick_first=not efficient)
             step_i += 1
-            c = solver.step_coefficients(cosmo, ta, tb, dt0, t0)
             rho.zero_()
             if efficient:
                 flags = JFLI_STEP_DRIFT | JFLI_STEP_PAINT

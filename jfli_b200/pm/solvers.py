@@ -147,6 +147,21 @@ class ReversibleDoubleKickDrift(AbstractNBodySolver):
         drift = (cj.Gp(cosmo, t1) - cj.Gp(cosmo, t0)) / cj.gp(cosmo, af_2) / (af_2**3 * cj.E(cosmo, af_2))
         return StepCoefficients(kick=float(kick), drift=float(drift), kick_first=True)
 
+    @staticmethod
+    def schedule_arrays(cosmo, t0s, t1s, dt, t_initial):
+        """Vectorised step_coefficients over arrays of step boundaries -> (kicks, drifts)."""
+        t0s = np.asarray(t0s, np.float64)
+        t1s = np.asarray(t1s, np.float64)
+        t_prev = np.maximum(t0s - dt, t_initial)
+        ai_1 = np.sqrt(t_prev * t0s)
+        af_2 = np.sqrt(t0s * t1s)
+        dg = cj.dGfa(cosmo, t0s)
+        k1 = (cj.Gf(cosmo, t0s) - cj.Gf(cosmo, ai_1)) / dg
+        k2 = (cj.Gf(cosmo, af_2) - cj.Gf(cosmo, t0s)) / dg
+        kick = 1.5 * cosmo.Omega_m * (k1 + k2) / (t0s**2 * cj.E(cosmo, t0s))
+        drift = (cj.Gp(cosmo, t1s) - cj.Gp(cosmo, t0s)) / cj.gp(cosmo, af_2) / (af_2**3 * cj.E(cosmo, af_2))
+        return kick, drift
+
     def init(self, displacement, velocities, t0, t1, dt, cosmo):
         return displacement, velocities, NBodyState(interp_state=self.interp_kernel.init(), t_initial=t0)
 

@@ -132,51 +132,58 @@ def target_spectrum(n: int, box: float, steps: int = 20) -> torch.Tensor:
 
 
 class GradientWorker:
-    """Runs gradient requests one at a time on its own CUDA stream from a host thread,
-    concurrently with the batched forward steps on the main stream."""
+    """Runs gradient requests from host threads, each thread on its own CUDA stream, so
+    that they run concurrently with the batched forward steps on the main stream and,
+    for small meshes that do not fill the GPU, with one another."""
 
-    def __init__(self):
+    def __init__(self, threads: int = 3):
         import queue
         import threading
 
-        self.stream = torch.cuda.Stream()
         self.inbox: "queue.Queue" = queue.Queue()
         self.outbox: "queue.Queue" = queue.Queue()
         self.targets: dict = {}
+        self.streams = [torch.cuda.Stream() for _ in range(max(1, threads))]
         self.t0 = time.perf_counter()
-        self._thread = threading.Thread(target=self._loop, daemon=True)
-        self._thread.start()
+        self._threads = [threading.Thread(target=self._loop, args=(st,), daemon=True) for st in self.streams]
+        for t in self._threads:
+            t.start()
 
     def target(self, n: int, box: float) -> torch.Tensor:
+        """Target spectrum of a mesh size (built once, before requests of that size run)."""
         key = (n, box)
         if key not in self.targets:
-            with torch.cuda.stream(self.stream):
-                self.targets[key] = target_spectrum(n, box)
-            self.stream.synchronize()
+            st = self.streams[0]
+            with torch.cuda.stream(st):
+                spec = target_spectrum(n, box)
+            st.synchronize()
+            self.targets[key] = spec
         return self.targets[key]
 
     def submit(self, req, prep):
         self.inbox.put((req, prep))
 
-    def _loop(self):
+    def _loop(self, stream):
         while True:
             item = self.inbox.get()
             if item is None:
                 return
             req, prep = item
             try:
-                with torch.cuda.stream(self.stream):
-                    loss, gw, gom, gs8 = gradient_request(req, prep, self.target(req.mesh, req.box))
+                with torch.cuda.stream(stream):
+                    loss, gw, gom, gs8 = gradient_request(req, prep, self.targets[(req.mesh, req.box)])
                     gw_h = torch.empty(gw.shape, dtype=torch.float32, pin_memory=True)
                     gw_h.copy_(gw, non_blocking=True)
-                self.stream.synchronize()
+                stream.synchronize()
                 self.outbox.put((req.rid, float(loss), gw_h, float(gom), float(gs8), time.perf_counter(), None))
             except Exception as exc:  # reported to the caller through the outbox
                 self.outbox.put((req.rid, None, None, None, None, time.perf_counter(), exc))
 
     def close(self):
-        self.inbox.put(None)
-        self._thread.join(timeout=60)
+        for _ in self._threads:
+            self.inbox.put(None)
+        for t in self._threads:
+            t.join(timeout=60)
 
 
 def device_white_noise(seed: int, n: int, device="cuda") -> torch.Tensor:
@@ -359,12 +366,13 @@ class Engine:
     """Admission by HBM budget, continuous batching per mesh size, CUDA-graph replay."""
 
     def __init__(self, sizes=(64, 96, 128, 192), hbm_budget_gb: float = 24.0, max_slots: int = 16,
-                 use_graph: bool = True, workers: int = 6, keep_density: bool = True):
+                 use_graph: bool = True, workers: int = 6, keep_density: bool = True, grad_threads: int = 3):
         self.groups: dict[int, SizeGroup] = {}
         for n, cap in slot_capacities(sizes, hbm_budget_gb, max_slots).items():
             self.groups[n] = SizeGroup(n, cap, use_graph=use_graph)
         self.workers = workers
         self.keep_density = keep_density
+        self.grad_threads = grad_threads
         self._pool = None
         self._ready = False
         self.results: dict[int, ForwardResult] = {}
@@ -398,7 +406,7 @@ class Engine:
 
     def _gradient_worker(self) -> GradientWorker:
         if self._grad is None:
-            self._grad = GradientWorker()
+            self._grad = GradientWorker(self.grad_threads)
         return self._grad
 
     def _finalize(self, g: SizeGroup, b: int):
