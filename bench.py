@@ -463,7 +463,7 @@ def run_reference(args):
     for _ in range(args.warmup):
         cpu_step_rate(n, 1)
     rate, dt = cpu_step_rate(n, args.steps)
-    line = {"metric": METRIC, "value": round(rate, 4), "unit": "Mpart-steps/s", "n_gpus": 0,
+    line = {"metric": METRIC, "value": round(rate, 4), "unit": "Mpart-steps/s", "n_gpus": args.gpus, "device": "cpu",
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",

@@ -74,6 +74,31 @@ def test_argument_errors_are_reported_not_raised(lib):
     assert rc == 1 and b"invalid mesh shape" in buf.value
 
 
+def test_oversized_mesh_rejected(lib):
+    """A mesh whose particle offsets would overflow 32 bits ((2^32 - 1)/3 cells) is refused
+    before any launch; 1024^3 is accepted by the shape check."""
+    buf = ctypes.create_string_buffer(256)
+    fn = lib.jfli_paint_cic
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_float,
+                   ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_char_p, ctypes.c_size_t]
+    rc = fn(None, ctypes.c_void_p(16), 0, None, 1.0, ctypes.c_void_p(16), 0, 1200, 1200, 1200, 1, buf, 256)
+    assert rc == 1 and b"invalid mesh shape" in buf.value
+    rc = fn(None, None, 0, None, 1.0, None, 0, 1024, 1024, 1024, 1, buf, 256)
+    assert rc == 1 and b"null pointer" in buf.value  # shape accepted, pointers checked next
+
+
+def test_force_mesh_alignment_checked(lib):
+    buf = ctypes.create_string_buffer(256)
+    fn = lib.jfli_force_mesh
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p] + [ctypes.c_int] * 4 + [
+        ctypes.c_char_p, ctypes.c_size_t]
+    rc = fn(None, ctypes.c_void_p(256), 1.0, ctypes.c_void_p(260), 16, 16, 16, 1, buf, 256)
+    assert rc == 1 and b"16-byte aligned" in buf.value
+
+
 def test_unsupported_fft_shape_reported(lib):
     buf = ctypes.create_string_buffer(256)
     fn = lib.jfli_rfft3d
