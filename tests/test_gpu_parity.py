@@ -104,9 +104,11 @@ def test_pm_forces_matches_oracle(n, scale):
     assert rel_l2(f, ref) < 1e-5
 
 
-@pytest.mark.parametrize("shape", [(32, 32, 32), (16, 24, 36), (12, 20, 42), (8, 8, 4)])
+@pytest.mark.parametrize("shape", [(32, 32, 32), (16, 24, 36), (12, 20, 42), (8, 8, 4), (16, 16, 64),
+                                   (48, 32, 128), (64, 64, 64)])
 def test_force_mesh_matches_stencil(shape):
-    """Force meshes -D_a pot (vectorised path when nz % 4 == 0 and nz >= 8, scalar otherwise)."""
+    """Force mesh -D pot: 2.5D-blocked path (nx % 16, ny % 16, nz % 64 == 0), four-cell
+    vectorised path (nz % 4 == 0, nz >= 8), scalar path otherwise."""
     pot = np.random.default_rng(sum(shape)).normal(size=shape)
     F = host(ops.force_mesh(dev(pot), scale=2.0))
     for ax in range(3):
