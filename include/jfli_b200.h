@@ -25,6 +25,7 @@
  *   jfli_force_mesh        <- the gradient_kernel stage of jaxpm pm_forces (pm/solvers.py:22)
  *   jfli_kick_drift_paint  <- pm/solvers.py:151-202 and 258-325 (the per-particle part of step())
  *   jfli_pm_step           <- one step() of EfficientDriftDoubleKick / ReversibleDoubleKickDrift
+ *   jfli_kkd_run           <- the ReversibleDoubleKickDrift time loop (pm/integrate.py:196-279)
  *   jfli_ic_filter         <- initial.py:167-182 (interpolate_initial_conditions), infer/dist.py:43-79
  *   jfli_lpt               <- pm/lpt.py:119 (jaxpm lpt, order 1 and 2)
  *   jfli_power_spectrum    <- _src/power/_compute.py:23-119 (_initialize_pk + _power)
@@ -36,7 +37,7 @@
  *                             SphericalDensity.angular_cl (_src/power/_compute.py:175-191)
  * Adjoints (the reverse-mode derivatives jax.grad takes through the same code, and the
  * backward loop of the reversible adjoint, pm/integrate.py:147-535):
- *   jfli_adjoint_unkick_paint, jfli_poisson_divergence, jfli_adjoint_position
+ *   jfli_adjoint_unkick_paint, jfli_poisson_divergence, jfli_adjoint_position, jfli_kkd_adjoint
  *                          <- _integrate_bwd (pm/integrate.py:288-535): solver.reverse
  *                             (pm/solvers.py:327-411) + VJP of ReversibleDoubleKickDrift.step
  *                             (pm/solvers.py:258-325) through _forces (pm/solvers.py:19-32)
@@ -225,6 +226,24 @@ int jfli_poisson_divergence(void* stream, const float* u, float alpha, const flo
                             char* err, size_t errlen);
 int jfli_adjoint_position(void* stream, const float* disp, const float* u, const float* rho_bar, const float* force,
                           float scale, float* lam_x, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* The reversible KKD loop and its reverse sweep as single calls, for callers that would
+ * otherwise issue several launches per step (the gradient of a forward model):
+ *   jfli_kkd_run: from positions disp and momenta vel, paint, solve and take the steps
+ *     v += kicks[i] F(x); x += drifts[i] v for i < nsteps (F from the current positions);
+ *     rho receives the CIC density of the final positions.
+ *   jfli_kkd_adjoint: the reverse sweep from the final state (disp, vel) with cotangents
+ *     (lam_x, lam_v), all updated in place to the initial state and its cotangents;
+ *     sens[i][2] (device, FP64) = (dL/dkicks[i], dL/ddrifts[i]).
+ * kicks and drifts are host arrays of nsteps floats. Workspace: jfli_kkd_workspace_bytes
+ * (the same buffer serves both). */
+size_t jfli_kkd_workspace_bytes(int nx, int ny, int nz, int batch);
+int jfli_kkd_run(void* stream, float* disp, float* vel, const float* kicks, const float* drifts, int nsteps,
+                 float* rho, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                 size_t errlen);
+int jfli_kkd_adjoint(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
+                     const float* drifts, int nsteps, double* sens, void* workspace, size_t workspace_bytes, int nx,
+                     int ny, int nz, int batch, char* err, size_t errlen);
 
 /* dL/dmesh of P(k): out = irfft(rfft(mesh) * weights[digitize(|k|, kedges)] / M), with
  * weights[b] = 2 (dL/dP_b) prod(L/N) / count_b for the kept bins and 0 for bin 0 and

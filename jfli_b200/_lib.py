@@ -100,6 +100,17 @@ _SIGNATURES = {
     "jfli_born_workspace_bytes": (c_size_t, [c_int, c_longlong]),
     "jfli_born": (c_int, [c_void_p, c_void_p, c_int, c_longlong, c_void_p, c_int, c_void_p, c_void_p, c_size_t, *_ERR]),
     "jfli_adjoint_partials_count": (c_size_t, _DIMS),
+    "jfli_kkd_workspace_bytes": (c_size_t, _DIMS),
+    "jfli_kkd_run": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_float), ctypes.POINTER(c_float), c_int, c_void_p, c_void_p,
+         c_size_t, *_DIMS, *_ERR],
+    ),
+    "jfli_kkd_adjoint": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_float), ctypes.POINTER(c_float), c_int,
+         c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
+    ),
     "jfli_adjoint_unkick_paint": (
         c_int,
         [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_float, c_void_p, c_void_p, c_size_t,

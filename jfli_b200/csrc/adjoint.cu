@@ -194,6 +194,39 @@ static dim3 adj_grid(const MeshDims& d) { return particle_grid_dims(d.cells(), d
 
 size_t adjoint_partials_count(const MeshDims& d) { return (size_t)2 * adj_grid(d).x * d.batch; }
 
+// out[b][2] = sums of the per-CTA partials of batch entry b: each thread adds a strided
+// slice, then a shared-memory tree in a fixed order (deterministic).
+__global__ void __launch_bounds__(256) k_sum_partials(const double* __restrict__ partials, int nctas,
+                                                      double* __restrict__ out) {
+  __shared__ double sk[256], sd[256];
+  const double* p = partials + 2ll * nctas * blockIdx.x;
+  double a = 0.0, c = 0.0;
+  for (int i = threadIdx.x; i < nctas; i += 256) {
+    a += p[2 * i];
+    c += p[2 * i + 1];
+  }
+  sk[threadIdx.x] = a;
+  sd[threadIdx.x] = c;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      sk[threadIdx.x] += sk[threadIdx.x + w];
+      sd[threadIdx.x] += sd[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = sk[0];
+    out[2 * blockIdx.x + 1] = sd[0];
+  }
+}
+
+cudaError_t sum_adjoint_partials(const double* partials, const MeshDims& d, double* out, cudaStream_t s) {
+  k_sum_partials<<<d.batch, 256, 0, s>>>(partials, (int)adj_grid(d).x, out);
+  note_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t adjoint_unkick_paint(const float* disp, float* vel, const float* lam_x, float* lam_v, const float* force,
                                  float kick, float drift, float* ubar, double* partials, const MeshDims& d,
                                  cudaStream_t s) {

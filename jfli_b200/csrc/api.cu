@@ -528,6 +528,127 @@ int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nring
                      "jfli_sht_alm2map");
 }
 
+// ---- reversible KKD loop and its reverse sweep -------------------------------------
+namespace {
+struct KkdWs {
+  float2* spec;
+  float *pot, *rho, *rho_bar, *div, *force, *ubar;
+  double* partials;
+};
+
+size_t kkd_ws_bytes(const MeshDims& d) {
+  return spec_bytes(d) + 4 * mesh_bytes(d) + align256(sizeof(float) * 4 * (size_t)d.cells() * d.batch) +
+         align256(sizeof(float) * 3 * (size_t)d.cells() * d.batch) +
+         align256(sizeof(double) * jfli::adjoint_partials_count(d));
+}
+
+KkdWs kkd_ws(void* w, const MeshDims& d) {
+  char* p = (char*)w;
+  KkdWs k;
+  k.spec = (float2*)p;
+  p += spec_bytes(d);
+  k.pot = (float*)p;
+  p += mesh_bytes(d);
+  k.rho = (float*)p;
+  p += mesh_bytes(d);
+  k.rho_bar = (float*)p;
+  p += mesh_bytes(d);
+  k.div = (float*)p;
+  p += mesh_bytes(d);
+  k.force = (float*)p;
+  p += align256(sizeof(float) * 4 * (size_t)d.cells() * d.batch);
+  k.ubar = (float*)p;
+  p += align256(sizeof(float) * 3 * (size_t)d.cells() * d.batch);
+  k.partials = (double*)p;
+  return k;
+}
+
+// density of the current positions -> force mesh (in ws.force)
+cudaError_t kkd_force(float* disp, float* vel, float* rho, const KkdWs& w, const MeshDims& d, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * d.batch * sizeof(float), s);
+  if (e == cudaSuccess) e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, 0.f, JFLI_STEP_PAINT, 1.0f, rho, d, s);
+  if (e == cudaSuccess) e = jfli::poisson_potential(rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
+  if (e == cudaSuccess) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
+  return e;
+}
+}  // namespace
+
+size_t jfli_kkd_workspace_bytes(int nx, int ny, int nz, int batch) {
+  return kkd_ws_bytes(MeshDims{nx, ny, nz, batch});
+}
+
+int jfli_kkd_run(void* stream, float* disp, float* vel, const float* kicks, const float* drifts, int nsteps,
+                 float* rho, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                 size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(disp);
+  CHECK_PTR(vel);
+  CHECK_PTR(kicks);
+  CHECK_PTR(drifts);
+  CHECK_PTR(rho);
+  CHECK_PTR(workspace);
+  CHECK_ALIGN16(workspace);
+  if (nsteps < 0) return fail(err, errlen, JFLI_EINVAL, "nsteps must be >= 0");
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < kkd_ws_bytes(d))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, kkd_ws_bytes(d));
+  cudaStream_t s = (cudaStream_t)stream;
+  const KkdWs w = kkd_ws(workspace, d);
+  cudaError_t e = kkd_force(disp, vel, rho, w, d, s);
+  for (int i = 0; i < nsteps && e == cudaSuccess; ++i) {
+    e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
+    if (e == cudaSuccess)
+      e = jfli::kick_drift_paint(disp, vel, w.force, kicks[i], drifts[i], JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
+                                 1.0f, rho, d, s);
+    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::poisson_potential(rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
+    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
+  }
+  return cuda_status(e, err, errlen, "jfli_kkd_run");
+}
+
+int jfli_kkd_adjoint(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
+                     const float* drifts, int nsteps, double* sens, void* workspace, size_t workspace_bytes, int nx,
+                     int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(disp);
+  CHECK_PTR(vel);
+  CHECK_PTR(lam_x);
+  CHECK_PTR(lam_v);
+  CHECK_PTR(kicks);
+  CHECK_PTR(drifts);
+  CHECK_PTR(sens);
+  CHECK_PTR(workspace);
+  CHECK_ALIGN16(workspace);
+  if (nsteps < 0) return fail(err, errlen, JFLI_EINVAL, "nsteps must be >= 0");
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < kkd_ws_bytes(d))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, kkd_ws_bytes(d));
+  cudaStream_t s = (cudaStream_t)stream;
+  const KkdWs w = kkd_ws(workspace, d);
+  cudaError_t e = cudaSuccess;
+  for (int i = nsteps - 1; i >= 0 && e == cudaSuccess; --i) {
+    const float k = kicks[i], dr = drifts[i];
+    // un-drift and paint the previous positions, force mesh there
+    e = cudaMemsetAsync(w.rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
+    if (e == cudaSuccess)
+      e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, -dr, JFLI_STEP_DRIFT | JFLI_STEP_PAINT, 1.0f, w.rho, d, s);
+    if (e == cudaSuccess) e = jfli::poisson_potential(w.rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
+    if (e == cudaSuccess) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
+    // un-kick, adjoint paint, dL/dk and dL/dd
+    if (e == cudaSuccess) e = jfli::adjoint_unkick_paint(disp, vel, lam_x, lam_v, w.force, k, dr, w.ubar, w.partials, d, s);
+    if (e == cudaSuccess) e = jfli::sum_adjoint_partials(w.partials, d, sens + 2ll * i * batch, s);
+    // rho_bar = P(div ubar); lam_x += k grad R[rho_bar + lam_v . F]
+    if (e == cudaSuccess) e = jfli::divergence_fd(w.ubar, 1.0f, nullptr, 0.0f, 0, 0, w.div, d, s);
+    if (e == cudaSuccess) e = jfli::poisson_potential(w.div, w.spec, w.rho_bar, d, 0.0f, 1.0f, s);
+    if (e == cudaSuccess) e = jfli::adjoint_position(disp, lam_v, w.rho_bar, w.force, k, lam_x, d, s);
+  }
+  return cuda_status(e, err, errlen, "jfli_kkd_adjoint");
+}
+
 // ---- adjoints --------------------------------------------------------------------
 size_t jfli_adjoint_partials_count(int nx, int ny, int nz, int batch) {
   return jfli::adjoint_partials_count(MeshDims{nx, ny, nz, batch});

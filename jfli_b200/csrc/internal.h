@@ -86,6 +86,7 @@ size_t adjoint_partials_count(const MeshDims& d);
 cudaError_t adjoint_unkick_paint(const float* disp, float* vel, const float* lam_x, float* lam_v, const float* force,
                                  float kick, float drift, float* ubar, double* partials, const MeshDims& d,
                                  cudaStream_t s);
+cudaError_t sum_adjoint_partials(const double* partials, const MeshDims& d, double* out, cudaStream_t s);
 cudaError_t divergence_fd(const float* u, float alpha, const float* w, float beta, int aos, int accumulate,
                           float* out, const MeshDims& d, cudaStream_t s);
 cudaError_t adjoint_position(const float* disp, const float* u, const float* rho_bar, const float* force, float scale,

@@ -11,6 +11,7 @@ fills the ones given. Shapes:
 
 from __future__ import annotations
 
+import ctypes
 import math
 
 import numpy as np
@@ -351,6 +352,47 @@ def adjoint_position(disp: torch.Tensor, lam_x: torch.Tensor, *, rho_bar: torch.
     (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
     call("jfli_adjoint_position", stream_ptr(), ptr(disp), ptr(u), ptr(rho_bar), ptr(force), float(scale), ptr(lam_x),
          nx, ny, nz, batch)
+
+
+def _host_floats(a):
+    arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    return arr, arr.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def kkd_run(disp: torch.Tensor, vel: torch.Tensor, kicks, drifts, rho: torch.Tensor) -> None:
+    """The ReversibleDoubleKickDrift loop in one call (in place on disp, vel); rho receives
+    the CIC density of the final positions."""
+    _check(disp, "disp")
+    _check(vel, "vel")
+    _check(rho, "rho")
+    (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
+    k_arr, k_ptr = _host_floats(kicks)
+    d_arr, d_ptr = _host_floats(drifts)
+    if k_arr.size != d_arr.size:
+        raise ValueError("kicks and drifts must have the same length")
+    nb = query("jfli_kkd_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "kkd", disp.device)
+    call("jfli_kkd_run", stream_ptr(), ptr(disp), ptr(vel), k_ptr, d_ptr, int(k_arr.size), ptr(rho), ptr(ws),
+         ws.numel(), nx, ny, nz, batch)
+
+
+def kkd_adjoint(disp: torch.Tensor, vel: torch.Tensor, lam_x: torch.Tensor, lam_v: torch.Tensor, kicks,
+                drifts) -> torch.Tensor:
+    """Reverse sweep of kkd_run in one call (in place on all four particle grids); returns
+    the (nsteps, 2) FP64 (dL/dkick, dL/ddrift) on the device."""
+    for name, t in (("disp", disp), ("vel", vel), ("lam_x", lam_x), ("lam_v", lam_v)):
+        _check(t, name)
+    (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
+    k_arr, k_ptr = _host_floats(kicks)
+    d_arr, d_ptr = _host_floats(drifts)
+    if k_arr.size != d_arr.size:
+        raise ValueError("kicks and drifts must have the same length")
+    sens = torch.zeros(k_arr.size, batch, 2, dtype=torch.float64, device=disp.device)
+    nb = query("jfli_kkd_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "kkd", disp.device)
+    call("jfli_kkd_adjoint", stream_ptr(), ptr(disp), ptr(vel), ptr(lam_x), ptr(lam_v), k_ptr, d_ptr,
+         int(k_arr.size), ptr(sens), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return sens if batch > 1 else sens[:, 0, :]
 
 
 def power_adjoint(mesh: torch.Tensor, kedges: torch.Tensor, weights: torch.Tensor, box_size) -> torch.Tensor:

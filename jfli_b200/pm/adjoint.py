@@ -183,44 +183,21 @@ class LPT(torch.autograd.Function):
         return gic, gom, None, None
 
 
-def kkd_forward(x: torch.Tensor, v: torch.Tensor, kicks, drifts, rho: torch.Tensor, force: torch.Tensor,
-                pot: torch.Tensor) -> None:
+def kkd_forward(x: torch.Tensor, v: torch.Tensor, kicks, drifts, rho: torch.Tensor, force: torch.Tensor | None = None,
+                pot: torch.Tensor | None = None) -> None:
     """The ReversibleDoubleKickDrift loop in place: per step kick with the force at the
-    current positions, drift, paint; rho ends as the CIC density of the final positions."""
-    rho.zero_()
-    ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT, rho)
-    ops.poisson_force(rho, 1.0, out=force, pot=pot)
-    n = len(kicks)
-    for i in range(n):
-        rho.zero_()
-        ops.kick_drift_paint(x, v, force, float(kicks[i]), float(drifts[i]),
-                             JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT, rho)
-        if i < n - 1:
-            ops.poisson_force(rho, 1.0, out=force, pot=pot)
+    current positions, drift, paint; rho ends as the CIC density of the final positions.
+    One library call (`jfli_kkd_run`); force and pot are accepted for callers that pass
+    buffers and are not used (the library keeps its own in its workspace)."""
+    ops.kkd_run(x, v, kicks, drifts, rho)
 
 
 def kkd_reverse_adjoint(x: torch.Tensor, v: torch.Tensor, lam_x: torch.Tensor, lam_v: torch.Tensor, kicks, drifts):
     """Backward sweep of kkd_forward, in place on (x, v, lam_x, lam_v): on return (x, v) is
     the recomputed initial state and (lam_x, lam_v) the cotangent at it. Returns the FP64
-    (dL/dkick_n, dL/ddrift_n) arrays."""
-    shape = x.shape[:-1]
-    rho = torch.empty(shape, dtype=torch.float32, device=x.device)
-    pot = torch.empty_like(rho)
-    force = torch.empty(tuple(shape) + (4,), dtype=torch.float32, device=x.device)
-    ubar = torch.empty((3,) + tuple(shape), dtype=torch.float32, device=x.device)
-    rho_bar = torch.empty_like(rho)
-    n = len(kicks)
-    sens = torch.zeros(n, 2, dtype=torch.float64, device=x.device)
-    for i in reversed(range(n)):
-        k, d = float(kicks[i]), float(drifts[i])
-        rho.zero_()
-        ops.kick_drift_paint(x, v, None, 0.0, -d, JFLI_STEP_DRIFT | JFLI_STEP_PAINT, rho)
-        ops.poisson_force(rho, 1.0, out=force, pot=pot)
-        _, s = ops.adjoint_unkick_paint(x, v, lam_x, lam_v, force, k, d, ubar)
-        sens[i] = s
-        ops.poisson_divergence(ubar, aos=False, out=rho_bar)
-        ops.adjoint_position(x, lam_x, rho_bar=rho_bar, u=lam_v, force=force, scale=k)
-    return sens
+    (dL/dkick_n, dL/ddrift_n) arrays. One library call (`jfli_kkd_adjoint`): per step
+    un-drift + paint, force mesh, un-kick + adjoint paint, P(div), CIC-gradient gather."""
+    return ops.kkd_adjoint(x, v, lam_x, lam_v, kicks, drifts)
 
 
 class ReversibleNBody(torch.autograd.Function):
@@ -230,11 +207,8 @@ class ReversibleNBody(torch.autograd.Function):
     def forward(ctx, dx, p, omega_c, tables: ForwardTables):
         x = dx.detach().contiguous().clone()
         v = p.detach().contiguous().clone()
-        shape = x.shape[:-1]
-        rho = torch.empty(shape, dtype=torch.float32, device=x.device)
-        pot = torch.empty_like(rho)
-        force = torch.empty(tuple(shape) + (4,), dtype=torch.float32, device=x.device)
-        kkd_forward(x, v, tables.kicks, tables.drifts, rho, force, pot)
+        rho = torch.empty(x.shape[:-1], dtype=torch.float32, device=x.device)
+        kkd_forward(x, v, tables.kicks, tables.drifts, rho)
         ctx.tables = tables
         ctx.omega_c = omega_c
         ctx.save_for_backward(x, v)
