@@ -62,7 +62,9 @@ def parse():
     ap.add_argument("--e2e-requests", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=512)
-    ap.add_argument("--serve-rate", type=float, default=150.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-rate", type=float, default=90.0,
+                    help="Poisson arrival rate, requests/s (about 85%% of the engine's measured capacity with 25%% "
+                         "gradient requests, 104-111 requests/s)")
     ap.add_argument("--serve-256", type=int, default=6, help="256^3 requests for the served-vs-plain pair")
     ap.add_argument("--grad-iters", type=int, default=5, help="timed gradient iterations at 128^3")
     ap.add_argument("--lightcone", type=int, default=0,
@@ -241,6 +243,7 @@ def run_gpu(args, world, rank):
 
     # ---- end-to-end through the public API, host buffers in and out
     e2e = run_e2e(args, cosmo, n, box)
+    shells = run_shells(args, cosmo, n, box) if n == N_MESH else None
     serve = run_serving(args) if world == 1 else None
     grad = run_gradient(args) if world == 1 else None
     # clocks are sampled every 200 ms from before the warm-up through the e2e requests
@@ -256,8 +259,15 @@ def run_gpu(args, world, rank):
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": ncu_traffic(n),
             "peak_source": "measured" if peaks else "fallback", "avg_launch_ms": round(kdp_avg_ms, 4),
             "algorithmic_bytes_per_launch": alg_bytes, "step_share": round(sum(kdp) / ms, 4)}
+    # whole-step roofline: 120 B per particle-step (each array read or written once per pass,
+    # with r2c + three Green x gradient + c2r chains) and this implementation's own 132 B
+    step_s = (ms_max / args.steps) / 1e3
+    step_roof = {"bytes_per_particle_step": 120, "achieved": round(120.0 * particles / step_s / 1e9, 1),
+                 "frac": round(120.0 * particles / step_s / 1e9 / peak, 4), "unit": "GB/s", "peak": peak,
+                 "own_bytes_per_particle_step": 132,
+                 "own_frac": round(132.0 * particles / step_s / 1e9 / peak, 4)}
     return dict(value=value, ms=ms_max, clocks=clk, launches=launches, e2e=e2e, roofline=roof, serving=serve,
-                gradient=grad)
+                gradient=grad, step_roofline=step_roof, shells=shells)
 
 
 def ncu_traffic(n):
@@ -315,12 +325,62 @@ def run_e2e(args, cosmo, n, box):
             "ms_per_request": round(ms / args.e2e_requests, 2)}
 
 
+def run_shells(args, cosmo, n, box):
+    """The same 256^3 run with its light-cone output: 4 equal-width HEALPix shells at
+    nside 256 (bilinear) painted at their snapshot times around a centred observer
+    (radii 0-500 Mpc/h, centres 437.5/312.5/187.5/62.5), from pinned host white noise to
+    the 4 maps on the host. The reference loop stops at the nearest shell's time, so the
+    step count (dt0 = 0.9/40 plus the partial steps that snapshot clipping creates) is
+    the one the run reports."""
+    import torch
+
+    import jfli_b200 as jf
+
+    if args.e2e_requests <= 0:
+        return None
+    noise = torch.from_numpy(jf.white_noise(0, (n, n, n))).pin_memory()
+    solver = jf.EfficientDriftDoubleKick(interp_kernel=jf.NoInterp(
+        painting=jf.PaintingOptions(target="spherical", scheme="bilinear")))
+    out = torch.empty(4, 12 * 256 * 256, dtype=torch.float32).pin_memory()
+    dt0 = 0.9 / E2E_STEPS
+    steps = None
+    stream = torch.cuda.current_stream()
+
+    def request():
+        nonlocal steps
+        w = noise.to("cuda", non_blocking=True)
+        ic = jf.interpolate_initial_conditions(w, (n, n, n), (box,) * 3, cosmo=cosmo, nside=256)
+        dx, p = jf.lpt(cosmo, ic, ts=0.1, order=2)
+        shells, run = jf.nbody(cosmo, dx, p, t0=0.1, t1=1.0, dt0=dt0, nb_shells=4, solver=solver,
+                               return_state=True)
+        out.copy_(shells.array, non_blocking=True)
+        steps = run.steps
+
+    request()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = max(1, args.e2e_requests // 2)
+    e0.record(stream)
+    for _ in range(reps):
+        request()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"value": round(n**3 * steps * reps / (ms / 1e3) / 1e6, 2), "unit": "Mpart-steps/s",
+            "steps_per_request": steps, "ms_per_request": round(ms / reps, 2),
+            "h2d_bytes_per_step": n**3 * 4, "d2h_bytes_per_step": int(out.numel()) * 4,
+            "shell_sums": [round(float(v), 1) for v in out.double().sum(dim=1)],
+            "per": "request: ICs + 2LPT + KDK to the nearest shell's time, 4 shells nside 256 painted en route"}
+
+
 def run_serving(args):
     """The request stream (Poisson arrivals; mesh 64/96/128/192; L = 4 Mpc/h per cell;
     Omega_c ~ U[0.20, 0.35]; sigma8 ~ U[0.70, 0.90]; 10-40 KDK steps; seed = request id)
     through the batched engine and through the plain per-call path at the same offered
     load, plus 256^3 requests (40 steps, L = 1000 Mpc/h) served two at a time vs one by
-    one. Every request returns its P(k) (32 bins) to the host; densities stay on the device."""
+    one. Every request returns its density (a CUDA tensor of its own) and its P(k) (32 bins,
+    on the host)."""
     import torch
 
     from jfli_b200 import serving
@@ -328,12 +388,25 @@ def run_serving(args):
     if args.serve_requests <= 0:
         return None
     reqs = serving.poisson_stream(args.serve_requests, args.serve_rate, seed=0, grad_fraction=0.25)
-    eng = serving.Engine(sizes=(64, 96, 128, 192), hbm_budget_gb=32.0, max_slots=16, keep_density=False)
+    delivered = {"engine": 0, "plain": 0}
+
+    def consumer(key):
+        """The caller's side: each result arrives with its density as a CUDA tensor of its
+        own; the consumer takes it (checks its shape) and lets it go, as a sampler would."""
+        def take(res):
+            d = res.density
+            assert d is not None and d.is_cuda and d.dim() == 3 and d.shape[0] == d.shape[1] == d.shape[2]
+            delivered[key] += 1
+            res.density = None
+        return take
+
+    eng = serving.Engine(sizes=(64, 96, 128, 192), hbm_budget_gb=32.0, max_slots=16, keep_density="device",
+                         on_result=consumer("engine"))
     warm = serving.poisson_stream(16, 0.0, seed=1, grad_fraction=0.0)
     for r in warm:
         r.rid += 10**6
     eng.run(warm, realtime=False)  # graphs, FFT tables, worker processes
-    serving.run_plain(warm[:4], realtime=False, keep_density=False)
+    serving.run_plain(warm[:4], realtime=False, keep_density="device", on_result=consumer("plain"))
     torch.cuda.synchronize()
     l0 = __import__("jfli_b200").ops.launch_count()
     served = eng.run(reqs, realtime=True)
@@ -342,7 +415,7 @@ def run_serving(args):
     burst = [dataclasses_replace(r, rid=r.rid + 2 * 10**6, arrival=0.0) for r in reqs]
     s_cap = serving.summarize(eng.run(burst, realtime=False), burst)
     eng.close()
-    plain = serving.run_plain(reqs, realtime=True, keep_density=False)
+    plain = serving.run_plain(reqs, realtime=True, keep_density="device", on_result=consumer("plain"))
     p_stats = serving.summarize(plain, reqs)
     worst = max(serving.pk_max_rel(served[r.rid].pk, plain[r.rid].pk) for r in reqs)
 
@@ -351,17 +424,19 @@ def run_serving(args):
                      f"10-40 KDK steps; {n_grad} also ask for the gradient of the 32-bin log-P(k) loss (reversible "
                      f"KKD adjoint, same mesh and step count) w.r.t. white noise, Omega_c and sigma8",
            "served": s_stats, "served_all_at_once": s_cap, "plain": p_stats,
-           "slots": eng.capacity(), "served_launches": launches,
+           "slots": eng.capacity(), "served_launches": launches, "densities_delivered": dict(delivered),
            "max_pk_rel_served_vs_plain": float(f"{worst:.3e}")}
     if args.serve_256 > 0:
         big = [serving.ForwardRequest(rid=3 * 10**6 + i, mesh=256, box=1000.0, omega_c=0.2607, sigma8=0.8102,
                                       steps=40, seed=i) for i in range(args.serve_256)]
-        e256 = serving.Engine(sizes=(256,), hbm_budget_gb=2.0, max_slots=2, keep_density=False, workers=2)
+        e256 = serving.Engine(sizes=(256,), hbm_budget_gb=2.0, max_slots=2, keep_density="device", workers=2,
+                              on_result=consumer("engine"))
         e256.run(big[:2], realtime=False)
         big2 = [dataclasses_replace(r, rid=r.rid + 100) for r in big]
         s256 = serving.summarize(e256.run(big2, realtime=False), big2)
         e256.close()
-        p256 = serving.summarize(serving.run_plain(big, realtime=False, keep_density=False), big)
+        p256 = serving.summarize(serving.run_plain(big, realtime=False, keep_density="device",
+                                                   on_result=consumer("plain")), big)
         out["at_256"] = {"requests": len(big), "served_mpart_steps_per_s": s256["mpart_steps_per_s"],
                          "plain_mpart_steps_per_s": p256["mpart_steps_per_s"], "served_p50_ms": s256["p50_ms"],
                          "plain_p50_ms": p256["p50_ms"], "slots": 2,
@@ -443,13 +518,14 @@ def cpu_step_rate(n, nsteps=1):
 
 
 def cpu_baseline_block(n):
-    """Two KDK steps at (n/2)^3, a bounded sample of the n^3 workload (~10 s of CPU work;
-    one step at 256^3 takes ~40 s on 8 cores and its per-particle rate is the same)."""
-    m = max(32, n // 2)
-    rate, dt = cpu_step_rate(m, 2)
+    """The FP32 NumPy/SciPy port on this host: one KDK step at n^3 (the workload itself,
+    ~20-40 s of CPU work at 256^3) and, for reference, five steps at 64^3."""
+    rate, dt = cpu_step_rate(n, 1)
+    rate64, dt64 = cpu_step_rate(64, 5)
     return {"value": round(rate, 4), "unit": "Mpart-steps/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"2 KDK steps (paint, 4 complex FFTs, 3 readouts) at {m}^3, a sample of the {n}^3 "
-                      f"workload, FP32 NumPy/SciPy, scipy.fft workers=all; {dt:.1f} s"}
+            "sample": f"1 KDK step (paint, 4 complex FFTs, 3 readouts) at {n}^3, FP32 NumPy/SciPy, scipy.fft "
+                      f"workers=all; {dt:.1f} s",
+            "at_64": {"value": round(rate64, 4), "sample": f"5 KDK steps at 64^3, {dt64:.1f} s"}}
 
 
 def run_reference(args):
@@ -538,8 +614,9 @@ def main():
                            "mesh": args.mesh, "particles": args.mesh**3, "box": BOX * args.mesh / N_MESH,
                            "solver": "EfficientDriftDoubleKick", "parallelism": f"replicas x{world}",
                            "l2": "particle state (x, v: 402 MB) exceeds the 126 MB L2; no flush"},
-                "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"], "clocks": res["clocks"],
-                "gpu_launches": res["launches"], "serving": res["serving"], "gradient": res["gradient"]}
+                "roofline": res["roofline"], "step_roofline": res["step_roofline"], "cpu_baseline": cpu, "e2e": res["e2e"], "clocks": res["clocks"],
+                "gpu_launches": res["launches"], "serving": res["serving"], "gradient": res["gradient"],
+                "e2e_with_shells": res["shells"]}
         print(json.dumps(line), flush=True)
     if world > 1:
         from jfli_b200 import replicas

@@ -366,13 +366,20 @@ class Engine:
     """Admission by HBM budget, continuous batching per mesh size, CUDA-graph replay."""
 
     def __init__(self, sizes=(64, 96, 128, 192), hbm_budget_gb: float = 24.0, max_slots: int = 16,
-                 use_graph: bool = True, workers: int = 6, keep_density: bool = True, grad_threads: int = 3):
+                 use_graph: bool = True, workers: int = 6, keep_density: bool | str = True, grad_threads: int = 3,
+                 on_result=None):
+        """keep_density: True returns each density in pinned host memory, "device" as a
+        CUDA tensor of the caller's own, False not at all (P(k) only).
+        on_result(res): called once per request as soon as its result is complete (the
+        density and P(k) ready to use), before it is stored in `results`; a consumer that
+        takes the density and sets `res.density = None` lets its memory be reused."""
         self.groups: dict[int, SizeGroup] = {}
         for n, cap in slot_capacities(sizes, hbm_budget_gb, max_slots).items():
             self.groups[n] = SizeGroup(n, cap, use_graph=use_graph)
         self.workers = workers
         self.keep_density = keep_density
         self.grad_threads = grad_threads
+        self.on_result = on_result
         self._pool = None
         self._ready = False
         self.results: dict[int, ForwardResult] = {}
@@ -414,7 +421,9 @@ class Engine:
         req = s.req
         sums = ops.power_sums(g.rho[b], g.kedges(s.prep, req.box), (req.box,) * 3)
         dens = None
-        if self.keep_density:
+        if self.keep_density == "device":
+            dens = g.rho[b].clone()  # the caller's own copy on the GPU (the slot is reused at once)
+        elif self.keep_density:
             dens = torch.empty(req.mesh, req.mesh, req.mesh, dtype=torch.float32, pin_memory=True)
             dens.copy_(g.rho[b], non_blocking=True)
         sums_h = torch.empty(sums.shape, dtype=torch.float64, pin_memory=True)
@@ -442,7 +451,7 @@ class Engine:
             if req.want_grad:
                 self._await_grad[res.rid] = res
             else:
-                self.results[res.rid] = res
+                self._deliver(res)
         self._inflight = keep
         if self._grad is not None:
             while not self._grad.outbox.empty():
@@ -455,10 +464,22 @@ class Engine:
             loss, gw, gom, gs8, t_done = self._grad_done.pop(rid)
             res.loss, res.grad_noise, res.grad_omega_c, res.grad_sigma8 = loss, gw, gom, gs8
             res.done = max(res.done, t_done)
-            self.results[rid] = res
+            self._deliver(res)
+
+    def _deliver(self, res):
+        if self.on_result is not None:
+            self.on_result(res)
+        self.results[res.rid] = res
 
     def run(self, requests, realtime: bool = True):
-        """Serve `requests` (arrival times in seconds after the call); returns {rid: ForwardResult}."""
+        """Serve `requests` (arrival times in seconds after the call); returns {rid: ForwardResult}.
+        Request ids must be unique, and new to this engine (results are keyed by id)."""
+        rids = [r.rid for r in requests]
+        if len(set(rids)) != len(rids):
+            raise ValueError("request ids must be unique within a run")
+        seen = [rid for rid in rids if rid in self.results]
+        if seen:
+            raise ValueError(f"request ids already served by this engine: {seen[:8]}")
         for r in requests:
             if r.mesh not in self.groups:
                 raise ValueError(f"request {r.rid}: mesh {r.mesh} has no slot group (sizes {list(self.groups)})")
@@ -516,8 +537,9 @@ class Engine:
         return self.results
 
 
-def run_plain(requests, realtime: bool = True, keep_density: bool = True):
-    """The plain per-call path: one request at a time through the public API, FIFO."""
+def run_plain(requests, realtime: bool = True, keep_density: bool | str = True, on_result=None):
+    """The plain per-call path: one request at a time through the public API, FIFO
+    (`keep_density` and `on_result` as for `Engine`)."""
     import jfli_b200 as jf
 
     reqs = sorted(requests, key=lambda r: r.arrival)
@@ -537,7 +559,7 @@ def run_plain(requests, realtime: bool = True, keep_density: bool = True):
         rho, run = jf.nbody(c, dx, p, t0=A_INIT, t1=1.0, dt0=(1.0 - A_INIT) / r.steps, solver=solver,
                             return_state=True)
         ps = rho.power(kedges=config_kedges(r.mesh, r.box))
-        dens = rho.array.cpu() if keep_density else None
+        dens = rho.array if keep_density == "device" else (rho.array.cpu() if keep_density else None)
         pk = ps.array.cpu().numpy()
         res = ForwardResult(rid=r.rid, density=dens, k=ps.wavenumber.cpu().numpy(), pk=pk, steps=run.steps,
                             arrival=r.arrival, admitted=start)
@@ -548,6 +570,8 @@ def run_plain(requests, realtime: bool = True, keep_density: bool = True):
             loss, gw, gom, gs8 = gradient_request(r, prepare(r), targets[key])
             res.loss, res.grad_noise, res.grad_omega_c, res.grad_sigma8 = float(loss), gw.cpu(), float(gom), float(gs8)
         res.done = now()
+        if on_result is not None:
+            on_result(res)
         out[r.rid] = res
     return out
 

@@ -95,6 +95,20 @@ def test_rejects_unknown_size():
         eng.run([r], realtime=False)
 
 
+def test_rejects_duplicate_request_ids():
+    """Results are keyed by request id: a run with a repeated id, or an id this engine
+    has already served, is refused before any work starts."""
+    from jfli_b200 import serving
+
+    eng = serving.Engine(sizes=(64,), max_slots=1, workers=0)
+    r = serving.ForwardRequest(rid=7, mesh=64, box=256.0, omega_c=0.25, sigma8=0.8, steps=10, seed=0)
+    with pytest.raises(ValueError, match="unique"):
+        eng.run([r, r], realtime=False)
+    eng.results[7] = None  # as if served
+    with pytest.raises(ValueError, match="already served"):
+        eng.run([r], realtime=False)
+
+
 def test_gradient_requests_in_the_mix():
     """Gradient requests served beside batched forwards (own stream, own thread) give the
     same loss and gradients as the same request computed alone."""
