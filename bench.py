@@ -62,9 +62,9 @@ def parse():
     ap.add_argument("--e2e-requests", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=512)
-    ap.add_argument("--serve-rate", type=float, default=90.0,
-                    help="Poisson arrival rate, requests/s (about 85%% of the engine's measured capacity with 25%% "
-                         "gradient requests, 104-111 requests/s)")
+    ap.add_argument("--serve-rate", type=float, default=0.0,
+                    help="Poisson arrival rate, requests/s; 0 = 85%% of the engine's capacity, measured first "
+                         "with the same requests queued at once")
     ap.add_argument("--serve-256", type=int, default=6, help="256^3 requests for the served-vs-plain pair")
     ap.add_argument("--grad-iters", type=int, default=5, help="timed gradient iterations at 128^3")
     ap.add_argument("--lightcone", type=int, default=0,
@@ -387,7 +387,6 @@ def run_serving(args):
 
     if args.serve_requests <= 0:
         return None
-    reqs = serving.poisson_stream(args.serve_requests, args.serve_rate, seed=0, grad_fraction=0.25)
     delivered = {"engine": 0, "plain": 0}
 
     def consumer(key):
@@ -402,27 +401,35 @@ def run_serving(args):
 
     eng = serving.Engine(sizes=(64, 96, 128, 192), hbm_budget_gb=32.0, max_slots=16, keep_density="device",
                          on_result=consumer("engine"))
-    warm = serving.poisson_stream(16, 0.0, seed=1, grad_fraction=0.0)
+    warm = serving.poisson_stream(16, 0.0, seed=1, grad_fraction=0.5)
     for r in warm:
         r.rid += 10**6
-    eng.run(warm, realtime=False)  # graphs, FFT tables, worker processes
+    eng.run(warm, realtime=False)  # graphs, FFT tables, worker processes, gradient workspaces
     serving.run_plain(warm[:4], realtime=False, keep_density="device", on_result=consumer("plain"))
     torch.cuda.synchronize()
+    # capacity: the whole stream queued at once (same requests, arrivals at 0)
+    burst = [dataclasses_replace(r, rid=r.rid + 2 * 10**6, arrival=0.0)
+             for r in serving.poisson_stream(args.serve_requests, 1.0, seed=0, grad_fraction=0.25)]
+    s_cap = serving.summarize(eng.run(burst, realtime=False), burst)
+    rate = args.serve_rate if args.serve_rate > 0 else round(0.85 * s_cap["requests_per_s"], 1)
+    reqs = serving.poisson_stream(args.serve_requests, rate, seed=0, grad_fraction=0.25)
     l0 = __import__("jfli_b200").ops.launch_count()
     served = eng.run(reqs, realtime=True)
     launches = __import__("jfli_b200").ops.launch_count() - l0
     s_stats = serving.summarize(served, reqs)
-    burst = [dataclasses_replace(r, rid=r.rid + 2 * 10**6, arrival=0.0) for r in reqs]
-    s_cap = serving.summarize(eng.run(burst, realtime=False), burst)
     eng.close()
     plain = serving.run_plain(reqs, realtime=True, keep_density="device", on_result=consumer("plain"))
     p_stats = serving.summarize(plain, reqs)
     worst = max(serving.pk_max_rel(served[r.rid].pk, plain[r.rid].pk) for r in reqs)
 
     n_grad = sum(r.want_grad for r in reqs)
-    out = {"stream": f"{len(reqs)} requests, Poisson arrivals at {args.serve_rate:g}/s, mesh U{{64,96,128,192}}, "
+    out = {"stream": f"{len(reqs)} requests, Poisson arrivals at {rate:g}/s, mesh U{{64,96,128,192}}, "
                      f"10-40 KDK steps; {n_grad} also ask for the gradient of the 32-bin log-P(k) loss (reversible "
                      f"KKD adjoint, same mesh and step count) w.r.t. white noise, Omega_c and sigma8",
+           "offered_rate": rate,
+           "offered_load": round(rate / s_cap["requests_per_s"], 3),
+           "rate_rule": "85% of the engine's capacity measured just before (the same requests queued at once)"
+                        if args.serve_rate <= 0 else "given on the command line",
            "served": s_stats, "served_all_at_once": s_cap, "plain": p_stats,
            "slots": eng.capacity(), "served_launches": launches, "densities_delivered": dict(delivered),
            "max_pk_rel_served_vs_plain": float(f"{worst:.3e}")}

@@ -71,8 +71,11 @@ class ForwardTables:
 def kkd_schedule(cosmo, t0: float, t1: float, dt0: float):
     """(kicks, drifts) of the ReversibleDoubleKickDrift steps from t0 to t1."""
     ev = [(e[1], e[2]) for e in time_events(t0, [t1], dt0) if e[0] == "step"]
-    cs = [ReversibleDoubleKickDrift.step_coefficients(cosmo, a, b, dt0, t0) for a, b in ev]
-    return np.array([c.kick for c in cs]), np.array([c.drift for c in cs])
+    if not ev:
+        return np.zeros(0), np.zeros(0)
+    t0s, t1s = zip(*ev)
+    kicks, drifts = ReversibleDoubleKickDrift.schedule_arrays(cosmo, t0s, t1s, dt0, t0)
+    return np.asarray(kicks, np.float64), np.asarray(drifts, np.float64)
 
 
 def forward_tables(omega_c: float, sigma8: float, *, t0: float, t1: float, dt0: float, n_table: int = 128,

@@ -127,12 +127,23 @@ def test_gradient_requests_in_the_mix():
         if not r.want_grad:
             assert res.loss is None
             continue
-        loss, gw, gom, gs8 = serving.gradient_request(r, serving.prepare(r), target)
+        prep = serving.prepare(r)
+        loss, gw, gom, gs8 = serving.gradient_request(r, prep, target)
+        again = [serving.gradient_request(r, prep, target) for _ in range(2)]  # alone again: run-to-run spread
+        gom_alone = [float(gom)] + [float(a[2]) for a in again]
+        gs8_alone = [float(gs8)] + [float(a[3]) for a in again]
         assert np.isfinite(res.loss) and abs(res.loss - float(loss)) <= 1e-6 * abs(float(loss))
         rel = float(torch.linalg.norm(res.grad_noise.cuda() - gw) / torch.linalg.norm(gw))
-        print(f"request {r.rid}: loss {res.loss:.5e}, grad rel L2 vs alone {rel:.2e}, dOmega_c {res.grad_omega_c:.4e}")
+        print(f"request {r.rid}: loss {res.loss:.5e}, grad rel L2 vs alone {rel:.2e}, dOmega_c {res.grad_omega_c:.6e} "
+              f"(alone {', '.join(f'{v:.6e}' for v in gom_alone)}), dsigma8 {res.grad_sigma8:.6e} "
+              f"(alone {', '.join(f'{v:.6e}' for v in gs8_alone)})")
         # The CIC paint accumulates with FP32 atomics, so the density differs in its last
-        # bits from run to run; 10-14 steps and the adjoint sweep grow that to ~1e-5.
+        # bits from run to run; 10-14 steps and the adjoint sweep grow that to ~1e-5 in the
+        # noise gradient. The cosmology derivatives are sums of contributions (ICs, LPT,
+        # every kick and drift) that partly cancel, so where one is small its run-to-run
+        # spread can exceed 1e-4 of it: the bound is 2e-4 relative or three times the range
+        # of three runs alone, whichever is larger.
         assert rel < 1e-4
-        assert abs(res.grad_omega_c - float(gom)) <= 1e-4 * abs(float(gom))
-        assert abs(res.grad_sigma8 - float(gs8)) <= 1e-4 * abs(float(gs8))
+        for mix, alone in ((res.grad_omega_c, gom_alone), (res.grad_sigma8, gs8_alone)):
+            spread = max(alone) - min(alone)
+            assert abs(mix - alone[0]) <= max(2e-4 * abs(alone[0]), 3.0 * spread)
