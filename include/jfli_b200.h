@@ -32,6 +32,9 @@
  *   jfli_healpix_paint     <- _src/fields/_painting.py:249-348 (jaxpm paint_particles_spherical)
  *   jfli_lightcone_drift   <- pm/interp.py:110-121 (_drift_to_time) as used by DriftInterp.paint
  *                             (pm/interp.py:254-318)
+ *   jfli_healpix_paint_tiled <- OnionTiler._paint_tiled_27 (pm/interp.py:418-504) and
+ *                             TelephotoInterp._paint_telephoto (pm/interp.py:643-699): the
+ *                             rotated, shifted (and drifted) replicas painted in one pass
  *   jfli_born              <- _src/lensing/_born.py:29-130 (_born_core_impl, _born_spherical)
  *   jfli_sht_map2alm / jfli_sht_alm2map <- the Legendre stages of healpy.anafast behind
  *                             SphericalDensity.angular_cl (_src/power/_compute.py:175-191)
@@ -166,6 +169,25 @@ int jfli_power_spectrum(void* stream, const float* mesh, const float* kedges, in
 int jfli_healpix_paint(void* stream, const float* disp, int absolute, const float* weights, float weight, float lx,
                        float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside, int scheme,
                        float* map, int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* HEALPix shell map of `ntiles` (<= 27) replicas of the particles, in one pass. For
+ * replica i, with c = x - observer (x in Mpc/h from the grid index and disp):
+ *   q = R_i c + s_i      R_i = rotations[9i..9i+8] (host, row-major; signed permutation
+ *                        matrices only), s_i = shifts[3i..3i+2] (host, Mpc/h)
+ * Without vel, q + observer is painted. With vel (the momenta) each replica is drifted to
+ * its light-cone crossing with the rotated momentum R_i v, as jfli_lightcone_drift does:
+ *   telephoto = 0: x' = q + observer, a_t from |x' - observer|, x' += D R_i v
+ *   telephoto = 1: a_t from |q - observer|, q += D R_i v, x' = q + observer
+ * D = (interp(a_t; ga, g) - gp_t) / interp(sqrt(t a_t); da, dgfa). dbound must bound |D|
+ * over the distance table; replicas farther than dbound |v| from the shell are skipped.
+ * Painting as jfli_healpix_paint (rmin < r <= rmax, scheme, weights * weight). */
+int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, const float* vel, const float* weights,
+                             float weight, float lx, float ly, float lz, float ox, float oy, float oz, int ntiles,
+                             const signed char* rotations, const float* shifts, int telephoto, float rmin, float rmax,
+                             float t, float gp_t, float dbound, const float* chi, const float* a_chi, int n_chi,
+                             const float* ga, const float* g, int n_g, const float* da, const float* dgfa, int n_d,
+                             int nside, int scheme, float* map, int accumulate, int nx, int ny, int nz, int batch,
+                             char* err, size_t errlen);
 
 /* Positions (Mpc/h) of the particles drifted to their light-cone crossing:
  *   x = (grid index + disp) / N * L;  a_t = interp(|x - observer|; chi, a_chi);

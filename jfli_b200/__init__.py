@@ -35,6 +35,7 @@ from .pm import (
     ReversibleDoubleKickDrift,
     SharpeningKernel,
     TelephotoInterp,
+    get_all_47_symmetries,
     lpt,
     nbody,
 )

@@ -422,6 +422,67 @@ int jfli_healpix_paint(void* stream, const float* disp, int absolute, const floa
       errlen, "jfli_healpix_paint");
 }
 
+int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, const float* vel, const float* weights,
+                             float weight, float lx, float ly, float lz, float ox, float oy, float oz, int ntiles,
+                             const signed char* rotations, const float* shifts, int telephoto, float rmin, float rmax,
+                             float t, float gp_t, float dbound, const float* chi, const float* a_chi, int n_chi,
+                             const float* ga, const float* g, int n_g, const float* da, const float* dgfa, int n_d,
+                             int nside, int scheme, float* map, int accumulate, int nx, int ny, int nz, int batch,
+                             char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(map);
+  CHECK_PTR(rotations);
+  CHECK_PTR(shifts);
+  if (nside < 1 || nside > 8192) return fail(err, errlen, JFLI_EINVAL, "nside %d outside [1, 8192]", nside);
+  if (scheme != JFLI_HEALPIX_NGP && scheme != JFLI_HEALPIX_BILINEAR)
+    return fail(err, errlen, JFLI_EUNSUPPORTED, "HEALPix scheme %d not supported (0 = ngp, 1 = bilinear)", scheme);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  if (ntiles < 1 || ntiles > jfli::kMaxTiles)
+    return fail(err, errlen, JFLI_EINVAL, "ntiles %d outside [1, %d]", ntiles, jfli::kMaxTiles);
+  for (int i = 0; i < ntiles; ++i) {  // signed permutation matrices only
+    int used = 0;
+    for (int r = 0; r < 3; ++r) {
+      int nz_in_row = 0;
+      for (int c = 0; c < 3; ++c) {
+        const int m = rotations[9 * i + 3 * r + c];
+        if (m == 0) continue;
+        if ((m != 1 && m != -1) || (used & (1 << c)))
+          return fail(err, errlen, JFLI_EINVAL, "tile %d: rotation is not a signed permutation matrix", i);
+        used |= 1 << c;
+        ++nz_in_row;
+      }
+      if (nz_in_row != 1) return fail(err, errlen, JFLI_EINVAL, "tile %d: rotation is not a signed permutation matrix", i);
+    }
+    for (int c = 0; c < 3; ++c)
+      if (!isfinite(shifts[3 * i + c])) return fail(err, errlen, JFLI_EINVAL, "tile %d: shift is not finite", i);
+  }
+  if (vel) {
+    CHECK_PTR(chi);
+    CHECK_PTR(a_chi);
+    CHECK_PTR(ga);
+    CHECK_PTR(g);
+    CHECK_PTR(da);
+    CHECK_PTR(dgfa);
+    if (n_chi < 2 || n_g < 2 || n_d < 2) return fail(err, errlen, JFLI_EINVAL, "tables need at least 2 entries");
+    if (!(t > 0)) return fail(err, errlen, JFLI_EINVAL, "scale factor must be positive");
+    if (!(dbound >= 0) || !isfinite(dbound)) return fail(err, errlen, JFLI_EINVAL, "drift bound must be finite, >= 0");
+  }
+  const MeshDims d{nx, ny, nz, batch};
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!accumulate) {
+    cudaError_t e = cudaMemsetAsync(map, 0, (size_t)12 * nside * nside * batch * sizeof(float), s);
+    if (e != cudaSuccess) return cuda_status(e, err, errlen, "jfli_healpix_paint_tiled memset");
+  }
+  const float box[3] = {lx, ly, lz};
+  const float obs[3] = {ox, oy, oz};
+  const jfli::DriftTables tb{chi, a_chi, n_chi, ga, g, n_g, da, dgfa, n_d};
+  return cuda_status(jfli::healpix_paint_tiled(disp, absolute, vel, weights, weight, d, box, obs, ntiles, rotations,
+                                               shifts, telephoto, rmin, rmax, t, gp_t, dbound, tb, nside, scheme, map,
+                                               s),
+                     err, errlen, "jfli_healpix_paint_tiled");
+}
+
 // P(k) for callers that cannot allocate device memory: the same sums as
 // jfli_power_spectrum, with the half spectrum and the histogram partials kept in a
 // fixed device array inside the library instead of a caller workspace. The array is

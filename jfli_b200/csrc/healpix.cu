@@ -11,8 +11,10 @@
 // Angles are computed in FP64 from the FP32 positions.
 #include <math.h>
 
+#include "cic.cuh"
 #include "common.cuh"
 #include "internal.h"
+#include "kspace_ops.cuh"
 
 namespace jfli {
 
@@ -160,6 +162,26 @@ __device__ __forceinline__ void interp_weights(double theta, double phi, int nsi
   }
 }
 
+// Deposit of weight w at direction (vx, vy, vz) (length rr > 0) on the RING map.
+__device__ __forceinline__ void deposit_direction(float vx, float vy, float vz, float rr, float w, int nside,
+                                                  int scheme, float* __restrict__ map) {
+  const long long npix = 12LL * nside * nside;
+  const double dr = (double)rr;
+  const double zc = (double)vz / dr;
+  const double phi = atan2((double)vy, (double)vx);
+  if (scheme == 0) {
+    const long long pix = ang2pix_ring(zc, phi, nside);
+    if (pix >= 0 && pix < npix) atomicAdd(map + pix, w);
+  } else {
+    long long pix[4];
+    double wt[4];
+    interp_weights(acos(fmin(1.0, fmax(-1.0, zc))), phi, nside, pix, wt);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (pix[q] >= 0 && pix[q] < npix) atomicAdd(map + pix[q], (float)(wt[q] * (double)w));
+  }
+}
+
 __global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, const float* __restrict__ weights,
                                 float weight, MeshDims d, float3 cell, float3 obs, float rmin, float rmax, int nside,
                                 int scheme, float* __restrict__ map) {
@@ -184,20 +206,116 @@ __global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, co
     const float vx = gx * cell.x - obs.x, vy = gy * cell.y - obs.y, vz = gz * cell.z - obs.z;
     const float rr = sqrtf(vx * vx + vy * vy + vz * vz);
     if (!(rr > rmin && rr <= rmax)) continue;
-    const float w = weights ? weights[p] * weight : weight;
-    const double dr = (double)rr;
-    const double zc = (double)vz / dr;
-    const double phi = atan2((double)vy, (double)vx);
-    if (scheme == 0) {
-      const long long pix = ang2pix_ring(zc, phi, nside);
-      if (pix >= 0 && pix < npix) atomicAdd(map + pix, w);
+    deposit_direction(vx, vy, vz, rr, weights ? weights[p] * weight : weight, nside, scheme, map);
+  }
+}
+
+// Tiled shell painting (OnionTiler._paint_tiled_27, pm/interp.py:418-504, and
+// TelephotoInterp._paint_telephoto, pm/interp.py:643-699). Every particle is read once and
+// placed in each of the tiles in turn: its observer-centred position c = x - o (x in
+// Mpc/h) becomes q = M c + s with M a signed permutation matrix (exact in FP32) and s the
+// tile's shift. With the light-cone drift on, q is drifted with the rotated momentum
+// M v by (Gp(a_t) - Gp(t)) / dGfa(sqrt(t a_t)), a_t = a_of_chi(distance):
+//   onion:     x' = q + o, distance |x' - o|, x' += D M v
+//   telephoto: distance |q - o| (the reference measures it from the observer-centred q),
+//              q += D M v, x' = q + o
+// and x' is painted on the shell rmin < |x' - o| <= rmax.
+//
+// Copies that cannot reach the shell are skipped before the drift. With D bounded by
+// dbound (the host's bound on |D| over the distance table: the Gp difference is at most
+// max(Gp(t), 1 - Gp(t)) after the clip to [0, 1], and dGfa is at least its smallest table
+// value over the scale factors sqrt(t a) reachable), the painted distance lies within
+// dbound |v| of |q|. A copy whose drift distance is beyond the table (extrapolated) is
+// always evaluated in full.
+struct TileSet {
+  int n;
+  signed char m[kMaxTiles][9];
+  float shift[kMaxTiles][3];
+};
+
+__global__ void k_healpix_paint_tiled(const float* __restrict__ disp, int absolute, const float* __restrict__ vel,
+                                      const float* __restrict__ weights, float weight, PGrid g, float3 box, float3 obs,
+                                      TileSet ts, int telephoto, float rmin, float rmax, float t, float gp_t,
+                                      float dbound, DriftTables tb, int nside, int scheme, float* __restrict__ map) {
+  const long long b = blockIdx.y;
+  const long long npix = 12LL * nside * nside;
+  disp += b * g.np * 3;
+  if (vel) vel += b * g.np * 3;
+  if (weights) weights += b * g.np;
+  map += b * npix;
+  const float nx = (float)g.nx, ny = (float)g.ny, nz = (float)g.nz;
+  const float chi_max = vel ? tb.chi[tb.n_chi - 1] : 0.f;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    float x, y, z;
+    if (absolute) {
+      x = disp[3 * p + 0] / nx * box.x;
+      y = disp[3 * p + 1] / ny * box.y;
+      z = disp[3 * p + 2] / nz * box.z;
     } else {
-      long long pix[4];
-      double wt[4];
-      interp_weights(acos(fmin(1.0, fmax(-1.0, zc))), phi, nside, pix, wt);
+      int i, j, k;
+      particle_ijk(g, p, i, j, k);
+      x = ((float)i + disp[3 * p + 0]) / nx * box.x;
+      y = ((float)j + disp[3 * p + 1]) / ny * box.y;
+      z = ((float)k + disp[3 * p + 2]) / nz * box.z;
+    }
+    const float c[3] = {x - obs.x, y - obs.y, z - obs.z};
+    float v[3] = {0.f, 0.f, 0.f}, vmag = 0.f;
+    if (vel) {
+      v[0] = vel[3 * p + 0];
+      v[1] = vel[3 * p + 1];
+      v[2] = vel[3 * p + 2];
+      vmag = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    }
+    const float w = weights ? weights[p] * weight : weight;
+    for (int tile = 0; tile < ts.n; ++tile) {
+      const signed char* M = ts.m[tile];
+      float q[3];
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (pix[q] >= 0 && pix[q] < npix) atomicAdd(map + pix[q], (float)(wt[q] * (double)w));
+      for (int r = 0; r < 3; ++r)
+        q[r] = (float)M[3 * r + 0] * c[0] + (float)M[3 * r + 1] * c[1] + (float)M[3 * r + 2] * c[2] + ts.shift[tile][r];
+      const float qn = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+      float px, py, pz;  // painted position, Mpc/h
+      if (vel) {
+        float dist;
+        if (telephoto) {
+          const float ex = q[0] - obs.x, ey = q[1] - obs.y, ez = q[2] - obs.z;
+          dist = sqrtf(ex * ex + ey * ey + ez * ez);
+        } else {
+          const float ex = (q[0] + obs.x) - obs.x, ey = (q[1] + obs.y) - obs.y, ez = (q[2] + obs.z) - obs.z;
+          dist = sqrtf(ex * ex + ey * ey + ez * ez);
+        }
+        if (dist <= chi_max) {
+          const float margin = dbound * vmag + 4e-3f + 4e-6f * qn;
+          if (qn + margin <= rmin || qn - margin > rmax) continue;
+        }
+        const float at = interp_table(dist, tb.chi, tb.a_chi, tb.n_chi);
+        const float ac = sqrtf(t * at);
+        const float gp_at = fminf(fmaxf(interp_table(at, tb.ga, tb.g, tb.n_g), 0.f), 1.f);
+        const float drift = (gp_at - gp_t) / interp_table(ac, tb.da, tb.dgfa, tb.n_d);
+        float vr[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+          vr[r] = (float)M[3 * r + 0] * v[0] + (float)M[3 * r + 1] * v[1] + (float)M[3 * r + 2] * v[2];
+        if (telephoto) {
+          px = (q[0] + drift * vr[0]) + obs.x;
+          py = (q[1] + drift * vr[1]) + obs.y;
+          pz = (q[2] + drift * vr[2]) + obs.z;
+        } else {
+          px = (q[0] + obs.x) + drift * vr[0];
+          py = (q[1] + obs.y) + drift * vr[1];
+          pz = (q[2] + obs.z) + drift * vr[2];
+        }
+      } else {
+        const float margin = 4e-3f + 4e-6f * qn;
+        if (qn + margin <= rmin || qn - margin > rmax) continue;
+        px = q[0] + obs.x;
+        py = q[1] + obs.y;
+        pz = q[2] + obs.z;
+      }
+      const float vx = px - obs.x, vy = py - obs.y, vz = pz - obs.z;
+      const float rr = sqrtf(vx * vx + vy * vy + vz * vz);
+      if (!(rr > rmin && rr <= rmax)) continue;
+      deposit_direction(vx, vy, vz, rr, w, nside, scheme, map);
     }
   }
 }
@@ -214,6 +332,25 @@ cudaError_t healpix_paint(const float* disp, int absolute, const float* weights,
   if (blocks > (long long)nsm * 16) blocks = (long long)nsm * 16;
   k_healpix_paint<<<dim3((unsigned)blocks, d.batch), 256, 0, s>>>(disp, absolute, weights, weight, d, cell, obs, rmin,
                                                                   rmax, nside, scheme, map);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t healpix_paint_tiled(const float* disp, int absolute, const float* vel, const float* weights, float weight,
+                                const MeshDims& d, const float* box, const float* observer, int ntiles,
+                                const signed char* rotations, const float* shifts, int telephoto, float rmin,
+                                float rmax, float t, float gp_t, float dbound, const DriftTables& tb, int nside,
+                                int scheme, float* map, cudaStream_t s) {
+  TileSet ts;
+  ts.n = ntiles;
+  for (int i = 0; i < ntiles; ++i) {
+    for (int e = 0; e < 9; ++e) ts.m[i][e] = rotations[9 * i + e];
+    for (int e = 0; e < 3; ++e) ts.shift[i][e] = shifts[3 * i + e];
+  }
+  k_healpix_paint_tiled<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(
+      disp, absolute, vel, weights, weight, make_pgrid(d), make_float3(box[0], box[1], box[2]),
+      make_float3(observer[0], observer[1], observer[2]), ts, telephoto, rmin, rmax, t, gp_t, dbound, tb, nside, scheme,
+      map);
   note_launch();
   return cudaGetLastError();
 }

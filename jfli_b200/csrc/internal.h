@@ -66,6 +66,21 @@ cudaError_t lpt2_source_adjoint(const float* pot, const float* sbar, float* q, f
                                 const MeshDims& d, cudaStream_t s);
 
 // ---- lightcone.cu ----
+// tables of the light-cone drift (chi -> a, growth D1, dGfa), all ascending
+struct DriftTables {
+  const float* chi;  // comoving distance (Mpc/h)
+  const float* a_chi;
+  int n_chi;
+  const float* ga;  // growth table scale factors
+  const float* g;   // D1 at ga
+  int n_g;
+  const float* da;  // dense scale-factor grid
+  const float* dgfa;
+  int n_d;
+};
+
+constexpr int kMaxTiles = 27;
+
 cudaError_t lightcone_drift(const float* disp, const float* vel, float* out, const float* box, const float* observer,
                             float t, float gp_t, const float* chi, const float* a_chi, int n_chi, const float* ga,
                             const float* gtab, int n_g, const float* da, const float* dgfa, int n_d, const MeshDims& d,
@@ -106,5 +121,10 @@ cudaError_t power_finalize(const double* partials, int nctas, int nbins, double*
 cudaError_t healpix_paint(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d,
                           const float* box, const float* observer, float rmin, float rmax, int nside, int scheme,
                           float* map, cudaStream_t s);
+cudaError_t healpix_paint_tiled(const float* disp, int absolute, const float* vel, const float* weights, float weight,
+                                const MeshDims& d, const float* box, const float* observer, int ntiles,
+                                const signed char* rotations, const float* shifts, int telephoto, float rmin,
+                                float rmax, float t, float gp_t, float dbound, const DriftTables& tb, int nside,
+                                int scheme, float* map, cudaStream_t s);
 
 }  // namespace jfli

@@ -15,18 +15,6 @@
 
 namespace jfli {
 
-struct DriftTables {
-  const float* chi;  // ascending comoving distance (Mpc/h)
-  const float* a_chi;
-  int n_chi;
-  const float* ga;  // growth table scale factors (ascending)
-  const float* g;   // D1 at ga
-  int n_g;
-  const float* da;  // dense scale-factor grid (ascending)
-  const float* dgfa;
-  int n_d;
-};
-
 __global__ void k_lightcone_drift(const float* __restrict__ disp, const float* __restrict__ vel,
                                   float* __restrict__ out, float lx, float ly, float lz, float ox, float oy,
                                   float oz, float t, float gp_t, DriftTables tb, PGrid g) {

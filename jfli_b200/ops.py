@@ -271,6 +271,78 @@ def drift_tables(cosmo, n_dense: int = 4096):
     return tuple(torch.as_tensor(np.ascontiguousarray(t, dtype=np.float32), device="cuda") for t in tabs)
 
 
+def drift_bound(tables, t: float, gp_t: float) -> float:
+    """Bound on |D| = |Gp(a_t) - Gp(t)| / dGfa(sqrt(t a_t)) as the drift kernels evaluate
+    it for any distance inside the distance table: the Gp difference is at most
+    max(Gp(t), 1 - Gp(t)) after the clip to [0, 1], and the interpolated dGfa is at least
+    the smallest value it takes over the reachable sqrt(t a_t) (table nodes, or the linear
+    extrapolation at the ends). Infinite when that minimum is not positive."""
+    chi, a_chi, ga, g, da, dg = (x.double().cpu().numpy() if isinstance(x, torch.Tensor) else np.asarray(x, np.float64)
+                                 for x in tables)
+    lo, hi = math.sqrt(t * float(a_chi.min())), math.sqrt(t * float(a_chi.max()))
+
+    def at(x):  # the kernels' linear interpolation with end extrapolation
+        i = int(np.clip(np.searchsorted(da, x, side="left") - 1, 0, len(da) - 2))
+        return dg[i] + (x - da[i]) * (dg[i + 1] - dg[i]) / (da[i + 1] - da[i])
+
+    inside = dg[(da >= lo) & (da <= hi)]
+    den = min([at(lo), at(hi)] + ([float(inside.min())] if inside.size else []))
+    if not den > 0:
+        return float("inf")
+    return max(gp_t, 1.0 - gp_t) / den * 1.001 + 1e-6
+
+
+def healpix_paint_tiled(pos: torch.Tensor, nside: int, box_size, observer_mpc, rmin: float, rmax: float, rotations,
+                        shifts, *, absolute: bool = False, vel: torch.Tensor | None = None, t: float | None = None,
+                        cosmo=None, telephoto: bool = False, scheme: str = "bilinear",
+                        weights: torch.Tensor | None = None, weight: float = 1.0, out: torch.Tensor | None = None,
+                        accumulate: bool = False, tables=None, dbound: float | None = None) -> torch.Tensor:
+    """Shell map of the rotated and shifted replicas of `pos` (one pass; see
+    jfli_healpix_paint_tiled). rotations (T, 3, 3) signed permutation matrices, shifts
+    (T, 3) in Mpc/h; with `vel` the replicas are drifted to the light cone at time t.
+    `dbound` replaces the computed drift bound (a larger one only skips fewer replicas)."""
+    from . import cosmology as cj
+
+    _check(pos, "pos")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    sch = {"ngp": _lib.JFLI_HEALPIX_NGP, "bilinear": _lib.JFLI_HEALPIX_BILINEAR}.get(scheme)
+    if sch is None:
+        raise NotImplementedError(f"spherical painting scheme {scheme!r} is not implemented (ngp, bilinear)")
+    rot = np.ascontiguousarray(np.rint(np.asarray(rotations, np.float64)).astype(np.int8).reshape(-1, 9))
+    sh = np.ascontiguousarray(np.asarray(shifts, np.float32).reshape(-1, 3))
+    if rot.shape[0] != sh.shape[0]:
+        raise ValueError(f"{rot.shape[0]} rotations for {sh.shape[0]} shifts")
+    if out is None:
+        out = torch.empty(*lead, 12 * nside * nside, dtype=torch.float32, device=pos.device)
+        accumulate = False
+    lx, ly, lz = (float(v) for v in box_size)
+    ox, oy, oz = (float(v) for v in observer_mpc)
+    tabs = (None,) * 6
+    t_arg = gp_t = 0.0
+    if vel is None:
+        dbound = 0.0
+    if vel is not None:
+        _check(vel, "vel")
+        if vel.shape != pos.shape:
+            raise ValueError("vel must have the shape of pos")
+        if t is None or cosmo is None:
+            raise ValueError("the light-cone drift needs the time t and the cosmology")
+        tabs = drift_tables(cosmo) if tables is None else tables
+        t_arg = float(t)
+        gp_t = float(cj.Gp(cosmo, t_arg))
+        if dbound is None:
+            dbound = drift_bound(tabs, t_arg, gp_t)
+        dbound = dbound if math.isfinite(dbound) else 1e30
+    chi, a_chi, ga, g, da, dg = tabs
+    n = lambda x: int(x.numel()) if x is not None else 0
+    call("jfli_healpix_paint_tiled", stream_ptr(), ptr(pos), int(absolute), ptr(vel), ptr(weights), float(weight),
+         lx, ly, lz, ox, oy, oz, int(rot.shape[0]), rot.ctypes.data_as(ctypes.POINTER(ctypes.c_byte)),
+         sh.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(bool(telephoto)), float(rmin), float(rmax), t_arg,
+         gp_t, float(dbound), ptr(chi), ptr(a_chi), n(chi), ptr(ga), ptr(g), n(ga), ptr(da), ptr(dg), n(da),
+         int(nside), sch, ptr(out), int(accumulate), nx, ny, nz, batch)
+    return out
+
+
 def lightcone_drift_array(disp: torch.Tensor, vel: torch.Tensor, t: float, cosmo, box_size, observer_mpc,
                           tables=None) -> torch.Tensor:
     """Drifted positions in Mpc/h of particles given as relative displacements."""

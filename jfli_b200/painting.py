@@ -40,3 +40,21 @@ def paint_shells(field, centers, widths, scheme="bilinear", weights=None, out=No
         ops.healpix_paint(pos, field.nside, field.box_size, field.observer_position_mpc, rmin, rmax, scheme=scheme,
                           absolute=absolute, weights=w, weight=scale, out=out[s])
     return out
+
+
+def paint_shell_tiled(field, vel, center: float, width: float, rotations, shifts, *, telephoto: bool = False,
+                      t: float | None = None, cosmo=None, scheme: str = "bilinear", weights=None) -> torch.Tensor:
+    """(12 nside^2,) map of one shell painted from rotated and shifted replicas of the
+    particles (OnionTiler / TelephotoInterp), each replica drifted to the light cone when
+    `vel` is given; normalised like paint_shells (number density per pixel volume)."""
+    if field.unit == PositionUnit.MPC_H:
+        field = field.to(PositionUnit.GRID_ABSOLUTE)
+    absolute = field.unit == PositionUnit.GRID_ABSOLUTE
+    w, ws = _weights_arg(weights)
+    rmin, rmax = float(center) - float(width) / 2.0, float(center) + float(width) / 2.0
+    vol = shell_volume_per_pixel(field.nside, rmin, rmax)
+    scale = ws / vol if vol > 0 else ws
+    v = vel.contiguous() if vel is not None else None
+    return ops.healpix_paint_tiled(field.array.contiguous(), field.nside, field.box_size, field.observer_position_mpc,
+                                   rmin, rmax, rotations, shifts, absolute=absolute, vel=v, t=t, cosmo=cosmo,
+                                   telephoto=telephoto, scheme=scheme, weights=w, weight=scale)

@@ -1,10 +1,11 @@
 """End-to-end forward models built from the public API.
 
 `lightcone_convergence` is the large light-cone chain of the reference's
-`make_full_field_model` (probabilistic_models/forward_model.py:24-79) with NoInterp
-spherical painting: white noise -> linear ICs -> LPT -> EfficientDriftDoubleKick (with an
-optional PGD correction) painting `nb_shells` HEALPix shells during the run -> Born
-convergence for the given source distributions. Every array stays on the GPU; the
+`make_full_field_model` (probabilistic_models/forward_model.py:24-79) with spherical
+painting (NoInterp inside the box, or OnionTiler replicas beyond it): white noise ->
+linear ICs -> LPT -> EfficientDriftDoubleKick (with an optional PGD correction) painting
+`nb_shells` HEALPix shells during the run -> Born convergence for the given source
+distributions. Every array stays on the GPU; the
 white noise is drawn on the device from the seed.
 """
 
@@ -34,8 +35,15 @@ def pgd_scales_to_grid(kl_hmpc: float, ks_hmpc: float, mesh: int, box: float):
 
 def lightcone_convergence(cosmo, *, mesh: int, box: float, seed: int, nb_shells: int, nside: int, nz_shear,
                           t0: float = 0.1, t1: float = 1.0, steps: int = 60, lpt_order: int = 2, pgd=None,
-                          min_z: float = 0.01, max_z: float = 1.0, n_integrate: int = 32) -> LightconeResult:
-    """pgd = (alpha, kl, ks) with kl, ks in h/Mpc, or None."""
+                          min_z: float = 0.01, max_z: float = 1.0, n_integrate: int = 32, tiler: str = "none",
+                          max_radius: float | None = None) -> LightconeResult:
+    """pgd = (alpha, kl, ks) with kl, ks in h/Mpc, or None.
+
+    tiler "none": nb_shells equal-width shells inside the box (NoInterp; radii up to the
+    largest sphere around the observer that the box holds, as nbody(nb_shells=...) gives).
+    tiler "onion": nb_shells equal-width shells from 0 to `max_radius` (default three times
+    that radius, which the 27 replicas cover completely around a centred observer), painted
+    with OnionTiler (replicas beyond the box, light-cone drift on)."""
     import jfli_b200 as jf
 
     timings = {}
@@ -57,11 +65,23 @@ def lightcone_convergence(cosmo, *, mesh: int, box: float, seed: int, nb_shells:
         alpha, kl, ks = pgd
         kl_g, ks_g = pgd_scales_to_grid(kl, ks, mesh, box)
         correction = jf.PGDKernel(alpha=float(alpha), kl=float(kl_g), ks=float(ks_g))
-    solver = jf.EfficientDriftDoubleKick(interp_kernel=jf.NoInterp(painting=jf.PaintingOptions(target="spherical")),
-                                         pgd_kernel=correction)
+    painting = jf.PaintingOptions(target="spherical")
+    if tiler == "none":
+        kernel, geom = jf.NoInterp(painting=painting), dict(nb_shells=nb_shells)
+    elif tiler == "onion":
+        from . import cosmology as cj
+
+        r_max = 3.0 * dx.max_comoving_radius if max_radius is None else float(max_radius)
+        edges = np.linspace(0.0, r_max, nb_shells + 1)[::-1]  # far -> near, as the time loop meets them
+        centres = 0.5 * (edges[1:] + edges[:-1])
+        kernel = jf.OnionTiler(painting=painting)
+        geom = dict(ts=np.asarray(cj.a_of_chi(cosmo, centres), np.float64), density_widths=edges[:-1] - edges[1:])
+    else:
+        raise ValueError(f"tiler must be 'none' or 'onion', not {tiler!r}")
+    solver = jf.EfficientDriftDoubleKick(interp_kernel=kernel, pgd_kernel=correction)
     t = time.perf_counter()
-    shells, run = jf.nbody(cosmo, dx, p, t0=t0, t1=t1, dt0=(t1 - t0) / steps, nb_shells=nb_shells, solver=solver,
-                           return_state=True)
+    shells, run = jf.nbody(cosmo, dx, p, t0=t0, t1=t1, dt0=(t1 - t0) / steps, solver=solver, return_state=True,
+                           **geom)
     sync()
     timings["nbody_s"] = time.perf_counter() - t
     n_steps = run.steps

@@ -2,7 +2,8 @@
 
 from .correction import AbstractCorrection, NoCorrection, PGDKernel, SharpeningKernel
 from .integrate import integrate, run_fused, run_stepwise, time_events
-from .interp import AbstractInterp, DriftInterp, InterpTilerState, NoInterp, OnionTiler, TelephotoInterp
+from .interp import (AbstractInterp, DriftInterp, InterpTilerState, NoInterp, OnionTiler, TelephotoInterp,
+                     get_all_47_symmetries)
 from .lpt import lpt, resolve_ts_geometry
 from .nbody import nbody
 from .solvers import AbstractNBodySolver, EfficientDriftDoubleKick, NBodyState, ReversibleDoubleKickDrift
@@ -12,4 +13,5 @@ __all__ = [
     "EfficientDriftDoubleKick", "ReversibleDoubleKickDrift", "AbstractNBodySolver", "NBodyState",
     "PGDKernel", "SharpeningKernel", "NoCorrection", "AbstractCorrection",
     "OnionTiler", "TelephotoInterp", "NoInterp", "DriftInterp", "InterpTilerState", "AbstractInterp",
+    "get_all_47_symmetries",
 ]

@@ -1,13 +1,16 @@
-"""Snapshot painters (reference pm/interp.py:46-318).
+"""Snapshot painters (reference pm/interp.py:46-699).
 
 `NoInterp` paints the particles as they are at the snapshot time; `DriftInterp` first
 drifts every particle to the scale factor at which its distance from the observer
-crosses the light cone. The shell index advances at each snapshot time.
+crosses the light cone. `OnionTiler` and `TelephotoInterp` paint shells beyond the box
+from rotated and shifted replicas of it. The shell index advances at each snapshot time.
 """
 
 from __future__ import annotations
 
 import dataclasses
+import itertools
+import math
 import warnings
 from typing import Any
 
@@ -49,7 +52,11 @@ class AbstractInterp:
         return InterpTilerState(rotation_idx=-1, shell_idx=-1, rotations=None)
 
     def _is_snapshot(self, t) -> bool:
-        return self.ts is not None and bool(np.isin(np.float64(t), np.asarray(self.ts, np.float64)))
+        """Whether t is one of the snapshot times. Compared in FP32, the precision of the
+        reference's time variables and of jnp.isin on its FP32 ts (pm/interp.py:148): the
+        time loop clips each step to the FP32 value of the next snapshot time, so the FP64
+        shell times (from the distance table) only match after the same rounding."""
+        return self.ts is not None and bool(np.isin(np.float32(t), np.asarray(self.ts, np.float32)))
 
     def advance(self, state: InterpTilerState, t) -> InterpTilerState:
         return dataclasses.replace(state, shell_idx=state.shell_idx + 1) if self._is_snapshot(t) else state
@@ -118,17 +125,150 @@ def drift_to_lightcone(dx, p, t: float, cosmo):
     return ops.lightcone_drift(dx, p, t, cosmo)
 
 
+def get_all_47_symmetries() -> np.ndarray:
+    """The 47 non-identity signed permutation matrices of the cube, (47, 3, 3) int
+    (reference pm/interp.py:31-43): sign triples in itertools.product((1, -1)) order outer,
+    axis permutations in itertools.permutations order inner, row i holding sign s_i in
+    column p_i; the first (the identity) is dropped. The order defines which matrix a
+    rotation index names."""
+    mats = []
+    for s in itertools.product([1, -1], repeat=3):
+        for p in itertools.permutations([0, 1, 2]):
+            m = np.zeros((3, 3), dtype=np.int16)
+            for i in range(3):
+                m[i, p[i]] = s[i]
+            mats.append(m)
+    return np.array(mats)[1:]
+
+
+def tile_shifts(observer_position, box_size) -> np.ndarray:
+    """(27, 3) Mpc/h shifts of the 27 replicas (reference pm/interp.py:441-444): the
+    offsets itertools.product((0, 1, -1), repeat=3), moved by +1 on axes where the
+    observer sits at fraction 0 and by -1 where it sits at 1, times the box size."""
+    sh = np.array(list(itertools.product([0, 1, -1], repeat=3)), dtype=np.int64)
+    obs = np.asarray(observer_position, dtype=np.float64)
+    sh = np.where(obs == 0, sh + 1, sh)
+    sh = np.where(obs == 1, sh - 1, sh)
+    return sh * np.asarray(box_size, dtype=np.float64)
+
+
+def _spherical_result(res, t, r_center, width):
+    from ..fields import DensityUnit, FieldStatus
+
+    return res.replace(status=FieldStatus.LIGHTCONE, unit=DensityUnit.DENSITY, scale_factors=t,
+                       comoving_centers=r_center, density_width=width)
+
+
 @dataclasses.dataclass(frozen=True)
 class OnionTiler(AbstractInterp):
-    """27-tile spherical painting (reference pm/interp.py:321-504); not on the B200 path yet."""
+    """27-replica spherical painting with random cube symmetries (reference
+    pm/interp.py:321-504). A shell inside the box (outer edge within the largest sphere
+    around the observer that the box holds) is painted from the particles as they are;
+    a shell beyond it from the 27 replicas of the box around the observer, replica i
+    rotated by its own symmetry. All replicas are painted in one pass over the particles.
+    With drift_on_lightcone each particle (each replica) is first drifted to its
+    light-cone crossing.
+
+    The reference draws the 27 rotation indices with jax.random.randint(PRNGKey(42), (27,),
+    0, 47); JAX is not available here, so `rotation_indices` takes them explicitly (for
+    maps identical to the reference's, pass those indices) and otherwise they are drawn
+    with numpy.random.default_rng(rotation_seed)."""
 
     drift_on_lightcone: bool = True
+    rotation_indices: tuple | None = None
+    rotation_seed: int = 42
+
+    def needs_velocity(self) -> bool:
+        return self.drift_on_lightcone
+
+    def init(self) -> InterpTilerState:
+        if self.painting is None or self.painting.target != "spherical":
+            raise ValueError("OnionTiler only supports spherical painting.")
+        if self.rotation_indices is not None:
+            idx = np.asarray(self.rotation_indices, dtype=np.int64)
+            if idx.shape != (27,) or idx.min() < 0 or idx.max() > 46:
+                raise ValueError("rotation_indices must be 27 integers in [0, 46]")
+        else:
+            idx = np.random.default_rng(self.rotation_seed).integers(0, 47, size=27)
+        return InterpTilerState(rotation_idx=-1, shell_idx=-1, rotations=get_all_47_symmetries()[idx])
 
     def paint(self, state, t, y, cosmo):
-        raise NotImplementedError("OnionTiler is not on the B200 path")
+        dx, p = y
+        r_center = float(self.r_centers[state.shell_idx])
+        width = float(self.density_widths[state.shell_idx])
+        pt = self.painting
+        if r_center + width / 2 <= self.max_comoving_distance:
+            src = drift_to_lightcone(dx, p, float(t), cosmo) if self.drift_on_lightcone else dx
+            res = self._paint_target(src, r_center, width)
+        else:
+            from ..fields import SphericalDensity
+            from ..painting import paint_shell_tiled
+
+            shifts = tile_shifts(dx.observer_position, dx.box_size)
+            m = paint_shell_tiled(dx, p.array if self.drift_on_lightcone else None, r_center, width, state.rotations,
+                                  shifts, telephoto=False, t=float(t), cosmo=cosmo, scheme=pt.scheme,
+                                  weights=pt.weights)
+            res = SphericalDensity.FromDensityMetadata(array=m, field=dx)
+        return _spherical_result(res, t, r_center, width)
 
 
 @dataclasses.dataclass(frozen=True)
 class TelephotoInterp(AbstractInterp):
+    """One rotated and shifted replica per shell beyond the box, for narrow fields of view
+    (reference pm/interp.py:507-699). The rotation index advances at each snapshot whose
+    shell centre lies beyond the box; the replica is the box rotated by the index's cube
+    symmetry (of the 47, cyclically) and pushed along z by floor(r / R) R, R the largest
+    radius the box holds. The drift distance is measured as the reference measures it,
+    from the observer-centred replica minus the observer's position. Spherical painting
+    only: the flat-sky painter is not built."""
+
+    drift_on_lightcone: bool = True
+
+    def needs_velocity(self) -> bool:
+        return self.drift_on_lightcone
+
+    def init(self) -> InterpTilerState:
+        tgt = self.painting.target if self.painting is not None else None
+        if tgt not in ("spherical", "flat"):
+            raise ValueError("TelephotoInterp only supports projections (flat or spherical).")
+        if tgt == "flat":
+            raise NotImplementedError("flat-sky painting is not on the B200 path")
+        warnings.warn("TelephotoInterp is designed for narrow FOV flat-sky projections. Using it for spherical "
+                      "painting will cause significant artifacts. use for illustriative purposes only.")
+        return InterpTilerState(rotation_idx=-1, shell_idx=-1, rotations=get_all_47_symmetries())
+
+    def advance(self, state, t):
+        if not self._is_snapshot(t):
+            return state
+        nxt = state.shell_idx + 1
+        inside = float(self.r_centers[nxt]) <= self.max_comoving_distance
+        return dataclasses.replace(state, shell_idx=nxt, rotation_idx=state.rotation_idx + (0 if inside else 1))
+
+    def rewind(self, state, t):
+        if not self._is_snapshot(t):
+            return state
+        rc = float(self.r_centers[state.shell_idx])
+        wd = float(self.density_widths[state.shell_idx])
+        outside = rc + wd / 2 > self.max_comoving_distance
+        return dataclasses.replace(state, shell_idx=state.shell_idx - 1,
+                                   rotation_idx=state.rotation_idx - (1 if outside else 0))
+
     def paint(self, state, t, y, cosmo):
-        raise NotImplementedError("TelephotoInterp is not on the B200 path")
+        dx, p = y
+        r_center = float(self.r_centers[state.shell_idx])
+        width = float(self.density_widths[state.shell_idx])
+        pt = self.painting
+        if r_center <= self.max_comoving_distance:
+            src = drift_to_lightcone(dx, p, float(t), cosmo) if self.drift_on_lightcone else dx
+            res = self._paint_target(src, r_center, width)
+        else:
+            from ..fields import SphericalDensity
+            from ..painting import paint_shell_tiled
+
+            rot = state.rotations[state.rotation_idx % 47][None]
+            R = self.max_comoving_distance
+            shift = np.array([[0.0, 0.0, math.floor(r_center / R) * R]])
+            m = paint_shell_tiled(dx, p.array if self.drift_on_lightcone else None, r_center, width, rot, shift,
+                                  telephoto=True, t=float(t), cosmo=cosmo, scheme=pt.scheme, weights=pt.weights)
+            res = SphericalDensity.FromDensityMetadata(array=m, field=dx)
+        return res.replace(scale_factors=t, comoving_centers=r_center, density_width=width)

@@ -148,3 +148,39 @@ def paint_shell(pos_mpc, observer, rmin, rmax, nside, scheme="bilinear", weight=
         return np.bincount(pix, minlength=npix) * weight
     pix, w = get_interp_weights(nside, theta, phi)
     return np.bincount(pix.ravel(), weights=w.ravel() * weight, minlength=npix)
+
+
+def paint_shell_tiled(disp, vel, box, observer, rmin, rmax, nside, rotations, shifts, *, telephoto=False, t=None,
+                      a_of_chi=None, Gp=None, dGfa=None, scheme="bilinear", weight=1.0):
+    """Raw weight sums of the rotated and shifted replicas of the particles (FP64), every
+    replica evaluated (no skipping). OnionTiler._paint_tiled_27 (reference
+    pm/interp.py:418-504) and TelephotoInterp._paint_telephoto (pm/interp.py:643-699):
+    c = x - o with x = (grid + disp) / N * L; q = R c + s; with velocities, the replica is
+    drifted by (Gp(a_t) - Gp(t)) / dGfa(sqrt(t a_t)) along R v, a_t = a_of_chi(distance),
+    the distance being |q + o - o| (onion) or |q - o| (telephoto, as the reference
+    measures it); the painted position is q + o (+ the drift)."""
+    shape = disp.shape[:3]
+    n = np.asarray(shape, np.float64)
+    L = np.asarray(box, np.float64)
+    o = np.asarray(observer, np.float64)
+    g = np.stack(np.meshgrid(*[np.arange(k, dtype=np.float64) for k in shape], indexing="ij"), axis=-1)
+    x = (g + disp.astype(np.float64)) / n * L
+    c = (x - o).reshape(-1, 3)
+    v = vel.astype(np.float64).reshape(-1, 3) if vel is not None else None
+    npix = 12 * nside * nside
+    out = np.zeros(npix)
+    for R, s in zip(np.asarray(rotations, np.float64), np.asarray(shifts, np.float64)):
+        q = c @ R.T + s
+        if v is None:
+            pos = q + o
+        else:
+            vr = v @ R.T
+            if telephoto:
+                dist = np.linalg.norm(q - o, axis=-1)
+            else:
+                dist = np.linalg.norm((q + o) - o, axis=-1)
+            at = a_of_chi(dist)
+            d = (Gp(at) - Gp(t)) / dGfa(np.sqrt(t * at))
+            pos = (q + d[:, None] * vr) + o if telephoto else (q + o) + d[:, None] * vr
+        out += paint_shell(pos, o, rmin, rmax, nside, scheme, weight)
+    return out

@@ -117,3 +117,27 @@ def test_no_cpu_fallback_in_product():
             if f.endswith(".py"):
                 src = open(os.path.join(dirpath, f)).read()
                 assert "oracle" not in re.sub(r"#.*", "", src).replace('"""', ""), f
+
+
+def test_tiled_paint_checks_rotations(lib):
+    """jfli_healpix_paint_tiled takes signed permutation matrices only (the exactness of
+    the replica rotation in FP32 rests on it), and at most 27 replicas."""
+    from jfli_b200 import _lib
+
+    res, args = _lib._SIGNATURES["jfli_healpix_paint_tiled"]
+    fn = lib.jfli_healpix_paint_tiled
+    fn.restype, fn.argtypes = res, args
+    buf = ctypes.create_string_buffer(256)
+
+    def call(rot, ntiles=None):
+        r = (ctypes.c_byte * 9 * len(rot))(*[(ctypes.c_byte * 9)(*m) for m in rot])
+        s = (ctypes.c_float * (3 * len(rot)))()
+        return fn(None, ctypes.c_void_p(256), 0, None, None, 1.0, 100.0, 100.0, 100.0, 50.0, 50.0, 50.0,
+                  len(rot) if ntiles is None else ntiles, ctypes.cast(r, ctypes.POINTER(ctypes.c_byte)),
+                  ctypes.cast(s, ctypes.POINTER(ctypes.c_float)), 0, 10.0, 20.0, 0.0, 0.0, 0.0, None, None, 0, None,
+                  None, 0, None, None, 0, 4, 1, ctypes.c_void_p(256), 0, 16, 16, 16, 1, buf, 256)
+
+    assert call([[1, 0, 0, 0, 1, 0, 1, 0, 0]]) == 1 and b"signed permutation" in buf.value  # column used twice
+    assert call([[2, 0, 0, 0, 1, 0, 0, 0, 1]]) == 1 and b"signed permutation" in buf.value
+    assert call([[1, 0, 0, 0, 0, 0, 0, 0, 1]]) == 1 and b"signed permutation" in buf.value  # empty row
+    assert call([[1, 0, 0, 0, 1, 0, 0, 0, 1]], ntiles=28) == 1 and b"ntiles" in buf.value
