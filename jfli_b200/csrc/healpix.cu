@@ -11,6 +11,12 @@
 // Angles are computed in FP64 from the FP32 positions.
 #include <math.h>
 
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <utility>
+#include <vector>
+
 #include "cic.cuh"
 #include "common.cuh"
 #include "internal.h"
@@ -25,29 +31,24 @@ struct RingInfo {
   int shifted;
 };
 
-__device__ __forceinline__ RingInfo ring_info(int ring, int nside) {
+// Ring geometry: start pixel, pixel count and half-pixel shift from integer arithmetic;
+// the colatitude from the table of the rings' FP64 colatitudes (ring_theta_table).
+__device__ __forceinline__ RingInfo ring_info_tab(int ring, int nside, const double* __restrict__ theta_tab) {
   const long long npix = 12LL * nside * nside;
   const long long ncap = 2LL * nside * (nside - 1);
   const int north = ring > 2 * nside ? 4 * nside - ring : ring;
   RingInfo r;
   if (north < nside) {
-    const double tmp = (double)north * north * (4.0 / (double)npix);
-    const double cth = 1.0 - tmp;
-    const double sth = sqrt(tmp * (2.0 - tmp));
-    r.theta = atan2(sth, cth);
     r.npix = 4 * north;
     r.shifted = 1;
     r.start = 2LL * north * (north - 1);
   } else {
-    r.theta = acos((double)(2 * nside - north) * (2.0 / (3.0 * nside)));
     r.npix = 4 * nside;
     r.shifted = ((north - nside) & 1) == 0;
     r.start = ncap + (long long)(north - nside) * 4 * nside;
   }
-  if (north != ring) {
-    r.theta = M_PI - r.theta;
-    r.start = npix - r.start - r.npix;
-  }
+  if (north != ring) r.start = npix - r.start - r.npix;
+  r.theta = __ldg(theta_tab + ring);
   return r;
 }
 
@@ -92,7 +93,8 @@ __device__ __forceinline__ long long ang2pix_ring(double z, double phi, int nsid
 
 // Bilinear interpolation pixels and weights (the 4-neighbour scheme of HEALPix
 // get_interpol / healpy get_interp_weights, RING ordering).
-__device__ __forceinline__ void interp_weights(double theta, double phi, int nside, long long pix[4], double w[4]) {
+__device__ __forceinline__ void interp_weights(double theta, double phi, int nside, const double* __restrict__ theta_tab,
+                                               long long pix[4], double w[4]) {
   const double twopi = 2.0 * M_PI;
   double ph = fmod(phi, twopi);
   if (ph < 0) ph += twopi;
@@ -102,7 +104,7 @@ __device__ __forceinline__ void interp_weights(double theta, double phi, int nsi
   const int ir2 = ir1 + 1;
   double theta1 = 0.0, theta2 = 0.0;
   if (ir1 > 0) {
-    const RingInfo r = ring_info(ir1, nside);
+    const RingInfo r = ring_info_tab(ir1, nside, theta_tab);
     theta1 = r.theta;
     const double dphi = twopi / r.npix;
     const double tmp = ph / dphi - 0.5 * r.shifted;
@@ -117,7 +119,7 @@ __device__ __forceinline__ void interp_weights(double theta, double phi, int nsi
     w[1] = wp;
   }
   if (ir2 < 4 * nside) {
-    const RingInfo r = ring_info(ir2, nside);
+    const RingInfo r = ring_info_tab(ir2, nside, theta_tab);
     theta2 = r.theta;
     const double dphi = twopi / r.npix;
     const double tmp = ph / dphi - 0.5 * r.shifted;
@@ -164,7 +166,8 @@ __device__ __forceinline__ void interp_weights(double theta, double phi, int nsi
 
 // Deposit of weight w at direction (vx, vy, vz) (length rr > 0) on the RING map.
 __device__ __forceinline__ void deposit_direction(float vx, float vy, float vz, float rr, float w, int nside,
-                                                  int scheme, float* __restrict__ map) {
+                                                  int scheme, const double* __restrict__ theta_tab,
+                                                  float* __restrict__ map) {
   const long long npix = 12LL * nside * nside;
   const double dr = (double)rr;
   const double zc = (double)vz / dr;
@@ -175,7 +178,7 @@ __device__ __forceinline__ void deposit_direction(float vx, float vy, float vz, 
   } else {
     long long pix[4];
     double wt[4];
-    interp_weights(acos(fmin(1.0, fmax(-1.0, zc))), phi, nside, pix, wt);
+    interp_weights(acos(fmin(1.0, fmax(-1.0, zc))), phi, nside, theta_tab, pix, wt);
 #pragma unroll
     for (int q = 0; q < 4; ++q)
       if (pix[q] >= 0 && pix[q] < npix) atomicAdd(map + pix[q], (float)(wt[q] * (double)w));
@@ -184,7 +187,7 @@ __device__ __forceinline__ void deposit_direction(float vx, float vy, float vz, 
 
 __global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, const float* __restrict__ weights,
                                 float weight, MeshDims d, float3 cell, float3 obs, float rmin, float rmax, int nside,
-                                int scheme, float* __restrict__ map) {
+                                int scheme, const double* __restrict__ theta_tab, float* __restrict__ map) {
   const long long np = d.cells();
   const long long npix = 12LL * nside * nside;
   const int b = blockIdx.y;
@@ -206,7 +209,7 @@ __global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, co
     const float vx = gx * cell.x - obs.x, vy = gy * cell.y - obs.y, vz = gz * cell.z - obs.z;
     const float rr = sqrtf(vx * vx + vy * vy + vz * vz);
     if (!(rr > rmin && rr <= rmax)) continue;
-    deposit_direction(vx, vy, vz, rr, weights ? weights[p] * weight : weight, nside, scheme, map);
+    deposit_direction(vx, vy, vz, rr, weights ? weights[p] * weight : weight, nside, scheme, theta_tab, map);
   }
 }
 
@@ -233,10 +236,11 @@ struct TileSet {
   float shift[kMaxTiles][3];
 };
 
-__global__ void k_healpix_paint_tiled(const float* __restrict__ disp, int absolute, const float* __restrict__ vel,
-                                      const float* __restrict__ weights, float weight, PGrid g, float3 box, float3 obs,
-                                      TileSet ts, int telephoto, float rmin, float rmax, float t, float gp_t,
-                                      float dbound, DriftTables tb, int nside, int scheme, float* __restrict__ map) {
+__global__ void __launch_bounds__(256, 4)
+    k_healpix_paint_tiled(const float* __restrict__ disp, int absolute, const float* __restrict__ vel,
+                          const float* __restrict__ weights, float weight, PGrid g, float3 box, float3 obs, TileSet ts,
+                          int telephoto, float rmin, float rmax, float t, float gp_t, float dbound, DriftTables tb,
+                          int nside, int scheme, const double* __restrict__ theta_tab, float* __restrict__ map) {
   const long long b = blockIdx.y;
   const long long npix = 12LL * nside * nside;
   disp += b * g.np * 3;
@@ -315,9 +319,46 @@ __global__ void k_healpix_paint_tiled(const float* __restrict__ disp, int absolu
       const float vx = px - obs.x, vy = py - obs.y, vz = pz - obs.z;
       const float rr = sqrtf(vx * vx + vy * vy + vz * vz);
       if (!(rr > rmin && rr <= rmax)) continue;
-      deposit_direction(vx, vy, vz, rr, w, nside, scheme, map);
+      deposit_direction(vx, vy, vz, rr, w, nside, scheme, theta_tab, map);
     }
   }
+}
+
+// FP64 colatitudes of rings 0 .. 4 nside (entries 0 and 4 nside unused), one table per
+// (device, nside), built once on the host: polar-cap rings from z = 1 - north^2 4 / npix
+// (colatitude via atan2 of sin and cos), equatorial rings from z = (2 nside - north) 2 / (3 nside).
+static std::mutex g_ring_mutex;
+static std::map<std::pair<int, int>, double*> g_ring_tables;
+
+static const double* ring_theta_table(int nside) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_ring_mutex);
+  const auto key = std::make_pair(dev, nside);
+  const auto it = g_ring_tables.find(key);
+  if (it != g_ring_tables.end()) return it->second;
+  const int nr = 4 * nside + 1;
+  const double npix = 12.0 * nside * nside;
+  std::vector<double> h(nr, 0.0);
+  for (int ring = 1; ring < 4 * nside; ++ring) {
+    const int north = ring > 2 * nside ? 4 * nside - ring : ring;
+    double th;
+    if (north < nside) {
+      const double tmp = (double)north * north * (4.0 / npix);
+      th = std::atan2(std::sqrt(tmp * (2.0 - tmp)), 1.0 - tmp);
+    } else {
+      th = std::acos((double)(2 * nside - north) * (2.0 / (3.0 * nside)));
+    }
+    h[ring] = north != ring ? M_PI - th : th;
+  }
+  double* d = nullptr;
+  if (cudaMalloc(&d, sizeof(double) * nr) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(d, h.data(), sizeof(double) * nr, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  g_ring_tables[key] = d;
+  return d;
 }
 
 cudaError_t healpix_paint(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d,
@@ -330,8 +371,10 @@ cudaError_t healpix_paint(const float* disp, int absolute, const float* weights,
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   long long blocks = (d.cells() + 255) / 256;
   if (blocks > (long long)nsm * 16) blocks = (long long)nsm * 16;
+  const double* tab = ring_theta_table(nside);
+  if (!tab) return cudaErrorMemoryAllocation;
   k_healpix_paint<<<dim3((unsigned)blocks, d.batch), 256, 0, s>>>(disp, absolute, weights, weight, d, cell, obs, rmin,
-                                                                  rmax, nside, scheme, map);
+                                                                  rmax, nside, scheme, tab, map);
   note_launch();
   return cudaGetLastError();
 }
@@ -347,10 +390,12 @@ cudaError_t healpix_paint_tiled(const float* disp, int absolute, const float* ve
     for (int e = 0; e < 9; ++e) ts.m[i][e] = rotations[9 * i + e];
     for (int e = 0; e < 3; ++e) ts.shift[i][e] = shifts[3 * i + e];
   }
+  const double* tab = ring_theta_table(nside);
+  if (!tab) return cudaErrorMemoryAllocation;
   k_healpix_paint_tiled<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(
       disp, absolute, vel, weights, weight, make_pgrid(d), make_float3(box[0], box[1], box[2]),
       make_float3(observer[0], observer[1], observer[2]), ts, telephoto, rmin, rmax, t, gp_t, dbound, tb, nside, scheme,
-      map);
+      tab, map);
   note_launch();
   return cudaGetLastError();
 }
