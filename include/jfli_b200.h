@@ -32,6 +32,10 @@
  *   jfli_healpix_paint     <- _src/fields/_painting.py:249-348 (jaxpm paint_particles_spherical)
  *   jfli_lightcone_drift   <- pm/interp.py:110-121 (_drift_to_time) as used by DriftInterp.paint
  *                             (pm/interp.py:254-318)
+ *   jfli_paint_flat        <- _src/fields/_painting.py:117-202 (_single_paint_2d, jaxpm cic_paint_2d)
+ *                             behind ParticleField.paint_2d (fields/particles.py:234-320)
+ *   jfli_flat_cl           <- _src/power/_compute.py:122-172 (_flat_cl) behind
+ *                             FlatDensity.angular_cl (fields/lightcone.py:197-233)
  *   jfli_healpix_paint_tiled <- OnionTiler._paint_tiled_27 (pm/interp.py:418-504) and
  *                             TelephotoInterp._paint_telephoto (pm/interp.py:643-699): the
  *                             rotated, shifted (and drifted) replicas painted in one pass
@@ -188,6 +192,25 @@ int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, cons
                              const float* ga, const float* g, int n_g, const float* da, const float* dgfa, int n_d,
                              int nside, int scheme, float* map, int accumulate, int nx, int ny, int nz, int batch,
                              char* err, size_t errlen);
+
+/* Flat-sky plane of the particles with zlo < z <= zhi (absolute grid units along z, from
+ * the box origin): x and y scaled to the map (npx / nx, npy / ny), wrapped, deposited with
+ * 2D CIC weights on map[batch][npx][npy]; weights * weight per particle (raw sums: divide by
+ * the pixel volume for DENSITY units). accumulate = 0 clears the map first. */
+int jfli_paint_flat(void* stream, const float* disp, int absolute, const float* weights, float weight, float zlo,
+                    float zhi, int npx, int npy, float* map, int accumulate, int nx, int ny, int nz, int batch,
+                    char* err, size_t errlen);
+
+/* Flat-sky angular power sums of maps [batch][npx][npy] (auto, or cross with map2):
+ * Re(F1 conj F2) of the full 2D FFT grid binned by ell = |2 pi fftfreq(n, d)| with
+ * numpy.digitize on ell_edges (FP32 ascending, nedges <= 1024); dnx = npx * d_x and
+ * dny = npy * d_y (radians). out[batch][3][nedges+1] (FP64): sum of power, mode count, sum
+ * of ell; bins 0 and nedges are the under/overflow bins. The normalisation
+ * (d_x d_y) / (npx npy) is the caller's. Workspace: jfli_flat_cl_workspace_bytes. */
+size_t jfli_flat_cl_workspace_bytes(int npx, int npy, int batch, int nedges, int cross);
+int jfli_flat_cl(void* stream, const float* map1, const float* map2, int npx, int npy, int batch, float dnx,
+                 float dny, const float* ell_edges, int nedges, double* out, void* workspace, size_t workspace_bytes,
+                 char* err, size_t errlen);
 
 /* Positions (Mpc/h) of the particles drifted to their light-cone crossing:
  *   x = (grid index + disp) / N * L;  a_t = interp(|x - observer|; chi, a_chi);

@@ -16,6 +16,7 @@ from .fields import (
     ParticleField,
     PhysicalUnit,
     PositionUnit,
+    FlatDensity,
     PowerSpectrum,
     SphericalDensity,
     convert_units,
@@ -39,7 +40,7 @@ from .pm import (
     lpt,
     nbody,
 )
-from .power import power
+from .power import angular_cl_flat, power
 from .utils import (
     centers,
     compute_box_size_from_redshift,

@@ -90,6 +90,16 @@ _SIGNATURES = {
         c_int,
         [c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_void_p, *_DIMS, *_ERR],
     ),
+    "jfli_paint_flat": (
+        c_int,
+        [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_int, c_int, c_void_p, c_int, *_DIMS, *_ERR],
+    ),
+    "jfli_flat_cl_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_int, c_int]),
+    "jfli_flat_cl": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float, c_void_p, c_int, c_void_p, c_void_p,
+         c_size_t, *_ERR],
+    ),
     "jfli_healpix_paint_tiled": (
         c_int,
         [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float, c_float,

@@ -483,6 +483,61 @@ int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, cons
                      err, errlen, "jfli_healpix_paint_tiled");
 }
 
+int jfli_paint_flat(void* stream, const float* disp, int absolute, const float* weights, float weight, float zlo,
+                    float zhi, int npx, int npy, float* map, int accumulate, int nx, int ny, int nz, int batch,
+                    char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(map);
+  if (npx < 1 || npy < 1 || (long long)npx * npy > (1LL << 30))
+    return fail(err, errlen, JFLI_EINVAL, "flat-sky map (%d, %d) outside [1, 2^30] pixels", npx, npy);
+  const MeshDims d{nx, ny, nz, batch};
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!accumulate) {
+    cudaError_t e = cudaMemsetAsync(map, 0, sizeof(float) * (size_t)npx * npy * batch, s);
+    if (e != cudaSuccess) return cuda_status(e, err, errlen, "jfli_paint_flat memset");
+  }
+  return cuda_status(jfli::paint_flat(disp, absolute, weights, weight, d, npx, npy, zlo, zhi, map, s), err, errlen,
+                     "jfli_paint_flat");
+}
+
+static bool flat_fft_supported(int npx, int npy) {
+  return npy % 2 == 0 && npy >= 4 && jfli::fft_axis_supported(npx) && jfli::fft_axis_supported(npy / 2);
+}
+
+size_t jfli_flat_cl_workspace_bytes(int npx, int npy, int batch, int nedges, int cross) {
+  if (npx < 1 || npy < 2 || batch < 1 || nedges < 1) return 0;
+  const size_t spec = align256(sizeof(float) * 2 * (size_t)npx * (npy / 2 + 1) * batch);
+  return spec * (cross ? 2 : 1) +
+         align256(sizeof(double) * 3 * (size_t)(nedges + 1) * jfli::flat_cl_ctas(npx, npy) * batch);
+}
+
+int jfli_flat_cl(void* stream, const float* map1, const float* map2, int npx, int npy, int batch, float dnx,
+                 float dny, const float* ell_edges, int nedges, double* out, void* workspace, size_t workspace_bytes,
+                 char* err, size_t errlen) {
+  CHECK_PTR(map1);
+  CHECK_PTR(ell_edges);
+  CHECK_PTR(out);
+  CHECK_PTR(workspace);
+  if (batch < 1) return fail(err, errlen, JFLI_EINVAL, "batch must be >= 1");
+  if (!flat_fft_supported(npx, npy))
+    return fail(err, errlen, JFLI_EUNSUPPORTED,
+                "flat-sky map (%d, %d) unsupported: npx must be 2^a 3^b <= 4096, npy even with npy/2 2^a 3^b", npx,
+                npy);
+  if (nedges < 1 || nedges > 1024) return fail(err, errlen, JFLI_EINVAL, "nedges %d outside [1, 1024]", nedges);
+  if (!(dnx > 0 && dny > 0)) return fail(err, errlen, JFLI_EINVAL, "n * pixel size must be positive");
+  const size_t need = jfli_flat_cl_workspace_bytes(npx, npy, batch, nedges, map2 != nullptr);
+  if (workspace_bytes < need)
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  const size_t spec = align256(sizeof(float) * 2 * (size_t)npx * (npy / 2 + 1) * batch);
+  float2* s1 = (float2*)workspace;
+  float2* s2 = map2 ? (float2*)((char*)workspace + spec) : nullptr;
+  double* partials = (double*)((char*)workspace + spec * (map2 ? 2 : 1));
+  return cuda_status(jfli::flat_cl(map1, map2, npx, npy, batch, dnx, dny, ell_edges, nedges, s1, s2, partials, out,
+                                   (cudaStream_t)stream),
+                     err, errlen, "jfli_flat_cl");
+}
+
 // P(k) for callers that cannot allocate device memory: the same sums as
 // jfli_power_spectrum, with the half spectrum and the histogram partials kept in a
 // fixed device array inside the library instead of a caller workspace. The array is

@@ -769,6 +769,13 @@ cudaError_t rfft3d_forward(const float* in, float2* spec, const MeshDims& d, flo
   return launch_cols<-1>(spec, x_geom(d), d.spec_elems(), d.batch, s);
 }
 
+// 2D r2c of (ny, nz) maps: the z and y passes of rfft3d_forward on a mesh with nx = 1
+cudaError_t rfft2d_forward(const float* in, float2* spec, const MeshDims& d, cudaStream_t s) {
+  cudaError_t e = launch_rfft_z(in, spec, d, 0.0f, s);
+  if (e != cudaSuccess) return e;
+  return launch_cols<-1>(spec, y_geom(d), d.spec_elems(), d.batch, s);
+}
+
 cudaError_t rfft3d_inverse(float2* spec, float* out, const MeshDims& d, float scale, cudaStream_t s) {
   cudaError_t e = launch_cols<1>(spec, x_geom(d), d.spec_elems(), d.batch, s);
   if (e != cudaSuccess) return e;

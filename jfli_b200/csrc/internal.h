@@ -22,6 +22,7 @@ bool mesh_fft_supported(int nx, int ny, int nz);
 int x_pass_ctas(const MeshDims& d);
 cudaError_t rfft3d_forward(const float* in, float2* spec, const MeshDims& d, float sub, cudaStream_t s);
 cudaError_t rfft3d_inverse(float2* spec, float* out, const MeshDims& d, float scale, cudaStream_t s);
+cudaError_t rfft2d_forward(const float* in, float2* spec, const MeshDims& d, cudaStream_t s);  // d.nx == 1
 cudaError_t poisson_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean,
                               float scale, cudaStream_t s);
 cudaError_t pgd_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean, float kl,
@@ -126,5 +127,13 @@ cudaError_t healpix_paint_tiled(const float* disp, int absolute, const float* ve
                                 const signed char* rotations, const float* shifts, int telephoto, float rmin,
                                 float rmax, float t, float gp_t, float dbound, const DriftTables& tb, int nside,
                                 int scheme, float* map, cudaStream_t s);
+
+// ---- flat.cu ----
+cudaError_t paint_flat(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d, int npx,
+                       int npy, float zlo, float zhi, float* map, cudaStream_t s);
+int flat_cl_ctas(int n0, int n1);
+cudaError_t flat_cl(const float* map1, const float* map2, int n0, int n1, int batch, float dn0, float dn1,
+                    const float* edges, int nedges, float2* spec1, float2* spec2, double* partials, double* out,
+                    cudaStream_t s);
 
 }  // namespace jfli

@@ -195,13 +195,48 @@ class SphericalDensity(AbstractField):
         return 1
 
     def angular_cl(self, lmax: int | None = None):
-        """Angular power spectrum of each map (computed on the host)."""
+        """Angular power spectrum of each map (healpy's anafast algorithm: FP64 Legendre
+        stages on the GPU, ring FFTs on the host)."""
         from .sht import anafast
 
         maps = self.array.detach().double().cpu().numpy()
         if maps.ndim == 1:
             return anafast(maps, lmax=lmax)
         return np.stack([anafast(m, lmax=lmax) for m in maps])
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class FlatDensity(AbstractField):
+    """Flat-sky planes (reference fields/lightcone.py:20-233): (npx, npy) or (S, npx, npy)
+    maps, the shape given by flatsky_npix."""
+
+    def _core_ndim(self) -> int:
+        return 2
+
+    def __post_init__(self):
+        super().__post_init__()
+        if self.array.ndim not in (2, 3, 4):
+            raise ValueError("FlatDensity array must have shape (ny, nx), (S, ny, nx), or (N, S, ny, nx).")
+        if self.flatsky_npix is None:
+            raise ValueError("FlatDensity requires `flatsky_npix`.")
+        if tuple(self.array.shape[-2:]) != tuple(self.flatsky_npix):
+            raise ValueError(f"Array spatial shape {tuple(self.array.shape[-2:])} does not match flatsky_npix "
+                             f"{tuple(self.flatsky_npix)}.")
+
+    def angular_cl(self, mesh2: "FlatDensity | None" = None, *, field_size=None, pixel_size=None, ell_edges=None,
+                   batch_size=None) -> PowerSpectrum:
+        """Flat-sky C_ell, auto or cross (reference fields/lightcone.py:197-233)."""
+        from .power import angular_cl_flat
+
+        data1 = self.array
+        data2 = mesh2.array if mesh2 is not None else None
+        if data1.ndim not in (2, 3):
+            raise ValueError("FlatDensity.angular_cl expects array shape (ny,nx) or (B,ny,nx)")
+        if data2 is not None and data2.shape != data1.shape:
+            raise ValueError("mesh2 must match shape for cross Cl")
+        ell, cl = angular_cl_flat(data1, data2, pixel_size=pixel_size, field_size=field_size or self.field_size,
+                                  ell_edges=ell_edges)
+        return PowerSpectrum(wavenumber=ell, array=cl, name="cl", scale_factors=self.scale_factors)
 
 
 @dataclasses.dataclass(frozen=True, eq=False)
@@ -263,6 +298,49 @@ class ParticleField(AbstractField):
         mesh = density_mesh.array if isinstance(density_mesh, AbstractField) else density_mesh
         vals = ops.readout_cic(self.array.contiguous(), mesh.contiguous(), absolute=absolute)
         return DensityField(array=vals, **self._meta_for_density(self.status))
+
+    def paint_2d(self, center, density_plane_width, *, weights=None, batch_size=None) -> FlatDensity:
+        """Flat-sky planes (reference fields/particles.py:234-320 -> _src/fields/_painting.py:117-202):
+        the particles with center - width/2 < z <= center + width/2 (z measured from the box
+        origin; center and width in Mpc/h) painted with 2D CIC on a flatsky_npix grid, x and
+        y scaled to it and wrapped, divided by the pixel volume (L_x / npx)(L_y / npy) width.
+        As in the reference (its light-cone mode), every plane takes the particles of every
+        snapshot of a batched (S, ...) input that fall in its z range."""
+        if self.flatsky_npix is None:
+            raise ValueError("ParticleField requires `flatsky_npix` for paint_2d.")
+        field = self if self.unit != PositionUnit.MPC_H else self.to(PositionUnit.GRID_ABSOLUTE)
+        absolute = field._grid_mode()
+        centers = np.atleast_1d(np.asarray(center, dtype=np.float64))
+        widths = np.atleast_1d(np.asarray(density_plane_width, dtype=np.float64))
+        if centers.shape != widths.shape:
+            raise ValueError(f"center and density_plane_width must have the same shape; got {centers.shape} and "
+                             f"{widths.shape}")
+        arr = field.array.contiguous()
+        if arr.ndim == 5:
+            if arr.shape[0] != centers.size:
+                raise ValueError(f"Batched input: center must have {arr.shape[0]} elements, got {centers.size}")
+        elif arr.ndim != 4:
+            raise ValueError(f"paint_2d() expects 4D or 5D array, got shape {tuple(arr.shape)}")
+        npx, npy = (int(v) for v in self.flatsky_npix)
+        nz = self.mesh_size[2]
+        Lx, Ly, Lz = (float(v) for v in self.box_size)
+        w, ws = _weights_arg(weights)
+        srcs = [arr[i] for i in range(arr.shape[0])] if arr.ndim == 5 else [arr]
+        maps = []
+        for c, wd in zip(centers, widths):
+            cg, wg = c * nz / Lz, wd * nz / Lz  # grid units along z
+            vol = (Lx / npx) * (Ly / npy) * wd
+            m = None
+            for src in srcs:
+                m = ops.paint_flat(src, (npx, npy), cg - wg / 2, cg + wg / 2, absolute=absolute, weights=w,
+                                   weight=ws / vol if vol > 0 else ws, out=m, accumulate=m is not None)
+            maps.append(m)
+        out = maps[0] if centers.size == 1 else torch.stack(maps)
+        return FlatDensity(array=out, mesh_size=self.mesh_size, box_size=self.box_size,
+                           observer_position=self.observer_position, flatsky_npix=(npx, npy),
+                           field_size=self.field_size, nside=self.nside, status=FieldStatus.LIGHTCONE,
+                           comoving_centers=centers, density_width=widths, scale_factors=self.scale_factors,
+                           unit=DensityUnit.DENSITY)
 
     def paint_spherical(self, center, density_plane_width, *, scheme: str = "bilinear", weights=None,
                         kernel_width_arcmin=None, smoothing_interpretation="fwhm", paint_nside=None,

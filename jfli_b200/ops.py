@@ -271,6 +271,43 @@ def drift_tables(cosmo, n_dense: int = 4096):
     return tuple(torch.as_tensor(np.ascontiguousarray(t, dtype=np.float32), device="cuda") for t in tabs)
 
 
+def paint_flat(pos: torch.Tensor, npix, zlo: float, zhi: float, *, absolute: bool = False,
+               weights: torch.Tensor | None = None, weight: float = 1.0, out: torch.Tensor | None = None,
+               accumulate: bool = False) -> torch.Tensor:
+    """Flat-sky plane (..., npx, npy) of the particles with zlo < z <= zhi (grid units):
+    raw 2D CIC sums (see jfli_paint_flat)."""
+    _check(pos, "pos")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    npx, npy = (int(v) for v in npix)
+    if out is None:
+        out = torch.empty(*lead, npx, npy, dtype=torch.float32, device=pos.device)
+        accumulate = False
+    call("jfli_paint_flat", stream_ptr(), ptr(pos), int(absolute), ptr(weights), float(weight), float(zlo), float(zhi),
+         npx, npy, ptr(out), int(accumulate), nx, ny, nz, batch)
+    return out
+
+
+def flat_cl_sums(map1: torch.Tensor, map2: torch.Tensor | None, dnx: float, dny: float,
+                 ell_edges: torch.Tensor) -> torch.Tensor:
+    """(batch, 3, nedges + 1) FP64 sums (power, modes, ell) of maps (..., npx, npy) binned by
+    |ell| (see jfli_flat_cl); dnx, dny = n times the pixel size in radians."""
+    _check(map1, "map1")
+    if map2 is not None:
+        _check(map2, "map2")
+        if map2.shape != map1.shape:
+            raise ValueError("map2 must have the shape of map1")
+    npx, npy = map1.shape[-2:]
+    batch = int(np.prod(map1.shape[:-2])) if map1.ndim > 2 else 1
+    edges = ell_edges.to(device=map1.device, dtype=torch.float32).contiguous()
+    nedges = int(edges.numel())
+    nb = query("jfli_flat_cl_workspace_bytes", npx, npy, batch, nedges, int(map2 is not None))
+    ws = workspace(nb, "flat_cl", map1.device)
+    out = torch.empty(batch, 3, nedges + 1, dtype=torch.float64, device=map1.device)
+    call("jfli_flat_cl", stream_ptr(), ptr(map1), ptr(map2), int(npx), int(npy), batch, float(dnx), float(dny),
+         ptr(edges), nedges, ptr(out), ptr(ws), ws.numel())
+    return out
+
+
 def drift_bound(tables, t: float, gp_t: float) -> float:
     """Bound on |D| = |Gp(a_t) - Gp(t)| / dGfa(sqrt(t a_t)) as the drift kernels evaluate
     it for any distance inside the distance table: the Gp difference is at most

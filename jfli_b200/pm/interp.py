@@ -82,6 +82,9 @@ class AbstractInterp:
                                       ud_grade_power=p.ud_grade_power, ud_grade_order_in=p.ud_grade_order_in,
                                       ud_grade_order_out=p.ud_grade_order_out, ud_grade_pess=p.ud_grade_pess,
                                       batch_size=p.batch_size)
+        if tgt == "flat":
+            return dx.paint_2d(center=r_center, density_plane_width=width, weights=self.painting.weights,
+                               batch_size=self.painting.batch_size)
         if tgt == "density":
             return dx.paint(weights=self.painting.weights, chunk_size=self.painting.chunk_size,
                             batch_size=self.painting.batch_size)
@@ -219,8 +222,8 @@ class TelephotoInterp(AbstractInterp):
     shell centre lies beyond the box; the replica is the box rotated by the index's cube
     symmetry (of the 47, cyclically) and pushed along z by floor(r / R) R, R the largest
     radius the box holds. The drift distance is measured as the reference measures it,
-    from the observer-centred replica minus the observer's position. Spherical painting
-    only: the flat-sky painter is not built."""
+    from the observer-centred replica minus the observer's position. Flat-sky targets are
+    painted for planes inside the box; beyond it, spherical only."""
 
     drift_on_lightcone: bool = True
 
@@ -231,10 +234,9 @@ class TelephotoInterp(AbstractInterp):
         tgt = self.painting.target if self.painting is not None else None
         if tgt not in ("spherical", "flat"):
             raise ValueError("TelephotoInterp only supports projections (flat or spherical).")
-        if tgt == "flat":
-            raise NotImplementedError("flat-sky painting is not on the B200 path")
-        warnings.warn("TelephotoInterp is designed for narrow FOV flat-sky projections. Using it for spherical "
-                      "painting will cause significant artifacts. use for illustriative purposes only.")
+        if tgt == "spherical":
+            warnings.warn("TelephotoInterp is designed for narrow FOV flat-sky projections. Using it for spherical "
+                          "painting will cause significant artifacts. use for illustriative purposes only.")
         return InterpTilerState(rotation_idx=-1, shell_idx=-1, rotations=get_all_47_symmetries())
 
     def advance(self, state, t):
@@ -265,6 +267,9 @@ class TelephotoInterp(AbstractInterp):
             from ..fields import SphericalDensity
             from ..painting import paint_shell_tiled
 
+            if pt.target == "flat":
+                raise NotImplementedError("TelephotoInterp: flat-sky planes beyond the box (a rotated, pushed "
+                                          "replica) are not on the B200 path; planes inside the box are")
             rot = state.rotations[state.rotation_idx % 47][None]
             R = self.max_comoving_distance
             shift = np.array([[0.0, 0.0, math.floor(r_center / R) * R]])

@@ -65,3 +65,52 @@ def power(mesh, mesh2=None, *, box_shape, kedges=None, multipoles=0, los=(0.0, 0
         return kavg, PowerSpectrum.apply(mesh, np.asarray(kedges, np.float64), box_shape)
     sums = power_sums(mesh, box_shape, kedges)
     return finalize(sums, mesh_shape, box_shape)
+
+
+def flat_ell_grid_max(npx: int, npy: int, px: float, py: float) -> np.float32:
+    """Largest |ell| of the flat-sky FFT grid, formed in FP32 as the kernel forms it."""
+    def comp(n, d):
+        k = np.float32(-(n // 2)) if n % 2 == 0 else np.float32((n - 1) // 2)
+        return np.float32(np.float32(2.0 * np.pi) * np.float32(k / np.float32(n * d)))
+
+    lx, ly = comp(npx, px), comp(npy, py)
+    return np.float32(np.sqrt(np.float32(np.float32(lx * lx) + np.float32(ly * ly))))
+
+
+def angular_cl_flat(map1, map2=None, *, pixel_size=None, field_size=None, ell_edges=None):
+    """Flat-sky C_ell (reference power/compute.py:70-86 -> _src/power/_compute.py:122-172):
+    (ell, cl) with cl the mean of Re(F1 conj F2) (px py) / (npx npy) over the modes of each
+    ell bin (numpy.digitize on the edges; under/overflow bins dropped) and ell the mean |ell|.
+    pixel_size (px, py) in radians per pixel, or field_size (fx, fy) with px = fx / npx.
+    Default edges: 50 from 0 to the largest |ell| of the grid."""
+    m1 = map1 if isinstance(map1, torch.Tensor) else torch.as_tensor(np.asarray(map1, np.float32), device="cuda")
+    m1 = m1.to(torch.float32).contiguous()
+    m2 = None
+    if map2 is not None:
+        m2 = map2 if isinstance(map2, torch.Tensor) else torch.as_tensor(np.asarray(map2, np.float32), device="cuda")
+        m2 = m2.to(torch.float32).contiguous()
+        if m2.shape != m1.shape:
+            raise ValueError("map2 must have the same shape as map2d for cross Cl")
+    npx, npy = m1.shape[-2:]
+    if pixel_size is None:
+        if field_size is None:
+            raise ValueError("pixel_size or field_size must be provided for flat-sky Cl")
+        fx, fy = (field_size, field_size) if np.ndim(field_size) == 0 else field_size
+        px, py = float(fx) / npx, float(fy) / npy
+    else:
+        px, py = (pixel_size, pixel_size) if np.ndim(pixel_size) == 0 else pixel_size
+        px, py = float(px), float(py)
+    if ell_edges is None:
+        top = flat_ell_grid_max(npx, npy, px, py)
+        edges = np.linspace(0.0, float(top), 50).astype(np.float32)
+        edges[-1] = top
+    else:
+        edges = np.asarray(ell_edges, dtype=np.float32)
+    sums = ops.flat_cl_sums(m1, m2, npx * px, npy * py, torch.as_tensor(edges))
+    norm = (px * py) / (npx * npy)
+    cnt = torch.where(sums[:, 1] > 0, sums[:, 1], torch.ones_like(sums[:, 1]))
+    cl = (sums[:, 0] / cnt * norm)[:, 1:-1]
+    ell = (sums[0, 2] / cnt[0])[1:-1]
+    if m1.ndim == 2:
+        cl = cl[0]
+    return ell, cl

@@ -188,3 +188,23 @@ def test_oracle_fp32_matches_fp64_forces():
     f64 = opm.pm_forces(dx, np.float64)
     f32 = opm.pm_forces(dx.astype(np.float32), np.float32)
     assert rel_l2(f32, f64) < 1e-5
+
+
+def test_flat_oracle_self_consistency():
+    """The flat-sky oracle: 2D CIC conserves weight inside the slab, and the flat C_ell of a
+    single cosine puts its power in the bin of its |ell| (Parseval with the (px py)/(nx ny)
+    normalisation)."""
+    from oracle import flat as of
+
+    rng = np.random.default_rng(0)
+    pos = rng.uniform(-5, 40, (2000, 3))
+    m = of.paint_2d(pos, (16, 24), 5.0, 20.0, (32, 32, 32))
+    inside = ((pos[:, 2] > 5.0) & (pos[:, 2] <= 20.0)).sum()
+    assert abs(m.sum() - inside) < 1e-9 * inside
+    nx, ny, px = 64, 64, 1e-3
+    x = np.arange(nx)[:, None] * np.ones((1, ny))
+    cosmap = np.cos(2 * np.pi * 5 * x / nx)
+    ell, cl = of.flat_cl(cosmap, px=px, py=px)
+    target = 2 * np.pi * 5 / (nx * px)
+    b = np.argmax(cl)
+    assert abs(ell[b] - target) < 0.6 * (ell[1] - ell[0])

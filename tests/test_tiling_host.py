@@ -77,8 +77,9 @@ def test_onion_tiler_rotations():
         jf.OnionTiler(painting=jf.PaintingOptions(target="spherical"), rotation_indices=(47,) * 27).init()
     with pytest.raises(ValueError):
         jf.OnionTiler(painting=jf.PaintingOptions(target="density")).init()
-    with pytest.raises(NotImplementedError):
-        jf.TelephotoInterp(painting=jf.PaintingOptions(target="flat")).init()
+    with pytest.raises(ValueError):
+        jf.TelephotoInterp(painting=jf.PaintingOptions(target="density")).init()
+    assert jf.TelephotoInterp(painting=jf.PaintingOptions(target="flat")).init().rotations.shape == (47, 3, 3)
 
 
 def test_snapshot_times_match_after_fp32_rounding():
