@@ -6,6 +6,7 @@ every operation on them runs in libjfli_b200's sm_100a kernels.
 """
 
 from . import cosmology, ops, utils
+from .catalog import CATALOG_VERSION, Catalog
 from .cosmology import Cosmology, Planck18
 from .fields import (
     AbstractField,

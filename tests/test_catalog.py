@@ -1,0 +1,83 @@
+"""Catalog on disk (reference io/catalog.py): the HuggingFace parquet rows written here use
+the reference's Features schema (format version 2), and every field type round-trips with
+its metadata and cosmology. CPU only."""
+
+import numpy as np
+import pytest
+import torch
+
+import jfli_b200 as jf
+
+datasets = pytest.importorskip("datasets")
+
+
+def _fields():
+    rng = np.random.default_rng(0)
+    meta = dict(mesh_size=(8, 8, 8), box_size=(100.0, 100.0, 100.0), observer_position=(0.5, 0.5, 0.5))
+    sph = jf.SphericalDensity(array=torch.as_tensor(rng.random((3, 12 * 4 * 4), dtype=np.float32)), nside=4,
+                              status=jf.FieldStatus.LIGHTCONE, unit=jf.DensityUnit.DENSITY,
+                              scale_factors=np.array([0.9, 0.8, 0.7]), z_sources=np.array([0.11, 0.25, 0.43]),
+                              comoving_centers=np.array([10.0, 30.0, 50.0]), density_width=np.array([20.0] * 3),
+                              **meta)
+    flat = jf.FlatDensity(array=torch.as_tensor(rng.random((16, 12), dtype=np.float32)), flatsky_npix=(16, 12),
+                          field_size=(2.0, 1.5), status=jf.FieldStatus.LIGHTCONE, unit=jf.DensityUnit.DENSITY,
+                          scale_factors=0.8, z_sources=0.25, comoving_centers=40.0, density_width=10.0, **meta)
+    dens = jf.DensityField(array=torch.as_tensor(rng.random((8, 8, 8), dtype=np.float32)),
+                           status=jf.FieldStatus.DENSITY_FIELD, unit=jf.DensityUnit.DENSITY, scale_factors=1.0,
+                           z_sources=0.0, comoving_centers=0.0, density_width=0.0, **meta)
+    parts = jf.ParticleField(array=torch.as_tensor(rng.standard_normal((2, 8, 8, 8, 3)).astype(np.float32)),
+                             status=jf.FieldStatus.PARTICLES, unit=jf.PositionUnit.GRID_RELATIVE,
+                             scale_factors=np.array([0.5, 1.0]), z_sources=np.array([1.0, 0.0]),
+                             comoving_centers=np.array([0.0, 0.0]), density_width=np.array([0.0, 0.0]), **meta)
+    return [sph, flat, dens, parts]
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+def test_catalog_round_trip(tmp_path, kind):
+    """One catalog per field type (a catalog's rows share one schema, as in the reference),
+    two entries each with their own cosmology."""
+    a = _fields()[kind]
+    b2 = a.replace(array=a.array * 2)
+    fields = [a, b2]
+    cosmos = [jf.Planck18(Omega_c=0.25 + 0.01 * i, sigma8=0.8 - 0.01 * i) for i in range(2)]
+    path = str(tmp_path / "cat.parquet")
+    jf.Catalog(fields, cosmos).to_parquet(path)
+    back = jf.Catalog.from_parquet(path, device="cpu")
+    assert len(back) == 2 and back.version == jf.CATALOG_VERSION
+    for x, y, cx, cy in zip(fields, back.field, cosmos, back.cosmology):
+        assert type(x) is type(y)
+        assert torch.equal(x.array, y.array)
+        assert (x.mesh_size, x.box_size, x.observer_position, x.status, x.unit) == \
+               (y.mesh_size, y.box_size, y.observer_position, y.status, y.unit)
+        for key in ("scale_factors", "z_sources", "comoving_centers", "density_width"):
+            np.testing.assert_allclose(np.asarray(getattr(y, key)), np.asarray(getattr(x, key)))
+        assert y.nside == x.nside and y.flatsky_npix == x.flatsky_npix
+        np.testing.assert_allclose([cy.Omega_c, cy.sigma8, cy.h], [cx.Omega_c, cx.sigma8, cx.h], rtol=1e-6)
+    if kind == 1:
+        assert back.field[0].field_size == (2.0, 1.5)
+    assert back[1].field[0].array.shape == a.array.shape and len(back[0:2]) == 2
+
+
+def test_catalog_schema_is_the_reference_schema(tmp_path):
+    """The features a reader finds in the file: the reference's names and types."""
+    path = str(tmp_path / "one.parquet")
+    jf.Catalog(_fields()[0], jf.Planck18()).to_parquet(path)
+    ds = datasets.load_dataset("parquet", data_files=path, split="train")
+    f = ds.features
+    assert type(f["array"]).__name__ == "Array2D" and tuple(f["array"].shape) == (None, 192)
+    assert f["array"].dtype == "float32"
+    seq = lambda k: (f[k].feature.dtype if hasattr(f[k], "feature") else f[k].dtype)
+    for k in ("z_sources", "scale_factors", "comoving_centers", "density_width"):
+        assert "float64" in str(seq(k)) or "float64" in str(f[k])
+    for k in ("Omega_c", "Omega_b", "h", "n_s", "sigma8", "w0", "wa", "Omega_k", "Omega_nu"):
+        assert f[k].dtype == "float32"
+    assert f["version"].dtype == "int32" and f["nside"].dtype == "int32"
+    row = ds[0]
+    assert row["field_type"] == "SphericalDensity" and row["status"] == "LIGHTCONE" and row["unit"] == "DENSITY"
+    assert row["version"] == 2 and row["mesh_size"] == [8, 8, 8]
+
+
+def test_catalog_rejects_mismatched_lengths():
+    f = _fields()[2]
+    with pytest.raises(ValueError):
+        jf.Catalog([f, f], [jf.Planck18()])
