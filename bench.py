@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--lightcone", type=int, default=0,
                     help="instead of the step benchmark, run the large light-cone chain at this mesh size "
                          "(box 1000 Mpc/h, 2LPT, 60 KDK steps with PGD, 16 shells at nside 1024, Born)")
+    ap.add_argument("--tiled-paint", type=int, default=0,
+                    help="instead of the step benchmark, time the 27-replica light-cone paint of one shell "
+                         "(this many particles per side, box 500 Mpc/h, shell 653-747 Mpc/h, nside 1024)")
     return ap.parse_args()
 
 
@@ -564,6 +567,49 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_tiled_paint(args):
+    """One OnionTiler shell beyond the box: N^3 particles (2LPT at a = 0.6, box 500 Mpc/h,
+    centred observer), 27 rotated replicas, shell 653-747 Mpc/h at nside 1024 (bilinear),
+    with and without the light-cone drift; --steps timed launches after --warmup."""
+    import torch
+
+    import jfli_b200 as jf
+    from jfli_b200 import cosmology as cj
+    from jfli_b200 import ops
+    from jfli_b200.pm.interp import get_all_47_symmetries, tile_shifts
+
+    n, L, nside = args.tiled_paint, 500.0, 1024
+    cosmo = jf.Planck18()
+    ic = jf.interpolate_initial_conditions(jf.white_noise(0, (n, n, n)), (n, n, n), (L, L, L), cosmo=cosmo,
+                                           nside=nside)
+    dx, p = jf.lpt(cosmo, ic, ts=0.6, order=2)
+    x, v = dx.array.contiguous(), p.array.contiguous()
+    rot = get_all_47_symmetries()[np.random.default_rng(42).integers(0, 47, 27)]
+    sh = tile_shifts((0.5, 0.5, 0.5), (L, L, L))
+    rc, wd = 700.0, 94.0
+    t = float(cj.a_of_chi(cosmo, rc))
+    tabs = ops.drift_tables(cosmo)
+    out = torch.empty(12 * nside * nside, device="cuda")
+    line = {"workload": f"27-replica shell paint, {n}^3 particles, box {L:g} Mpc/h, shell {rc - wd / 2:g}-"
+                        f"{rc + wd / 2:g} Mpc/h, nside {nside}",
+            "deposits_expected": round(n**3 / L**3 * 4 * np.pi / 3 * ((rc + wd / 2)**3 - (rc - wd / 2)**3))}
+    for name, vel in (("drift", v), ("no_drift", None)):
+        call = lambda: ops.healpix_paint_tiled(x, nside, (L, L, L), (L / 2,) * 3, rc - wd / 2, rc + wd / 2, rot, sh,
+                                               vel=vel, t=t, cosmo=cosmo, tables=tabs, out=out)
+        for _ in range(args.warmup):
+            call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            call()
+        e1.record()
+        torch.cuda.synchronize()
+        line[f"{name}_ms"] = round(e0.elapsed_time(e1) / args.steps, 4)
+        line[f"{name}_weight"] = float(out.double().sum())
+    print(json.dumps(line), flush=True)
+
+
 def run_lightcone(args):
     """The large light-cone chain: N^3 particles on an N^3 mesh, box 1000 Mpc/h, 2LPT to
     a = 0.1, 60 KDK steps with PGD (alpha 0.3, kl 1.5 h/Mpc, ks 8 h/Mpc), 16 HEALPix shells
@@ -612,6 +658,9 @@ def main():
     args = parse()
     if args.lightcone:
         run_lightcone(args)
+        return
+    if args.tiled_paint:
+        run_tiled_paint(args)
         return
     if args.impl == "reference":
         run_reference(args)
