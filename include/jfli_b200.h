@@ -42,6 +42,7 @@
  *   jfli_born              <- _src/lensing/_born.py:29-130 (_born_core_impl, _born_spherical)
  *   jfli_sht_map2alm / jfli_sht_alm2map <- the Legendre stages of healpy.anafast behind
  *                             SphericalDensity.angular_cl (_src/power/_compute.py:175-191)
+ *   jfli_sht_ring_analysis / jfli_sht_ring_synthesis <- the ring FFTs along phi of the same
  * Adjoints (the reverse-mode derivatives jax.grad takes through the same code, and the
  * backward loop of the reversible adjoint, pm/integrate.py:147-535):
  *   jfli_adjoint_unkick_paint, jfli_poisson_divergence, jfli_adjoint_position, jfli_kkd_adjoint
@@ -240,6 +241,16 @@ int jfli_born(void* stream, const float* maps, int nplanes, long long npix, cons
  *   jfli_sht_alm2map: G[r][m] = sum_l alm[l][m] lambda_lm(theta_r)
  * lambda_lm: orthonormal associated Legendre functions with the Condon-Shortley phase.
  * lmax <= 8191, nrings <= 65535. */
+/* Ring transforms along phi of a RING-ordered map [12 nside^2] (FP64), rings north to south
+ * (4 nside - 1 of them), phi_j = phi_0 + 2 pi j / n_r:
+ *   jfli_sht_ring_analysis:  F[r][m] = sum_j map_j e^{-i m phi_j},  m = 0..lmax
+ *   jfli_sht_ring_synthesis: map_j = Re G[r][0] + 2 sum_{m=1..lmax} Re(G[r][m] e^{i m phi_j})
+ * Direct FP64 sums (phases exact every 64 terms). nside <= 4096, lmax <= 8191. */
+int jfli_sht_ring_analysis(void* stream, const double* map, int nside, int lmax, double* F, char* err,
+                           size_t errlen);
+int jfli_sht_ring_synthesis(void* stream, const double* G, int nside, int lmax, double* map, char* err,
+                            size_t errlen);
+
 int jfli_sht_map2alm(void* stream, const double* F, const double* z, int nrings, int lmax, double weight,
                      double* alm, char* err, size_t errlen);
 int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nrings, int lmax, double* G, char* err,

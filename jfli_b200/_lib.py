@@ -113,6 +113,8 @@ _SIGNATURES = {
          c_float, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, *_DIMS, *_ERR],
     ),
     "jfli_sht_map2alm": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, ctypes.c_double, c_void_p, *_ERR]),
+    "jfli_sht_ring_analysis": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
+    "jfli_sht_ring_synthesis": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
     "jfli_sht_alm2map": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
     "jfli_born_workspace_bytes": (c_size_t, [c_int, c_longlong]),
     "jfli_born": (c_int, [c_void_p, c_void_p, c_int, c_longlong, c_void_p, c_int, c_void_p, c_void_p, c_size_t, *_ERR]),

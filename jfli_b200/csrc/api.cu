@@ -633,6 +633,26 @@ int jfli_sht_map2alm(void* stream, const double* F, const double* z, int nrings,
                      "jfli_sht_map2alm");
 }
 
+int jfli_sht_ring_analysis(void* stream, const double* map, int nside, int lmax, double* F, char* err,
+                           size_t errlen) {
+  CHECK_PTR(map);
+  CHECK_PTR(F);
+  if (nside < 1 || nside > 4096) return fail(err, errlen, JFLI_EINVAL, "nside %d outside [1, 4096]", nside);
+  if (lmax < 0 || lmax > 8191) return fail(err, errlen, JFLI_EINVAL, "lmax %d outside [0, 8191]", lmax);
+  return cuda_status(jfli::sht_ring_analysis(map, nside, lmax, F, (cudaStream_t)stream), err, errlen,
+                     "jfli_sht_ring_analysis");
+}
+
+int jfli_sht_ring_synthesis(void* stream, const double* G, int nside, int lmax, double* map, char* err,
+                            size_t errlen) {
+  CHECK_PTR(G);
+  CHECK_PTR(map);
+  if (nside < 1 || nside > 4096) return fail(err, errlen, JFLI_EINVAL, "nside %d outside [1, 4096]", nside);
+  if (lmax < 0 || lmax > 8191) return fail(err, errlen, JFLI_EINVAL, "lmax %d outside [0, 8191]", lmax);
+  return cuda_status(jfli::sht_ring_synthesis(G, nside, lmax, map, (cudaStream_t)stream), err, errlen,
+                     "jfli_sht_ring_synthesis");
+}
+
 int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nrings, int lmax, double* G, char* err,
                      size_t errlen) {
   CHECK_PTR(alm);

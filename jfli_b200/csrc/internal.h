@@ -96,6 +96,8 @@ cudaError_t born_convergence(const float* maps, int nplanes, long long npix, con
 cudaError_t sht_analysis(const double* F, const double* z, int nrings, int lmax, double weight, double* alm,
                          cudaStream_t s);
 cudaError_t sht_synthesis(const double* alm, const double* z, int nrings, int lmax, double* G, cudaStream_t s);
+cudaError_t sht_ring_analysis(const double* map, int nside, int lmax, double* F, cudaStream_t s);
+cudaError_t sht_ring_synthesis(const double* G, int nside, int lmax, double* map, cudaStream_t s);
 
 // ---- adjoint.cu ----
 size_t adjoint_partials_count(const MeshDims& d);

@@ -161,6 +161,132 @@ __global__ void __launch_bounds__(kShtThreads) k_sht_synthesis(const double2* __
   if (active) G[(long long)r * (lmax + 1) + m] = make_double2(gx, gy);
 }
 
+// ---- ring transforms along phi ------------------------------------------------------
+// RING geometry of ring r (0 = northernmost, i = r + 1): pixel count, first pixel, and the
+// longitude of the first pixel centre (Gorski et al. 2005).
+struct RingPhi {
+  long long start;
+  int n;
+  double phi0;
+};
+
+__device__ __forceinline__ RingPhi ring_phi(int r, int nside) {
+  const int i = r + 1;
+  const long long npix = 12LL * nside * nside;
+  RingPhi g;
+  if (i < nside) {
+    g.n = 4 * i;
+    g.start = 2LL * i * (i - 1);
+    g.phi0 = 3.14159265358979323846 / (4.0 * i);
+  } else if (i <= 3 * nside) {
+    g.n = 4 * nside;
+    g.start = 2LL * nside * (nside - 1) + (long long)(i - nside) * 4 * nside;
+    g.phi0 = ((i - nside + 1) % 2 == 1) ? 0.0 : 3.14159265358979323846 / (4.0 * nside);
+  } else {
+    const int j = 4 * nside - i;
+    g.n = 4 * j;
+    g.start = npix - 2LL * j * (j + 1);
+    g.phi0 = 3.14159265358979323846 / (4.0 * j);
+  }
+  return g;
+}
+
+constexpr int kRingThreads = 128;
+constexpr int kReseed = 64;  // exact phase every 64 terms; rotations in between
+
+// e^{-i m phi_j}, phi_j = phi0 + 2 pi j / n, with the angle reduced exactly: (m j) mod n.
+__device__ __forceinline__ double2 phase(int m, int j, int n, double phi0, double sign) {
+  const long long q = ((long long)m * j) % n;
+  const double ang = (double)m * phi0 + 6.283185307179586476925 * (double)q / (double)n;
+  double sn, cs;
+  sincos(ang, &sn, &cs);
+  return make_double2(cs, sign * sn);
+}
+
+// F[r][m] = sum_j f_j e^{-i m phi_j}, m = 0..lmax (aliasing for m >= n is the DFT's own).
+// One block per (ring, 128 m); the ring's values staged in shared memory.
+__global__ void __launch_bounds__(kRingThreads) k_ring_analysis(const double* __restrict__ map, int nside, int lmax,
+                                                                double2* __restrict__ F) {
+  extern __shared__ double ring[];
+  const int r = blockIdx.y;
+  const RingPhi g = ring_phi(r, nside);
+  for (int j = threadIdx.x; j < g.n; j += blockDim.x) ring[j] = map[g.start + j];
+  __syncthreads();
+  const int m = blockIdx.x * kRingThreads + threadIdx.x;
+  if (m > lmax) return;
+  double2 step;  // e^{-i 2 pi m / n}
+  {
+    const double ang = 6.283185307179586476925 * (double)(m % g.n) / (double)g.n;
+    double sn, cs;
+    sincos(ang, &sn, &cs);
+    step = make_double2(cs, -sn);
+  }
+  double sx = 0.0, sy = 0.0;
+  for (int j0 = 0; j0 < g.n; j0 += kReseed) {
+    double2 w = phase(m, j0, g.n, g.phi0, -1.0);
+    const int j1 = min(j0 + kReseed, g.n);
+    for (int j = j0; j < j1; ++j) {
+      const double f = ring[j];
+      sx += f * w.x;
+      sy += f * w.y;
+      w = make_double2(w.x * step.x - w.y * step.y, w.x * step.y + w.y * step.x);
+    }
+  }
+  F[(long long)r * (lmax + 1) + m] = make_double2(sx, sy);
+}
+
+// f_j = Re G[r][0] + 2 sum_{m >= 1} Re(G[r][m] e^{i m phi_j}). One block per (ring, 128
+// pixels); the ring's coefficients staged in shared memory.
+__global__ void __launch_bounds__(kRingThreads) k_ring_synthesis(const double2* __restrict__ G, int nside, int lmax,
+                                                                 double* __restrict__ map) {
+  extern __shared__ double2 coef[];
+  const int r = blockIdx.y;
+  const RingPhi g = ring_phi(r, nside);
+  for (int m = threadIdx.x; m <= lmax; m += blockDim.x) coef[m] = G[(long long)r * (lmax + 1) + m];
+  __syncthreads();
+  const int j = blockIdx.x * kRingThreads + threadIdx.x;
+  if (j >= g.n) return;
+  const double phij = g.phi0 + 6.283185307179586476925 * (double)j / (double)g.n;
+  double2 step;  // e^{i phi_j}
+  {
+    double sn, cs;
+    sincos(phij, &sn, &cs);
+    step = make_double2(cs, sn);
+  }
+  double acc = 0.0;
+  for (int m0 = 1; m0 <= lmax; m0 += kReseed) {
+    double2 w = phase(m0, j, g.n, g.phi0, 1.0);
+    const int m1 = min(m0 + kReseed, lmax + 1);
+    for (int m = m0; m < m1; ++m) {
+      acc += coef[m].x * w.x - coef[m].y * w.y;
+      w = make_double2(w.x * step.x - w.y * step.y, w.x * step.y + w.y * step.x);
+    }
+  }
+  map[g.start + j] = coef[0].x + 2.0 * acc;
+}
+
+cudaError_t sht_ring_analysis(const double* map, int nside, int lmax, double* F, cudaStream_t s) {
+  const int nrings = 4 * nside - 1;
+  const size_t smem = sizeof(double) * 4 * (size_t)nside;
+  cudaError_t e = cudaFuncSetAttribute(k_ring_analysis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((lmax + kRingThreads) / kRingThreads, nrings);
+  k_ring_analysis<<<grid, kRingThreads, smem, s>>>(map, nside, lmax, reinterpret_cast<double2*>(F));
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t sht_ring_synthesis(const double* G, int nside, int lmax, double* map, cudaStream_t s) {
+  const int nrings = 4 * nside - 1;
+  const size_t smem = sizeof(double2) * (size_t)(lmax + 1);
+  cudaError_t e = cudaFuncSetAttribute(k_ring_synthesis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((4 * nside + kRingThreads - 1) / kRingThreads, nrings);
+  k_ring_synthesis<<<grid, kRingThreads, smem, s>>>(reinterpret_cast<const double2*>(G), nside, lmax, map);
+  note_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t sht_analysis(const double* F, const double* z, int nrings, int lmax, double weight, double* alm,
                          cudaStream_t s) {
   const long long nalm = alm_offset(lmax + 1, lmax);

@@ -1,4 +1,4 @@
-"""Spherical harmonic analysis of HEALPix RING maps on the host (FP64), for C_ell.
+"""Spherical harmonic analysis of HEALPix RING maps (FP64), for C_ell.
 
 The reference computes angular power spectra with healpy.anafast
 (_src/power/_compute.py:175-191 -> hp.anafast / jhp.anafast). This module restates that
@@ -15,11 +15,13 @@ phase, built by the standard three-term recursion in l at fixed m; the starting 
 lambda_mm is formed in log space so that polar rings at large m underflow to zero
 instead of to NaN.
 
-Two engines share the ring FFTs along phi, which run on the host (numpy):
-* "gpu" (default): the O(lmax^2 x rings) Legendre stages run in the library's FP64 kernels
-  (`jfli_sht_map2alm`, `jfli_sht_alm2map`; a_lm packed by m);
-* "host": the same recursion in numpy, kept as the restatement the GPU engine is tested
-  against and for maps small enough that the transfer is not worth it.
+Two engines:
+* "gpu" (default): everything on the device in the library's FP64 kernels: the ring
+  transforms along phi as direct DFTs (`jfli_sht_ring_analysis`, `jfli_sht_ring_synthesis`)
+  and the O(lmax^2 x rings) Legendre stages (`jfli_sht_map2alm`, `jfli_sht_alm2map`; a_lm
+  packed by m); the map and the a_lm stay on the device through the iterations;
+* "host": numpy FFTs along the rings and the same recursion in numpy, kept as the
+  restatement the GPU engine is tested against.
 """
 
 from __future__ import annotations
@@ -190,7 +192,8 @@ def _ring_synth(G: np.ndarray, nside: int, lmax: int) -> np.ndarray:
 
 
 class _GpuSht:
-    """Device tables of one (nside, lmax) and the two Legendre stages."""
+    """Device tables of one (nside, lmax) and the four device stages: ring transforms along
+    phi (direct FP64 DFTs) and the Legendre stages. Maps and a_lm stay on the device."""
 
     def __init__(self, nside: int, lmax: int):
         import torch
@@ -200,27 +203,31 @@ class _GpuSht:
         self.nrings = z.size
         self.z = torch.as_tensor(z, dtype=torch.float64, device="cuda")
         self.nalm = (lmax + 1) * (lmax + 2) // 2
+        self.F = torch.empty(self.nrings, lmax + 1, dtype=torch.complex128, device="cuda")
 
-    def map2alm_once(self, m: np.ndarray) -> np.ndarray:
+    def map2alm_once(self, m):
+        """Packed a_lm (device, complex128) of a device FP64 map."""
         import torch
 
         from ._lib import call, stream_ptr
 
-        F = torch.as_tensor(_ring_ffts(m, self.nside, self.lmax), device="cuda")
+        call("jfli_sht_ring_analysis", stream_ptr(), m.data_ptr(), self.nside, self.lmax, self.F.data_ptr())
         alm = torch.empty(self.nalm, dtype=torch.complex128, device="cuda")
-        call("jfli_sht_map2alm", stream_ptr(), F.data_ptr(), self.z.data_ptr(), self.nrings, self.lmax,
-             4.0 * math.pi / m.size, alm.data_ptr())
-        return alm.cpu().numpy()
+        call("jfli_sht_map2alm", stream_ptr(), self.F.data_ptr(), self.z.data_ptr(), self.nrings, self.lmax,
+             4.0 * math.pi / m.numel(), alm.data_ptr())
+        return alm
 
-    def alm2map(self, alm: np.ndarray) -> np.ndarray:
+    def alm2map(self, alm):
+        """Device FP64 map of packed device a_lm."""
         import torch
 
         from ._lib import call, stream_ptr
 
-        a = torch.as_tensor(np.ascontiguousarray(alm, dtype=np.complex128), device="cuda")
-        G = torch.empty(self.nrings, self.lmax + 1, dtype=torch.complex128, device="cuda")
-        call("jfli_sht_alm2map", stream_ptr(), a.data_ptr(), self.z.data_ptr(), self.nrings, self.lmax, G.data_ptr())
-        return _ring_synth(G.cpu().numpy(), self.nside, self.lmax)
+        call("jfli_sht_alm2map", stream_ptr(), alm.data_ptr(), self.z.data_ptr(), self.nrings, self.lmax,
+             self.F.data_ptr())
+        out = torch.empty(12 * self.nside * self.nside, dtype=torch.float64, device="cuda")
+        call("jfli_sht_ring_synthesis", stream_ptr(), self.F.data_ptr(), self.nside, self.lmax, out.data_ptr())
+        return out
 
 
 def packed_offsets(lmax: int) -> np.ndarray:
@@ -236,11 +243,14 @@ def map2alm_gpu(m: np.ndarray, lmax: int | None = None, iter: int = 3) -> np.nda
     if 12 * nside * nside != m.size:
         raise ValueError("map size is not 12 nside^2")
     lmax = 3 * nside - 1 if lmax is None else int(lmax)
+    import torch
+
     eng = _GpuSht(nside, lmax)
-    alm = eng.map2alm_once(m)
+    md = torch.as_tensor(m, dtype=torch.float64, device="cuda")
+    alm = eng.map2alm_once(md)
     for _ in range(iter):
-        alm = alm + eng.map2alm_once(m - eng.alm2map(alm))
-    return alm
+        alm = alm + eng.map2alm_once(md - eng.alm2map(alm))
+    return alm.cpu().numpy()
 
 
 def packed_to_dict(alm: np.ndarray, lmax: int) -> dict:

@@ -56,15 +56,17 @@ def test_known_maps():
 def test_gpu_legendre_stages_match_host(nside, lmax):
     """The GPU Legendre stages against the host recursion: packed a_lm of one analysis and
     one synthesis, and the iterated C_ell."""
+    import torch
+
     rng = np.random.default_rng(nside)
     m = rng.standard_normal(12 * nside * nside)
     eng = sht._GpuSht(nside, lmax)
-    a_gpu = eng.map2alm_once(m)
+    a_gpu = eng.map2alm_once(torch.as_tensor(m, device="cuda")).cpu().numpy()
     a_host = sht._map2alm_once(m, nside, lmax)
     d = sht.packed_to_dict(a_gpu, lmax)
     scale = max(np.abs(v).max() for v in a_host.values())
     assert max(np.abs(d[k] - a_host[k]).max() for k in a_host) < 1e-12 * scale
-    back_gpu = eng.alm2map(a_gpu)
+    back_gpu = eng.alm2map(torch.as_tensor(a_gpu, device="cuda")).cpu().numpy()
     back_host = sht.alm2map(a_host, nside, lmax)
     assert np.abs(back_gpu - back_host).max() < 1e-11 * np.abs(back_host).max()
     cg = sht.anafast(m, lmax, engine="gpu")
@@ -81,9 +83,38 @@ def test_gpu_sht_large_lmax_round_trip():
     alm = rng.standard_normal(n) + 1j * rng.standard_normal(n)
     off = sht.packed_offsets(lmax)
     alm[off[0]:off[1]] = alm[off[0]:off[1]].real
+    import torch
+
     eng = sht._GpuSht(nside, lmax)
-    mp = eng.alm2map(alm)
+    mp = eng.alm2map(torch.as_tensor(alm, device="cuda")).cpu().numpy()
     back = sht.map2alm_gpu(mp, lmax, iter=3)
     err = np.abs(back - alm).max() / np.abs(alm).max()
     print(f"nside 256 lmax 500 round trip max rel err {err:.2e}")
     assert err < 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nside,lmax", [(4, 40), (16, 47), (64, 300)])
+def test_gpu_ring_transforms_match_host_ffts(nside, lmax):
+    """The device ring transforms against numpy's ring FFTs: analysis with m beyond the ring
+    lengths (aliasing), and synthesis (the host folds m onto the ring's FFT bins)."""
+    import torch
+
+    from jfli_b200._lib import call, stream_ptr
+
+    rng = np.random.default_rng(7)
+    m = rng.standard_normal(12 * nside * nside)
+    nr = 4 * nside - 1
+    F = torch.empty(nr, lmax + 1, dtype=torch.complex128, device="cuda")
+    call("jfli_sht_ring_analysis", stream_ptr(), torch.as_tensor(m, device="cuda").data_ptr(), nside, lmax,
+         F.data_ptr())
+    ref = sht._ring_ffts(m, nside, lmax)
+    err = np.abs(F.cpu().numpy() - ref).max() / np.abs(ref).max()
+    G = rng.standard_normal((nr, lmax + 1)) + 1j * rng.standard_normal((nr, lmax + 1))
+    out = torch.empty(12 * nside * nside, dtype=torch.float64, device="cuda")
+    call("jfli_sht_ring_synthesis", stream_ptr(), torch.as_tensor(G, device="cuda").data_ptr(), nside, lmax,
+         out.data_ptr())
+    back = sht._ring_synth(G, nside, lmax)
+    err2 = np.abs(out.cpu().numpy() - back).max() / np.abs(back).max()
+    print(f"nside {nside} lmax {lmax}: analysis {err:.2e}, synthesis {err2:.2e}")
+    assert err < 1e-12 and err2 < 1e-12
