@@ -163,18 +163,30 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
   vel += b * g.np * 3;
   if (force) force += b * g.np * 4;
   if (rho) rho += b * g.np;
+  // positions and velocities stream through once per pass: streaming (evict-first) loads
+  // and stores, so that they do not push the force and density meshes out of L2
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
     particle_ijk(g, p, i, j, k);
-    float x0 = disp[3 * p + 0], x1 = disp[3 * p + 1], x2 = disp[3 * p + 2];
+    float x0 = __ldcs(disp + 3 * p + 0), x1 = __ldcs(disp + 3 * p + 1), x2 = __ldcs(disp + 3 * p + 2);
+    const bool use_v = flags & (kStepKick | kStepDrift);
+    float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+    if (use_v) {
+      v0 = __ldcs(vel + 3 * p + 0);
+      v1 = __ldcs(vel + 3 * p + 1);
+      v2 = __ldcs(vel + 3 * p + 2);
+    }
     if (flags & (kStepKick | kStepCorrect)) {
       const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
       float fx, fy, fz;
       gather_force_mesh(force, g, cx, cy, cz, fx, fy, fz);
       if (flags & kStepKick) {
-        vel[3 * p + 0] += fx * kick;
-        vel[3 * p + 1] += fy * kick;
-        vel[3 * p + 2] += fz * kick;
+        v0 += fx * kick;
+        v1 += fy * kick;
+        v2 += fz * kick;
+        __stcs(vel + 3 * p + 0, v0);
+        __stcs(vel + 3 * p + 1, v1);
+        __stcs(vel + 3 * p + 2, v2);
       } else {
         x0 += fx * kick;
         x1 += fy * kick;
@@ -182,14 +194,14 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
       }
     }
     if (flags & kStepDrift) {
-      x0 += vel[3 * p + 0] * drift;
-      x1 += vel[3 * p + 1] * drift;
-      x2 += vel[3 * p + 2] * drift;
+      x0 += v0 * drift;
+      x1 += v1 * drift;
+      x2 += v2 * drift;
     }
     if (flags & (kStepDrift | kStepCorrect)) {
-      disp[3 * p + 0] = x0;
-      disp[3 * p + 1] = x1;
-      disp[3 * p + 2] = x2;
+      __stcs(disp + 3 * p + 0, x0);
+      __stcs(disp + 3 * p + 1, x1);
+      __stcs(disp + 3 * p + 2, x2);
     }
     if (flags & kStepPaint) {
       const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
