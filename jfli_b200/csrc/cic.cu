@@ -247,7 +247,10 @@ __global__ void k_force_mesh4(const float* __restrict__ pot, float* __restrict__
   const float s = scale / 12.0f;
   const unsigned nq = g.np >> 2;  // groups of 4 cells
   const int nz4 = g.nz >> 2;
-  for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+  // the mesh is written tail first: its head, which the next particle pass (Lagrangian
+  // order, head first) gathers from first, is then the part still in L2
+  for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < nq; q0 += gridDim.x * blockDim.x) {
+    const unsigned q = nq - 1 - q0;
     const unsigned row = q / (unsigned)nz4;  // i * ny + j
     const int k0 = (int)(q - row * (unsigned)nz4) << 2;
     const int i = (int)(row / (unsigned)g.ny);
