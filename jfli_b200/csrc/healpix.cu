@@ -248,7 +248,14 @@ __global__ void __launch_bounds__(256, 4)
   if (weights) weights += b * g.np;
   map += b * npix;
   const float nx = (float)g.nx, ny = (float)g.ny, nz = (float)g.nz;
-  const float chi_max = vel ? tb.chi[tb.n_chi - 1] : 0.f;
+  // |q| below which the drift distance is inside the table: |q| itself (onion), or up to
+  // |q| + |observer| (telephoto's distance from the observer-centred replica)
+  float cm2 = 0.f;
+  if (vel) {
+    const float onorm = sqrtf(obs.x * obs.x + obs.y * obs.y + obs.z * obs.z);
+    const float cm = tb.chi[tb.n_chi - 1] * (1.f - 1e-5f) - 0.01f - (telephoto ? onorm : 0.f);
+    cm2 = cm > 0.f ? cm * cm * (1.f - 1e-6f) : -1.f;
+  }
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     float x, y, z;
     if (absolute) {
@@ -271,13 +278,21 @@ __global__ void __launch_bounds__(256, 4)
       vmag = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
     }
     const float w = weights ? weights[p] * weight : weight;
+    // skip bounds on the squared undrifted distance: a replica with |q| <= lo or |q| > hi
+    // cannot land in the shell (margin = dbound |v| + FP32 slack 4e-3 + 4e-6 |q|, solved
+    // for |q|; the squares widened by 1e-6 against rounding)
+    const float dv = dbound * vmag;
+    const float lo = (rmin - dv - 4e-3f) / (1.f + 4e-6f), hi = (rmax + dv + 4e-3f) / (1.f - 4e-6f);
+    const float lo2 = lo > 0.f ? lo * lo * (1.f - 1e-6f) : -1.f, hi2 = hi * hi * (1.f + 1e-6f);
     for (int tile = 0; tile < ts.n; ++tile) {
       const signed char* M = ts.m[tile];
       float q[3];
 #pragma unroll
       for (int r = 0; r < 3; ++r)
         q[r] = (float)M[3 * r + 0] * c[0] + (float)M[3 * r + 1] * c[1] + (float)M[3 * r + 2] * c[2] + ts.shift[tile][r];
-      const float qn = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+      const float qn2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+      // the bounds hold while the drift distance lies inside the distance table
+      if ((!vel || qn2 <= cm2) && (qn2 <= lo2 || qn2 > hi2)) continue;
       float px, py, pz;  // painted position, Mpc/h
       if (vel) {
         float dist;
@@ -287,10 +302,6 @@ __global__ void __launch_bounds__(256, 4)
         } else {
           const float ex = (q[0] + obs.x) - obs.x, ey = (q[1] + obs.y) - obs.y, ez = (q[2] + obs.z) - obs.z;
           dist = sqrtf(ex * ex + ey * ey + ez * ez);
-        }
-        if (dist <= chi_max) {
-          const float margin = dbound * vmag + 4e-3f + 4e-6f * qn;
-          if (qn + margin <= rmin || qn - margin > rmax) continue;
         }
         const float at = interp_table(dist, tb.chi, tb.a_chi, tb.n_chi);
         const float ac = sqrtf(t * at);
@@ -310,8 +321,6 @@ __global__ void __launch_bounds__(256, 4)
           pz = (q[2] + obs.z) + drift * vr[2];
         }
       } else {
-        const float margin = 4e-3f + 4e-6f * qn;
-        if (qn + margin <= rmin || qn - margin > rmax) continue;
         px = q[0] + obs.x;
         py = q[1] + obs.y;
         pz = q[2] + obs.z;
