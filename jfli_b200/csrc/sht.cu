@@ -18,7 +18,10 @@
 namespace jfli {
 
 constexpr int kShtThreads = 128;
-constexpr int kShtLTile = 32;
+constexpr int kShtLTile = 16;
+// row stride of the per-tile contributions (one row per l): one element of padding so that
+// the reduction's lanes, which read one element per row, fall in different banks
+constexpr int kShtRow = kShtThreads + 1;
 
 __host__ __device__ __forceinline__ long long alm_offset(int m, int lmax) {
   return (long long)m * (lmax + 1) - (long long)m * (m - 1) / 2;
@@ -71,7 +74,7 @@ __device__ __forceinline__ void legendre_coeffs(int l, int m, double& a, double&
 
 __global__ void __launch_bounds__(kShtThreads) k_sht_analysis(const double2* __restrict__ F, const double* __restrict__ z,
                                                                int nrings, int lmax, double w, double2* __restrict__ alm) {
-  extern __shared__ double2 contrib[];  // [kShtLTile][kShtThreads]
+  extern __shared__ double2 contrib[];  // [kShtLTile][kShtRow]
   __shared__ double coef[2][kShtLTile];
   __shared__ double2 part[kShtThreads / kShtLTile][kShtLTile];
   const int m = blockIdx.y;
@@ -97,14 +100,14 @@ __global__ void __launch_bounds__(kShtThreads) k_sht_analysis(const double2* __r
         lam = st.cur * st.escale;
       else if (l <= lmax)
         lam = legendre_step(st, zr, coef[0][t], coef[1][t]);
-      contrib[t * kShtThreads + threadIdx.x] = active ? make_double2(lam * f.x, lam * f.y) : make_double2(0.0, 0.0);
+      contrib[t * kShtRow + threadIdx.x] = active ? make_double2(lam * f.x, lam * f.y) : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    {  // thread (q, row): sum of 32 rings of one l
+    {  // thread (q, row): sum of kShtLTile rings of one l
       const int row = threadIdx.x & (kShtLTile - 1), q = threadIdx.x / kShtLTile;
       double sx = 0.0, sy = 0.0;
       for (int i = 0; i < kShtLTile; ++i) {
-        const double2 c = contrib[row * kShtThreads + q * kShtLTile + i];
+        const double2 c = contrib[row * kShtRow + q * kShtLTile + i];
         sx += c.x;
         sy += c.y;
       }
@@ -292,7 +295,7 @@ cudaError_t sht_analysis(const double* F, const double* z, int nrings, int lmax,
   const long long nalm = alm_offset(lmax + 1, lmax);
   cudaError_t e = cudaMemsetAsync(alm, 0, sizeof(double2) * (size_t)nalm, s);
   if (e != cudaSuccess) return e;
-  const size_t smem = sizeof(double2) * kShtLTile * kShtThreads;
+  const size_t smem = sizeof(double2) * kShtLTile * kShtRow;
   e = cudaFuncSetAttribute(k_sht_analysis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const dim3 grid((nrings + kShtThreads - 1) / kShtThreads, lmax + 1);
