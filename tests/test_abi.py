@@ -141,3 +141,39 @@ def test_tiled_paint_checks_rotations(lib):
     assert call([[2, 0, 0, 0, 1, 0, 0, 0, 1]]) == 1 and b"signed permutation" in buf.value
     assert call([[1, 0, 0, 0, 0, 0, 0, 0, 1]]) == 1 and b"signed permutation" in buf.value  # empty row
     assert call([[1, 0, 0, 0, 1, 0, 0, 0, 1]], ntiles=28) == 1 and b"ntiles" in buf.value
+
+
+def _bound(lib, name):
+    from jfli_b200 import _lib
+
+    res, args = _lib._SIGNATURES[name]
+    fn = getattr(lib, name)
+    fn.restype, fn.argtypes = res, args
+    return fn
+
+
+def test_flat_sky_entry_points_check_sizes(lib):
+    """jfli_paint_flat and jfli_flat_cl refuse bad map sizes, edge counts and workspaces
+    before any launch."""
+    buf = ctypes.create_string_buffer(256)
+    paint = _bound(lib, "jfli_paint_flat")
+    p = ctypes.c_void_p(256)
+    assert paint(None, p, 0, None, 1.0, 0.0, 1.0, 0, 16, p, 0, 16, 16, 16, 1, buf, 256) == 1
+    assert b"flat-sky map" in buf.value
+    cl = _bound(lib, "jfli_flat_cl")
+    assert cl(None, p, None, 64, 47, 1, 1.0, 1.0, p, 10, p, p, 1 << 20, buf, 256) == 3  # npy odd
+    assert b"unsupported" in buf.value
+    assert cl(None, p, None, 64, 64, 1, 1.0, 1.0, p, 2000, p, p, 1 << 20, buf, 256) == 1
+    assert b"nedges" in buf.value
+    assert cl(None, p, None, 64, 64, 1, 1.0, 1.0, p, 10, p, p, 16, buf, 256) == 1
+    assert b"workspace too small" in buf.value
+
+
+def test_sht_ring_entry_points_check_limits(lib):
+    buf = ctypes.create_string_buffer(256)
+    p = ctypes.c_void_p(256)
+    for name in ("jfli_sht_ring_analysis", "jfli_sht_ring_synthesis"):
+        fn = _bound(lib, name)
+        assert fn(None, p, 8192, 100, p, buf, 256) == 1 and b"nside" in buf.value
+        assert fn(None, p, 64, 9000, p, buf, 256) == 1 and b"lmax" in buf.value
+        assert fn(None, None, 64, 100, p, buf, 256) == 1 and b"null pointer" in buf.value
