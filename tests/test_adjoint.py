@@ -230,7 +230,7 @@ def test_full_chain_gradient_matches_oracle_fd():
 
 def test_differentiation_config_128_matches_gpu_fd():
     """128^3, box 500, 20 KKD steps from a = 0.1, 2LPT, 32-bin log-P loss against a
-    second seed; gradients (four random white-noise directions, Omega_c, sigma8) vs central
+    second seed; gradients (sixteen random white-noise directions, Omega_c, sigma8) vs central
     differences (eps = 1e-3) of the GPU forward."""
     import time
 
@@ -264,7 +264,7 @@ def test_differentiation_config_128_matches_gpu_fd():
     e = 1e-3
     gen = torch.Generator(device="cuda").manual_seed(12)
     pairs = []
-    for _ in range(4):  # four random white-noise directions
+    for _ in range(16):  # sixteen random white-noise directions
         r = torch.randn(n, n, n, device="cuda", generator=gen)
         g_w = float(torch.sum(w.grad.double() * r.double()))
         fd_w = (loss_at(w0 + e * r, oc, s8) - loss_at(w0 - e * r, oc, s8)) / (2 * e)
