@@ -32,6 +32,8 @@
  *   jfli_healpix_paint     <- _src/fields/_painting.py:249-348 (jaxpm paint_particles_spherical)
  *   jfli_lightcone_drift   <- pm/interp.py:110-121 (_drift_to_time) as used by DriftInterp.paint
  *                             (pm/interp.py:254-318)
+ *   jfli_replica_positions <- TelephotoInterp._paint_telephoto's transformed positions
+ *                             (pm/interp.py:666-685) for its flat-sky planes
  *   jfli_paint_flat        <- _src/fields/_painting.py:117-202 (_single_paint_2d, jaxpm cic_paint_2d)
  *                             behind ParticleField.paint_2d (fields/particles.py:234-320)
  *   jfli_flat_cl           <- _src/power/_compute.py:122-172 (_flat_cl) behind
@@ -193,6 +195,16 @@ int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, cons
                              const float* ga, const float* g, int n_g, const float* da, const float* dgfa, int n_d,
                              int nside, int scheme, float* map, int accumulate, int nx, int ny, int nz, int batch,
                              char* err, size_t errlen);
+
+/* Positions (Mpc/h, particle layout) of one replica of the particles: rotation (host,
+ * row-major signed permutation matrix) and shift (host, Mpc/h) applied to x - observer, and
+ * with vel the light-cone drift, exactly as one replica of jfli_healpix_paint_tiled (same
+ * telephoto convention). Feeds the flat-sky painter for TelephotoInterp planes beyond the box. */
+int jfli_replica_positions(void* stream, const float* disp, int absolute, const float* vel, float lx, float ly,
+                           float lz, float ox, float oy, float oz, const signed char* rotation, const float* shift,
+                           int telephoto, float t, float gp_t, const float* chi, const float* a_chi, int n_chi,
+                           const float* ga, const float* g, int n_g, const float* da, const float* dgfa, int n_d,
+                           float* out, int nx, int ny, int nz, int batch, char* err, size_t errlen);
 
 /* Flat-sky plane of the particles with zlo < z <= zhi (absolute grid units along z, from
  * the box origin): x and y scaled to the map (npx / nx, npy / ny), wrapped, deposited with

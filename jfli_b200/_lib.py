@@ -90,6 +90,12 @@ _SIGNATURES = {
         c_int,
         [c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_void_p, *_DIMS, *_ERR],
     ),
+    "jfli_replica_positions": (
+        c_int,
+        [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float,
+         ctypes.POINTER(ctypes.c_byte), ctypes.POINTER(c_float), c_int, c_float, c_float, c_void_p, c_void_p, c_int,
+         c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, *_DIMS, *_ERR],
+    ),
     "jfli_paint_flat": (
         c_int,
         [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_int, c_int, c_void_p, c_int, *_DIMS, *_ERR],

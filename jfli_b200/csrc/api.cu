@@ -483,6 +483,48 @@ int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, cons
                      err, errlen, "jfli_healpix_paint_tiled");
 }
 
+int jfli_replica_positions(void* stream, const float* disp, int absolute, const float* vel, float lx, float ly,
+                           float lz, float ox, float oy, float oz, const signed char* rotation, const float* shift,
+                           int telephoto, float t, float gp_t, const float* chi, const float* a_chi, int n_chi,
+                           const float* ga, const float* g, int n_g, const float* da, const float* dgfa, int n_d,
+                           float* out, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(out);
+  CHECK_PTR(rotation);
+  CHECK_PTR(shift);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  int used = 0;
+  for (int r = 0; r < 3; ++r) {
+    int nnz = 0;
+    for (int c = 0; c < 3; ++c) {
+      const int m = rotation[3 * r + c];
+      if (m == 0) continue;
+      if ((m != 1 && m != -1) || (used & (1 << c)))
+        return fail(err, errlen, JFLI_EINVAL, "rotation is not a signed permutation matrix");
+      used |= 1 << c;
+      ++nnz;
+    }
+    if (nnz != 1) return fail(err, errlen, JFLI_EINVAL, "rotation is not a signed permutation matrix");
+  }
+  if (vel) {
+    CHECK_PTR(chi);
+    CHECK_PTR(a_chi);
+    CHECK_PTR(ga);
+    CHECK_PTR(g);
+    CHECK_PTR(da);
+    CHECK_PTR(dgfa);
+    if (n_chi < 2 || n_g < 2 || n_d < 2) return fail(err, errlen, JFLI_EINVAL, "tables need at least 2 entries");
+    if (!(t > 0)) return fail(err, errlen, JFLI_EINVAL, "scale factor must be positive");
+  }
+  const MeshDims d{nx, ny, nz, batch};
+  const float box[3] = {lx, ly, lz}, obs[3] = {ox, oy, oz};
+  const jfli::DriftTables tb{chi, a_chi, n_chi, ga, g, n_g, da, dgfa, n_d};
+  return cuda_status(jfli::replica_positions(disp, absolute, vel, d, box, obs, rotation, shift, telephoto, t, gp_t, tb,
+                                             out, (cudaStream_t)stream),
+                     err, errlen, "jfli_replica_positions");
+}
+
 int jfli_paint_flat(void* stream, const float* disp, int absolute, const float* weights, float weight, float zlo,
                     float zhi, int npx, int npy, float* map, int accumulate, int nx, int ny, int nz, int batch,
                     char* err, size_t errlen) {

@@ -333,6 +333,84 @@ __global__ void __launch_bounds__(256, 4)
   }
 }
 
+// Positions (Mpc/h) of one rotated, shifted replica, drifted to the light cone when vel is
+// given, with the same conventions as k_healpix_paint_tiled (TelephotoInterp's flat planes
+// beyond the box paint these with the flat-sky painter, pm/interp.py:643-699).
+__global__ void k_replica_positions(const float* __restrict__ disp, int absolute, const float* __restrict__ vel,
+                                    PGrid g, float3 box, float3 obs, TileSet ts, int telephoto, float t, float gp_t,
+                                    DriftTables tb, float* __restrict__ out) {
+  const long long b = blockIdx.y;
+  disp += b * g.np * 3;
+  out += b * g.np * 3;
+  if (vel) vel += b * g.np * 3;
+  const float nx = (float)g.nx, ny = (float)g.ny, nz = (float)g.nz;
+  const signed char* M = ts.m[0];
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    float x, y, z;
+    if (absolute) {
+      x = disp[3 * p + 0] / nx * box.x;
+      y = disp[3 * p + 1] / ny * box.y;
+      z = disp[3 * p + 2] / nz * box.z;
+    } else {
+      int i, j, k;
+      particle_ijk(g, p, i, j, k);
+      x = ((float)i + disp[3 * p + 0]) / nx * box.x;
+      y = ((float)j + disp[3 * p + 1]) / ny * box.y;
+      z = ((float)k + disp[3 * p + 2]) / nz * box.z;
+    }
+    const float c[3] = {x - obs.x, y - obs.y, z - obs.z};
+    float q[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      q[r] = (float)M[3 * r + 0] * c[0] + (float)M[3 * r + 1] * c[1] + (float)M[3 * r + 2] * c[2] + ts.shift[0][r];
+    float o[3] = {q[0] + obs.x, q[1] + obs.y, q[2] + obs.z};
+    if (vel) {
+      const float v[3] = {vel[3 * p + 0], vel[3 * p + 1], vel[3 * p + 2]};
+      float vr[3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        vr[r] = (float)M[3 * r + 0] * v[0] + (float)M[3 * r + 1] * v[1] + (float)M[3 * r + 2] * v[2];
+      float dist;
+      if (telephoto) {
+        const float ex = q[0] - obs.x, ey = q[1] - obs.y, ez = q[2] - obs.z;
+        dist = sqrtf(ex * ex + ey * ey + ez * ez);
+      } else {
+        const float ex = o[0] - obs.x, ey = o[1] - obs.y, ez = o[2] - obs.z;
+        dist = sqrtf(ex * ex + ey * ey + ez * ez);
+      }
+      const float at = interp_table(dist, tb.chi, tb.a_chi, tb.n_chi);
+      const float ac = sqrtf(t * at);
+      const float gp_at = fminf(fmaxf(interp_table(at, tb.ga, tb.g, tb.n_g), 0.f), 1.f);
+      const float drift = (gp_at - gp_t) / interp_table(ac, tb.da, tb.dgfa, tb.n_d);
+      if (telephoto) {
+        const float ob[3] = {obs.x, obs.y, obs.z};
+#pragma unroll
+        for (int r = 0; r < 3; ++r) o[r] = (q[r] + drift * vr[r]) + ob[r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) o[r] = o[r] + drift * vr[r];
+      }
+    }
+    out[3 * p + 0] = o[0];
+    out[3 * p + 1] = o[1];
+    out[3 * p + 2] = o[2];
+  }
+}
+
+cudaError_t replica_positions(const float* disp, int absolute, const float* vel, const MeshDims& d, const float* box,
+                              const float* observer, const signed char* rotation, const float* shift, int telephoto,
+                              float t, float gp_t, const DriftTables& tb, float* out, cudaStream_t s) {
+  TileSet ts;
+  ts.n = 1;
+  for (int e = 0; e < 9; ++e) ts.m[0][e] = rotation[e];
+  for (int e = 0; e < 3; ++e) ts.shift[0][e] = shift[e];
+  k_replica_positions<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(
+      disp, absolute, vel, make_pgrid(d), make_float3(box[0], box[1], box[2]),
+      make_float3(observer[0], observer[1], observer[2]), ts, telephoto, t, gp_t, tb, out);
+  note_launch();
+  return cudaGetLastError();
+}
+
 // FP64 colatitudes of rings 0 .. 4 nside (entries 0 and 4 nside unused), one table per
 // (device, nside), built once on the host: polar-cap rings from z = 1 - north^2 4 / npix
 // (colatitude via atan2 of sin and cos), equatorial rings from z = (2 nside - north) 2 / (3 nside).

@@ -124,6 +124,9 @@ cudaError_t power_finalize(const double* partials, int nctas, int nbins, double*
 cudaError_t healpix_paint(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d,
                           const float* box, const float* observer, float rmin, float rmax, int nside, int scheme,
                           float* map, cudaStream_t s);
+cudaError_t replica_positions(const float* disp, int absolute, const float* vel, const MeshDims& d, const float* box,
+                              const float* observer, const signed char* rotation, const float* shift, int telephoto,
+                              float t, float gp_t, const DriftTables& tb, float* out, cudaStream_t s);
 cudaError_t healpix_paint_tiled(const float* disp, int absolute, const float* vel, const float* weights, float weight,
                                 const MeshDims& d, const float* box, const float* observer, int ntiles,
                                 const signed char* rotations, const float* shifts, int telephoto, float rmin,

@@ -271,6 +271,38 @@ def drift_tables(cosmo, n_dense: int = 4096):
     return tuple(torch.as_tensor(np.ascontiguousarray(t, dtype=np.float32), device="cuda") for t in tabs)
 
 
+def replica_positions(pos: torch.Tensor, box_size, observer_mpc, rotation, shift, *, absolute: bool = False,
+                      vel: torch.Tensor | None = None, t: float | None = None, cosmo=None, telephoto: bool = False,
+                      tables=None) -> torch.Tensor:
+    """Mpc/h positions of one rotated, shifted (and, with vel, light-cone drifted) replica
+    of the particles (see jfli_replica_positions)."""
+    from . import cosmology as cj
+
+    _check(pos, "pos")
+    (nx, ny, nz), batch, _ = _mesh_dims(pos, True)
+    rot = np.ascontiguousarray(np.rint(np.asarray(rotation, np.float64)).astype(np.int8).reshape(9))
+    sh = np.ascontiguousarray(np.asarray(shift, np.float32).reshape(3))
+    tabs = (None,) * 6
+    t_arg = gp_t = 0.0
+    if vel is not None:
+        _check(vel, "vel")
+        if t is None or cosmo is None:
+            raise ValueError("the light-cone drift needs the time t and the cosmology")
+        tabs = drift_tables(cosmo) if tables is None else tables
+        t_arg = float(t)
+        gp_t = float(cj.Gp(cosmo, t_arg))
+    chi, a_chi, ga, g, da, dg = tabs
+    n = lambda x: int(x.numel()) if x is not None else 0
+    out = torch.empty_like(pos)
+    lx, ly, lz = (float(v) for v in box_size)
+    ox, oy, oz = (float(v) for v in observer_mpc)
+    call("jfli_replica_positions", stream_ptr(), ptr(pos), int(absolute), ptr(vel), lx, ly, lz, ox, oy, oz,
+         rot.ctypes.data_as(ctypes.POINTER(ctypes.c_byte)), sh.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+         int(bool(telephoto)), t_arg, gp_t, ptr(chi), ptr(a_chi), n(chi), ptr(ga), ptr(g), n(ga), ptr(da), ptr(dg),
+         n(da), ptr(out), nx, ny, nz, batch)
+    return out
+
+
 def paint_flat(pos: torch.Tensor, npix, zlo: float, zhi: float, *, absolute: bool = False,
                weights: torch.Tensor | None = None, weight: float = 1.0, out: torch.Tensor | None = None,
                accumulate: bool = False) -> torch.Tensor:

@@ -222,8 +222,8 @@ class TelephotoInterp(AbstractInterp):
     shell centre lies beyond the box; the replica is the box rotated by the index's cube
     symmetry (of the 47, cyclically) and pushed along z by floor(r / R) R, R the largest
     radius the box holds. The drift distance is measured as the reference measures it,
-    from the observer-centred replica minus the observer's position. Flat-sky targets are
-    painted for planes inside the box; beyond it, spherical only."""
+    from the observer-centred replica minus the observer's position. Spherical shells and
+    flat-sky planes, inside the box and beyond it."""
 
     drift_on_lightcone: bool = True
 
@@ -267,12 +267,20 @@ class TelephotoInterp(AbstractInterp):
             from ..fields import SphericalDensity
             from ..painting import paint_shell_tiled
 
-            if pt.target == "flat":
-                raise NotImplementedError("TelephotoInterp: flat-sky planes beyond the box (a rotated, pushed "
-                                          "replica) are not on the B200 path; planes inside the box are")
             rot = state.rotations[state.rotation_idx % 47][None]
             R = self.max_comoving_distance
             shift = np.array([[0.0, 0.0, math.floor(r_center / R) * R]])
+            if pt.target == "flat":  # the replica's positions, then the flat-sky painter
+                from .. import ops
+
+                rel = dx if dx.unit != PositionUnit.MPC_H else dx.to(PositionUnit.GRID_ABSOLUTE)
+                pos = ops.replica_positions(rel.array.contiguous(), dx.box_size, dx.observer_position_mpc, rot[0],
+                                            shift[0], absolute=rel.unit == PositionUnit.GRID_ABSOLUTE,
+                                            vel=p.array.contiguous() if self.drift_on_lightcone else None,
+                                            t=float(t), cosmo=cosmo, telephoto=True)
+                res = dx.replace(array=pos, unit=PositionUnit.MPC_H).paint_2d(
+                    center=r_center, density_plane_width=width, weights=pt.weights, batch_size=pt.batch_size)
+                return res.replace(scale_factors=t, comoving_centers=r_center, density_width=width)
             m = paint_shell_tiled(dx, p.array if self.drift_on_lightcone else None, r_center, width, rot, shift,
                                   telephoto=True, t=float(t), cosmo=cosmo, scheme=pt.scheme, weights=pt.weights)
             res = SphericalDensity.FromDensityMetadata(array=m, field=dx)

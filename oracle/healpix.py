@@ -150,6 +150,31 @@ def paint_shell(pos_mpc, observer, rmin, rmax, nside, scheme="bilinear", weight=
     return np.bincount(pix.ravel(), weights=w.ravel() * weight, minlength=npix)
 
 
+def replica_positions(disp, vel, box, observer, R, shift, *, telephoto=False, t=None, a_of_chi=None, Gp=None,
+                      dGfa=None):
+    """Mpc/h positions (FP64, flattened to (P, 3)) of one replica: c = x - o with
+    x = (grid + disp) / N * L, q = R c + s; with velocities drifted along R v by
+    (Gp(a_t) - Gp(t)) / dGfa(sqrt(t a_t)), a_t = a_of_chi(distance), the distance being
+    |q + o - o| (onion) or |q - o| (telephoto, as the reference measures it); the
+    position q + o (+ the drift). TelephotoInterp._paint_telephoto (pm/interp.py:643-699)
+    and one replica of OnionTiler._paint_tiled_27 (pm/interp.py:418-504)."""
+    shape = disp.shape[:3]
+    n = np.asarray(shape, np.float64)
+    L = np.asarray(box, np.float64)
+    o = np.asarray(observer, np.float64)
+    g = np.stack(np.meshgrid(*[np.arange(k, dtype=np.float64) for k in shape], indexing="ij"), axis=-1)
+    c = ((g + disp.astype(np.float64)) / n * L - o).reshape(-1, 3)
+    R = np.asarray(R, np.float64)
+    q = c @ R.T + np.asarray(shift, np.float64)
+    if vel is None:
+        return q + o
+    vr = vel.astype(np.float64).reshape(-1, 3) @ R.T
+    dist = np.linalg.norm(q - o, axis=-1) if telephoto else np.linalg.norm((q + o) - o, axis=-1)
+    at = a_of_chi(dist)
+    d = (Gp(at) - Gp(t)) / dGfa(np.sqrt(t * at))
+    return (q + d[:, None] * vr) + o if telephoto else (q + o) + d[:, None] * vr
+
+
 def paint_shell_tiled(disp, vel, box, observer, rmin, rmax, nside, rotations, shifts, *, telephoto=False, t=None,
                       a_of_chi=None, Gp=None, dGfa=None, scheme="bilinear", weight=1.0):
     """Raw weight sums of the rotated and shifted replicas of the particles (FP64), every

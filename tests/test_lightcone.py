@@ -251,3 +251,44 @@ def test_lightcone_shells_are_their_own_shells(cosmo):
         # few particles across the shell edges
         assert err < 2e-2
         assert abs(got.mean() / ref.mean() - 1) < 2e-3
+
+
+def test_replica_positions_and_telephoto_flat_plane(cosmo):
+    """One rotated, pushed replica drifted to the light cone (TelephotoInterp's transform)
+    against the FP64 oracle, and the flat-sky plane TelephotoInterp paints from it beyond
+    the box against the oracle positions painted flat."""
+    from jfli_b200.pm.interp import get_all_47_symmetries
+    from oracle import flat as of
+
+    n, L = 32, 200.0
+    disp, vel = _state(n, 24, amp=1.5)
+    obs = (100.0, 100.0, 100.0)
+    R, shift = get_all_47_symmetries()[7], np.array([0.0, 0.0, 200.0])
+    t = float(cj.a_of_chi(cosmo, 230.0))
+    got = ops.replica_positions(torch.as_tensor(disp, device="cuda"), (L, L, L), obs, R, shift,
+                                vel=torch.as_tensor(vel, device="cuda"), t=t, cosmo=cosmo,
+                                telephoto=True).cpu().numpy().reshape(-1, 3)
+    ref = oh.replica_positions(disp, vel, (L, L, L), obs, R, shift, telephoto=True, t=t, **_funcs(cosmo))
+    err = np.abs(got - ref).max()
+    print(f"replica positions: max |GPU - oracle| {err:.2e} Mpc/h")
+    assert err < 2e-3  # FP32 positions up to ~400 Mpc/h (ulp 3e-5) plus table rounding
+
+    noise = jf.white_noise(3, (n, n, n))
+    ic = jf.interpolate_initial_conditions(noise, (n, n, n), (L, L, L), cosmo=cosmo, flatsky_npix=(48, 48))
+    dx, p = jf.lpt(cosmo, ic, ts=0.5, order=1)
+    dx = dx.replace(array=torch.as_tensor(disp, device="cuda"))
+    p = p.replace(array=torch.as_tensor(vel, device="cuda"))
+    rc, wd = 230.0, 40.0  # beyond the 100 Mpc/h the box holds around its centre
+    interp = jf.TelephotoInterp(painting=jf.PaintingOptions(target="flat")).update_geometry(
+        np.array([t]), np.array([rc]), np.array([wd]), 100.0)
+    st = interp.advance(interp.init(), t)
+    assert st.shell_idx == 0 and st.rotation_idx == 0
+    plane = interp.paint(st, t, (dx, p), cosmo).array.cpu().numpy()
+    rot = st.rotations[0]
+    pos = oh.replica_positions(disp, vel, (L, L, L), obs, rot, np.array([0.0, 0.0, 200.0]), telephoto=True, t=t,
+                               **_funcs(cosmo))
+    cg, wg = rc * n / L, wd * n / L
+    ref_plane = of.paint_2d(pos / L * n, (48, 48), cg - wg / 2, cg + wg / 2, (n, n, n)) / ((L / 48) ** 2 * wd)
+    e2 = rel_l2(plane, ref_plane)
+    print(f"telephoto flat plane: weight {ref_plane.sum():.3e}, rel L2 {e2:.2e}")
+    assert ref_plane.sum() > 0 and e2 < 1e-3
