@@ -240,13 +240,21 @@ __global__ void k_force_mesh(const float* __restrict__ pot, float* __restrict__ 
 
 // The same stencil for four consecutive z cells per thread (nz % 4 == 0): 11 aligned
 // 16-byte loads and 4 16-byte stores per 4 cells, row offsets and wraps shared.
-__global__ void k_force_mesh4(const float* __restrict__ pot, float* __restrict__ F, float scale, PGrid g) {
+constexpr int kForceMeshThreads = 256;
+
+__global__ void __launch_bounds__(kForceMeshThreads) k_force_mesh4(const float* __restrict__ pot,
+                                                                   float* __restrict__ F, float scale, PGrid g) {
   const long long b = blockIdx.y;
   pot += b * g.np;
   F += b * g.np * 4;
   const float s = scale / 12.0f;
   const unsigned nq = g.np >> 2;  // groups of 4 cells
   const int nz4 = g.nz >> 2;
+  // A warp's 32 groups are 128 consecutive cells: their float4 results go through shared
+  // memory so that each store instruction writes 512 contiguous bytes (a thread's own four
+  // cells would make every store half-fill 32 sectors).
+  __shared__ float4 stage[kForceMeshThreads / 32][128];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // the mesh is written tail first: its head, which the next particle pass (Lagrangian
   // order, head first) gathers from first, is then the part still in L2
   for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < nq; q0 += gridDim.x * blockDim.x) {
@@ -275,11 +283,28 @@ __global__ void k_force_mesh4(const float* __restrict__ pot, float* __restrict__
     const float fx2[4] = {xp2.x - xm2.x, xp2.y - xm2.y, xp2.z - xm2.z, xp2.w - xm2.w};
     const float fy[4] = {yp1.x - ym1.x, yp1.y - ym1.y, yp1.z - ym1.z, yp1.w - ym1.w};
     const float fy2[4] = {yp2.x - ym2.x, yp2.y - ym2.y, yp2.z - ym2.z, yp2.w - ym2.w};
-    float4* out = reinterpret_cast<float4*>(F) + (xo + yo + k0);
+    float4 res[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const float gz = -(8.0f * (w[5 + t] - w[3 + t]) - (w[6 + t] - w[2 + t])) * s;
-      out[t] = make_float4(-(8.0f * fx[t] - fx2[t]) * s, -(8.0f * fy[t] - fy2[t]) * s, gz, 0.f);
+      res[t] = make_float4(-(8.0f * fx[t] - fx2[t]) * s, -(8.0f * fy[t] - fy2[t]) * s, gz, 0.f);
+    }
+    // the whole warp is in this iteration when its last lane's group exists (q0 of lane L
+    // is the warp's first q0 plus L: block size and grid stride are multiples of 32)
+    const unsigned q0_first = q0 - lane;
+    if (q0_first + 31 < nq) {
+      const unsigned q_min = nq - 1 - (q0_first + 31);  // group of lane 31; lane L holds q_min + 31 - L
+#pragma unroll
+      for (int t = 0; t < 4; ++t) stage[warp][4 * (31 - lane) + t] = res[t];
+      __syncwarp();
+      float4* base = reinterpret_cast<float4*>(F) + 4ull * q_min;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) base[32 * t + lane] = stage[warp][32 * t + lane];
+      __syncwarp();
+    } else {
+      float4* out = reinterpret_cast<float4*>(F) + (xo + yo + k0);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) out[t] = res[t];
     }
   }
 }
@@ -494,8 +519,8 @@ cudaError_t kick_drift_paint_slots(float* disp, float* vel, const float* force, 
 cudaError_t force_mesh(const float* pot, float* force, float scale, const MeshDims& d, cudaStream_t s) {
   const bool vec4 = d.nz % 4 == 0 && d.nz >= 8 && ((uintptr_t)pot % 16) == 0 && ((uintptr_t)force % 16) == 0;
   if (vec4)
-    k_force_mesh4<<<particle_grid_dims(d.cells() / 4, d.batch, 256, 16), 256, 0, s>>>(pot, force, scale,
-                                                                                     make_pgrid(d));
+    k_force_mesh4<<<particle_grid_dims(d.cells() / 4, d.batch, kForceMeshThreads, 16), kForceMeshThreads, 0, s>>>(
+        pot, force, scale, make_pgrid(d));
   else
     k_force_mesh<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, force, scale, make_pgrid(d));
   note_launch();
