@@ -104,8 +104,9 @@ def test_pm_forces_matches_oracle(n, scale):
     assert rel_l2(f, ref) < 1e-5
 
 
+# (12, 12, 12) and (6, 18, 20): 432 and 540 groups of 4 cells, so the last warp is partial
 @pytest.mark.parametrize("shape", [(32, 32, 32), (16, 24, 36), (12, 20, 42), (8, 8, 4), (16, 16, 64),
-                                   (48, 32, 128), (64, 64, 64)])
+                                   (48, 32, 128), (64, 64, 64), (12, 12, 12), (6, 18, 20)])
 def test_force_mesh_matches_stencil(shape):
     """Force mesh -D pot: 2.5D-blocked path (nx % 16, ny % 16, nz % 64 == 0), four-cell
     vectorised path (nz % 4 == 0, nz >= 8), scalar path otherwise."""
