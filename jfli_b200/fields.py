@@ -178,6 +178,11 @@ class PowerSpectrum:
 
 @dataclasses.dataclass(frozen=True, eq=False)
 class DensityField(AbstractField):
+    def to(self, unit, *, omega_m=None, h=None, mean_density=None) -> "DensityField":
+        """Unit conversion with the voxel volume prod(L / N) (reference fields/density.py:66-124)."""
+        vol = float(np.prod(np.asarray(self.box_size, np.float64) / np.asarray(self.mesh_size, np.float64)))
+        return _density_to(self, unit, vol, omega_m, h, mean_density)
+
     def power(self, mesh2: "DensityField" | None = None, *, kedges=None, multipoles=0, los=(0.0, 0.0, 1.0),
               batch_size=None) -> PowerSpectrum:
         """P(k) of the mesh (reference fields/density.py:275-318)."""
@@ -194,9 +199,21 @@ class SphericalDensity(AbstractField):
     def _core_ndim(self) -> int:
         return 1
 
+    def to(self, unit, *, omega_m=None, h=None, mean_density=None) -> "SphericalDensity":
+        """Unit conversion with each shell's exact pixel volume (4 pi / npix)(R_max^3 - R_min^3) / 3
+        (reference fields/lightcone.py:480-535)."""
+        if self.unit == unit:
+            return self
+        if self.comoving_centers is None or self.density_width is None:
+            raise ValueError("comoving_centers and density_width metadata are required for unit conversion.")
+        c = np.asarray(self.comoving_centers, np.float64)
+        w = np.asarray(self.density_width, np.float64)
+        vol = 4.0 * np.pi / (12 * self.nside * self.nside) * ((c + w / 2) ** 3 - (c - w / 2) ** 3) / 3.0
+        return _density_to(self, unit, vol, omega_m, h, mean_density)
+
     def angular_cl(self, lmax: int | None = None):
-        """Angular power spectrum of each map (healpy's anafast algorithm: FP64 Legendre
-        stages on the GPU, ring FFTs on the host)."""
+        """Angular power spectrum of each map (healpy's anafast algorithm on the GPU: ring
+        transforms and Legendre stages in FP64)."""
         from .sht import anafast
 
         maps = self.array.detach().double().cpu().numpy()
@@ -222,6 +239,14 @@ class FlatDensity(AbstractField):
         if tuple(self.array.shape[-2:]) != tuple(self.flatsky_npix):
             raise ValueError(f"Array spatial shape {tuple(self.array.shape[-2:])} does not match flatsky_npix "
                              f"{tuple(self.flatsky_npix)}.")
+
+    def to(self, unit, *, omega_m=None, h=None, mean_density=None) -> "FlatDensity":
+        """Unit conversion with the pixel volume the reference's FlatDensity.to uses
+        (fields/lightcone.py:51-98): (L_x / flatsky_npix[1]) (L_y / flatsky_npix[0]) width."""
+        ny_pix, nx_pix = self.flatsky_npix
+        Lx, Ly, _ = self.box_size
+        vol = (Lx / nx_pix) * (Ly / ny_pix) * np.asarray(self.density_width, np.float64)
+        return _density_to(self, unit, vol, omega_m, h, mean_density)
 
     def angular_cl(self, mesh2: "FlatDensity | None" = None, *, field_size=None, pixel_size=None, ell_edges=None,
                    batch_size=None) -> PowerSpectrum:
@@ -382,6 +407,69 @@ def uniform_particles(mesh_size, device="cuda") -> torch.Tensor:
     return torch.stack(g, dim=-1)
 
 
-def convert_units(array, origin, destination, mesh_size, box_size, **_):
-    f = ParticleField(array=array, mesh_size=tuple(mesh_size), box_size=tuple(box_size), unit=origin)
-    return f.to(destination).array
+def convert_units(array, origin, destination, mesh_size, box_size, h=None, omega_m=None, mean_density=None,
+                  volume_element=None, sharding=None):
+    """Convert an array between units of one family (reference fields/units.py:22-258):
+    positions through GRID_ABSOLUTE, densities through DENSITY (particles per (Mpc/h)^3)."""
+    if origin == destination:
+        return array
+    if type(origin) is not type(destination):
+        raise TypeError(f"Cannot convert between different unit families: {type(origin).__name__} -> "
+                        f"{type(destination).__name__}")
+    if isinstance(origin, PositionUnit):
+        f = ParticleField(array=array, mesh_size=tuple(mesh_size), box_size=tuple(box_size), unit=origin)
+        return f.to(destination).array
+    if isinstance(origin, DensityUnit):
+        return _convert_density(array, origin, destination, volume_element, omega_m, h, mean_density)
+    raise NotImplementedError(f"Conversion not implemented for {type(origin).__name__}")
+
+
+def _convert_density(array, origin, destination, volume_element, omega_m, h, mean_density):
+    """DENSITY as the hub (reference fields/units.py:133-258): COUNTS = DENSITY x V,
+    OVERDENSITY = DENSITY / mean - 1 (mean of the array when not given), MSUN_H_PER_MPC3 =
+    DENSITY x (Omega_m 2.775e11 h^2 V / h^3) h, V the volume per voxel or pixel in (Mpc/h)^3
+    (one value, or one per leading entry)."""
+    if volume_element is None:
+        raise ValueError("volume_element is required for density unit conversions")
+    x = array if isinstance(array, torch.Tensor) else torch.as_tensor(np.asarray(array))
+    v = torch.as_tensor(np.asarray(volume_element, dtype=np.float64), dtype=x.dtype, device=x.device)
+    v = v.reshape(v.shape + (1,) * (x.ndim - v.ndim))
+    mass = None
+    if DensityUnit.MSUN_H_PER_MPC3 in (origin, destination):
+        if omega_m is None or h is None:
+            raise ValueError("omega_m and h required for MSUN_H_PER_MPC3 conversion")
+        mass = omega_m * 2.775e11 * h**2 * (v / h**3)  # solar masses per particle at mean 1 per voxel
+    if origin == DensityUnit.DENSITY:
+        density = x
+    elif origin == DensityUnit.COUNTS:
+        density = x / v
+    elif origin == DensityUnit.OVERDENSITY:
+        if mean_density is None:
+            raise ValueError("mean_density required to convert from OVERDENSITY")
+        density = (x + 1.0) * mean_density
+    elif origin == DensityUnit.MSUN_H_PER_MPC3:
+        density = (x * v / h) / mass / v
+    else:
+        raise ValueError(f"Unknown origin unit: {origin}")
+    if destination == DensityUnit.DENSITY:
+        return density
+    if destination == DensityUnit.COUNTS:
+        return density * v
+    if destination == DensityUnit.OVERDENSITY:
+        mean = density.mean() if mean_density is None else torch.as_tensor(mean_density, dtype=x.dtype)
+        eps = torch.finfo(density.dtype).eps
+        safe = torch.where(mean == 0, torch.as_tensor(eps, dtype=x.dtype, device=x.device), mean)
+        return density / safe - 1.0
+    if destination == DensityUnit.MSUN_H_PER_MPC3:
+        return density * v * mass * h / v
+    raise ValueError(f"Unknown destination unit: {destination}")
+
+
+def _density_to(field, unit, volume_element, omega_m, h, mean_density):
+    if field.unit == unit:
+        return field
+    if not isinstance(unit, DensityUnit):
+        raise TypeError(f"{type(field).__name__}.to() expected a DensityUnit for 'unit', got {unit!r}")
+    arr = convert_units(field.array, field.unit, unit, field.mesh_size, field.box_size, h=h, omega_m=omega_m,
+                        mean_density=mean_density, volume_element=volume_element)
+    return field.replace(array=arr, unit=unit)
