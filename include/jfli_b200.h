@@ -29,6 +29,7 @@
  *   jfli_ic_filter         <- initial.py:167-182 (interpolate_initial_conditions), infer/dist.py:43-79
  *   jfli_lpt               <- pm/lpt.py:119 (jaxpm lpt, order 1 and 2)
  *   jfli_power_spectrum    <- _src/power/_compute.py:23-119 (_initialize_pk + _power)
+ *   jfli_power_poles       <- the same _power with mesh2 (cross) and multipoles != 0
  *   jfli_healpix_paint     <- _src/fields/_painting.py:249-348 (jaxpm paint_particles_spherical)
  *   jfli_lightcone_drift   <- pm/interp.py:110-121 (_drift_to_time) as used by DriftInterp.paint
  *                             (pm/interp.py:254-318)
@@ -169,6 +170,20 @@ size_t jfli_power_spectrum_workspace_bytes(int nx, int ny, int nz, int batch, in
 int jfli_power_spectrum(void* stream, const float* mesh, const float* kedges, int nedges, float lx, float ly,
                         float lz, double* out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
                         int batch, char* err, size_t errlen);
+
+/* Cross spectra and multipoles: FP64 sums over the full Fourier grid of `mesh` (and
+ * `mesh2`, or mesh itself when NULL), ortho normalisation, binned by numpy.digitize(|k|,
+ * kedges). For each multipole l = ells[e] (host array, nell <= 8, l <= 16):
+ *   out[batch][2e][bin], out[batch][2e+1][bin] = sums of Re, Im of (2l + 1) L_l(mu) F1 conj(F2)
+ * with mu = (k . los) / |k| (0 at k = 0); then out[batch][2 nell] = mode count and
+ * out[batch][2 nell + 1] = sum of |k|. nedges <= 512. The caller forms |sum| (cross) or the
+ * real sum (auto), divides by the count, drops bins 0 and nedges and multiplies by
+ * prod(L/N). Workspace: jfli_power_poles_workspace_bytes (cross = mesh2 != NULL). */
+size_t jfli_power_poles_workspace_bytes(int nx, int ny, int nz, int batch, int nedges, int nell, int cross);
+int jfli_power_poles(void* stream, const float* mesh, const float* mesh2, const float* kedges, int nedges, float lx,
+                     float ly, float lz, float losx, float losy, float losz, const int* ells, int nell, double* out,
+                     void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                     size_t errlen);
 
 /* HEALPix RING-ordered shell map of the particles with rmin < |x - observer| <= rmax
  * (Mpc/h), deposited by `scheme` (JFLI_HEALPIX_NGP or JFLI_HEALPIX_BILINEAR).

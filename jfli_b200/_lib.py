@@ -96,6 +96,12 @@ _SIGNATURES = {
          ctypes.POINTER(ctypes.c_byte), ctypes.POINTER(c_float), c_int, c_float, c_float, c_void_p, c_void_p, c_int,
          c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, *_DIMS, *_ERR],
     ),
+    "jfli_power_poles_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_int, c_int, c_int, c_int]),
+    "jfli_power_poles": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_float, c_float, c_float,
+         ctypes.POINTER(c_int), c_int, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
+    ),
     "jfli_paint_flat": (
         c_int,
         [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_int, c_int, c_void_p, c_int, *_DIMS, *_ERR],

@@ -399,6 +399,42 @@ int jfli_power_spectrum(void* stream, const float* mesh, const float* kedges, in
   return cuda_status(e, err, errlen, "jfli_power_spectrum");
 }
 
+size_t jfli_power_poles_workspace_bytes(int nx, int ny, int nz, int batch, int nedges, int nell, int cross) {
+  if (nedges < 1 || nell < 1) return 0;
+  const MeshDims d{nx, ny, nz, batch};
+  return spec_bytes(d) * (cross ? 2 : 1) +
+         align256(sizeof(double) * (size_t)(2 * nell + 2) * (nedges + 1) * jfli::power_poles_ctas(d) * batch);
+}
+
+int jfli_power_poles(void* stream, const float* mesh, const float* mesh2, const float* kedges, int nedges, float lx,
+                     float ly, float lz, float losx, float losy, float losz, const int* ells, int nell, double* out,
+                     void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                     size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(mesh);
+  CHECK_PTR(kedges);
+  CHECK_PTR(ells);
+  CHECK_PTR(out);
+  CHECK_PTR(workspace);
+  if (nedges < 1 || nedges > 512) return fail(err, errlen, JFLI_EINVAL, "nedges %d outside [1, 512]", nedges);
+  if (nell < 1 || nell > 8) return fail(err, errlen, JFLI_EINVAL, "%d multipoles outside [1, 8]", nell);
+  for (int i = 0; i < nell; ++i)
+    if (ells[i] < 0 || ells[i] > 16) return fail(err, errlen, JFLI_EINVAL, "multipole %d outside [0, 16]", ells[i]);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  const size_t need = jfli_power_poles_workspace_bytes(nx, ny, nz, batch, nedges, nell, mesh2 != nullptr);
+  if (workspace_bytes < need)
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  float2* s1 = (float2*)workspace;
+  float2* s2 = mesh2 ? (float2*)((char*)workspace + spec_bytes(d)) : nullptr;
+  double* partials = (double*)((char*)workspace + spec_bytes(d) * (mesh2 ? 2 : 1));
+  const float box[3] = {lx, ly, lz}, los[3] = {losx, losy, losz};
+  return cuda_status(jfli::power_poles(mesh, mesh2, d, kedges, nedges, box, los, ells, nell, s1, s2, partials, out,
+                                       (cudaStream_t)stream),
+                     err, errlen, "jfli_power_poles");
+}
+
 int jfli_healpix_paint(void* stream, const float* disp, int absolute, const float* weights, float weight, float lx,
                        float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside, int scheme,
                        float* map, int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen) {

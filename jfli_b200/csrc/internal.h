@@ -119,6 +119,12 @@ cudaError_t power_partials_noalloc(const float* mesh, float2* spec, double* part
 
 // ---- spectra.cu ----
 cudaError_t power_finalize(const double* partials, int nctas, int nbins, double* out, int batch, cudaStream_t s);
+cudaError_t sums_finalize(const double* partials, int nctas, int nvals, double* out, int batch, cudaStream_t s);
+// ---- poles.cu ----
+int power_poles_ctas(const MeshDims& d);
+cudaError_t power_poles(const float* mesh1, const float* mesh2, const MeshDims& d, const float* kedges, int nedges,
+                        const float* box, const float* los, const int* ells, int nell, float2* spec1, float2* spec2,
+                        double* partials, double* out, cudaStream_t s);
 
 // ---- healpix.cu ----
 cudaError_t healpix_paint(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d,

@@ -23,6 +23,14 @@ __global__ void k_power_finalize(const double* __restrict__ partials, int nctas,
   out[(long long)b * nvals + v] = s;
 }
 
+// The same fixed-order reduction for nvals values per CTA (layout [batch][nctas][nvals]).
+cudaError_t sums_finalize(const double* partials, int nctas, int nvals, double* out, int batch, cudaStream_t s) {
+  const int total = nvals * batch;
+  k_power_finalize<<<(total + 127) / 128, 128, 0, s>>>(partials, nctas, nvals, out, batch);
+  note_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t power_finalize(const double* partials, int nctas, int nbins, double* out, int batch, cudaStream_t s) {
   const int nvals = 3 * nbins;
   const int total = nvals * batch;

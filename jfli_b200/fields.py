@@ -188,9 +188,8 @@ class DensityField(AbstractField):
         """P(k) of the mesh (reference fields/density.py:275-318)."""
         from .power import power as power_fn
 
-        if mesh2 is not None:
-            raise NotImplementedError("cross power spectra are not on the B200 path")
-        k, pk = power_fn(self.array, box_shape=self.box_size, kedges=kedges, multipoles=multipoles, los=los)
+        m2 = mesh2.array if isinstance(mesh2, AbstractField) else mesh2
+        k, pk = power_fn(self.array, m2, box_shape=self.box_size, kedges=kedges, multipoles=multipoles, los=los)
         return PowerSpectrum(wavenumber=k, array=pk, name="pk", scale_factors=self.scale_factors)
 
 

@@ -43,12 +43,43 @@ def finalize(sums: torch.Tensor, mesh_shape, box_shape):
     return kavg, pk
 
 
+def power_poles(mesh: torch.Tensor, mesh2, box_shape, kedges, poles, los):
+    """Cross spectra and/or multipoles (reference _src/power/_compute.py:68-119): for each
+    multipole the sum over the full grid of (2l + 1) L_l(mu) F1 conj(F2) per bin, its real
+    part for an auto spectrum and its modulus for a cross spectrum, over the mode count,
+    bins 0 and nedges dropped, times prod(L/N). -> (kavg, pk (npoles, nbins) or (nbins,))."""
+    mesh_shape = tuple(int(v) for v in mesh.shape[-3:])
+    lead = tuple(mesh.shape[:-3])
+    batch = int(np.prod(lead)) if lead else 1
+    edges = torch.as_tensor(np.asarray(kedges, np.float32), device=mesh.device)
+    ells = np.ascontiguousarray(np.asarray(poles, dtype=np.int32))
+    nell, nedges = int(ells.size), int(edges.numel())
+    nb = ops.query("jfli_power_poles_workspace_bytes", *mesh_shape, batch, nedges, nell, int(mesh2 is not None))
+    ws = ops.workspace(nb, "poles", mesh.device)
+    out = torch.empty(batch, 2 * nell + 2, nedges + 1, dtype=torch.float64, device=mesh.device)
+    lv = np.asarray(los, np.float64)
+    lv = lv / np.linalg.norm(lv)
+    import ctypes
+
+    ops.call("jfli_power_poles", ops.stream_ptr(), ops.ptr(mesh), ops.ptr(mesh2), ops.ptr(edges), nedges,
+             *(float(v) for v in box_shape), *(float(v) for v in lv), ells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+             nell, ops.ptr(out), ops.ptr(ws), ws.numel(), *mesh_shape, batch)
+    cnt = out[:, 2 * nell]
+    norm = torch.where(cnt > 0, cnt, torch.ones_like(cnt))
+    re, im = out[:, 0:2 * nell:2], out[:, 1:2 * nell:2]
+    psum = torch.sqrt(re**2 + im**2) if mesh2 is not None else re
+    vol = float(np.prod(np.asarray(box_shape, np.float64) / np.asarray(mesh_shape, np.float64)))
+    pk = (psum / norm[:, None, :])[..., 1:-1] * vol
+    kavg = (out[0, 2 * nell + 1] / norm[0])[1:-1]
+    pk = pk.reshape(*lead, nell, -1) if lead else pk[0]
+    if nell == 1:
+        pk = pk[..., 0, :]
+    return kavg, pk
+
+
 def power(mesh, mesh2=None, *, box_shape, kedges=None, multipoles=0, los=(0.0, 0.0, 1.0)):
-    """Array-level 3D auto power spectrum -> (wavenumber, spectra)."""
-    if mesh2 is not None:
-        raise NotImplementedError("cross spectra are not on the B200 path")
-    if multipoles not in (0, (0,), [0]):
-        raise NotImplementedError("only the monopole is on the B200 path")
+    """Array-level 3D power spectrum -> (wavenumber, spectra): auto or cross (mesh2), the
+    monopole or Legendre multipoles along `los` (reference power/compute.py:13-33)."""
     if not isinstance(mesh, torch.Tensor):
         mesh = torch.as_tensor(np.asarray(mesh, dtype=np.float32), device="cuda")
     mesh = mesh.to(torch.float32)
@@ -56,6 +87,19 @@ def power(mesh, mesh2=None, *, box_shape, kedges=None, multipoles=0, los=(0.0, 0
     box_shape = tuple(float(v) for v in box_shape)
     if kedges is None:
         kedges = default_kedges(mesh_shape, box_shape)
+    poles = tuple(multipoles) if isinstance(multipoles, (list, tuple)) else (multipoles,)
+    if mesh2 is not None or poles != (0,):
+        if torch.is_grad_enabled() and mesh.requires_grad:
+            raise NotImplementedError("gradients of cross spectra and multipoles are not on the B200 path")
+        m2 = None
+        if mesh2 is not None:
+            m2 = mesh2 if isinstance(mesh2, torch.Tensor) else torch.as_tensor(np.asarray(mesh2, np.float32),
+                                                                                device="cuda")
+            m2 = m2.to(torch.float32).contiguous()
+            if m2.shape != mesh.shape:
+                raise ValueError("mesh2 must have the shape of mesh")
+        # multipoles == 0 uses mu = 1 in the reference (no line of sight): L_0 = 1 either way
+        return power_poles(mesh.contiguous(), m2, box_shape, kedges, poles, los)
     if torch.is_grad_enabled() and mesh.requires_grad:
         # differentiable path: the adjoint kernel gives dL/dmesh (pm/adjoint.py)
         from .pm.adjoint import PowerSpectrum

@@ -312,3 +312,56 @@ def lightcone_drift(disp, vel, box, observer, t, a_of_chi, Gp, dGfa):
     at = a_of_chi(r)
     drift = (Gp(at) - Gp(t)) / dGfa(np.sqrt(t * at))
     return x + drift[..., None] * vel.astype(np.float64)
+
+
+def power_poles(mesh, mesh2, box, kedges, multipoles=0, los=(0.0, 0.0, 1.0)):
+    """Reference _power with cross spectra and multipoles (_src/power/_compute.py:5-119):
+    full complex fftn (ortho, FP64 here), k grid (2 pi m / L) fftfreq(m) in float32 as the
+    reference builds it, digitize, mu = (k . los) / |k| (0 at k = 0), weights
+    (2l + 1) L_l(mu) (the reference's recurrence), bincount of Re and Im; the modulus for a
+    cross spectrum, the real sum for an auto one; / counts, [1:-1], * prod(L/N)."""
+    shape = mesh.shape
+    box = np.asarray(box, np.float64)
+    poles = multipoles if isinstance(multipoles, (list, tuple)) else (multipoles,)
+    f1 = np.fft.fftn(mesh.astype(np.float64), norm="ortho")
+    mmk = (f1.real**2 + f1.imag**2) if mesh2 is None else f1 * np.conj(np.fft.fftn(mesh2.astype(np.float64),
+                                                                                     norm="ortho"))
+    kvec = []
+    for i, (m, b) in enumerate(zip(shape, box)):
+        fr = np.fft.fftfreq(m).astype(np.float32)
+        sh = [1] * 3
+        sh[i] = m
+        kvec.append((np.float32(2 * np.pi * m / b) * fr).reshape(sh).astype(np.float32))
+    kmesh = np.sqrt((kvec[0] ** 2 + kvec[1] ** 2 + kvec[2] ** 2).astype(np.float32)).astype(np.float32)
+    kmesh = np.broadcast_to(kmesh, shape)
+    edges = np.asarray(kedges, np.float32)
+    dig = np.digitize(kmesh.reshape(-1), edges)
+    nb = edges.size + 1
+    cnt = np.bincount(dig, minlength=nb).astype(np.float64)
+    kavg = (np.bincount(dig, weights=kmesh.reshape(-1).astype(np.float64), minlength=nb) / np.maximum(cnt, 1))[1:-1]
+    if poles == (0,):
+        mu = np.ones(shape)
+    else:
+        lv = np.asarray(los, np.float64) / np.linalg.norm(los)
+        dot = sum(np.broadcast_to(kvec[i].astype(np.float64), shape) * lv[i] for i in range(3))
+        mu = np.where(kmesh == 0, 0.0, dot / np.where(kmesh == 0, 1.0, kmesh))
+    out = []
+    for ell in poles:
+        p0, p1 = np.ones_like(mu), mu
+        if ell == 0:
+            L = p0
+        elif ell == 1:
+            L = p1
+        else:
+            for n in range(2, ell + 1):
+                p0, p1 = p1, ((2 * n - 1) * mu * p1 - (n - 1) * p0) / n
+            L = p1
+        w = (mmk * (2 * ell + 1) * L).reshape(-1)
+        if mesh2 is None:
+            ps = np.bincount(dig, weights=w.real, minlength=nb)
+        else:
+            ps = np.hypot(np.bincount(dig, weights=w.real, minlength=nb), np.bincount(dig, weights=w.imag,
+                                                                                       minlength=nb))
+        out.append((ps / np.maximum(cnt, 1))[1:-1] * np.prod(box / np.asarray(shape)))
+    pk = np.stack(out)
+    return kavg, (pk[0] if len(poles) == 1 else pk)
