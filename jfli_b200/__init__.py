@@ -41,7 +41,8 @@ from .pm import (
     lpt,
     nbody,
 )
-from .power import angular_cl_flat, power
+from .power import (angular_cl_flat, angular_cl_spherical, coherence, cross_angular_cl_spherical, power,
+                    transfer)
 from .utils import (
     centers,
     compute_box_size_from_redshift,

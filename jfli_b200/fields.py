@@ -210,15 +210,37 @@ class SphericalDensity(AbstractField):
         vol = 4.0 * np.pi / (12 * self.nside * self.nside) * ((c + w / 2) ** 3 - (c - w / 2) ** 3) / 3.0
         return _density_to(self, unit, vol, omega_m, h, mean_density)
 
-    def angular_cl(self, lmax: int | None = None):
-        """Angular power spectrum of each map (healpy's anafast algorithm on the GPU: ring
-        transforms and Legendre stages in FP64)."""
-        from .sht import anafast
+    def angular_cl(self, mesh2: "SphericalDensity | None" = None, *, lmax: int | None = None, method: str = "jax",
+                   batch_size=None) -> PowerSpectrum:
+        """C_ell of each map, auto or cross with mesh2 (reference fields/lightcone.py:632-674):
+        healpy's anafast algorithm in this library's GPU engine (ring transforms and
+        Legendre stages in FP64)."""
+        from .power import angular_cl_spherical
 
-        maps = self.array.detach().double().cpu().numpy()
-        if maps.ndim == 1:
-            return anafast(maps, lmax=lmax)
-        return np.stack([anafast(m, lmax=lmax) for m in maps])
+        d1 = self.array
+        d2 = mesh2.array if mesh2 is not None else None
+        if d1.ndim not in (1, 2):
+            raise ValueError("SphericalDensity.angular_cl expects array shape (npix) or (B,npix)")
+        if d2 is not None and d2.shape != d1.shape:
+            raise ValueError("mesh2 must match shape for cross Cl")
+        rows1 = [d1] if d1.ndim == 1 else list(d1)
+        rows2 = [None] * len(rows1) if d2 is None else ([d2] if d2.ndim == 1 else list(d2))
+        ell, spectra = None, []
+        for a, b in zip(rows1, rows2):
+            ell, cl = angular_cl_spherical(a, b, lmax=lmax, method=method)
+            spectra.append(cl)
+        arr = np.stack(spectra) if d1.ndim == 2 else spectra[0]
+        return PowerSpectrum(wavenumber=ell, array=arr, name="cl", scale_factors=self.scale_factors)
+
+    def cross_angular_cl(self, *, lmax: int | None = None, method: str = "healpy", batch_size=None) -> PowerSpectrum:
+        """All auto and cross C_ell of the batched maps, healpy's alm2cl order (reference
+        fields/lightcone.py:676-720)."""
+        from .power import cross_angular_cl_spherical
+
+        if self.array.ndim != 2:
+            raise ValueError("cross_angular_cl needs batched maps (B, npix)")
+        ell, cls = cross_angular_cl_spherical(self.array, lmax=lmax, method=method)
+        return PowerSpectrum(wavenumber=ell, array=cls, name="cl", scale_factors=self.scale_factors)
 
 
 @dataclasses.dataclass(frozen=True, eq=False)

@@ -8,6 +8,8 @@ the sums are FP64 and reduced in a fixed order.
 
 from __future__ import annotations
 
+import math
+
 import numpy as np
 import torch
 
@@ -158,3 +160,50 @@ def angular_cl_flat(map1, map2=None, *, pixel_size=None, field_size=None, ell_ed
     if m1.ndim == 2:
         cl = cl[0]
     return ell, cl
+
+
+def transfer(mesh0, mesh1, *, box_shape, kedges=None):
+    """Monopole transfer function sqrt(P1 / P0) (reference _src/power/_compute.py:239-243)."""
+    k, pk0 = power(mesh0, box_shape=box_shape, kedges=kedges)
+    _, pk1 = power(mesh1, box_shape=box_shape, kedges=kedges)
+    return k, (pk1 / pk0) ** 0.5
+
+
+def coherence(mesh0, mesh1, *, box_shape, kedges=None):
+    """Monopole coherence P01 / sqrt(P0 P1) (reference _src/power/_compute.py:246-251)."""
+    k, pk01 = power(mesh0, mesh1, box_shape=box_shape, kedges=kedges)
+    _, pk0 = power(mesh0, box_shape=box_shape, kedges=kedges)
+    _, pk1 = power(mesh1, box_shape=box_shape, kedges=kedges)
+    return k, pk01 / (pk0 * pk1) ** 0.5
+
+
+def _host_map(m):
+    return (m.detach().double().cpu().numpy() if isinstance(m, torch.Tensor)
+            else np.asarray(m, dtype=np.float64))
+
+
+def angular_cl_spherical(map_sphere, map_sphere2=None, *, lmax: int | None = None, method: str = "jax"):
+    """Spherical C_l, auto or cross (reference power/compute.py:89-98 -> healpy anafast):
+    (ell, cl). Both method values run healpy's algorithm in this library's GPU engine."""
+    from . import sht
+
+    if method not in ("jax", "healpy"):
+        raise ValueError(f"unknown method {method!r}")
+    m1 = _host_map(map_sphere)
+    nside = int(round(math.sqrt(m1.size / 12)))
+    lmax = 3 * nside - 1 if lmax is None else int(lmax)
+    if map_sphere2 is None:
+        cl = sht.anafast(m1, lmax)
+    else:
+        cl = sht.alm2cl_cross_packed(sht.map2alm_gpu(m1, lmax), sht.map2alm_gpu(_host_map(map_sphere2), lmax), lmax)
+    return np.arange(cl.shape[-1]) * 1.0, cl
+
+
+def cross_angular_cl_spherical(maps, *, lmax: int | None = None, method: str = "healpy"):
+    """All cross C_l of B maps in healpy's order (reference power/compute.py:101-109)."""
+    from . import sht
+
+    if method != "healpy":
+        raise ValueError(f"cross_angular_cl_spherical only supports method='healpy', got method='{method}'.")
+    cls = sht.cross_cls(_host_map(maps), lmax)
+    return np.arange(cls.shape[-1]) * 1.0, cls

@@ -277,3 +277,25 @@ def anafast(m: np.ndarray, lmax: int | None = None, iter: int = 3, engine: str =
     if engine != "host":
         raise ValueError(f"unknown engine {engine!r} (gpu, host)")
     return alm2cl(map2alm(m, lmax, iter), lmax)
+
+
+def alm2cl_cross_packed(a1: np.ndarray, a2: np.ndarray, lmax: int) -> np.ndarray:
+    """Cross C_l of two packed a_lm sets: (Re a1_l0 a2_l0* + 2 sum_{m>0} Re a1_lm a2_lm*) / (2l + 1)."""
+    off = packed_offsets(lmax)
+    p = (a1 * np.conj(a2)).real
+    cl = p[off[0]:off[1]].copy()
+    for mm in range(1, lmax + 1):
+        cl[mm:] += 2.0 * p[off[mm]:off[mm + 1]]
+    return cl / (2.0 * np.arange(lmax + 1) + 1.0)
+
+
+def cross_cls(maps, lmax: int | None = None, iter: int = 3) -> np.ndarray:
+    """All auto and cross C_l of B maps (B, npix), each map analysed once (GPU engine), in
+    healpy's alm2cl order: the diagonal first (11, 22, ...), then the first off-diagonal
+    (12, 23, ...), and so on. -> (B (B + 1) / 2, lmax + 1)."""
+    maps = np.atleast_2d(np.asarray(maps, dtype=np.float64))
+    nside = int(round(math.sqrt(maps.shape[1] / 12)))
+    lmax = 3 * nside - 1 if lmax is None else int(lmax)
+    alms = [map2alm_gpu(m, lmax, iter) for m in maps]
+    b = len(alms)
+    return np.stack([alm2cl_cross_packed(alms[i], alms[i + d], lmax) for d in range(b) for i in range(b - d)])

@@ -461,3 +461,16 @@ def test_power_cross_and_multipoles_match_oracle(cross, poles, los):
     print(f"cross {cross} poles {poles} los {los}: max |GPU - oracle| / scale {err:.2e}")
     np.testing.assert_allclose(k.cpu().numpy(), kr, rtol=1e-6)
     assert err < 1e-4
+
+
+def test_transfer_and_coherence():
+    rng = np.random.default_rng(12)
+    a = torch.as_tensor(rng.standard_normal((32, 32, 32)).astype(np.float32), device="cuda")
+    edges = np.geomspace(0.05, 0.45, 8)
+    _, t = jf.transfer(a, 2.0 * a, box_shape=(200.0,) * 3, kedges=edges)
+    _, c = jf.coherence(a, 2.0 * a, box_shape=(200.0,) * 3, kedges=edges)
+    np.testing.assert_allclose(t.cpu().numpy(), 2.0, rtol=1e-5)
+    np.testing.assert_allclose(c.cpu().numpy(), 1.0, rtol=1e-5)
+    b = torch.as_tensor(rng.standard_normal((32, 32, 32)).astype(np.float32), device="cuda")
+    _, c2 = jf.coherence(a, b, box_shape=(200.0,) * 3, kedges=edges)
+    assert np.all(np.abs(c2.cpu().numpy()) < 0.5)  # independent fields: weakly coherent

@@ -108,7 +108,9 @@ def test_angular_cl_of_gpu_shell_matches_oracle_shell(cosmo):
     assert rel < 1e-4
     dens = jf.SphericalDensity(array=torch.as_tensor(gpu, device="cuda"), mesh_size=(n,) * 3, box_size=(L,) * 3,
                                nside=nside)
-    np.testing.assert_allclose(dens.angular_cl(lmax=lmax), sht.anafast(gpu, lmax, engine="host"), rtol=1e-9)
+    ps = dens.angular_cl(lmax=lmax)
+    np.testing.assert_allclose(ps.array, sht.anafast(gpu, lmax, engine="host"), rtol=1e-9)
+    assert ps.name == "cl" and ps.wavenumber[-1] == lmax
 
 
 # ------------------------------------------------------------------ tiled light cones
