@@ -6,6 +6,8 @@ every operation on them runs in libjfli_b200's sm_100a kernels.
 """
 
 from . import cosmology, ops, utils
+from . import catalog as io
+from . import fields as units
 from .catalog import CATALOG_VERSION, Catalog
 from .cosmology import Cosmology, Planck18
 from .fields import (
@@ -17,9 +19,15 @@ from .fields import (
     ParticleField,
     PhysicalUnit,
     PositionUnit,
+    ConvergenceUnit,
+    FieldMetadata,
     FlatDensity,
+    FlatKappaField,
+    FlatShearField,
     PowerSpectrum,
     SphericalDensity,
+    SphericalKappaField,
+    SphericalShearField,
     convert_units,
     uniform_particles,
 )

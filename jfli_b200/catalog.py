@@ -3,9 +3,9 @@
 One row per (field, cosmology) entry, written through HuggingFace `datasets` with the
 reference's Features schema, so files written here load in jax-fli's `Catalog.from_parquet`
 and the reverse:
-- "array": the batched array (B, ...) as Array2D (SphericalDensity, (B, npix)),
-  Array3D (FlatDensity, (B, npx, npy)), Array4D (DensityField) or Array5D (ParticleField),
-  first dimension variable;
+- "array": the batched array (B, ...) as Array2D (SphericalDensity, SphericalKappaField:
+  (B, npix)), Array3D (FlatDensity, FlatKappaField: (B, npx, npy)), Array4D (DensityField)
+  or Array5D (ParticleField), first dimension variable;
 - dynamic metadata "z_sources", "scale_factors", "comoving_centers", "density_width":
   float64 sequences of length B;
 - static metadata "mesh_size", "box_size", "observer_position", "halo_size", enum names
@@ -22,16 +22,18 @@ import numpy as np
 import torch
 
 from .cosmology import Cosmology
-from .fields import (AbstractField, DensityField, DensityUnit, FieldStatus, FlatDensity, ParticleField,
-                     PositionUnit, SphericalDensity)
+from .fields import (AbstractField, ConvergenceUnit, DensityField, DensityUnit, FieldStatus, FlatDensity,
+                     FlatKappaField, ParticleField, PositionUnit, SphericalDensity, SphericalKappaField)
 
 CATALOG_VERSION = 2
 
 __all__ = ["Catalog", "CATALOG_VERSION"]
 
-_FIELD_CLASSES = {"SphericalDensity": SphericalDensity, "FlatDensity": FlatDensity, "DensityField": DensityField,
+_FIELD_CLASSES = {"SphericalDensity": SphericalDensity, "SphericalKappaField": SphericalKappaField,
+                  "FlatDensity": FlatDensity, "FlatKappaField": FlatKappaField, "DensityField": DensityField,
                   "ParticleField": ParticleField}
-_CORE_NDIM = {"SphericalDensity": 1, "FlatDensity": 2, "DensityField": 3, "ParticleField": 4}
+_CORE_NDIM = {"SphericalDensity": 1, "SphericalKappaField": 1, "FlatDensity": 2, "FlatKappaField": 2,
+              "DensityField": 3, "ParticleField": 4}
 
 
 def _batched(array: np.ndarray, field_type: str) -> np.ndarray:
@@ -70,8 +72,8 @@ def _features(field_type: str, element_shape, dtype: str, field: AbstractField):
     """The reference's Features schema (io/catalog.py:113-177)."""
     from datasets import Array2D, Array3D, Array4D, Array5D, Features, Sequence, Value
 
-    array_cls = {"SphericalDensity": Array2D, "FlatDensity": Array3D, "DensityField": Array4D,
-                 "ParticleField": Array5D}[field_type]
+    array_cls = {"SphericalDensity": Array2D, "SphericalKappaField": Array2D, "FlatDensity": Array3D,
+                 "FlatKappaField": Array3D, "DensityField": Array4D, "ParticleField": Array5D}[field_type]
     feats = {
         "array": array_cls(shape=(None, *element_shape), dtype=dtype),
         "z_sources": Sequence(Value("float64")),
@@ -144,6 +146,8 @@ def _field_from_row(item: dict, device) -> tuple[AbstractField, Cosmology, int]:
     cls = _FIELD_CLASSES[field_type]
     if cls is ParticleField:
         unit = PositionUnit[item["unit"]]
+    elif cls in (SphericalKappaField, FlatKappaField):
+        unit = ConvergenceUnit[item["unit"]]
     elif item["unit"] in DensityUnit.__members__:
         unit = DensityUnit[item["unit"]]
     else:

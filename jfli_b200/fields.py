@@ -50,6 +50,11 @@ class DensityUnit(str, Enum):
     MSUN_H_PER_MPC3 = auto()
 
 
+class ConvergenceUnit(str, Enum):
+    DIMENSIONLESS = auto()
+    EFFECTIVE_DENSITY = auto()
+
+
 @dataclasses.dataclass(frozen=True)
 class PaintingOptions:
     """Painting configuration (reference fields/painting.py:15-96)."""
@@ -442,6 +447,8 @@ def convert_units(array, origin, destination, mesh_size, box_size, h=None, omega
         return f.to(destination).array
     if isinstance(origin, DensityUnit):
         return _convert_density(array, origin, destination, volume_element, omega_m, h, mean_density)
+    if isinstance(origin, ConvergenceUnit):  # both are kappa = Sigma / Sigma_crit
+        return array
     raise NotImplementedError(f"Conversion not implemented for {type(origin).__name__}")
 
 
@@ -494,3 +501,66 @@ def _density_to(field, unit, volume_element, omega_m, h, mean_density):
     arr = convert_units(field.array, field.unit, unit, field.mesh_size, field.box_size, h=h, omega_m=omega_m,
                         mean_density=mean_density, volume_element=volume_element)
     return field.replace(array=arr, unit=unit)
+
+
+# ----------------------------------------------------------------------- lensing maps
+# Convergence and shear maps (reference fields/lensing_maps.py): the density containers
+# with convergence units. The reference does not implement the kappa <-> shear conversions
+# either; they raise the same NotImplementedError.
+def _convergence_to(field, unit):
+    if field.unit == unit:
+        return field
+    if not isinstance(unit, ConvergenceUnit):
+        raise TypeError(f"{type(field).__name__}.to() expected a ConvergenceUnit, got {unit!r}")
+    return field.replace(unit=unit)
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class SphericalKappaField(SphericalDensity):
+    """HEALPix convergence maps (npix,) or (n_sources, npix)."""
+
+    def to(self, unit, **_):
+        return _convergence_to(self, unit)
+
+    def get_shear(self, cosmo=None):
+        raise NotImplementedError("Shear computation from kappa (spherical) not implemented yet.")
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class FlatKappaField(FlatDensity):
+    """Flat-sky convergence maps."""
+
+    def to(self, unit, **_):
+        return _convergence_to(self, unit)
+
+    def get_shear(self, cosmo=None):
+        raise NotImplementedError("Shear computation from kappa (flat-sky) not implemented yet.")
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class SphericalShearField(SphericalDensity):
+    def to(self, unit, **_):
+        return _convergence_to(self, unit)
+
+    def get_convergence(self, cosmo=None):
+        raise NotImplementedError("Convergence from shear (spherical) not implemented yet.")
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class FlatShearField(FlatDensity):
+    def to(self, unit, **_):
+        return _convergence_to(self, unit)
+
+    def get_convergence(self, cosmo=None):
+        raise NotImplementedError("Convergence from shear (flat-sky) not implemented yet.")
+
+
+@dataclasses.dataclass(frozen=True, eq=False)
+class FieldMetadata(AbstractField):
+    """Metadata-only field (array None), as the reference's to_metadata() produces."""
+
+    def is_batched(self) -> bool:
+        return False
+
+    def is_multi_batched(self) -> bool:
+        return False

@@ -125,8 +125,9 @@ def born_maps(maps: torch.Tensor, weights: np.ndarray) -> torch.Tensor:
     return out
 
 
-def born(cosmo, lightcone: SphericalDensity, nz_shear, min_z=0.01, max_z=1.5, n_integrate=32) -> SphericalDensity:
-    """Born convergence maps (K, npix) of a spherical light cone (status LIGHTCONE)."""
+def born(cosmo, lightcone: SphericalDensity, nz_shear, min_z=0.01, max_z=1.5, n_integrate=32):
+    """Born convergence maps (K, npix) of a spherical light cone (status LIGHTCONE), as a
+    SphericalKappaField (unit DIMENSIONLESS) like the reference's."""
     if nz_shear is None:
         raise ValueError("nz_shear must be provided for lensing")
     if lightcone.status != FieldStatus.LIGHTCONE:
@@ -139,6 +140,9 @@ def born(cosmo, lightcone: SphericalDensity, nz_shear, min_z=0.01, max_z=1.5, n_
                             n_integrate)
     kappa = born_maps(lightcone.array, W)
     a_src = 1.0 / (1.0 + z_eff)
-    return lightcone.replace(array=kappa, status=FieldStatus.KAPPA, z_sources=z_eff, scale_factors=a_src,
-                             comoving_centers=cj.radial_comoving_distance(cosmo, a_src),
-                             density_width=np.zeros_like(z_eff))
+    from .fields import ConvergenceUnit, SphericalKappaField
+
+    return SphericalKappaField.FromDensityMetadata(
+        array=kappa, field=lightcone, status=FieldStatus.KAPPA, unit=ConvergenceUnit.DIMENSIONLESS, z_sources=z_eff,
+        scale_factors=a_src, comoving_centers=cj.radial_comoving_distance(cosmo, a_src),
+        density_width=np.zeros_like(z_eff))

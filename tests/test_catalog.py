@@ -81,3 +81,22 @@ def test_catalog_rejects_mismatched_lengths():
     f = _fields()[2]
     with pytest.raises(ValueError):
         jf.Catalog([f, f], [jf.Planck18()])
+
+
+def test_catalog_kappa_field(tmp_path):
+    """Convergence maps (born's SphericalKappaField) keep their class and unit."""
+    sph = _fields()[0]
+    kap = jf.SphericalKappaField.FromDensityMetadata(array=sph.array[:2], field=sph, status=jf.FieldStatus.KAPPA,
+                                                     unit=jf.ConvergenceUnit.DIMENSIONLESS,
+                                                     z_sources=np.array([0.5, 1.0]),
+                                                     scale_factors=np.array([0.67, 0.5]),
+                                                     comoving_centers=np.array([0.0, 0.0]),
+                                                     density_width=np.array([0.0, 0.0]))
+    path = str(tmp_path / "kappa.parquet")
+    jf.Catalog(kap, jf.Planck18()).to_parquet(path)
+    back = jf.Catalog.from_parquet(path, device="cpu").field[0]
+    assert type(back) is jf.SphericalKappaField and back.unit == jf.ConvergenceUnit.DIMENSIONLESS
+    assert torch.equal(back.array, kap.array)
+    assert kap.to(jf.ConvergenceUnit.EFFECTIVE_DENSITY).unit == jf.ConvergenceUnit.EFFECTIVE_DENSITY
+    with pytest.raises(NotImplementedError):
+        kap.get_shear()
