@@ -43,6 +43,7 @@
  *                             TelephotoInterp._paint_telephoto (pm/interp.py:643-699): the
  *                             rotated, shifted (and drifted) replicas painted in one pass
  *   jfli_born              <- _src/lensing/_born.py:29-130 (_born_core_impl, _born_spherical)
+ *   jfli_born_flat         <- _src/lensing/_born.py:29-97 and 133-186 (_born_flat)
  *   jfli_sht_map2alm / jfli_sht_alm2map <- the Legendre stages of healpy.anafast behind
  *                             SphericalDensity.angular_cl (_src/power/_compute.py:175-191)
  *   jfli_sht_ring_analysis / jfli_sht_ring_synthesis <- the ring FFTs along phi of the same
@@ -258,6 +259,14 @@ int jfli_lightcone_drift(void* stream, const float* disp, const float* vel, floa
 size_t jfli_born_workspace_bytes(int nplanes, long long npix);
 int jfli_born(void* stream, const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
               float* out, void* workspace, size_t workspace_bytes, char* err, size_t errlen);
+
+/* Born convergence of nplanes flat-sky planes [nplanes][n0][n1]: out[k][i0][i1] =
+ * sum_p weights[k][p] (v_p / mean_p - 1), v_p the periodic bilinear sample of plane p at
+ * axis-0 coordinate i1 s0[p] - 0.5 and axis-1 coordinate i0 s1[p] - 0.5 (s0, s1 device
+ * arrays: pixel angle x chi_p / pixel size). Workspace: jfli_born_workspace_bytes. */
+int jfli_born_flat(void* stream, const float* maps, int nplanes, int n0, int n1, const float* weights, int nsrc,
+                   const float* s0, const float* s1, float* out, void* workspace, size_t workspace_bytes, char* err,
+                   size_t errlen);
 
 /* Legendre stages of the spherical harmonic transform of a HEALPix RING map (FP64).
  * F and G are [nrings][lmax + 1] complex (interleaved doubles): per ring r the Fourier

@@ -129,6 +129,11 @@ _SIGNATURES = {
     "jfli_sht_ring_synthesis": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
     "jfli_sht_alm2map": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
     "jfli_born_workspace_bytes": (c_size_t, [c_int, c_longlong]),
+    "jfli_born_flat": (
+        c_int,
+        [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t,
+         *_ERR],
+    ),
     "jfli_born": (c_int, [c_void_p, c_void_p, c_int, c_longlong, c_void_p, c_int, c_void_p, c_void_p, c_size_t, *_ERR]),
     "jfli_adjoint_partials_count": (c_size_t, _DIMS),
     "jfli_kkd_workspace_bytes": (c_size_t, _DIMS),

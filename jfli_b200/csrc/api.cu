@@ -700,6 +700,29 @@ int jfli_born(void* stream, const float* maps, int nplanes, long long npix, cons
       errlen, "jfli_born");
 }
 
+int jfli_born_flat(void* stream, const float* maps, int nplanes, int n0, int n1, const float* weights, int nsrc,
+                   const float* s0, const float* s1, float* out, void* workspace, size_t workspace_bytes, char* err,
+                   size_t errlen) {
+  CHECK_PTR(maps);
+  CHECK_PTR(weights);
+  CHECK_PTR(s0);
+  CHECK_PTR(s1);
+  CHECK_PTR(out);
+  CHECK_PTR(workspace);
+  if (nplanes < 1 || nplanes > 256) return fail(err, errlen, JFLI_EINVAL, "nplanes %d outside [1, 256]", nplanes);
+  if (nsrc < 1 || nsrc > 32) return fail(err, errlen, JFLI_EINVAL, "nsrc %d outside [1, 32]", nsrc);
+  if (n0 < 1 || n1 < 1) return fail(err, errlen, JFLI_EINVAL, "plane shape must be positive");
+  const long long npix = (long long)n0 * n1;
+  const size_t need = jfli_born_workspace_bytes(nplanes, npix);
+  if (workspace_bytes < need)
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  double* partials = (double*)workspace;
+  float* mean = (float*)((char*)workspace + align256(sizeof(double) * (size_t)nplanes * jfli::born_ctas(npix)));
+  return cuda_status(jfli::born_flat(maps, nplanes, n0, n1, weights, nsrc, s0, s1, out, partials, mean,
+                                     (cudaStream_t)stream),
+                     err, errlen, "jfli_born_flat");
+}
+
 int jfli_sht_map2alm(void* stream, const double* F, const double* z, int nrings, int lmax, double weight,
                      double* alm, char* err, size_t errlen) {
   CHECK_PTR(F);

@@ -69,6 +69,55 @@ __global__ void k_born_combine(const float* __restrict__ maps, int nplanes, long
   }
 }
 
+// Flat-sky planes (reference _src/lensing/_born.py:29-97 with coords, and _born_flat,
+// 133-186): each output pixel (i0, i1) samples plane p by periodic bilinear interpolation
+// (jax map_coordinates, order 1, mode "wrap") at axis-0 coordinate i1 s0_p - 0.5 and axis-1
+// coordinate i0 s1_p - 0.5, where s0_p, s1_p (host) are the pixel angle times chi_p over the
+// plane's pixel size, in the reference's pairing of grid axes; then delta = v / mean_p - 1
+// and kappa_k = sum_p W[k][p] delta.
+__global__ void k_born_flat(const float* __restrict__ maps, int nplanes, int n0, int n1,
+                            const float* __restrict__ mean, const float* __restrict__ w, int nsrc,
+                            const float* __restrict__ s0, const float* __restrict__ s1, float* __restrict__ out) {
+  extern __shared__ float sm[];  // mean[nplanes], s0[nplanes], s1[nplanes], w[nsrc][nplanes]
+  for (int i = threadIdx.x; i < nplanes; i += blockDim.x) {
+    sm[i] = mean[i];
+    sm[nplanes + i] = s0[i];
+    sm[2 * nplanes + i] = s1[i];
+  }
+  for (int i = threadIdx.x; i < nsrc * nplanes; i += blockDim.x) sm[3 * nplanes + i] = w[i];
+  __syncthreads();
+  const long long npix = (long long)n0 * n1;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < npix; q += (long long)gridDim.x * blockDim.x) {
+    const int i0 = (int)(q / n1), i1 = (int)(q - (long long)i0 * n1);
+    float acc[8];
+    for (int k0 = 0; k0 < nsrc; k0 += 8) {
+      const int kn = (nsrc - k0) < 8 ? (nsrc - k0) : 8;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[k] = 0.f;
+      for (int p = 0; p < nplanes; ++p) {
+        const float u = (float)i1 * sm[nplanes + p] - 0.5f;  // along axis 0 of the plane
+        const float v = (float)i0 * sm[2 * nplanes + p] - 0.5f;  // along axis 1
+        const float fu = floorf(u), fv = floorf(v);
+        const float wu = u - fu, wv = v - fv;
+        int a0 = (int)fu % n0, b0 = (int)fv % n1;
+        if (a0 < 0) a0 += n0;
+        if (b0 < 0) b0 += n1;
+        const int a1 = a0 + 1 == n0 ? 0 : a0 + 1, b1 = b0 + 1 == n1 ? 0 : b0 + 1;
+        const float* m = maps + (long long)p * npix;
+        const float val = (1.f - wu) * ((1.f - wv) * m[(long long)a0 * n1 + b0] + wv * m[(long long)a0 * n1 + b1]) +
+                          wu * ((1.f - wv) * m[(long long)a1 * n1 + b0] + wv * m[(long long)a1 * n1 + b1]);
+        const float d = val / sm[p] - 1.0f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (k < kn) acc[k] += sm[3 * nplanes + (k0 + k) * nplanes + p] * d;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (k < kn) out[(long long)(k0 + k) * npix + q] = acc[k];
+    }
+  }
+}
+
 int born_ctas(long long npix) {
   long long b = (npix + kBornThreads - 1) / kBornThreads;
   const long long cap = (long long)sm_count() * 4;
@@ -88,6 +137,24 @@ cudaError_t born_convergence(const float* maps, int nplanes, long long npix, con
   if (e != cudaSuccess) return e;
   const size_t smem = sizeof(float) * (size_t)nplanes * (1 + nsrc);
   k_born_combine<<<born_ctas(npix), kBornThreads, smem, s>>>(maps, nplanes, npix, mean, weights, nsrc, out);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t born_flat(const float* maps, int nplanes, int n0, int n1, const float* weights, int nsrc, const float* s0,
+                      const float* s1, float* out, double* partials, float* mean, cudaStream_t s) {
+  const long long npix = (long long)n0 * n1;
+  const int nctas = born_ctas(npix);
+  k_plane_partials<<<dim3(nctas, nplanes), kBornThreads, 0, s>>>(maps, npix, partials);
+  note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_plane_means<<<(nplanes + 127) / 128, 128, 0, s>>>(partials, nctas, nplanes, npix, mean);
+  note_launch();
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t smem = sizeof(float) * (size_t)nplanes * (3 + nsrc);
+  k_born_flat<<<born_ctas(npix), kBornThreads, smem, s>>>(maps, nplanes, n0, n1, mean, weights, nsrc, s0, s1, out);
   note_launch();
   return cudaGetLastError();
 }

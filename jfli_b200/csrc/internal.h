@@ -91,6 +91,8 @@ cudaError_t lightcone_drift(const float* disp, const float* vel, float* out, con
 int born_ctas(long long npix);
 cudaError_t born_convergence(const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
                              float* out, double* partials, float* mean, cudaStream_t s);
+cudaError_t born_flat(const float* maps, int nplanes, int n0, int n1, const float* weights, int nsrc, const float* s0,
+                      const float* s1, float* out, double* partials, float* mean, cudaStream_t s);
 
 // ---- sht.cu ----
 cudaError_t sht_analysis(const double* F, const double* z, int nrings, int lmax, double weight, double* alm,

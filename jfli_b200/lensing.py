@@ -13,6 +13,8 @@ from __future__ import annotations
 
 import dataclasses
 
+import math
+
 import numpy as np
 import torch
 
@@ -125,6 +127,43 @@ def born_maps(maps: torch.Tensor, weights: np.ndarray) -> torch.Tensor:
     return out
 
 
+def born_flat_maps(planes: torch.Tensor, weights: np.ndarray, s0: np.ndarray, s1: np.ndarray) -> torch.Tensor:
+    """kappa (K, n0, n1) of flat planes (P, n0, n1): W @ (bilinear samples / mean - 1) on the GPU."""
+    if planes.dtype != torch.float32 or not planes.is_cuda:
+        raise TypeError("planes must be a float32 CUDA tensor")
+    planes = planes.contiguous()
+    if planes.ndim == 2:
+        planes = planes[None]
+    nplanes, n0, n1 = (int(v) for v in planes.shape)
+    dev = planes.device
+    w = torch.as_tensor(np.ascontiguousarray(weights, dtype=np.float32), device=dev)
+    if tuple(w.shape) != (w.shape[0], nplanes):
+        raise ValueError("weights must be (sources, planes)")
+    t0 = torch.as_tensor(np.asarray(s0, np.float32), device=dev)
+    t1 = torch.as_tensor(np.asarray(s1, np.float32), device=dev)
+    out = torch.empty(w.shape[0], n0, n1, dtype=torch.float32, device=dev)
+    nb = int(query("jfli_born_workspace_bytes", nplanes, n0 * n1))
+    from .ops import workspace
+
+    ws = workspace(nb, "born", dev)
+    call("jfli_born_flat", stream_ptr(), ptr(planes), nplanes, n0, n1, ptr(w), int(w.shape[0]), ptr(t0), ptr(t1),
+         ptr(out), ptr(ws), ws.numel())
+    return out
+
+
+def flat_sample_scales(field_size, flatsky_npix, box_size, chi):
+    """Per-plane sample steps of flat Born (reference _src/lensing/_born.py:52-64, 155-160): the
+    grid axis-1 angle (linspace(0, f_x, n_1) in degrees) times chi over the pixel size
+    box_y / n_0 drives the plane's axis 0, and the axis-0 angle times chi over box_x / n_1
+    its axis 1, as the reference pairs coords with pixel_size."""
+    fx, fy = (field_size, field_size) if np.ndim(field_size) == 0 else field_size
+    n0, n1 = flatsky_npix  # the reference names them (ny, nx)
+    ps0, ps1 = box_size[1] / n0, box_size[0] / n1
+    deg = math.pi / 180.0
+    chi = np.asarray(chi, np.float64)
+    return (fx / n1) * deg * chi / ps0, (fy / n0) * deg * chi / ps1
+
+
 def born(cosmo, lightcone: SphericalDensity, nz_shear, min_z=0.01, max_z=1.5, n_integrate=32):
     """Born convergence maps (K, npix) of a spherical light cone (status LIGHTCONE), as a
     SphericalKappaField (unit DIMENSIONLESS) like the reference's."""
@@ -132,15 +171,32 @@ def born(cosmo, lightcone: SphericalDensity, nz_shear, min_z=0.01, max_z=1.5, n_
         raise ValueError("nz_shear must be provided for lensing")
     if lightcone.status != FieldStatus.LIGHTCONE:
         raise ValueError(f"Expected lightcone with status=LIGHTCONE, got {lightcone.status}")
+    from .fields import ConvergenceUnit, FlatDensity, FlatKappaField
+
+    if isinstance(lightcone, FlatDensity):
+        if lightcone.field_size is None:
+            raise ValueError("field_size is required on lightcone for flat-sky convergence")
+        if lightcone.array.ndim != 3:
+            raise ValueError(f"Lightcone array must be 3D (flat), got {lightcone.array.ndim}D")
+        a = np.atleast_1d(np.asarray(lightcone.scale_factors, np.float64))
+        W, z_eff = born_weights(cosmo, a, lightcone.max_comoving_radius, nz_shear, min_z, max_z, n_integrate)
+        s0, s1 = flat_sample_scales(lightcone.field_size, lightcone.flatsky_npix, lightcone.box_size,
+                                    cj.radial_comoving_distance(cosmo, a))
+        kappa = born_flat_maps(lightcone.array, W, s0, s1)
+        a_src = 1.0 / (1.0 + z_eff)
+        return FlatKappaField.FromDensityMetadata(
+            array=kappa, field=lightcone, status=FieldStatus.KAPPA, unit=ConvergenceUnit.DIMENSIONLESS,
+            z_sources=z_eff, scale_factors=a_src, comoving_centers=cj.radial_comoving_distance(cosmo, a_src),
+            density_width=np.zeros_like(z_eff))
     if not isinstance(lightcone, SphericalDensity):
-        raise NotImplementedError("flat-sky Born is not on the B200 path")
+        raise TypeError(f"born needs a SphericalDensity or FlatDensity light cone, got {type(lightcone).__name__}")
     if lightcone.array.ndim != 2:
         raise ValueError(f"Lightcone array must be 2D (spherical), got {lightcone.array.ndim}D")
     W, z_eff = born_weights(cosmo, lightcone.scale_factors, lightcone.max_comoving_radius, nz_shear, min_z, max_z,
                             n_integrate)
     kappa = born_maps(lightcone.array, W)
     a_src = 1.0 / (1.0 + z_eff)
-    from .fields import ConvergenceUnit, SphericalKappaField
+    from .fields import SphericalKappaField
 
     return SphericalKappaField.FromDensityMetadata(
         array=kappa, field=lightcone, status=FieldStatus.KAPPA, unit=ConvergenceUnit.DIMENSIONLESS, z_sources=z_eff,
