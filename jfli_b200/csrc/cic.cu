@@ -144,10 +144,65 @@ __global__ void k_readout_gradient(const float* __restrict__ pos, int absolute, 
   }
 }
 
-// One fused particle pass of a PM step. Order inside: kick (with the force at the
-// current position) -> drift (with the kicked velocity) -> paint (at the new position).
-// With per-slot arrays (kicks != nullptr) every batch entry b takes its own kick, drift
-// and flags from kicks[b], drifts[b], slot_flags[b]; flags 0 leaves the slot untouched.
+// One particle of the fused pass. Order inside: kick (with the force at the current
+// position) -> drift (with the kicked velocity) -> paint (at the new position). Positions
+// and velocities stream through once per pass: streaming (evict-first) loads and stores,
+// so that they do not push the force and density meshes out of L2.
+__device__ __forceinline__ void kdp_particle(float* __restrict__ disp, float* __restrict__ vel,
+                                             const float* __restrict__ force, float kick, float drift, int flags,
+                                             float weight, float* __restrict__ rho, const PGrid& g, unsigned p, int i,
+                                             int j, int k) {
+  float x0 = __ldcs(disp + 3 * p + 0), x1 = __ldcs(disp + 3 * p + 1), x2 = __ldcs(disp + 3 * p + 2);
+  const bool use_v = flags & (kStepKick | kStepDrift);
+  float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+  if (use_v) {
+    v0 = __ldcs(vel + 3 * p + 0);
+    v1 = __ldcs(vel + 3 * p + 1);
+    v2 = __ldcs(vel + 3 * p + 2);
+  }
+  if (flags & (kStepKick | kStepCorrect)) {
+    const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
+    float fx, fy, fz;
+    gather_force_mesh(force, g, cx, cy, cz, fx, fy, fz);
+    if (flags & kStepKick) {
+      v0 += fx * kick;
+      v1 += fy * kick;
+      v2 += fz * kick;
+      __stcs(vel + 3 * p + 0, v0);
+      __stcs(vel + 3 * p + 1, v1);
+      __stcs(vel + 3 * p + 2, v2);
+    } else {
+      x0 += fx * kick;
+      x1 += fy * kick;
+      x2 += fz * kick;
+    }
+  }
+  if (flags & kStepDrift) {
+    x0 += v0 * drift;
+    x1 += v1 * drift;
+    x2 += v2 * drift;
+  }
+  if (flags & (kStepDrift | kStepCorrect)) {
+    __stcs(disp + 3 * p + 0, x0);
+    __stcs(disp + 3 * p + 1, x1);
+    __stcs(disp + 3 * p + 2, x2);
+  }
+  if (flags & kStepPaint) {
+    const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
+    deposit_lane_merged(rho, g, cx, cy, cz, weight);
+  }
+}
+
+constexpr int kBrickY = 8, kBrickZ = 32, kBrickX = 8;  // CTA of 256 = 8 warps; x walked in chunks
+
+// One fused particle pass of a PM step over all particles. With per-slot arrays (kicks !=
+// nullptr) every batch entry b takes its own kick, drift and flags from kicks[b],
+// drifts[b], slot_flags[b]; flags 0 leaves the slot untouched.
+// Work order: when nz is a multiple of 32 and ny of 8 (and the CTA has 256 threads), a CTA
+// takes an 8 (y) x 32 (z) brick of Lagrangian cells and walks it along x in chunks of 8
+// planes; warps stay on z rows (the lane-merged deposit needs them), but the rows and
+// planes whose particles share CIC corners are gathered on one SM close in time, so the
+// force-mesh lines they share are served by L1. Other shapes use a grid-stride walk.
 __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ force,
                                    float kick, float drift, int flags, float weight, float* __restrict__ rho,
                                    PGrid g, const float* __restrict__ kicks, const float* __restrict__ drifts,
@@ -163,50 +218,27 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
   vel += b * g.np * 3;
   if (force) force += b * g.np * 4;
   if (rho) rho += b * g.np;
-  // positions and velocities stream through once per pass: streaming (evict-first) loads
-  // and stores, so that they do not push the force and density meshes out of L2
+  if (blockDim.x == kBrickY * kBrickZ && g.nz % kBrickZ == 0 && g.ny % kBrickY == 0) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int tz = g.nz / kBrickZ, ty = g.ny / kBrickY, txc = (g.nx + kBrickX - 1) / kBrickX;
+    const long long items = (long long)tz * ty * txc;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+      const int iz = (int)(it % tz);
+      const long long rest = it / tz;
+      const int iy = (int)(rest % ty), xc = (int)(rest / ty);
+      const int j = iy * kBrickY + w, k = iz * kBrickZ + lane;
+      const int i1 = min(g.nx, (xc + 1) * kBrickX);
+      for (int i = xc * kBrickX; i < i1; ++i) {
+        const unsigned p = ((unsigned)i * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)k;
+        kdp_particle(disp, vel, force, kick, drift, flags, weight, rho, g, p, i, j, k);
+      }
+    }
+    return;
+  }
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
     particle_ijk(g, p, i, j, k);
-    float x0 = __ldcs(disp + 3 * p + 0), x1 = __ldcs(disp + 3 * p + 1), x2 = __ldcs(disp + 3 * p + 2);
-    const bool use_v = flags & (kStepKick | kStepDrift);
-    float v0 = 0.f, v1 = 0.f, v2 = 0.f;
-    if (use_v) {
-      v0 = __ldcs(vel + 3 * p + 0);
-      v1 = __ldcs(vel + 3 * p + 1);
-      v2 = __ldcs(vel + 3 * p + 2);
-    }
-    if (flags & (kStepKick | kStepCorrect)) {
-      const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
-      float fx, fy, fz;
-      gather_force_mesh(force, g, cx, cy, cz, fx, fy, fz);
-      if (flags & kStepKick) {
-        v0 += fx * kick;
-        v1 += fy * kick;
-        v2 += fz * kick;
-        __stcs(vel + 3 * p + 0, v0);
-        __stcs(vel + 3 * p + 1, v1);
-        __stcs(vel + 3 * p + 2, v2);
-      } else {
-        x0 += fx * kick;
-        x1 += fy * kick;
-        x2 += fz * kick;
-      }
-    }
-    if (flags & kStepDrift) {
-      x0 += v0 * drift;
-      x1 += v1 * drift;
-      x2 += v2 * drift;
-    }
-    if (flags & (kStepDrift | kStepCorrect)) {
-      __stcs(disp + 3 * p + 0, x0);
-      __stcs(disp + 3 * p + 1, x1);
-      __stcs(disp + 3 * p + 2, x2);
-    }
-    if (flags & kStepPaint) {
-      const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
-      deposit_lane_merged(rho, g, cx, cy, cz, weight);
-    }
+    kdp_particle(disp, vel, force, kick, drift, flags, weight, rho, g, p, i, j, k);
   }
 }
 

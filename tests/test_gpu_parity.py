@@ -258,20 +258,21 @@ def test_kick_drift_paint_matches_unfused(cosmo):
 @pytest.mark.parametrize("spread", [0.3, 6.0, 14.0])
 def test_kick_drift_paint_small_and_large_displacements(spread):
     """Displacements from a fraction of a cell to many cells (periodic wrap of the CIC
-    corners and of the force meshes), on a power-of-two and a 40^3 mesh."""
+    corners and of the force meshes). Meshes: 32^3 and 12 x 16 x 64 walk 8 x 32 bricks along
+    x (the latter with a short last chunk of planes), 40^3 takes the grid-stride walk."""
     from jfli_b200._lib import JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
 
-    for n in (32, 40):
-        rng = np.random.default_rng(int(spread * 10) + n)
-        x0 = rng.uniform(-spread, spread, (n, n, n, 3)).astype(np.float32)
-        v0 = rng.normal(0, 1.0, (n, n, n, 3)).astype(np.float32)
+    for shape in ((32, 32, 32), (40, 40, 40), (12, 16, 64)):
+        rng = np.random.default_rng(int(spread * 10) + shape[0])
+        x0 = rng.uniform(-spread, spread, (*shape, 3)).astype(np.float32)
+        v0 = rng.normal(0, 1.0, (*shape, 3)).astype(np.float32)
         kick, drift = 0.25, 0.5
-        pot64 = opm.potential_real(1.0 + 0.3 * rng.normal(size=(n, n, n)))
+        pot64 = opm.potential_real(1.0 + 0.3 * rng.normal(size=shape))
         x, v = dev(x0), dev(v0)
-        rho = torch.zeros(n, n, n, device="cuda")
+        rho = torch.zeros(shape, device="cuda")
         force = ops.force_mesh(dev(pot64))
         ops.kick_drift_paint(x, v, force, kick, drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT, rho)
-        kvec = opm.fftk((n, n, n))
+        kvec = opm.fftk(shape)
         pk = np.fft.fftn(pot64)
         F = np.stack([opm.cic_read(-np.fft.ifftn(opm.gradient_kernel(kvec, i) * pk).real, x0.astype(np.float64))
                       for i in range(3)], -1)
