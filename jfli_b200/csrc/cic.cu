@@ -193,13 +193,13 @@ __device__ __forceinline__ void kdp_particle(float* __restrict__ disp, float* __
   }
 }
 
-constexpr int kBrickY = 8, kBrickZ = 32, kBrickX = 8;  // CTA of 256 = 8 warps; x walked in chunks
+constexpr int kBrickY = 8, kBrickZ = 32, kBrickX = 16;  // CTA of 256 = 8 warps; x walked in chunks
 
 // One fused particle pass of a PM step over all particles. With per-slot arrays (kicks !=
 // nullptr) every batch entry b takes its own kick, drift and flags from kicks[b],
 // drifts[b], slot_flags[b]; flags 0 leaves the slot untouched.
 // Work order: when nz is a multiple of 32 and ny of 8 (and the CTA has 256 threads), a CTA
-// takes an 8 (y) x 32 (z) brick of Lagrangian cells and walks it along x in chunks of 8
+// takes an 8 (y) x 32 (z) brick of Lagrangian cells and walks it along x in chunks of 16
 // planes; warps stay on z rows (the lane-merged deposit needs them), but the rows and
 // planes whose particles share CIC corners are gathered on one SM close in time, so the
 // force-mesh lines they share are served by L1. Other shapes use a grid-stride walk.
