@@ -23,6 +23,8 @@ schedule restarts from the initial conditions inside the timed region.
           (jfli_b200.serving) and through the plain per-call path at the same offered
           load: p50/p99 latency and Mpart-steps/s of each, the engine's capacity with all
           requests queued at once, and 256^3 requests served two at a time vs one by one
+  fft_vs_cufft : this library's 3D r2c and c2r beside cuFFT (torch.fft) on the same
+          256^3 mesh, as a comparison only (cuFFT is on no path of this library)
 
 --gpus N runs N independent replicas (one per GPU, no collective on the data path);
 value is the sum over ranks / the max-over-ranks time. --impl reference times the CPU
@@ -530,6 +532,52 @@ def cpu_step_rate(n, nsteps=1):
     return n**3 * nsteps / dt / 1e6, dt
 
 
+def fft_vs_cufft(n, iters=20):
+    """This library's 3D real FFT beside cuFFT (through torch.fft) on the same seeded n^3
+    mesh, as a comparison only: CUDA-event milliseconds per forward (r2c) and inverse (c2r)
+    transform, each the mean of `iters` launches after 3 warm-ups into preallocated
+    outputs, and the largest difference of the two forward spectra relative to the largest
+    modulus. torch's c2r copies its input first (cuFFT may overwrite it); this library's
+    c2r overwrites its input in place, so neither inverse time includes a caller-side copy."""
+    import torch
+
+    from jfli_b200._lib import call, ptr, stream_ptr
+
+    g = torch.Generator(device="cuda").manual_seed(11)
+    mesh = torch.randn((n, n, n), device="cuda", generator=g)
+    spec = torch.empty((n, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    spec_t = torch.empty_like(spec)
+    work = torch.empty_like(spec)
+    out = torch.empty_like(mesh)
+    out_t = torch.empty_like(mesh)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(iters):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / iters
+
+    fwd = lambda: call("jfli_rfft3d", stream_ptr(), ptr(mesh), ptr(spec), n, n, n, 1)
+    inv = lambda: call("jfli_irfft3d", stream_ptr(), ptr(work), ptr(out), n, n, n, 1)
+    fwd_t = lambda: torch.fft.rfftn(mesh, out=spec_t)
+    inv_t = lambda: torch.fft.irfftn(spec_t, s=(n, n, n), out=out_t)
+    res = {"mesh": n, "iters": iters, "r2c_ms": round(timed(fwd), 4), "r2c_cufft_ms": round(timed(fwd_t), 4)}
+    work.copy_(spec)
+    res["c2r_ms"] = round(timed(inv), 4)
+    res["c2r_cufft_ms"] = round(timed(inv_t), 4)
+    fwd()
+    fwd_t()
+    torch.cuda.synchronize()
+    res["r2c_max_rel_diff"] = float((spec - spec_t).abs().max() / spec_t.abs().max())
+    return res
+
+
 def cpu_baseline_block(n):
     """The FP32 NumPy/SciPy port on this host: one KDK step at n^3 (the workload itself,
     ~20-40 s of CPU work at 256^3) and, for reference, five steps at 64^3."""
@@ -668,6 +716,7 @@ def main():
     world, rank, local = dist_setup(args)
     res = run_gpu(args, world, rank)
     if rank == 0:
+        fft_cmp = fft_vs_cufft(args.mesh)
         cpu = None if args.no_cpu_baseline else cpu_baseline_block(args.mesh)
         line = {"metric": METRIC, "value": round(res["value"], 2), "unit": "Mpart-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(res["ms"] / args.steps, 4),
@@ -680,7 +729,7 @@ def main():
                            "l2": "particle state (x, v: 402 MB) exceeds the 126 MB L2; no flush"},
                 "roofline": res["roofline"], "step_roofline": res["step_roofline"], "cpu_baseline": cpu, "e2e": res["e2e"], "clocks": res["clocks"],
                 "gpu_launches": res["launches"], "serving": res["serving"], "gradient": res["gradient"],
-                "e2e_with_shells": res["shells"]}
+                "e2e_with_shells": res["shells"], "fft_vs_cufft": fft_cmp}
         print(json.dumps(line), flush=True)
     if world > 1:
         from jfli_b200 import replicas
