@@ -6,7 +6,7 @@ every operation on them runs in libjfli_b200's sm_100a kernels.
 """
 
 from . import cosmology, ops, utils
-from . import catalog as io
+from . import io_api as io
 from . import fields as units
 from .catalog import CATALOG_VERSION, Catalog
 from .cosmology import Cosmology, Planck18
@@ -32,7 +32,7 @@ from .fields import (
     uniform_particles,
 )
 from .initial import gaussian_initial_conditions, interpolate_initial_conditions, white_noise
-from .lensing import RedshiftDistribution, born, smail_nz, tophat_nz
+from .lensing import RedshiftDistribution, born, kde_nz, smail_nz, tophat_nz
 from .pm import (
     AbstractNBodySolver,
     DriftInterp,

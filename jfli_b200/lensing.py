@@ -33,19 +33,25 @@ def simpson_weights(a: float, b: float, n: int) -> np.ndarray:
     return w * ((b - a) / n / 3.0)
 
 
-@dataclasses.dataclass(frozen=True)
+@dataclasses.dataclass(frozen=True, eq=False)
 class RedshiftDistribution:
     """n(z) normalised on [0, zmax] with Simpson's rule on 256 intervals, like
-    jax_cosmo.redshift.redshift_distribution (pz_fn(z, *params) / norm)."""
+    jax_cosmo.redshift.redshift_distribution (pz_fn(z, *params) / norm), with its
+    galaxy density (gals_per_arcmin2, default 1)."""
 
     pz_fn: object
     params: tuple = ()
     zmax: float = 10.0
+    gals_per_arcmin2: float = 1.0
 
     @property
     def norm(self) -> float:
         z = np.linspace(0.0, self.zmax, 257)
         return float(np.sum(simpson_weights(0.0, self.zmax, 256) * self.pz_fn(z, *self.params)))
+
+    @property
+    def gals_per_steradian(self) -> float:
+        return self.gals_per_arcmin2 * (180.0 * 60.0 / math.pi) ** 2
 
     def __call__(self, z):
         z = np.asarray(z, dtype=np.float64)
@@ -66,6 +72,29 @@ def _smail(z, a, b, z0):
 
 def smail_nz(a: float, b: float, z0: float, zmax: float = 10.0) -> RedshiftDistribution:
     return RedshiftDistribution(_smail, (float(a), float(b), float(z0)), zmax=float(zmax))
+
+
+def _kde(z, zcat, weight, bw):
+    """Weighted Gaussian kernel density estimate: sum_i w_i N(z; zcat_i, bw) / sum_i w_i."""
+    d = (np.atleast_1d(z)[None, :] - zcat[:, None]) / bw
+    k = np.exp(-0.5 * d * d) / (math.sqrt(2.0 * math.pi) * bw)
+    out = weight @ k / np.sum(weight)
+    return out if np.ndim(z) else out[0]
+
+
+def kde_nz(zcat, weight, bw: float, zmax: float = 10.0, gals_per_arcmin2: float = 1.0) -> RedshiftDistribution:
+    """n(z) as a Gaussian kernel density estimate of the samples `zcat` with weights
+    `weight` and bandwidth `bw`, normalised on [0, zmax] (jax_cosmo.redshift.kde_nz, from
+    the jax_cosmo fork jax-fli pins at ASKabalan/jax_cosmo@ALL-MODIF, pyproject.toml:33;
+    used by io/cosmogrid.py:25-67 for the Stage-3 distributions)."""
+    zcat = np.asarray(zcat, dtype=np.float64).ravel()
+    weight = np.asarray(weight, dtype=np.float64).ravel()
+    if zcat.shape != weight.shape or zcat.size == 0:
+        raise ValueError("zcat and weight must be non-empty and of the same length")
+    if not bw > 0:
+        raise ValueError("bw must be positive")
+    return RedshiftDistribution(_kde, (zcat, weight, float(bw)), zmax=float(zmax),
+                                gals_per_arcmin2=float(gals_per_arcmin2))
 
 
 def _sources(nz_shear):
