@@ -181,11 +181,47 @@ def _field_from_row(item: dict, device) -> tuple[AbstractField, Cosmology, int]:
     return field, cosmo, int(item["version"])
 
 
+_COSMO_PARAMS = ("Omega_c", "Omega_b", "h", "n_s", "sigma8", "Omega_k", "w0", "wa")
+
+
+def _cosmology_batch(c: Cosmology) -> int:
+    """1 for a cosmology of scalars, N when its parameters are length-N arrays."""
+    sizes = {int(np.size(getattr(c, k))) for k in _COSMO_PARAMS}
+    sizes.discard(1)
+    if len(sizes) > 1:
+        raise ValueError(f"batched cosmology parameters have different lengths {sorted(sizes)}")
+    return sizes.pop() if sizes else 1
+
+
+def _cosmology_entry(c: Cosmology, i: int) -> Cosmology:
+    """Entry i of a batched cosmology (scalar parameters are shared)."""
+    pick = lambda v: float(np.ravel(v)[i]) if np.size(v) > 1 else float(np.ravel(v)[0])
+    return Cosmology(**{k: pick(getattr(c, k)) for k in _COSMO_PARAMS})
+
+
 class Catalog:
     """Fields and their cosmologies (reference io/catalog.py:340-510): lists of equal length;
-    a single field and cosmology are wrapped into length-1 lists."""
+    a single field and cosmology are wrapped into length-1 lists, or split into N entries
+    when the cosmology is batched (parameters given as length-N arrays)."""
 
     def __init__(self, field, cosmology, version: int = CATALOG_VERSION):
+        if isinstance(field, AbstractField) and isinstance(cosmology, Cosmology):
+            # one field with one cosmology; a batched cosmology (parameters as length-N
+            # arrays) splits a field with leading dimension N into N entries
+            # (reference io/catalog.py:361-382)
+            cosmo_n = _cosmology_batch(cosmology)
+            if cosmo_n > 1:
+                field_n = field.array.shape[0] if field.is_batched() else 1
+                if field_n != cosmo_n:
+                    raise ValueError(f"Cosmology batch size {cosmo_n} != field leading dimension {field_n}.")
+                field = [field[i] for i in range(cosmo_n)]
+                cosmology = [_cosmology_entry(cosmology, i) for i in range(cosmo_n)]
+            elif field.is_multi_batched() and field.array.shape[0] > 1:
+                raise ValueError(f"Scalar cosmology cannot pair with a multi-batched field (shape "
+                                 f"{tuple(field.array.shape)}, N={field.array.shape[0]} > 1). Pass a batched cosmology "
+                                 f"of size N, or split the field first.")
+            else:
+                field, cosmology = [field], [cosmology]
         if isinstance(field, AbstractField):
             field = [field]
         if isinstance(cosmology, Cosmology):

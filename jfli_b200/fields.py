@@ -155,8 +155,68 @@ class AbstractField:
     def is_batched(self) -> bool:
         return self.array.ndim > self._core_ndim()
 
+    def is_multi_batched(self) -> bool:
+        """True for an (N, S, ...) field: a simulation batch N and a snapshot batch S
+        (reference fields/density.py:491, fields/lightcone.py:441,858, fields/particles.py:635)."""
+        return self.array.ndim == self._core_ndim() + 2
+
     def _core_ndim(self) -> int:
         return 3
+
+    _DYNAMIC = ("z_sources", "scale_factors", "comoving_centers", "density_width")
+
+    @classmethod
+    def _join(cls, fields, how: str):
+        """Stack or concatenate the arrays and the dynamic metadata of fields whose static
+        metadata agree (reference _src/base/_core.py:248-282, a tree map over the array leaves)."""
+        first = fields[0]
+        static = [f.name for f in dataclasses.fields(first) if f.name != "array" and f.name not in cls._DYNAMIC]
+        for f in fields[1:]:
+            if type(f) is not type(first):
+                raise ValueError(f"cannot {how} fields of types {type(first).__name__} and {type(f).__name__}")
+            for name in static:
+                if getattr(f, name) != getattr(first, name):
+                    raise ValueError(f"cannot {how} fields whose {name} differ")
+        arrays = [f.array for f in fields]
+        if isinstance(arrays[0], torch.Tensor):
+            array = torch.stack(arrays) if how == "stack" else torch.cat(arrays)
+        else:
+            array = np.stack(arrays) if how == "stack" else np.concatenate(arrays)
+
+        def meta(name):
+            vals = [getattr(f, name) for f in fields]
+            if all(v is None for v in vals):
+                return None
+            if any(v is None for v in vals):
+                raise ValueError(f"cannot {how} fields where only some carry {name}")
+            vals = [v.detach().cpu().numpy() if isinstance(v, torch.Tensor) else np.asarray(v, np.float64)
+                    for v in vals]
+            return np.stack(vals) if how == "stack" else np.concatenate(vals)
+
+        return first.replace(array=array, **{name: meta(name) for name in cls._DYNAMIC})
+
+    @classmethod
+    def stack(cls, fields):
+        """Stack fields along a new axis 0: (S, ...) inputs give an (N, S, ...) multi-batched
+        field. Multi-batched inputs are refused; concat joins those."""
+        fields = tuple(fields)
+        if not fields:
+            raise ValueError("stack requires at least one field.")
+        if any(f.is_multi_batched() for f in fields):
+            raise ValueError("Cannot stack multi-batched (N, S, ...) fields: the extra leading dimension would be "
+                             "ambiguous. Use <FieldClass>.concat(fields) to join along the N axis instead.")
+        return cls._join(fields, "stack")
+
+    @classmethod
+    def concat(cls, fields):
+        """Concatenate multi-batched (N, S, ...) fields along the N axis."""
+        fields = tuple(fields)
+        if not fields:
+            raise ValueError("concat requires at least one field.")
+        if any(not f.is_multi_batched() for f in fields):
+            raise ValueError("concat only works on multi-batched (N, S, ...) fields. Use stack() to create an "
+                             "(N, S, ...) field from (S, ...) inputs.")
+        return cls._join(fields, "concat")
 
     def __getitem__(self, key):
         if not self.is_batched():

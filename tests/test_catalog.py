@@ -100,3 +100,104 @@ def test_catalog_kappa_field(tmp_path):
     assert kap.to(jf.ConvergenceUnit.EFFECTIVE_DENSITY).unit == jf.ConvergenceUnit.EFFECTIVE_DENSITY
     with pytest.raises(NotImplementedError):
         kap.get_shear()
+
+
+# ------------------------------------------------------- multi-batched fields (N, S, ...)
+MESH = (8, 8, 8)
+
+
+def _density(array, **dyn):
+    meta = dict(mesh_size=MESH, box_size=(100.0, 100.0, 100.0), observer_position=(0.5, 0.5, 0.5),
+                status=jf.FieldStatus.DENSITY_FIELD, unit=jf.DensityUnit.DENSITY)
+    base = dict(z_sources=1.0, scale_factors=0.8, comoving_centers=300.0, density_width=25.0)
+    base.update(dyn)
+    return jf.DensityField(array=array, **meta, **base)
+
+
+def _multi(N, S, seed=0):
+    rng = np.random.default_rng(seed)
+    return _density(torch.as_tensor(rng.standard_normal((N, S, *MESH)).astype(np.float32)),
+                    z_sources=rng.uniform(0.5, 2.0, (N, S)), scale_factors=rng.uniform(0.5, 1.0, (N, S)),
+                    comoving_centers=rng.uniform(100, 500, (N, S)), density_width=rng.uniform(10, 50, (N, S)))
+
+
+def _batched_cosmo(n):
+    """A cosmology whose parameters are length-n arrays (the reference's batched jc.Cosmology)."""
+    return jf.Cosmology(Omega_c=np.full(n, 0.3), Omega_b=np.full(n, 0.05), h=np.full(n, 0.7),
+                        n_s=np.full(n, 0.96), sigma8=np.linspace(0.7, 0.9, n), Omega_k=np.zeros(n),
+                        w0=np.full(n, -1.0), wa=np.zeros(n))
+
+
+def test_multi_batched_predicates():
+    """(N, S, spatial...) arrays are batched and multi-batched for every field type
+    (reference tests/test_catalog.py:306-368)."""
+    N, S = 2, 4
+    meta = dict(mesh_size=MESH, box_size=(100.0, 100.0, 100.0))
+    fields = [jf.SphericalDensity(array=torch.zeros(N, S, 192), nside=4, **meta),
+              jf.SphericalKappaField(array=torch.zeros(N, S, 192), nside=4, **meta),
+              jf.FlatDensity(array=torch.zeros(N, S, 16, 16), flatsky_npix=(16, 16), **meta),
+              jf.FlatKappaField(array=torch.zeros(N, S, 16, 16), flatsky_npix=(16, 16), **meta),
+              jf.DensityField(array=torch.zeros(N, S, *MESH), **meta),
+              jf.ParticleField(array=torch.zeros(N, S, *MESH, 3), **meta)]
+    for f in fields:
+        assert f.is_multi_batched() and f.is_batched(), type(f).__name__
+        assert not f[0].is_multi_batched() and f[0].is_batched()
+        assert not f[0][0].is_batched()
+
+
+def test_stack_and_concat():
+    S = 4
+    f1 = _density(torch.zeros(S, *MESH))
+    f2 = _density(torch.ones(S, *MESH), z_sources=1.2, scale_factors=0.75, comoving_centers=350.0,
+                  density_width=20.0)
+    st = jf.DensityField.stack([f1, f2])
+    assert tuple(st.array.shape) == (2, S, *MESH) and st.is_multi_batched()
+    np.testing.assert_allclose(st.z_sources, [1.0, 1.2])
+    assert torch.equal(st[1].array, f2.array)
+    with pytest.raises(ValueError, match="concat"):
+        jf.DensityField.stack([st, st])
+    a, b = _multi(2, S, seed=1), _multi(2, S, seed=2)
+    cat = jf.DensityField.concat([a, b])
+    assert tuple(cat.array.shape) == (4, S, *MESH) and cat.is_multi_batched()
+    assert cat.z_sources.shape == (4, S)
+    np.testing.assert_allclose(cat.z_sources[2:], b.z_sources)
+    with pytest.raises(ValueError, match="stack"):
+        jf.DensityField.concat([f1])
+    with pytest.raises(ValueError):
+        jf.DensityField.stack([f1, f1.replace(box_size=(200.0, 200.0, 200.0))])
+    with pytest.raises(ValueError):
+        jf.DensityField.stack([])
+
+
+def test_catalog_expands_batched_cosmology(tmp_path):
+    """(N, S, ...) field + cosmology of N -> N entries of (S, ...); (S, ...) field + cosmology
+    of S -> S unbatched entries; a scalar cosmology with N > 1 is refused (reference
+    tests/test_catalog.py:447-517)."""
+    N, S = 2, 4
+    field = _multi(N, S)
+    cat = jf.Catalog(field=field, cosmology=_batched_cosmo(N))
+    assert len(cat) == N
+    for i, entry in enumerate(cat.field):
+        assert tuple(entry.array.shape) == (S, *MESH) and entry.is_batched() and not entry.is_multi_batched()
+        np.testing.assert_allclose(entry.z_sources, field.z_sources[i])
+    assert [c.sigma8 for c in cat.cosmology] == pytest.approx([0.7, 0.9])
+    assert all(isinstance(c.Omega_c, float) for c in cat.cosmology)
+    path = str(tmp_path / "multi.parquet")
+    cat.to_parquet(path)
+    back = jf.Catalog.from_parquet(path, device="cpu")
+    assert len(back) == N
+    for x, y in zip(cat.field, back.field):
+        assert tuple(y.array.shape) == (S, *MESH) and y.is_batched() and not y.is_multi_batched()
+        assert torch.equal(x.array, y.array)
+
+    snap = _multi(1, 3)[0]
+    cat = jf.Catalog(field=snap, cosmology=_batched_cosmo(3))
+    assert len(cat) == 3
+    assert all(tuple(e.array.shape) == MESH and not e.is_batched() for e in cat.field)
+
+    with pytest.raises(ValueError, match="Scalar cosmology"):
+        jf.Catalog(field=field, cosmology=jf.Planck18())
+    with pytest.raises(ValueError, match="batch size"):
+        jf.Catalog(field=field, cosmology=_batched_cosmo(3))
+    single = jf.Catalog(field=_multi(1, S), cosmology=jf.Planck18())
+    assert len(single) == 1
