@@ -160,6 +160,134 @@ class AbstractField:
         (reference fields/density.py:491, fields/lightcone.py:441,858, fields/particles.py:635)."""
         return self.array.ndim == self._core_ndim() + 2
 
+    # ------------------------------------------ array shorthands (reference _src/base/_core.py:25-171)
+    @property
+    def shape(self) -> tuple:
+        return tuple(self.array.shape)
+
+    @property
+    def ndim(self) -> int:
+        return self.array.ndim
+
+    @property
+    def size(self) -> int:
+        return int(self.array.numel()) if isinstance(self.array, torch.Tensor) else int(np.size(self.array))
+
+    @property
+    def dtype(self):
+        return self.array.dtype
+
+    def __len__(self) -> int:
+        return len(self.array)
+
+    def __iter__(self):
+        """The entries along the first dimension, each a field of this class."""
+        for i in range(len(self)):
+            yield self[i]
+
+    # Arithmetic acts on the array and keeps the metadata of the left-hand field; another
+    # field contributes its array.
+    @staticmethod
+    def _operand(other):
+        return other.array if isinstance(other, AbstractField) else other
+
+    def __add__(self, other):
+        return self.replace(array=self.array + self._operand(other))
+
+    def __radd__(self, other):
+        return self.replace(array=self._operand(other) + self.array)
+
+    def __sub__(self, other):
+        return self.replace(array=self.array - self._operand(other))
+
+    def __rsub__(self, other):
+        return self.replace(array=self._operand(other) - self.array)
+
+    def __mul__(self, other):
+        return self.replace(array=self.array * self._operand(other))
+
+    def __rmul__(self, other):
+        return self.replace(array=self._operand(other) * self.array)
+
+    def __truediv__(self, other):
+        return self.replace(array=self.array / self._operand(other))
+
+    def __rtruediv__(self, other):
+        return self.replace(array=self._operand(other) / self.array)
+
+    def __neg__(self):
+        return self.replace(array=-self.array)
+
+    def __pos__(self):
+        return self
+
+    def __abs__(self):
+        return self.replace(array=abs(self.array))
+
+    def _reduce(self, name: str, axis=None, keepdims: bool = False):
+        a = self.array
+        if isinstance(a, torch.Tensor):
+            if name == "std":  # population standard deviation, as numpy's and jnp's default
+                return torch.std(a, correction=0) if axis is None else torch.std(a, dim=axis, correction=0,
+                                                                                 keepdim=keepdims)
+            fn = {"min": torch.amin, "max": torch.amax, "mean": torch.mean}[name]
+            if axis is None:
+                return fn(a) if not keepdims else fn(a, dim=tuple(range(a.ndim)), keepdim=True)
+            return fn(a, dim=axis, keepdim=keepdims)
+        return getattr(np, name)(a, axis=axis, keepdims=keepdims)
+
+    def min(self, axis=None, keepdims: bool = False):
+        return self._reduce("min", axis, keepdims)
+
+    def max(self, axis=None, keepdims: bool = False):
+        return self._reduce("max", axis, keepdims)
+
+    def mean(self, axis=None, keepdims: bool = False):
+        return self._reduce("mean", axis, keepdims)
+
+    def std(self, axis=None, keepdims: bool = False):
+        return self._reduce("std", axis, keepdims)
+
+    def transpose(self, *axes):
+        a = self.array
+        if len(axes) == 1 and isinstance(axes[0], (tuple, list)):
+            axes = tuple(axes[0])
+        if isinstance(a, torch.Tensor):
+            return self.replace(array=a.permute(*(axes or tuple(reversed(range(a.ndim))))))
+        return self.replace(array=np.transpose(a, axes or None))
+
+    @property
+    def T(self):
+        return self.transpose()
+
+    def apply_fn(self, fn, *args, **kwargs):
+        """A field of this class holding fn(array, *args, **kwargs)."""
+        return self.replace(array=fn(self.array, *args, **kwargs))
+
+    def __array__(self, dtype=None, copy=None):
+        a = self.array
+        if isinstance(a, torch.Tensor):
+            a = a.detach().cpu().numpy()
+        return np.asarray(a, dtype=dtype)
+
+    def block_until_ready(self):
+        """Waits for the device work that produces the array."""
+        if isinstance(self.array, torch.Tensor) and self.array.is_cuda:
+            torch.cuda.synchronize(self.array.device)
+        return self
+
+    def to_metadata(self) -> "FieldMetadata":
+        """The metadata alone, as a FieldMetadata with no array (reference _src/base/_core.py:478-496)."""
+        return FieldMetadata(array=None, **self._meta())
+
+    @staticmethod
+    def _full(shape, fill_value, like):
+        a = getattr(like, "array", None)
+        if isinstance(a, torch.Tensor):
+            return torch.full(tuple(shape), float(fill_value), dtype=torch.float32, device=a.device)
+        device = "cuda" if torch.cuda.is_available() else "cpu"
+        return torch.full(tuple(shape), float(fill_value), dtype=torch.float32, device=device)
+
     def _core_ndim(self) -> int:
         return 3
 
@@ -243,6 +371,12 @@ class PowerSpectrum:
 
 @dataclasses.dataclass(frozen=True, eq=False)
 class DensityField(AbstractField):
+    @classmethod
+    def full_like(cls, field: AbstractField, fill_value: float = 0.0) -> "DensityField":
+        """A mesh of mesh_size filled with fill_value, with field's metadata (reference
+        fields/density.py:476-485)."""
+        return cls.FromDensityMetadata(array=cls._full(field.mesh_size, fill_value, field), field=field)
+
     def to(self, unit, *, omega_m=None, h=None, mean_density=None) -> "DensityField":
         """Unit conversion with the voxel volume prod(L / N) (reference fields/density.py:66-124)."""
         vol = float(np.prod(np.asarray(self.box_size, np.float64) / np.asarray(self.mesh_size, np.float64)))
@@ -262,6 +396,15 @@ class DensityField(AbstractField):
 class SphericalDensity(AbstractField):
     def _core_ndim(self) -> int:
         return 1
+
+    @classmethod
+    def full_like(cls, field: AbstractField, fill_value: float = 0.0) -> "SphericalDensity":
+        """One HEALPix map of field's nside filled with fill_value (reference
+        fields/lightcone.py:840-852)."""
+        if field.nside is None:
+            raise ValueError("nside metadata is required to create full_like SphericalDensity.")
+        return cls.FromDensityMetadata(array=cls._full((12 * field.nside * field.nside,), fill_value, field),
+                                       field=field)
 
     def to(self, unit, *, omega_m=None, h=None, mean_density=None) -> "SphericalDensity":
         """Unit conversion with each shell's exact pixel volume (4 pi / npix)(R_max^3 - R_min^3) / 3
@@ -316,6 +459,14 @@ class FlatDensity(AbstractField):
     def _core_ndim(self) -> int:
         return 2
 
+    @classmethod
+    def full_like(cls, field: AbstractField, fill_value: float = 0.0) -> "FlatDensity":
+        """One flat map of field's flatsky_npix filled with fill_value (reference
+        fields/lightcone.py:423-435, which shapes it by field_size)."""
+        if field.flatsky_npix is None:
+            raise ValueError("flatsky_npix metadata is required to create full_like FlatDensity.")
+        return cls.FromDensityMetadata(array=cls._full(field.flatsky_npix, fill_value, field), field=field)
+
     def __post_init__(self):
         super().__post_init__()
         if self.array.ndim not in (2, 3, 4):
@@ -354,6 +505,12 @@ class FlatDensity(AbstractField):
 class ParticleField(AbstractField):
     def _core_ndim(self) -> int:
         return 4
+
+    @classmethod
+    def full_like(cls, field: AbstractField, fill_value: float = 0.0) -> "ParticleField":
+        """A (mesh_size, 3) particle grid filled with fill_value (reference fields/particles.py:620-629)."""
+        return cls.FromDensityMetadata(array=cls._full(tuple(field.mesh_size) + (3,), fill_value, field),
+                                       field=field)
 
     def to(self, unit: PositionUnit) -> "ParticleField":
         """Unit conversion through GRID_ABSOLUTE (reference fields/units.py:78-130)."""
@@ -618,6 +775,10 @@ class FlatShearField(FlatDensity):
 @dataclasses.dataclass(frozen=True, eq=False)
 class FieldMetadata(AbstractField):
     """Metadata-only field (array None), as the reference's to_metadata() produces."""
+
+    @classmethod
+    def full_like(cls, field: AbstractField, fill_value: float = 0.0):
+        raise NotImplementedError("FieldMetadata is metadata-only; use a concrete field class.")
 
     def is_batched(self) -> bool:
         return False

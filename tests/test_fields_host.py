@@ -1,0 +1,80 @@
+"""Field containers on the host: the array shorthands, arithmetic, reductions, full_like,
+to_metadata and iteration of the reference's field pytrees (_src/base/_core.py:25-171,
+fields/*.py full_like), on CPU tensors."""
+
+import numpy as np
+import pytest
+import torch
+
+import jfli_b200 as jf
+
+MESH = (4, 6, 8)
+META = dict(mesh_size=MESH, box_size=(100.0, 150.0, 200.0), observer_position=(0.5, 0.5, 0.5))
+
+
+def _density(array, **kw):
+    return jf.DensityField(array=array, status=jf.FieldStatus.DENSITY_FIELD, unit=jf.DensityUnit.DENSITY,
+                           scale_factors=kw.pop("scale_factors", 0.8), **META, **kw)
+
+
+def test_shorthands_and_reductions():
+    rng = np.random.default_rng(0)
+    a = torch.as_tensor(rng.standard_normal((3, *MESH)).astype(np.float32))
+    f = _density(a, scale_factors=np.array([0.5, 0.7, 0.9]))
+    assert f.shape == (3, *MESH) and f.ndim == 4 and f.size == a.numel() and f.dtype == torch.float32
+    assert len(f) == 3
+    entries = list(f)
+    assert len(entries) == 3 and all(isinstance(e, jf.DensityField) for e in entries)
+    assert torch.equal(entries[2].array, a[2]) and float(entries[2].scale_factors) == 0.9
+    x = a.double().numpy()
+    assert float(f.mean()) == pytest.approx(x.mean(), rel=1e-6)
+    assert float(f.std()) == pytest.approx(x.std(), rel=1e-5)  # population, as jnp.std
+    assert float(f.min()) == x.min() and float(f.max()) == x.max()
+    np.testing.assert_allclose(f.mean(axis=0).numpy(), x.mean(0), rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(f.std(axis=(1, 2, 3)).numpy(), x.std(axis=(1, 2, 3)), rtol=1e-5)
+    assert tuple(f.max(axis=1, keepdims=True).shape) == (3, 1, 6, 8)
+    np.testing.assert_array_equal(np.asarray(f), a.numpy())
+    assert f.T.shape == (8, 6, 4, 3) and f.transpose(0, 2, 1, 3).shape == (3, 6, 4, 8)
+    assert f.apply_fn(torch.clamp, min=0.0).min() >= 0
+    assert f.block_until_ready() is f
+    # numpy-backed fields behave the same way
+    g = _density(x[0])
+    assert g.mean() == pytest.approx(x[0].mean()) and g.T.shape == MESH[::-1]
+
+
+def test_arithmetic_keeps_metadata():
+    a = torch.full(MESH, 2.0)
+    b = torch.full(MESH, 0.5)
+    f, g = _density(a), _density(b)
+    delta = f / f.mean() - 1
+    assert isinstance(delta, jf.DensityField) and delta.box_size == f.box_size and delta.unit == f.unit
+    assert torch.equal(delta.array, torch.zeros(MESH))
+    assert torch.equal((f + g).array, a + b) and torch.equal((f - g).array, a - b)
+    assert torch.equal((f * g).array, a * b) and torch.equal((f / g).array, a / b)
+    assert torch.equal((3 * f).array, 3 * a) and torch.equal((1 + f).array, 1 + a)
+    assert torch.equal((1 - f).array, 1 - a) and torch.equal((1 / f).array, 1 / a)
+    assert torch.equal((-f).array, -a) and (+f) is f and torch.equal(abs(-f).array, a)
+    assert torch.equal(sum([f, g]).array, a + b)
+
+
+def test_full_like_and_metadata():
+    base = _density(torch.zeros(MESH), nside=4, flatsky_npix=(5, 7), field_size=(2.0, 3.0))
+    d = jf.DensityField.full_like(base, 2.5)
+    assert d.shape == MESH and torch.all(d.array == 2.5) and d.box_size == base.box_size
+    p = jf.ParticleField.full_like(base)
+    assert p.shape == (*MESH, 3) and torch.all(p.array == 0)
+    s = jf.SphericalDensity.full_like(base, 1.0)
+    assert s.shape == (12 * 16,) and s.nside == 4
+    fl = jf.FlatDensity.full_like(base, -1.0)
+    assert fl.shape == (5, 7)
+    with pytest.raises(ValueError, match="nside"):
+        jf.SphericalDensity.full_like(base.replace(nside=None))
+    with pytest.raises(ValueError, match="flatsky_npix"):
+        jf.FlatDensity.full_like(base.replace(flatsky_npix=None))
+    m = base.to_metadata()
+    assert isinstance(m, jf.FieldMetadata) and m.array is None
+    assert (m.mesh_size, m.box_size, m.nside, m.flatsky_npix, m.status, m.unit) == \
+           (base.mesh_size, base.box_size, base.nside, base.flatsky_npix, base.status, base.unit)
+    assert not m.is_batched() and not m.is_multi_batched()
+    with pytest.raises(NotImplementedError):
+        jf.FieldMetadata.full_like(base)
