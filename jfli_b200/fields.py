@@ -355,6 +355,27 @@ class AbstractField:
                             density_width=sub(self.density_width))
 
 
+def _stack(rows):
+    return torch.stack(rows) if isinstance(rows[0], torch.Tensor) else np.stack(rows)
+
+
+def _cl_transfer(field, other, **kw) -> "PowerSpectrum":
+    """sqrt(C_other / C_self) of two map fields (reference fields/lightcone.py:318-365,746-788)."""
+    cl_self = field.angular_cl(**kw)
+    cl_other = other.angular_cl(**kw)
+    return PowerSpectrum(wavenumber=cl_self.wavenumber, array=(cl_other.array / cl_self.array) ** 0.5,
+                         name="transfer", scale_factors=field.scale_factors)
+
+
+def _cl_coherence(field, other, **kw) -> "PowerSpectrum":
+    """C_cross / sqrt(C_self C_other) of two map fields (reference fields/lightcone.py:367-421,790-838)."""
+    cl_self = field.angular_cl(**kw)
+    cl_other = other.angular_cl(**kw)
+    cl_cross = field.angular_cl(other, **kw)
+    return PowerSpectrum(wavenumber=cl_self.wavenumber, array=cl_cross.array / (cl_self.array * cl_other.array) ** 0.5,
+                         name="coherence", scale_factors=field.scale_factors)
+
+
 @dataclasses.dataclass(frozen=True, eq=False)
 class PowerSpectrum:
     """P(k) container (reference power/power_spec.py:20-60)."""
@@ -390,6 +411,69 @@ class DensityField(AbstractField):
         m2 = mesh2.array if isinstance(mesh2, AbstractField) else mesh2
         k, pk = power_fn(self.array, m2, box_shape=self.box_size, kedges=kedges, multipoles=multipoles, los=los)
         return PowerSpectrum(wavenumber=k, array=pk, name="pk", scale_factors=self.scale_factors)
+
+    def cross_power(self, *, kedges=None, multipoles=0, los=(0.0, 0.0, 1.0), batch_size=None) -> PowerSpectrum:
+        """P(k) of every pair (i, j), i <= j, of a batch of B meshes, in upper-triangular
+        order (0,0), (0,1), ..., (0,B-1), (1,1), ...: array (B(B+1)/2, ...) (reference
+        fields/density.py:319-403)."""
+        from .power import power as power_fn
+
+        data = self.array
+        if data.ndim != 4:
+            raise ValueError(f"cross_power requires batched array with shape (B, X, Y, Z), got array with "
+                             f"{data.ndim} dimensions. Use power() for single fields.")
+        if data.shape[0] < 2:
+            raise ValueError(f"cross_power requires at least 2 maps in batch dimension, got {data.shape[0]}. "
+                             f"Use power() for single fields.")
+        k, spectra = None, []
+        for i in range(data.shape[0]):
+            for j in range(i, data.shape[0]):
+                k_ij, pk = power_fn(data[i], data[j], box_shape=self.box_size, kedges=kedges,
+                                    multipoles=multipoles, los=los)
+                k = k_ij if k is None else k
+                spectra.append(pk)
+        return PowerSpectrum(wavenumber=k, array=_stack(spectra), name="cross_pk", scale_factors=self.scale_factors)
+
+    def _paired(self, other, fn, name, kedges):
+        data1, data2 = self.array, other.array
+        if data1.ndim not in (3, 4):
+            raise ValueError(f"DensityField.{name} expects array shape (X,Y,Z) or (B,X,Y,Z)")
+        if tuple(data2.shape) != tuple(data1.shape):
+            raise ValueError(f"other array must match shape for {name}")
+        rows = [(data1, data2)] if data1.ndim == 3 else list(zip(data1, data2))
+        k, spectra = None, []
+        for m1, m2 in rows:
+            k_i, r = fn(m1, m2, box_shape=self.box_size, kedges=kedges)
+            k = k_i if k is None else k
+            spectra.append(r)
+        arr = _stack(spectra) if data1.ndim == 4 else spectra[0]
+        return PowerSpectrum(wavenumber=k, array=arr, name=name, scale_factors=self.scale_factors)
+
+    def transfer(self, other: "DensityField", *, kedges=None, batch_size=None) -> PowerSpectrum:
+        """Monopole transfer function sqrt(P_other / P_self), per batch entry (reference
+        fields/density.py:404-439)."""
+        from .power import transfer
+
+        return self._paired(other, transfer, "transfer", kedges)
+
+    def coherence(self, other: "DensityField", *, kedges=None, batch_size=None) -> PowerSpectrum:
+        """Monopole coherence P_cross / sqrt(P_self P_other), per batch entry (reference
+        fields/density.py:440-475)."""
+        from .power import coherence
+
+        return self._paired(other, coherence, "coherence", kedges)
+
+    def project(self, nz_slices: int = 10) -> "FlatDensity":
+        """Sum of the last nz_slices planes along z as a flat map of shape (X, Y) or (B, X, Y),
+        status PROJECTED_DENSITY (reference fields/density.py:127-159)."""
+        data = self.array
+        if data.ndim not in (3, 4):
+            raise ValueError(f"project() expects 3D array or batch of 3D arrays, got shape {tuple(data.shape)}")
+        sl = data[..., -nz_slices:]
+        proj = sl.sum(dim=-1) if isinstance(sl, torch.Tensor) else np.sum(sl, axis=-1)
+        npix = tuple(int(v) for v in proj.shape[-2:])
+        return FlatDensity.FromDensityMetadata(array=proj, field=self.replace(flatsky_npix=npix),
+                                               status=FieldStatus.PROJECTED_DENSITY)
 
 
 @dataclasses.dataclass(frozen=True, eq=False)
@@ -439,6 +523,16 @@ class SphericalDensity(AbstractField):
             spectra.append(cl)
         arr = np.stack(spectra) if d1.ndim == 2 else spectra[0]
         return PowerSpectrum(wavenumber=ell, array=arr, name="cl", scale_factors=self.scale_factors)
+
+    def transfer(self, other: "SphericalDensity", *, lmax: int | None = None, method: str = "jax",
+                 batch_size=None) -> PowerSpectrum:
+        """Transfer function sqrt(C_other / C_self) (reference fields/lightcone.py:746-788)."""
+        return _cl_transfer(self, other, lmax=lmax, method=method)
+
+    def coherence(self, other: "SphericalDensity", *, lmax: int | None = None, method: str = "jax",
+                  batch_size=None) -> PowerSpectrum:
+        """Coherence C_cross / sqrt(C_self C_other) (reference fields/lightcone.py:790-838)."""
+        return _cl_coherence(self, other, lmax=lmax, method=method)
 
     def cross_angular_cl(self, *, lmax: int | None = None, method: str = "healpy", batch_size=None) -> PowerSpectrum:
         """All auto and cross C_ell of the batched maps, healpy's alm2cl order (reference
@@ -499,6 +593,16 @@ class FlatDensity(AbstractField):
         ell, cl = angular_cl_flat(data1, data2, pixel_size=pixel_size, field_size=field_size or self.field_size,
                                   ell_edges=ell_edges)
         return PowerSpectrum(wavenumber=ell, array=cl, name="cl", scale_factors=self.scale_factors)
+
+    def transfer(self, other: "FlatDensity", *, field_size=None, pixel_size=None, ell_edges=None,
+                 batch_size=None) -> PowerSpectrum:
+        """Angular transfer function sqrt(C_other / C_self) (reference fields/lightcone.py:318-365)."""
+        return _cl_transfer(self, other, field_size=field_size, pixel_size=pixel_size, ell_edges=ell_edges)
+
+    def coherence(self, other: "FlatDensity", *, field_size=None, pixel_size=None, ell_edges=None,
+                  batch_size=None) -> PowerSpectrum:
+        """Angular coherence C_cross / sqrt(C_self C_other) (reference fields/lightcone.py:367-421)."""
+        return _cl_coherence(self, other, field_size=field_size, pixel_size=pixel_size, ell_edges=ell_edges)
 
 
 @dataclasses.dataclass(frozen=True, eq=False)

@@ -2,6 +2,8 @@
 to_metadata and iteration of the reference's field pytrees (_src/base/_core.py:25-171,
 fields/*.py full_like), on CPU tensors."""
 
+import importlib
+
 import numpy as np
 import pytest
 import torch
@@ -78,3 +80,80 @@ def test_full_like_and_metadata():
     assert not m.is_batched() and not m.is_multi_batched()
     with pytest.raises(NotImplementedError):
         jf.FieldMetadata.full_like(base)
+
+
+# ---------------------------------------------- spectral comparisons, with the spectra faked
+def _fake_power(mesh, mesh2=None, *, box_shape, kedges=None, multipoles=0, los=(0.0, 0.0, 1.0)):
+    """Stands in for the GPU P(k): one 'bin' per value of a 3-vector, <m1 m2> times (1, 2, 3)."""
+    m2 = mesh if mesh2 is None else mesh2
+    v = float((mesh.double() * m2.double()).mean())
+    return torch.tensor([0.1, 0.2, 0.3]), torch.tensor([v, 2 * v, 3 * v])
+
+
+def test_density_cross_power_transfer_coherence(monkeypatch):
+    pw = importlib.import_module("jfli_b200.power")  # the package's `power` attribute is the function
+
+    monkeypatch.setattr(pw, "power", _fake_power)
+    rng = np.random.default_rng(1)
+    a = torch.as_tensor(rng.uniform(1, 2, (3, *MESH)))
+    f = _density(a, scale_factors=np.array([0.5, 0.7, 0.9]))
+    cp = f.cross_power()
+    assert cp.name == "cross_pk" and tuple(cp.array.shape) == (6, 3)
+    order = [(i, j) for i in range(3) for j in range(i, 3)]
+    for row, (i, j) in zip(cp.array, order):
+        assert float(row[0]) == pytest.approx(float((a[i] * a[j]).mean()))
+    with pytest.raises(ValueError, match="batched"):
+        f[0].cross_power()
+    with pytest.raises(ValueError, match="at least 2"):
+        _density(a[:1]).cross_power()
+
+    g = f * 2.0
+    tr = f.transfer(g)
+    assert tr.name == "transfer" and tuple(tr.array.shape) == (3, 3)
+    np.testing.assert_allclose(tr.array.numpy(), 2.0, rtol=1e-12)  # sqrt(P(2a) / P(a))
+    co = f[0].coherence(g[0])
+    assert tuple(co.array.shape) == (3,)
+    np.testing.assert_allclose(co.array.numpy(), 1.0, rtol=1e-6)  # P01 / sqrt(P0 P1) of a and 2a
+    with pytest.raises(ValueError, match="match shape"):
+        f.transfer(g[0])
+
+
+def test_map_transfer_and_coherence(monkeypatch):
+    pw = importlib.import_module("jfli_b200.power")  # the package's `power` attribute is the function
+
+    def fake_flat(m1, m2=None, *, pixel_size=None, field_size=None, ell_edges=None):
+        m2 = m1 if m2 is None else m2
+        v = (m1.double() * m2.double()).mean(dim=(-2, -1))
+        return torch.tensor([10.0, 20.0]), torch.stack([v, 4 * v], -1)
+
+    def fake_sph(m1, m2=None, *, lmax=None, method="jax"):
+        m2 = m1 if m2 is None else m2
+        v = float((m1.double() * m2.double()).mean())
+        return np.arange(3), np.array([v, v, v])
+
+    monkeypatch.setattr(pw, "angular_cl_flat", fake_flat)
+    monkeypatch.setattr(pw, "angular_cl_spherical", fake_sph)
+    rng = np.random.default_rng(2)
+    fl = jf.FlatDensity(array=torch.as_tensor(rng.uniform(1, 2, (2, 5, 7))), flatsky_npix=(5, 7),
+                        field_size=(1.0, 1.0), **META)
+    tr = fl.transfer(fl * 3.0)
+    np.testing.assert_allclose(tr.array.numpy(), 3.0, rtol=1e-12)
+    co = fl.coherence(fl * 3.0)
+    np.testing.assert_allclose(co.array.numpy(), 1.0, rtol=1e-12)
+    sp = jf.SphericalDensity(array=torch.as_tensor(rng.uniform(1, 2, 192)), nside=4, **META)
+    np.testing.assert_allclose(sp.transfer(sp * 4.0).array, 4.0, rtol=1e-12)
+    np.testing.assert_allclose(sp.coherence(-sp).array, -1.0, rtol=1e-12)
+
+
+def test_project():
+    rng = np.random.default_rng(3)
+    a = torch.as_tensor(rng.standard_normal((2, *MESH)).astype(np.float32))
+    f = _density(a)
+    p = f[0].project(nz_slices=3)
+    assert isinstance(p, jf.FlatDensity) and p.status == jf.FieldStatus.PROJECTED_DENSITY
+    assert p.flatsky_npix == (4, 6) and p.box_size == f.box_size
+    assert torch.allclose(p.array, a[0, :, :, -3:].sum(-1))
+    pb = f.project()
+    assert tuple(pb.array.shape) == (2, 4, 6) and torch.allclose(pb.array, a.sum(-1))
+    with pytest.raises(ValueError):
+        _density(torch.zeros(2, 2, *MESH)).project()
