@@ -42,6 +42,31 @@ def paint_shells(field, centers, widths, scheme="bilinear", weights=None, out=No
     return out
 
 
+def check_grade_orders(order_in: str, order_out: str) -> None:
+    """ud_grade orders a painter accepts: RING in (the painters write RING maps), RING or
+    NESTED out."""
+    from .healpix_order import _order
+
+    if _order(order_in) != "RING":
+        raise NotImplementedError("painted maps are RING ordered: ud_grade_order_in must be 'RING'")
+    _order(order_out)
+
+
+def regrade(maps: torch.Tensor, nside: int, paint_nside, *, power: float = 0.0, order_in: str = "RING",
+            order_out: str = "RING", pess: bool = False) -> torch.Tensor:
+    """Painted RING maps (..., 12 paint_nside^2) brought to the field's nside with healpy's
+    ud_grade (PaintingOptions.paint_nside and ud_grade_* options, reference
+    fields/painting.py:78-96); unchanged when paint_nside is unset or equal to nside. The
+    painters write RING maps, so order_in must be RING; order_out may be NESTED."""
+    from .healpix_order import ud_grade
+
+    check_grade_orders(order_in, order_out)
+    if paint_nside is None or int(paint_nside) == int(nside):
+        return maps
+    return ud_grade(maps, int(nside), pess=bool(pess), order_in="RING", order_out=order_out,
+                    power=float(power) if power else None)
+
+
 def paint_shell_tiled(field, vel, center: float, width: float, rotations, shifts, *, telephoto: bool = False,
                       t: float | None = None, cosmo=None, scheme: str = "bilinear", weights=None) -> torch.Tensor:
     """(12 nside^2,) map of one shell painted from rotated and shifted replicas of the

@@ -155,6 +155,20 @@ def tile_shifts(observer_position, box_size) -> np.ndarray:
     return sh * np.asarray(box_size, dtype=np.float64)
 
 
+def _at_paint_nside(dx, painting):
+    """The particles to paint, at PaintingOptions.paint_nside when it is given."""
+    return dx if painting.paint_nside is None else dx.replace(nside=int(painting.paint_nside))
+
+
+def _regrade(m, dx, painting):
+    """A map painted at paint_nside brought to the particles' nside (healpy's ud_grade)."""
+    from ..painting import regrade
+
+    return regrade(m, dx.nside, painting.paint_nside, power=painting.ud_grade_power,
+                   order_in=painting.ud_grade_order_in, order_out=painting.ud_grade_order_out,
+                   pess=painting.ud_grade_pess)
+
+
 def _spherical_result(res, t, r_center, width):
     from ..fields import DensityUnit, FieldStatus
 
@@ -208,10 +222,10 @@ class OnionTiler(AbstractInterp):
             from ..painting import paint_shell_tiled
 
             shifts = tile_shifts(dx.observer_position, dx.box_size)
-            m = paint_shell_tiled(dx, p.array if self.drift_on_lightcone else None, r_center, width, state.rotations,
-                                  shifts, telephoto=False, t=float(t), cosmo=cosmo, scheme=pt.scheme,
-                                  weights=pt.weights)
-            res = SphericalDensity.FromDensityMetadata(array=m, field=dx)
+            m = paint_shell_tiled(_at_paint_nside(dx, pt), p.array if self.drift_on_lightcone else None, r_center,
+                                  width, state.rotations, shifts, telephoto=False, t=float(t), cosmo=cosmo,
+                                  scheme=pt.scheme, weights=pt.weights)
+            res = SphericalDensity.FromDensityMetadata(array=_regrade(m, dx, pt), field=dx)
         return _spherical_result(res, t, r_center, width)
 
 
@@ -281,7 +295,8 @@ class TelephotoInterp(AbstractInterp):
                 res = dx.replace(array=pos, unit=PositionUnit.MPC_H).paint_2d(
                     center=r_center, density_plane_width=width, weights=pt.weights, batch_size=pt.batch_size)
                 return res.replace(scale_factors=t, comoving_centers=r_center, density_width=width)
-            m = paint_shell_tiled(dx, p.array if self.drift_on_lightcone else None, r_center, width, rot, shift,
-                                  telephoto=True, t=float(t), cosmo=cosmo, scheme=pt.scheme, weights=pt.weights)
-            res = SphericalDensity.FromDensityMetadata(array=m, field=dx)
+            m = paint_shell_tiled(_at_paint_nside(dx, pt), p.array if self.drift_on_lightcone else None, r_center,
+                                  width, rot, shift, telephoto=True, t=float(t), cosmo=cosmo, scheme=pt.scheme,
+                                  weights=pt.weights)
+            res = SphericalDensity.FromDensityMetadata(array=_regrade(m, dx, pt), field=dx)
         return res.replace(scale_factors=t, comoving_centers=r_center, density_width=width)

@@ -83,6 +83,37 @@ def pix2ang(nside, pix):
     return theta[r], phi
 
 
+UNSEEN = -1.6375e30
+
+
+def ring_parents(nside_in, nside_out):
+    """For every RING pixel at nside_in, the RING pixel at nside_out < nside_in that holds its
+    centre: the pixel hierarchy from the geometry alone, with no NESTED numbering."""
+    theta, phi = pix2ang(nside_in, np.arange(nside2npix(nside_in)))
+    return ang2pix(nside_out, theta, phi)
+
+
+def ud_grade_ring(m, nside_out, pess=False, power=None):
+    """healpy.ud_grade of one RING map (healpy's documented rules: averages of the children
+    that are not UNSEEN, UNSEEN where none is (or any, with pess), power p scaling by
+    (nside_out / nside_in)^p, copies when upgrading), built on ring_parents."""
+    m = np.asarray(m, np.float64)
+    nside_in = int(round(np.sqrt(m.size / 12)))
+    ratio = (nside_out / nside_in) ** power if power else 1.0
+    if nside_out == nside_in:
+        return m.copy()
+    if nside_out > nside_in:
+        return m[ring_parents(nside_out, nside_in)] * ratio
+    par = ring_parents(nside_in, nside_out)
+    k = (nside_in // nside_out) ** 2
+    good = ~((np.abs(m - UNSEEN) <= 1e-8 + 1e-5 * abs(UNSEEN)) | ~np.isfinite(m))
+    npix_out = nside2npix(nside_out)
+    total = np.bincount(par, weights=m * good, minlength=npix_out)
+    nhit = np.bincount(par, weights=good.astype(np.float64), minlength=npix_out)
+    out = np.where(nhit > 0, total / np.where(nhit > 0, nhit, 1.0) * ratio, total)
+    return np.where((nhit < k) if pess else (nhit == 0), UNSEEN, out)
+
+
 def get_interp_weights(nside, theta, phi):
     """(pix (4, N), weights (4, N)) bilinear interpolation on the RING grid."""
     theta = np.atleast_1d(np.asarray(theta, np.float64))
