@@ -20,7 +20,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
-from typing import Any
+from typing import Any, Literal
 
 import numpy as np
 import torch
@@ -228,6 +228,9 @@ def _stack(snapshots):
         meta[key] = None if any(v is None for v in vals) else np.asarray([float(np.asarray(v).reshape(-1)[0])
                                                                          for v in vals])
     return first.replace(array=arr, **meta)
+
+
+AdjointType = Literal["reverse", "checkpointed"]  # the adjoint modes of integrate (reference pm/integrate.py:14)
 
 
 def integrate(displacements, velocities, cosmo, ts, solver, t0, t1, dt0, adjoint="checkpointed", checkpoints=None,
