@@ -359,6 +359,22 @@ def _stack(rows):
     return torch.stack(rows) if isinstance(rows[0], torch.Tensor) else np.stack(rows)
 
 
+def _linear_resize_weights(n_in: int, n_out: int) -> np.ndarray:
+    """(n_in, n_out) weights of jax.image.resize's "bilinear" method along one axis (its
+    scale_and_translate with a triangle kernel, antialiased, no translation): output pixel j
+    samples the input at (j + 0.5) n_in / n_out - 0.5; the kernel is widened by n_in / n_out
+    when downsampling; weights are normalised per output pixel (zero when their sum is
+    negligible) and zero for samples outside [-0.5, n_in - 0.5]."""
+    inv = n_in / n_out
+    width = max(inv, 1.0)
+    sample = (np.arange(n_out, dtype=np.float64) + 0.5) * inv - 0.5
+    w = np.maximum(0.0, 1.0 - np.abs(sample[None, :] - np.arange(n_in, dtype=np.float64)[:, None]) / width)
+    total = w.sum(axis=0, keepdims=True)
+    w = np.where(np.abs(total) > 1000.0 * float(np.finfo(np.float32).eps), w / np.where(total != 0, total, 1.0), 0.0)
+    inside = (sample >= -0.5) & (sample <= n_in - 0.5)
+    return np.where(inside[None, :], w, 0.0)
+
+
 def _cl_transfer(field, other, **kw) -> "PowerSpectrum":
     """sqrt(C_other / C_self) of two map fields (reference fields/lightcone.py:318-365,746-788)."""
     cl_self = field.angular_cl(**kw)
@@ -593,6 +609,22 @@ class FlatDensity(AbstractField):
         ell, cl = angular_cl_flat(data1, data2, pixel_size=pixel_size, field_size=field_size or self.field_size,
                                   ell_edges=ell_edges)
         return PowerSpectrum(wavenumber=ell, array=cl, name="cl", scale_factors=self.scale_factors)
+
+    def ud_sample(self, new_npix: int) -> "FlatDensity":
+        """The maps resampled to (new_npix, new_npix) with jax.image.resize's bilinear rule
+        (reference fields/lightcone.py:184-195)."""
+        a = self.array
+        if a.ndim not in (2, 3):
+            raise ValueError("ud_sample expects maps of shape (ny, nx) or (B, ny, nx)")
+        w0 = _linear_resize_weights(int(a.shape[-2]), int(new_npix))
+        w1 = _linear_resize_weights(int(a.shape[-1]), int(new_npix))
+        if isinstance(a, torch.Tensor):
+            t0 = torch.as_tensor(w0, dtype=a.dtype, device=a.device)
+            t1 = torch.as_tensor(w1, dtype=a.dtype, device=a.device)
+            out = torch.einsum("...ij,ik,jl->...kl", a, t0, t1)
+        else:
+            out = np.einsum("...ij,ik,jl->...kl", a, w0.astype(a.dtype), w1.astype(a.dtype))
+        return self.replace(array=out, flatsky_npix=(int(new_npix), int(new_npix)))
 
     def transfer(self, other: "FlatDensity", *, field_size=None, pixel_size=None, ell_edges=None,
                  batch_size=None) -> PowerSpectrum:

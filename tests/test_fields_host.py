@@ -157,3 +157,45 @@ def test_project():
     assert tuple(pb.array.shape) == (2, 4, 6) and torch.allclose(pb.array, a.sum(-1))
     with pytest.raises(ValueError):
         _density(torch.zeros(2, 2, *MESH)).project()
+
+
+def _resize_loop(a, n_out):
+    """jax.image.resize 'bilinear' along both axes, restated with explicit loops."""
+    def axis_w(n_in):
+        scale = n_out / n_in
+        width = max(1.0 / scale, 1.0)
+        W = np.zeros((n_in, n_out))
+        for j in range(n_out):
+            s = (j + 0.5) / scale - 0.5
+            col = [max(0.0, 1.0 - abs(s - i) / width) for i in range(n_in)]
+            tot = sum(col)
+            if abs(tot) > 1000 * np.finfo(np.float32).eps and -0.5 <= s <= n_in - 0.5:
+                W[:, j] = np.array(col) / tot
+        return W
+
+    return axis_w(a.shape[0]).T @ a @ axis_w(a.shape[1])
+
+
+@pytest.mark.parametrize("n_in,n_out", [(8, 16), (16, 8), (12, 5), (6, 6)])
+def test_flat_ud_sample(n_in, n_out):
+    rng = np.random.default_rng(n_in + n_out)
+    a = rng.standard_normal((2, n_in, n_in))
+    fl = jf.FlatDensity(array=torch.as_tensor(a), flatsky_npix=(n_in, n_in), **META)
+    out = fl.ud_sample(n_out)
+    assert out.flatsky_npix == (n_out, n_out) and tuple(out.array.shape) == (2, n_out, n_out)
+    for b in range(2):
+        np.testing.assert_allclose(out.array[b].numpy(), _resize_loop(a[b], n_out), rtol=1e-12, atol=1e-12)
+    one = jf.FlatDensity(array=torch.ones(n_in, n_in, dtype=torch.float64), flatsky_npix=(n_in, n_in), **META)
+    np.testing.assert_allclose(one.ud_sample(n_out).array.numpy(), 1.0, rtol=1e-12)
+    if n_in == n_out:
+        np.testing.assert_allclose(out.array.numpy(), a, rtol=1e-12)
+
+
+def test_flat_ud_sample_linear_ramp():
+    ramp = np.tile(np.arange(16, dtype=np.float64)[:, None], (1, 16))
+    fl = jf.FlatDensity(array=torch.as_tensor(ramp), flatsky_npix=(16, 16), **META)
+    up = fl.ud_sample(32).array.numpy()
+    j = np.arange(32)
+    np.testing.assert_allclose(up[2:-2, 5], (j / 2 - 0.25)[2:-2], rtol=1e-12)  # interpolation at j/2 - 1/4
+    down = fl.ud_sample(8).array.numpy()
+    np.testing.assert_allclose(down[1:-1, 3], (2 * np.arange(8) + 0.5)[1:-1], rtol=1e-12)  # antialiased mean
