@@ -303,7 +303,11 @@ class AbstractField:
             if type(f) is not type(first):
                 raise ValueError(f"cannot {how} fields of types {type(first).__name__} and {type(f).__name__}")
             for name in static:
-                if getattr(f, name) != getattr(first, name):
+                a, b = getattr(f, name), getattr(first, name)
+                same = (np.array_equal(np.asarray(a), np.asarray(b))
+                        if isinstance(a, (np.ndarray, tuple, list)) or isinstance(b, (np.ndarray, tuple, list))
+                        else a == b)
+                if not same:
                     raise ValueError(f"cannot {how} fields whose {name} differ")
         arrays = [f.array for f in fields]
         if isinstance(arrays[0], torch.Tensor):
