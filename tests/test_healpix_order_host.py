@@ -108,3 +108,20 @@ def test_paint_spherical_at_paint_nside(monkeypatch):
         parts.paint_spherical(3.0, 1.0, paint_nside=16, ud_grade_order_in="NESTED")
     with pytest.raises(ValueError):
         parts.paint_spherical(3.0, 1.0, paint_nside=16, ud_grade_order_out="SPIRAL")
+
+
+def test_tiled_interp_paint_nside_helpers():
+    """OnionTiler / TelephotoInterp paint replicas at paint_nside and grade to the field's nside."""
+    from jfli_b200.pm import interp
+
+    parts = jf.ParticleField(array=torch.zeros(4, 4, 4, 3), mesh_size=(4, 4, 4), box_size=(10.0, 10.0, 10.0),
+                             nside=4, unit=jf.PositionUnit.GRID_RELATIVE, status=jf.FieldStatus.PARTICLES)
+    plain = jf.PaintingOptions(target="spherical")
+    fine = jf.PaintingOptions(target="spherical", paint_nside=16, ud_grade_power=-2.0, ud_grade_order_out="NESTED")
+    assert interp._at_paint_nside(parts, plain) is parts
+    assert interp._at_paint_nside(parts, fine).nside == 16
+    m = torch.arange(12 * 256, dtype=torch.float64)
+    assert interp._regrade(m[:192], parts, plain) is not None
+    graded = interp._regrade(m, parts, fine)
+    ref = oh.ud_grade_ring(m.numpy(), 4, power=-2.0)
+    np.testing.assert_allclose(graded.numpy(), ref[ho._nest2ring_table(4)], rtol=1e-12)  # NESTED out
