@@ -280,6 +280,12 @@ class AbstractField:
         """The metadata alone, as a FieldMetadata with no array (reference _src/base/_core.py:478-496)."""
         return FieldMetadata(array=None, **self._meta())
 
+    @classmethod
+    def full_like(cls, field: "AbstractField", fill_value: float = 0.0):
+        """A field of this class with field's metadata, filled with fill_value; each concrete
+        class gives its own array shape (reference _src/base/_core.py:339-355)."""
+        raise NotImplementedError("full_like must be implemented in subclasses.")
+
     @staticmethod
     def _full(shape, fill_value, like):
         a = getattr(like, "array", None)
@@ -544,6 +550,13 @@ class SphericalDensity(AbstractField):
         arr = np.stack(spectra) if d1.ndim == 2 else spectra[0]
         return PowerSpectrum(wavenumber=ell, array=arr, name="cl", scale_factors=self.scale_factors)
 
+    def ud_sample(self, new_nside: int) -> "SphericalDensity":
+        """The RING maps at new_nside with healpy's ud_grade (reference fields/lightcone.py:625-630)."""
+        from .healpix_order import ud_grade
+
+        a = self.array if isinstance(self.array, torch.Tensor) else torch.as_tensor(np.asarray(self.array))
+        return self.replace(array=ud_grade(a, int(new_nside)), nside=int(new_nside))
+
     def transfer(self, other: "SphericalDensity", *, lmax: int | None = None, method: str = "jax",
                  batch_size=None) -> PowerSpectrum:
         """Transfer function sqrt(C_other / C_self) (reference fields/lightcone.py:746-788)."""
@@ -613,6 +626,29 @@ class FlatDensity(AbstractField):
         ell, cl = angular_cl_flat(data1, data2, pixel_size=pixel_size, field_size=field_size or self.field_size,
                                   ell_edges=ell_edges)
         return PowerSpectrum(wavenumber=ell, array=cl, name="cl", scale_factors=self.scale_factors)
+
+    def cross_angular_cl(self, *, field_size=None, pixel_size=None, ell_edges=None, batch_size=None) -> PowerSpectrum:
+        """Flat-sky C_ell of every pair (i, j), i <= j, of B maps in upper-triangular order
+        (0,0), (0,1), ..., (0,B-1), (1,1), ...: array (B(B+1)/2, nbins) (reference
+        fields/lightcone.py:236-316)."""
+        from .power import angular_cl_flat
+
+        data = self.array
+        if data.ndim != 3:
+            raise ValueError(f"cross_angular_cl requires batched array with shape (B, ny, nx), got array with "
+                             f"{data.ndim} dimensions. Use angular_cl() for single maps.")
+        if data.shape[0] < 2:
+            raise ValueError(f"cross_angular_cl requires at least 2 maps in batch dimension, got {data.shape[0]}. "
+                             f"Use angular_cl() for single maps.")
+        fs = field_size or self.field_size
+        ell, spectra = None, []
+        for i in range(data.shape[0]):
+            for j in range(i, data.shape[0]):
+                ell_ij, cl = angular_cl_flat(data[i], data[j], pixel_size=pixel_size, field_size=fs,
+                                             ell_edges=ell_edges)
+                ell = ell_ij if ell is None else ell
+                spectra.append(cl)
+        return PowerSpectrum(wavenumber=ell, array=_stack(spectra), name="cross_cl", scale_factors=self.scale_factors)
 
     def ud_sample(self, new_npix: int) -> "FlatDensity":
         """The maps resampled to (new_npix, new_npix) with jax.image.resize's bilinear rule

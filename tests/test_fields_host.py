@@ -199,3 +199,36 @@ def test_flat_ud_sample_linear_ramp():
     np.testing.assert_allclose(up[2:-2, 5], (j / 2 - 0.25)[2:-2], rtol=1e-12)  # interpolation at j/2 - 1/4
     down = fl.ud_sample(8).array.numpy()
     np.testing.assert_allclose(down[1:-1, 3], (2 * np.arange(8) + 0.5)[1:-1], rtol=1e-12)  # antialiased mean
+
+
+def test_flat_cross_angular_cl_pairs(monkeypatch):
+    pw = importlib.import_module("jfli_b200.power")
+
+    def fake_flat(m1, m2=None, *, pixel_size=None, field_size=None, ell_edges=None):
+        m2 = m1 if m2 is None else m2
+        return torch.tensor([10.0, 20.0]), torch.stack([(m1 * m2).mean(), 2 * (m1 * m2).mean()])
+
+    monkeypatch.setattr(pw, "angular_cl_flat", fake_flat)
+    rng = np.random.default_rng(4)
+    a = torch.as_tensor(rng.uniform(1, 2, (3, 5, 7)))
+    fl = jf.FlatDensity(array=a, flatsky_npix=(5, 7), field_size=(1.0, 1.0), **META)
+    cc = fl.cross_angular_cl()
+    assert cc.name == "cross_cl" and tuple(cc.array.shape) == (6, 2)
+    for row, (i, j) in zip(cc.array, [(i, j) for i in range(3) for j in range(i, 3)]):
+        assert float(row[0]) == pytest.approx(float((a[i] * a[j]).mean()))
+    with pytest.raises(ValueError, match="batched"):
+        fl[0].cross_angular_cl()
+
+
+def test_spherical_ud_sample_and_base_full_like():
+    from oracle import healpix as oh
+
+    rng = np.random.default_rng(7)
+    m = rng.uniform(size=(2, 12 * 64))
+    sp = jf.SphericalDensity(array=torch.as_tensor(m), nside=8, **META)
+    down = sp.ud_sample(2)
+    assert down.nside == 2 and tuple(down.array.shape) == (2, 48)
+    np.testing.assert_allclose(down.array[1].numpy(), oh.ud_grade_ring(m[1], 2), rtol=1e-12)
+    assert sp.ud_sample(16).nside == 16
+    with pytest.raises(NotImplementedError):
+        jf.AbstractField.full_like(sp)
