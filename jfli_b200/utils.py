@@ -63,8 +63,9 @@ def distances(centers, r_left=None):
     return e[1] - e[0]
 
 
-def centers(distances_, r_left, is_descending=False):
-    d = np.asarray(distances_, dtype=np.float64)
+def centers(distances, r_left, is_descending=False):
+    """Shell centres from shell widths laid out from r_left (reference utils.py:297-312)."""
+    d = np.asarray(distances, dtype=np.float64)
     da = d[::-1] if is_descending else d
     r_edges = np.concatenate([[r_left], r_left + np.cumsum(da)])
     c = 0.5 * (r_edges[1:] + r_edges[:-1])
