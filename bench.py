@@ -17,7 +17,8 @@ schedule restarts from the initial conditions inside the timed region.
           48 B/particle (read+write position and velocity) + 20 B/cell (float4 force mesh
           read, density written) per launch, over its CUDA-event time, against
           MEASURED_PEAKS.json
-  cpu_baseline : the NumPy/SciPy FP32 port of the same step (oracle/pm.py) on this host
+  cpu_baseline : the FP32 oracle port of the same steps (oracle/pm.py with the C/OpenMP
+          CIC of oracle/cic.c) on this host, a bounded sample of the schedule
   serving : the request stream (512 Poisson arrivals over mesh 64/96/128/192, 10-40 KDK
           steps, mixed cosmologies) through the continuous-batching engine
           (jfli_b200.serving) and through the plain per-call path at the same offered
@@ -28,7 +29,8 @@ schedule restarts from the initial conditions inside the timed region.
 
 --gpus N runs N independent replicas (one per GPU, no collective on the data path);
 value is the sum over ranks / the max-over-ranks time. --impl reference times the CPU
-port of the reference algorithm (JAX and the JaxPM fork are not installable here).
+port of the reference algorithm on the same 256^3 workload and schedule (JAX and the JaxPM
+fork are not installable here).
 """
 
 from __future__ import annotations
@@ -196,17 +198,17 @@ def run_gpu(args, world, rank):
         v.copy_(v0)
         rho.zero_()
         ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT, rho)
-        ops.poisson_force(rho, 1.0, out=force, pot=pot)
+        ops.poisson_force(rho, 1.0, out=force, pot=pot, clear=True)
         st["idx"], st["pending"] = 0, init_kick
 
     restart()
 
     def one_step(timed_kdp=None):
         """Step idx of the schedule: kick (previous force) + drift + paint, then the new
-        force meshes; after the last step of the schedule the next call restarts from
-        the initial conditions (the restart is inside the timed region)."""
+        force meshes (the forward FFT clears the density mesh for the next paint); after
+        the last step of the schedule the next call restarts from the initial conditions
+        (the restart is inside the timed region)."""
         c = coeffs[st["idx"]]
-        rho.zero_()
         if timed_kdp is not None:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -216,7 +218,7 @@ def run_gpu(args, world, rank):
             timed_kdp.append((e0, e1))
         else:
             ops.kick_drift_paint(x, v, force, st["pending"], c.drift, flags, rho)
-        ops.poisson_force(rho, 1.0, out=force, pot=pot)
+        ops.poisson_force(rho, 1.0, out=force, pot=pot, clear=True)
         st["pending"] = c.kick
         st["idx"] += 1
         if st["idx"] == len(coeffs):
@@ -295,7 +297,7 @@ def run_e2e(args, cosmo, n, box):
 
     import jfli_b200 as jf
 
-    noise = torch.from_numpy(jf.white_noise(1, (n, n, n))).pin_memory()
+    noise = torch.from_numpy(jf.white_noise(0, (n, n, n))).pin_memory()
     kedges = np.geomspace(2 * np.pi / box * (1 - 1e-6), np.pi * n / box, 33)
     solver = jf.EfficientDriftDoubleKick(interp_kernel=jf.NoInterp(painting=jf.PaintingOptions(target="density")))
     out_rho = torch.empty(n, n, n, dtype=torch.float32).pin_memory()
@@ -328,9 +330,28 @@ def run_e2e(args, cosmo, n, box):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     val = n**3 * steps * args.e2e_requests / (ms / 1e3) / 1e6
-    return {"value": round(val, 2), "unit": "Mpart-steps/s", "h2d_bytes_per_step": n**3 * 4,
-            "d2h_bytes_per_step": n**3 * 4 + 32 * 8, "per": "request (ICs + 2LPT + %d KDK steps + P(k))" % steps,
-            "ms_per_request": round(ms / args.e2e_requests, 2)}
+    h2d, d2h = noise.numel() * 4, out_rho.numel() * 4 + pk.numel() * pk.element_size()
+    out = {"value": round(val, 2), "unit": "Mpart-steps/s", "h2d_bytes_per_step": round(h2d / steps),
+           "d2h_bytes_per_step": round(d2h / steps), "h2d_bytes_per_request": h2d, "d2h_bytes_per_request": d2h,
+           "per": "request (ICs + 2LPT + %d KDK steps + P(k)); one noise upload and one density + P(k) download "
+                  "per request, bytes per step = per request / steps" % steps,
+           "ms_per_request": round(ms / args.e2e_requests, 2)}
+    out.update(pk_vs_oracle(pk.numpy(), n, box))
+    return out
+
+
+def pk_vs_oracle(pk, n, box):
+    """Largest per-bin relative error of the request's P(k) against the committed FP64 and
+    FP32 oracle runs of the same configuration (tests/golden/config2_256.npz, written by
+    tests/golden/make_config2.py), with the oracle's own FP32-vs-FP64 gap beside it."""
+    path = os.path.join(ROOT, "tests", "golden", "config2_256.npz")
+    if n != N_MESH or box != BOX or not os.path.exists(path):
+        return {}
+    ref = np.load(path)
+    p = np.asarray(pk, np.float64)
+    return {"pk_err_vs_fp64_oracle": float(np.abs(p / ref["pk_f64"] - 1).max()),
+            "pk_err_vs_fp32_oracle": float(np.abs(p / ref["pk_f32"] - 1).max()),
+            "pk_gap_fp32_vs_fp64_oracle": float(ref["gap_pk_f32"])}
 
 
 def run_shells(args, cosmo, n, box):
@@ -377,7 +398,8 @@ def run_shells(args, cosmo, n, box):
     ms = e0.elapsed_time(e1)
     return {"value": round(n**3 * steps * reps / (ms / 1e3) / 1e6, 2), "unit": "Mpart-steps/s",
             "steps_per_request": steps, "ms_per_request": round(ms / reps, 2),
-            "h2d_bytes_per_step": n**3 * 4, "d2h_bytes_per_step": int(out.numel()) * 4,
+            "h2d_bytes_per_step": round(n**3 * 4 / steps), "d2h_bytes_per_step": round(int(out.numel()) * 4 / steps),
+            "h2d_bytes_per_request": n**3 * 4, "d2h_bytes_per_request": int(out.numel()) * 4,
             "shell_sums": [round(float(v), 1) for v in out.double().sum(dim=1)],
             "per": "request: ICs + 2LPT + KDK to the nearest shell's time, 4 shells nside 256 painted en route"}
 
@@ -517,19 +539,67 @@ def dataclasses_replace(obj, **kw):
 
 
 # ----------------------------------------------------------------------------- CPU arm
-def cpu_step_rate(n, nsteps=1):
-    """Mpart-steps/s of the FP32 NumPy/SciPy port (oracle/pm.py), all host threads."""
-    from oracle import pm as opm
+class CpuKdk:
+    """The bench workload on the host cores with the FP32 oracle (oracle/pm.py: CIC paint
+    and readout in the OpenMP restatement oracle/cic.c, scipy.fft with all workers): the
+    same seeded white noise, 2LPT to a = 0.1 and the 40-step EfficientDriftDoubleKick
+    schedule (dt0 = 0.9/40) with the same FP64 factors as the GPU arm. A step is one drift,
+    one force evaluation (paint, 4 complex FFTs, 3 readouts) and one kick; past the end of
+    the schedule the run restarts from the 2LPT state, as the GPU arm does."""
 
-    rng = np.random.default_rng(0)
-    x = (2.0 * rng.standard_normal((n, n, n, 3))).astype(np.float32)
-    v = (0.5 * rng.standard_normal((n, n, n, 3))).astype(np.float32)
-    t0 = time.perf_counter()
-    for _ in range(nsteps):
-        v += opm.pm_forces(x, np.float32) * np.float32(0.3)
-        x += v * np.float32(0.02)
-    dt = time.perf_counter() - t0
-    return n**3 * nsteps / dt / 1e6, dt
+    def __init__(self, n):
+        from oracle import pm as opm
+
+        import jfli_b200 as jf
+        from jfli_b200 import cosmology as cj
+        from jfli_b200.pm.integrate import time_events
+        from jfli_b200.pm.lpt import lpt_coefficients
+        from jfli_b200.pm.solvers import EfficientDriftDoubleKick as EDK
+
+        self.opm, self.n = opm, n
+        box = BOX * n / N_MESH
+        cosmo = jf.Planck18()
+        k, pk = cj.pk_table(cosmo, 128)
+        t0 = time.perf_counter()
+        ic = opm.ic_filter(jf.white_noise(0, (n, n, n)).astype(np.float64), (box,) * 3, k, pk)
+        self.x0, self.v0 = opm.lpt(ic.astype(np.float32), *lpt_coefficients(cosmo, 0.1), order=2, dtype=np.float32)
+        dt0 = 0.9 / E2E_STEPS
+        sched = [(e[1], e[2]) for e in time_events(0.1, [1.0], dt0) if e[0] == "step"]
+        kicks, drifts = EDK.schedule_arrays(cosmo, [a for a, _ in sched], [b for _, b in sched], dt0)
+        self.sched = [(np.float32(kk), np.float32(d)) for kk, d in zip(kicks, drifts)]
+        self.init_kick = np.float32(EDK.init_kick(cosmo, 0.1, 0.1 + dt0))
+        self.restart()
+        self.setup_s = time.perf_counter() - t0
+
+    def restart(self):
+        self.x = self.x0.copy()
+        self.v = self.v0 + self.opm.pm_forces(self.x, np.float32) * self.init_kick
+        self.idx = 0
+
+    def step(self):
+        kick, drift = self.sched[self.idx]
+        self.x += self.v * drift
+        self.v += self.opm.pm_forces(self.x, np.float32) * kick
+        self.idx += 1
+        if self.idx == len(self.sched):
+            self.restart()
+
+    def rate(self, warmup, steps):
+        """(Mpart-steps/s, seconds) over `steps` steps after `warmup` untimed ones."""
+        for _ in range(warmup):
+            self.step()
+        self.restart()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            self.step()
+        dt = time.perf_counter() - t0
+        return self.n**3 * steps / dt / 1e6, dt
+
+
+def cpu_threads():
+    from oracle import clib
+
+    return clib.threads()
 
 
 def fft_vs_cufft(n, iters=20):
@@ -579,37 +649,40 @@ def fft_vs_cufft(n, iters=20):
 
 
 def cpu_baseline_block(n):
-    """The FP32 NumPy/SciPy port on this host: one KDK step at n^3 (the workload itself,
-    ~20-40 s of CPU work at 256^3) and, for reference, five steps at 64^3."""
-    rate, dt = cpu_step_rate(n, 1)
-    rate64, dt64 = cpu_step_rate(64, 5)
-    return {"value": round(rate, 4), "unit": "Mpart-steps/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"1 KDK step (paint, 4 complex FFTs, 3 readouts) at {n}^3, FP32 NumPy/SciPy, scipy.fft "
-                      f"workers=all; {dt:.1f} s",
-            "at_64": {"value": round(rate64, 4), "sample": f"5 KDK steps at 64^3, {dt64:.1f} s"}}
+    """The FP32 oracle port on this host, on a bounded sample of the workload: the first 5
+    steps of the 40-step schedule at n^3 (~10-20 s of CPU work at 256^3 on 16 cores)."""
+    cpu = CpuKdk(n)
+    rate, dt = cpu.rate(0, 5)
+    return {"value": round(rate, 4), "unit": "Mpart-steps/s", "cores": cpu_threads(), "kind": "port",
+            "sample": f"the first 5 KDK steps of the 40-step schedule at {n}^3 from the same 2LPT ICs (FP32 oracle: "
+                      f"CIC in C/OpenMP, 4 complex scipy FFTs per step with all workers); {dt:.1f} s"}
 
 
 def run_reference(args):
+    """The reference arm: the FP32 oracle port of the reference algorithm (jax and the
+    JaxPM fork are not installable on this image) on the host cores, on the GPU arm's
+    workload (256^3, box 1000 Mpc/h, 2LPT, the 40-step schedule), --warmup untimed steps
+    then --steps timed steps; rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    # bounded sample of the workload: ~5 s per step at 128^3, ~2 s at 96^3, so the run
-    # stays within a few minutes for any --steps
-    k = args.steps + args.warmup
-    n = args.mesh // 2 if k <= 24 else (args.mesh * 3 // 8 if k <= 60 else args.mesh // 4)
-    for _ in range(args.warmup):
-        cpu_step_rate(n, 1)
-    rate, dt = cpu_step_rate(n, args.steps)
+    n = args.mesh
+    cpu = CpuKdk(n)
+    rate, dt = cpu.rate(args.warmup, args.steps)
+    box = BOX * n / N_MESH
     line = {"metric": METRIC, "value": round(rate, 4), "unit": "Mpart-steps/s", "n_gpus": args.gpus, "device": "cpu",
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"PM KDK step, {n}^3 particles/mesh (sample of the 256^3 config)",
-                       "mesh": n, "box": BOX * n / N_MESH},
-            "cpu_baseline": {"value": round(rate, 4), "unit": "Mpart-steps/s", "cores": os.cpu_count(),
-                             "kind": "port",
-                             "sample": f"{args.steps} KDK steps at {n}^3 (FP32 NumPy/SciPy port of the reference "
-                                       f"algorithm; jax and the JaxPM fork are not installable on this image)"},
+            "config": {"workload": f"PM KDK step at {n}^3 particles on a {n}^3 mesh, box {box:g} Mpc/h, 2LPT ICs "
+                                   f"(seeded white noise)",
+                       "mesh": n, "particles": n**3, "box": box, "solver": "EfficientDriftDoubleKick",
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": round(rate, 4), "unit": "Mpart-steps/s", "cores": cpu_threads(), "kind": "port",
+                             "sample": f"{args.steps} KDK steps of the 40-step schedule at {n}^3 after {args.warmup} "
+                                       f"untimed ones (FP32 oracle port of the reference algorithm: CIC in C/OpenMP, "
+                                       f"scipy.fft with all workers; jax and the JaxPM fork are not installable on "
+                                       f"this image); setup {cpu.setup_s:.1f} s untimed"},
             "e2e": {"value": round(rate, 4), "unit": "Mpart-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -683,8 +756,8 @@ def run_lightcone(args):
     from jfli_b200 import sht
 
     t = time.perf_counter()
-    shell = res.shells.array[-1].double().cpu().numpy()
-    cl = sht.anafast(shell / shell.mean() - 1.0, lmax=3000)
+    shell = res.shells.array[-1].double()
+    cl = sht.anafast(shell / shell.mean() - 1.0, lmax=3000).cpu().numpy()
     t_cl = time.perf_counter() - t
     kap = res.kappa.array
     centres = np.asarray(res.shells.comoving_centers, np.float64)

@@ -128,6 +128,15 @@ int jfli_pm_forces(void* stream, const float* pos, int absolute, float scale, fl
  * the force of jaxpm pm_forces (pm/solvers.py:19-32). */
 int jfli_force_mesh(void* stream, const float* pot, float scale, float* force, int nx, int ny, int nz, int batch,
                     char* err, size_t errlen);
+/* Force meshes of a density: pot = jfli_poisson_potential(rho, rho_mean), then
+ * force = jfli_force_mesh(pot, scale), in one call (the Poisson solve and gradient of
+ * pm/solvers.py:19-32 _forces, jaxpm pm_forces, before the readout). With clear_rho != 0
+ * the density mesh is set to 0 as the forward FFT reads it, ready for the next paint (the
+ * fused step loop then needs no memset); pot must not alias rho then. Workspace:
+ * jfli_poisson_workspace_bytes. */
+int jfli_poisson_force(void* stream, float* rho, float rho_mean, int clear_rho, float scale, float* pot, float* force,
+                       void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                       size_t errlen);
 /* Fused particle pass: [kick, or with CORRECT a position shift, by kick * the CIC readout
  * of `force` (jfli_force_mesh layout) at the current position] -> [drift] -> [paint into
  * rho (accumulating)]. Positions are relative (displacements). */
@@ -291,6 +300,12 @@ int jfli_sht_map2alm(void* stream, const double* F, const double* z, int nrings,
                      double* alm, char* err, size_t errlen);
 int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nrings, int lmax, double* G, char* err,
                      size_t errlen);
+/* Angular power spectrum of packed a_lm (healpy alm2cl, reference
+ * _src/power/_compute.py:175-191 via anafast): cl[l] = (Re a_l0 b_l0* + 2 sum_{m=1..l}
+ * Re a_lm b_lm*) / (2l + 1), l = 0..lmax; alm2 NULL gives the auto spectrum of alm1.
+ * FP64, summed in increasing m. */
+int jfli_sht_alm2cl(void* stream, const double* alm1, const double* alm2, int lmax, double* cl, char* err,
+                    size_t errlen);
 
 /* ---- adjoints ------------------------------------------------------------------
  * Reverse sweep of one reversible KKD step  v' = v + kick F(x);  x' = x + drift v'
@@ -362,15 +377,16 @@ int jfli_ic_filter_tangent(void* stream, const float* noise, float* out, const f
 /* P(k) that allocates nothing. This entry point has no counterpart in the reference.
  *
  * Some callers cannot allocate device memory when they need P(k): a JAX/XLA custom-call
- * handler in a process where XLA has already reserved most of the GPU memory for its own
- * pool, or code that is being recorded into a CUDA graph, where cudaMalloc is not
- * allowed. This variant takes the same inputs and writes the same out[batch][3][nedges+1]
+ * handler runs in a process where XLA has already reserved most of the GPU memory for its
+ * own pool, so a cudaMalloc from inside the handler can fail or break XLA's accounting,
+ * and the handler has no workspace of its own unless XLA hands it one. This variant takes the same inputs and writes the same out[batch][3][nedges+1]
  * sums as jfli_power_spectrum, but needs no workspace: its scratch (the half spectrum and
  * the histogram partials) is an 11 MiB array compiled into the library, which every GPU
  * that loads the library holds until the process exits. That bounds the mesh: up to
  * 128^3 cells (with up to 128 bin edges); larger requests return JFLI_EUNSUPPORTED.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress),
- * so make that first call before any stream capture. Every call overwrites the array, so
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress;
+ * again after the device's context has been re-created), so make that first call before
+ * any stream capture. Every call overwrites the array, so
  * two calls that run on the GPU at the same time (other streams, other host threads)
  * corrupt each other's results; serialise them. */
 int jfli_power_spectrum_noalloc(void* stream, const float* mesh, const float* kedges, int nedges, float lx, float ly,

@@ -128,6 +128,9 @@ _SIGNATURES = {
     "jfli_sht_ring_analysis": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
     "jfli_sht_ring_synthesis": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
     "jfli_sht_alm2map": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
+    "jfli_sht_alm2cl": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, *_ERR]),
+    "jfli_poisson_force": (c_int, [c_void_p, c_void_p, c_float, c_int, c_float, c_void_p, c_void_p, c_void_p,
+                                   c_size_t, *_DIMS, *_ERR]),
     "jfli_born_workspace_bytes": (c_size_t, [c_int, c_longlong]),
     "jfli_born_flat": (
         c_int,

@@ -310,6 +310,28 @@ int jfli_pm_step_slots(void* stream, float* disp, float* vel, const float* kicks
   return cuda_status(e, err, errlen, "jfli_pm_step_slots");
 }
 
+int jfli_poisson_force(void* stream, float* rho, float rho_mean, int clear_rho, float scale, float* pot, float* force,
+                       void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                       size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(rho);
+  CHECK_PTR(pot);
+  CHECK_PTR(force);
+  CHECK_ALIGN16(force);
+  CHECK_PTR(workspace);
+  const MeshDims d{nx, ny, nz, batch};
+  const size_t need = jfli_poisson_workspace_bytes(nx, ny, nz, batch);
+  if (workspace_bytes < need)
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  if (pot == rho && clear_rho) return fail(err, errlen, JFLI_EINVAL, "pot must not alias rho when clear_rho is set");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = jfli::poisson_potential(rho, (float2*)workspace, pot, d, rho_mean, 1.0f, s, clear_rho ? rho : nullptr);
+  if (e == cudaSuccess) e = jfli::force_mesh(pot, force, scale, d, s);
+  return cuda_status(e, err, errlen, "jfli_poisson_force");
+}
+
 int jfli_ic_filter(void* stream, const float* noise, float* out, const float* ktab, const float* ptab, int ntab,
                    float lx, float ly, float lz, int zero_mode_one, void* workspace, size_t workspace_bytes, int nx,
                    int ny, int nz, int batch, char* err, size_t errlen) {
@@ -765,6 +787,14 @@ int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nring
                      "jfli_sht_alm2map");
 }
 
+int jfli_sht_alm2cl(void* stream, const double* alm1, const double* alm2, int lmax, double* cl, char* err,
+                    size_t errlen) {
+  CHECK_PTR(alm1);
+  CHECK_PTR(cl);
+  if (lmax < 0 || lmax > 8191) return fail(err, errlen, JFLI_EINVAL, "lmax %d outside [0, 8191]", lmax);
+  return cuda_status(jfli::sht_alm2cl(alm1, alm2, lmax, cl, (cudaStream_t)stream), err, errlen, "jfli_sht_alm2cl");
+}
+
 // ---- reversible KKD loop and its reverse sweep -------------------------------------
 namespace {
 struct KkdWs {
@@ -800,11 +830,13 @@ KkdWs kkd_ws(void* w, const MeshDims& d) {
   return k;
 }
 
-// density of the current positions -> force mesh (in ws.force)
-cudaError_t kkd_force(float* disp, float* vel, float* rho, const KkdWs& w, const MeshDims& d, cudaStream_t s) {
+// density of the current positions -> force mesh (in ws.force); with clear_rho the
+// density mesh comes out cleared (the r2c pass zeroes what it has read)
+cudaError_t kkd_force(float* disp, float* vel, float* rho, const KkdWs& w, const MeshDims& d, cudaStream_t s,
+                      bool clear_rho) {
   cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * d.batch * sizeof(float), s);
   if (e == cudaSuccess) e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, 0.f, JFLI_STEP_PAINT, 1.0f, rho, d, s);
-  if (e == cudaSuccess) e = jfli::poisson_potential(rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
+  if (e == cudaSuccess) e = jfli::poisson_potential(rho, w.spec, w.pot, d, 1.0f, 1.0f, s, clear_rho ? rho : nullptr);
   if (e == cudaSuccess) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
   return e;
 }
@@ -833,13 +865,13 @@ int jfli_kkd_run(void* stream, float* disp, float* vel, const float* kicks, cons
     return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, kkd_ws_bytes(d));
   cudaStream_t s = (cudaStream_t)stream;
   const KkdWs w = kkd_ws(workspace, d);
-  cudaError_t e = kkd_force(disp, vel, rho, w, d, s);
+  // rho enters every step cleared by the r2c pass of the force before it; the last step's
+  // paint stays in rho (the density of the final positions)
+  cudaError_t e = kkd_force(disp, vel, rho, w, d, s, nsteps > 0);
   for (int i = 0; i < nsteps && e == cudaSuccess; ++i) {
-    e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
-    if (e == cudaSuccess)
-      e = jfli::kick_drift_paint(disp, vel, w.force, kicks[i], drifts[i], JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
-                                 1.0f, rho, d, s);
-    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::poisson_potential(rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
+    e = jfli::kick_drift_paint(disp, vel, w.force, kicks[i], drifts[i], JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
+                               1.0f, rho, d, s);
+    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::poisson_potential(rho, w.spec, w.pot, d, 1.0f, 1.0f, s, rho);
     if (e == cudaSuccess && i + 1 < nsteps) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
   }
   return cuda_status(e, err, errlen, "jfli_kkd_run");
@@ -866,14 +898,13 @@ int jfli_kkd_adjoint(void* stream, float* disp, float* vel, float* lam_x, float*
     return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, kkd_ws_bytes(d));
   cudaStream_t s = (cudaStream_t)stream;
   const KkdWs w = kkd_ws(workspace, d);
-  cudaError_t e = cudaSuccess;
+  // w.rho is cleared once here; afterwards each step's r2c pass clears what it has read
+  cudaError_t e = cudaMemsetAsync(w.rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
   for (int i = nsteps - 1; i >= 0 && e == cudaSuccess; --i) {
     const float k = kicks[i], dr = drifts[i];
     // un-drift and paint the previous positions, force mesh there
-    e = cudaMemsetAsync(w.rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
-    if (e == cudaSuccess)
-      e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, -dr, JFLI_STEP_DRIFT | JFLI_STEP_PAINT, 1.0f, w.rho, d, s);
-    if (e == cudaSuccess) e = jfli::poisson_potential(w.rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
+    e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, -dr, JFLI_STEP_DRIFT | JFLI_STEP_PAINT, 1.0f, w.rho, d, s);
+    if (e == cudaSuccess) e = jfli::poisson_potential(w.rho, w.spec, w.pot, d, 1.0f, 1.0f, s, w.rho);
     if (e == cudaSuccess) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
     // un-kick, adjoint paint, dL/dk and dL/dd
     if (e == cudaSuccess) e = jfli::adjoint_unkick_paint(disp, vel, lam_x, lam_v, w.force, k, dr, w.ubar, w.partials, d, s);

@@ -144,14 +144,97 @@ __global__ void k_readout_gradient(const float* __restrict__ pos, int absolute, 
   }
 }
 
+// The upper-x corners (x plane cx.i1) of a lane's previous particle in the brick walk,
+// held back in registers: when the lane's next particle, one Lagrangian plane further in
+// x, has its lower-x corners in the same four cells (neighbours that moved together), the
+// two deposits are added before one atomic each, so a plane of cells takes one set of
+// atomics instead of two.
+struct XCarry {
+  int xo, yo0, yo1, z0, z1;  // cell offsets of the 2 (y) x 2 (z) corners: x ny nz, y nz, z
+  float w00, w01, w10, w11;  // weights [y][z]
+  bool valid;
+};
+
+// Deposit, for every lane of a full warp, the 2 (y) x 2 (z) corners of one x plane, with
+// the z lane merge of deposit_lane_merged: when lane L's upper-z pair of cells is lane
+// L+1's lower-z pair (same x and y cells, next z cell), lane L hands its two upper-z
+// weights to lane L+1, which adds them to its own lower-z deposits. Lanes with `on` false
+// deposit nothing and take part in no merge. Cell offsets are unique per cell, so equal
+// offsets mean equal cells.
+__device__ __forceinline__ void deposit_plane_merged(float* rho, bool on, int xo, int yo0, int yo1, int z0, int z1,
+                                                     float w00, float w01, float w10, float w11) {
+  const int lane = threadIdx.x & 31;
+  const int lo = on ? xo + yo0 + z0 : -1;
+  const int hi = on ? xo + yo0 + z1 : -2;
+  const int next_lo = __shfl_down_sync(0xffffffffu, lo, 1);
+  const int prev_hi = __shfl_up_sync(0xffffffffu, hi, 1);
+  const bool give = on && lane < 31 && next_lo == hi;
+  const bool take = on && lane > 0 && prev_hi == lo;
+  const float r0 = __shfl_up_sync(0xffffffffu, w01, 1);
+  const float r1 = __shfl_up_sync(0xffffffffu, w11, 1);
+  if (on) {
+    atomicAdd(rho + (xo + yo0 + z0), take ? w00 + r0 : w00);
+    atomicAdd(rho + (xo + yo1 + z0), take ? w10 + r1 : w10);
+    if (!give) {
+      atomicAdd(rho + (xo + yo0 + z1), w01);
+      atomicAdd(rho + (xo + yo1 + z1), w11);
+    }
+  }
+}
+
+__device__ __forceinline__ void carry_flush(float* rho, XCarry& c) {
+  atomicAdd(rho + (c.xo + c.yo0 + c.z0), c.w00);
+  atomicAdd(rho + (c.xo + c.yo0 + c.z1), c.w01);
+  atomicAdd(rho + (c.xo + c.yo1 + c.z0), c.w10);
+  atomicAdd(rho + (c.xo + c.yo1 + c.z1), c.w11);
+  c.valid = false;
+}
+
+// CIC deposit of one particle in the brick walk (full warps, lanes on consecutive z
+// particles of one row, successive calls of a lane on successive x planes): the lower-x
+// plane is deposited now, with the carried upper-x plane of the lane's previous particle
+// added when the cells are the same (otherwise the carry is deposited on its own first),
+// and the upper-x plane becomes the new carry. The sums reaching each cell are those of
+// deposit(); only the FP32 addition order differs.
+__device__ __forceinline__ void deposit_carried(float* rho, const PGrid& g, const Cic1& cx, const Cic1& cy,
+                                                const Cic1& cz, float w, XCarry& c) {
+  const float wx0 = cx.w0 * w, wx1 = cx.w1 * w;
+  const int xo0 = cx.i0 * g.yz, yo0 = cy.i0 * g.nz, yo1 = cy.i1 * g.nz;
+  float a00 = (wx0 * cy.w0) * cz.w0, a01 = (wx0 * cy.w0) * cz.w1;
+  float a10 = (wx0 * cy.w1) * cz.w0, a11 = (wx0 * cy.w1) * cz.w1;
+  if (c.valid) {
+    if (c.xo == xo0 && c.yo0 == yo0 && c.z0 == cz.i0) {
+      a00 += c.w00;
+      a01 += c.w01;
+      a10 += c.w10;
+      a11 += c.w11;
+    } else {
+      carry_flush(rho, c);
+    }
+  }
+  deposit_plane_merged(rho, true, xo0, yo0, yo1, cz.i0, cz.i1, a00, a01, a10, a11);
+  c.xo = cx.i1 * g.yz;
+  c.yo0 = yo0;
+  c.yo1 = yo1;
+  c.z0 = cz.i0;
+  c.z1 = cz.i1;
+  c.w00 = (wx1 * cy.w0) * cz.w0;
+  c.w01 = (wx1 * cy.w0) * cz.w1;
+  c.w10 = (wx1 * cy.w1) * cz.w0;
+  c.w11 = (wx1 * cy.w1) * cz.w1;
+  c.valid = true;
+}
+
 // One particle of the fused pass. Order inside: kick (with the force at the current
 // position) -> drift (with the kicked velocity) -> paint (at the new position). Positions
 // and velocities stream through once per pass: streaming (evict-first) loads and stores,
-// so that they do not push the force and density meshes out of L2.
+// so that they do not push the force and density meshes out of L2. With a carry (the
+// brick walk) the deposit holds back the upper-x plane for the lane's next particle.
+template <bool kCarry>
 __device__ __forceinline__ void kdp_particle(float* __restrict__ disp, float* __restrict__ vel,
                                              const float* __restrict__ force, float kick, float drift, int flags,
                                              float weight, float* __restrict__ rho, const PGrid& g, unsigned p, int i,
-                                             int j, int k) {
+                                             int j, int k, XCarry& carry) {
   float x0 = __ldcs(disp + 3 * p + 0), x1 = __ldcs(disp + 3 * p + 1), x2 = __ldcs(disp + 3 * p + 2);
   const bool use_v = flags & (kStepKick | kStepDrift);
   float v0 = 0.f, v1 = 0.f, v2 = 0.f;
@@ -189,7 +272,10 @@ __device__ __forceinline__ void kdp_particle(float* __restrict__ disp, float* __
   }
   if (flags & kStepPaint) {
     const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
-    deposit_lane_merged(rho, g, cx, cy, cz, weight);
+    if (kCarry)
+      deposit_carried(rho, g, cx, cy, cz, weight, carry);
+    else
+      deposit_lane_merged(rho, g, cx, cy, cz, weight);
   }
 }
 
@@ -228,17 +314,24 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
       const int iy = (int)(rest % ty), xc = (int)(rest / ty);
       const int j = iy * kBrickY + w, k = iz * kBrickZ + lane;
       const int i1 = min(g.nx, (xc + 1) * kBrickX);
+      XCarry carry;
+      carry.valid = false;
       for (int i = xc * kBrickX; i < i1; ++i) {
         const unsigned p = ((unsigned)i * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)k;
-        kdp_particle(disp, vel, force, kick, drift, flags, weight, rho, g, p, i, j, k);
+        kdp_particle<true>(disp, vel, force, kick, drift, flags, weight, rho, g, p, i, j, k, carry);
       }
+      // every lane of the warp ran the same planes: the carries go out together, z-merged
+      deposit_plane_merged(rho, carry.valid, carry.xo, carry.yo0, carry.yo1, carry.z0, carry.z1, carry.w00,
+                           carry.w01, carry.w10, carry.w11);
     }
     return;
   }
+  XCarry none;
+  none.valid = false;
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
     particle_ijk(g, p, i, j, k);
-    kdp_particle(disp, vel, force, kick, drift, flags, weight, rho, g, p, i, j, k);
+    kdp_particle<false>(disp, vel, force, kick, drift, flags, weight, rho, g, p, i, j, k, none);
   }
 }
 

@@ -354,11 +354,13 @@ __global__ void __launch_bounds__(ColCfg<N>::T) k_x_op_reg(float2* __restrict__ 
 }
 
 // r2c along z, nh = nz/2 = N complex per row, R rows per CTA.
+// With `clear` (the input mesh itself) each input value is overwritten with 0 by the thread
+// that read it, so a density mesh comes out cleared for the next paint.
 template <int N>
-__global__ void __launch_bounds__(RowCfg<N>::T) k_rfft_z_reg(const float* __restrict__ in, float2* __restrict__ out,
+__global__ void __launch_bounds__(RowCfg<N>::T) k_rfft_z_reg(const float* in, float2* __restrict__ out,
                                                              int nrows, float sub, const float2* __restrict__ twg,
                                                              const float2* __restrict__ twg2, long long in_b,
-                                                             long long out_b) {
+                                                             long long out_b, float* clear) {
   constexpr int P = Split<N>::P, Q = Split<N>::Q, R = RowCfg<N>::R, T = RowCfg<N>::T;
   constexpr int S = P * (Q + 1);
   extern __shared__ float2 sm[];
@@ -367,6 +369,7 @@ __global__ void __launch_bounds__(RowCfg<N>::T) k_rfft_z_reg(const float* __rest
   float2* ybuf = tw2 + N + 1;  // R*S; reused for the Z rows (stride N+1 <= S)
   in += (long long)blockIdx.y * in_b;
   out += (long long)blockIdx.y * out_b;
+  if (clear) clear += (long long)blockIdx.y * in_b;
   const int tid = threadIdx.x;
   for (int m = tid; m < N; m += T) tw[m] = twg[m];
   for (int m = tid; m <= N; m += T) tw2[m] = twg2[m];
@@ -383,6 +386,11 @@ __global__ void __launch_bounds__(RowCfg<N>::T) k_rfft_z_reg(const float* __rest
       for (int m = 0; m < Q; ++m) {
         const float2 z = src[P * m];
         u[m] = make_float2(z.x - sub, z.y - sub);
+      }
+      if (clear) {
+        float2* dst = reinterpret_cast<float2*>(clear) + (long long)row * N + t;
+#pragma unroll
+        for (int m = 0; m < Q; ++m) dst[P * m] = make_float2(0.f, 0.f);
       }
     } else {
 #pragma unroll
@@ -588,7 +596,8 @@ static int reg_col_w(int n) {
 }
 
 template <int N>
-static cudaError_t rfft_z_reg(const float* in, float2* out, const MeshDims& d, float sub, cudaStream_t s) {
+static cudaError_t rfft_z_reg(const float* in, float2* out, const MeshDims& d, float sub, cudaStream_t s,
+                              float* clear) {
   constexpr int R = RowCfg<N>::R, T = RowCfg<N>::T, P = Split<N>::P, Q = Split<N>::Q;
   const float2* tw = twiddle_table(N);
   const float2* tw2 = twiddle_table(2 * N);
@@ -597,7 +606,7 @@ static cudaError_t rfft_z_reg(const float* in, float2* out, const MeshDims& d, f
   const size_t smem = ((size_t)N + N + 1 + (size_t)R * P * (Q + 1)) * sizeof(float2);
   cudaFuncSetAttribute(k_rfft_z_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_rfft_z_reg<N><<<dim3((nrows + R - 1) / R, d.batch), T, smem, s>>>(in, out, nrows, sub, tw, tw2, d.cells(),
-                                                                       d.spec_elems());
+                                                                       d.spec_elems(), clear);
   note_launch();
   return cudaGetLastError();
 }
@@ -644,11 +653,13 @@ static cudaError_t x_op_reg(float2* data, const ColGeom& g, const Op& op, long l
 }
 
 // ---- generic (shared-memory Stockham) launchers for the remaining lengths
-static cudaError_t launch_rfft_z(const float* in, float2* out, const MeshDims& d, float sub, cudaStream_t s) {
+// `clear`: the input mesh, set to 0 once it has been read (nullptr: left as it is).
+static cudaError_t launch_rfft_z(const float* in, float2* out, const MeshDims& d, float sub, cudaStream_t s,
+                                 float* clear = nullptr) {
   switch (d.nz / 2) {
 #define JFLI_CASE(N_) \
   case N_:            \
-    return rfft_z_reg<N_>(in, out, d, sub, s);
+    return rfft_z_reg<N_>(in, out, d, sub, s, clear);
     JFLI_REG_SIZES(JFLI_CASE)
 #undef JFLI_CASE
     default:
@@ -664,7 +675,9 @@ static cudaError_t launch_rfft_z(const float* in, float2* out, const MeshDims& d
   cudaFuncSetAttribute(k_rfft_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_rfft_z<<<grid, kFftThreads, smem, s>>>(in, out, nrows, d.nz, rows, pl, sub, d.cells(), d.spec_elems());
   note_launch();
-  return cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && clear) e = cudaMemsetAsync(clear, 0, sizeof(float) * (size_t)d.cells() * d.batch, s);
+  return e;
 }
 
 static cudaError_t launch_irfft_z(const float2* in, float* out, const MeshDims& d, float scale, cudaStream_t s) {
@@ -787,8 +800,8 @@ cudaError_t rfft3d_inverse(float2* spec, float* out, const MeshDims& d, float sc
 // real mesh -> (forward 3D FFT, k-space op, inverse 3D FFT) -> real mesh.
 template <class Op>
 static cudaError_t filter_chain(const float* in, float2* spec, float* out, const MeshDims& d, float sub, const Op& op,
-                                cudaStream_t s) {
-  cudaError_t e = launch_rfft_z(in, spec, d, sub, s);
+                                cudaStream_t s, float* clear = nullptr) {
+  cudaError_t e = launch_rfft_z(in, spec, d, sub, s, clear);
   if (e != cudaSuccess) return e;
   e = launch_cols<-1>(spec, y_geom(d), d.spec_elems(), d.batch, s);
   if (e != cudaSuccess) return e;
@@ -800,13 +813,13 @@ static cudaError_t filter_chain(const float* in, float2* spec, float* out, const
 }
 
 cudaError_t poisson_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean,
-                              float scale, cudaStream_t s) {
+                              float scale, cudaStream_t s, float* clear) {
   PoissonOp op;
   op.nx = d.nx;
   op.ny = d.ny;
   op.nz = d.nz;
   op.norm = scale / ((float)d.nx * (float)d.ny * (float)d.nz);
-  return filter_chain(rho, spec, pot, d, rho_mean, op, s);
+  return filter_chain(rho, spec, pot, d, rho_mean, op, s, clear);
 }
 
 cudaError_t pgd_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean, float kl,
@@ -890,20 +903,42 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 constexpr int kNoAllocMaxDevices = 64;
 static std::mutex g_noalloc_mutex;
 static void* g_noalloc_ptr[kNoAllocMaxDevices];  // device -> address of g_noalloc_scratch on it
+static void* g_noalloc_ctx[kNoAllocMaxDevices];  // the context that address belongs to
+
+// The calling thread's current driver context (cuCtxGetCurrent through the runtime's
+// driver entry point, so the library needs no link to libcuda), or nullptr.
+static void* current_context() {
+  using GetCurrent = int (*)(void**);
+  static GetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetCurrent>(f);
+  }();
+  void* ctx = nullptr;
+  if (fn == nullptr || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
 
 // Device address of the scratch array on the current device. The first call on a device
 // looks it up with cudaGetSymbolAddress (with that device current); later calls reuse it.
+// The address is tied to the device's context: a new context on the device (after
+// cudaDeviceReset, for instance) gets a new lookup, so no call uses a stale address.
 cudaError_t noalloc_scratch(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (g_noalloc_ptr[dev] == nullptr) {
+  void* ctx = g_noalloc_ptr[dev] ? current_context() : nullptr;
+  if (g_noalloc_ptr[dev] == nullptr || ctx == nullptr || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // makes the device's primary context current
     if (e != cudaSuccess) return e;
     g_noalloc_ptr[dev] = p;
+    g_noalloc_ctx[dev] = current_context();
   }
   *out = g_noalloc_ptr[dev];
   return cudaSuccess;

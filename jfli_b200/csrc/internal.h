@@ -23,8 +23,10 @@ int x_pass_ctas(const MeshDims& d);
 cudaError_t rfft3d_forward(const float* in, float2* spec, const MeshDims& d, float sub, cudaStream_t s);
 cudaError_t rfft3d_inverse(float2* spec, float* out, const MeshDims& d, float scale, cudaStream_t s);
 cudaError_t rfft2d_forward(const float* in, float2* spec, const MeshDims& d, cudaStream_t s);  // d.nx == 1
+// clear: the density mesh (rho itself), set to 0 by the r2c pass once read, so the next
+// paint needs no memset; nullptr leaves rho as it is.
 cudaError_t poisson_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean,
-                              float scale, cudaStream_t s);
+                              float scale, cudaStream_t s, float* clear = nullptr);
 cudaError_t pgd_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean, float kl,
                           float ks, float scale, cudaStream_t s);
 // dptab != null: the tangent of the filter along a change dptab of the P(k) table.
@@ -100,6 +102,7 @@ cudaError_t sht_analysis(const double* F, const double* z, int nrings, int lmax,
 cudaError_t sht_synthesis(const double* alm, const double* z, int nrings, int lmax, double* G, cudaStream_t s);
 cudaError_t sht_ring_analysis(const double* map, int nside, int lmax, double* F, cudaStream_t s);
 cudaError_t sht_ring_synthesis(const double* G, int nside, int lmax, double* map, cudaStream_t s);
+cudaError_t sht_alm2cl(const double* alm1, const double* alm2, int lmax, double* cl, cudaStream_t s);
 
 // ---- adjoint.cu ----
 size_t adjoint_partials_count(const MeshDims& d);

@@ -313,4 +313,29 @@ cudaError_t sht_synthesis(const double* alm, const double* z, int nrings, int lm
   return cudaGetLastError();
 }
 
+// C_l = (Re a_l0 b_l0* + 2 sum_{m=1..l} Re a_lm b_lm*) / (2l + 1) (healpy alm2cl), one
+// thread per l, FP64 sums in increasing m (a fixed order: the result is deterministic).
+__global__ void k_sht_alm2cl(const double2* __restrict__ a, const double2* __restrict__ b, int lmax,
+                             double* __restrict__ cl) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l > lmax) return;
+  double acc = 0.0;
+  for (int m = 1; m <= l; ++m) {
+    const long long o = alm_offset(m, lmax) + (l - m);
+    const double2 x = a[o], y = b[o];
+    acc += x.x * y.x + x.y * y.y;
+  }
+  const double2 x0 = a[l], y0 = b[l];
+  cl[l] = (x0.x * y0.x + x0.y * y0.y + 2.0 * acc) / (2.0 * l + 1.0);
+}
+
+cudaError_t sht_alm2cl(const double* alm1, const double* alm2, int lmax, double* cl, cudaStream_t s) {
+  const int threads = 128;
+  k_sht_alm2cl<<<(lmax + threads) / threads, threads, 0, s>>>(reinterpret_cast<const double2*>(alm1),
+                                                            reinterpret_cast<const double2*>(alm2 ? alm2 : alm1),
+                                                            lmax, cl);
+  note_launch();
+  return cudaGetLastError();
+}
+
 }  // namespace jfli

@@ -547,7 +547,7 @@ class SphericalDensity(AbstractField):
         for a, b in zip(rows1, rows2):
             ell, cl = angular_cl_spherical(a, b, lmax=lmax, method=method)
             spectra.append(cl)
-        arr = np.stack(spectra) if d1.ndim == 2 else spectra[0]
+        arr = torch.stack(spectra) if d1.ndim == 2 else spectra[0]
         return PowerSpectrum(wavenumber=ell, array=arr, name="cl", scale_factors=self.scale_factors)
 
     def ud_sample(self, new_nside: int) -> "SphericalDensity":

@@ -161,10 +161,23 @@ def force_mesh(pot: torch.Tensor, scale: float = 1.0, out: torch.Tensor | None =
 
 
 def poisson_force(rho: torch.Tensor, rho_mean: float = 1.0, out: torch.Tensor | None = None,
-                  pot: torch.Tensor | None = None) -> torch.Tensor:
-    """Force meshes of a density: Poisson solve, then the finite-difference gradient."""
-    pot = poisson_potential(rho, rho_mean, out=pot)
-    return force_mesh(pot, out=out)
+                  pot: torch.Tensor | None = None, clear: bool = False) -> torch.Tensor:
+    """Force meshes of a density: Poisson solve, then the finite-difference gradient (one
+    library call). With clear=True the density mesh comes back zeroed (the forward FFT
+    clears what it reads), ready for the next paint."""
+    _check(rho, "rho")
+    (nx, ny, nz), batch, lead = _mesh_dims(rho, False)
+    if pot is None:
+        pot = torch.empty_like(rho)
+    if out is None:
+        out = torch.empty(*lead, nx, ny, nz, 4, dtype=torch.float32, device=rho.device)
+    elif out.numel() != 4 * batch * nx * ny * nz:
+        raise ValueError("out must hold (nx, ny, nz, 4) per mesh")
+    nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "spec", rho.device)
+    call("jfli_poisson_force", stream_ptr(), ptr(rho), float(rho_mean), int(bool(clear)), 1.0, ptr(pot), ptr(out),
+         ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return out
 
 
 def kick_drift_paint(disp: torch.Tensor, vel: torch.Tensor, force: torch.Tensor | None, kick: float, drift: float,

@@ -36,8 +36,13 @@ def pgd_scales_to_grid(kl_hmpc: float, ks_hmpc: float, mesh: int, box: float):
 def lightcone_convergence(cosmo, *, mesh: int, box: float, seed: int, nb_shells: int, nside: int, nz_shear,
                           t0: float = 0.1, t1: float = 1.0, steps: int = 60, lpt_order: int = 2, pgd=None,
                           min_z: float = 0.01, max_z: float = 1.0, n_integrate: int = 32, tiler: str = "none",
-                          max_radius: float | None = None) -> LightconeResult:
+                          max_radius: float | None = None, noise=None,
+                          rotation_indices=None) -> LightconeResult:
     """pgd = (alpha, kl, ks) with kl, ks in h/Mpc, or None.
+
+    noise: the (mesh,)^3 white noise (array or tensor) to start from; when None it is
+    drawn on the device from `seed`. rotation_indices: OnionTiler's 27 cube-symmetry
+    indices (None: its seeded draw).
 
     tiler "none": nb_shells equal-width shells inside the box (NoInterp; radii up to the
     largest sphere around the observer that the box holds, as nbody(nb_shells=...) gives).
@@ -49,8 +54,13 @@ def lightcone_convergence(cosmo, *, mesh: int, box: float, seed: int, nb_shells:
     timings = {}
     sync = torch.cuda.synchronize
     t = time.perf_counter()
-    gen = torch.Generator(device="cuda").manual_seed(int(seed))
-    noise = torch.randn((mesh,) * 3, generator=gen, device="cuda", dtype=torch.float32)
+    if noise is None:
+        gen = torch.Generator(device="cuda").manual_seed(int(seed))
+        noise = torch.randn((mesh,) * 3, generator=gen, device="cuda", dtype=torch.float32)
+    else:
+        noise = torch.as_tensor(noise, dtype=torch.float32).to("cuda")
+        if tuple(noise.shape) != (mesh,) * 3:
+            raise ValueError(f"noise must have shape {(mesh,) * 3}")
     ic = jf.interpolate_initial_conditions(noise, (mesh,) * 3, (box,) * 3, cosmo=cosmo, nside=nside)
     del noise
     dx, p = jf.lpt(cosmo, ic, ts=t0, order=lpt_order)
@@ -74,7 +84,8 @@ def lightcone_convergence(cosmo, *, mesh: int, box: float, seed: int, nb_shells:
         r_max = 3.0 * dx.max_comoving_radius if max_radius is None else float(max_radius)
         edges = np.linspace(0.0, r_max, nb_shells + 1)[::-1]  # far -> near, as the time loop meets them
         centres = 0.5 * (edges[1:] + edges[:-1])
-        kernel = jf.OnionTiler(painting=painting)
+        kernel = jf.OnionTiler(painting=painting, rotation_indices=None if rotation_indices is None
+                               else tuple(int(i) for i in rotation_indices))
         geom = dict(ts=np.asarray(cj.a_of_chi(cosmo, centres), np.float64), density_widths=edges[:-1] - edges[1:])
     else:
         raise ValueError(f"tiler must be 'none' or 'onion', not {tiler!r}")

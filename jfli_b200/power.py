@@ -177,26 +177,20 @@ def coherence(mesh0, mesh1, *, box_shape, kedges=None):
     return k, pk01 / (pk0 * pk1) ** 0.5
 
 
-def _host_map(m):
-    return (m.detach().double().cpu().numpy() if isinstance(m, torch.Tensor)
-            else np.asarray(m, dtype=np.float64))
-
-
 def angular_cl_spherical(map_sphere, map_sphere2=None, *, lmax: int | None = None, method: str = "jax"):
     """Spherical C_l, auto or cross (reference power/compute.py:89-98 -> healpy anafast):
-    (ell, cl). Both method values run healpy's algorithm in this library's GPU engine."""
+    (ell, cl) as device float64 tensors. Both method values run healpy's algorithm in this
+    library's GPU engine; the maps, a_lm and spectra stay on the device."""
     from . import sht
 
     if method not in ("jax", "healpy"):
         raise ValueError(f"unknown method {method!r}")
-    m1 = _host_map(map_sphere)
-    nside = int(round(math.sqrt(m1.size / 12)))
-    lmax = 3 * nside - 1 if lmax is None else int(lmax)
-    if map_sphere2 is None:
-        cl = sht.anafast(m1, lmax)
-    else:
-        cl = sht.alm2cl_cross_packed(sht.map2alm_gpu(m1, lmax), sht.map2alm_gpu(_host_map(map_sphere2), lmax), lmax)
-    return np.arange(cl.shape[-1]) * 1.0, cl
+    npix = map_sphere.numel() if isinstance(map_sphere, torch.Tensor) else np.asarray(map_sphere).size
+    lmax = 3 * sht._nside_of(int(npix)) - 1 if lmax is None else int(lmax)
+    a1 = sht.map2alm(map_sphere, lmax)
+    a2 = None if map_sphere2 is None else sht.map2alm(map_sphere2, lmax)
+    cl = sht.alm2cl(a1, lmax, a2)
+    return torch.arange(lmax + 1, dtype=torch.float64, device=cl.device), cl
 
 
 def cross_angular_cl_spherical(maps, *, lmax: int | None = None, method: str = "healpy"):
@@ -205,5 +199,5 @@ def cross_angular_cl_spherical(maps, *, lmax: int | None = None, method: str = "
 
     if method != "healpy":
         raise ValueError(f"cross_angular_cl_spherical only supports method='healpy', got method='{method}'.")
-    cls = sht.cross_cls(_host_map(maps), lmax)
-    return np.arange(cls.shape[-1]) * 1.0, cls
+    cls = sht.cross_cls(maps, lmax)
+    return torch.arange(cls.shape[-1], dtype=torch.float64, device=cls.device), cls

@@ -71,8 +71,9 @@ def _cic_corners(disp, shape, absolute=False):
     return np.stack(idx, axis=1), np.stack(wts, axis=1)
 
 
-def cic_paint(disp, shape=None, weight=1.0, absolute=False):
-    """Trilinear deposit onto a periodic mesh; positions are grid + disp (relative)."""
+def cic_paint_np(disp, shape=None, weight=1.0, absolute=False):
+    """Trilinear deposit onto a periodic mesh; positions are grid + disp (relative).
+    NumPy form (bincount accumulates in FP64); cic_paint runs the same arithmetic in C."""
     shape = tuple(disp.shape[:3]) if shape is None else tuple(shape)
     idx, w = _cic_corners(disp, shape, absolute)
     if np.ndim(weight) > 0:
@@ -83,10 +84,51 @@ def cic_paint(disp, shape=None, weight=1.0, absolute=False):
     return mesh.reshape(shape).astype(disp.dtype)
 
 
-def cic_read(mesh, disp, absolute=False):
+def cic_read_np(mesh, disp, absolute=False):
+    """NumPy form of cic_read."""
     idx, w = _cic_corners(disp, mesh.shape, absolute)
     vals = mesh.reshape(-1)[idx]
     return (vals * w).sum(axis=1).reshape(disp.shape[:3]).astype(disp.dtype)
+
+
+def _work_dtype(disp):
+    return np.float32 if disp.dtype == np.float32 else np.float64
+
+
+def cic_paint(disp, shape=None, weight=1.0, absolute=False):
+    """Trilinear deposit onto a periodic mesh; positions are grid + disp (relative) or the
+    positions themselves in cells (absolute). The arithmetic of cic_paint_np, run by the
+    OpenMP restatement in oracle/cic.c."""
+    from . import clib
+
+    dt = _work_dtype(disp)
+    shape = tuple(disp.shape[:3]) if shape is None else tuple(int(s) for s in shape)
+    pos = np.ascontiguousarray(disp, dtype=dt).reshape(-1, 3)
+    wts = None
+    if np.ndim(weight) > 0:
+        wts = np.ascontiguousarray(np.broadcast_to(np.asarray(weight, dtype=dt).reshape(-1), (pos.shape[0],)))
+        weight = 1.0
+    mesh = np.empty(shape, dtype=dt)
+    clib.paint(pos, shape, absolute, wts, weight, mesh)
+    return mesh.astype(disp.dtype, copy=False)
+
+
+def cic_read(mesh, disp, absolute=False):
+    """CIC readout of one mesh (or a stack of meshes along a leading axis) at the particles."""
+    from . import clib
+
+    dt = _work_dtype(disp)
+    stack = np.ascontiguousarray(mesh, dtype=dt)
+    single = stack.ndim == 3
+    if single:
+        stack = stack[None]
+    pos = np.ascontiguousarray(disp, dtype=dt).reshape(-1, 3)
+    out = np.empty((pos.shape[0], stack.shape[0]), dtype=dt)
+    clib.read(stack, pos, absolute, out)
+    lead = disp.shape[:3] if not absolute else disp.shape[:-1]
+    if single:
+        return out[:, 0].reshape(lead).astype(disp.dtype, copy=False)
+    return out.reshape(*lead, stack.shape[0]).astype(disp.dtype, copy=False)
 
 
 # -------------------------------------------------------------------------- k-space kernels
@@ -131,11 +173,8 @@ def potential_k(delta_k, kvec):
 def forces_from_delta_k(delta_k, disp, dtype=np.float64):
     kvec = fftk(delta_k.shape, dtype)
     pot_k = potential_k(delta_k, kvec)
-    comps = []
-    for i in range(3):
-        f = ifft3(-gradient_kernel(kvec, i) * pot_k).real.astype(dtype)
-        comps.append(cic_read(f, disp))
-    return np.stack(comps, axis=-1)
+    meshes = np.stack([ifft3(-gradient_kernel(kvec, i) * pot_k).real.astype(dtype) for i in range(3)])
+    return cic_read(meshes, disp.astype(dtype))
 
 
 def pm_forces(disp, dtype=np.float64):
@@ -249,8 +288,7 @@ def pgd_correction(disp, alpha, kl, ks, dtype=np.float64):
     safe = np.where(kk == 0, 1, kk)
     rng = np.where(kk == 0, 0, np.exp(-(kl**2) / safe) * np.exp(-(kk**2) / ks**4))
     pot_k = fft3(cic_paint(disp)) * invlaplace(kvec) * rng
-    f = np.stack([cic_read(ifft3(-gradient_kernel(kvec, i) * pot_k).real.astype(dtype), disp) for i in range(3)],
-                 axis=-1)
+    f = cic_read(np.stack([ifft3(-gradient_kernel(kvec, i) * pot_k).real.astype(dtype) for i in range(3)]), disp)
     return disp + dtype(alpha) * f
 
 

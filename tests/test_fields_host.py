@@ -128,8 +128,8 @@ def test_map_transfer_and_coherence(monkeypatch):
 
     def fake_sph(m1, m2=None, *, lmax=None, method="jax"):
         m2 = m1 if m2 is None else m2
-        v = float((m1.double() * m2.double()).mean())
-        return np.arange(3), np.array([v, v, v])
+        v = (m1.double() * m2.double()).mean()
+        return torch.arange(3, dtype=torch.float64), torch.stack([v, v, v])
 
     monkeypatch.setattr(pw, "angular_cl_flat", fake_flat)
     monkeypatch.setattr(pw, "angular_cl_spherical", fake_sph)
@@ -141,8 +141,8 @@ def test_map_transfer_and_coherence(monkeypatch):
     co = fl.coherence(fl * 3.0)
     np.testing.assert_allclose(co.array.numpy(), 1.0, rtol=1e-12)
     sp = jf.SphericalDensity(array=torch.as_tensor(rng.uniform(1, 2, 192)), nside=4, **META)
-    np.testing.assert_allclose(sp.transfer(sp * 4.0).array, 4.0, rtol=1e-12)
-    np.testing.assert_allclose(sp.coherence(-sp).array, -1.0, rtol=1e-12)
+    np.testing.assert_allclose(sp.transfer(sp * 4.0).array.numpy(), 4.0, rtol=1e-12)
+    np.testing.assert_allclose(sp.coherence(-sp).array.numpy(), -1.0, rtol=1e-12)
 
 
 def test_project():
