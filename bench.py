@@ -440,13 +440,17 @@ def run_serving(args):
     # capacity: the whole stream queued at once (same requests, arrivals at 0)
     burst = [dataclasses_replace(r, rid=r.rid + 2 * 10**6, arrival=0.0)
              for r in serving.poisson_stream(args.serve_requests, 1.0, seed=0, grad_fraction=0.25)]
+    eng.stats = {k: 0 for k in eng.stats}
     s_cap = serving.summarize(eng.run(burst, realtime=False), burst)
+    s_cap["host_s"] = {k: round(v, 3) for k, v in eng.stats.items()}
+    eng.stats = {k: 0 for k in eng.stats}
     rate = args.serve_rate if args.serve_rate > 0 else round(0.85 * s_cap["requests_per_s"], 1)
     reqs = serving.poisson_stream(args.serve_requests, rate, seed=0, grad_fraction=0.25)
     l0 = __import__("jfli_b200").ops.launch_count()
     served = eng.run(reqs, realtime=True)
     launches = __import__("jfli_b200").ops.launch_count() - l0
     s_stats = serving.summarize(served, reqs)
+    s_stats["host_s"] = {k: round(v, 3) for k, v in eng.stats.items()}
     eng.close()
     plain = serving.run_plain(reqs, realtime=True, keep_density="device", on_result=consumer("plain"))
     p_stats = serving.summarize(plain, reqs)
@@ -648,6 +652,42 @@ def fft_vs_cufft(n, iters=20):
     return res
 
 
+def x_pass_variants(n, iters=20):
+    """The Poisson chain (r2c, y, fused x pass, y^-1, c2r) on the same seeded n^3 density
+    with the register x pass and with the TMA-staged x pass (jfli_set_fft_x_pass): CUDA-
+    event ms per chain, mean of `iters` after 3 warm-ups, and the potentials' relative
+    difference. The two chains differ only in the x pass."""
+    import torch
+
+    from jfli_b200 import ops
+    from jfli_b200._lib import call
+
+    g = torch.Generator(device="cuda").manual_seed(5)
+    rho = 1.0 + 0.3 * torch.randn((n, n, n), device="cuda", generator=g)
+    pot = torch.empty_like(rho)
+    out = {}
+    pots = {}
+    try:
+        for name, mode in (("register", 0), ("tma", 1)):
+            call("jfli_set_fft_x_pass", mode)
+            for _ in range(3):
+                ops.poisson_potential(rho, 1.0, out=pot)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(iters):
+                ops.poisson_potential(rho, 1.0, out=pot)
+            e1.record()
+            torch.cuda.synchronize()
+            out[f"{name}_chain_ms"] = round(e0.elapsed_time(e1) / iters, 4)
+            pots[name] = pot.clone()
+    finally:
+        call("jfli_set_fft_x_pass", 0)
+    out["rel_diff"] = float((pots["tma"] - pots["register"]).norm() / pots["register"].norm())
+    out["mesh"] = n
+    return out
+
+
 def cpu_baseline_block(n):
     """The FP32 oracle port on this host, on a bounded sample of the workload: the first 5
     steps of the 40-step schedule at n^3 (~10-20 s of CPU work at 256^3 on 16 cores)."""
@@ -790,6 +830,7 @@ def main():
     res = run_gpu(args, world, rank)
     if rank == 0:
         fft_cmp = fft_vs_cufft(args.mesh)
+        xpass = x_pass_variants(args.mesh)
         cpu = None if args.no_cpu_baseline else cpu_baseline_block(args.mesh)
         line = {"metric": METRIC, "value": round(res["value"], 2), "unit": "Mpart-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(res["ms"] / args.steps, 4),
@@ -802,7 +843,7 @@ def main():
                            "l2": "particle state (x, v: 402 MB) exceeds the 126 MB L2; no flush"},
                 "roofline": res["roofline"], "step_roofline": res["step_roofline"], "cpu_baseline": cpu, "e2e": res["e2e"], "clocks": res["clocks"],
                 "gpu_launches": res["launches"], "serving": res["serving"], "gradient": res["gradient"],
-                "e2e_with_shells": res["shells"], "fft_vs_cufft": fft_cmp}
+                "e2e_with_shells": res["shells"], "fft_vs_cufft": fft_cmp, "x_pass_variants": xpass}
         print(json.dumps(line), flush=True)
     if world > 1:
         from jfli_b200 import replicas

@@ -300,6 +300,18 @@ int jfli_sht_map2alm(void* stream, const double* F, const double* z, int nrings,
                      double* alm, char* err, size_t errlen);
 int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nrings, int lmax, double* G, char* err,
                      size_t errlen);
+/* Variant of the x pass of the Poisson, PGD and initial-condition filter chains (the
+ * forward x FFT, k-space operator and inverse x FFT in one read and write of the half
+ * spectrum): 0 (default) loads each pencil tile from global memory into registers; 1
+ * stages the tile in shared memory with a TMA bulk tensor load and writes it back with a
+ * bulk tensor store (meshes whose x-plane stride is a multiple of 16 bytes; others keep
+ * mode 0). Both give the same spectrum to FP32 rounding. Process-wide. */
+int jfli_set_fft_x_pass(int mode, char* err, size_t errlen);
+/* Status word of the library's bounded device waits: bit 0 is set when a kernel's wait on
+ * an mbarrier ran out of its bound (the kernel then left its output untouched). Read
+ * synchronously; reset != 0 clears it. */
+int jfli_device_status(unsigned* status, int reset, char* err, size_t errlen);
+
 /* Angular power spectrum of packed a_lm (healpy alm2cl, reference
  * _src/power/_compute.py:175-191 via anafast): cl[l] = (Re a_l0 b_l0* + 2 sum_{m=1..l}
  * Re a_lm b_lm*) / (2l + 1), l = 0..lmax; alm2 NULL gives the auto spectrum of alm1.

@@ -787,6 +787,17 @@ int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nring
                      "jfli_sht_alm2map");
 }
 
+int jfli_set_fft_x_pass(int mode, char* err, size_t errlen) {
+  if (mode != 0 && mode != 1) return fail(err, errlen, JFLI_EINVAL, "x pass mode %d is not 0 or 1", mode);
+  jfli::set_x_pass_mode(mode);
+  return JFLI_OK;
+}
+
+int jfli_device_status(unsigned* status, int reset, char* err, size_t errlen) {
+  CHECK_PTR(status);
+  return cuda_status(jfli::device_status(status, reset != 0), err, errlen, "jfli_device_status");
+}
+
 int jfli_sht_alm2cl(void* stream, const double* alm1, const double* alm2, int lmax, double* cl, char* err,
                     size_t errlen) {
   CHECK_PTR(alm1);

@@ -11,6 +11,7 @@
 //   x_op     : read+write the half spectrum (forward x, multiply, inverse x)
 //   cols(y)^-1
 //   irfft_z  : read the half spectrum, write 4M B real
+#include <atomic>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -20,6 +21,7 @@
 #include "common.cuh"
 #include "fft_engine.cuh"
 #include "fft_reg.cuh"
+#include "fft_tma.cuh"
 #include "internal.h"
 #include "kspace_ops.cuh"
 
@@ -746,9 +748,86 @@ static cudaError_t launch_cols(float2* data, const ColGeom& g, long long bstride
   return cudaGetLastError();
 }
 
+// ---- TMA-staged x pass
+static std::atomic<int> g_x_pass_mode{0};  // 0 register pass, 1 TMA-staged pass
+
+void set_x_pass_mode(int mode) { g_x_pass_mode.store(mode); }
+int x_pass_mode() { return g_x_pass_mode.load(); }
+
+cudaError_t device_status(unsigned* out, bool reset) {
+  cudaError_t e = cudaMemcpyFromSymbol(out, g_jfli_status, sizeof(unsigned));
+  if (e == cudaSuccess && reset) {
+    const unsigned zero = 0;
+    e = cudaMemcpyToSymbol(g_jfli_status, &zero, sizeof(unsigned));
+  }
+  return e;
+}
+
+bool x_pass_tensor_map(CUtensorMap* map, const float2* spec, const MeshDims& d, int w) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<Encode>(f);
+  }();
+  if (encode == nullptr || ((uintptr_t)spec % 16) != 0) return false;
+  const cuuint64_t inner = 2ull * (cuuint64_t)d.ny * (cuuint64_t)d.hz();  // floats of one x plane
+  const cuuint64_t plane_bytes = inner * sizeof(float);
+  const cuuint64_t batch_bytes = (cuuint64_t)d.spec_elems() * sizeof(float2);
+  if (plane_bytes % 16 != 0 || batch_bytes % 16 != 0 || (2 * w * sizeof(float)) % 16 != 0) return false;
+  const cuuint64_t dims[3] = {inner, (cuuint64_t)d.nx, (cuuint64_t)d.batch};
+  const cuuint64_t strides[2] = {plane_bytes, batch_bytes};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * w), (cuuint32_t)(d.nx > kTmaBoxRows ? kTmaBoxRows : d.nx), 1u};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float2*>(spec), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int N, class Op>
+static cudaError_t x_op_tma(float2* data, const MeshDims& d, const Op& op, bool* done, cudaStream_t s) {
+  *done = false;
+  constexpr int W = ColCfg<N>::W, T = ColCfg<N>::T;
+  if (N % TmaCfg<N>::ROWS != 0) return cudaSuccess;
+  CUtensorMap map;
+  if (!x_pass_tensor_map(&map, data, d, W)) return cudaSuccess;
+  const float2* tw = twiddle_table(N);
+  if (!tw) return cudaErrorMemoryAllocation;
+  const ColGeom g = x_geom(d);
+  const size_t smem = TmaCfg<N>::tile_bytes * 2 + sizeof(float2) * (size_t)N + Op::smem_bytes(op);
+  cudaError_t e = cudaFuncSetAttribute(k_x_op_tma<N, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_x_op_tma<N, Op><<<dim3((g.ncols + W - 1) / W, d.batch), T, smem, s>>>(map, g, tw, op);
+  note_launch();
+  *done = true;
+  return cudaGetLastError();
+}
+
 template <class Op>
 static cudaError_t launch_x_op(float2* data, const MeshDims& d, const Op& op, cudaStream_t s) {
   const ColGeom g = x_geom(d);
+  if constexpr (Op::kInverse) {
+    if (x_pass_mode() == 1) {
+      bool done = false;
+      cudaError_t e = cudaSuccess;
+      switch (g.n) {
+#define JFLI_CASE(N_)                              \
+  case N_:                                         \
+    e = x_op_tma<N_, Op>(data, d, op, &done, s);   \
+    break;
+        JFLI_REG_SIZES(JFLI_CASE)
+#undef JFLI_CASE
+        default:
+          break;
+      }
+      if (e != cudaSuccess || done) return e;
+    }
+  }
   switch (g.n) {
 #define JFLI_CASE(N_) \
   case N_:            \

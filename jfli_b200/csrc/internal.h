@@ -103,6 +103,11 @@ cudaError_t sht_synthesis(const double* alm, const double* z, int nrings, int lm
 cudaError_t sht_ring_analysis(const double* map, int nside, int lmax, double* F, cudaStream_t s);
 cudaError_t sht_ring_synthesis(const double* G, int nside, int lmax, double* map, cudaStream_t s);
 cudaError_t sht_alm2cl(const double* alm1, const double* alm2, int lmax, double* cl, cudaStream_t s);
+// x pass of the Poisson / PGD / IC filter chains: 0 register pass, 1 TMA-staged pass
+void set_x_pass_mode(int mode);
+int x_pass_mode();
+// status word of bounded device waits (bit 0: an mbarrier wait ran out); read, optionally cleared
+cudaError_t device_status(unsigned* out, bool reset);
 
 // ---- adjoint.cu ----
 size_t adjoint_partials_count(const MeshDims& d);

@@ -387,6 +387,12 @@ class Engine:
         self._grad = None
         self._await_grad: dict[int, ForwardResult] = {}  # forward done, gradient pending
         self._grad_done: dict[int, tuple] = {}  # gradient done, forward pending
+        # host seconds of the serving loop by phase (admit: ICs + 2LPT + first force enqueued;
+        # tick: batched step launches; finalize: P(k) and copies enqueued; poll: results
+        # collected; idle: waits for the GPU, for arrivals or for gradients) and the number
+        # of loop passes in which an arrived request waited for its host tables
+        self.stats = dict(admit_s=0.0, tick_s=0.0, finalize_s=0.0, poll_s=0.0, idle_s=0.0, prep_waits=0,
+                          loop_passes=0)
 
     def capacity(self) -> dict:
         return {n: g.B for n, g in self.groups.items()}
@@ -498,7 +504,10 @@ class Engine:
         nxt = 0
         total = len(reqs)
         base = len(self.results)
+        st = self.stats
+        clock = time.perf_counter
         while len(self.results) - base < total:
+            st["loop_passes"] += 1
             t = now()
             while nxt < total and (not realtime or reqs[nxt].arrival <= t):
                 r = reqs[nxt]
@@ -506,10 +515,13 @@ class Engine:
                 waiting.append(r)
                 nxt += 1
             still = deque()
+            ta = clock()
             for r in waiting:
                 f = futures[r.rid]
                 g = self.groups[r.mesh]
                 if not g.has_room() or (f is not None and not f.done()):
+                    if g.has_room():
+                        st["prep_waits"] += 1
                     still.append(r)
                     continue
                 prep = f.result() if f is not None else prepare(r)
@@ -518,13 +530,22 @@ class Engine:
                 if r.want_grad:
                     self._grad.submit(r, prep)
             waiting = still
+            st["admit_s"] += clock() - ta
             ran = False
             for g in self.groups.values():
                 if g.n_active():
-                    for b in g.tick():
+                    t1 = clock()
+                    done = g.tick()
+                    t2 = clock()
+                    st["tick_s"] += t2 - t1
+                    for b in done:
                         self._finalize(g, b)
+                    st["finalize_s"] += clock() - t2
                     ran = True
+            tc = clock()
             self._poll(now)
+            st["poll_s"] += clock() - tc
+            tc = clock()
             if not ran:
                 if self._inflight:
                     self._inflight[0][0].synchronize()
@@ -534,6 +555,7 @@ class Engine:
                     time.sleep(max(0.0, min(0.002, reqs[nxt].arrival - now())))
                 elif waiting:
                     time.sleep(0.0002)
+            st["idle_s"] += clock() - tc
         return self.results
 
 
