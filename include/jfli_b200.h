@@ -172,6 +172,21 @@ int jfli_ic_filter(void* stream, const float* noise, float* out, const float* kt
 size_t jfli_lpt_workspace_bytes(int nx, int ny, int nz, int batch);
 int jfli_lpt(void* stream, const float* ic, int order, float c1x, float c2x, float c1p, float c2p, float* dx, float* p,
              void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* Light-cone-mode LPT (reference pm/lpt.py:110-130, the per-particle scale factors of
+ * utils.py:234-244 compute_particle_scale_factors): each particle takes
+ * a = a_of_chi(|x - observer|), x its Lagrangian grid point in Mpc/h ((i, j, k) L / N), and
+ *   dx = D1(a) F1 + 3/7 D2(a) F2,   p = a^2 E(a) (f1(a) D1(a) F1 + f2(a) 3/7 D2(a) F2)
+ * with F1, F2 the LPT forces at the grid points (as jfli_lpt). FP64 arithmetic from
+ * `tables` (device, FP64): [chi | a(chi)] of n_chi points, chi ascending, then
+ * [a | D1 | f1 | D2 | f2] of n_g points (linear interpolation with end extrapolation, D1
+ * clipped to [0, 1]); `background` (host, 5 doubles): Omega_m, Omega_k, Omega_de, w0, wa
+ * for E(a). a_out (optional, [batch][nx][ny][nz]) receives each particle's a.
+ * Workspace: jfli_lpt_lightcone_workspace_bytes. */
+size_t jfli_lpt_lightcone_workspace_bytes(int nx, int ny, int nz, int batch);
+int jfli_lpt_lightcone(void* stream, const float* ic, int order, const double* tables, int n_chi, int n_g,
+                       const double* background, float lx, float ly, float lz, float ox, float oy, float oz, float* dx,
+                       float* p, float* a_out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
+                       int batch, char* err, size_t errlen);
 
 /* P(k) sums over the full Fourier grid of `mesh` (ortho normalisation), binned with
  * numpy.digitize(|k|, kedges). out[batch][3][nedges+1] (FP64): sum |delta_k|^2, mode

@@ -130,6 +130,10 @@ _SIGNATURES = {
     "jfli_sht_alm2map": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
     "jfli_sht_alm2cl": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, *_ERR]),
     "jfli_set_fft_x_pass": (c_int, [c_int, *_ERR]),
+    "jfli_lpt_lightcone_workspace_bytes": (c_size_t, _DIMS),
+    "jfli_lpt_lightcone": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_void_p, c_float, c_float,
+                                   c_float, c_float, c_float, c_float, c_void_p, c_void_p, c_void_p, c_void_p,
+                                   c_size_t, *_DIMS, *_ERR]),
     "jfli_device_status": (c_int, [c_void_p, c_int, *_ERR]),
     "jfli_poisson_force": (c_int, [c_void_p, c_void_p, c_float, c_int, c_float, c_void_p, c_void_p, c_void_p,
                                    c_size_t, *_DIMS, *_ERR]),

@@ -390,6 +390,64 @@ int jfli_lpt(void* stream, const float* ic, int order, float c1x, float c2x, flo
   return cuda_status(e, err, errlen, "jfli_lpt");
 }
 
+int jfli_lpt_lightcone(void* stream, const float* ic, int order, const double* tables, int n_chi, int n_g,
+                       const double* background, float lx, float ly, float lz, float ox, float oy, float oz, float* dx,
+                       float* p, float* a_out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
+                       int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_STENCIL(nx, ny, nz);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(ic);
+  CHECK_PTR(tables);
+  CHECK_PTR(background);
+  CHECK_PTR(dx);
+  CHECK_PTR(p);
+  CHECK_PTR(workspace);
+  if (order != 1 && order != 2) return fail(err, errlen, JFLI_EINVAL, "LPT order must be 1 or 2, got %d", order);
+  if (n_chi < 2 || n_g < 2) return fail(err, errlen, JFLI_EINVAL, "tables need at least 2 points");
+  const MeshDims d{nx, ny, nz, batch};
+  // F1 (and F2) need a mesh of three components each beyond the LPT workspace
+  const size_t need = jfli_lpt_workspace_bytes(nx, ny, nz, batch) + align256(sizeof(float) * 3 * (size_t)d.cells() * batch);
+  if (workspace_bytes < need)
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  cudaStream_t s = (cudaStream_t)stream;
+  char* w = (char*)workspace;
+  float2* spec = (float2*)w;
+  float* pot = (float*)(w + spec_bytes(d));
+  float* src = (float*)(w + spec_bytes(d) + mesh_bytes(d));
+  float* f2 = (float*)(w + spec_bytes(d) + 2 * mesh_bytes(d));
+  float* f1 = (float*)(w + jfli_lpt_workspace_bytes(nx, ny, nz, batch));
+  cudaError_t e = jfli::poisson_potential(ic, spec, pot, d, 0.0f, 1.0f, s);
+  if (e == cudaSuccess) e = jfli::grid_gradient(pot, f1, 1.0f, 0, d, s);
+  if (e == cudaSuccess && order == 2) {
+    e = jfli::lpt2_source(pot, src, d, s);
+    if (e == cudaSuccess) e = jfli::poisson_potential(src, spec, pot, d, 0.0f, 1.0f, s);
+    if (e == cudaSuccess) e = jfli::grid_gradient(pot, f2, 1.0f, 0, d, s);
+  }
+  jfli::LptLightcone lc;
+  lc.tables = tables;
+  lc.n_chi = n_chi;
+  lc.n_g = n_g;
+  lc.box[0] = lx;
+  lc.box[1] = ly;
+  lc.box[2] = lz;
+  lc.obs[0] = ox;
+  lc.obs[1] = oy;
+  lc.obs[2] = oz;
+  lc.om = background[0];
+  lc.ok = background[1];
+  lc.ode = background[2];
+  lc.w0 = background[3];
+  lc.wa = background[4];
+  if (e == cudaSuccess) e = jfli::lpt_combine_lightcone(f1, order == 2 ? f2 : nullptr, dx, p, a_out, lc, d, s);
+  return cuda_status(e, err, errlen, "jfli_lpt_lightcone");
+}
+
+size_t jfli_lpt_lightcone_workspace_bytes(int nx, int ny, int nz, int batch) {
+  const MeshDims d{nx, ny, nz, batch};
+  return jfli_lpt_workspace_bytes(nx, ny, nz, batch) + align256(sizeof(float) * 3 * (size_t)d.cells() * batch);
+}
+
 size_t jfli_power_spectrum_workspace_bytes(int nx, int ny, int nz, int batch, int nedges) {
   const MeshDims d{nx, ny, nz, batch};
   const size_t partial = (size_t)jfli::x_pass_ctas(d) * batch * 3 * (nedges + 1) * sizeof(double);

@@ -82,6 +82,17 @@ struct DriftTables {
   int n_d;
 };
 
+// Light-cone-mode LPT: FP64 tables packed as [chi | a_chi] (n_chi each; chi ascending)
+// then [ga | D1 | f1 | D2 | f2] (n_g each), and the background for E(a).
+struct LptLightcone {
+  const double* tables;
+  int n_chi, n_g;
+  double box[3], obs[3];
+  double om, ok, ode, w0, wa;
+};
+cudaError_t lpt_combine_lightcone(const float* f1, const float* f2, float* dx, float* p, float* a_out,
+                                  const LptLightcone& lc, const MeshDims& d, cudaStream_t s);
+
 constexpr int kMaxTiles = 27;
 
 cudaError_t lightcone_drift(const float* disp, const float* vel, float* out, const float* box, const float* observer,

@@ -52,4 +52,88 @@ cudaError_t lightcone_drift(const float* disp, const float* vel, float* out, con
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------------
+// Light-cone-mode LPT (reference pm/lpt.py:110-130 with utils.py:234-244): every particle
+// takes the scale factor of its own light-cone crossing, a = a_of_chi(|x - observer|) with
+// x its Lagrangian grid point in Mpc/h, and the LPT growth coefficients at that a:
+//   dx = D1(a) F1 + 3/7 D2(a) F2,  p = a^2 E(a) (f1(a) D1(a) F1 + f2(a) 3/7 D2(a) F2)
+// (jaxpm lpt with an array of scale factors). F1, F2 are the first- and second-order LPT
+// forces at the grid points. All of it in FP64 from the host's FP64 tables, interpolated
+// as the host functions do (a_of_chi on the 256-point distance table; D1 clipped to
+// [0, 1], f1, D2, f2 on the 128-point growth table; E(a) in closed form).
+__device__ __forceinline__ double interp_table_f64(double x, const double* xp, const double* fp, int n) {
+  int lo = 0, hi = n;  // first index with xp[i] >= x (searchsorted, side="left")
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (xp[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  int i = lo - 1;
+  i = i < 0 ? 0 : (i > n - 2 ? n - 2 : i);
+  return fp[i] + (x - xp[i]) * ((fp[i + 1] - fp[i]) / (xp[i + 1] - xp[i]));
+}
+
+__global__ void k_lpt_combine_lightcone(const float* __restrict__ f1, const float* __restrict__ f2,
+                                        float* __restrict__ dx, float* __restrict__ pv, float* __restrict__ a_out,
+                                        LptLightcone lc, PGrid g) {
+  const long long b = blockIdx.y;
+  f1 += b * g.np * 3;
+  if (f2) f2 += b * g.np * 3;
+  dx += b * g.np * 3;
+  pv += b * g.np * 3;
+  if (a_out) a_out += b * g.np;
+  const int nc = lc.n_chi, ng = lc.n_g;
+  const double* chi = lc.tables;
+  const double* a_chi = chi + nc;
+  const double* ga = a_chi + nc;
+  const double* gg = ga + ng;
+  const double* gf = gg + ng;
+  const double* g2 = gf + ng;
+  const double* f2t = g2 + ng;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    int i, j, k;
+    particle_ijk(g, p, i, j, k);
+    const double x = (double)i / g.nx * lc.box[0] - lc.obs[0];
+    const double y = (double)j / g.ny * lc.box[1] - lc.obs[1];
+    const double z = (double)k / g.nz * lc.box[2] - lc.obs[2];
+    const double r = sqrt(x * x + y * y + z * z);
+    const double a = interp_table_f64(r, chi, a_chi, nc);
+    const double d1 = fmin(fmax(interp_table_f64(a, ga, gg, ng), 0.0), 1.0);
+    const double rate1 = interp_table_f64(a, ga, gf, ng);
+    const double d2 = interp_table_f64(a, ga, g2, ng);
+    const double rate2 = interp_table_f64(a, ga, f2t, ng);
+    double de;
+    if (lc.wa == 0.0)
+      de = lc.ode * pow(a, -3.0 * (1.0 + lc.w0));
+    else
+      de = lc.ode * pow(a, -3.0 * (1.0 + lc.w0 + lc.wa) + 3.0 * lc.wa * (a - 1.0) / log(a));
+    const double e = sqrt(lc.om / (a * a * a) + lc.ok / (a * a) + de);
+    const double c1x = d1, c2x = 3.0 / 7.0 * d2, c1p = a * a * rate1 * e, c2p = a * a * rate2 * e;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double u = f1[3ull * p + c];
+      double xv = c1x * u;
+      double vv = c1p * xv;
+      if (f2) {
+        const double x2 = c2x * (double)f2[3ull * p + c];
+        xv += x2;
+        vv += c2p * x2;
+      }
+      dx[3ull * p + c] = (float)xv;
+      pv[3ull * p + c] = (float)vv;
+    }
+    if (a_out) a_out[p] = (float)a;
+  }
+}
+
+cudaError_t lpt_combine_lightcone(const float* f1, const float* f2, float* dx, float* p, float* a_out,
+                                  const LptLightcone& lc, const MeshDims& d, cudaStream_t s) {
+  k_lpt_combine_lightcone<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(f1, f2, dx, p, a_out, lc,
+                                                                                          make_pgrid(d));
+  note_launch();
+  return cudaGetLastError();
+}
+
 }  // namespace jfli

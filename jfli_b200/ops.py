@@ -217,6 +217,33 @@ def ic_filter(noise: torch.Tensor, ktab: torch.Tensor, ptab: torch.Tensor, box_s
     return out
 
 
+def lpt_lightcone(ic: torch.Tensor, order: int, cosmo, box_size, observer_mpc):
+    """(displacement, momentum, scale factor) particle grids of light-cone-mode LPT: every
+    particle at the scale factor of its Lagrangian grid point's light-cone crossing
+    (jfli_lpt_lightcone), from the cosmology's FP64 distance and growth tables."""
+    import numpy as np
+
+    from . import cosmology as cj
+
+    _check(ic, "ic")
+    (nx, ny, nz), batch, lead = _mesh_dims(ic, False)
+    dt = cj.distance_table(cosmo)
+    gt = cj.growth_table(cosmo)
+    tables = np.concatenate([dt.chi[::-1], dt.a[::-1], gt.a, gt.g, gt.f, gt.g2, gt.f2]).astype(np.float64)
+    tab = torch.as_tensor(tables, device=ic.device)
+    bg = (ctypes.c_double * 5)(cosmo.Omega_m, cosmo.Omega_k, cosmo.Omega_de, cosmo.w0, cosmo.wa)
+    dx = torch.empty((*lead, nx, ny, nz, 3), dtype=torch.float32, device=ic.device)
+    p = torch.empty_like(dx)
+    a = torch.empty((*lead, nx, ny, nz), dtype=torch.float32, device=ic.device)
+    nb = query("jfli_lpt_lightcone_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "lpt_lightcone", ic.device)
+    lx, ly, lz = (float(v) for v in box_size)
+    ox, oy, oz = (float(v) for v in observer_mpc)
+    call("jfli_lpt_lightcone", stream_ptr(), ptr(ic), int(order), ptr(tab), len(dt.chi), len(gt.a), bg, lx, ly, lz,
+         ox, oy, oz, ptr(dx), ptr(p), ptr(a), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return dx, p, a
+
+
 def lpt(ic: torch.Tensor, order: int, c1x: float, c2x: float, c1p: float, c2p: float,
         dx: torch.Tensor | None = None, p: torch.Tensor | None = None):
     """(displacement, momentum) particle grids; written into dx / p when given."""

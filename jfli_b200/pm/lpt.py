@@ -89,7 +89,7 @@ def lpt(cosmo, initial_field: DensityField, *, ts=None, nb_shells=None, density_
         cosmo, initial_field, painting=painting, ts=ts, nb_shells=nb_shells, density_widths=density_widths,
         equal_vol=equal_vol, min_width=min_width)
     if is_lightcone:
-        raise NotImplementedError("lightcone-mode LPT (per-particle scale factors) is not on the B200 path")
+        return _lpt_lightcone(cosmo, initial_field, order, painting, r_centers, widths)
     if painting.target not in ("particles", "density"):
         raise ValueError(
             f"Painting target {painting.target} is incompatible with snapshot mode. Use 'particles' or 'density'.")
@@ -110,6 +110,65 @@ def lpt(cosmo, initial_field: DensityField, *, ts=None, nb_shells=None, density_
     dx_field = ParticleField.FromDensityMetadata(array=dx, field=initial_field, **meta)
     p_field = ParticleField.FromDensityMetadata(array=p, field=initial_field, **meta)
     if painting.target == "density":
+        dx_field = dx_field.paint(weights=painting.weights, chunk_size=painting.chunk_size,
+                                  batch_size=painting.batch_size)
+    return dx_field, p_field
+
+
+def _device_interp(x: torch.Tensor, xp: np.ndarray, fp: np.ndarray) -> torch.Tensor:
+    """The host `interp` (linear, end extrapolation, searchsorted side="left") on a device
+    tensor, in FP64."""
+    xpt = torch.as_tensor(np.asarray(xp, np.float64), device=x.device)
+    fpt = torch.as_tensor(np.asarray(fp, np.float64), device=x.device)
+    xd = x.double()
+    i = (torch.searchsorted(xpt, xd.contiguous(), side="left") - 1).clamp(0, xpt.numel() - 2)
+    slope = (fpt[i + 1] - fpt[i]) / (xpt[i + 1] - xpt[i])
+    return fpt[i] + (xd - xpt[i]) * slope
+
+
+def _lpt_lightcone(cosmo, initial_field, order, painting, r_centers, widths):
+    """Light-cone-mode LPT (reference pm/lpt.py:110-213): each particle at the scale factor
+    of its own light-cone crossing (compute_particle_scale_factors, utils.py:234-244), then
+    the lightcone painted as the painting target asks (spherical shells or flat planes at
+    the shell centres, a density, or the particles themselves). The fields carry the
+    per-particle scale factors, shape (..., nx, ny, nz, 1), as the reference's do."""
+    ic = initial_field.array.contiguous()
+    if torch.is_grad_enabled() and ic.requires_grad:
+        raise NotImplementedError("gradients through light-cone-mode LPT are not on the B200 path")
+    dx, p, a = ops.lpt_lightcone(ic, order, cosmo, initial_field.box_size, initial_field.observer_position_mpc)
+    a = a[..., None]
+    dt = cj.distance_table(cosmo)
+    chi = _device_interp(a, dt.a, dt.chi).clamp(0.0, 1e6).float()
+    meta = dict(status=FieldStatus.LIGHTCONE, scale_factors=a, comoving_centers=chi, z_sources=1.0 / a - 1.0,
+                unit=PositionUnit.GRID_RELATIVE)
+    dx_field = ParticleField.FromDensityMetadata(array=dx, field=initial_field, **meta)
+    p_field = ParticleField.FromDensityMetadata(array=p, field=initial_field, **meta)
+    target = painting.target if painting is not None else "particles"
+    if target in ("flat", "spherical"):
+        if target == "flat":
+            res = dx_field.paint_2d(center=r_centers, density_plane_width=widths, weights=painting.weights,
+                                    batch_size=painting.batch_size)
+        else:
+            res = dx_field.paint_spherical(center=r_centers, density_plane_width=widths, scheme=painting.scheme,
+                                           weights=painting.weights, kernel_width_arcmin=painting.kernel_width_arcmin,
+                                           smoothing_interpretation=painting.smoothing_interpretation,
+                                           paint_nside=painting.paint_nside, ud_grade_power=painting.ud_grade_power,
+                                           ud_grade_order_in=painting.ud_grade_order_in,
+                                           ud_grade_order_out=painting.ud_grade_order_out,
+                                           ud_grade_pess=painting.ud_grade_pess, batch_size=painting.batch_size)
+        a_snap = np.asarray(cj.a_of_chi(cosmo, np.asarray(r_centers, np.float64)), np.float64)
+        res = res.replace(scale_factors=a_snap, z_sources=cj.a2z(a_snap))
+        if res.is_batched():  # the reference returns the shells reversed: res[::-1]
+            res = res.replace(array=res.array.flip(0), scale_factors=a_snap[::-1].copy(),
+                              z_sources=cj.a2z(a_snap)[::-1].copy(),
+                              comoving_centers=np.asarray(res.comoving_centers)[::-1].copy()
+                              if np.ndim(res.comoving_centers) else res.comoving_centers,
+                              density_width=np.asarray(res.density_width)[::-1].copy()
+                              if np.ndim(res.density_width) else res.density_width)
+        dx_field = res
+    elif target not in ("density", "particles"):
+        raise ValueError(f"Unknown painting target {target}.")
+    if target == "density":
         dx_field = dx_field.paint(weights=painting.weights, chunk_size=painting.chunk_size,
                                   batch_size=painting.batch_size)
     return dx_field, p_field

@@ -209,6 +209,47 @@ def ic_filter(noise, box, ktab, ptab, zero_mode_one=False, dtype=np.float64):
 
 
 # ------------------------------------------------------------------------------------ LPT
+def lpt_forces(ic, order=1, dtype=np.float64):
+    """(F1, F2) of JaxPM lpt at the grid points: the first-order force -grad_FD laplace^-1 ic
+    and, for order 2, the force of the second-order source sum_{i<j} phi_ii phi_jj - phi_ij^2
+    (F2 None for order 1)."""
+    ic = ic.astype(dtype)
+    zeros = np.zeros(ic.shape + (3,), dtype)
+    delta_k = fft3(ic)
+    F1 = forces_from_delta_k(delta_k, zeros, dtype)
+    if order != 2:
+        return F1, None
+    kvec = fftk(ic.shape, dtype)
+    pot_k = potential_k(delta_k, kvec)
+    delta2 = 0
+    shear_acc = 0
+    for i in range(3):
+        shear_ii = ifft3(gradient_kernel(kvec, i) ** 2 * pot_k).real
+        delta2 = delta2 + shear_ii * shear_acc
+        shear_acc = shear_acc + shear_ii
+        for j in range(i + 1, 3):
+            delta2 = delta2 - ifft3(gradient_kernel(kvec, i) * gradient_kernel(kvec, j) * pot_k).real ** 2
+    return F1, forces_from_delta_k(fft3(delta2), zeros, dtype)
+
+
+def lpt_lightcone(ic, order, box, observer, a_of_chi, coefficients, dtype=np.float64):
+    """Light-cone-mode LPT (reference pm/lpt.py:110-130, utils.py:234-244): every particle
+    at a = a_of_chi(|x - observer|), x its grid point in Mpc/h, with the LPT coefficients
+    (c1x, c2x, c1p, c2p) = coefficients(a) (arrays); returns (dx, p, a)."""
+    F1, F2 = lpt_forces(ic, order, dtype)
+    shape = ic.shape
+    x = grid(shape) / np.asarray(shape, np.float64) * np.asarray(box, np.float64)
+    a = a_of_chi(np.linalg.norm(x - np.asarray(observer, np.float64), axis=-1))
+    c1x, c2x, c1p, c2p = (np.asarray(c, np.float64)[..., None] for c in coefficients(a))
+    dx = c1x * F1
+    p = c1p * dx
+    if F2 is not None:
+        dx2 = c2x * F2
+        dx = dx + dx2
+        p = p + c2p * dx2
+    return dx.astype(dtype), p.astype(dtype), a
+
+
 def lpt(ic, c1x, c2x, c1p, c2p, order=1, dtype=np.float64):
     """JaxPM lpt at the grid points: dx = c1x F1 (+ c2x F2), p = c1p c1x F1 (+ c2p c2x F2)."""
     ic = ic.astype(dtype)
