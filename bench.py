@@ -349,9 +349,10 @@ def pk_vs_oracle(pk, n, box):
         return {}
     ref = np.load(path)
     p = np.asarray(pk, np.float64)
-    return {"pk_err_vs_fp64_oracle": float(np.abs(p / ref["pk_f64"] - 1).max()),
-            "pk_err_vs_fp32_oracle": float(np.abs(p / ref["pk_f32"] - 1).max()),
-            "pk_gap_fp32_vs_fp64_oracle": float(ref["gap_pk_f32"])}
+    ok = ref["pk_f64"] > 0  # bins that hold modes (an empty bin is 0/0, as in the reference)
+    return {"pk_err_vs_fp64_oracle": float(np.abs(p[ok] / ref["pk_f64"][ok] - 1).max()),
+            "pk_err_vs_fp32_oracle": float(np.abs(p[ok] / ref["pk_f32"][ok] - 1).max()),
+            "pk_gap_fp32_vs_fp64_oracle": float(ref["gap_pk_f32"]), "pk_bins_compared": int(ok.sum())}
 
 
 def run_shells(args, cosmo, n, box):

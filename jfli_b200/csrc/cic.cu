@@ -225,24 +225,11 @@ __device__ __forceinline__ void deposit_carried(float* rho, const PGrid& g, cons
   c.valid = true;
 }
 
-// One particle of the fused pass. Order inside: kick (with the force at the current
-// position) -> drift (with the kicked velocity) -> paint (at the new position). Positions
-// and velocities stream through once per pass: streaming (evict-first) loads and stores,
-// so that they do not push the force and density meshes out of L2. With a carry (the
-// brick walk) the deposit holds back the upper-x plane for the lane's next particle.
-template <bool kCarry>
-__device__ __forceinline__ void kdp_particle(float* __restrict__ disp, float* __restrict__ vel,
-                                             const float* __restrict__ force, float kick, float drift, int flags,
-                                             float weight, float* __restrict__ rho, const PGrid& g, unsigned p, int i,
-                                             int j, int k, XCarry& carry) {
-  float x0 = __ldcs(disp + 3 * p + 0), x1 = __ldcs(disp + 3 * p + 1), x2 = __ldcs(disp + 3 * p + 2);
-  const bool use_v = flags & (kStepKick | kStepDrift);
-  float v0 = 0.f, v1 = 0.f, v2 = 0.f;
-  if (use_v) {
-    v0 = __ldcs(vel + 3 * p + 0);
-    v1 = __ldcs(vel + 3 * p + 1);
-    v2 = __ldcs(vel + 3 * p + 2);
-  }
+// Kick (with the CIC readout of the force mesh at the current position), drift (with the
+// kicked velocity) of one particle held in registers; `flags` as for the fused pass.
+__device__ __forceinline__ void kdp_update(const float* __restrict__ force, float kick, float drift, int flags,
+                                           const PGrid& g, int i, int j, int k, float& x0, float& x1, float& x2,
+                                           float& v0, float& v1, float& v2) {
   if (flags & (kStepKick | kStepCorrect)) {
     const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
     float fx, fy, fz;
@@ -251,9 +238,6 @@ __device__ __forceinline__ void kdp_particle(float* __restrict__ disp, float* __
       v0 += fx * kick;
       v1 += fy * kick;
       v2 += fz * kick;
-      __stcs(vel + 3 * p + 0, v0);
-      __stcs(vel + 3 * p + 1, v1);
-      __stcs(vel + 3 * p + 2, v2);
     } else {
       x0 += fx * kick;
       x1 += fy * kick;
@@ -265,6 +249,30 @@ __device__ __forceinline__ void kdp_particle(float* __restrict__ disp, float* __
     x1 += v1 * drift;
     x2 += v2 * drift;
   }
+}
+
+// One particle of the fused pass in the grid-stride walk. Order inside: kick -> drift ->
+// paint (at the new position). Positions and velocities stream through once per pass:
+// streaming (evict-first) loads and stores, so that they do not push the force and
+// density meshes out of L2.
+__device__ __forceinline__ void kdp_particle(float* __restrict__ disp, float* __restrict__ vel,
+                                             const float* __restrict__ force, float kick, float drift, int flags,
+                                             float weight, float* __restrict__ rho, const PGrid& g, unsigned p, int i,
+                                             int j, int k) {
+  float x0 = __ldcs(disp + 3 * p + 0), x1 = __ldcs(disp + 3 * p + 1), x2 = __ldcs(disp + 3 * p + 2);
+  const bool use_v = flags & (kStepKick | kStepDrift);
+  float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+  if (use_v) {
+    v0 = __ldcs(vel + 3 * p + 0);
+    v1 = __ldcs(vel + 3 * p + 1);
+    v2 = __ldcs(vel + 3 * p + 2);
+  }
+  kdp_update(force, kick, drift, flags, g, i, j, k, x0, x1, x2, v0, v1, v2);
+  if (flags & kStepKick) {
+    __stcs(vel + 3 * p + 0, v0);
+    __stcs(vel + 3 * p + 1, v1);
+    __stcs(vel + 3 * p + 2, v2);
+  }
   if (flags & (kStepDrift | kStepCorrect)) {
     __stcs(disp + 3 * p + 0, x0);
     __stcs(disp + 3 * p + 1, x1);
@@ -272,10 +280,58 @@ __device__ __forceinline__ void kdp_particle(float* __restrict__ disp, float* __
   }
   if (flags & kStepPaint) {
     const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
-    if (kCarry)
-      deposit_carried(rho, g, cx, cy, cz, weight, carry);
-    else
-      deposit_lane_merged(rho, g, cx, cy, cz, weight);
+    deposit_lane_merged(rho, g, cx, cy, cz, weight);
+  }
+}
+
+// The 32 particles of one z row of the brick walk: their positions (and velocities) are
+// 384 contiguous, 16-byte aligned bytes per array. Lanes 0..23 move them as float4 with
+// streaming loads and stores through the warp's shared buffers (24 float4 per array), and
+// every lane reads or writes its own 3 floats there (stride 3: no bank conflicts). A warp
+// thus issues one 16-byte load and one store per array and row instead of three 4-byte
+// ones, each touching 12 sectors. The deposit holds back the upper-x plane for the lane's
+// next particle (deposit_carried).
+__device__ __forceinline__ void kdp_brick_row(float* __restrict__ disp, float* __restrict__ vel,
+                                              const float* __restrict__ force, float kick, float drift, int flags,
+                                              float weight, float* __restrict__ rho, const PGrid& g, unsigned p0, int i,
+                                              int j, int k, int lane, float4* bx, float4* bv, XCarry& carry) {
+  const bool use_v = flags & (kStepKick | kStepDrift);
+  const float4* xr = reinterpret_cast<const float4*>(disp + 3ull * p0);
+  const float4* vr = reinterpret_cast<const float4*>(vel + 3ull * p0);
+  if (lane < 24) {
+    const float4 a = __ldcs(xr + lane);
+    float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (use_v) c = __ldcs(vr + lane);
+    bx[lane] = a;
+    bv[lane] = c;
+  }
+  __syncwarp();
+  const float* fx = reinterpret_cast<const float*>(bx);
+  const float* fv = reinterpret_cast<const float*>(bv);
+  float x0 = fx[3 * lane], x1 = fx[3 * lane + 1], x2 = fx[3 * lane + 2];
+  float v0 = fv[3 * lane], v1 = fv[3 * lane + 1], v2 = fv[3 * lane + 2];
+  __syncwarp();
+  kdp_update(force, kick, drift, flags, g, i, j, k, x0, x1, x2, v0, v1, v2);
+  const bool store_v = flags & kStepKick, store_x = flags & (kStepDrift | kStepCorrect);
+  if (store_v || store_x) {
+    float* wx = reinterpret_cast<float*>(bx);
+    float* wv = reinterpret_cast<float*>(bv);
+    wx[3 * lane] = x0;
+    wx[3 * lane + 1] = x1;
+    wx[3 * lane + 2] = x2;
+    wv[3 * lane] = v0;
+    wv[3 * lane + 1] = v1;
+    wv[3 * lane + 2] = v2;
+    __syncwarp();
+    if (lane < 24) {
+      if (store_x) __stcs(reinterpret_cast<float4*>(disp + 3ull * p0) + lane, bx[lane]);
+      if (store_v) __stcs(reinterpret_cast<float4*>(vel + 3ull * p0) + lane, bv[lane]);
+    }
+    __syncwarp();
+  }
+  if (flags & kStepPaint) {
+    const Cic1 cx = cic_rel(i, x0, g.nx), cy = cic_rel(j, x1, g.ny), cz = cic_rel(k, x2, g.nz);
+    deposit_carried(rho, g, cx, cy, cz, weight, carry);
   }
 }
 
@@ -304,7 +360,9 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
   vel += b * g.np * 3;
   if (force) force += b * g.np * 4;
   if (rho) rho += b * g.np;
-  if (blockDim.x == kBrickY * kBrickZ && g.nz % kBrickZ == 0 && g.ny % kBrickY == 0) {
+  __shared__ float4 rowbuf[kBrickY][2][24];  // per warp: positions, velocities of one z row
+  if (blockDim.x == kBrickY * kBrickZ && g.nz % kBrickZ == 0 && g.ny % kBrickY == 0 &&
+      ((reinterpret_cast<uintptr_t>(disp) | reinterpret_cast<uintptr_t>(vel)) & 15) == 0) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int tz = g.nz / kBrickZ, ty = g.ny / kBrickY, txc = (g.nx + kBrickX - 1) / kBrickX;
     const long long items = (long long)tz * ty * txc;
@@ -317,8 +375,9 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
       XCarry carry;
       carry.valid = false;
       for (int i = xc * kBrickX; i < i1; ++i) {
-        const unsigned p = ((unsigned)i * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)k;
-        kdp_particle<true>(disp, vel, force, kick, drift, flags, weight, rho, g, p, i, j, k, carry);
+        const unsigned p0 = ((unsigned)i * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)(k - lane);
+        kdp_brick_row(disp, vel, force, kick, drift, flags, weight, rho, g, p0, i, j, k, lane, rowbuf[w][0],
+                      rowbuf[w][1], carry);
       }
       // every lane of the warp ran the same planes: the carries go out together, z-merged
       deposit_plane_merged(rho, carry.valid, carry.xo, carry.yo0, carry.yo1, carry.z0, carry.z1, carry.w00,
@@ -326,12 +385,10 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
     }
     return;
   }
-  XCarry none;
-  none.valid = false;
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
     particle_ijk(g, p, i, j, k);
-    kdp_particle<false>(disp, vel, force, kick, drift, flags, weight, rho, g, p, i, j, k, none);
+    kdp_particle(disp, vel, force, kick, drift, flags, weight, rho, g, p, i, j, k);
   }
 }
 
