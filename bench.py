@@ -13,10 +13,10 @@ schedule restarts from the initial conditions inside the timed region.
   e2e   : the same metric through the public API (jfli_b200.interpolate_initial_conditions
           -> lpt -> nbody -> power) from pinned host white noise to host density + P(k),
           40 KDK steps per request, copies inside the timed region
-  roofline : the fused particle pass (k_kick_drift_paint), algorithmic bytes
-          48 B/particle (read+write position and velocity) + 20 B/cell (float4 force mesh
-          read, density written) per launch, over its CUDA-event time, against
-          MEASURED_PEAKS.json
+  roofline : the particle pass call (density clear + k_kick_drift_paint), algorithmic
+          bytes 48 B/particle (read+write position and velocity) + 20 B/cell (the three
+          force components read, the density zeroed and written) per call, over its
+          CUDA-event time, against MEASURED_PEAKS.json
   cpu_baseline : the FP32 oracle port of the same steps (oracle/pm.py with the C/OpenMP
           CIC of oracle/cic.c) on this host, a bounded sample of the schedule
   serving : the request stream (512 Poisson arrivals over mesh 64/96/128/192, 10-40 KDK
@@ -77,6 +77,10 @@ def parse():
     ap.add_argument("--lightcone", type=int, default=0,
                     help="instead of the step benchmark, run the large light-cone chain at this mesh size "
                          "(box 1000 Mpc/h, 2LPT, 60 KDK steps with PGD, 16 shells at nside 1024, Born)")
+    ap.add_argument("--xpass", type=int, default=0,
+                    help="instead of the step benchmark, run the Poisson chain on a seeded density of this mesh size "
+                         "twice with the register x pass and twice with the TMA-staged one (a short case to profile "
+                         "the two x-pass kernels) and print their CUDA-event times")
     ap.add_argument("--tiled-paint", type=int, default=0,
                     help="instead of the step benchmark, time the 27-replica light-cone paint of one shell "
                          "(this many particles per side, box 500 Mpc/h, shell 653-747 Mpc/h, nside 1024)")
@@ -168,7 +172,7 @@ def run_gpu(args, world, rank):
 
     import jfli_b200 as jf
     from jfli_b200 import ops
-    from jfli_b200._lib import JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
+    from jfli_b200._lib import JFLI_STEP_CLEAR, JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
     from jfli_b200.pm.solvers import EfficientDriftDoubleKick as EDK
 
     n = args.mesh
@@ -187,7 +191,7 @@ def run_gpu(args, world, rank):
     sched = [(e[1], e[2]) for e in time_events(0.1, [1.0], dt0) if e[0] == "step"]
     coeffs = [EDK.step_coefficients(cosmo, a, b, dt0) for a, b in sched]
     init_kick = EDK.init_kick(cosmo, 0.1, 0.1 + dt0)
-    flags = JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT
+    flags = JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT | JFLI_STEP_CLEAR
     stream = torch.cuda.current_stream()
     x0, v0 = x.clone(), v.clone()
     st = {"idx": 0, "pending": init_kick}
@@ -196,18 +200,16 @@ def run_gpu(args, world, rank):
         """Back to the 2LPT initial conditions: first force evaluation and pending kick."""
         x.copy_(x0)
         v.copy_(v0)
-        rho.zero_()
-        ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT, rho)
-        ops.poisson_force(rho, 1.0, out=force, pot=pot, clear=True)
+        ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT | JFLI_STEP_CLEAR, rho)
+        ops.poisson_force(rho, 1.0, out=force, pot=pot)
         st["idx"], st["pending"] = 0, init_kick
 
     restart()
 
     def one_step(timed_kdp=None):
-        """Step idx of the schedule: kick (previous force) + drift + paint, then the new
-        force meshes (the forward FFT clears the density mesh for the next paint); after
-        the last step of the schedule the next call restarts from the initial conditions
-        (the restart is inside the timed region)."""
+        """Step idx of the schedule: clear the density mesh, kick (previous force) + drift +
+        paint, then the new force meshes; after the last step of the schedule the next call
+        restarts from the initial conditions (the restart is inside the timed region)."""
         c = coeffs[st["idx"]]
         if timed_kdp is not None:
             e0 = torch.cuda.Event(enable_timing=True)
@@ -218,7 +220,7 @@ def run_gpu(args, world, rank):
             timed_kdp.append((e0, e1))
         else:
             ops.kick_drift_paint(x, v, force, st["pending"], c.drift, flags, rho)
-        ops.poisson_force(rho, 1.0, out=force, pot=pot, clear=True)
+        ops.poisson_force(rho, 1.0, out=force, pot=pot)
         st["pending"] = c.kick
         st["idx"] += 1
         if st["idx"] == len(coeffs):
@@ -263,7 +265,9 @@ def run_gpu(args, world, rank):
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     kdp_avg_ms = statistics.mean(kdp)
-    alg_bytes = 68.0 * particles  # x, v read+write (48 B); float4 force mesh read (16 B); density written (4 B)
+    # the timed call clears the density mesh and runs the particle pass: x, v read and written
+    # (48 B), the three force components read (12 B), the density zeroed and written (8 B)
+    alg_bytes = 68.0 * particles
     achieved = alg_bytes / (kdp_avg_ms / 1e3) / 1e9
     roof = {"kernel": "k_kick_drift_paint", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": ncu_traffic(n),
@@ -671,7 +675,7 @@ def x_pass_variants(n, iters=20):
     try:
         for name, mode in (("register", 0), ("tma", 1)):
             call("jfli_set_fft_x_pass", mode)
-            for _ in range(3):
+            for _ in range(3 if iters > 2 else 0):
                 ops.poisson_potential(rho, 1.0, out=pot)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -823,6 +827,9 @@ def main():
         return
     if args.tiled_paint:
         run_tiled_paint(args)
+        return
+    if args.xpass:
+        print(json.dumps({"x_pass_variants": x_pass_variants(args.xpass, iters=2)}), flush=True)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -76,6 +76,7 @@ extern "C" {
 #define JFLI_STEP_PAINT 4  /* CIC deposit at the new position */
 #define JFLI_STEP_FORCE 8  /* (jfli_pm_step) solve the Poisson equation for the new positions */
 #define JFLI_STEP_CORRECT 16 /* x += F(x) * kick instead of a kick (PGD position correction) */
+#define JFLI_STEP_CLEAR 32 /* (jfli_kick_drift_paint) clear rho right before the pass paints into it */
 
 #define JFLI_HEALPIX_NGP 0
 #define JFLI_HEALPIX_BILINEAR 1
@@ -131,8 +132,9 @@ int jfli_force_mesh(void* stream, const float* pot, float scale, float* force, i
 /* Force meshes of a density: pot = jfli_poisson_potential(rho, rho_mean), then
  * force = jfli_force_mesh(pot, scale), in one call (the Poisson solve and gradient of
  * pm/solvers.py:19-32 _forces, jaxpm pm_forces, before the readout). With clear_rho != 0
- * the density mesh is set to 0 as the forward FFT reads it, ready for the next paint (the
- * fused step loop then needs no memset); pot must not alias rho then. Workspace:
+ * the density mesh is set to 0 as the forward FFT reads it, ready for a later paint; pot
+ * must not alias rho then. (A step loop does better with JFLI_STEP_CLEAR on the paint: the
+ * zeroed lines are then still in L2 when the deposits arrive.) Workspace:
  * jfli_poisson_workspace_bytes. */
 int jfli_poisson_force(void* stream, float* rho, float rho_mean, int clear_rho, float scale, float* pot, float* force,
                        void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
@@ -216,6 +218,16 @@ int jfli_power_poles(void* stream, const float* mesh, const float* mesh2, const 
 int jfli_healpix_paint(void* stream, const float* disp, int absolute, const float* weights, float weight, float lx,
                        float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside, int scheme,
                        float* map, int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* HEALPix shell painting with the "rbf_neighbor" scheme (reference
+ * _src/fields/_painting.py:18,291; its arithmetic lives in the absent jaxpm fork, so this
+ * is the library's own definition): each particle in rmin < r <= rmax deposits onto the 4
+ * pixels around its direction (those of the bilinear scheme), weighted by
+ * exp(-d^2 / (2 sigma^2)) of the angle d to each pixel centre and normalised to sum 1;
+ * sigma in radians, 0 < sigma < pi. Otherwise as jfli_healpix_paint. */
+int jfli_healpix_paint_rbf(void* stream, const float* disp, int absolute, const float* weights, float weight,
+                           float lx, float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside,
+                           float sigma, float* map, int accumulate, int nx, int ny, int nz, int batch, char* err,
+                           size_t errlen);
 
 /* HEALPix shell map of `ntiles` (<= 27) replicas of the particles, in one pass. For
  * replica i, with c = x - observer (x in Mpc/h from the grid index and disp):

@@ -28,6 +28,7 @@ JFLI_STEP_DRIFT = 2
 JFLI_STEP_PAINT = 4
 JFLI_STEP_FORCE = 8
 JFLI_STEP_CORRECT = 16
+JFLI_STEP_CLEAR = 32
 JFLI_HEALPIX_NGP = 0
 JFLI_HEALPIX_BILINEAR = 1
 
@@ -130,6 +131,9 @@ _SIGNATURES = {
     "jfli_sht_alm2map": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
     "jfli_sht_alm2cl": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, *_ERR]),
     "jfli_set_fft_x_pass": (c_int, [c_int, *_ERR]),
+    "jfli_healpix_paint_rbf": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_float,
+                                       c_float, c_float, c_float, c_float, c_float, c_int, c_float, c_void_p, c_int,
+                                       *_DIMS, *_ERR]),
     "jfli_lpt_lightcone_workspace_bytes": (c_size_t, _DIMS),
     "jfli_lpt_lightcone": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_void_p, c_float, c_float,
                                    c_float, c_float, c_float, c_float, c_void_p, c_void_p, c_void_p, c_void_p,

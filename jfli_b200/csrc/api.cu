@@ -233,7 +233,7 @@ int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* fo
   CHECK_DIMS(nx, ny, nz, batch);
   CHECK_PTR(disp);
   CHECK_PTR(vel);
-  if ((flags & ~(JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT | JFLI_STEP_CORRECT)) != 0)
+  if ((flags & ~(JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT | JFLI_STEP_CORRECT | JFLI_STEP_CLEAR)) != 0)
     return fail(err, errlen, JFLI_EINVAL, "unknown step flags 0x%x", flags);
   if ((flags & JFLI_STEP_KICK) && (flags & JFLI_STEP_CORRECT))
     return fail(err, errlen, JFLI_EINVAL, "KICK and CORRECT are exclusive");
@@ -241,9 +241,16 @@ int jfli_kick_drift_paint(void* stream, float* disp, float* vel, const float* fo
     return fail(err, errlen, JFLI_EINVAL, "kick requested without a force mesh");
   if (force) CHECK_ALIGN16(force);
   if ((flags & JFLI_STEP_PAINT) && !rho) return fail(err, errlen, JFLI_EINVAL, "paint requested without a mesh");
+  if ((flags & JFLI_STEP_CLEAR) && !(flags & JFLI_STEP_PAINT))
+    return fail(err, errlen, JFLI_EINVAL, "CLEAR needs PAINT");
   const MeshDims d{nx, ny, nz, batch};
-  return cuda_status(jfli::kick_drift_paint(disp, vel, force, kick, drift, flags, weight, rho, d, (cudaStream_t)stream),
-                     err, errlen, "jfli_kick_drift_paint");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaSuccess;
+  // cleared right before the pass, so the zeroed lines are still in L2 when the deposits arrive
+  if (flags & JFLI_STEP_CLEAR) e = jfli::zero_floats(rho, d.cells() * batch, s);
+  if (e == cudaSuccess)
+    e = jfli::kick_drift_paint(disp, vel, force, kick, drift, flags & ~JFLI_STEP_CLEAR, weight, rho, d, s);
+  return cuda_status(e, err, errlen, "jfli_kick_drift_paint");
 }
 
 size_t jfli_pm_step_workspace_bytes(int nx, int ny, int nz, int batch) {
@@ -272,7 +279,7 @@ int jfli_pm_step(void* stream, float* disp, float* vel, float kick, float drift,
   cudaStream_t s = (cudaStream_t)stream;
   float2* spec = (float2*)workspace;
   float* pot = (float*)((char*)workspace + spec_bytes(d));
-  cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
+  cudaError_t e = jfli::zero_floats(rho, d.cells() * batch, s);
   if (e == cudaSuccess)
     e = jfli::kick_drift_paint(disp, vel, force, kick, drift,
                                (flags & (JFLI_STEP_KICK | JFLI_STEP_DRIFT)) | JFLI_STEP_PAINT, 1.0f, rho, d, s);
@@ -303,7 +310,7 @@ int jfli_pm_step_slots(void* stream, float* disp, float* vel, const float* kicks
   cudaStream_t s = (cudaStream_t)stream;
   float2* spec = (float2*)workspace;
   float* pot = (float*)((char*)workspace + spec_bytes(d));
-  cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
+  cudaError_t e = jfli::zero_floats(rho, d.cells() * batch, s);
   if (e == cudaSuccess) e = jfli::kick_drift_paint_slots(disp, vel, force, kicks, drifts, slot_flags, 1.0f, rho, d, s);
   if (e == cudaSuccess) e = jfli::poisson_potential(rho, spec, pot, d, 1.0f, 1.0f, s);
   if (e == cudaSuccess) e = jfli::force_mesh(pot, force, 1.0f, d, s);
@@ -536,6 +543,29 @@ int jfli_healpix_paint(void* stream, const float* disp, int absolute, const floa
   return cuda_status(
       jfli::healpix_paint(disp, absolute, weights, weight, d, box, obs, rmin, rmax, nside, scheme, map, s), err,
       errlen, "jfli_healpix_paint");
+}
+
+int jfli_healpix_paint_rbf(void* stream, const float* disp, int absolute, const float* weights, float weight,
+                           float lx, float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside,
+                           float sigma, float* map, int accumulate, int nx, int ny, int nz, int batch, char* err,
+                           size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(map);
+  if (nside < 1 || nside > 8192) return fail(err, errlen, JFLI_EINVAL, "nside %d outside [1, 8192]", nside);
+  if (!(sigma > 0.f) || !(sigma < 3.2f)) return fail(err, errlen, JFLI_EINVAL, "kernel sigma must be in (0, pi) radians");
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!accumulate) {
+    cudaError_t e = cudaMemsetAsync(map, 0, (size_t)12 * nside * nside * batch * sizeof(float), s);
+    if (e != cudaSuccess) return cuda_status(e, err, errlen, "jfli_healpix_paint_rbf memset");
+  }
+  const float box[3] = {lx, ly, lz};
+  const float obs[3] = {ox, oy, oz};
+  return cuda_status(
+      jfli::healpix_paint(disp, absolute, weights, weight, d, box, obs, rmin, rmax, nside, 2, map, s, sigma), err,
+      errlen, "jfli_healpix_paint_rbf");
 }
 
 int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, const float* vel, const float* weights,
@@ -934,13 +964,15 @@ int jfli_kkd_run(void* stream, float* disp, float* vel, const float* kicks, cons
     return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, kkd_ws_bytes(d));
   cudaStream_t s = (cudaStream_t)stream;
   const KkdWs w = kkd_ws(workspace, d);
-  // rho enters every step cleared by the r2c pass of the force before it; the last step's
-  // paint stays in rho (the density of the final positions)
-  cudaError_t e = kkd_force(disp, vel, rho, w, d, s, nsteps > 0);
+  // rho is cleared right before each paint (zeroed lines still in L2 when the deposits come);
+  // the last step's paint stays in rho (the density of the final positions)
+  cudaError_t e = kkd_force(disp, vel, rho, w, d, s, false);
   for (int i = 0; i < nsteps && e == cudaSuccess; ++i) {
-    e = jfli::kick_drift_paint(disp, vel, w.force, kicks[i], drifts[i], JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
-                               1.0f, rho, d, s);
-    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::poisson_potential(rho, w.spec, w.pot, d, 1.0f, 1.0f, s, rho);
+    e = jfli::zero_floats(rho, d.cells() * batch, s);
+    if (e == cudaSuccess)
+      e = jfli::kick_drift_paint(disp, vel, w.force, kicks[i], drifts[i], JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
+                                 1.0f, rho, d, s);
+    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::poisson_potential(rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
     if (e == cudaSuccess && i + 1 < nsteps) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
   }
   return cuda_status(e, err, errlen, "jfli_kkd_run");
@@ -967,13 +999,14 @@ int jfli_kkd_adjoint(void* stream, float* disp, float* vel, float* lam_x, float*
     return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, kkd_ws_bytes(d));
   cudaStream_t s = (cudaStream_t)stream;
   const KkdWs w = kkd_ws(workspace, d);
-  // w.rho is cleared once here; afterwards each step's r2c pass clears what it has read
-  cudaError_t e = cudaMemsetAsync(w.rho, 0, (size_t)d.cells() * batch * sizeof(float), s);
+  cudaError_t e = cudaSuccess;
   for (int i = nsteps - 1; i >= 0 && e == cudaSuccess; --i) {
     const float k = kicks[i], dr = drifts[i];
     // un-drift and paint the previous positions, force mesh there
-    e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, -dr, JFLI_STEP_DRIFT | JFLI_STEP_PAINT, 1.0f, w.rho, d, s);
-    if (e == cudaSuccess) e = jfli::poisson_potential(w.rho, w.spec, w.pot, d, 1.0f, 1.0f, s, w.rho);
+    e = jfli::zero_floats(w.rho, d.cells() * batch, s);
+    if (e == cudaSuccess)
+      e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, -dr, JFLI_STEP_DRIFT | JFLI_STEP_PAINT, 1.0f, w.rho, d, s);
+    if (e == cudaSuccess) e = jfli::poisson_potential(w.rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
     if (e == cudaSuccess) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
     // un-kick, adjoint paint, dL/dk and dL/dd
     if (e == cudaSuccess) e = jfli::adjoint_unkick_paint(disp, vel, lam_x, lam_v, w.force, k, dr, w.ubar, w.partials, d, s);

@@ -289,21 +289,19 @@ __device__ __forceinline__ void kdp_particle(float* __restrict__ disp, float* __
 // streaming loads and stores through the warp's shared buffers (24 float4 per array), and
 // every lane reads or writes its own 3 floats there (stride 3: no bank conflicts). A warp
 // thus issues one 16-byte load and one store per array and row instead of three 4-byte
-// ones, each touching 12 sectors. The deposit holds back the upper-x plane for the lane's
-// next particle (deposit_carried).
+// ones, each touching 12 sectors. The row is loaded one iteration ahead (xa, va hold it
+// when the call starts; the next row's loads are issued before this row's force gathers),
+// so the gathers, not the row loads, are the latency of an iteration. The deposit holds
+// back the upper-x plane for the lane's next particle (deposit_carried).
 __device__ __forceinline__ void kdp_brick_row(float* __restrict__ disp, float* __restrict__ vel,
                                               const float* __restrict__ force, float kick, float drift, int flags,
                                               float weight, float* __restrict__ rho, const PGrid& g, unsigned p0, int i,
-                                              int j, int k, int lane, float4* bx, float4* bv, XCarry& carry) {
+                                              int j, int k, int lane, float4* bx, float4* bv, XCarry& carry,
+                                              float4& xa, float4& va, bool prefetch, unsigned p_next) {
   const bool use_v = flags & (kStepKick | kStepDrift);
-  const float4* xr = reinterpret_cast<const float4*>(disp + 3ull * p0);
-  const float4* vr = reinterpret_cast<const float4*>(vel + 3ull * p0);
   if (lane < 24) {
-    const float4 a = __ldcs(xr + lane);
-    float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (use_v) c = __ldcs(vr + lane);
-    bx[lane] = a;
-    bv[lane] = c;
+    bx[lane] = xa;
+    bv[lane] = va;
   }
   __syncwarp();
   const float* fx = reinterpret_cast<const float*>(bx);
@@ -311,6 +309,10 @@ __device__ __forceinline__ void kdp_brick_row(float* __restrict__ disp, float* _
   float x0 = fx[3 * lane], x1 = fx[3 * lane + 1], x2 = fx[3 * lane + 2];
   float v0 = fv[3 * lane], v1 = fv[3 * lane + 1], v2 = fv[3 * lane + 2];
   __syncwarp();
+  if (prefetch && lane < 24) {
+    xa = __ldcs(reinterpret_cast<const float4*>(disp + 3ull * p_next) + lane);
+    if (use_v) va = __ldcs(reinterpret_cast<const float4*>(vel + 3ull * p_next) + lane);
+  }
   kdp_update(force, kick, drift, flags, g, i, j, k, x0, x1, x2, v0, v1, v2);
   const bool store_v = flags & kStepKick, store_x = flags & (kStepDrift | kStepCorrect);
   if (store_v || store_x) {
@@ -374,11 +376,17 @@ __global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__
       const int i1 = min(g.nx, (xc + 1) * kBrickX);
       XCarry carry;
       carry.valid = false;
-      for (int i = xc * kBrickX; i < i1; ++i) {
-        const unsigned p0 = ((unsigned)i * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)(k - lane);
-        kdp_brick_row(disp, vel, force, kick, drift, flags, weight, rho, g, p0, i, j, k, lane, rowbuf[w][0],
-                      rowbuf[w][1], carry);
+      const unsigned row_stride = (unsigned)g.ny * (unsigned)g.nz;  // one x plane
+      const bool use_v = flags & (kStepKick | kStepDrift);
+      unsigned p0 = ((unsigned)(xc * kBrickX) * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)(k - lane);
+      float4 xa = make_float4(0.f, 0.f, 0.f, 0.f), va = xa;
+      if (lane < 24) {
+        xa = __ldcs(reinterpret_cast<const float4*>(disp + 3ull * p0) + lane);
+        if (use_v) va = __ldcs(reinterpret_cast<const float4*>(vel + 3ull * p0) + lane);
       }
+      for (int i = xc * kBrickX; i < i1; ++i, p0 += row_stride)
+        kdp_brick_row(disp, vel, force, kick, drift, flags, weight, rho, g, p0, i, j, k, lane, rowbuf[w][0],
+                      rowbuf[w][1], carry, xa, va, i + 1 < i1, p0 + row_stride);
       // every lane of the warp ran the same planes: the carries go out together, z-merged
       deposit_plane_merged(rho, carry.valid, carry.xo, carry.yo0, carry.yo1, carry.z0, carry.z1, carry.w00,
                            carry.w01, carry.w10, carry.w11);
@@ -651,6 +659,22 @@ __global__ void k_lpt_combine(const float* __restrict__ f1, const float* __restr
     dx[q] = x;
     pv[q] = v;
   }
+}
+
+// Zero n floats (16-byte stores where the pointer allows; the tail element by element).
+__global__ void k_zero(float* __restrict__ y, long long n) {
+  const long long n4 = ((reinterpret_cast<uintptr_t>(y) & 15) == 0) ? n / 4 : 0;
+  float4* y4 = reinterpret_cast<float4*>(y);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride)
+    y4[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (long long q = 4 * n4 + (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) y[q] = 0.f;
+}
+
+cudaError_t zero_floats(float* y, long long n, cudaStream_t s) {
+  k_zero<<<particle_grid_dims((n + 3) / 4, 1, 256, 16), 256, 0, s>>>(y, n);
+  note_launch();
+  return cudaGetLastError();
 }
 
 __global__ void k_axpy(float* __restrict__ y, const float* __restrict__ x, float a, long long n) {

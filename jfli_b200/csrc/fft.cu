@@ -749,7 +749,7 @@ static cudaError_t launch_cols(float2* data, const ColGeom& g, long long bstride
 }
 
 // ---- TMA-staged x pass
-static std::atomic<int> g_x_pass_mode{0};  // 0 register pass, 1 TMA-staged pass
+static std::atomic<int> g_x_pass_mode{1};  // 0 register pass, 1 TMA-staged pass (default)
 
 void set_x_pass_mode(int mode) { g_x_pass_mode.store(mode); }
 int x_pass_mode() { return g_x_pass_mode.load(); }

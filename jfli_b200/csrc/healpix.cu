@@ -164,10 +164,32 @@ __device__ __forceinline__ void interp_weights(double theta, double phi, int nsi
   }
 }
 
+// Centre (theta, phi) of RING pixel pix: its ring found by bisection on the rings' start
+// pixels, phi = (index in ring + shift / 2) 2 pi / pixels in ring.
+__device__ __forceinline__ void pix_centre_ring(long long pix, int nside, const double* __restrict__ theta_tab,
+                                                double& theta, double& phi) {
+  int lo = 1, hi = 4 * nside - 1;  // last ring whose start <= pix
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (ring_info_tab(mid, nside, theta_tab).start <= pix)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const RingInfo r = ring_info_tab(lo, nside, theta_tab);
+  theta = r.theta;
+  phi = ((double)(pix - r.start) + 0.5 * r.shifted) * (2.0 * M_PI / r.npix);
+}
+
 // Deposit of weight w at direction (vx, vy, vz) (length rr > 0) on the RING map.
+// scheme 0: nearest pixel; 1: bilinear weights of the 4 surrounding pixel centres; 2 (the
+// "rbf_neighbor" scheme): the same 4 pixels weighted by a Gaussian radial basis function of
+// the angle d between the direction and each pixel centre, exp(-d^2 / (2 sigma^2)),
+// normalised to sum 1 (sigma in radians; taken relative to the nearest centre, so the
+// weights never all underflow).
 __device__ __forceinline__ void deposit_direction(float vx, float vy, float vz, float rr, float w, int nside,
                                                   int scheme, const double* __restrict__ theta_tab,
-                                                  float* __restrict__ map) {
+                                                  float* __restrict__ map, float sigma = 0.f) {
   const long long npix = 12LL * nside * nside;
   const double dr = (double)rr;
   const double zc = (double)vz / dr;
@@ -175,6 +197,32 @@ __device__ __forceinline__ void deposit_direction(float vx, float vy, float vz, 
   if (scheme == 0) {
     const long long pix = ang2pix_ring(zc, phi, nside);
     if (pix >= 0 && pix < npix) atomicAdd(map + pix, w);
+  } else if (scheme == 2) {
+    long long pix[4];
+    double wt[4];
+    interp_weights(acos(fmin(1.0, fmax(-1.0, zc))), phi, nside, theta_tab, pix, wt);
+    const double ux = (double)vx / dr, uy = (double)vy / dr, uz = zc;
+    double d2[4], dmin = 1e300;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double th, ph;
+      pix_centre_ring(pix[q], nside, theta_tab, th, ph);
+      const double st = sin(th);
+      const double cx = st * cos(ph) - ux, cy = st * sin(ph) - uy, cz = cos(th) - uz;
+      const double d = 2.0 * asin(fmin(1.0, 0.5 * sqrt(cx * cx + cy * cy + cz * cz)));
+      d2[q] = d * d;
+      dmin = fmin(dmin, d2[q]);
+    }
+    const double inv = 1.0 / (2.0 * (double)sigma * (double)sigma);
+    double sum = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      wt[q] = exp(-(d2[q] - dmin) * inv);
+      sum += wt[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (pix[q] >= 0 && pix[q] < npix) atomicAdd(map + pix[q], (float)(wt[q] / sum * (double)w));
   } else {
     long long pix[4];
     double wt[4];
@@ -187,7 +235,8 @@ __device__ __forceinline__ void deposit_direction(float vx, float vy, float vz, 
 
 __global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, const float* __restrict__ weights,
                                 float weight, MeshDims d, float3 cell, float3 obs, float rmin, float rmax, int nside,
-                                int scheme, const double* __restrict__ theta_tab, float* __restrict__ map) {
+                                int scheme, const double* __restrict__ theta_tab, float* __restrict__ map,
+                                float sigma) {
   const long long np = d.cells();
   const long long npix = 12LL * nside * nside;
   const int b = blockIdx.y;
@@ -209,7 +258,7 @@ __global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, co
     const float vx = gx * cell.x - obs.x, vy = gy * cell.y - obs.y, vz = gz * cell.z - obs.z;
     const float rr = sqrtf(vx * vx + vy * vy + vz * vz);
     if (!(rr > rmin && rr <= rmax)) continue;
-    deposit_direction(vx, vy, vz, rr, weights ? weights[p] * weight : weight, nside, scheme, theta_tab, map);
+    deposit_direction(vx, vy, vz, rr, weights ? weights[p] * weight : weight, nside, scheme, theta_tab, map, sigma);
   }
 }
 
@@ -450,7 +499,7 @@ static const double* ring_theta_table(int nside) {
 
 cudaError_t healpix_paint(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d,
                           const float* box, const float* observer, float rmin, float rmax, int nside, int scheme,
-                          float* map, cudaStream_t s) {
+                          float* map, cudaStream_t s, float sigma) {
   const float3 cell = make_float3(box[0] / d.nx, box[1] / d.ny, box[2] / d.nz);
   const float3 obs = make_float3(observer[0], observer[1], observer[2]);
   int dev = 0, nsm = 148;
@@ -461,7 +510,7 @@ cudaError_t healpix_paint(const float* disp, int absolute, const float* weights,
   const double* tab = ring_theta_table(nside);
   if (!tab) return cudaErrorMemoryAllocation;
   k_healpix_paint<<<dim3((unsigned)blocks, d.batch), 256, 0, s>>>(disp, absolute, weights, weight, d, cell, obs, rmin,
-                                                                  rmax, nside, scheme, tab, map);
+                                                                  rmax, nside, scheme, tab, map, sigma);
   note_launch();
   return cudaGetLastError();
 }

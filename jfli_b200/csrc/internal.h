@@ -114,6 +114,7 @@ cudaError_t sht_synthesis(const double* alm, const double* z, int nrings, int lm
 cudaError_t sht_ring_analysis(const double* map, int nside, int lmax, double* F, cudaStream_t s);
 cudaError_t sht_ring_synthesis(const double* G, int nside, int lmax, double* map, cudaStream_t s);
 cudaError_t sht_alm2cl(const double* alm1, const double* alm2, int lmax, double* cl, cudaStream_t s);
+cudaError_t zero_floats(float* y, long long n, cudaStream_t s);
 // x pass of the Poisson / PGD / IC filter chains: 0 register pass, 1 TMA-staged pass
 void set_x_pass_mode(int mode);
 int x_pass_mode();
@@ -150,7 +151,7 @@ cudaError_t power_poles(const float* mesh1, const float* mesh2, const MeshDims& 
 // ---- healpix.cu ----
 cudaError_t healpix_paint(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d,
                           const float* box, const float* observer, float rmin, float rmax, int nside, int scheme,
-                          float* map, cudaStream_t s);
+                          float* map, cudaStream_t s, float sigma = 0.f);
 cudaError_t replica_positions(const float* disp, int absolute, const float* vel, const MeshDims& d, const float* box,
                               const float* observer, const signed char* rotation, const float* shift, int telephoto,
                               float t, float gp_t, const DriftTables& tb, float* out, cudaStream_t s);

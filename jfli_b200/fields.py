@@ -793,8 +793,8 @@ class ParticleField(AbstractField):
         """HEALPix shell painting (reference fields/particles.py:326-442)."""
         if self.nside is None:
             raise ValueError("Spherical painting requires `nside`.")
-        if kernel_width_arcmin is not None or scheme == "rbf_neighbor":
-            raise NotImplementedError("rbf_neighbor smoothing is not on the B200 path")
+        if kernel_width_arcmin is not None and scheme != "rbf_neighbor":
+            raise NotImplementedError("kernel_width_arcmin applies to the rbf_neighbor scheme only")
         from .painting import check_grade_orders, paint_shells, regrade
 
         # painted at paint_nside when given, then brought to nside with healpy's ud_grade
@@ -802,6 +802,8 @@ class ParticleField(AbstractField):
         grade = dict(power=ud_grade_power, order_in=ud_grade_order_in, order_out=ud_grade_order_out,
                      pess=ud_grade_pess)
         src = self if paint_nside is None else self.replace(nside=int(paint_nside))
+        sigma = ops.rbf_sigma(src.nside, kernel_width_arcmin, smoothing_interpretation) \
+            if scheme == "rbf_neighbor" else None
 
         centers = np.atleast_1d(np.asarray(center, dtype=np.float64))
         widths = np.atleast_1d(np.asarray(density_plane_width, dtype=np.float64))
@@ -812,9 +814,9 @@ class ParticleField(AbstractField):
             if arr.shape[0] != centers.size:
                 raise ValueError(f"Batched input: center must have {arr.shape[0]} elements")
             maps = torch.stack([paint_shells(src.replace(array=arr[i]), centers[i:i + 1], widths[i:i + 1], scheme,
-                                             weights)[0] for i in range(arr.shape[0])])
+                                             weights, sigma=sigma)[0] for i in range(arr.shape[0])])
         else:
-            maps = paint_shells(src, centers, widths, scheme, weights)
+            maps = paint_shells(src, centers, widths, scheme, weights, sigma=sigma)
         maps = regrade(maps, self.nside, paint_nside, **grade)
         if maps.shape[0] == 1:
             maps = maps[0]

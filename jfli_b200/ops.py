@@ -281,19 +281,43 @@ def power_sums(mesh: torch.Tensor, kedges: torch.Tensor, box_size) -> torch.Tens
     return out
 
 
+def rbf_sigma(nside: int, kernel_width_arcmin=None, smoothing_interpretation: str = "fwhm") -> float:
+    """Gaussian sigma (radians) of the rbf_neighbor scheme: kernel_width_arcmin read as a
+    FWHM (sigma = FWHM / sqrt(8 ln 2)) or as sigma itself; without a width, the pixel size
+    sqrt(4 pi / npix) is the FWHM."""
+    if smoothing_interpretation not in ("fwhm", "sigma"):
+        raise ValueError(f"smoothing_interpretation must be 'fwhm' or 'sigma', got {smoothing_interpretation!r}")
+    if kernel_width_arcmin is None:
+        width, smoothing_interpretation = math.sqrt(4.0 * math.pi / (12 * nside * nside)), "fwhm"
+    else:
+        width = float(kernel_width_arcmin) * math.pi / (180.0 * 60.0)
+    if not width > 0:
+        raise ValueError("kernel_width_arcmin must be positive")
+    return width / math.sqrt(8.0 * math.log(2.0)) if smoothing_interpretation == "fwhm" else width
+
+
 def healpix_paint(pos: torch.Tensor, nside: int, box_size, observer_mpc, rmin: float, rmax: float, *,
                   scheme: str = "bilinear", absolute: bool = False, weights: torch.Tensor | None = None,
-                  weight: float = 1.0, out: torch.Tensor | None = None, accumulate: bool = False) -> torch.Tensor:
+                  weight: float = 1.0, out: torch.Tensor | None = None, accumulate: bool = False,
+                  sigma: float | None = None) -> torch.Tensor:
+    """Shell map; `sigma` (radians) is the Gaussian width of the rbf_neighbor scheme
+    (default: rbf_sigma(nside))."""
     _check(pos, "pos")
     (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
-    sch = {"ngp": _lib.JFLI_HEALPIX_NGP, "bilinear": _lib.JFLI_HEALPIX_BILINEAR}.get(scheme)
+    sch = {"ngp": _lib.JFLI_HEALPIX_NGP, "bilinear": _lib.JFLI_HEALPIX_BILINEAR, "rbf_neighbor": 2}.get(scheme)
     if sch is None:
-        raise NotImplementedError(f"spherical painting scheme {scheme!r} is not implemented (ngp, bilinear)")
+        raise NotImplementedError(f"spherical painting scheme {scheme!r} is not implemented (ngp, bilinear, "
+                                  f"rbf_neighbor)")
     if out is None:
         out = torch.empty(*lead, 12 * nside * nside, dtype=torch.float32, device=pos.device)
         accumulate = False
     lx, ly, lz = (float(v) for v in box_size)
     ox, oy, oz = (float(v) for v in observer_mpc)
+    if sch == 2:
+        sg = rbf_sigma(nside) if sigma is None else float(sigma)
+        call("jfli_healpix_paint_rbf", stream_ptr(), ptr(pos), int(absolute), ptr(weights), float(weight), lx, ly, lz,
+             ox, oy, oz, float(rmin), float(rmax), int(nside), sg, ptr(out), int(accumulate), nx, ny, nz, batch)
+        return out
     call("jfli_healpix_paint", stream_ptr(), ptr(pos), int(absolute), ptr(weights), float(weight), lx, ly, lz, ox,
          oy, oz, float(rmin), float(rmax), int(nside), sch, ptr(out), int(accumulate), nx, ny, nz, batch)
     return out

@@ -21,8 +21,9 @@ def shell_volume_per_pixel(nside: int, rmin: float, rmax: float) -> float:
     return (4.0 * math.pi / (12 * nside * nside)) * (rmax**3 - rmin**3) / 3.0
 
 
-def paint_shells(field, centers, widths, scheme="bilinear", weights=None, out=None) -> torch.Tensor:
-    """(S, 12 nside^2) maps of one particle set for S shells."""
+def paint_shells(field, centers, widths, scheme="bilinear", weights=None, out=None, sigma=None) -> torch.Tensor:
+    """(S, 12 nside^2) maps of one particle set for S shells (`sigma`: the rbf_neighbor
+    scheme's Gaussian width in radians)."""
     if field.unit == PositionUnit.MPC_H:
         field = field.to(PositionUnit.GRID_ABSOLUTE)
     absolute = field.unit == PositionUnit.GRID_ABSOLUTE
@@ -38,7 +39,7 @@ def paint_shells(field, centers, widths, scheme="bilinear", weights=None, out=No
         vol = shell_volume_per_pixel(field.nside, rmin, rmax)
         scale = ws / vol if vol > 0 else ws
         ops.healpix_paint(pos, field.nside, field.box_size, field.observer_position_mpc, rmin, rmax, scheme=scheme,
-                          absolute=absolute, weights=w, weight=scale, out=out[s])
+                          absolute=absolute, weights=w, weight=scale, out=out[s], sigma=sigma)
     return out
 
 

@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from .. import ops
-from .._lib import JFLI_STEP_CORRECT, JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
+from .._lib import JFLI_STEP_CLEAR, JFLI_STEP_CORRECT, JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
 from ..fields import ParticleField, PositionUnit
 from .correction import NoCorrection, PGDKernel, pgd_potential
 from .solvers import (AbstractNBodySolver, EfficientDriftDoubleKick, NBodyState, ReversibleDoubleKickDrift,
@@ -108,32 +108,21 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
     w_snap = _scalar_weight(interp.painting.weights) if interp.painting is not None else 1.0
     density_from_force_mesh = tgt == "density" and w_snap == 1.0
 
-    def keep_density(next_event: int) -> bool:
-        """True when the event after a force solve is a save that copies the density mesh
-        (then the solve leaves the mesh as painted; otherwise its forward FFT clears it
-        for the next paint)."""
-        return density_from_force_mesh and next_event < len(events) and events[next_event][0] == "save"
-
-    # force at the initial positions
-    rho.zero_()
-    ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT, rho)
-    rho_clear = not keep_density(0)
-    ops.poisson_force(rho, 1.0, out=force, pot=pot, clear=rho_clear)
+    # force at the initial positions (every paint clears the density mesh right before it)
+    ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT | JFLI_STEP_CLEAR, rho)
+    ops.poisson_force(rho, 1.0, out=force, pot=pot)
     pending = EfficientDriftDoubleKick.init_kick(cosmo, t0, t0 + dt0) if efficient else None
-    rho_is_current = not rho_clear  # rho holds the paint of the current positions
+    rho_is_current = True  # rho holds the paint of the current positions
 
     snapshots = []
     step_i = 0
-    for ev_i, ev in enumerate(events):
+    for ev in events:
         if ev[0] == "step":
             _, ta, tb = ev
             c = StepCoefficients(kick=float(kicks_all[step_i]), drift=float(drifts_all[step_i]), kick_first=not efficient)
             step_i += 1
-            if not rho_clear:
-                rho.zero_()
-            clear_next = not keep_density(ev_i + 1)
             if efficient:
-                flags = JFLI_STEP_DRIFT | JFLI_STEP_PAINT
+                flags = JFLI_STEP_DRIFT | JFLI_STEP_PAINT | JFLI_STEP_CLEAR
                 kick = 0.0
                 if pending is not None:
                     flags |= JFLI_STEP_KICK
@@ -142,21 +131,18 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
                     ops.kick_drift_paint(x, v, force, kick, c.drift, flags, rho)
                     pgd_potential(rho, pgd.kl, pgd.ks, 1.0, out=pot)
                     ops.force_mesh(pot, out=force)
-                    rho.zero_()
-                    ops.kick_drift_paint(x, v, force, pgd.alpha, 0.0, JFLI_STEP_CORRECT | JFLI_STEP_PAINT, rho)
+                    ops.kick_drift_paint(x, v, force, pgd.alpha, 0.0,
+                                         JFLI_STEP_CORRECT | JFLI_STEP_PAINT | JFLI_STEP_CLEAR, rho)
                 else:
                     ops.kick_drift_paint(x, v, force, kick, c.drift, flags, rho)
-                ops.poisson_force(rho, 1.0, out=force, pot=pot, clear=clear_next)
-                rho_clear = clear_next
+                ops.poisson_force(rho, 1.0, out=force, pot=pot)
                 pending = c.kick
             else:
-                ops.kick_drift_paint(x, v, force, c.kick, c.drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
-                                     rho)
-                rho_clear = False
+                ops.kick_drift_paint(x, v, force, c.kick, c.drift,
+                                     JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT | JFLI_STEP_CLEAR, rho)
                 if step_i < n_steps:
-                    ops.poisson_force(rho, 1.0, out=force, pot=pot, clear=clear_next)
-                    rho_clear = clear_next
-            rho_is_current = not rho_clear
+                    ops.poisson_force(rho, 1.0, out=force, pot=pot)
+            rho_is_current = True
             state = NBodyState(interp_state=interp.advance(state.interp_state, tb), t_initial=t0)
         else:
             _, i, t_target = ev

@@ -34,7 +34,7 @@ import numpy as np
 import torch
 
 from . import _lib, ops
-from ._lib import JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
+from ._lib import JFLI_STEP_CLEAR, JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
 
 A_INIT = 0.1
 
@@ -304,8 +304,7 @@ class SizeGroup:
         b = len(self.slots)
         setup_request(req, prep, self.x[b], self.v[b])
         # force at the slot's initial positions
-        self.rho[b].zero_()
-        ops.kick_drift_paint(self.x[b], self.v[b], None, 0.0, 0.0, JFLI_STEP_PAINT, self.rho[b])
+        ops.kick_drift_paint(self.x[b], self.v[b], None, 0.0, 0.0, JFLI_STEP_PAINT | JFLI_STEP_CLEAR, self.rho[b])
         ops.poisson_force(self.rho[b], 1.0, out=self.force[b], pot=self.pot1)
         self.slots.append(_Slot(req, prep, now))
         return b

@@ -163,8 +163,24 @@ def get_interp_weights(nside, theta, phi):
     return p_out, w_out
 
 
-def paint_shell(pos_mpc, observer, rmin, rmax, nside, scheme="bilinear", weight=1.0):
-    """Raw weight sums per pixel of the particles with rmin < r <= rmax (FP64)."""
+def rbf_weights(nside, theta, phi, sigma):
+    """(pixels (4, P), weights (4, P)) of the library's rbf_neighbor scheme: the 4 pixels of
+    the bilinear scheme, weighted by exp(-d^2 / (2 sigma^2)) of the angle d between the
+    direction and each pixel centre, normalised to sum 1 (sigma in radians)."""
+    pix, _ = get_interp_weights(nside, theta, phi)
+    tc, pc = pix2ang(nside, pix.ravel())
+    tc, pc = tc.reshape(pix.shape), pc.reshape(pix.shape)
+    u = np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta)])
+    c = np.stack([np.sin(tc) * np.cos(pc), np.sin(tc) * np.sin(pc), np.cos(tc)])
+    d = 2.0 * np.arcsin(np.minimum(1.0, 0.5 * np.linalg.norm(c - u[:, None, :], axis=0)))
+    d2 = d * d
+    w = np.exp(-(d2 - d2.min(axis=0)) / (2.0 * sigma * sigma))
+    return pix, w / w.sum(axis=0)
+
+
+def paint_shell(pos_mpc, observer, rmin, rmax, nside, scheme="bilinear", weight=1.0, sigma=None):
+    """Raw weight sums per pixel of the particles with rmin < r <= rmax (FP64); `sigma`
+    (radians) for the rbf_neighbor scheme."""
     v = pos_mpc.reshape(-1, 3).astype(np.float64) - np.asarray(observer, np.float64)
     r = np.sqrt((v**2).sum(-1))
     sel = (r > rmin) & (r <= rmax)
@@ -177,6 +193,9 @@ def paint_shell(pos_mpc, observer, rmin, rmax, nside, scheme="bilinear", weight=
     if scheme == "ngp":
         pix = ang2pix(nside, theta, phi)
         return np.bincount(pix, minlength=npix) * weight
+    if scheme == "rbf_neighbor":
+        pix, w = rbf_weights(nside, theta, phi, sigma)
+        return np.bincount(pix.ravel(), weights=w.ravel() * weight, minlength=npix)
     pix, w = get_interp_weights(nside, theta, phi)
     return np.bincount(pix.ravel(), weights=w.ravel() * weight, minlength=npix)
 

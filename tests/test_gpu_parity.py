@@ -530,3 +530,30 @@ def test_transfer_and_coherence():
     b = torch.as_tensor(rng.standard_normal((32, 32, 32)).astype(np.float32), device="cuda")
     _, c2 = jf.coherence(a, b, box_shape=(200.0,) * 3, kedges=edges)
     assert np.all(np.abs(c2.cpu().numpy()) < 0.5)  # independent fields: weakly coherent
+
+
+@pytest.mark.parametrize("nside,width,interp", [(16, None, "fwhm"), (32, 90.0, "fwhm"), (32, 40.0, "sigma")])
+def test_healpix_rbf_neighbor_matches_oracle(cosmo, nside, width, interp):
+    """The rbf_neighbor scheme (Gaussian weights of the 4 surrounding pixel centres,
+    normalised per particle) against the oracle's restatement, through
+    ParticleField.paint_spherical; each particle's weight sums to one."""
+    from oracle import healpix as oh
+
+    n, L = 32, 200.0
+    disp = lpt_disp(n, 2.0, seed=21).astype(np.float32)
+    field = jf.ParticleField(array=dev(disp), mesh_size=(n,) * 3, box_size=(L,) * 3, nside=nside)
+    rc, wd = 60.0, 40.0
+    m = host(field.paint_spherical(rc, wd, scheme="rbf_neighbor", kernel_width_arcmin=width,
+                                   smoothing_interpretation=interp).array).astype(np.float64)
+    sigma = ops.rbf_sigma(nside, width, interp)
+    obs = field.observer_position_mpc
+    pos = (opm.grid((n, n, n)) + disp.astype(np.float64)) * (L / n)
+    rmin, rmax = rc - wd / 2, rc + wd / 2
+    vol = (4 * np.pi / (12 * nside * nside)) * (rmax**3 - rmin**3) / 3
+    ref = oh.paint_shell(pos.reshape(-1, 3), obs, rmin, rmax, nside, "rbf_neighbor", sigma=sigma) / vol
+    r = np.linalg.norm(pos.reshape(-1, 3) - np.asarray(obs), axis=1)
+    inside = int(((r > rmin) & (r <= rmax)).sum())
+    err = rel_l2(m, ref)
+    print(f"nside {nside}, width {width} ({interp}): rel L2 {err:.2e}; total {m.sum() * vol:.1f} of {inside}")
+    assert inside > 0 and err < 2e-5
+    assert abs(m.sum() * vol / inside - 1) < 1e-5

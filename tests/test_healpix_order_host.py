@@ -90,7 +90,7 @@ def test_paint_spherical_at_paint_nside(monkeypatch):
     painting = importlib.import_module("jfli_b200.painting")
     seen = []
 
-    def fake_paint_shells(field, centers, widths, scheme="bilinear", weights=None, out=None):
+    def fake_paint_shells(field, centers, widths, scheme="bilinear", weights=None, out=None, sigma=None):
         seen.append(field.nside)
         npix = 12 * field.nside * field.nside
         return torch.arange(npix, dtype=torch.float64).repeat(len(centers), 1) + 1.0
