@@ -91,7 +91,7 @@ def parse():
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
@@ -120,7 +120,7 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        sm, smax, reasons = [], [], set()
+        sm, smax, util, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
@@ -134,8 +134,16 @@ class ClockSampler:
             for nm, val in zip(names, parts[5:9]):
                 if val.lower() == "active":
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+            if len(parts) > 9:
+                try:
+                    util.append(float(parts[9]))
+                except ValueError:
+                    pass
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+               "reasons": sorted(reasons), "samples": len(sm)}
+        if util:
+            out["gpu_util_pct_median"] = statistics.median(util)
+        return out
 
 
 # --------------------------------------------------------------------------- distributed
@@ -452,9 +460,13 @@ def run_serving(args):
     rate = args.serve_rate if args.serve_rate > 0 else round(0.85 * s_cap["requests_per_s"], 1)
     reqs = serving.poisson_stream(args.serve_requests, rate, seed=0, grad_fraction=0.25)
     l0 = __import__("jfli_b200").ops.launch_count()
+    util = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    util.start()
     served = eng.run(reqs, realtime=True)
+    u = util.stop()
     launches = __import__("jfli_b200").ops.launch_count() - l0
     s_stats = serving.summarize(served, reqs)
+    s_stats["gpu_util_pct_median"] = u.get("gpu_util_pct_median")
     s_stats["host_s"] = {k: round(v, 3) for k, v in eng.stats.items()}
     eng.close()
     plain = serving.run_plain(reqs, realtime=True, keep_density="device", on_result=consumer("plain"))

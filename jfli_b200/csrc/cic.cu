@@ -347,7 +347,7 @@ constexpr int kBrickY = 8, kBrickZ = 32, kBrickX = 16;  // CTA of 256 = 8 warps;
 // planes; warps stay on z rows (the lane-merged deposit needs them), but the rows and
 // planes whose particles share CIC corners are gathered on one SM close in time, so the
 // force-mesh lines they share are served by L1. Other shapes use a grid-stride walk.
-__global__ void k_kick_drift_paint(float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ force,
+__global__ void __launch_bounds__(256, 4) k_kick_drift_paint(float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ force,
                                    float kick, float drift, int flags, float weight, float* __restrict__ rho,
                                    PGrid g, const float* __restrict__ kicks, const float* __restrict__ drifts,
                                    const int* __restrict__ slot_flags) {
