@@ -13,10 +13,10 @@ schedule restarts from the initial conditions inside the timed region.
   e2e   : the same metric through the public API (jfli_b200.interpolate_initial_conditions
           -> lpt -> nbody -> power) from pinned host white noise to host density + P(k),
           40 KDK steps per request, copies inside the timed region
-  roofline : the particle pass call (density clear + k_kick_drift_paint), algorithmic
-          bytes 48 B/particle (read+write position and velocity) + 20 B/cell (the three
-          force components read, the density zeroed and written) per call, over its
-          CUDA-event time, against MEASURED_PEAKS.json
+  roofline : the fused particle pass (k_kick_drift_paint), algorithmic bytes 48 B/particle
+          (read+write position and velocity) + 16 B/cell (the three force components read,
+          the density written) per launch, over its CUDA-event time, against
+          MEASURED_PEAKS.json
   cpu_baseline : the FP32 oracle port of the same steps (oracle/pm.py with the C/OpenMP
           CIC of oracle/cic.c) on this host, a bounded sample of the schedule
   serving : the request stream (512 Poisson arrivals over mesh 64/96/128/192, 10-40 KDK
@@ -199,7 +199,7 @@ def run_gpu(args, world, rank):
     sched = [(e[1], e[2]) for e in time_events(0.1, [1.0], dt0) if e[0] == "step"]
     coeffs = [EDK.step_coefficients(cosmo, a, b, dt0) for a, b in sched]
     init_kick = EDK.init_kick(cosmo, 0.1, 0.1 + dt0)
-    flags = JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT | JFLI_STEP_CLEAR
+    flags = JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT
     stream = torch.cuda.current_stream()
     x0, v0 = x.clone(), v.clone()
     st = {"idx": 0, "pending": init_kick}
@@ -219,6 +219,7 @@ def run_gpu(args, world, rank):
         paint, then the new force meshes; after the last step of the schedule the next call
         restarts from the initial conditions (the restart is inside the timed region)."""
         c = coeffs[st["idx"]]
+        ops.zero_(rho)  # right before the paint: the zeroed lines are still in L2 when the deposits come
         if timed_kdp is not None:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -273,9 +274,9 @@ def run_gpu(args, world, rank):
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     kdp_avg_ms = statistics.mean(kdp)
-    # the timed call clears the density mesh and runs the particle pass: x, v read and written
-    # (48 B), the three force components read (12 B), the density zeroed and written (8 B)
-    alg_bytes = 68.0 * particles
+    # x, v read and written (48 B), the three force components read (12 B), the density
+    # written (4 B) per particle of the pass
+    alg_bytes = 64.0 * particles
     achieved = alg_bytes / (kdp_avg_ms / 1e3) / 1e9
     roof = {"kernel": "k_kick_drift_paint", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": ncu_traffic(n),

@@ -334,6 +334,9 @@ int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nring
  * bulk tensor store (meshes whose x-plane stride is a multiple of 16 bytes; others keep
  * mode 0). Both give the same spectrum to FP32 rounding. Process-wide. */
 int jfli_set_fft_x_pass(int mode, char* err, size_t errlen);
+/* Set n floats to zero (the library's own kernel: 16-byte stores where aligned). A step
+ * loop clears its density mesh with it, or with JFLI_STEP_CLEAR, right before the paint. */
+int jfli_zero(void* stream, float* data, long long n, char* err, size_t errlen);
 /* Status word of the library's bounded device waits: bit 0 is set when a kernel's wait on
  * an mbarrier ran out of its bound (the kernel then left its output untouched). Read
  * synchronously; reset != 0 clears it. */

@@ -131,6 +131,7 @@ _SIGNATURES = {
     "jfli_sht_alm2map": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, *_ERR]),
     "jfli_sht_alm2cl": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, *_ERR]),
     "jfli_set_fft_x_pass": (c_int, [c_int, *_ERR]),
+    "jfli_zero": (c_int, [c_void_p, c_void_p, ctypes.c_longlong, *_ERR]),
     "jfli_healpix_paint_rbf": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_float,
                                        c_float, c_float, c_float, c_float, c_float, c_int, c_float, c_void_p, c_int,
                                        *_DIMS, *_ERR]),

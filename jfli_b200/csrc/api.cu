@@ -875,6 +875,12 @@ int jfli_sht_alm2map(void* stream, const double* alm, const double* z, int nring
                      "jfli_sht_alm2map");
 }
 
+int jfli_zero(void* stream, float* data, long long n, char* err, size_t errlen) {
+  CHECK_PTR(data);
+  if (n < 0) return fail(err, errlen, JFLI_EINVAL, "n must be >= 0");
+  return cuda_status(jfli::zero_floats(data, n, (cudaStream_t)stream), err, errlen, "jfli_zero");
+}
+
 int jfli_set_fft_x_pass(int mode, char* err, size_t errlen) {
   if (mode != 0 && mode != 1) return fail(err, errlen, JFLI_EINVAL, "x pass mode %d is not 0 or 1", mode);
   jfli::set_x_pass_mode(mode);

@@ -202,6 +202,13 @@ def pm_step(disp, vel, kick, drift, flags, rho, force) -> None:
          ptr(force), ptr(ws), ws.numel(), nx, ny, nz, batch)
 
 
+def zero_(t: torch.Tensor) -> torch.Tensor:
+    """Set a float32 CUDA tensor to zero in place with the library's kernel (jfli_zero)."""
+    _check(t, "t")
+    call("jfli_zero", stream_ptr(), ptr(t), int(t.numel()))
+    return t
+
+
 def ic_filter(noise: torch.Tensor, ktab: torch.Tensor, ptab: torch.Tensor, box_size, *,
               zero_mode_one: bool = False) -> torch.Tensor:
     _check(noise, "noise")
