@@ -23,7 +23,7 @@ schedule restarts from the initial conditions inside the timed region.
           steps, mixed cosmologies) through the continuous-batching engine
           (jfli_b200.serving) and through the plain per-call path at the same offered
           load: p50/p99 latency and Mpart-steps/s of each, the engine's capacity with all
-          requests queued at once, and 256^3 requests served two at a time vs one by one
+          requests queued at once, and 256^3 requests served four at a time vs one by one
   fft_vs_cufft : this library's 3D r2c and c2r beside cuFFT (torch.fft) on the same
           256^3 mesh, as a comparison only (cuFFT is on no path of this library)
 
@@ -69,7 +69,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=0.0,
                     help="Poisson arrival rate, requests/s; 0 = 85%% of the engine's capacity, measured first "
                          "with the same requests queued at once")
-    ap.add_argument("--serve-256", type=int, default=6, help="256^3 requests for the served-vs-plain pair")
+    ap.add_argument("--serve-256", type=int, default=16,
+                    help="256^3 requests for the served-vs-plain pair (served four at a time)")
     ap.add_argument("--grad-iters", type=int, default=5, help="timed gradient iterations at 128^3")
     ap.add_argument("--lightcone-tiler", default="onion", choices=["none", "onion"],
                     help="none: shells inside the box (to 500 Mpc/h around the centred observer); onion: 27 "
@@ -81,6 +82,9 @@ def parse():
                     help="instead of the step benchmark, run the Poisson chain on a seeded density of this mesh size "
                          "twice with the register x pass and twice with the TMA-staged one (a short case to profile "
                          "the two x-pass kernels) and print their CUDA-event times")
+    ap.add_argument("--paint-order", type=int, default=0,
+                    help="instead of the step benchmark, evolve this mesh size to the last of the 40 steps and time "
+                         "the CIC paint and readout in Lagrangian and in cell-sorted particle order, and the sort")
     ap.add_argument("--tiled-paint", type=int, default=0,
                     help="instead of the step benchmark, time the 27-replica light-cone paint of one shell "
                          "(this many particles per side, box 500 Mpc/h, shell 653-747 Mpc/h, nside 1024)")
@@ -270,9 +274,7 @@ def run_gpu(args, world, rank):
     # clocks are sampled every 200 ms from before the warm-up through the e2e requests
     clk = clocks.stop() if rank == 0 else None
 
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
-    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    peak, source = hbm_peak()
     kdp_avg_ms = statistics.mean(kdp)
     # x, v read and written (48 B), the three force components read (12 B), the density
     # written (4 B) per particle of the pass
@@ -280,7 +282,7 @@ def run_gpu(args, world, rank):
     achieved = alg_bytes / (kdp_avg_ms / 1e3) / 1e9
     roof = {"kernel": "k_kick_drift_paint", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": ncu_traffic(n),
-            "peak_source": "measured" if peaks else "fallback", "avg_launch_ms": round(kdp_avg_ms, 4),
+            "peak_source": source, "avg_launch_ms": round(kdp_avg_ms, 4),
             "algorithmic_bytes_per_launch": alg_bytes, "step_share": round(sum(kdp) / ms, 4)}
     # whole-step roofline: 120 B per particle-step (each array read or written once per pass,
     # with r2c + three Green x gradient + c2r chains) and this implementation's own 132 B
@@ -291,6 +293,15 @@ def run_gpu(args, world, rank):
                  "own_frac": round(132.0 * particles / step_s / 1e9 / peak, 4)}
     return dict(value=value, ms=ms_max, clocks=clk, launches=launches, e2e=e2e, roofline=roof, serving=serve,
                 gradient=grad, step_roofline=step_roof, shells=shells)
+
+
+def hbm_peak():
+    """(HBM GB/s, "measured" | "fallback"): the measured copy bandwidth of MEASURED_PEAKS.json,
+    else the pool's earlier measurement."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
 
 
 def ncu_traffic(n):
@@ -422,7 +433,7 @@ def run_serving(args):
     """The request stream (Poisson arrivals; mesh 64/96/128/192; L = 4 Mpc/h per cell;
     Omega_c ~ U[0.20, 0.35]; sigma8 ~ U[0.70, 0.90]; 10-40 KDK steps; seed = request id)
     through the batched engine and through the plain per-call path at the same offered
-    load, plus 256^3 requests (40 steps, L = 1000 Mpc/h) served two at a time vs one by
+    load, plus 256^3 requests (40 steps, L = 1000 Mpc/h) served four at a time vs one by
     one. Every request returns its density (a CUDA tensor of its own) and its P(k) (32 bins,
     on the host)."""
     import torch
@@ -486,19 +497,32 @@ def run_serving(args):
            "slots": eng.capacity(), "served_launches": launches, "densities_delivered": dict(delivered),
            "max_pk_rel_served_vs_plain": float(f"{worst:.3e}")}
     if args.serve_256 > 0:
+        slots = 4
         big = [serving.ForwardRequest(rid=3 * 10**6 + i, mesh=256, box=1000.0, omega_c=0.2607, sigma8=0.8102,
                                       steps=40, seed=i) for i in range(args.serve_256)]
-        e256 = serving.Engine(sizes=(256,), hbm_budget_gb=2.0, max_slots=2, keep_density="device", workers=2,
-                              on_result=consumer("engine"))
-        e256.run(big[:2], realtime=False)
-        big2 = [dataclasses_replace(r, rid=r.rid + 100) for r in big]
-        s256 = serving.summarize(e256.run(big2, realtime=False), big2)
+        # one 940 MB slot per request in flight (x, v, density, force mesh, spectrum)
+        e256 = serving.Engine(sizes=(256,), hbm_budget_gb=slots * 1.0, max_slots=slots, keep_density="device",
+                              workers=2, on_result=consumer("engine"))
+        e256.run([dataclasses_replace(r, rid=r.rid + 10**5) for r in big[:slots]], realtime=False)
+        s256 = serving.summarize(e256.run(big, realtime=False), big)
+        slots = e256.capacity()[256]
         e256.close()
+        serving.run_plain([dataclasses_replace(r, rid=r.rid + 10**5) for r in big[:1]], realtime=False,
+                          keep_density="device", on_result=consumer("plain"))
         p256 = serving.summarize(serving.run_plain(big, realtime=False, keep_density="device",
                                                    on_result=consumer("plain")), big)
-        out["at_256"] = {"requests": len(big), "served_mpart_steps_per_s": s256["mpart_steps_per_s"],
-                         "plain_mpart_steps_per_s": p256["mpart_steps_per_s"], "served_p50_ms": s256["p50_ms"],
-                         "plain_p50_ms": p256["p50_ms"], "slots": 2,
+        peak, source = hbm_peak()
+
+        def frac(mps):  # 120 B per particle-step against the HBM peak
+            return round(mps * 1e6 * 120.0 / (peak * 1e9), 4)
+
+        out["at_256"] = {"requests": len(big), "slots": slots, "queued": "all at once, both arms warmed",
+                         "served_mpart_steps_per_s": s256["mpart_steps_per_s"],
+                         "plain_mpart_steps_per_s": p256["mpart_steps_per_s"],
+                         "served_frac": frac(s256["mpart_steps_per_s"]), "plain_frac": frac(p256["mpart_steps_per_s"]),
+                         "frac_basis": f"120 B per particle-step over the {source} HBM peak {peak} GB/s",
+                         "served_p50_ms": s256["p50_ms"], "served_p99_ms": s256["p99_ms"],
+                         "plain_p50_ms": p256["p50_ms"], "plain_p99_ms": p256["p99_ms"],
                          "per": "request: ICs + 2LPT + 40 KDK steps + P(k) to host"}
     return out
 
@@ -706,6 +730,84 @@ def x_pass_variants(n, iters=20):
     return out
 
 
+def paint_order_probe(n, iters=10):
+    """What a cell-ordered particle sort would buy the particle pass, measured on the
+    state entering the last of the 40 steps at n^3 (the most clustered state of the run):
+    the CIC paint (jfli_paint_cic, accumulating) and the CIC readout (jfli_readout_cic) of
+    the same absolute positions in Lagrangian order and sorted by cell, the fused pass
+    itself in Lagrangian order, and the sort's own cost (a radix sort of the 32-bit cell
+    keys, then the gather of positions and velocities into that order). CUDA-event ms,
+    mean of `iters` after 3 warm-ups."""
+    import torch
+
+    import jfli_b200 as jf
+    from jfli_b200 import ops
+    from jfli_b200._lib import JFLI_STEP_CLEAR, JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
+    from jfli_b200.pm.integrate import time_events
+    from jfli_b200.pm.solvers import EfficientDriftDoubleKick as EDK
+
+    cosmo = jf.Planck18()
+    dx, p = setup_state(n, cosmo)
+    x, v = dx.array.clone(), p.array.clone()
+    rho = torch.empty(n, n, n, device="cuda")
+    pot = torch.empty_like(rho)
+    force = torch.empty(n, n, n, 4, device="cuda")
+    dt0 = 0.9 / E2E_STEPS
+    sched = [(e[1], e[2]) for e in time_events(0.1, [1.0], dt0) if e[0] == "step"]
+    coeffs = [EDK.step_coefficients(cosmo, a, b, dt0) for a, b in sched]
+    pending = EDK.init_kick(cosmo, 0.1, 0.1 + dt0)
+    flags = JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT | JFLI_STEP_CLEAR
+    ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT | JFLI_STEP_CLEAR, rho)
+    ops.poisson_force(rho, 1.0, out=force, pot=pot)
+    for c in coeffs[:-1]:
+        ops.kick_drift_paint(x, v, force, pending, c.drift, flags, rho)
+        ops.poisson_force(rho, 1.0, out=force, pot=pot)
+        pending = c.kick
+    xs, vs = x.clone(), v.clone()
+
+    def timed(fn, reset=None):
+        ts = []
+        for it in range(3 + iters):
+            if reset is not None:
+                reset()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            if it >= 3:
+                ts.append(e0.elapsed_time(e1))
+        return round(float(np.mean(ts)), 4)
+
+    def reset():
+        x.copy_(xs)
+        v.copy_(vs)
+
+    out = {"mesh": n, "a": round(float(sched[-1][0]), 4)}
+    out["fused_pass_lagrangian_ms"] = timed(
+        lambda: ops.kick_drift_paint(x, v, force, pending, coeffs[-1].drift, flags, rho), reset)
+    ar = torch.arange(n, device="cuda", dtype=torch.float32)
+    grid = torch.stack(torch.meshgrid(ar, ar, ar, indexing="ij"), dim=-1)
+    pos = torch.remainder(grid + xs, float(n)).contiguous()
+    del grid
+    cell = pos.floor().to(torch.int32).clamp_(0, n - 1)
+    key = ((cell[..., 0] * n + cell[..., 1]) * n + cell[..., 2]).reshape(-1)
+    del cell
+    out["sort_keys_ms"] = timed(lambda: torch.sort(key))
+    order = torch.sort(key).indices
+    flat_p, flat_v = pos.reshape(-1, 3), vs.reshape(-1, 3)
+    out["gather_xv_ms"] = timed(lambda: (flat_p.index_select(0, order), flat_v.index_select(0, order)))
+    pos_sorted = flat_p.index_select(0, order).reshape(n, n, n, 3).contiguous()
+    mesh_l = torch.zeros(n, n, n, device="cuda")
+    mesh_s = torch.zeros_like(mesh_l)
+    out["paint_lagrangian_ms"] = timed(lambda: ops.paint_cic(pos, absolute=True, out=mesh_l, accumulate=True))
+    out["paint_sorted_ms"] = timed(lambda: ops.paint_cic(pos_sorted, absolute=True, out=mesh_s, accumulate=True))
+    out["paint_rel_diff"] = float((mesh_s - mesh_l).norm() / mesh_l.norm())
+    out["readout_lagrangian_ms"] = timed(lambda: ops.readout_cic(pos, rho, absolute=True))
+    out["readout_sorted_ms"] = timed(lambda: ops.readout_cic(pos_sorted, rho, absolute=True))
+    return out
+
+
 def cpu_baseline_block(n):
     """The FP32 oracle port on this host, on a bounded sample of the workload: the first 5
     steps of the 40-step schedule at n^3 (~10-20 s of CPU work at 256^3 on 16 cores)."""
@@ -840,6 +942,9 @@ def main():
         return
     if args.tiled_paint:
         run_tiled_paint(args)
+        return
+    if args.paint_order:
+        print(json.dumps({"paint_order_probe": paint_order_probe(args.paint_order)}), flush=True)
         return
     if args.xpass:
         res = x_pass_variants(args.xpass, iters=2)  # a profiling case: the first calls include set-up

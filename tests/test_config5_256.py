@@ -37,14 +37,15 @@ def _band(c, lmax):
     return c[1:nb + 1].reshape(-1, 8).mean(axis=1)
 
 
-def _check_cl(label, cl, c64, c32, lmax):
+def _check_cl(label, cl, c64, c32, lmax, failures):
     e = np.abs(cl[1:] / c64[1:] - 1)
     g = np.abs(c32[1:] / c64[1:] - 1)
     eb = np.abs(_band(cl, lmax) / _band(c64, lmax) - 1)
     gb = np.abs(_band(c32, lmax) / _band(c64, lmax) - 1)
     print(f"{label} C_ell vs FP64 oracle: max {e.max():.2e} per multipole, {eb.max():.2e} per band of 8 (FP32 "
           f"oracle {g.max():.2e}, {gb.max():.2e})")
-    assert eb.max() < max(1e-4, 2 * gb.max()) and e.max() < max(5e-4, 2 * g.max())
+    if not (eb.max() < max(1e-4, 2 * gb.max()) and e.max() < max(5e-4, 2 * g.max())):
+        failures.append(f"{label} C_ell")
 
 
 def _coarse4(m):
@@ -69,11 +70,12 @@ def test_config5_lightcone_chain(cosmo):
     assert res.steps == int(ref["steps"])
     np.testing.assert_allclose(np.asarray(res.shells.comoving_centers), ref["shell_centers"], rtol=1e-12)
     lmax, nc = int(ref["lmax"]), int(ref["nside_coarse"])
+    failures = []  # every figure is printed before the test fails on any of them
     maps = res.shells.array.double()
     kappa = res.kappa.array[0].double()
     # convergence map
     kcl = sht.anafast(kappa, lmax).cpu().numpy()
-    _check_cl("kappa", kcl, ref["kappa_cl_f64"], ref["kappa_cl_f32"], lmax)
+    _check_cl("kappa", kcl, ref["kappa_cl_f64"], ref["kappa_cl_f32"], lmax, failures)
     kc = ud_grade(kappa, nc).cpu().numpy()
     e_map = rel_l2(kc, ref["kappa_coarse_f64"])
     e4 = rel_l2(_coarse4(kc), _coarse4(ref["kappa_coarse_f64"]))
@@ -81,7 +83,10 @@ def test_config5_lightcone_chain(cosmo):
     rms = float(kappa.std())
     print(f"kappa map vs FP64 oracle: at nside {nc} {e_map:.2e}, at nside 4 {e4:.2e} (gap {g4:.2e}; full-map gap "
           f"{float(ref['gap_kappa_f32']):.2e}); rms {rms:.4e} vs {float(ref['kappa_rms_f64']):.4e}")
-    assert e4 < max(1e-5, 2 * g4)
+    k64 = ref["kappa_coarse_f64"]
+    print(f"kappa mean {float(kappa.mean()):.3e}; coarse-map projection on the FP64 one {kc @ k64 / (k64 @ k64):.8f}")
+    if not e4 < max(1e-5, 2 * g4):
+        failures.append("kappa map")
     # shells
     coarse = ud_grade(maps, nc).cpu().numpy()
     sums = maps.sum(dim=1).cpu().numpy()
@@ -92,9 +97,10 @@ def test_config5_lightcone_chain(cosmo):
         g4 = rel_l2(_coarse4(ref["shells_coarse_f32"][s]), _coarse4(ref["shells_coarse_f64"][s]))
         print(f"shell {s} ({ref['shell_centers'][s]:.0f} Mpc/h): map at nside {nc} {e_s:.2e}, at nside 4 {e4:.2e} "
               f"(gap {g4:.2e}; full-map gap {float(ref['gap_shells_f32'][s]):.2e}), total {e_sum[s]:.2e}")
-        assert e4 < max(1e-5, 2 * g4)
-        assert e_sum[s] < 1e-5
+        if not (e4 < max(1e-5, 2 * g4) and e_sum[s] < 1e-5):
+            failures.append(f"shell {s} map")
     for row, s in enumerate(ref["cl_shells"]):
         m = maps[int(s)]
         cl = sht.anafast(m / m.mean() - 1.0, lmax).cpu().numpy()
-        _check_cl(f"shell {int(s)}", cl, ref["shell_cl_f64"][row], ref["shell_cl_f32"][row], lmax)
+        _check_cl(f"shell {int(s)}", cl, ref["shell_cl_f64"][row], ref["shell_cl_f32"][row], lmax, failures)
+    assert not failures, failures
