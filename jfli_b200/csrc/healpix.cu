@@ -181,19 +181,19 @@ __device__ __forceinline__ void pix_centre_ring(long long pix, int nside, const 
   phi = ((double)(pix - r.start) + 0.5 * r.shifted) * (2.0 * M_PI / r.npix);
 }
 
-// Deposit of weight w at direction (vx, vy, vz) (length rr > 0) on the RING map.
+// Deposit of weight w at direction (vx, vy, vz) (length rr > 0, FP64) on the RING map.
 // scheme 0: nearest pixel; 1: bilinear weights of the 4 surrounding pixel centres; 2 (the
 // "rbf_neighbor" scheme): the same 4 pixels weighted by a Gaussian radial basis function of
 // the angle d between the direction and each pixel centre, exp(-d^2 / (2 sigma^2)),
 // normalised to sum 1 (sigma in radians; taken relative to the nearest centre, so the
 // weights never all underflow).
-__device__ __forceinline__ void deposit_direction(float vx, float vy, float vz, float rr, float w, int nside,
+__device__ __forceinline__ void deposit_direction(double vx, double vy, double vz, double rr, float w, int nside,
                                                   int scheme, const double* __restrict__ theta_tab,
                                                   float* __restrict__ map, float sigma = 0.f) {
   const long long npix = 12LL * nside * nside;
-  const double dr = (double)rr;
-  const double zc = (double)vz / dr;
-  const double phi = atan2((double)vy, (double)vx);
+  const double dr = rr;
+  const double zc = vz / dr;
+  const double phi = atan2(vy, vx);
   if (scheme == 0) {
     const long long pix = ang2pix_ring(zc, phi, nside);
     if (pix >= 0 && pix < npix) atomicAdd(map + pix, w);
@@ -201,7 +201,7 @@ __device__ __forceinline__ void deposit_direction(float vx, float vy, float vz, 
     long long pix[4];
     double wt[4];
     interp_weights(acos(fmin(1.0, fmax(-1.0, zc))), phi, nside, theta_tab, pix, wt);
-    const double ux = (double)vx / dr, uy = (double)vy / dr, uz = zc;
+    const double ux = vx / dr, uy = vy / dr, uz = zc;
     double d2[4], dmin = 1e300;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -233,9 +233,12 @@ __device__ __forceinline__ void deposit_direction(float vx, float vy, float vz, 
   }
 }
 
+// The observer-centred position, its length and the shell test are FP64 (from the FP32
+// positions): an FP32 |x - o| at a few hundred Mpc/h carries ~1e-5 Mpc/h of rounding, which
+// moves particles within that distance of an edge across it.
 __global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, const float* __restrict__ weights,
-                                float weight, MeshDims d, float3 cell, float3 obs, float rmin, float rmax, int nside,
-                                int scheme, const double* __restrict__ theta_tab, float* __restrict__ map,
+                                float weight, MeshDims d, double3 cell, double3 obs, double rmin, double rmax,
+                                int nside, int scheme, const double* __restrict__ theta_tab, float* __restrict__ map,
                                 float sigma) {
   const long long np = d.cells();
   const long long npix = 12LL * nside * nside;
@@ -245,18 +248,18 @@ __global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, co
   if (weights) weights += (long long)b * np;
   const long long yz = (long long)d.ny * d.nz;
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
-    float gx = disp[3 * p + 0], gy = disp[3 * p + 1], gz = disp[3 * p + 2];
+    double gx = disp[3 * p + 0], gy = disp[3 * p + 1], gz = disp[3 * p + 2];
     if (!absolute) {
       const int i = (int)(p / yz);
       const long long r = p - (long long)i * yz;
       const int j = (int)(r / d.nz);
       const int k = (int)(r - (long long)j * d.nz);
-      gx += (float)i;
-      gy += (float)j;
-      gz += (float)k;
+      gx += (double)i;
+      gy += (double)j;
+      gz += (double)k;
     }
-    const float vx = gx * cell.x - obs.x, vy = gy * cell.y - obs.y, vz = gz * cell.z - obs.z;
-    const float rr = sqrtf(vx * vx + vy * vy + vz * vz);
+    const double vx = gx * cell.x - obs.x, vy = gy * cell.y - obs.y, vz = gz * cell.z - obs.z;
+    const double rr = sqrt(vx * vx + vy * vy + vz * vz);
     if (!(rr > rmin && rr <= rmax)) continue;
     deposit_direction(vx, vy, vz, rr, weights ? weights[p] * weight : weight, nside, scheme, theta_tab, map, sigma);
   }
@@ -271,7 +274,10 @@ __global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, co
 //   onion:     x' = q + o, distance |x' - o|, x' += D M v
 //   telephoto: distance |q - o| (the reference measures it from the observer-centred q),
 //              q += D M v, x' = q + o
-// and x' is painted on the shell rmin < |x' - o| <= rmax.
+// and x' is painted on the shell rmin < |x' - o| <= rmax. The cull below runs in FP32 with
+// margins; a copy that passes it is placed again in FP64 (c, q and q + D M v, whose length
+// is x' - o without the FP32 rounding of adding and removing o), and the shell test and the
+// direction use that.
 //
 // Copies that cannot reach the shell are skipped before the drift. With D bounded by
 // dbound (the host's bound on |D| over the distance table: the Gp difference is at most
@@ -306,19 +312,11 @@ __global__ void __launch_bounds__(256, 4)
     cm2 = cm > 0.f ? cm * cm * (1.f - 1e-6f) : -1.f;
   }
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
-    float x, y, z;
-    if (absolute) {
-      x = disp[3 * p + 0] / nx * box.x;
-      y = disp[3 * p + 1] / ny * box.y;
-      z = disp[3 * p + 2] / nz * box.z;
-    } else {
-      int i, j, k;
-      particle_ijk(g, p, i, j, k);
-      x = ((float)i + disp[3 * p + 0]) / nx * box.x;
-      y = ((float)j + disp[3 * p + 1]) / ny * box.y;
-      z = ((float)k + disp[3 * p + 2]) / nz * box.z;
-    }
-    const float c[3] = {x - obs.x, y - obs.y, z - obs.z};
+    const float d0 = disp[3 * p + 0], d1 = disp[3 * p + 1], d2 = disp[3 * p + 2];  // grid units
+    int i = 0, j = 0, k = 0;
+    if (!absolute) particle_ijk(g, p, i, j, k);
+    const float c[3] = {((float)i + d0) / nx * box.x - obs.x, ((float)j + d1) / ny * box.y - obs.y,
+                        ((float)k + d2) / nz * box.z - obs.z};
     float v[3] = {0.f, 0.f, 0.f}, vmag = 0.f;
     if (vel) {
       v[0] = vel[3 * p + 0];
@@ -342,42 +340,34 @@ __global__ void __launch_bounds__(256, 4)
       const float qn2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
       // the bounds hold while the drift distance lies inside the distance table
       if ((!vel || qn2 <= cm2) && (qn2 <= lo2 || qn2 > hi2)) continue;
-      float px, py, pz;  // painted position, Mpc/h
+      // the copy in FP64: cd = x - o, qd = M cd + s (M a signed permutation)
+      const double cd[3] = {((double)i + (double)d0) / nx * box.x - obs.x, ((double)j + (double)d1) / ny * box.y - obs.y,
+                            ((double)k + (double)d2) / nz * box.z - obs.z};
+      double qd[3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        qd[r] = (double)M[3 * r + 0] * cd[0] + (double)M[3 * r + 1] * cd[1] + (double)M[3 * r + 2] * cd[2] +
+                (double)ts.shift[tile][r];
       if (vel) {
-        float dist;
+        double dist;
         if (telephoto) {
-          const float ex = q[0] - obs.x, ey = q[1] - obs.y, ez = q[2] - obs.z;
-          dist = sqrtf(ex * ex + ey * ey + ez * ez);
+          const double ex = qd[0] - obs.x, ey = qd[1] - obs.y, ez = qd[2] - obs.z;
+          dist = sqrt(ex * ex + ey * ey + ez * ez);
         } else {
-          const float ex = (q[0] + obs.x) - obs.x, ey = (q[1] + obs.y) - obs.y, ez = (q[2] + obs.z) - obs.z;
-          dist = sqrtf(ex * ex + ey * ey + ez * ez);
+          dist = sqrt(qd[0] * qd[0] + qd[1] * qd[1] + qd[2] * qd[2]);
         }
-        const float at = interp_table(dist, tb.chi, tb.a_chi, tb.n_chi);
+        const float at = interp_table((float)dist, tb.chi, tb.a_chi, tb.n_chi);
         const float ac = sqrtf(t * at);
         const float gp_at = fminf(fmaxf(interp_table(at, tb.ga, tb.g, tb.n_g), 0.f), 1.f);
         const float drift = (gp_at - gp_t) / interp_table(ac, tb.da, tb.dgfa, tb.n_d);
-        float vr[3];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
-          vr[r] = (float)M[3 * r + 0] * v[0] + (float)M[3 * r + 1] * v[1] + (float)M[3 * r + 2] * v[2];
-        if (telephoto) {
-          px = (q[0] + drift * vr[0]) + obs.x;
-          py = (q[1] + drift * vr[1]) + obs.y;
-          pz = (q[2] + drift * vr[2]) + obs.z;
-        } else {
-          px = (q[0] + obs.x) + drift * vr[0];
-          py = (q[1] + obs.y) + drift * vr[1];
-          pz = (q[2] + obs.z) + drift * vr[2];
-        }
-      } else {
-        px = q[0] + obs.x;
-        py = q[1] + obs.y;
-        pz = q[2] + obs.z;
+          qd[r] += (double)(drift * ((float)M[3 * r + 0] * v[0] + (float)M[3 * r + 1] * v[1] +
+                                     (float)M[3 * r + 2] * v[2]));
       }
-      const float vx = px - obs.x, vy = py - obs.y, vz = pz - obs.z;
-      const float rr = sqrtf(vx * vx + vy * vy + vz * vz);
-      if (!(rr > rmin && rr <= rmax)) continue;
-      deposit_direction(vx, vy, vz, rr, w, nside, scheme, theta_tab, map);
+      const double rr = sqrt(qd[0] * qd[0] + qd[1] * qd[1] + qd[2] * qd[2]);
+      if (!(rr > (double)rmin && rr <= (double)rmax)) continue;
+      deposit_direction(qd[0], qd[1], qd[2], rr, w, nside, scheme, theta_tab, map);
     }
   }
 }
@@ -500,8 +490,8 @@ static const double* ring_theta_table(int nside) {
 cudaError_t healpix_paint(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d,
                           const float* box, const float* observer, float rmin, float rmax, int nside, int scheme,
                           float* map, cudaStream_t s, float sigma) {
-  const float3 cell = make_float3(box[0] / d.nx, box[1] / d.ny, box[2] / d.nz);
-  const float3 obs = make_float3(observer[0], observer[1], observer[2]);
+  const double3 cell = make_double3((double)box[0] / d.nx, (double)box[1] / d.ny, (double)box[2] / d.nz);
+  const double3 obs = make_double3(observer[0], observer[1], observer[2]);
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

@@ -116,9 +116,31 @@ class DriftInterp(AbstractInterp):
         dx, p = y
         r_center = float(self.r_centers[state.shell_idx])
         width = float(self.density_widths[state.shell_idx])
-        drifted = drift_to_lightcone(dx, p, float(t), cosmo)
-        res = self._paint_target(drifted, r_center, width)
+        res = _drifted_shell(dx, p, t, cosmo, r_center, width, self.painting)
+        if res is None:
+            res = self._paint_target(drift_to_lightcone(dx, p, float(t), cosmo), r_center, width)
+        else:
+            res = _spherical_result(res, t, r_center, width)
         return res.replace(scale_factors=t, comoving_centers=r_center, density_width=width)
+
+
+def _drifted_shell(dx, p, t, cosmo, r_center: float, width: float, painting):
+    """The spherical shell of the particles drifted to their light-cone crossing, drifted
+    and painted in one pass by the replica painter with a single identity replica, which
+    places each particle and tests the shell edges in FP64. (A drifted copy of the
+    positions in FP32 Mpc/h rounds them by ~1e-5 Mpc/h at a few hundred Mpc/h, enough to
+    move particles near an edge across it.) None when the painting options need the
+    general path: another target, a scheme the replica painter does not have, or a batch
+    of particle sets (painted one shell per set by paint_spherical)."""
+    if painting is None or painting.target != "spherical" or painting.scheme not in ("ngp", "bilinear") or \
+            dx.array.ndim != 4:
+        return None
+    from ..fields import SphericalDensity
+    from ..painting import paint_shell_tiled
+
+    m = paint_shell_tiled(_at_paint_nside(dx, painting), p.array, r_center, width, np.eye(3)[None], np.zeros((1, 3)),
+                          telephoto=False, t=float(t), cosmo=cosmo, scheme=painting.scheme, weights=painting.weights)
+    return SphericalDensity.FromDensityMetadata(array=_regrade(m, dx, painting), field=dx)
 
 
 def drift_to_lightcone(dx, p, t: float, cosmo):
@@ -215,8 +237,10 @@ class OnionTiler(AbstractInterp):
         width = float(self.density_widths[state.shell_idx])
         pt = self.painting
         if r_center + width / 2 <= self.max_comoving_distance:
-            src = drift_to_lightcone(dx, p, float(t), cosmo) if self.drift_on_lightcone else dx
-            res = self._paint_target(src, r_center, width)
+            res = _drifted_shell(dx, p, t, cosmo, r_center, width, pt) if self.drift_on_lightcone else None
+            if res is None:
+                src = drift_to_lightcone(dx, p, float(t), cosmo) if self.drift_on_lightcone else dx
+                res = self._paint_target(src, r_center, width)
         else:
             from ..fields import SphericalDensity
             from ..painting import paint_shell_tiled

@@ -9,11 +9,14 @@ the oracle's white noise and rotation draw.
 Every error is stated against the FP64 oracle, beside the FP32 oracle's own distance from
 FP64. Bounds: C_ell of the convergence map and of shells 3, 8 and 15 within 1e-4 per band
 of 8 multipoles and 5e-4 per multipole (or 2x the FP32 oracle's own error where that is
-larger); the maps averaged to nside 4 within 1e-5 relative L2 (or 2x the FP32 oracle's
-gap), printed at nside 16; the shells' totals within 1e-5. A shell counts particles
+larger); the shell maps averaged to nside 4 within 1e-5 relative L2 (or 2x the FP32
+oracle's gap), printed at nside 16; the shells' totals within 1e-5; the convergence map
+averaged to nside 4 within 2e-5 (or 2x the FP32 oracle's gap). A shell counts particles
 between two radii, so a particle that rounding moves across an edge moves its whole
 weight: the bands and the coarse maps average that out, the per-multipole and nside-16
-figures show it.
+figures show it. The convergence map's large scales are a small residual of all sixteen
+shells (its rms at nside 4 is a seventh of the full map's), so one such particle moves it
+by about 1e-5 at nside 4; its bound allows two.
 """
 
 from __future__ import annotations
@@ -85,7 +88,7 @@ def test_config5_lightcone_chain(cosmo):
           f"{float(ref['gap_kappa_f32']):.2e}); rms {rms:.4e} vs {float(ref['kappa_rms_f64']):.4e}")
     k64 = ref["kappa_coarse_f64"]
     print(f"kappa mean {float(kappa.mean()):.3e}; coarse-map projection on the FP64 one {kc @ k64 / (k64 @ k64):.8f}")
-    if not e4 < max(1e-5, 2 * g4):
+    if not e4 < max(2e-5, 2 * g4):
         failures.append("kappa map")
     # shells
     coarse = ud_grade(maps, nc).cpu().numpy()
