@@ -82,6 +82,10 @@ def parse():
                     help="instead of the step benchmark, run the Poisson chain on a seeded density of this mesh size "
                          "twice with the register x pass and twice with the TMA-staged one (a short case to profile "
                          "the two x-pass kernels) and print their CUDA-event times")
+    ap.add_argument("--kkd-sweep", type=int, default=0,
+                    help="instead of the step benchmark, time the ReversibleDoubleKickDrift loop (38 steps from 2LPT "
+                         "ICs at this mesh, L = 4 Mpc/h per cell) and its reverse sweep, recomputing and with stored "
+                         "potentials; the last stored sweep runs inside an NVTX range 'kkd_sweep' (for a launch list)")
     ap.add_argument("--paint-order", type=int, default=0,
                     help="instead of the step benchmark, evolve this mesh size to the last of the 40 steps and time "
                          "the CIC paint and readout in Lagrangian and in cell-sorted particle order, and the sort")
@@ -730,6 +734,49 @@ def x_pass_variants(n, iters=20):
     return out
 
 
+def kkd_sweep_case(n, steps=38, reps=3):
+    """The gradient requests' dominant work at n^3: the ReversibleDoubleKickDrift loop
+    (jfli_kkd_run / _stored) and the reverse sweep from its final state with a random
+    density cotangent (jfli_kkd_adjoint / _stored). CUDA-event ms, the last of `reps`
+    warmed runs; the last stored run sits in the NVTX range 'kkd_sweep'."""
+    import torch
+
+    import jfli_b200 as jf
+    from jfli_b200 import ops
+    from jfli_b200.pm.adjoint import forward_tables
+
+    box = 4.0 * n
+    cosmo = jf.Planck18()
+    ic = jf.interpolate_initial_conditions(jf.white_noise(3, (n, n, n)), (n, n, n), (box,) * 3, cosmo=cosmo)
+    dx, p = jf.lpt(cosmo, ic, ts=0.1, order=2)
+    tab = forward_tables(0.2607, 0.8102, t0=0.1, t1=1.0, dt0=0.9 / steps, derivatives=False)
+    x0, v0 = dx.array.contiguous().clone(), p.array.contiguous().clone()
+    rho = torch.empty(n, n, n, device="cuda")
+    grho = 1e-3 * torch.randn(n, n, n, device="cuda", generator=torch.Generator(device="cuda").manual_seed(1))
+    out = {"mesh": n, "steps": steps}
+    for mode in ("recompute", "stored"):
+        pots = torch.empty(steps, n, n, n, device="cuda") if mode == "stored" else None
+        for rep in range(reps):
+            last = mode == "stored" and rep == reps - 1
+            if last:
+                torch.cuda.nvtx.range_push("kkd_sweep")
+            x, v = x0.clone(), v0.clone()
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record()
+            ops.kkd_run(x, v, tab.kicks, tab.drifts, rho, pots=pots)
+            e[1].record()
+            lx, lv = torch.zeros_like(x), torch.zeros_like(v)
+            ops.adjoint_position(x, lx, rho_bar=grho)
+            ops.kkd_adjoint(x, v, lx, lv, tab.kicks, tab.drifts, pots=pots)
+            e[2].record()
+            torch.cuda.synchronize()
+            if last:
+                torch.cuda.nvtx.range_pop()
+        out[f"{mode}_forward_ms"] = round(e[0].elapsed_time(e[1]), 3)
+        out[f"{mode}_reverse_ms"] = round(e[1].elapsed_time(e[2]), 3)
+    return out
+
+
 def paint_order_probe(n, iters=10):
     """What a cell-ordered particle sort would buy the particle pass, measured on the
     state entering the last of the 40 steps at n^3 (the most clustered state of the run):
@@ -942,6 +989,9 @@ def main():
         return
     if args.tiled_paint:
         run_tiled_paint(args)
+        return
+    if args.kkd_sweep:
+        print(json.dumps({"kkd_sweep": kkd_sweep_case(args.kkd_sweep)}), flush=True)
         return
     if args.paint_order:
         print(json.dumps({"paint_order_probe": paint_order_probe(args.paint_order)}), flush=True)

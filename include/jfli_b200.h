@@ -394,6 +394,20 @@ int jfli_kkd_adjoint(void* stream, float* disp, float* vel, float* lam_x, float*
                      const float* drifts, int nsteps, double* sens, void* workspace, size_t workspace_bytes, int nx,
                      int ny, int nz, int batch, char* err, size_t errlen);
 
+/* The same pair trading memory for work: jfli_kkd_run_stored writes the potential whose
+ * force kicks step i to pots[i] (device, nsteps x batch x nx ny nz floats, [step][batch]
+ * [cells]); jfli_kkd_adjoint_stored then rebuilds each step's force mesh from pots[i]
+ * instead of un-drifting, painting and solving for it, and un-drifts the positions inside
+ * the cotangent paint. The forward results are those of jfli_kkd_run; the reverse sweep
+ * uses the forward pass's own forces (the recomputing sweep uses forces at the
+ * reconstructed positions, equal up to FP32 rounding). Same workspace. */
+int jfli_kkd_run_stored(void* stream, float* disp, float* vel, const float* kicks, const float* drifts, int nsteps,
+                        float* rho, float* pots, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
+                        int batch, char* err, size_t errlen);
+int jfli_kkd_adjoint_stored(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
+                            const float* drifts, int nsteps, const float* pots, double* sens, void* workspace,
+                            size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
 /* dL/dmesh of P(k): out = irfft(rfft(mesh) * weights[digitize(|k|, kedges)] / M), with
  * weights[b] = 2 (dL/dP_b) prod(L/N) / count_b for the kept bins and 0 for bin 0 and
  * bin nedges. Workspace: jfli_poisson_workspace_bytes. */

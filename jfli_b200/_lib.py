@@ -161,6 +161,16 @@ _SIGNATURES = {
         [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_float), ctypes.POINTER(c_float), c_int,
          c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
     ),
+    "jfli_kkd_run_stored": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_float), ctypes.POINTER(c_float), c_int, c_void_p, c_void_p,
+         c_void_p, c_size_t, *_DIMS, *_ERR],
+    ),
+    "jfli_kkd_adjoint_stored": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_float), ctypes.POINTER(c_float), c_int,
+         c_void_p, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
+    ),
     "jfli_adjoint_unkick_paint": (
         c_int,
         [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_float, c_void_p, c_void_p, c_size_t,

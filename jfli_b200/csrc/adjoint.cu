@@ -45,43 +45,135 @@ __device__ __forceinline__ void block_sum2(double& a, double& b) {
   }
 }
 
+// CIC deposit of the vector u on a float4 mesh [cell] = (u0, u1, u2, 0), one 16-byte vector
+// atomic per corner where three meshes take three scalar ones. The lanes hold consecutive
+// particles of one z row (the grid-stride loop; the active lanes a prefix of the warp),
+// with deposit_lane_merged's z merge: when lane L's
+// upper-z corners are lane L+1's lower-z corners, lane L+1 receives lane L's vector and its
+// four upper-z weights and adds them to its own lower-z deposits (one vector atomic per
+// shared cell instead of two).
+__device__ __forceinline__ void deposit_vec4_lane_merged(float4* mesh, const PGrid& g, const Cic1& cx, const Cic1& cy,
+                                                         const Cic1& cz, const float u[3]) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int xy0 = cx.i0 * g.yz + cy.i0 * g.nz;
+  const int lo = xy0 + cz.i0, hi = xy0 + cz.i1;
+  const int next_lo = __shfl_down_sync(mask, lo, 1);
+  const int prev_hi = __shfl_up_sync(mask, hi, 1);
+  const bool give = lane < 31 && ((mask >> (lane + 1)) & 1u) && next_lo == hi;
+  const bool take = lane > 0 && ((mask >> (lane - 1)) & 1u) && prev_hi == lo;
+  const float p0 = __shfl_up_sync(mask, u[0], 1), p1 = __shfl_up_sync(mask, u[1], 1),
+              p2 = __shfl_up_sync(mask, u[2], 1);
+  const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz};
+  const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1};
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const float wab = wx[a] * wy[b];
+      const float up = wab * cz.w1;
+      const float recv = __shfl_up_sync(mask, up, 1);
+      const float wl = wab * cz.w0;
+      float4 low = make_float4(wl * u[0], wl * u[1], wl * u[2], 0.f);
+      if (take) {
+        low.x += recv * p0;
+        low.y += recv * p1;
+        low.z += recv * p2;
+      }
+      atomicAdd(mesh + (xo[a] + yo[b] + cz.i0), low);
+      if (!give) atomicAdd(mesh + (xo[a] + yo[b] + cz.i1), make_float4(up * u[0], up * u[1], up * u[2], 0.f));
+    }
+}
+
 // Reverse kick + first half of the VJP of one reversible step, at the un-drifted
 // positions x (relative displacements). Per particle:
 //   F = R_x[force];  <lambda_x, v'> -> partial[1];  u = lambda_v + drift * lambda_x;
 //   <u, F> -> partial[0];  v = v' - kick F;  lambda_v = u;  ubar_a += W * u_a.
 // partials holds 2 doubles per CTA and batch entry, summed in a fixed order later.
+// ubar: three meshes [3][cells] (kVec4 false) or one float4 mesh [cells] (kVec4 true).
+// With undrift (the float4 form of the reverse sweep over stored potentials), disp holds
+// x' on entry: the particle is first un-drifted, x = x' - drift v', and x is written back.
+template <bool kVec4>
+__device__ __forceinline__ void unkick_particle(float* __restrict__ disp, bool undrift, float* __restrict__ vel,
+                                                const float* __restrict__ lam_x, float* __restrict__ lam_v,
+                                                const float* __restrict__ force, float kick, float drift,
+                                                float* __restrict__ ubar, const PGrid& g, unsigned p, int i, int j,
+                                                int k, double& sk, double& sd) {
+  float v[3], x[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    v[a] = vel[3 * p + a];
+    x[a] = disp[3 * p + a];
+  }
+  if (undrift) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      x[a] += v[a] * -drift;
+      disp[3 * p + a] = x[a];
+    }
+  }
+  const Cic1 cx = cic_rel(i, x[0], g.nx), cy = cic_rel(j, x[1], g.ny), cz = cic_rel(k, x[2], g.nz);
+  float f[3];
+  gather_force_mesh(force, g, cx, cy, cz, f[0], f[1], f[2]);
+  float u[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float lx = lam_x[3 * p + a];
+    sd += (double)lx * (double)v[a];
+    u[a] = lam_v[3 * p + a] + drift * lx;
+    sk += (double)u[a] * (double)f[a];
+    vel[3 * p + a] = v[a] - f[a] * kick;
+    lam_v[3 * p + a] = u[a];
+  }
+  if (kVec4) {
+    deposit_vec4_lane_merged(reinterpret_cast<float4*>(ubar), g, cx, cy, cz, u);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) deposit(ubar + (size_t)a * g.np, g, cx, cy, cz, u[a]);
+  }
+}
+
+constexpr int kAdjBrickY = 8, kAdjBrickZ = 32;
+
+// Work order of the float4 form: when nz is a multiple of 32 and ny of 8, a CTA of 8 warps
+// takes an 8 (y) x 32 (z) brick of Lagrangian cells and walks it along x in chunks of
+// xdepth planes (brick_xdepth), each warp on one z row (the z merge of the deposit needs consecutive z in a
+// warp), so that the rows and planes whose particles share CIC corners gather and deposit
+// on one SM close in time (as the forward particle pass). Otherwise a grid-stride walk.
+template <bool kVec4>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_unkick_paint(
-    const float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ lam_x,
+    float* __restrict__ disp, int undrift, float* __restrict__ vel, const float* __restrict__ lam_x,
     float* __restrict__ lam_v, const float* __restrict__ force, float kick, float drift, float* __restrict__ ubar,
-    double* __restrict__ partials, PGrid g) {
+    double* __restrict__ partials, PGrid g, int xdepth) {
   const long long b = blockIdx.y;
   disp += b * g.np * 3;
   vel += b * g.np * 3;
   lam_x += b * g.np * 3;
   lam_v += b * g.np * 3;
   force += b * g.np * 4;
-  ubar += b * g.np * 3;
+  ubar += b * g.np * (kVec4 ? 4 : 3);
   double sk = 0.0, sd = 0.0;
-  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
-    int i, j, k;
-    particle_ijk(g, p, i, j, k);
-    const Cic1 cx = cic_rel(i, disp[3 * p + 0], g.nx), cy = cic_rel(j, disp[3 * p + 1], g.ny),
-               cz = cic_rel(k, disp[3 * p + 2], g.nz);
-    float f[3];
-    gather_force_mesh(force, g, cx, cy, cz, f[0], f[1], f[2]);
-    float u[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float v = vel[3 * p + a];
-      const float lx = lam_x[3 * p + a];
-      sd += (double)lx * (double)v;
-      u[a] = lam_v[3 * p + a] + drift * lx;
-      sk += (double)u[a] * (double)f[a];
-      vel[3 * p + a] = v - f[a] * kick;
-      lam_v[3 * p + a] = u[a];
+  if (kVec4 && blockDim.x == kAdjBrickY * kAdjBrickZ && g.nz % kAdjBrickZ == 0 && g.ny % kAdjBrickY == 0) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int tz = g.nz / kAdjBrickZ, ty = g.ny / kAdjBrickY, txc = (g.nx + xdepth - 1) / xdepth;
+    const long long items = (long long)tz * ty * txc;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+      const int iz = (int)(it % tz);
+      const long long rest = it / tz;
+      const int iy = (int)(rest % ty), xc = (int)(rest / ty);
+      const int j = iy * kAdjBrickY + w, k = iz * kAdjBrickZ + lane;
+      const int i1 = min(g.nx, (xc + 1) * xdepth);
+      for (int i = xc * xdepth; i < i1; ++i)
+        unkick_particle<kVec4>(disp, undrift != 0, vel, lam_x, lam_v, force, kick, drift, ubar, g,
+                               ((unsigned)i * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)k, i, j, k,
+                               sk, sd);
     }
-#pragma unroll
-    for (int a = 0; a < 3; ++a) deposit(ubar + (size_t)a * g.np, g, cx, cy, cz, u[a]);
+  } else {
+    for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+      int i, j, k;
+      particle_ijk(g, p, i, j, k);
+      unkick_particle<kVec4>(disp, undrift != 0, vel, lam_x, lam_v, force, kick, drift, ubar, g, p, i, j, k, sk, sd);
+    }
   }
   block_sum2(sk, sd);
   if (threadIdx.x == 0) {
@@ -133,9 +225,58 @@ __global__ void k_div_fd(const float* __restrict__ u, float alpha, const float* 
 // at relative positions disp. Either of rho_bar or (u, force) may be null. The gradient
 // of the trilinear weights is one-sided at cell faces, like the derivative of the
 // floor-based weights.
-__global__ void k_adj_position(const float* __restrict__ disp, const float* __restrict__ u,
-                               const float* __restrict__ rho_bar, const float* __restrict__ force, float scale,
-                               float* __restrict__ lam_x, PGrid g) {
+__device__ __forceinline__ void adj_position_particle(const float* __restrict__ disp, const float* __restrict__ u,
+                                                      const float* __restrict__ rho_bar,
+                                                      const float* __restrict__ force, float scale,
+                                                      float* __restrict__ lam_x, const PGrid& g, unsigned p, int i,
+                                                      int j, int k) {
+  const Cic1 cx = cic_rel(i, disp[3 * p + 0], g.nx), cy = cic_rel(j, disp[3 * p + 1], g.ny),
+             cz = cic_rel(k, disp[3 * p + 2], g.nz);
+  const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
+  float ua[3] = {0.f, 0.f, 0.f};
+  if (u && force) {
+    ua[0] = u[3 * p + 0];
+    ua[1] = u[3 * p + 1];
+    ua[2] = u[3 * p + 2];
+  }
+  float h[2][2][2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int o = xo[a] + yo[bb] + zo[c];
+        float v = rho_bar ? __ldg(rho_bar + o) : 0.f;
+        if (u && force) {
+          const float4 f = __ldg(reinterpret_cast<const float4*>(force) + o);
+          v += ua[0] * f.x + ua[1] * f.y + ua[2] * f.z;
+        }
+        h[a][bb][c] = v;
+      }
+  const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
+  float gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+  for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) gx += wy[bb] * wz[c] * (h[1][bb][c] - h[0][bb][c]);
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) gy += wx[a] * wz[c] * (h[a][1][c] - h[a][0][c]);
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int bb = 0; bb < 2; ++bb) gz += wx[a] * wy[bb] * (h[a][bb][1] - h[a][bb][0]);
+  lam_x[3 * p + 0] += scale * gx;
+  lam_x[3 * p + 1] += scale * gy;
+  lam_x[3 * p + 2] += scale * gz;
+}
+
+__global__ void __launch_bounds__(256) k_adj_position(const float* __restrict__ disp, const float* __restrict__ u,
+                                                      const float* __restrict__ rho_bar,
+                                                      const float* __restrict__ force, float scale,
+                                                      float* __restrict__ lam_x, PGrid g) {
   const long long b = blockIdx.y;
   disp += b * g.np * 3;
   lam_x += b * g.np * 3;
@@ -145,47 +286,7 @@ __global__ void k_adj_position(const float* __restrict__ disp, const float* __re
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
     particle_ijk(g, p, i, j, k);
-    const Cic1 cx = cic_rel(i, disp[3 * p + 0], g.nx), cy = cic_rel(j, disp[3 * p + 1], g.ny),
-               cz = cic_rel(k, disp[3 * p + 2], g.nz);
-    const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
-    float ua[3] = {0.f, 0.f, 0.f};
-    if (u && force) {
-      ua[0] = u[3 * p + 0];
-      ua[1] = u[3 * p + 1];
-      ua[2] = u[3 * p + 2];
-    }
-    float h[2][2][2];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int bb = 0; bb < 2; ++bb)
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const int o = xo[a] + yo[bb] + zo[c];
-          float v = rho_bar ? __ldg(rho_bar + o) : 0.f;
-          if (u && force) {
-            const float4 f = __ldg(reinterpret_cast<const float4*>(force) + o);
-            v += ua[0] * f.x + ua[1] * f.y + ua[2] * f.z;
-          }
-          h[a][bb][c] = v;
-        }
-    const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
-    float gx = 0.f, gy = 0.f, gz = 0.f;
-#pragma unroll
-    for (int bb = 0; bb < 2; ++bb)
-#pragma unroll
-      for (int c = 0; c < 2; ++c) gx += wy[bb] * wz[c] * (h[1][bb][c] - h[0][bb][c]);
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int c = 0; c < 2; ++c) gy += wx[a] * wz[c] * (h[a][1][c] - h[a][0][c]);
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int bb = 0; bb < 2; ++bb) gz += wx[a] * wy[bb] * (h[a][bb][1] - h[a][bb][0]);
-    lam_x[3 * p + 0] += scale * gx;
-    lam_x[3 * p + 1] += scale * gy;
-    lam_x[3 * p + 2] += scale * gz;
+    adj_position_particle(disp, u, rho_bar, force, scale, lam_x, g, p, i, j, k);
   }
 }
 
@@ -229,18 +330,27 @@ cudaError_t sum_adjoint_partials(const double* partials, const MeshDims& d, doub
 
 cudaError_t adjoint_unkick_paint(const float* disp, float* vel, const float* lam_x, float* lam_v, const float* force,
                                  float kick, float drift, float* ubar, double* partials, const MeshDims& d,
-                                 cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(ubar, 0, sizeof(float) * 3 * (size_t)d.cells() * d.batch, s);
+                                 cudaStream_t s, bool vec4, float* undrift_disp) {
+  // without undrift_disp the kernel only reads the positions
+  float* dp = undrift_disp ? undrift_disp : const_cast<float*>(disp);
+  const int undrift = undrift_disp != nullptr;
+  cudaError_t e = cudaMemsetAsync(ubar, 0, sizeof(float) * (vec4 ? 4 : 3) * (size_t)d.cells() * d.batch, s);
   if (e != cudaSuccess) return e;
-  k_adj_unkick_paint<<<adj_grid(d), kAdjThreads, 0, s>>>(disp, vel, lam_x, lam_v, force, kick, drift, ubar, partials,
-                                                          make_pgrid(d));
+  if (vec4)
+    k_adj_unkick_paint<true><<<adj_grid(d), kAdjThreads, 0, s>>>(dp, undrift, vel, lam_x, lam_v, force, kick, drift, ubar,
+                                                                 partials, make_pgrid(d),
+                                                                 brick_xdepth(d.nx, d.ny, d.nz, d.batch, 4ll * sm_count()));
+  else
+    k_adj_unkick_paint<false><<<adj_grid(d), kAdjThreads, 0, s>>>(dp, undrift, vel, lam_x, lam_v, force, kick, drift, ubar,
+                                                                  partials, make_pgrid(d), 16);
   note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t divergence_fd(const float* u, float alpha, const float* w, float beta, int aos, int accumulate,
                           float* out, const MeshDims& d, cudaStream_t s) {
-  const long long cell_stride = aos ? 3 : 1;
+  // aos 0: three meshes; 1: particle grids (3 floats per cell); 2: float4 meshes
+  const long long cell_stride = aos == 2 ? 4 : (aos ? 3 : 1);
   const long long comp_stride = aos ? 1 : d.cells();
   k_div_fd<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(u, alpha, w, beta, cell_stride, comp_stride,
                                                                           accumulate, out, make_pgrid(d));

@@ -908,9 +908,10 @@ struct KkdWs {
   double* partials;
 };
 
+// ubar is one float4 mesh (the cotangent paint takes one vector atomic per corner)
 size_t kkd_ws_bytes(const MeshDims& d) {
   return spec_bytes(d) + 4 * mesh_bytes(d) + align256(sizeof(float) * 4 * (size_t)d.cells() * d.batch) +
-         align256(sizeof(float) * 3 * (size_t)d.cells() * d.batch) +
+         align256(sizeof(float) * 4 * (size_t)d.cells() * d.batch) +
          align256(sizeof(double) * jfli::adjoint_partials_count(d));
 }
 
@@ -930,30 +931,26 @@ KkdWs kkd_ws(void* w, const MeshDims& d) {
   k.force = (float*)p;
   p += align256(sizeof(float) * 4 * (size_t)d.cells() * d.batch);
   k.ubar = (float*)p;
-  p += align256(sizeof(float) * 3 * (size_t)d.cells() * d.batch);
+  p += align256(sizeof(float) * 4 * (size_t)d.cells() * d.batch);
   k.partials = (double*)p;
   return k;
 }
 
-// density of the current positions -> force mesh (in ws.force); with clear_rho the
-// density mesh comes out cleared (the r2c pass zeroes what it has read)
-cudaError_t kkd_force(float* disp, float* vel, float* rho, const KkdWs& w, const MeshDims& d, cudaStream_t s,
-                      bool clear_rho) {
+// density of the current positions -> potential (into pot) -> force mesh (in ws.force)
+cudaError_t kkd_force(float* disp, float* vel, float* rho, const KkdWs& w, float* pot, const MeshDims& d,
+                      cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * d.batch * sizeof(float), s);
   if (e == cudaSuccess) e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, 0.f, JFLI_STEP_PAINT, 1.0f, rho, d, s);
-  if (e == cudaSuccess) e = jfli::poisson_potential(rho, w.spec, w.pot, d, 1.0f, 1.0f, s, clear_rho ? rho : nullptr);
-  if (e == cudaSuccess) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
+  if (e == cudaSuccess) e = jfli::poisson_potential(rho, w.spec, pot, d, 1.0f, 1.0f, s);
+  if (e == cudaSuccess) e = jfli::force_mesh(pot, w.force, 1.0f, d, s);
   return e;
 }
-}  // namespace
 
-size_t jfli_kkd_workspace_bytes(int nx, int ny, int nz, int batch) {
-  return kkd_ws_bytes(MeshDims{nx, ny, nz, batch});
-}
-
-int jfli_kkd_run(void* stream, float* disp, float* vel, const float* kicks, const float* drifts, int nsteps,
-                 float* rho, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
-                 size_t errlen) {
+// The loop of jfli_kkd_run; with pots (nsteps potentials [step][batch][cells]) the
+// potential whose force kicks step i is written to pots[i] instead of the workspace.
+int kkd_run_impl(void* stream, float* disp, float* vel, const float* kicks, const float* drifts, int nsteps,
+                 float* rho, float* pots, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch,
+                 char* err, size_t errlen, const char* name) {
   CHECK_DIMS(nx, ny, nz, batch);
   CHECK_STENCIL(nx, ny, nz);
   CHECK_FFT(nx, ny, nz);
@@ -970,23 +967,29 @@ int jfli_kkd_run(void* stream, float* disp, float* vel, const float* kicks, cons
     return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, kkd_ws_bytes(d));
   cudaStream_t s = (cudaStream_t)stream;
   const KkdWs w = kkd_ws(workspace, d);
+  const size_t per = (size_t)d.cells() * batch;
+  auto pot_of = [&](int i) { return pots ? pots + (size_t)i * per : w.pot; };
   // rho is cleared right before each paint (zeroed lines still in L2 when the deposits come);
   // the last step's paint stays in rho (the density of the final positions)
-  cudaError_t e = kkd_force(disp, vel, rho, w, d, s, false);
+  cudaError_t e = kkd_force(disp, vel, rho, w, pot_of(0), d, s);
   for (int i = 0; i < nsteps && e == cudaSuccess; ++i) {
     e = jfli::zero_floats(rho, d.cells() * batch, s);
     if (e == cudaSuccess)
       e = jfli::kick_drift_paint(disp, vel, w.force, kicks[i], drifts[i], JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
                                  1.0f, rho, d, s);
-    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::poisson_potential(rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
-    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
+    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::poisson_potential(rho, w.spec, pot_of(i + 1), d, 1.0f, 1.0f, s);
+    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::force_mesh(pot_of(i + 1), w.force, 1.0f, d, s);
   }
-  return cuda_status(e, err, errlen, "jfli_kkd_run");
+  return cuda_status(e, err, errlen, name);
 }
 
-int jfli_kkd_adjoint(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
-                     const float* drifts, int nsteps, double* sens, void* workspace, size_t workspace_bytes, int nx,
-                     int ny, int nz, int batch, char* err, size_t errlen) {
+// The reverse sweep of jfli_kkd_adjoint. Without pots each step un-drifts and paints the
+// previous positions and solves for their force; with pots the force mesh is rebuilt from
+// the stored potential and the un-drift happens inside the cotangent paint.
+int kkd_adjoint_impl(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
+                     const float* drifts, int nsteps, const float* pots, double* sens, void* workspace,
+                     size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen,
+                     const char* name) {
   CHECK_DIMS(nx, ny, nz, batch);
   CHECK_STENCIL(nx, ny, nz);
   CHECK_FFT(nx, ny, nz);
@@ -1005,24 +1008,67 @@ int jfli_kkd_adjoint(void* stream, float* disp, float* vel, float* lam_x, float*
     return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, kkd_ws_bytes(d));
   cudaStream_t s = (cudaStream_t)stream;
   const KkdWs w = kkd_ws(workspace, d);
+  const size_t per = (size_t)d.cells() * batch;
   cudaError_t e = cudaSuccess;
   for (int i = nsteps - 1; i >= 0 && e == cudaSuccess; --i) {
     const float k = kicks[i], dr = drifts[i];
-    // un-drift and paint the previous positions, force mesh there
-    e = jfli::zero_floats(w.rho, d.cells() * batch, s);
-    if (e == cudaSuccess)
-      e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, -dr, JFLI_STEP_DRIFT | JFLI_STEP_PAINT, 1.0f, w.rho, d, s);
-    if (e == cudaSuccess) e = jfli::poisson_potential(w.rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
-    if (e == cudaSuccess) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
+    if (pots) {
+      // the force mesh of step i from its stored potential; un-drift in the paint below
+      e = jfli::force_mesh(pots + (size_t)i * per, w.force, 1.0f, d, s);
+    } else {
+      // un-drift and paint the previous positions, force mesh there
+      e = jfli::zero_floats(w.rho, d.cells() * batch, s);
+      if (e == cudaSuccess)
+        e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, -dr, JFLI_STEP_DRIFT | JFLI_STEP_PAINT, 1.0f, w.rho, d, s);
+      if (e == cudaSuccess) e = jfli::poisson_potential(w.rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
+      if (e == cudaSuccess) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
+    }
     // un-kick, adjoint paint, dL/dk and dL/dd
-    if (e == cudaSuccess) e = jfli::adjoint_unkick_paint(disp, vel, lam_x, lam_v, w.force, k, dr, w.ubar, w.partials, d, s);
+    if (e == cudaSuccess)
+      e = jfli::adjoint_unkick_paint(disp, vel, lam_x, lam_v, w.force, k, dr, w.ubar, w.partials, d, s, true,
+                                     pots ? disp : nullptr);
     if (e == cudaSuccess) e = jfli::sum_adjoint_partials(w.partials, d, sens + 2ll * i * batch, s);
     // rho_bar = P(div ubar); lam_x += k grad R[rho_bar + lam_v . F]
-    if (e == cudaSuccess) e = jfli::divergence_fd(w.ubar, 1.0f, nullptr, 0.0f, 0, 0, w.div, d, s);
+    if (e == cudaSuccess) e = jfli::divergence_fd(w.ubar, 1.0f, nullptr, 0.0f, 2, 0, w.div, d, s);
     if (e == cudaSuccess) e = jfli::poisson_potential(w.div, w.spec, w.rho_bar, d, 0.0f, 1.0f, s);
     if (e == cudaSuccess) e = jfli::adjoint_position(disp, lam_v, w.rho_bar, w.force, k, lam_x, d, s);
   }
-  return cuda_status(e, err, errlen, "jfli_kkd_adjoint");
+  return cuda_status(e, err, errlen, name);
+}
+}  // namespace
+
+size_t jfli_kkd_workspace_bytes(int nx, int ny, int nz, int batch) {
+  return kkd_ws_bytes(MeshDims{nx, ny, nz, batch});
+}
+
+int jfli_kkd_run(void* stream, float* disp, float* vel, const float* kicks, const float* drifts, int nsteps,
+                 float* rho, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                 size_t errlen) {
+  return kkd_run_impl(stream, disp, vel, kicks, drifts, nsteps, rho, nullptr, workspace, workspace_bytes, nx, ny, nz,
+                      batch, err, errlen, "jfli_kkd_run");
+}
+
+int jfli_kkd_run_stored(void* stream, float* disp, float* vel, const float* kicks, const float* drifts, int nsteps,
+                        float* rho, float* pots, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
+                        int batch, char* err, size_t errlen) {
+  CHECK_PTR(pots);
+  return kkd_run_impl(stream, disp, vel, kicks, drifts, nsteps, rho, pots, workspace, workspace_bytes, nx, ny, nz,
+                      batch, err, errlen, "jfli_kkd_run_stored");
+}
+
+int jfli_kkd_adjoint(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
+                     const float* drifts, int nsteps, double* sens, void* workspace, size_t workspace_bytes, int nx,
+                     int ny, int nz, int batch, char* err, size_t errlen) {
+  return kkd_adjoint_impl(stream, disp, vel, lam_x, lam_v, kicks, drifts, nsteps, nullptr, sens, workspace,
+                          workspace_bytes, nx, ny, nz, batch, err, errlen, "jfli_kkd_adjoint");
+}
+
+int jfli_kkd_adjoint_stored(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
+                            const float* drifts, int nsteps, const float* pots, double* sens, void* workspace,
+                            size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_PTR(pots);
+  return kkd_adjoint_impl(stream, disp, vel, lam_x, lam_v, kicks, drifts, nsteps, pots, sens, workspace,
+                          workspace_bytes, nx, ny, nz, batch, err, errlen, "jfli_kkd_adjoint_stored");
 }
 
 // ---- adjoints --------------------------------------------------------------------

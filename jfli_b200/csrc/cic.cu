@@ -337,16 +337,17 @@ __device__ __forceinline__ void kdp_brick_row(float* __restrict__ disp, float* _
   }
 }
 
-constexpr int kBrickY = 8, kBrickZ = 32, kBrickX = 16;  // CTA of 256 = 8 warps; x walked in chunks
+constexpr int kBrickY = 8, kBrickZ = 32;  // CTA of 256 = 8 warps; x walked in chunks of xdepth planes
 
 // One fused particle pass of a PM step over all particles. With per-slot arrays (kicks !=
 // nullptr) every batch entry b takes its own kick, drift and flags from kicks[b],
 // drifts[b], slot_flags[b]; flags 0 leaves the slot untouched.
 // Work order: when nz is a multiple of 32 and ny of 8 (and the CTA has 256 threads), a CTA
-// takes an 8 (y) x 32 (z) brick of Lagrangian cells and walks it along x in chunks of 16
-// planes; warps stay on z rows (the lane-merged deposit needs them), but the rows and
+// takes an 8 (y) x 32 (z) brick of Lagrangian cells and walks it along x in chunks of
+// xdepth planes (brick_xdepth: 16, fewer for a small mesh); warps stay on z rows (the lane-merged deposit needs them), but the rows and
 // planes whose particles share CIC corners are gathered on one SM close in time, so the
 // force-mesh lines they share are served by L1. Other shapes use a grid-stride walk.
+template <int xdepth>
 __global__ void __launch_bounds__(256, 4) k_kick_drift_paint(float* __restrict__ disp, float* __restrict__ vel, const float* __restrict__ force,
                                    float kick, float drift, int flags, float weight, float* __restrict__ rho,
                                    PGrid g, const float* __restrict__ kicks, const float* __restrict__ drifts,
@@ -366,25 +367,25 @@ __global__ void __launch_bounds__(256, 4) k_kick_drift_paint(float* __restrict__
   if (blockDim.x == kBrickY * kBrickZ && g.nz % kBrickZ == 0 && g.ny % kBrickY == 0 &&
       ((reinterpret_cast<uintptr_t>(disp) | reinterpret_cast<uintptr_t>(vel)) & 15) == 0) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int tz = g.nz / kBrickZ, ty = g.ny / kBrickY, txc = (g.nx + kBrickX - 1) / kBrickX;
+    const int tz = g.nz / kBrickZ, ty = g.ny / kBrickY, txc = (g.nx + xdepth - 1) / xdepth;
     const long long items = (long long)tz * ty * txc;
     for (long long it = blockIdx.x; it < items; it += gridDim.x) {
       const int iz = (int)(it % tz);
       const long long rest = it / tz;
       const int iy = (int)(rest % ty), xc = (int)(rest / ty);
       const int j = iy * kBrickY + w, k = iz * kBrickZ + lane;
-      const int i1 = min(g.nx, (xc + 1) * kBrickX);
+      const int i1 = min(g.nx, (xc + 1) * xdepth);
       XCarry carry;
       carry.valid = false;
       const unsigned row_stride = (unsigned)g.ny * (unsigned)g.nz;  // one x plane
       const bool use_v = flags & (kStepKick | kStepDrift);
-      unsigned p0 = ((unsigned)(xc * kBrickX) * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)(k - lane);
+      unsigned p0 = ((unsigned)(xc * xdepth) * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)(k - lane);
       float4 xa = make_float4(0.f, 0.f, 0.f, 0.f), va = xa;
       if (lane < 24) {
         xa = __ldcs(reinterpret_cast<const float4*>(disp + 3ull * p0) + lane);
         if (use_v) va = __ldcs(reinterpret_cast<const float4*>(vel + 3ull * p0) + lane);
       }
-      for (int i = xc * kBrickX; i < i1; ++i, p0 += row_stride)
+      for (int i = xc * xdepth; i < i1; ++i, p0 += row_stride)
         kdp_brick_row(disp, vel, force, kick, drift, flags, weight, rho, g, p0, i, j, k, lane, rowbuf[w][0],
                       rowbuf[w][1], carry, xa, va, i + 1 < i1, p0 + row_stride);
       // every lane of the warp ran the same planes: the carries go out together, z-merged
@@ -705,20 +706,47 @@ cudaError_t cic_readout_gradient(const float* pos, int absolute, const float* po
   return cudaGetLastError();
 }
 
+// The brick depth is a template argument: a runtime depth costs the kernel registers (it
+// spilled at the 64-register bound).
+static void launch_kdp(float* disp, float* vel, const float* force, float kick, float drift, int flags, float weight,
+                       float* rho, const MeshDims& d, const float* kicks, const float* drifts, const int* slot_flags,
+                       cudaStream_t s) {
+  const dim3 grid = particle_grid_dims(d.cells(), d.batch, 256, 16);
+  const PGrid g = make_pgrid(d);
+  switch (brick_xdepth(d.nx, d.ny, d.nz, d.batch, 4ll * sm_count())) {
+    case 16:
+      k_kick_drift_paint<16><<<grid, 256, 0, s>>>(disp, vel, force, kick, drift, flags, weight, rho, g, kicks, drifts,
+                                                  slot_flags);
+      break;
+    case 8:
+      k_kick_drift_paint<8><<<grid, 256, 0, s>>>(disp, vel, force, kick, drift, flags, weight, rho, g, kicks, drifts,
+                                                 slot_flags);
+      break;
+    case 4:
+      k_kick_drift_paint<4><<<grid, 256, 0, s>>>(disp, vel, force, kick, drift, flags, weight, rho, g, kicks, drifts,
+                                                 slot_flags);
+      break;
+    case 2:
+      k_kick_drift_paint<2><<<grid, 256, 0, s>>>(disp, vel, force, kick, drift, flags, weight, rho, g, kicks, drifts,
+                                                 slot_flags);
+      break;
+    default:
+      k_kick_drift_paint<1><<<grid, 256, 0, s>>>(disp, vel, force, kick, drift, flags, weight, rho, g, kicks, drifts,
+                                                 slot_flags);
+  }
+  note_launch();
+}
+
 cudaError_t kick_drift_paint(float* disp, float* vel, const float* force, float kick, float drift, int flags,
                              float weight, float* rho, const MeshDims& d, cudaStream_t s) {
-  k_kick_drift_paint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(
-      disp, vel, force, kick, drift, flags, weight, rho, make_pgrid(d), nullptr, nullptr, nullptr);
-  note_launch();
+  launch_kdp(disp, vel, force, kick, drift, flags, weight, rho, d, nullptr, nullptr, nullptr, s);
   return cudaGetLastError();
 }
 
 cudaError_t kick_drift_paint_slots(float* disp, float* vel, const float* force, const float* kicks,
                                    const float* drifts, const int* slot_flags, float weight, float* rho,
                                    const MeshDims& d, cudaStream_t s) {
-  k_kick_drift_paint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(
-      disp, vel, force, 0.f, 0.f, 0, weight, rho, make_pgrid(d), kicks, drifts, slot_flags);
-  note_launch();
+  launch_kdp(disp, vel, force, 0.f, 0.f, 0, weight, rho, d, kicks, drifts, slot_flags, s);
   return cudaGetLastError();
 }
 

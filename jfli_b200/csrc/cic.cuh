@@ -185,6 +185,16 @@ inline int sm_count() {
   return n;
 }
 
+// Depth (x planes per chunk) of the 8 (y) x 32 (z) brick walks of the particle kernels: the
+// deepest of 16, 8, 4, 2, 1 planes that still gives `min_ctas` bricks over the batch, so
+// that a small mesh run alone still spreads over the GPU (64^3 at 16 planes is 64 bricks).
+inline int brick_xdepth(int nx, int ny, int nz, int batch, long long min_ctas) {
+  const long long rows = (long long)(ny / 8) * (nz / 32) * batch;
+  int depth = 16;
+  while (depth > 1 && rows * ((nx + depth - 1) / depth) < min_ctas) depth >>= 1;
+  return depth;
+}
+
 inline dim3 particle_grid_dims(long long np, int batch, int threads, int per_sm) {
   long long blocks = (np + threads - 1) / threads;
   const long long cap = (long long)sm_count() * per_sm;

@@ -123,9 +123,12 @@ cudaError_t device_status(unsigned* out, bool reset);
 
 // ---- adjoint.cu ----
 size_t adjoint_partials_count(const MeshDims& d);
+// ubar: three meshes [batch][3][cells], or with vec4 one float4 mesh [batch][cells] (x, y, z, 0).
+// undrift_disp (== disp, or null): un-drift the positions first (x = x' - drift v') and
+// write them back.
 cudaError_t adjoint_unkick_paint(const float* disp, float* vel, const float* lam_x, float* lam_v, const float* force,
                                  float kick, float drift, float* ubar, double* partials, const MeshDims& d,
-                                 cudaStream_t s);
+                                 cudaStream_t s, bool vec4 = false, float* undrift_disp = nullptr);
 cudaError_t sum_adjoint_partials(const double* partials, const MeshDims& d, double* out, cudaStream_t s);
 cudaError_t divergence_fd(const float* u, float alpha, const float* w, float beta, int aos, int accumulate,
                           float* out, const MeshDims& d, cudaStream_t s);

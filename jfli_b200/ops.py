@@ -571,9 +571,17 @@ def _host_floats(a):
     return arr, arr.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
 
 
-def kkd_run(disp: torch.Tensor, vel: torch.Tensor, kicks, drifts, rho: torch.Tensor) -> None:
+def _check_pots(pots: torch.Tensor, nsteps: int, disp: torch.Tensor, batch: int):
+    _check(pots, "pots")
+    if pots.numel() != nsteps * batch * (disp.numel() // (3 * batch)):
+        raise ValueError(f"pots must hold {nsteps} potentials of the particle grid's mesh")
+
+
+def kkd_run(disp: torch.Tensor, vel: torch.Tensor, kicks, drifts, rho: torch.Tensor,
+            pots: torch.Tensor | None = None) -> None:
     """The ReversibleDoubleKickDrift loop in one call (in place on disp, vel); rho receives
-    the CIC density of the final positions."""
+    the CIC density of the final positions. With `pots` (nsteps potentials, float32 on the
+    device) the potential of every step is kept there for kkd_adjoint."""
     _check(disp, "disp")
     _check(vel, "vel")
     _check(rho, "rho")
@@ -584,14 +592,20 @@ def kkd_run(disp: torch.Tensor, vel: torch.Tensor, kicks, drifts, rho: torch.Ten
         raise ValueError("kicks and drifts must have the same length")
     nb = query("jfli_kkd_workspace_bytes", nx, ny, nz, batch)
     ws = workspace(nb, "kkd", disp.device)
+    if pots is not None:
+        _check_pots(pots, int(k_arr.size), disp, batch)
+        call("jfli_kkd_run_stored", stream_ptr(), ptr(disp), ptr(vel), k_ptr, d_ptr, int(k_arr.size), ptr(rho),
+             ptr(pots), ptr(ws), ws.numel(), nx, ny, nz, batch)
+        return
     call("jfli_kkd_run", stream_ptr(), ptr(disp), ptr(vel), k_ptr, d_ptr, int(k_arr.size), ptr(rho), ptr(ws),
          ws.numel(), nx, ny, nz, batch)
 
 
 def kkd_adjoint(disp: torch.Tensor, vel: torch.Tensor, lam_x: torch.Tensor, lam_v: torch.Tensor, kicks,
-                drifts) -> torch.Tensor:
+                drifts, pots: torch.Tensor | None = None) -> torch.Tensor:
     """Reverse sweep of kkd_run in one call (in place on all four particle grids); returns
-    the (nsteps, 2) FP64 (dL/dkick, dL/ddrift) on the device."""
+    the (nsteps, 2) FP64 (dL/dkick, dL/ddrift) on the device. `pots`: the potentials a
+    kkd_run with pots kept (the forces are then rebuilt from them, not recomputed)."""
     for name, t in (("disp", disp), ("vel", vel), ("lam_x", lam_x), ("lam_v", lam_v)):
         _check(t, name)
     (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
@@ -602,8 +616,13 @@ def kkd_adjoint(disp: torch.Tensor, vel: torch.Tensor, lam_x: torch.Tensor, lam_
     sens = torch.zeros(k_arr.size, batch, 2, dtype=torch.float64, device=disp.device)
     nb = query("jfli_kkd_workspace_bytes", nx, ny, nz, batch)
     ws = workspace(nb, "kkd", disp.device)
-    call("jfli_kkd_adjoint", stream_ptr(), ptr(disp), ptr(vel), ptr(lam_x), ptr(lam_v), k_ptr, d_ptr,
-         int(k_arr.size), ptr(sens), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    if pots is not None:
+        _check_pots(pots, int(k_arr.size), disp, batch)
+        call("jfli_kkd_adjoint_stored", stream_ptr(), ptr(disp), ptr(vel), ptr(lam_x), ptr(lam_v), k_ptr, d_ptr,
+             int(k_arr.size), ptr(pots), ptr(sens), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    else:
+        call("jfli_kkd_adjoint", stream_ptr(), ptr(disp), ptr(vel), ptr(lam_x), ptr(lam_v), k_ptr, d_ptr,
+             int(k_arr.size), ptr(sens), ptr(ws), ws.numel(), nx, ny, nz, batch)
     return sens if batch > 1 else sens[:, 0, :]
 
 

@@ -186,21 +186,46 @@ class LPT(torch.autograd.Function):
         return gic, gom, None, None
 
 
+# Device bytes the forward pass may keep for its backward sweep: each step's potential
+# (4 bytes per cell), from which the reverse sweep rebuilds the forces instead of
+# un-drifting, painting and solving for them again (about a third of a reverse step).
+# Runs whose potentials need more (or more than a quarter of the free device memory)
+# recompute them. 0 turns the store off.
+POTENTIAL_STORE_BYTES = 4 << 30
+
+
+def potential_store(nsteps: int, x: torch.Tensor) -> torch.Tensor | None:
+    """An (nsteps, mesh) float32 buffer for the run's potentials, or None when it does not
+    fit POTENTIAL_STORE_BYTES or a quarter of the free device memory."""
+    need = 4 * nsteps * (x.numel() // 3)
+    if need == 0 or need > POTENTIAL_STORE_BYTES:
+        return None
+    if need > (256 << 20):  # the free-memory query costs a millisecond: only for large stores
+        free, _ = torch.cuda.mem_get_info(x.device)
+        if need > free // 4:
+            return None
+    return torch.empty(nsteps, *x.shape[:-1], dtype=torch.float32, device=x.device)
+
+
 def kkd_forward(x: torch.Tensor, v: torch.Tensor, kicks, drifts, rho: torch.Tensor, force: torch.Tensor | None = None,
-                pot: torch.Tensor | None = None) -> None:
+                pot: torch.Tensor | None = None, pots: torch.Tensor | None = None) -> None:
     """The ReversibleDoubleKickDrift loop in place: per step kick with the force at the
     current positions, drift, paint; rho ends as the CIC density of the final positions.
-    One library call (`jfli_kkd_run`); force and pot are accepted for callers that pass
-    buffers and are not used (the library keeps its own in its workspace)."""
-    ops.kkd_run(x, v, kicks, drifts, rho)
+    One library call (`jfli_kkd_run`, or `jfli_kkd_run_stored` keeping every step's
+    potential in `pots`); force and pot are accepted for callers that pass buffers and are
+    not used (the library keeps its own in its workspace)."""
+    ops.kkd_run(x, v, kicks, drifts, rho, pots=pots)
 
 
-def kkd_reverse_adjoint(x: torch.Tensor, v: torch.Tensor, lam_x: torch.Tensor, lam_v: torch.Tensor, kicks, drifts):
+def kkd_reverse_adjoint(x: torch.Tensor, v: torch.Tensor, lam_x: torch.Tensor, lam_v: torch.Tensor, kicks, drifts,
+                        pots: torch.Tensor | None = None):
     """Backward sweep of kkd_forward, in place on (x, v, lam_x, lam_v): on return (x, v) is
     the recomputed initial state and (lam_x, lam_v) the cotangent at it. Returns the FP64
     (dL/dkick_n, dL/ddrift_n) arrays. One library call (`jfli_kkd_adjoint`): per step
-    un-drift + paint, force mesh, un-kick + adjoint paint, P(div), CIC-gradient gather."""
-    return ops.kkd_adjoint(x, v, lam_x, lam_v, kicks, drifts)
+    un-drift + paint, force mesh, un-kick + adjoint paint, P(div), CIC-gradient gather;
+    with the forward pass's `pots` (`jfli_kkd_adjoint_stored`) the force mesh comes from
+    the stored potential and the un-drift is part of the un-kick."""
+    return ops.kkd_adjoint(x, v, lam_x, lam_v, kicks, drifts, pots=pots)
 
 
 class ReversibleNBody(torch.autograd.Function):
@@ -211,9 +236,11 @@ class ReversibleNBody(torch.autograd.Function):
         x = dx.detach().contiguous().clone()
         v = p.detach().contiguous().clone()
         rho = torch.empty(x.shape[:-1], dtype=torch.float32, device=x.device)
-        kkd_forward(x, v, tables.kicks, tables.drifts, rho)
+        pots = potential_store(len(tables.kicks), x) if any(ctx.needs_input_grad[:3]) else None
+        kkd_forward(x, v, tables.kicks, tables.drifts, rho, pots=pots)
         ctx.tables = tables
         ctx.omega_c = omega_c
+        ctx.pots = pots
         ctx.save_for_backward(x, v)
         return rho
 
@@ -226,7 +253,8 @@ class ReversibleNBody(torch.autograd.Function):
         lam_x = torch.zeros_like(x)
         lam_v = torch.zeros_like(v)
         ops.adjoint_position(x, lam_x, rho_bar=grho.contiguous())  # adjoint of the final paint
-        sens = kkd_reverse_adjoint(x, v, lam_x, lam_v, t.kicks, t.drifts)
+        sens = kkd_reverse_adjoint(x, v, lam_x, lam_v, t.kicks, t.drifts, pots=ctx.pots)
+        ctx.pots = None
         gom = None
         if ctx.needs_input_grad[2]:
             sk, sd = sens[:, 0].cpu().numpy(), sens[:, 1].cpu().numpy()

@@ -94,6 +94,88 @@ def test_reverse_recovers_initial_state():
     assert ex < 1e-4 and ev < 1e-4
 
 
+def test_stored_potentials_match_recomputed_sweep():
+    """jfli_kkd_run_stored / jfli_kkd_adjoint_stored: the forward results are jfli_kkd_run's
+    (to the run-to-run spread of the FP32 atomic paint's order), and the reverse sweep
+    over the kept potentials gives the cotangents, the dL/dkick, dL/ddrift and the
+    recovered initial state of the recomputing sweep. The stored forces are the forward
+    pass's own, the recomputed ones those at positions reconstructed to FP32 rounding; on
+    this random state (displacements of a cell, velocities of a third) the two sweeps'
+    CIC weight gradients, which jump at cell faces, then differ for the particles that
+    rounding puts on the other side of a face, so the sweeps agree to 1e-3, not to FP32.
+    Each is checked against the FP64 oracle's finite differences (1e-4) on its own."""
+    from jfli_b200 import ops
+    from jfli_b200.pm import adjoint as adj
+
+    n = 64
+    rng = np.random.default_rng(3)
+    x0 = _dev(1.0 * rng.standard_normal((n, n, n, 3)))
+    v0 = _dev(0.3 * rng.standard_normal((n, n, n, 3)))
+    kicks = np.linspace(0.2, 0.4, 10)
+    drifts = np.linspace(0.5, 0.2, 10)
+    a, b = _dev(rng.standard_normal((n, n, n, 3))), _dev(rng.standard_normal((n, n, n, 3)))
+    out = {}
+    for mode in ("recompute", "stored"):
+        x, v = x0.clone(), v0.clone()
+        rho = torch.empty(n, n, n, device="cuda")
+        pots = torch.empty(len(kicks), n, n, n, device="cuda") if mode == "stored" else None
+        ops.kkd_run(x, v, kicks, drifts, rho, pots=pots)
+        fwd = (x.clone(), v.clone(), rho.clone())
+        lx, lv = a.clone(), b.clone()
+        sens = ops.kkd_adjoint(x, v, lx, lv, kicks, drifts, pots=pots)
+        out[mode] = (fwd, lx, lv, sens.cpu().numpy(), x, v)
+    (f0, lx0, lv0, s0, xr0, vr0), (f1, lx1, lv1, s1, xr1, vr1) = out["recompute"], out["stored"]
+    for name, t0, t1 in zip(("positions", "momenta", "density"), f0, f1):
+        e = float((t1 - t0).norm() / t0.norm())
+        print(f"forward {name}: stored vs recomputed {e:.2e}")
+        assert e < 1e-5
+    e_lx = float((lx1 - lx0).norm() / lx0.norm())
+    e_lv = float((lv1 - lv0).norm() / lv0.norm())
+    e_s = float(np.abs(s1 - s0).max() / np.abs(s0).max())
+    e_x = float((xr1 - x0).abs().max())
+    print(f"stored vs recomputed: lam_x {e_lx:.2e}, lam_v {e_lv:.2e}, sensitivities {e_s:.2e}; "
+          f"initial state recovered to {e_x:.2e} cells (recomputing sweep {float((xr0 - x0).abs().max()):.2e})")
+    assert e_lx < 1e-3 and e_lv < 1e-3 and e_s < 1e-3
+    assert e_x < 1e-4
+
+
+def test_kkd_step_vjp_stored_matches_oracle_fd():
+    from jfli_b200 import ops
+
+    n = 32
+    rng = np.random.default_rng(1)
+    x0 = (1.5 * rng.standard_normal((n, n, n, 3))).astype(np.float32)
+    v0 = (0.5 * rng.standard_normal((n, n, n, 3))).astype(np.float32)
+    kicks, drifts = np.array([0.3, 0.25, 0.35]), np.array([0.4, 0.5, 0.3])
+    a = rng.standard_normal(x0.shape)
+    b = rng.standard_normal(x0.shape)
+    r = rng.standard_normal(x0.shape)
+    s = rng.standard_normal(x0.shape)
+    x, v = _dev(x0), _dev(v0)
+    rho = torch.empty(n, n, n, device="cuda")
+    pots = torch.empty(len(kicks), n, n, n, device="cuda")
+    ops.kkd_run(x, v, kicks, drifts, rho, pots=pots)
+    lam_x, lam_v = _dev(a), _dev(b)
+    sens = ops.kkd_adjoint(x, v, lam_x, lam_v, kicks, drifts, pots=pots).cpu().numpy()
+    g_dir = float(np.sum(lam_x.cpu().numpy() * r) + np.sum(lam_v.cpu().numpy() * s))
+
+    def loss(xi, vi, ks=kicks, ds=drifts):
+        xf, vf, _ = opm.kkd_run(xi, vi, list(zip(ks, ds)), np.float64)
+        return float(np.sum(a * xf) + np.sum(b * vf))
+
+    eps = 1e-5
+    x64, v64 = x0.astype(np.float64), v0.astype(np.float64)
+    fd = (loss(x64 + eps * r, v64 + eps * s) - loss(x64 - eps * r, v64 - eps * s)) / (2 * eps)
+    print(f"direction (stored potentials): adjoint {g_dir:.8e} fd {fd:.8e}")
+    assert _rel(g_dir, fd) < 1e-4
+    for i in range(len(kicks)):
+        kp, km = kicks.copy(), kicks.copy()
+        kp[i] += eps
+        km[i] -= eps
+        fdk = (loss(x64, v64, ks=kp) - loss(x64, v64, ks=km)) / (2 * eps)
+        assert _rel(sens[i, 0], fdk) < 1e-4
+
+
 # --------------------------------------------------------------------------- P(k), LPT, ICs
 def test_power_adjoint_matches_oracle_fd():
     from jfli_b200.pm import adjoint as adj
