@@ -91,26 +91,16 @@ __device__ __forceinline__ void deposit_vec4_lane_merged(float4* mesh, const PGr
 //   <u, F> -> partial[0];  v = v' - kick F;  lambda_v = u;  ubar_a += W * u_a.
 // partials holds 2 doubles per CTA and batch entry, summed in a fixed order later.
 // ubar: three meshes [3][cells] (kVec4 false) or one float4 mesh [cells] (kVec4 true).
-// With undrift (the float4 form of the reverse sweep over stored potentials), disp holds
-// x' on entry: the particle is first un-drifted, x = x' - drift v', and x is written back.
+// The arithmetic of one particle, on its values in registers: x, v, lx (lambda_x), lv
+// (lambda_v) in; x (un-drifted when undrift), v (un-kicked) and lv (= u) out.
 template <bool kVec4>
-__device__ __forceinline__ void unkick_particle(float* __restrict__ disp, bool undrift, float* __restrict__ vel,
-                                                const float* __restrict__ lam_x, float* __restrict__ lam_v,
-                                                const float* __restrict__ force, float kick, float drift,
-                                                float* __restrict__ ubar, const PGrid& g, unsigned p, int i, int j,
-                                                int k, double& sk, double& sd) {
-  float v[3], x[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    v[a] = vel[3 * p + a];
-    x[a] = disp[3 * p + a];
-  }
+__device__ __forceinline__ void unkick_core(float x[3], float v[3], const float lx[3], float lv[3], bool undrift,
+                                            const float* __restrict__ force, float kick, float drift,
+                                            float* __restrict__ ubar, const PGrid& g, int i, int j, int k, double& sk,
+                                            double& sd) {
   if (undrift) {
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      x[a] += v[a] * -drift;
-      disp[3 * p + a] = x[a];
-    }
+    for (int a = 0; a < 3; ++a) x[a] += v[a] * -drift;
   }
   const Cic1 cx = cic_rel(i, x[0], g.nx), cy = cic_rel(j, x[1], g.ny), cz = cic_rel(k, x[2], g.nz);
   float f[3];
@@ -118,12 +108,11 @@ __device__ __forceinline__ void unkick_particle(float* __restrict__ disp, bool u
   float u[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const float lx = lam_x[3 * p + a];
-    sd += (double)lx * (double)v[a];
-    u[a] = lam_v[3 * p + a] + drift * lx;
+    sd += (double)lx[a] * (double)v[a];
+    u[a] = lv[a] + drift * lx[a];
     sk += (double)u[a] * (double)f[a];
-    vel[3 * p + a] = v[a] - f[a] * kick;
-    lam_v[3 * p + a] = u[a];
+    v[a] = v[a] - f[a] * kick;
+    lv[a] = u[a];
   }
   if (kVec4) {
     deposit_vec4_lane_merged(reinterpret_cast<float4*>(ubar), g, cx, cy, cz, u);
@@ -131,6 +120,86 @@ __device__ __forceinline__ void unkick_particle(float* __restrict__ disp, bool u
 #pragma unroll
     for (int a = 0; a < 3; ++a) deposit(ubar + (size_t)a * g.np, g, cx, cy, cz, u[a]);
   }
+}
+
+// One particle with its own 4-byte loads and stores. With undrift (the float4 form of the
+// reverse sweep over stored potentials), disp holds x' on entry: the particle is first
+// un-drifted, x = x' - drift v', and x is written back.
+template <bool kVec4>
+__device__ __forceinline__ void unkick_particle(float* __restrict__ disp, bool undrift, float* __restrict__ vel,
+                                                const float* __restrict__ lam_x, float* __restrict__ lam_v,
+                                                const float* __restrict__ force, float kick, float drift,
+                                                float* __restrict__ ubar, const PGrid& g, unsigned p, int i, int j,
+                                                int k, double& sk, double& sd) {
+  float x[3], v[3], lx[3], lv[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    x[a] = disp[3 * p + a];
+    v[a] = vel[3 * p + a];
+    lx[a] = lam_x[3 * p + a];
+    lv[a] = lam_v[3 * p + a];
+  }
+  unkick_core<kVec4>(x, v, lx, lv, undrift, force, kick, drift, ubar, g, i, j, k, sk, sd);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (undrift) disp[3 * p + a] = x[a];
+    vel[3 * p + a] = v[a];
+    lam_v[3 * p + a] = lv[a];
+  }
+}
+
+// The 32 particles of one z row (lane = z offset; the row's arrays start 16-byte aligned):
+// lanes 0..23 move each array's 384 bytes as float4 with streaming loads and stores
+// through the warp's shared buffers (4 x 24 float4), and every lane reads and writes its
+// own 3 floats there (stride 3, no bank conflicts): one 16-byte instruction per array and
+// row where the lanes' own accesses take three 4-byte ones.
+template <bool kVec4>
+__device__ __forceinline__ void unkick_row(float* __restrict__ disp, bool undrift, float* __restrict__ vel,
+                                           const float* __restrict__ lam_x, float* __restrict__ lam_v,
+                                           const float* __restrict__ force, float kick, float drift,
+                                           float* __restrict__ ubar, const PGrid& g, unsigned p0, int i, int j, int k,
+                                           int lane, float4 (*buf)[24], double& sk, double& sd) {
+  float4* d4 = reinterpret_cast<float4*>(disp + 3ull * p0);
+  float4* v4 = reinterpret_cast<float4*>(vel + 3ull * p0);
+  const float4* x4 = reinterpret_cast<const float4*>(lam_x + 3ull * p0);
+  float4* l4 = reinterpret_cast<float4*>(lam_v + 3ull * p0);
+  if (lane < 24) {
+    buf[0][lane] = __ldcs(d4 + lane);
+    buf[1][lane] = __ldcs(v4 + lane);
+    buf[2][lane] = __ldcs(x4 + lane);
+    buf[3][lane] = __ldcs(l4 + lane);
+  }
+  __syncwarp();
+  float x[3], v[3], lx[3], lv[3];
+  const float* f0 = reinterpret_cast<const float*>(buf[0]);
+  const float* f1 = reinterpret_cast<const float*>(buf[1]);
+  const float* f2 = reinterpret_cast<const float*>(buf[2]);
+  const float* f3 = reinterpret_cast<const float*>(buf[3]);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    x[a] = f0[3 * lane + a];
+    v[a] = f1[3 * lane + a];
+    lx[a] = f2[3 * lane + a];
+    lv[a] = f3[3 * lane + a];
+  }
+  __syncwarp();
+  unkick_core<kVec4>(x, v, lx, lv, undrift, force, kick, drift, ubar, g, i, j, k, sk, sd);
+  float* w0 = reinterpret_cast<float*>(buf[0]);
+  float* w1 = reinterpret_cast<float*>(buf[1]);
+  float* w3 = reinterpret_cast<float*>(buf[3]);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    w0[3 * lane + a] = x[a];
+    w1[3 * lane + a] = v[a];
+    w3[3 * lane + a] = lv[a];
+  }
+  __syncwarp();
+  if (lane < 24) {
+    if (undrift) __stcs(d4 + lane, buf[0][lane]);
+    __stcs(v4 + lane, buf[1][lane]);
+    __stcs(l4 + lane, buf[3][lane]);
+  }
+  __syncwarp();
 }
 
 constexpr int kAdjBrickY = 8, kAdjBrickZ = 32;
@@ -141,7 +210,7 @@ constexpr int kAdjBrickY = 8, kAdjBrickZ = 32;
 // warp), so that the rows and planes whose particles share CIC corners gather and deposit
 // on one SM close in time (as the forward particle pass). Otherwise a grid-stride walk.
 template <bool kVec4>
-__global__ void __launch_bounds__(kAdjThreads) k_adj_unkick_paint(
+__global__ void __launch_bounds__(kAdjThreads, 3) k_adj_unkick_paint(
     float* __restrict__ disp, int undrift, float* __restrict__ vel, const float* __restrict__ lam_x,
     float* __restrict__ lam_v, const float* __restrict__ force, float kick, float drift, float* __restrict__ ubar,
     double* __restrict__ partials, PGrid g, int xdepth) {
@@ -153,8 +222,11 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_unkick_paint(
   force += b * g.np * 4;
   ubar += b * g.np * (kVec4 ? 4 : 3);
   double sk = 0.0, sd = 0.0;
+  __shared__ float4 rowbuf[kVec4 ? kAdjBrickY : 1][4][24];  // per warp: disp, vel, lam_x, lam_v of one z row
   if (kVec4 && blockDim.x == kAdjBrickY * kAdjBrickZ && g.nz % kAdjBrickZ == 0 && g.ny % kAdjBrickY == 0) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const bool staged = ((reinterpret_cast<uintptr_t>(disp) | reinterpret_cast<uintptr_t>(vel) |
+                          reinterpret_cast<uintptr_t>(lam_x) | reinterpret_cast<uintptr_t>(lam_v)) & 15) == 0;
     const int tz = g.nz / kAdjBrickZ, ty = g.ny / kAdjBrickY, txc = (g.nx + xdepth - 1) / xdepth;
     const long long items = (long long)tz * ty * txc;
     for (long long it = blockIdx.x; it < items; it += gridDim.x) {
@@ -163,10 +235,15 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_unkick_paint(
       const int iy = (int)(rest % ty), xc = (int)(rest / ty);
       const int j = iy * kAdjBrickY + w, k = iz * kAdjBrickZ + lane;
       const int i1 = min(g.nx, (xc + 1) * xdepth);
-      for (int i = xc * xdepth; i < i1; ++i)
-        unkick_particle<kVec4>(disp, undrift != 0, vel, lam_x, lam_v, force, kick, drift, ubar, g,
-                               ((unsigned)i * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)k, i, j, k,
-                               sk, sd);
+      for (int i = xc * xdepth; i < i1; ++i) {
+        const unsigned p = ((unsigned)i * (unsigned)g.ny + (unsigned)j) * (unsigned)g.nz + (unsigned)k;
+        if (staged)
+          unkick_row<kVec4>(disp, undrift != 0, vel, lam_x, lam_v, force, kick, drift, ubar, g, p - (unsigned)lane,
+                            i, j, k, lane, rowbuf[kVec4 ? w : 0], sk, sd);
+        else
+          unkick_particle<kVec4>(disp, undrift != 0, vel, lam_x, lam_v, force, kick, drift, ubar, g, p, i, j, k, sk,
+                                 sd);
+      }
     }
   } else {
     for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
@@ -225,20 +302,14 @@ __global__ void k_div_fd(const float* __restrict__ u, float alpha, const float* 
 // at relative positions disp. Either of rho_bar or (u, force) may be null. The gradient
 // of the trilinear weights is one-sided at cell faces, like the derivative of the
 // floor-based weights.
-__device__ __forceinline__ void adj_position_particle(const float* __restrict__ disp, const float* __restrict__ u,
-                                                      const float* __restrict__ rho_bar,
-                                                      const float* __restrict__ force, float scale,
-                                                      float* __restrict__ lam_x, const PGrid& g, unsigned p, int i,
-                                                      int j, int k) {
-  const Cic1 cx = cic_rel(i, disp[3 * p + 0], g.nx), cy = cic_rel(j, disp[3 * p + 1], g.ny),
-             cz = cic_rel(k, disp[3 * p + 2], g.nz);
+// The gradient of R_x[h] at one particle from its position x and vector u in registers:
+// (gx, gy, gz) = grad_x R_x[rho_bar + sum_a u_a force_a].
+__device__ __forceinline__ void adj_position_core(const float x[3], const float ua[3], bool use_u,
+                                                  const float* __restrict__ rho_bar,
+                                                  const float* __restrict__ force, const PGrid& g, int i, int j, int k,
+                                                  float& gx, float& gy, float& gz) {
+  const Cic1 cx = cic_rel(i, x[0], g.nx), cy = cic_rel(j, x[1], g.ny), cz = cic_rel(k, x[2], g.nz);
   const int xo[2] = {cx.i0 * g.yz, cx.i1 * g.yz}, yo[2] = {cy.i0 * g.nz, cy.i1 * g.nz}, zo[2] = {cz.i0, cz.i1};
-  float ua[3] = {0.f, 0.f, 0.f};
-  if (u && force) {
-    ua[0] = u[3 * p + 0];
-    ua[1] = u[3 * p + 1];
-    ua[2] = u[3 * p + 2];
-  }
   float h[2][2][2];
 #pragma unroll
   for (int a = 0; a < 2; ++a)
@@ -248,14 +319,16 @@ __device__ __forceinline__ void adj_position_particle(const float* __restrict__ 
       for (int c = 0; c < 2; ++c) {
         const int o = xo[a] + yo[bb] + zo[c];
         float v = rho_bar ? __ldg(rho_bar + o) : 0.f;
-        if (u && force) {
+        if (use_u) {
           const float4 f = __ldg(reinterpret_cast<const float4*>(force) + o);
           v += ua[0] * f.x + ua[1] * f.y + ua[2] * f.z;
         }
         h[a][bb][c] = v;
       }
   const float wx[2] = {cx.w0, cx.w1}, wy[2] = {cy.w0, cy.w1}, wz[2] = {cz.w0, cz.w1};
-  float gx = 0.f, gy = 0.f, gz = 0.f;
+  gx = 0.f;
+  gy = 0.f;
+  gz = 0.f;
 #pragma unroll
   for (int bb = 0; bb < 2; ++bb)
 #pragma unroll
@@ -268,6 +341,23 @@ __device__ __forceinline__ void adj_position_particle(const float* __restrict__ 
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int bb = 0; bb < 2; ++bb) gz += wx[a] * wy[bb] * (h[a][bb][1] - h[a][bb][0]);
+}
+
+__device__ __forceinline__ void adj_position_particle(const float* __restrict__ disp, const float* __restrict__ u,
+                                                      const float* __restrict__ rho_bar,
+                                                      const float* __restrict__ force, float scale,
+                                                      float* __restrict__ lam_x, const PGrid& g, unsigned p, int i,
+                                                      int j, int k) {
+  const float x[3] = {disp[3 * p + 0], disp[3 * p + 1], disp[3 * p + 2]};
+  const bool use_u = u && force;
+  float ua[3] = {0.f, 0.f, 0.f};
+  if (use_u) {
+    ua[0] = u[3 * p + 0];
+    ua[1] = u[3 * p + 1];
+    ua[2] = u[3 * p + 2];
+  }
+  float gx, gy, gz;
+  adj_position_core(x, ua, use_u, rho_bar, force, g, i, j, k, gx, gy, gz);
   lam_x[3 * p + 0] += scale * gx;
   lam_x[3 * p + 1] += scale * gy;
   lam_x[3 * p + 2] += scale * gz;
@@ -283,6 +373,7 @@ __global__ void __launch_bounds__(256) k_adj_position(const float* __restrict__ 
   if (u) u += b * g.np * 3;
   if (force) force += b * g.np * 4;
   if (rho_bar) rho_bar += b * g.np;
+  // (staging its rows through shared memory, as the un-kick does, measured 10% slower)
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int i, j, k;
     particle_ijk(g, p, i, j, k);
