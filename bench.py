@@ -907,6 +907,16 @@ def cpu_baseline_block(n):
                       f"CIC in C/OpenMP, 4 complex scipy FFTs per step with all workers); {dt:.1f} s"}
 
 
+def workload_config(n, world):
+    """The `config` of both arms' lines (the same dict, so the two measure one workload)."""
+    box = BOX * n / N_MESH
+    return {"workload": f"PM KDK step at {n}^3 particles on a {n}^3 mesh, box {box:g} Mpc/h, 2LPT ICs (seeded white "
+                        f"noise), the {E2E_STEPS}-step schedule from a = 0.1 to a = 1",
+            "mesh": n, "particles": n**3, "box": box, "solver": "EfficientDriftDoubleKick", "steps_in_schedule": E2E_STEPS,
+            "parallelism": f"replicas x{world}",
+            "l2": "particle state (x, v: 24 B per particle, 402 MB at 256^3) exceeds the 126 MB L2; no flush"}
+
+
 def run_reference(args):
     """The reference arm: the FP32 oracle port of the reference algorithm (jax and the
     JaxPM fork are not installable on this image) on the host cores, on the GPU arm's
@@ -918,15 +928,10 @@ def run_reference(args):
     n = args.mesh
     cpu = CpuKdk(n)
     rate, dt = cpu.rate(args.warmup, args.steps)
-    box = BOX * n / N_MESH
     line = {"metric": METRIC, "value": round(rate, 4), "unit": "Mpart-steps/s", "n_gpus": args.gpus, "device": "cpu",
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": f"PM KDK step at {n}^3 particles on a {n}^3 mesh, box {box:g} Mpc/h, 2LPT ICs "
-                                   f"(seeded white noise)",
-                       "mesh": n, "particles": n**3, "box": box, "solver": "EfficientDriftDoubleKick",
-                       "parallelism": "host threads"},
+            "impl": "reference", "config": workload_config(n, args.gpus), "same_config": True,
             "cpu_baseline": {"value": round(rate, 4), "unit": "Mpart-steps/s", "cores": cpu_threads(), "kind": "port",
                              "sample": f"{args.steps} KDK steps of the 40-step schedule at {n}^3 after {args.warmup} "
                                        f"untimed ones (FP32 oracle port of the reference algorithm: CIC in C/OpenMP, "
@@ -1055,11 +1060,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(res["ms"] / args.steps, 4),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
-                "config": {"workload": f"PM KDK step at {args.mesh}^3 particles on a {args.mesh}^3 mesh, "
-                                       f"box {BOX * args.mesh / N_MESH:g} Mpc/h, 2LPT ICs (seeded white noise)",
-                           "mesh": args.mesh, "particles": args.mesh**3, "box": BOX * args.mesh / N_MESH,
-                           "solver": "EfficientDriftDoubleKick", "parallelism": f"replicas x{world}",
-                           "l2": "particle state (x, v: 402 MB) exceeds the 126 MB L2; no flush"},
+                "config": workload_config(args.mesh, world), "same_config": True,
                 "roofline": res["roofline"], "step_roofline": res["step_roofline"], "cpu_baseline": cpu, "e2e": res["e2e"], "clocks": res["clocks"],
                 "gpu_launches": res["launches"], "serving": res["serving"], "gradient": res["gradient"],
                 "e2e_with_shells": res["shells"], "fft_vs_cufft": fft_cmp, "x_pass_variants": xpass}
