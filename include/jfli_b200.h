@@ -218,6 +218,18 @@ int jfli_power_poles(void* stream, const float* mesh, const float* mesh2, const 
 int jfli_healpix_paint(void* stream, const float* disp, int absolute, const float* weights, float weight, float lx,
                        float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside, int scheme,
                        float* map, int accumulate, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* Several shells of one particle set (batch 1) in one pass over the particles: shell s
+ * keeps rmin[s] < |x - observer| <= rmax[s] and receives weight * scale[s] per particle
+ * (weights[p] * weight * scale[s] with per-particle weights) into maps[s][12 nside^2];
+ * shells may overlap. rmin, rmax, scale: host arrays of nshells. scheme 0 (ngp), 1
+ * (bilinear) or 2 (rbf_neighbor, with sigma as jfli_healpix_paint_rbf). accumulate = 0
+ * clears the nshells maps first. The same maps as one jfli_healpix_paint per shell, with
+ * the particle set read once instead of nshells times. */
+int jfli_healpix_paint_shells(void* stream, const float* disp, int absolute, const float* weights, float weight,
+                              float lx, float ly, float lz, float ox, float oy, float oz, int nshells,
+                              const double* rmin, const double* rmax, const float* scale, int nside, int scheme,
+                              float sigma, float* maps, int accumulate, int nx, int ny, int nz, int batch, char* err,
+                              size_t errlen);
 /* HEALPix shell painting with the "rbf_neighbor" scheme (reference
  * _src/fields/_painting.py:18,291; its arithmetic lives in the absent jaxpm fork, so this
  * is the library's own definition): each particle in rmin < r <= rmax deposits onto the 4

@@ -199,6 +199,12 @@ _SIGNATURES = {
         [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_int,
          c_void_p, c_size_t, *_DIMS, *_ERR],
     ),
+    "jfli_healpix_paint_shells": (
+        c_int,
+        [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float, c_float, c_int,
+         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_float), c_int, c_int,
+         c_float, c_void_p, c_int, *_DIMS, *_ERR],
+    ),
     "jfli_healpix_paint": (
         c_int,
         [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float, c_float,

@@ -545,6 +545,39 @@ int jfli_healpix_paint(void* stream, const float* disp, int absolute, const floa
       errlen, "jfli_healpix_paint");
 }
 
+int jfli_healpix_paint_shells(void* stream, const float* disp, int absolute, const float* weights, float weight,
+                              float lx, float ly, float lz, float ox, float oy, float oz, int nshells,
+                              const double* rmin, const double* rmax, const float* scale, int nside, int scheme,
+                              float sigma, float* maps, int accumulate, int nx, int ny, int nz, int batch, char* err,
+                              size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(maps);
+  if (batch != 1) return fail(err, errlen, JFLI_EUNSUPPORTED, "one particle set per call (batch %d)", batch);
+  if (nshells < 1) return fail(err, errlen, JFLI_EINVAL, "nshells must be >= 1");
+  CHECK_PTR(rmin);
+  CHECK_PTR(rmax);
+  CHECK_PTR(scale);
+  if (nside < 1 || nside > 8192) return fail(err, errlen, JFLI_EINVAL, "nside %d outside [1, 8192]", nside);
+  if (scheme != JFLI_HEALPIX_NGP && scheme != JFLI_HEALPIX_BILINEAR && scheme != 2)
+    return fail(err, errlen, JFLI_EUNSUPPORTED, "HEALPix scheme %d not supported (0 ngp, 1 bilinear, 2 rbf_neighbor)",
+                scheme);
+  if (scheme == 2 && !(sigma > 0.f && sigma < 3.2f))
+    return fail(err, errlen, JFLI_EINVAL, "rbf_neighbor sigma %g outside (0, pi)", (double)sigma);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!accumulate) {
+    cudaError_t e = cudaMemsetAsync(maps, 0, (size_t)12 * nside * nside * nshells * sizeof(float), s);
+    if (e != cudaSuccess) return cuda_status(e, err, errlen, "jfli_healpix_paint_shells memset");
+  }
+  const float box[3] = {lx, ly, lz};
+  const float obs[3] = {ox, oy, oz};
+  return cuda_status(jfli::healpix_paint_shells(disp, absolute, weights, weight, d, box, obs, nshells, rmin, rmax,
+                                                scale, nside, scheme, maps, s, scheme == 2 ? sigma : 0.f),
+                     err, errlen, "jfli_healpix_paint_shells");
+}
+
 int jfli_healpix_paint_rbf(void* stream, const float* disp, int absolute, const float* weights, float weight,
                            float lx, float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside,
                            float sigma, float* map, int accumulate, int nx, int ny, int nz, int batch, char* err,

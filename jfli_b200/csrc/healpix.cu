@@ -265,6 +265,44 @@ __global__ void k_healpix_paint(const float* __restrict__ disp, int absolute, co
   }
 }
 
+// Several shells of one particle set in one pass (paint_spherical with an array of
+// centres, light-cone LPT painted straight to its shells): each particle's FP64 distance
+// is tested against every shell (overlapping shells each get their deposit), and the
+// particle set is read once instead of once per shell. Shell s deposits weight * scale[s]
+// into maps[s].
+struct ShellSet {
+  int n;
+  double rmin[kMaxShellsPerPass], rmax[kMaxShellsPerPass];
+  float scale[kMaxShellsPerPass];
+};
+
+__global__ void k_healpix_paint_shells(const float* __restrict__ disp, int absolute, const float* __restrict__ weights,
+                                       float weight, MeshDims d, double3 cell, double3 obs, ShellSet shells,
+                                       int nside, int scheme, const double* __restrict__ theta_tab,
+                                       float* __restrict__ maps, float sigma) {
+  const long long np = d.cells();
+  const long long npix = 12LL * nside * nside;
+  const long long yz = (long long)d.ny * d.nz;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+    double gx = disp[3 * p + 0], gy = disp[3 * p + 1], gz = disp[3 * p + 2];
+    if (!absolute) {
+      const int i = (int)(p / yz);
+      const long long r = p - (long long)i * yz;
+      const int j = (int)(r / d.nz);
+      const int k = (int)(r - (long long)j * d.nz);
+      gx += (double)i;
+      gy += (double)j;
+      gz += (double)k;
+    }
+    const double vx = gx * cell.x - obs.x, vy = gy * cell.y - obs.y, vz = gz * cell.z - obs.z;
+    const double rr = sqrt(vx * vx + vy * vy + vz * vz);
+    const float w = weights ? weights[p] * weight : weight;
+    for (int sh = 0; sh < shells.n; ++sh)
+      if (rr > shells.rmin[sh] && rr <= shells.rmax[sh])
+        deposit_direction(vx, vy, vz, rr, w * shells.scale[sh], nside, scheme, theta_tab, maps + sh * npix, sigma);
+  }
+}
+
 // Tiled shell painting (OnionTiler._paint_tiled_27, pm/interp.py:418-504, and
 // TelephotoInterp._paint_telephoto, pm/interp.py:643-699). Every particle is read once and
 // placed in each of the tiles in turn: its observer-centred position c = x - o (x in
@@ -503,6 +541,34 @@ cudaError_t healpix_paint(const float* disp, int absolute, const float* weights,
                                                                   rmax, nside, scheme, tab, map, sigma);
   note_launch();
   return cudaGetLastError();
+}
+
+cudaError_t healpix_paint_shells(const float* disp, int absolute, const float* weights, float weight,
+                                 const MeshDims& d, const float* box, const float* observer, int nshells,
+                                 const double* rmin, const double* rmax, const float* scale, int nside, int scheme,
+                                 float* maps, cudaStream_t s, float sigma) {
+  const double3 cell = make_double3((double)box[0] / d.nx, (double)box[1] / d.ny, (double)box[2] / d.nz);
+  const double3 obs = make_double3(observer[0], observer[1], observer[2]);
+  long long blocks = (d.cells() + 255) / 256;
+  if (blocks > (long long)sm_count() * 16) blocks = (long long)sm_count() * 16;
+  const double* tab = ring_theta_table(nside);
+  if (!tab) return cudaErrorMemoryAllocation;
+  const long long npix = 12LL * nside * nside;
+  for (int s0 = 0; s0 < nshells; s0 += kMaxShellsPerPass) {
+    ShellSet set;
+    set.n = nshells - s0 < kMaxShellsPerPass ? nshells - s0 : kMaxShellsPerPass;
+    for (int i = 0; i < set.n; ++i) {
+      set.rmin[i] = rmin[s0 + i];
+      set.rmax[i] = rmax[s0 + i];
+      set.scale[i] = scale[s0 + i];
+    }
+    k_healpix_paint_shells<<<(unsigned)blocks, 256, 0, s>>>(disp, absolute, weights, weight, d, cell, obs, set, nside,
+                                                            scheme, tab, maps + s0 * npix, sigma);
+    note_launch();
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t healpix_paint_tiled(const float* disp, int absolute, const float* vel, const float* weights, float weight,

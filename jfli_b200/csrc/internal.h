@@ -155,6 +155,13 @@ cudaError_t power_poles(const float* mesh1, const float* mesh2, const MeshDims& 
 cudaError_t healpix_paint(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d,
                           const float* box, const float* observer, float rmin, float rmax, int nside, int scheme,
                           float* map, cudaStream_t s, float sigma = 0.f);
+// Up to kMaxShellsPerPass shells per launch (more are painted in further launches);
+// shell s: rmin[s] < r <= rmax[s], weight * scale[s], into maps + s * 12 nside^2.
+constexpr int kMaxShellsPerPass = 64;
+cudaError_t healpix_paint_shells(const float* disp, int absolute, const float* weights, float weight,
+                                 const MeshDims& d, const float* box, const float* observer, int nshells,
+                                 const double* rmin, const double* rmax, const float* scale, int nside, int scheme,
+                                 float* maps, cudaStream_t s, float sigma = 0.f);
 cudaError_t replica_positions(const float* disp, int absolute, const float* vel, const MeshDims& d, const float* box,
                               const float* observer, const signed char* rotation, const float* shift, int telephoto,
                               float t, float gp_t, const DriftTables& tb, float* out, cudaStream_t s);

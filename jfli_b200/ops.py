@@ -330,6 +330,42 @@ def healpix_paint(pos: torch.Tensor, nside: int, box_size, observer_mpc, rmin: f
     return out
 
 
+def healpix_paint_shells(pos: torch.Tensor, nside: int, box_size, observer_mpc, rmin, rmax, scale, *,
+                         scheme: str = "bilinear", absolute: bool = False, weights: torch.Tensor | None = None,
+                         weight: float = 1.0, out: torch.Tensor | None = None, accumulate: bool = False,
+                         sigma: float | None = None) -> torch.Tensor:
+    """(S, 12 nside^2) maps of S shells of one particle set in one pass (see
+    jfli_healpix_paint_shells); rmin, rmax, scale: S values each."""
+    _check(pos, "pos")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    if batch != 1:
+        raise ValueError("healpix_paint_shells paints one particle set")
+    sch = {"ngp": _lib.JFLI_HEALPIX_NGP, "bilinear": _lib.JFLI_HEALPIX_BILINEAR, "rbf_neighbor": 2}.get(scheme)
+    if sch is None:
+        raise NotImplementedError(f"spherical painting scheme {scheme!r} is not implemented (ngp, bilinear, "
+                                  f"rbf_neighbor)")
+    lo = np.ascontiguousarray(np.atleast_1d(np.asarray(rmin, np.float64)))
+    hi = np.ascontiguousarray(np.atleast_1d(np.asarray(rmax, np.float64)))
+    sc = np.ascontiguousarray(np.atleast_1d(np.asarray(scale, np.float32)))
+    if not (lo.shape == hi.shape == sc.shape):
+        raise ValueError("rmin, rmax and scale must have one value per shell")
+    npix = 12 * nside * nside
+    if out is None:
+        out = torch.empty(lo.size, npix, dtype=torch.float32, device=pos.device)
+        accumulate = False
+    elif tuple(out.shape) != (lo.size, npix) or not out.is_contiguous():
+        raise ValueError(f"out must be a contiguous ({lo.size}, {npix}) tensor")
+    lx, ly, lz = (float(v) for v in box_size)
+    ox, oy, oz = (float(v) for v in observer_mpc)
+    sg = (rbf_sigma(nside) if sigma is None else float(sigma)) if sch == 2 else 0.0
+    dp = ctypes.POINTER(ctypes.c_double)
+    call("jfli_healpix_paint_shells", stream_ptr(), ptr(pos), int(absolute), ptr(weights), float(weight), lx, ly, lz,
+         ox, oy, oz, int(lo.size), lo.ctypes.data_as(dp), hi.ctypes.data_as(dp),
+         sc.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(nside), sch, sg, ptr(out), int(accumulate), nx, ny,
+         nz, batch)
+    return out
+
+
 def drift_tables(cosmo, n_dense: int = 4096):
     """Device FP32 copies of the FP64 host tables the light-cone drift interpolates:
     (chi ascending, a at chi), (growth a, D1), (dense a, dGfa)."""

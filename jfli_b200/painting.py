@@ -34,12 +34,18 @@ def paint_shells(field, centers, widths, scheme="bilinear", weights=None, out=No
     if out is None:
         out = torch.empty(centers.size, npix, dtype=torch.float32, device=field.array.device)
     pos = field.array.contiguous()
-    for s, (c, wd) in enumerate(zip(centers, widths)):
-        rmin, rmax = c - wd / 2.0, c + wd / 2.0
-        vol = shell_volume_per_pixel(field.nside, rmin, rmax)
-        scale = ws / vol if vol > 0 else ws
-        ops.healpix_paint(pos, field.nside, field.box_size, field.observer_position_mpc, rmin, rmax, scheme=scheme,
-                          absolute=absolute, weights=w, weight=scale, out=out[s], sigma=sigma)
+    rmin, rmax = centers - widths / 2.0, centers + widths / 2.0
+    vol = np.array([shell_volume_per_pixel(field.nside, a, b) for a, b in zip(rmin, rmax)])
+    scale = np.where(vol > 0, ws / np.where(vol > 0, vol, 1.0), ws)
+    if pos.dim() == 4 and out.is_contiguous():
+        # one pass over the particles for all the shells
+        ops.healpix_paint_shells(pos, field.nside, field.box_size, field.observer_position_mpc, rmin, rmax, scale,
+                                 scheme=scheme, absolute=absolute, weights=w, out=out, sigma=sigma)
+        return out
+    for s in range(centers.size):
+        ops.healpix_paint(pos, field.nside, field.box_size, field.observer_position_mpc, rmin[s], rmax[s],
+                          scheme=scheme, absolute=absolute, weights=w, weight=float(scale[s]), out=out[s],
+                          sigma=sigma)
     return out
 
 

@@ -209,16 +209,15 @@ def test_healpix_paint_matches_oracle(scheme, nside):
     n, L = 32, 200.0
     disp = lpt_disp(n, 2.0, seed=3).astype(np.float32)
     obs = (100.0, 100.0, 100.0)
-    cell = np.float32(L / n)
-    # positions exactly as the kernel forms them (FP32), angles in FP64
-    g = opm.grid((n, n, n), np.float32)
-    pos = ((g + disp) * cell - np.asarray(obs, np.float32)).astype(np.float32)
-    r32 = np.sqrt((pos * pos).sum(-1, dtype=np.float32), dtype=np.float32)
+    # positions as the kernel forms them: FP64 from the FP32 displacements
+    g = opm.grid((n, n, n), np.float64)
+    pos = (g + disp.astype(np.float64)) * (L / n) - np.asarray(obs, np.float64)
+    r64 = np.sqrt((pos * pos).sum(-1))
     rmin, rmax = 40.0, 90.0
     out = host(ops.healpix_paint(dev(disp), nside, (L, L, L), obs, rmin, rmax, scheme=scheme))
-    sel = (r32 > np.float32(rmin)) & (r32 <= np.float32(rmax))
-    v = pos[sel].astype(np.float64)
-    r = r32[sel].astype(np.float64)
+    sel = (r64 > rmin) & (r64 <= rmax)
+    v = pos[sel]
+    r = r64[sel]
     th = np.arccos(np.clip(v[:, 2] / r, -1, 1))
     ph = np.arctan2(v[:, 1], v[:, 0])
     npix = 12 * nside * nside
@@ -228,10 +227,37 @@ def test_healpix_paint_matches_oracle(scheme, nside):
     else:
         p, w = oh.get_interp_weights(nside, th, ph)
         ref = np.bincount(p.ravel(), weights=w.ravel(), minlength=npix)
-        # bilinear weights move continuously with the FP32 position (the kernel may fuse
-        # multiply-adds), ~1e-7 rad over a pixel of 0.016 rad at nside 64
+        # the kernel may contract the FP64 arithmetic into fused multiply-adds; the weights
+        # move continuously with it
         assert rel_l2(out, ref) < 2e-5
     assert abs(out.sum() - sel.sum()) < 1e-3 * max(sel.sum(), 1)
+
+
+@pytest.mark.parametrize("scheme", ["ngp", "bilinear", "rbf_neighbor"])
+def test_healpix_paint_shells_one_pass(scheme):
+    """jfli_healpix_paint_shells (S shells of one particle set in one pass) against one
+    jfli_healpix_paint per shell: per-particle weights, overlapping shells, and 70 shells
+    (more than one launch's 64)."""
+    n, L, nside = 32, 200.0, 16
+    disp = dev(lpt_disp(n, 2.0, seed=5).astype(np.float32))
+    w = dev(np.random.default_rng(6).uniform(0.5, 1.5, (n, n, n)).astype(np.float32))
+    obs = (100.0, 100.0, 100.0)
+    edges = np.linspace(5.0, 100.0, 71)
+    rmin = np.concatenate([edges[:-1], [30.0]])  # the last shell overlaps several others
+    rmax = np.concatenate([edges[1:], [60.0]])
+    scale = np.linspace(0.5, 2.0, rmin.size)
+    maps = host(ops.healpix_paint_shells(disp, nside, (L, L, L), obs, rmin, rmax, scale, scheme=scheme, weights=w,
+                                         weight=0.75))
+    worst = 0.0
+    for s in range(rmin.size):
+        ref = host(ops.healpix_paint(disp, nside, (L, L, L), obs, rmin[s], rmax[s], scheme=scheme, weights=w,
+                                     weight=0.75 * float(np.float32(scale[s]))))
+        if ref.sum() == 0:
+            assert maps[s].sum() == 0
+            continue
+        worst = max(worst, rel_l2(maps[s], ref))
+    print(f"{scheme}: {rmin.size} shells in one pass vs one pass per shell: worst {worst:.2e}")
+    assert worst < 1e-6
 
 
 def test_healpix_paint_at_paint_nside():
