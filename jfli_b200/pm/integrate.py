@@ -170,28 +170,41 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
 
 def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t0: float, dt0: float,
                        dtype=np.float32) -> RunResult:
-    """The ReversibleDoubleKickDrift loop as one autograd node whose backward is the
-    reversible adjoint (pm/adjoint.py), for inputs that require gradients. The
-    reference's equivalent is nbody(..., adjoint="reverse") under jax.grad
-    (pm/integrate.py:147-535). Covers one density snapshot without a correction kernel."""
+    """The N-body loop as one autograd node whose backward is the reversible adjoint
+    (pm/adjoint.py), for inputs that require gradients. The reference's equivalents are
+    nbody(..., adjoint="reverse") and nbody(..., adjoint="checkpointed") under jax.grad
+    (pm/integrate.py:109-535). Covers one density snapshot without a correction kernel.
+
+    EfficientDriftDoubleKick takes the same route: its fused step kicks with the pending
+    factor (the initial half kick at step 0, step i-1's kick after that) and then drifts,
+    v' = v + k_i F(x), x' = x + d_i v', which is the reversible step with the kick array
+    shifted by one; its last kick only touches the final velocities, not the density."""
     from .adjoint import ForwardTables, ReversibleNBody
     from .interp import NoInterp
 
     interp = solver.interp_kernel
     tgt = interp.painting.target if interp.painting is not None else "particles"
     ts_arr = np.atleast_1d(np.asarray(ts))
-    if not (isinstance(solver, ReversibleDoubleKickDrift) and isinstance(solver.pgd_kernel, NoCorrection)
+    efficient = isinstance(solver, EfficientDriftDoubleKick)
+    if not ((efficient or isinstance(solver, ReversibleDoubleKickDrift)) and isinstance(solver.pgd_kernel, NoCorrection)
             and isinstance(interp, NoInterp) and tgt == "density" and ts_arr.size == 1
             and _scalar_weight(interp.painting.weights) == 1.0):
         raise NotImplementedError(
-            "gradients run through the reversible adjoint: ReversibleDoubleKickDrift with NoCorrection and a "
-            "NoInterp density snapshot at one time")
+            "gradients run through the reversible adjoint: ReversibleDoubleKickDrift or EfficientDriftDoubleKick "
+            "with NoCorrection and a NoInterp density snapshot at one time")
     if dx.unit != PositionUnit.GRID_RELATIVE:
         raise NotImplementedError("differentiable integration takes GRID_RELATIVE displacements")
     steps = [(e[1], e[2]) for e in time_events(t0, ts, dt0, dtype) if e[0] == "step"]
-    cs = [solver.step_coefficients(cosmo, a, b, dt0, t0) for a, b in steps]
-    tables = ForwardTables(ktab=None, ptab=None, lpt=None, kicks=np.array([c.kick for c in cs]),
-                           drifts=np.array([c.drift for c in cs]))
+    if efficient:
+        kicks, drifts = EfficientDriftDoubleKick.schedule_arrays(cosmo, [a for a, _ in steps], [b for _, b in steps],
+                                                                 dt0)
+        kicks = np.concatenate([[EfficientDriftDoubleKick.init_kick(cosmo, t0, t0 + dt0)],
+                                np.asarray(kicks, np.float64)[:-1]])
+    else:
+        cs = [solver.step_coefficients(cosmo, a, b, dt0, t0) for a, b in steps]
+        kicks, drifts = np.array([c.kick for c in cs]), np.array([c.drift for c in cs])
+    tables = ForwardTables(ktab=None, ptab=None, lpt=None, kicks=np.asarray(kicks, np.float64),
+                           drifts=np.asarray(drifts, np.float64))
     rho = ReversibleNBody.apply(dx.array.contiguous(), p.array.contiguous(), None, tables)
     from ..fields import DensityField, FieldStatus
 

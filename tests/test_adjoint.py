@@ -368,6 +368,54 @@ def test_differentiation_config_128_matches_gpu_fd():
     assert _rel(float(sg.grad), fd_s8) < 1e-2
 
 
+def test_edk_density_gradient_matches_oracle_fd():
+    """nbody with EfficientDriftDoubleKick (the reference's default solver, adjoint
+    "checkpointed") on displacements and momenta that require grad: the density equals the
+    fused loop's, and the directional derivative of <a, rho(final)> with respect to
+    (dx, p) matches central differences of the FP64 oracle's FastPM loop (oracle/pm.py
+    kdk_run) driven by the same host coefficients."""
+    import jfli_b200 as jf
+    from jfli_b200.pm.integrate import time_events
+    from jfli_b200.pm.solvers import EfficientDriftDoubleKick as EDK
+
+    n, box, t0, t1, dt0 = 32, 128.0, 0.1, 1.0, 0.15
+    cosmo = jf.Planck18()
+    ic = jf.interpolate_initial_conditions(jf.white_noise(21, (n,) * 3), (n,) * 3, (box,) * 3, cosmo=cosmo)
+    dx, p = jf.lpt(cosmo, ic, ts=t0, order=2)
+    x0, v0 = dx.array.detach().contiguous().clone(), p.array.detach().contiguous().clone()
+    rng = np.random.default_rng(22)
+    a = rng.standard_normal((n, n, n))
+    r = rng.standard_normal((n, n, n, 3))
+    s = rng.standard_normal((n, n, n, 3))
+    solver = jf.EfficientDriftDoubleKick(interp_kernel=jf.NoInterp(painting=jf.PaintingOptions(target="density")))
+    xg, vg = x0.clone().requires_grad_(True), v0.clone().requires_grad_(True)
+    rho = jf.nbody(cosmo, dx.replace(array=xg), p.replace(array=vg), t0=t0, t1=t1, dt0=dt0, solver=solver)
+    loss = (rho.array.double() * torch.as_tensor(a, device="cuda")).sum()
+    loss.backward()
+    g_dir = float(np.sum(xg.grad.cpu().numpy() * r) + np.sum(vg.grad.cpu().numpy() * s))
+    with torch.no_grad():
+        rho_f = jf.nbody(cosmo, dx.replace(array=x0), p.replace(array=v0), t0=t0, t1=t1, dt0=dt0, solver=solver)
+    e_fwd = float((rho.array.detach() - rho_f.array).norm() / rho_f.array.norm())
+
+    steps = [(e[1], e[2]) for e in time_events(t0, [t1], dt0) if e[0] == "step"]
+    kicks, drifts = EDK.schedule_arrays(cosmo, [q for q, _ in steps], [q for _, q in steps], dt0)
+    coeffs = dict(init_kick=EDK.init_kick(cosmo, t0, t0 + dt0), steps=list(zip(kicks, drifts)))
+
+    def oracle_loss(x, v):
+        xf, _, _ = opm.kdk_run(x, v, coeffs, np.float64)
+        return float(np.sum(a * opm.cic_paint(xf)))
+
+    x64, v64 = x0.cpu().numpy().astype(np.float64), v0.cpu().numpy().astype(np.float64)
+    eps = 1e-5
+    fd = (oracle_loss(x64 + eps * r, v64 + eps * s) - oracle_loss(x64 - eps * r, v64 - eps * s)) / (2 * eps)
+    L0 = oracle_loss(x64, v64)
+    print(f"EDK: density vs the fused loop {e_fwd:.2e}; loss GPU {float(loss):.8e} oracle {L0:.8e}; "
+          f"directional derivative {g_dir:.6e} vs oracle central difference {fd:.6e}")
+    assert e_fwd < 1e-5
+    assert _rel(float(loss), L0) < 1e-4
+    assert _rel(g_dir, fd) < 1e-3
+
+
 def test_public_api_gradient_equals_forward_model():
     """interpolate_initial_conditions -> lpt -> nbody(ReversibleDoubleKickDrift) -> power
     through the public API with a noise field that requires grad gives the same gradient
