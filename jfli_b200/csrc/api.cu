@@ -389,7 +389,7 @@ int jfli_lpt(void* stream, const float* ic, int order, float c1x, float c2x, flo
   cudaError_t e = jfli::poisson_potential(ic, spec, pot, d, 0.0f, 1.0f, s);
   if (e == cudaSuccess) e = jfli::grid_gradient(pot, dx, 1.0f, 0, d, s);
   if (e == cudaSuccess && order == 2) {
-    e = jfli::lpt2_source(pot, src, d, s);
+    e = jfli::lpt2_source(dx, src, d, s);
     if (e == cudaSuccess) e = jfli::poisson_potential(src, spec, pot, d, 0.0f, 1.0f, s);
     if (e == cudaSuccess) e = jfli::grid_gradient(pot, f2, 1.0f, 0, d, s);
   }
@@ -427,7 +427,7 @@ int jfli_lpt_lightcone(void* stream, const float* ic, int order, const double* t
   cudaError_t e = jfli::poisson_potential(ic, spec, pot, d, 0.0f, 1.0f, s);
   if (e == cudaSuccess) e = jfli::grid_gradient(pot, f1, 1.0f, 0, d, s);
   if (e == cudaSuccess && order == 2) {
-    e = jfli::lpt2_source(pot, src, d, s);
+    e = jfli::lpt2_source(f1, src, d, s);
     if (e == cudaSuccess) e = jfli::poisson_potential(src, spec, pot, d, 0.0f, 1.0f, s);
     if (e == cudaSuccess) e = jfli::grid_gradient(pot, f2, 1.0f, 0, d, s);
   }

@@ -572,25 +572,40 @@ __device__ __forceinline__ float hess_component(const float* __restrict__ f, con
   return acc;
 }
 
-// The 2LPT source itself (reference call site pm/lpt.py:119).
-__global__ void k_lpt2_source(const float* __restrict__ pot, float* __restrict__ out, PGrid g) {
+// The 2LPT source (reference call site pm/lpt.py:119), from the first-order field
+// F = -D phi (AoS, as k_grid_gradient writes it, which the LPT has just computed):
+// phi_ab = D_b D_a phi = -D_b F_a, since the FD operators are convolutions and commute.
+// Four loads per component instead of the 16 of hess_component's two-stencil product;
+// the same operator, with F rounded to FP32 in between.
+__global__ void k_lpt2_source_grad(const float* __restrict__ F, float* __restrict__ out, PGrid g) {
   const long long b = blockIdx.y;
-  pot += b * g.np;
+  F += b * g.np * 3;
   out += b * g.np;
   const int n3[3] = {g.nx, g.ny, g.nz};
   const int st[3] = {g.yz, g.nz, 1};
+  const float inv12 = 1.0f / 12.0f;
   for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
     int c3[3];
     particle_ijk(g, p, c3[0], c3[1], c3[2]);
-    const int base = c3[0] * g.yz + c3[1] * g.nz + c3[2];
     float h[3][3];
-    for (int a = 0; a < 3; ++a)
-      for (int bb = a; bb < 3; ++bb) h[a][bb] = hess_component(pot, c3, n3, st, base, a, bb);
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb) {
+      const int rest = (int)p - c3[bb] * st[bb];
+      const int m2 = 3 * (rest + wrap1(c3[bb] - 2, n3[bb]) * st[bb]);
+      const int m1 = 3 * (rest + wrap1(c3[bb] - 1, n3[bb]) * st[bb]);
+      const int p1 = 3 * (rest + wrap1(c3[bb] + 1, n3[bb]) * st[bb]);
+      const int p2 = 3 * (rest + wrap1(c3[bb] + 2, n3[bb]) * st[bb]);
+#pragma unroll
+      for (int a = 0; a <= bb; ++a)
+        h[a][bb] = -(8.0f * (__ldg(F + p1 + a) - __ldg(F + m1 + a)) - (__ldg(F + p2 + a) - __ldg(F + m2 + a))) * inv12;
+    }
     // accumulate in the reference's loop order
     float delta2 = 0.f, acc_diag = 0.f;
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
       delta2 += h[a][a] * acc_diag;
       acc_diag += h[a][a];
+#pragma unroll
       for (int bb = a + 1; bb < 3; ++bb) delta2 -= h[a][bb] * h[a][bb];
     }
     out[p] = delta2;
@@ -768,8 +783,8 @@ cudaError_t grid_gradient(const float* pot, float* out, float scale, int accumul
   return cudaGetLastError();
 }
 
-cudaError_t lpt2_source(const float* pot, float* out, const MeshDims& d, cudaStream_t s) {
-  k_lpt2_source<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(pot, out, make_pgrid(d));
+cudaError_t lpt2_source(const float* grad, float* out, const MeshDims& d, cudaStream_t s) {
+  k_lpt2_source_grad<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(grad, out, make_pgrid(d));
   note_launch();
   return cudaGetLastError();
 }

@@ -60,7 +60,8 @@ cudaError_t kick_drift_paint_slots(float* disp, float* vel, const float* force, 
                                    const MeshDims& d, cudaStream_t s);
 cudaError_t grid_gradient(const float* pot, float* out, float scale, int accumulate, const MeshDims& d,
                           cudaStream_t s);
-cudaError_t lpt2_source(const float* pot, float* out, const MeshDims& d, cudaStream_t s);
+// 2LPT source from the first-order field F = -D phi1 (AoS, k_grid_gradient's layout)
+cudaError_t lpt2_source(const float* grad, float* out, const MeshDims& d, cudaStream_t s);
 cudaError_t lpt_combine(const float* f1, const float* f2, float c1x, float c2x, float c1p, float c2p, float* dx,
                         float* p, const MeshDims& d, cudaStream_t s);
 cudaError_t axpy_particles(float* y, const float* x, float a, const MeshDims& d, cudaStream_t s);
