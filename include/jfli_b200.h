@@ -230,6 +230,18 @@ int jfli_healpix_paint_shells(void* stream, const float* disp, int absolute, con
                               const double* rmin, const double* rmax, const float* scale, int nside, int scheme,
                               float sigma, float* maps, int accumulate, int nx, int ny, int nz, int batch, char* err,
                               size_t errlen);
+/* Adjoint of jfli_healpix_paint_shells (ngp or bilinear), the shell painter's `_bwd`: with
+ * maps_bar[s][12 nside^2] the cotangent of shell s's map, adds to disp_bar (particle grid
+ * layout) each particle's weight_p scale_s sum_q maps_bar[s][pix_q] d w_q / d disp (zero
+ * for ngp), and, when weights_bar is not NULL, weight scale_s sum_q maps_bar[s][pix_q] w_q
+ * to weights_bar. Shell membership (a step in the distance) contributes nothing. The other
+ * arguments as jfli_healpix_paint_shells; batch 1. */
+int jfli_healpix_paint_shells_adjoint(void* stream, const float* disp, int absolute, const float* weights,
+                                      float weight, float lx, float ly, float lz, float ox, float oy, float oz,
+                                      int nshells, const double* rmin, const double* rmax, const float* scale,
+                                      int nside, int scheme, const float* maps_bar, float* disp_bar,
+                                      float* weights_bar, int nx, int ny, int nz, int batch, char* err,
+                                      size_t errlen);
 /* HEALPix shell painting with the "rbf_neighbor" scheme (reference
  * _src/fields/_painting.py:18,291; its arithmetic lives in the absent jaxpm fork, so this
  * is the library's own definition): each particle in rmin < r <= rmax deposits onto the 4
@@ -307,6 +319,14 @@ int jfli_lightcone_drift(void* stream, const float* disp, const float* vel, floa
 size_t jfli_born_workspace_bytes(int nplanes, long long npix);
 int jfli_born(void* stream, const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
               float* out, void* workspace, size_t workspace_bytes, char* err, size_t errlen);
+/* Adjoint of jfli_born (its `_bwd`): maps_bar[p][pix] = u_p / mean_p - sum_pix' u_p m_p /
+ * (mean_p^2 npix) with u_p = sum_k weights[k][p] kappa_bar[k][pix], the maps' cotangent
+ * from the convergence maps' (the second term is the share through each plane's mean).
+ * Workspace: jfli_born_adjoint_workspace_bytes. */
+size_t jfli_born_adjoint_workspace_bytes(int nplanes, long long npix);
+int jfli_born_adjoint(void* stream, const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
+                      const float* kappa_bar, float* maps_bar, void* workspace, size_t workspace_bytes, char* err,
+                      size_t errlen);
 
 /* Born convergence of nplanes flat-sky planes [nplanes][n0][n1]: out[k][i0][i1] =
  * sum_p weights[k][p] (v_p / mean_p - 1), v_p the periodic bilinear sample of plane p at

@@ -149,6 +149,9 @@ _SIGNATURES = {
          *_ERR],
     ),
     "jfli_born": (c_int, [c_void_p, c_void_p, c_int, c_longlong, c_void_p, c_int, c_void_p, c_void_p, c_size_t, *_ERR]),
+    "jfli_born_adjoint_workspace_bytes": (c_size_t, [c_int, c_longlong]),
+    "jfli_born_adjoint": (
+        c_int, [c_void_p, c_void_p, c_int, c_longlong, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_size_t, *_ERR]),
     "jfli_adjoint_partials_count": (c_size_t, _DIMS),
     "jfli_kkd_workspace_bytes": (c_size_t, _DIMS),
     "jfli_kkd_run": (
@@ -204,6 +207,12 @@ _SIGNATURES = {
         [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float, c_float, c_int,
          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_float), c_int, c_int,
          c_float, c_void_p, c_int, *_DIMS, *_ERR],
+    ),
+    "jfli_healpix_paint_shells_adjoint": (
+        c_int,
+        [c_void_p, c_void_p, c_int, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float, c_float, c_int,
+         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_float), c_int, c_int,
+         c_void_p, c_void_p, c_void_p, *_DIMS, *_ERR],
     ),
     "jfli_healpix_paint": (
         c_int,

@@ -578,6 +578,35 @@ int jfli_healpix_paint_shells(void* stream, const float* disp, int absolute, con
                      err, errlen, "jfli_healpix_paint_shells");
 }
 
+int jfli_healpix_paint_shells_adjoint(void* stream, const float* disp, int absolute, const float* weights,
+                                      float weight, float lx, float ly, float lz, float ox, float oy, float oz,
+                                      int nshells, const double* rmin, const double* rmax, const float* scale,
+                                      int nside, int scheme, const float* maps_bar, float* disp_bar,
+                                      float* weights_bar, int nx, int ny, int nz, int batch, char* err,
+                                      size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(maps_bar);
+  CHECK_PTR(disp_bar);
+  if (batch != 1) return fail(err, errlen, JFLI_EUNSUPPORTED, "one particle set per call (batch %d)", batch);
+  if (nshells < 1) return fail(err, errlen, JFLI_EINVAL, "nshells must be >= 1");
+  CHECK_PTR(rmin);
+  CHECK_PTR(rmax);
+  CHECK_PTR(scale);
+  if (nside < 1 || nside > 8192) return fail(err, errlen, JFLI_EINVAL, "nside %d outside [1, 8192]", nside);
+  if (scheme != JFLI_HEALPIX_NGP && scheme != JFLI_HEALPIX_BILINEAR)
+    return fail(err, errlen, JFLI_EUNSUPPORTED, "the shell-painting adjoint has the ngp (0) and bilinear (1) schemes, "
+                "not %d", scheme);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const MeshDims d{nx, ny, nz, batch};
+  const float box[3] = {lx, ly, lz};
+  const float obs[3] = {ox, oy, oz};
+  return cuda_status(jfli::healpix_paint_shells_adjoint(disp, absolute, weights, weight, d, box, obs, nshells, rmin,
+                                                        rmax, scale, nside, scheme, maps_bar, disp_bar, weights_bar,
+                                                        (cudaStream_t)stream),
+                     err, errlen, "jfli_healpix_paint_shells_adjoint");
+}
+
 int jfli_healpix_paint_rbf(void* stream, const float* disp, int absolute, const float* weights, float weight,
                            float lx, float ly, float lz, float ox, float oy, float oz, float rmin, float rmax, int nside,
                            float sigma, float* map, int accumulate, int nx, int ny, int nz, int batch, char* err,
@@ -841,6 +870,32 @@ int jfli_born(void* stream, const float* maps, int nplanes, long long npix, cons
   return cuda_status(
       jfli::born_convergence(maps, nplanes, npix, weights, nsrc, out, partials, mean, (cudaStream_t)stream), err,
       errlen, "jfli_born");
+}
+
+size_t jfli_born_adjoint_workspace_bytes(int nplanes, long long npix) {
+  return jfli_born_workspace_bytes(nplanes, npix) + align256(sizeof(float) * (nplanes > 0 ? nplanes : 0));
+}
+
+int jfli_born_adjoint(void* stream, const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
+                      const float* kappa_bar, float* maps_bar, void* workspace, size_t workspace_bytes, char* err,
+                      size_t errlen) {
+  CHECK_PTR(maps);
+  CHECK_PTR(weights);
+  CHECK_PTR(kappa_bar);
+  CHECK_PTR(maps_bar);
+  CHECK_PTR(workspace);
+  if (nplanes < 1 || nplanes > 256) return fail(err, errlen, JFLI_EINVAL, "nplanes %d outside [1, 256]", nplanes);
+  if (nsrc < 1 || nsrc > 32) return fail(err, errlen, JFLI_EINVAL, "nsrc %d outside [1, 32]", nsrc);
+  if (npix < 1) return fail(err, errlen, JFLI_EINVAL, "npix must be positive");
+  const size_t need = jfli_born_adjoint_workspace_bytes(nplanes, npix);
+  if (workspace_bytes < need)
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  double* partials = (double*)workspace;
+  float* mean = (float*)((char*)workspace + align256(sizeof(double) * (size_t)nplanes * jfli::born_ctas(npix)));
+  float* c = (float*)((char*)workspace + jfli_born_workspace_bytes(nplanes, npix));
+  return cuda_status(jfli::born_convergence_adjoint(maps, nplanes, npix, weights, nsrc, kappa_bar, maps_bar,
+                                                    partials, mean, c, (cudaStream_t)stream),
+                     err, errlen, "jfli_born_adjoint");
 }
 
 int jfli_born_flat(void* stream, const float* maps, int nplanes, int n0, int n1, const float* weights, int nsrc,

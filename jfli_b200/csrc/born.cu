@@ -69,6 +69,82 @@ __global__ void k_born_combine(const float* __restrict__ maps, int nplanes, long
   }
 }
 
+// Adjoint of k_born_combine, the maps' cotangent from kappa's (kbar):
+//   u_p = sum_k W[k][p] kbar_k,   mbar_p = u_p / mean_p - c_p,
+//   c_p = sum_pix u_p m_p / (mean_p^2 npix)   (the share through the plane's mean).
+// First pass, one CTA row per plane: mbar_p = u_p / mean_p and per-CTA FP64 partials of
+// sum u_p m_p.
+__global__ void __launch_bounds__(kBornThreads) k_born_adj_u(const float* __restrict__ maps, long long npix,
+                                                            const float* __restrict__ mean,
+                                                            const float* __restrict__ w, int nsrc, int nplanes,
+                                                            const float* __restrict__ kbar,
+                                                            float* __restrict__ maps_bar,
+                                                            double* __restrict__ dots) {
+  const int p = blockIdx.y;
+  const float* m = maps + p * npix;
+  float* mb = maps_bar + p * npix;
+  const float inv_mean = 1.0f / mean[p];
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += (long long)gridDim.x * blockDim.x) {
+    float u = 0.f;
+    for (int k = 0; k < nsrc; ++k) u += __ldg(w + k * nplanes + p) * kbar[k * npix + i];
+    mb[i] = u * inv_mean;
+    acc += (double)u * (double)m[i];
+  }
+  __shared__ double sh[kBornThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < kBornThreads / 32; ++i) s += sh[i];
+    dots[p * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// One thread per plane: c_p from the partials in CTA order.
+__global__ void k_born_adj_c(const double* __restrict__ dots, int nctas, int nplanes, long long npix,
+                             const float* __restrict__ mean, float* __restrict__ c) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nplanes) return;
+  double s = 0.0;
+  for (int i = 0; i < nctas; ++i) s += dots[(long long)p * nctas + i];
+  const double mu = (double)mean[p];
+  c[p] = (float)(s / (mu * mu * (double)npix));
+}
+
+__global__ void k_born_adj_sub(float* __restrict__ maps_bar, long long npix, const float* __restrict__ c) {
+  const int p = blockIdx.y;
+  const float cp = c[p];
+  float* mb = maps_bar + p * npix;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += (long long)gridDim.x * blockDim.x)
+    mb[i] -= cp;
+}
+
+cudaError_t born_convergence_adjoint(const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
+                                     const float* kappa_bar, float* maps_bar, double* partials, float* mean,
+                                     float* c, cudaStream_t s) {
+  const int nctas = born_ctas(npix);
+  k_plane_partials<<<dim3(nctas, nplanes), kBornThreads, 0, s>>>(maps, npix, partials);
+  note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_plane_means<<<(nplanes + 127) / 128, 128, 0, s>>>(partials, nctas, nplanes, npix, mean);
+  note_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_born_adj_u<<<dim3(nctas, nplanes), kBornThreads, 0, s>>>(maps, npix, mean, weights, nsrc, nplanes, kappa_bar,
+                                                            maps_bar, partials);
+  note_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_born_adj_c<<<(nplanes + 127) / 128, 128, 0, s>>>(partials, nctas, nplanes, npix, mean, c);
+  note_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_born_adj_sub<<<dim3(nctas, nplanes), kBornThreads, 0, s>>>(maps_bar, npix, c);
+  note_launch();
+  return cudaGetLastError();
+}
+
 // Flat-sky planes (reference _src/lensing/_born.py:29-97 with coords, and _born_flat,
 // 133-186): each output pixel (i0, i1) samples plane p by periodic bilinear interpolation
 // (jax map_coordinates, order 1, mode "wrap") at axis-0 coordinate i1 s0_p - 0.5 and axis-1

@@ -164,6 +164,76 @@ __device__ __forceinline__ void interp_weights(double theta, double phi, int nsi
   }
 }
 
+// interp_weights with the weights' derivatives along theta and phi (the adjoint of the
+// bilinear deposit). Inside a ring pair the weights are products of the ring weight
+// (linear in theta between the two rings' thetas) and the in-ring weights (linear in phi
+// between the two bracketing pixel centres); the polar caps add the quarter weights of
+// the four polar pixels, linear in theta. A weight's jump where the bracket changes is
+// continuous in the map, so the piecewise derivatives are the map's.
+__device__ __forceinline__ void interp_weights_grad(double theta, double phi, int nside,
+                                                    const double* __restrict__ theta_tab, long long pix[4],
+                                                    double w[4], double dth[4], double dph[4]) {
+  interp_weights(theta, phi, nside, theta_tab, pix, w);
+  const double twopi = 2.0 * M_PI;
+  const double z = cos(theta);
+  const int ir1 = ring_above(z, nside);
+  const int ir2 = ir1 + 1;
+  double theta1 = 0.0, theta2 = 0.0, a[4] = {0.0, 0.0, 0.0, 0.0}, da[4] = {0.0, 0.0, 0.0, 0.0};
+  double ph = fmod(phi, twopi);
+  if (ph < 0) ph += twopi;
+  if (ir1 > 0) {
+    const RingInfo r = ring_info_tab(ir1, nside, theta_tab);
+    theta1 = r.theta;
+    const double dphi = twopi / r.npix;
+    const double tmp = ph / dphi - 0.5 * r.shifted;
+    const long long i1 = tmp < 0 ? (long long)tmp - 1 : (long long)tmp;
+    const double wp = (ph - (i1 + 0.5 * r.shifted) * dphi) / dphi;
+    a[0] = 1.0 - wp;
+    a[1] = wp;
+    da[0] = -1.0 / dphi;
+    da[1] = 1.0 / dphi;
+  }
+  if (ir2 < 4 * nside) {
+    const RingInfo r = ring_info_tab(ir2, nside, theta_tab);
+    theta2 = r.theta;
+    const double dphi = twopi / r.npix;
+    const double tmp = ph / dphi - 0.5 * r.shifted;
+    const long long i1 = tmp < 0 ? (long long)tmp - 1 : (long long)tmp;
+    const double wp = (ph - (i1 + 0.5 * r.shifted) * dphi) / dphi;
+    a[2] = 1.0 - wp;
+    a[3] = wp;
+    da[2] = -1.0 / dphi;
+    da[3] = 1.0 / dphi;
+  }
+  if (ir1 == 0) {
+    const double wt = theta / theta2, dwt = 1.0 / theta2;
+    dth[0] = dth[1] = -0.25 * dwt;
+    dth[2] = a[2] * dwt - 0.25 * dwt;
+    dth[3] = a[3] * dwt - 0.25 * dwt;
+    dph[0] = dph[1] = 0.0;
+    dph[2] = da[2] * wt;
+    dph[3] = da[3] * wt;
+  } else if (ir2 == 4 * nside) {
+    const double wt = (theta - theta1) / (M_PI - theta1), dwt = 1.0 / (M_PI - theta1);
+    dth[0] = -a[0] * dwt + 0.25 * dwt;
+    dth[1] = -a[1] * dwt + 0.25 * dwt;
+    dth[2] = dth[3] = 0.25 * dwt;
+    dph[0] = da[0] * (1.0 - wt);
+    dph[1] = da[1] * (1.0 - wt);
+    dph[2] = dph[3] = 0.0;
+  } else {
+    const double wt = (theta - theta1) / (theta2 - theta1), dwt = 1.0 / (theta2 - theta1);
+    dth[0] = -a[0] * dwt;
+    dth[1] = -a[1] * dwt;
+    dth[2] = a[2] * dwt;
+    dth[3] = a[3] * dwt;
+    dph[0] = da[0] * (1.0 - wt);
+    dph[1] = da[1] * (1.0 - wt);
+    dph[2] = da[2] * wt;
+    dph[3] = da[3] * wt;
+  }
+}
+
 // Centre (theta, phi) of RING pixel pix: its ring found by bisection on the rings' start
 // pixels, phi = (index in ring + shift / 2) 2 pi / pixels in ring.
 __device__ __forceinline__ void pix_centre_ring(long long pix, int nside, const double* __restrict__ theta_tab,
@@ -300,6 +370,85 @@ __global__ void k_healpix_paint_shells(const float* __restrict__ disp, int absol
     for (int sh = 0; sh < shells.n; ++sh)
       if (rr > shells.rmin[sh] && rr <= shells.rmax[sh])
         deposit_direction(vx, vy, vz, rr, w * shells.scale[sh], nside, scheme, theta_tab, maps + sh * npix, sigma);
+  }
+}
+
+// Adjoint of k_healpix_paint_shells for the bilinear and ngp schemes. With maps_bar[s] the
+// cotangent of shell s's map, a particle of shell s deposited weight_p scale_s w_q at
+// pixels pix_q, so it adds
+//   to its position cotangent:  weight_p scale_s sum_q maps_bar[s][pix_q] d w_q / d disp
+//   to its weight cotangent:    weight scale_s sum_q maps_bar[s][pix_q] w_q
+// (ngp: w = 1 at one pixel, no position term). Shell membership is a step in the distance
+// and contributes nothing (as the derivative of a mask). d w / d disp chains the weights'
+// theta and phi derivatives with theta = acos(v_z / r), phi = atan2(v_y, v_x),
+// v = (grid + disp) cell - observer. Accumulates into disp_bar (and weights_bar).
+__global__ void k_healpix_paint_shells_adjoint(const float* __restrict__ disp, int absolute,
+                                               const float* __restrict__ weights, float weight, MeshDims d,
+                                               double3 cell, double3 obs, ShellSet shells, int nside, int scheme,
+                                               const double* __restrict__ theta_tab,
+                                               const float* __restrict__ maps_bar, float* __restrict__ disp_bar,
+                                               float* __restrict__ weights_bar) {
+  const long long np = d.cells();
+  const long long npix = 12LL * nside * nside;
+  const long long yz = (long long)d.ny * d.nz;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+    double gx = disp[3 * p + 0], gy = disp[3 * p + 1], gz = disp[3 * p + 2];
+    if (!absolute) {
+      const int i = (int)(p / yz);
+      const long long r = p - (long long)i * yz;
+      const int j = (int)(r / d.nz);
+      const int k = (int)(r - (long long)j * d.nz);
+      gx += (double)i;
+      gy += (double)j;
+      gz += (double)k;
+    }
+    const double vx = gx * cell.x - obs.x, vy = gy * cell.y - obs.y, vz = gz * cell.z - obs.z;
+    const double rr = sqrt(vx * vx + vy * vy + vz * vz);
+    bool any = false;
+    long long pix[4] = {-1, -1, -1, -1};
+    double w[4] = {0.0, 0.0, 0.0, 0.0}, dth[4] = {0.0, 0.0, 0.0, 0.0}, dph[4] = {0.0, 0.0, 0.0, 0.0};
+    double g_th = 0.0, g_ph = 0.0, g_w = 0.0;
+    for (int sh = 0; sh < shells.n; ++sh) {
+      if (!(rr > shells.rmin[sh] && rr <= shells.rmax[sh])) continue;
+      if (!any) {
+        any = true;
+        const double zc = vz / rr;
+        const double phi = atan2(vy, vx);
+        if (scheme == 0) {
+          pix[0] = ang2pix_ring(zc, phi, nside);
+          w[0] = 1.0;
+        } else {
+          interp_weights_grad(acos(fmin(1.0, fmax(-1.0, zc))), phi, nside, theta_tab, pix, w, dth, dph);
+        }
+      }
+      const float* mb = maps_bar + sh * npix;
+      double gt = 0.0, gp = 0.0, gs = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (pix[q] < 0 || pix[q] >= npix) continue;
+        const double m = (double)__ldg(mb + pix[q]);
+        gt += m * dth[q];
+        gp += m * dph[q];
+        gs += m * w[q];
+      }
+      const double sc = (double)shells.scale[sh];
+      g_th += sc * gt;
+      g_ph += sc * gp;
+      g_w += sc * gs;
+    }
+    if (!any) continue;
+    if (weights_bar) weights_bar[p] += (float)((double)weight * g_w);
+    if (scheme == 0) continue;
+    const double wp = weights ? (double)weights[p] * (double)weight : (double)weight;
+    const double s2 = vx * vx + vy * vy;
+    if (!(s2 > 0.0)) continue;  // on the polar axis: phi is undefined (measure zero)
+    const double sxy = sqrt(s2), r2 = rr * rr;
+    const double gvx = wp * (g_th * vz * vx / (r2 * sxy) - g_ph * vy / s2);
+    const double gvy = wp * (g_th * vz * vy / (r2 * sxy) + g_ph * vx / s2);
+    const double gvz = wp * (-g_th * sxy / r2);
+    disp_bar[3 * p + 0] += (float)(gvx * cell.x);
+    disp_bar[3 * p + 1] += (float)(gvy * cell.y);
+    disp_bar[3 * p + 2] += (float)(gvz * cell.z);
   }
 }
 
@@ -564,6 +713,36 @@ cudaError_t healpix_paint_shells(const float* disp, int absolute, const float* w
     }
     k_healpix_paint_shells<<<(unsigned)blocks, 256, 0, s>>>(disp, absolute, weights, weight, d, cell, obs, set, nside,
                                                             scheme, tab, maps + s0 * npix, sigma);
+    note_launch();
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t healpix_paint_shells_adjoint(const float* disp, int absolute, const float* weights, float weight,
+                                         const MeshDims& d, const float* box, const float* observer, int nshells,
+                                         const double* rmin, const double* rmax, const float* scale, int nside,
+                                         int scheme, const float* maps_bar, float* disp_bar, float* weights_bar,
+                                         cudaStream_t s) {
+  const double3 cell = make_double3((double)box[0] / d.nx, (double)box[1] / d.ny, (double)box[2] / d.nz);
+  const double3 obs = make_double3(observer[0], observer[1], observer[2]);
+  long long blocks = (d.cells() + 255) / 256;
+  if (blocks > (long long)sm_count() * 16) blocks = (long long)sm_count() * 16;
+  const double* tab = ring_theta_table(nside);
+  if (!tab) return cudaErrorMemoryAllocation;
+  const long long npix = 12LL * nside * nside;
+  for (int s0 = 0; s0 < nshells; s0 += kMaxShellsPerPass) {
+    ShellSet set;
+    set.n = nshells - s0 < kMaxShellsPerPass ? nshells - s0 : kMaxShellsPerPass;
+    for (int i = 0; i < set.n; ++i) {
+      set.rmin[i] = rmin[s0 + i];
+      set.rmax[i] = rmax[s0 + i];
+      set.scale[i] = scale[s0 + i];
+    }
+    k_healpix_paint_shells_adjoint<<<(unsigned)blocks, 256, 0, s>>>(disp, absolute, weights, weight, d, cell, obs, set,
+                                                                    nside, scheme, tab, maps_bar + s0 * npix,
+                                                                    disp_bar, weights_bar);
     note_launch();
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -105,6 +105,11 @@ cudaError_t lightcone_drift(const float* disp, const float* vel, float* out, con
 int born_ctas(long long npix);
 cudaError_t born_convergence(const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
                              float* out, double* partials, float* mean, cudaStream_t s);
+// Adjoint of born_convergence: maps_bar[p][pix] from kappa_bar[k][pix] (partials: nplanes x
+// born_ctas doubles; mean, c: nplanes floats of scratch).
+cudaError_t born_convergence_adjoint(const float* maps, int nplanes, long long npix, const float* weights, int nsrc,
+                                     const float* kappa_bar, float* maps_bar, double* partials, float* mean,
+                                     float* c, cudaStream_t s);
 cudaError_t born_flat(const float* maps, int nplanes, int n0, int n1, const float* weights, int nsrc, const float* s0,
                       const float* s1, float* out, double* partials, float* mean, cudaStream_t s);
 
@@ -159,6 +164,13 @@ cudaError_t healpix_paint(const float* disp, int absolute, const float* weights,
 // Up to kMaxShellsPerPass shells per launch (more are painted in further launches);
 // shell s: rmin[s] < r <= rmax[s], weight * scale[s], into maps + s * 12 nside^2.
 constexpr int kMaxShellsPerPass = 64;
+// Adjoint of healpix_paint_shells (scheme 0 or 1): accumulates the position cotangent
+// into disp_bar and, when non-null, the weight cotangent into weights_bar.
+cudaError_t healpix_paint_shells_adjoint(const float* disp, int absolute, const float* weights, float weight,
+                                         const MeshDims& d, const float* box, const float* observer, int nshells,
+                                         const double* rmin, const double* rmax, const float* scale, int nside,
+                                         int scheme, const float* maps_bar, float* disp_bar, float* weights_bar,
+                                         cudaStream_t s);
 cudaError_t healpix_paint_shells(const float* disp, int absolute, const float* weights, float weight,
                                  const MeshDims& d, const float* box, const float* observer, int nshells,
                                  const double* rmin, const double* rmax, const float* scale, int nside, int scheme,

@@ -136,10 +136,45 @@ def born_weights(cosmo, scale_factors, max_radius: float, nz_shear, min_z=0.01, 
     return W, z_eff
 
 
+class BornMaps(torch.autograd.Function):
+    """kappa = W (maps / mean - 1) as an autograd node: backward jfli_born_adjoint."""
+
+    @staticmethod
+    def forward(ctx, maps, weights):
+        ctx.weights = weights
+        ctx.save_for_backward(maps)
+        return _born_maps(maps.detach(), weights)
+
+    @staticmethod
+    def backward(ctx, kbar):
+        (maps,) = ctx.saved_tensors
+        maps = maps.detach().contiguous()
+        squeeze = maps.ndim == 1
+        m2 = maps[None] if squeeze else maps
+        nplanes, npix = int(m2.shape[0]), int(m2.shape[1])
+        w = torch.as_tensor(np.ascontiguousarray(ctx.weights, dtype=np.float32), device=maps.device)
+        kb = kbar.contiguous()
+        if tuple(kb.shape) != (w.shape[0], npix):
+            raise ValueError("kappa cotangent shape differs from the convergence maps'")
+        out = torch.empty_like(m2)
+        from .ops import workspace
+
+        ws = workspace(int(query("jfli_born_adjoint_workspace_bytes", nplanes, npix)), "born", maps.device)
+        call("jfli_born_adjoint", stream_ptr(), ptr(m2), nplanes, npix, ptr(w), int(w.shape[0]), ptr(kb), ptr(out),
+             ptr(ws), ws.numel())
+        return (out[0] if squeeze else out), None
+
+
 def born_maps(maps: torch.Tensor, weights: np.ndarray) -> torch.Tensor:
-    """kappa (K, npix) = W @ (maps / mean - 1) on the GPU."""
+    """kappa (K, npix) = W @ (maps / mean - 1) on the GPU (differentiable in the maps)."""
     if maps.dtype != torch.float32 or not maps.is_cuda:
         raise TypeError("maps must be a float32 CUDA tensor")
+    if torch.is_grad_enabled() and maps.requires_grad:
+        return BornMaps.apply(maps, weights)
+    return _born_maps(maps, weights)
+
+
+def _born_maps(maps: torch.Tensor, weights: np.ndarray) -> torch.Tensor:
     maps = maps.contiguous()
     if maps.ndim == 1:
         maps = maps[None]

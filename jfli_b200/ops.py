@@ -366,6 +366,39 @@ def healpix_paint_shells(pos: torch.Tensor, nside: int, box_size, observer_mpc, 
     return out
 
 
+def healpix_paint_shells_adjoint(pos: torch.Tensor, maps_bar: torch.Tensor, nside: int, box_size, observer_mpc, rmin,
+                                 rmax, scale, *, scheme: str = "bilinear", absolute: bool = False,
+                                 weights: torch.Tensor | None = None, weight: float = 1.0,
+                                 pos_bar: torch.Tensor | None = None,
+                                 weights_bar: torch.Tensor | None = None) -> torch.Tensor:
+    """Adjoint of healpix_paint_shells: accumulates into pos_bar (zeros when None, returned)
+    and, when given, weights_bar (see jfli_healpix_paint_shells_adjoint)."""
+    _check(pos, "pos")
+    _check(maps_bar, "maps_bar")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    if batch != 1:
+        raise ValueError("healpix_paint_shells_adjoint takes one particle set")
+    sch = {"ngp": _lib.JFLI_HEALPIX_NGP, "bilinear": _lib.JFLI_HEALPIX_BILINEAR}.get(scheme)
+    if sch is None:
+        raise NotImplementedError(f"the shell-painting adjoint has the ngp and bilinear schemes, not {scheme!r}")
+    lo = np.ascontiguousarray(np.atleast_1d(np.asarray(rmin, np.float64)))
+    hi = np.ascontiguousarray(np.atleast_1d(np.asarray(rmax, np.float64)))
+    sc = np.ascontiguousarray(np.atleast_1d(np.asarray(scale, np.float32)))
+    npix = 12 * nside * nside
+    if tuple(maps_bar.shape) != (lo.size, npix) or not maps_bar.is_contiguous():
+        raise ValueError(f"maps_bar must be a contiguous ({lo.size}, {npix}) tensor")
+    if pos_bar is None:
+        pos_bar = torch.zeros_like(pos)
+    lx, ly, lz = (float(v) for v in box_size)
+    ox, oy, oz = (float(v) for v in observer_mpc)
+    dp = ctypes.POINTER(ctypes.c_double)
+    call("jfli_healpix_paint_shells_adjoint", stream_ptr(), ptr(pos), int(absolute), ptr(weights), float(weight), lx,
+         ly, lz, ox, oy, oz, int(lo.size), lo.ctypes.data_as(dp), hi.ctypes.data_as(dp),
+         sc.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(nside), sch, ptr(maps_bar), ptr(pos_bar),
+         ptr(weights_bar), nx, ny, nz, batch)
+    return pos_bar
+
+
 def drift_tables(cosmo, n_dense: int = 4096):
     """Device FP32 copies of the FP64 host tables the light-cone drift interpolates:
     (chi ascending, a at chi), (growth a, D1), (dense a, dGfa)."""

@@ -21,6 +21,34 @@ def shell_volume_per_pixel(nside: int, rmin: float, rmax: float) -> float:
     return (4.0 * math.pi / (12 * nside * nside)) * (rmax**3 - rmin**3) / 3.0
 
 
+class PaintShells(torch.autograd.Function):
+    """Shells of one particle set as an autograd node: forward jfli_healpix_paint_shells,
+    backward its adjoint (position and per-particle weight cotangents; the shell edges are
+    steps in the distance and pass nothing back)."""
+
+    @staticmethod
+    def forward(ctx, pos, wts, geom):
+        nside, box, obs, rmin, rmax, scale, scheme, absolute = geom
+        out = ops.healpix_paint_shells(pos.detach().contiguous(), nside, box, obs, rmin, rmax, scale, scheme=scheme,
+                                       absolute=absolute, weights=None if wts is None else wts.detach().contiguous())
+        ctx.geom = geom
+        ctx.save_for_backward(pos, wts) if wts is not None else ctx.save_for_backward(pos)
+        ctx.has_w = wts is not None
+        return out
+
+    @staticmethod
+    def backward(ctx, maps_bar):
+        nside, box, obs, rmin, rmax, scale, scheme, absolute = ctx.geom
+        saved = ctx.saved_tensors
+        pos = saved[0].detach().contiguous()
+        wts = saved[1].detach().contiguous() if ctx.has_w else None
+        w_bar = torch.zeros_like(wts) if (wts is not None and ctx.needs_input_grad[1]) else None
+        pos_bar = ops.healpix_paint_shells_adjoint(pos, maps_bar.contiguous(), nside, box, obs, rmin, rmax, scale,
+                                                   scheme=scheme, absolute=absolute, weights=wts,
+                                                   weights_bar=w_bar)
+        return pos_bar, w_bar, None
+
+
 def paint_shells(field, centers, widths, scheme="bilinear", weights=None, out=None, sigma=None) -> torch.Tensor:
     """(S, 12 nside^2) maps of one particle set for S shells (`sigma`: the rbf_neighbor
     scheme's Gaussian width in radians)."""
@@ -31,12 +59,20 @@ def paint_shells(field, centers, widths, scheme="bilinear", weights=None, out=No
     npix = 12 * field.nside * field.nside
     centers = np.atleast_1d(np.asarray(centers, dtype=np.float64))
     widths = np.atleast_1d(np.asarray(widths, dtype=np.float64))
-    if out is None:
-        out = torch.empty(centers.size, npix, dtype=torch.float32, device=field.array.device)
     pos = field.array.contiguous()
     rmin, rmax = centers - widths / 2.0, centers + widths / 2.0
     vol = np.array([shell_volume_per_pixel(field.nside, a, b) for a, b in zip(rmin, rmax)])
     scale = np.where(vol > 0, ws / np.where(vol > 0, vol, 1.0), ws)
+    if torch.is_grad_enabled() and (pos.requires_grad or (w is not None and w.requires_grad)):
+        if pos.dim() != 4 or scheme not in ("ngp", "bilinear"):
+            raise NotImplementedError("gradients of spherical painting: one particle set, ngp or bilinear")
+        if out is not None:
+            raise ValueError("out= is not supported when painting differentiably")
+        geom = (field.nside, tuple(field.box_size), tuple(field.observer_position_mpc), rmin, rmax, scale, scheme,
+                absolute)
+        return PaintShells.apply(pos, w, geom)
+    if out is None:
+        out = torch.empty(centers.size, npix, dtype=torch.float32, device=field.array.device)
     if pos.dim() == 4 and out.is_contiguous():
         # one pass over the particles for all the shells
         ops.healpix_paint_shells(pos, field.nside, field.box_size, field.observer_position_mpc, rmin, rmax, scale,
