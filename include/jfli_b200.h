@@ -115,6 +115,17 @@ int jfli_poisson_potential(void* stream, const float* rho, float rho_mean, float
  * (kl, ks in radians per cell). Replaces pm/correction.py:170-189 (PGDKernel.apply). */
 int jfli_pgd_potential(void* stream, const float* rho, float rho_mean, float kl, float ks, float* pot, void* workspace,
                        size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* Adjoint of the PGD correction x' = x + alpha F_pgd(x) (the `jfli_pgd` entries' `_bwd`;
+ * F_pgd the CIC readout of the FD force mesh of jfli_pgd_potential's potential of the
+ * particles' own density, reference pm/correction.py:157-202): lam_x += alpha J^T u with J
+ * = dF_pgd/dx at the relative positions disp and u the cotangent of x' (pass lam_x = u to
+ * get the full cotangent of x). J^T u = grad_x R_x[sum_a u_a F_a] + grad_x R_x[rho_bar],
+ * rho_bar = P_pgd(div_FD paint(u)), the PGD filter being symmetric. Workspace:
+ * jfli_pgd_adjoint_workspace_bytes. */
+size_t jfli_pgd_adjoint_workspace_bytes(int nx, int ny, int nz, int batch);
+int jfli_pgd_adjoint(void* stream, const float* disp, const float* u, float alpha, float kl, float ks, float* lam_x,
+                     void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                     size_t errlen);
 /* forces[p] = scale * CIC readout of -grad_FD(pot) at the particle positions. */
 int jfli_readout_gradient(void* stream, const float* pos, int absolute, const float* pot, float scale, float* forces,
                           int nx, int ny, int nz, int batch, char* err, size_t errlen);

@@ -260,6 +260,30 @@ __global__ void __launch_bounds__(kAdjThreads, 3) k_adj_unkick_paint(
   }
 }
 
+// CIC paint of a vector per particle (u, 3 floats, particle grid layout) onto a float4
+// mesh, cleared by the caller: the cotangent paint of the PGD correction's adjoint.
+__global__ void k_paint_vec4(const float* __restrict__ disp, const float* __restrict__ u, float* __restrict__ ubar,
+                             PGrid g) {
+  const long long b = blockIdx.y;
+  disp += b * g.np * 3;
+  u += b * g.np * 3;
+  ubar += b * g.np * 4;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    int i, j, k;
+    particle_ijk(g, p, i, j, k);
+    const Cic1 cx = cic_rel(i, disp[3 * p + 0], g.nx), cy = cic_rel(j, disp[3 * p + 1], g.ny),
+               cz = cic_rel(k, disp[3 * p + 2], g.nz);
+    const float uu[3] = {u[3 * p + 0], u[3 * p + 1], u[3 * p + 2]};
+    deposit_vec4_lane_merged(reinterpret_cast<float4*>(ubar), g, cx, cy, cz, uu);
+  }
+}
+
+cudaError_t paint_vec4(const float* disp, const float* u, float* ubar, const MeshDims& d, cudaStream_t s) {
+  k_paint_vec4<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(disp, u, ubar, make_pgrid(d));
+  note_launch();
+  return cudaGetLastError();
+}
+
 // out(c) = [accumulate ? out(c) : 0] + sum_a D_a (alpha u_a + beta w_a)(c), with
 // D_a f(c) = [8 (f(c+e_a) - f(c-e_a)) - (f(c+2e_a) - f(c-2e_a))] / 12. Component a of
 // cell c is at index c * cell_stride + a * comp_stride (SoA meshes: 1, cells; AoS

@@ -138,6 +138,8 @@ cudaError_t adjoint_unkick_paint(const float* disp, float* vel, const float* lam
 cudaError_t sum_adjoint_partials(const double* partials, const MeshDims& d, double* out, cudaStream_t s);
 cudaError_t divergence_fd(const float* u, float alpha, const float* w, float beta, int aos, int accumulate,
                           float* out, const MeshDims& d, cudaStream_t s);
+// CIC paint of u (3 per particle) onto a float4 mesh (x, y, z, 0) cleared by the caller
+cudaError_t paint_vec4(const float* disp, const float* u, float* ubar, const MeshDims& d, cudaStream_t s);
 cudaError_t adjoint_position(const float* disp, const float* u, const float* rho_bar, const float* force, float scale,
                              float* lam_x, const MeshDims& d, cudaStream_t s);
 

@@ -55,12 +55,9 @@ class PGDKernel(AbstractCorrection):
 
         if pos.unit != PositionUnit.GRID_RELATIVE:
             pos = pos.to(PositionUnit.GRID_RELATIVE)
-        x = pos.array.contiguous().clone()
-        rho = ops.paint_cic(x)
-        force = ops.force_mesh(pgd_potential(rho, self.kl, self.ks, 1.0))
-        dummy_v = torch.empty_like(x)
-        ops.kick_drift_paint(x, dummy_v, force, self.alpha, 0.0, JFLI_STEP_CORRECT)
-        return pos.replace(array=x), vel
+        if torch.is_grad_enabled() and pos.array.requires_grad:
+            return pos.replace(array=PgdCorrection.apply(pos.array, (self.alpha, self.kl, self.ks))), vel
+        return pos.replace(array=pgd_correct(pos.array, self.alpha, self.kl, self.ks)), vel
 
     def rewind(self, t, pos, vel, full_drift_factor):
         raise NotImplementedError("PGDKernel is not reversible")
@@ -79,6 +76,41 @@ class SharpeningKernel(AbstractCorrection):
 
     def rewind(self, t, pos, vel, full_drift_factor):
         raise NotImplementedError("SharpeningKernel is not on the B200 path")
+
+
+def pgd_correct(x: torch.Tensor, alpha: float, kl: float, ks: float) -> torch.Tensor:
+    """x + alpha F_pgd(x) for relative displacements x (a new tensor)."""
+    x = x.detach().contiguous().clone()
+    rho = ops.paint_cic(x)
+    force = ops.force_mesh(pgd_potential(rho, kl, ks, 1.0))
+    ops.kick_drift_paint(x, torch.empty_like(x), force, alpha, 0.0, JFLI_STEP_CORRECT)
+    return x
+
+
+class PgdCorrection(torch.autograd.Function):
+    """x -> x + alpha F_pgd(x) as an autograd node; backward jfli_pgd_adjoint (the readout
+    and density parts of J^T, at the uncorrected positions)."""
+
+    @staticmethod
+    def forward(ctx, x, params):
+        ctx.params = params
+        ctx.save_for_backward(x)
+        return pgd_correct(x, *params)
+
+    @staticmethod
+    def backward(ctx, g):
+        from .._lib import call, ptr, query, stream_ptr
+
+        (x,) = ctx.saved_tensors
+        alpha, kl, ks = ctx.params
+        x = x.detach().contiguous()
+        u = g.contiguous()
+        lam = u.clone()
+        (nx, ny, nz), batch, _ = ops._mesh_dims(x, True)
+        ws = ops.workspace(int(query("jfli_pgd_adjoint_workspace_bytes", nx, ny, nz, batch)), "pgd_adj", x.device)
+        call("jfli_pgd_adjoint", stream_ptr(), ptr(x), ptr(u), float(alpha), float(kl), float(ks), ptr(lam), ptr(ws),
+             ws.numel(), nx, ny, nz, batch)
+        return lam, None
 
 
 def pgd_potential(rho: torch.Tensor, kl: float, ks: float, rho_mean: float = 1.0,
