@@ -263,6 +263,60 @@ class ReversibleNBody(torch.autograd.Function):
         return lam_x, lam_v, gom, None
 
 
+class ReversibleNBodyShells(torch.autograd.Function):
+    """(dx, p) -> HEALPix shells painted at snapshot times along the KKD loop (S, npix).
+
+    The loop runs in segments: `segments[j]` steps, then shell j painted from the positions
+    there (shell j: rmin, rmax, scale, with the scheme and nside of `geom`). The backward
+    walks the segments in reverse: at each shell the painter's adjoint adds that shell's
+    cotangent to lambda_x at the reconstructed positions, then the segment's steps are
+    reversed (jfli_kkd_adjoint, over the potentials kept by the forward when they fit)."""
+
+    @staticmethod
+    def forward(ctx, dx, p, tables: ForwardTables, segments, geom):
+        nside, box, obs, rmin, rmax, scale, scheme = geom
+        x = dx.detach().contiguous().clone()
+        v = p.detach().contiguous().clone()
+        n_all = int(sum(segments))
+        pots = potential_store(n_all, x) if any(ctx.needs_input_grad[:2]) else None
+        rho = torch.empty(x.shape[:-1], dtype=torch.float32, device=x.device)
+        maps = torch.empty(len(segments), 12 * nside * nside, dtype=torch.float32, device=x.device)
+        s0 = 0
+        for j, c in enumerate(segments):
+            if c > 0:
+                kkd_forward(x, v, tables.kicks[s0:s0 + c], tables.drifts[s0:s0 + c], rho,
+                            pots=None if pots is None else pots[s0:s0 + c])
+            ops.healpix_paint_shells(x, nside, box, obs, rmin[j:j + 1], rmax[j:j + 1], scale[j:j + 1], scheme=scheme,
+                                     out=maps[j:j + 1])
+            s0 += c
+        ctx.tables, ctx.segments, ctx.geom, ctx.pots = tables, list(segments), geom, pots
+        ctx.save_for_backward(x, v)
+        return maps
+
+    @staticmethod
+    def backward(ctx, maps_bar):
+        nside, box, obs, rmin, rmax, scale, scheme = ctx.geom
+        x, v = ctx.saved_tensors
+        x = x.clone()
+        v = v.clone()
+        t, pots = ctx.tables, ctx.pots
+        lam_x = torch.zeros_like(x)
+        lam_v = torch.zeros_like(v)
+        mb = maps_bar.contiguous()
+        s1 = int(sum(ctx.segments))
+        for j in range(len(ctx.segments) - 1, -1, -1):
+            ops.healpix_paint_shells_adjoint(x, mb[j:j + 1], nside, box, obs, rmin[j:j + 1], rmax[j:j + 1],
+                                             scale[j:j + 1], scheme=scheme, pos_bar=lam_x)
+            c = ctx.segments[j]
+            if c > 0:
+                s0 = s1 - c
+                kkd_reverse_adjoint(x, v, lam_x, lam_v, t.kicks[s0:s1], t.drifts[s0:s1],
+                                    pots=None if pots is None else pots[s0:s1])
+                s1 = s0
+        ctx.pots = None
+        return lam_x, lam_v, None, None, None
+
+
 class PowerSpectrum(torch.autograd.Function):
     """density -> P(k) in the kept bins (FP64), the jax-fli `power` estimator."""
 

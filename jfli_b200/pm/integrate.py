@@ -186,12 +186,18 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
     tgt = interp.painting.target if interp.painting is not None else "particles"
     ts_arr = np.atleast_1d(np.asarray(ts))
     efficient = isinstance(solver, EfficientDriftDoubleKick)
-    if not ((efficient or isinstance(solver, ReversibleDoubleKickDrift)) and isinstance(solver.pgd_kernel, NoCorrection)
-            and isinstance(interp, NoInterp) and tgt == "density" and ts_arr.size == 1
-            and _scalar_weight(interp.painting.weights) == 1.0):
+    solver_ok = (efficient or isinstance(solver, ReversibleDoubleKickDrift)) and isinstance(solver.pgd_kernel,
+                                                                                            NoCorrection)
+    pt = interp.painting
+    shells_ok = (solver_ok and isinstance(interp, NoInterp) and tgt == "spherical" and pt.scheme in ("ngp", "bilinear")
+                 and pt.paint_nside is None and isinstance(pt.weights, (type(None), int, float))
+                 and bool(np.all(np.diff(ts_arr) > 0)))
+    if not shells_ok and not (solver_ok and isinstance(interp, NoInterp) and tgt == "density" and ts_arr.size == 1
+                              and _scalar_weight(interp.painting.weights) == 1.0):
         raise NotImplementedError(
             "gradients run through the reversible adjoint: ReversibleDoubleKickDrift or EfficientDriftDoubleKick "
-            "with NoCorrection and a NoInterp density snapshot at one time")
+            "with NoCorrection and NoInterp, painting a density snapshot at one time or HEALPix shells (ngp or "
+            "bilinear) at increasing times")
     if dx.unit != PositionUnit.GRID_RELATIVE:
         raise NotImplementedError("differentiable integration takes GRID_RELATIVE displacements")
     steps = [(e[1], e[2]) for e in time_events(t0, ts, dt0, dtype) if e[0] == "step"]
@@ -205,6 +211,8 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
         kicks, drifts = np.array([c.kick for c in cs]), np.array([c.drift for c in cs])
     tables = ForwardTables(ktab=None, ptab=None, lpt=None, kicks=np.asarray(kicks, np.float64),
                            drifts=np.asarray(drifts, np.float64))
+    if shells_ok:
+        return _run_differentiable_shells(interp, dx, p, t0, ts, dt0, dtype, tables)
     rho = ReversibleNBody.apply(dx.array.contiguous(), p.array.contiguous(), None, tables)
     from ..fields import DensityField, FieldStatus
 
@@ -214,6 +222,41 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
     snap = snap.replace(scale_factors=t_target, comoving_centers=float(interp.r_centers[state.interp_state.shell_idx]),
                         density_width=float(interp.density_widths[state.interp_state.shell_idx]))
     return RunResult(snapshots=[snap], disp=None, vel=None, steps=len(steps))
+
+
+def _run_differentiable_shells(interp, dx: ParticleField, p: ParticleField, t0: float, ts, dt0: float, dtype,
+                               tables) -> RunResult:
+    """NoInterp HEALPix shells along the loop as one autograd node (adjoint.ReversibleNBodyShells):
+    shell i is painted at the i-th snapshot time from the positions there, with the geometry
+    and normalisation of the fused loop's shells (NoInterp.paint -> paint_spherical)."""
+    from ..painting import shell_volume_per_pixel
+    from .adjoint import ReversibleNBodyShells
+    from .interp import _spherical_result
+
+    events = time_events(t0, ts, dt0, dtype)
+    segments, count = [], 0
+    for ev in events:
+        if ev[0] == "step":
+            count += 1
+        else:
+            segments.append(count)
+            count = 0
+    nshell = len(segments)
+    rc = np.asarray(interp.r_centers, np.float64)[:nshell]
+    wd = np.asarray(interp.density_widths, np.float64)[:nshell]
+    rmin, rmax = rc - wd / 2.0, rc + wd / 2.0
+    ws = _scalar_weight(interp.painting.weights)
+    vol = np.array([shell_volume_per_pixel(dx.nside, a, b) for a, b in zip(rmin, rmax)])
+    scale = np.where(vol > 0, ws / np.where(vol > 0, vol, 1.0), ws)
+    geom = (int(dx.nside), tuple(dx.box_size), tuple(dx.observer_position_mpc), rmin, rmax, scale,
+            interp.painting.scheme)
+    maps = ReversibleNBodyShells.apply(dx.array.contiguous(), p.array.contiguous(), tables, segments, geom)
+    template = dx.replace(array=dx.array.detach()).paint_spherical(center=rc[0], density_plane_width=wd[0],
+                                                                   scheme=interp.painting.scheme)
+    saves = [ev for ev in events if ev[0] == "save"]
+    snaps = [_spherical_result(template.replace(array=maps[j]), float(saves[j][2]), float(rc[j]), float(wd[j]))
+             for j in range(nshell)]
+    return RunResult(snapshots=snaps, disp=None, vel=None, steps=int(sum(segments)))
 
 
 def run_stepwise(solver, dx, p, cosmo, ts, t0, dt0, dtype=np.float32) -> RunResult:

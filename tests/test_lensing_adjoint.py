@@ -202,3 +202,73 @@ def test_lensing_loss_gradient_matches_oracle_fd():
           f"vs oracle central difference {fd:.6e}")
     assert _rel(float(loss), oracle_loss(d64)) < 1e-4
     assert _rel(g_dir, fd) < 1e-4
+
+
+def test_nbody_shells_gradient_matches_oracle_fd():
+    """nbody(EfficientDriftDoubleKick, NoInterp spherical shells, nb_shells=3) on displacements
+    and momenta that require grad: the shells equal the fused loop's, and the directional
+    derivative of a linear loss of the shells matches central differences of an FP64 oracle
+    loop (oracle/pm.py forces, FastPM steps, oracle/healpix.py painting at each snapshot)."""
+    import jfli_b200 as jf
+    from jfli_b200.painting import shell_volume_per_pixel
+    from jfli_b200.pm.integrate import time_events
+    from jfli_b200.pm.solvers import EfficientDriftDoubleKick as EDK
+
+    n, box, nside, t0, t1, dt0 = 32, 200.0, 16, 0.1, 1.0, 0.15
+    cosmo = jf.Planck18()
+    ic = jf.interpolate_initial_conditions(jf.white_noise(41, (n,) * 3), (n,) * 3, (box,) * 3, cosmo=cosmo,
+                                           nside=nside)
+    dx, p = jf.lpt(cosmo, ic, ts=t0, order=2)
+    x0, v0 = dx.array.detach().contiguous().clone(), p.array.detach().contiguous().clone()
+    solver = jf.EfficientDriftDoubleKick(interp_kernel=jf.NoInterp(painting=jf.PaintingOptions(target="spherical")))
+    kw = dict(t0=t0, t1=t1, dt0=dt0, nb_shells=3, solver=solver)
+    xg, vg = x0.clone().requires_grad_(True), v0.clone().requires_grad_(True)
+    lc = jf.nbody(cosmo, dx.replace(array=xg), p.replace(array=vg), **kw)
+    rng = np.random.default_rng(42)
+    b = rng.standard_normal(tuple(lc.array.shape))
+    r = rng.standard_normal((n, n, n, 3))
+    s = rng.standard_normal((n, n, n, 3))
+    loss = (lc.array.double() * torch.as_tensor(b, device="cuda")).sum()
+    loss.backward()
+    g_dir = float(np.sum(xg.grad.cpu().numpy() * r) + np.sum(vg.grad.cpu().numpy() * s))
+    with torch.no_grad():
+        lc_f = jf.nbody(cosmo, dx.replace(array=x0), p.replace(array=v0), **kw)
+    e_fwd = float((lc.array.detach() - lc_f.array).norm() / lc_f.array.norm())
+
+    # the oracle loop on the same schedule (snapshot times ascending, as the loop meets them)
+    ts = np.asarray(lc.scale_factors, np.float64)[::-1]
+    rc = np.asarray(lc.comoving_centers, np.float64)[::-1]
+    wd = np.asarray(lc.density_width, np.float64)[::-1]
+    events = time_events(t0, ts, dt0)
+    steps = [(e[1], e[2]) for e in events if e[0] == "step"]
+    kicks, drifts = EDK.schedule_arrays(cosmo, [q for q, _ in steps], [q for _, q in steps], dt0)
+    k_init = EDK.init_kick(cosmo, t0, t0 + dt0)
+    g = opm.grid((n, n, n), np.float64)
+    obs = np.asarray(dx.observer_position_mpc, np.float64)
+
+    def oracle_shells(x, v):
+        x, v = x.copy(), v.copy()
+        v += opm.pm_forces(x, np.float64) * k_init
+        maps, si = [], 0
+        for ev in events:
+            if ev[0] == "step":
+                x += v * drifts[si]
+                v += opm.pm_forces(x, np.float64) * kicks[si]
+                si += 1
+            else:
+                i = ev[1]
+                lo, hi = rc[i] - wd[i] / 2, rc[i] + wd[i] / 2
+                m = oh.paint_shell(((g + x) * (box / n)).reshape(-1, 3), obs, lo, hi, nside, "bilinear")
+                maps.append(m / shell_volume_per_pixel(nside, lo, hi))
+        return np.stack(maps[::-1])  # near -> far, as nbody returns them
+
+    x64, v64 = x0.cpu().numpy().astype(np.float64), v0.cpu().numpy().astype(np.float64)
+    eps = 1e-6
+    fd = (np.sum(b * oracle_shells(x64 + eps * r, v64 + eps * s))
+          - np.sum(b * oracle_shells(x64 - eps * r, v64 - eps * s))) / (2 * eps)
+    L0 = float(np.sum(b * oracle_shells(x64, v64)))
+    print(f"nbody shells: vs the fused loop {e_fwd:.2e}; loss GPU {float(loss):.8e} oracle {L0:.8e}; directional "
+          f"derivative {g_dir:.6e} vs oracle central difference {fd:.6e}")
+    assert e_fwd < 1e-5
+    assert _rel(float(loss), L0) < 1e-3
+    assert _rel(g_dir, fd) < 1e-3
