@@ -25,8 +25,8 @@ def _pk_tables(cosmo, pk_fn, n_table: int, mesh_size, box_size):
         kmin = 2 * np.pi / max(box_size) * 0.99
         k = np.concatenate([[0.0], np.logspace(np.log10(kmin), np.log10(kmax), 4096)])
         pk = np.asarray(pk_fn(k), dtype=np.float64)
-    kt = torch.as_tensor(np.asarray(k, np.float32), device="cuda")
-    pt = torch.as_tensor(np.asarray(pk, np.float32), device="cuda")
+    kt = ops.device_table(k)
+    pt = ops.device_table(pk)
     return kt, pt
 
 

@@ -11,6 +11,7 @@ fills the ones given. Shapes:
 
 from __future__ import annotations
 
+import collections
 import ctypes
 import math
 
@@ -34,6 +35,29 @@ def workspace(nbytes: int, key: str = "default", device=None) -> torch.Tensor:
         buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)
         _workspaces[k] = buf
     return buf
+
+
+_TABLES: "collections.OrderedDict[tuple, torch.Tensor]" = collections.OrderedDict()
+
+
+def device_table(values, device="cuda", dtype=np.float32) -> torch.Tensor:
+    """A small host table (bin edges, P(k) samples) on the device, cached by content and
+    read-only for callers. A copy from pageable host memory makes the host wait until the
+    stream has drained, which stalls a caller that enqueues the next request while the GPU
+    works on this one: a table met before is reused, a new one goes up through pinned
+    memory without blocking."""
+    a = np.ascontiguousarray(np.asarray(values, dtype=dtype))
+    dev = torch.device(device)
+    key = (a.tobytes(), a.shape, a.dtype.str, str(dev))
+    t = _TABLES.get(key)
+    if t is None:
+        t = torch.from_numpy(a.copy()).pin_memory().to(dev, non_blocking=True)
+        _TABLES[key] = t
+        if len(_TABLES) > 64:
+            _TABLES.popitem(last=False)
+    else:
+        _TABLES.move_to_end(key)
+    return t
 
 
 def release_workspaces():

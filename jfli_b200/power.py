@@ -29,7 +29,7 @@ def default_kedges(mesh_shape, box_shape) -> np.ndarray:
 
 
 def power_sums(mesh: torch.Tensor, box_shape, kedges) -> torch.Tensor:
-    ke = torch.as_tensor(np.asarray(kedges, dtype=np.float32), device=mesh.device)
+    ke = ops.device_table(kedges, mesh.device)
     return ops.power_sums(mesh.contiguous(), ke, box_shape)
 
 
@@ -53,7 +53,7 @@ def power_poles(mesh: torch.Tensor, mesh2, box_shape, kedges, poles, los):
     mesh_shape = tuple(int(v) for v in mesh.shape[-3:])
     lead = tuple(mesh.shape[:-3])
     batch = int(np.prod(lead)) if lead else 1
-    edges = torch.as_tensor(np.asarray(kedges, np.float32), device=mesh.device)
+    edges = ops.device_table(kedges, mesh.device)
     ells = np.ascontiguousarray(np.asarray(poles, dtype=np.int32))
     nell, nedges = int(ells.size), int(edges.numel())
     nb = ops.query("jfli_power_poles_workspace_bytes", *mesh_shape, batch, nedges, nell, int(mesh2 is not None))
