@@ -51,7 +51,8 @@ def device_table(values, device="cuda", dtype=np.float32) -> torch.Tensor:
     key = (a.tobytes(), a.shape, a.dtype.str, str(dev))
     t = _TABLES.get(key)
     if t is None:
-        t = torch.from_numpy(a.copy()).pin_memory().to(dev, non_blocking=True)
+        t = torch.from_numpy(a.copy())
+        t = t.pin_memory().to(dev, non_blocking=True) if dev.type == "cuda" else t.to(dev)
         _TABLES[key] = t
         if len(_TABLES) > 64:
             _TABLES.popitem(last=False)
