@@ -139,6 +139,38 @@ def test_stored_potentials_match_recomputed_sweep():
     assert e_x < 1e-4
 
 
+@pytest.mark.parametrize("shape,batch", [((32, 48, 64), 1), ((24, 36, 32), 1), ((32, 32, 32), 2)])
+def test_stored_sweep_shapes_and_batch(shape, batch):
+    """The stored-potential loop and sweep on non-cubic meshes (the brick walk of the
+    cotangent paint where ny % 8 == 0 and nz % 32 == 0, the grid-stride walk otherwise) and
+    with two particle sets at once, against the recomputing sweep."""
+    from jfli_b200 import ops
+
+    rng = np.random.default_rng(sum(shape) + batch)
+    lead = (batch,) if batch > 1 else ()
+    x0 = _dev(0.7 * rng.standard_normal(lead + shape + (3,)))
+    v0 = _dev(0.2 * rng.standard_normal(lead + shape + (3,)))
+    a, b = _dev(rng.standard_normal(lead + shape + (3,))), _dev(rng.standard_normal(lead + shape + (3,)))
+    kicks, drifts = np.linspace(0.2, 0.3, 5), np.linspace(0.4, 0.3, 5)
+    out = {}
+    for mode in ("recompute", "stored"):
+        x, v = x0.clone(), v0.clone()
+        rho = torch.empty(lead + shape, device="cuda")
+        pots = torch.empty((len(kicks),) + lead + shape, device="cuda") if mode == "stored" else None
+        ops.kkd_run(x, v, kicks, drifts, rho, pots=pots)
+        fwd = rho.clone()
+        lx, lv = a.clone(), b.clone()
+        sens = ops.kkd_adjoint(x, v, lx, lv, kicks, drifts, pots=pots)
+        out[mode] = (fwd, lx, lv, sens, x)
+    (r0, lx0, lv0, s0, xr0), (r1, lx1, lv1, s1, xr1) = out["recompute"], out["stored"]
+    e_rho = float((r1 - r0).norm() / r0.norm())
+    e_lx = float((lx1 - lx0).norm() / lx0.norm())
+    e_s = float((s1 - s0).abs().max() / s0.abs().max())
+    e_x = float((xr1 - x0).abs().max())
+    print(f"{shape} x{batch}: density {e_rho:.2e}, lam_x {e_lx:.2e}, sensitivities {e_s:.2e}, initial state {e_x:.2e}")
+    assert e_rho < 1e-5 and e_lx < 1e-3 and e_s < 1e-3 and e_x < 1e-4
+
+
 def test_kkd_step_vjp_stored_matches_oracle_fd():
     from jfli_b200 import ops
 
