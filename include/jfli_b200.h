@@ -282,6 +282,21 @@ int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, cons
                              const float* ga, const float* g, int n_g, const float* da, const float* dgfa, int n_d,
                              int nside, int scheme, float* map, int accumulate, int nx, int ny, int nz, int batch,
                              char* err, size_t errlen);
+/* Adjoint of jfli_healpix_paint_tiled (its `_bwd`; ngp or bilinear): for the cotangent
+ * map_bar[batch][12 nside^2] of the shell, each painted copy q' = q + D(r) M v (q = M c + s,
+ * r = |q| or, telephoto, |q - o|) passes back the painter's g = dL/dq' (as
+ * jfli_healpix_paint_shells_adjoint) as dL/dc += M^T (g + D'(r) (M v . g) dr/dq) and
+ * dL/dv += D M^T g, D' the derivative of the interpolated drift tables (zero where the
+ * growth is clipped). Adds to disp_bar (particle grid layout), vel_bar (with vel) and
+ * weights_bar (when not NULL). The other arguments as jfli_healpix_paint_tiled. */
+int jfli_healpix_paint_tiled_adjoint(void* stream, const float* disp, int absolute, const float* vel,
+                                     const float* weights, float weight, float lx, float ly, float lz, float ox,
+                                     float oy, float oz, int ntiles, const signed char* rotations, const float* shifts,
+                                     int telephoto, float rmin, float rmax, float t, float gp_t, float dbound,
+                                     const float* chi, const float* a_chi, int n_chi, const float* ga, const float* g,
+                                     int n_g, const float* da, const float* dgfa, int n_d, int nside, int scheme,
+                                     const float* map_bar, float* disp_bar, float* vel_bar, float* weights_bar,
+                                     int nx, int ny, int nz, int batch, char* err, size_t errlen);
 
 /* Positions (Mpc/h, particle layout) of one replica of the particles: rotation (host,
  * row-major signed permutation matrix) and shift (host, Mpc/h) applied to x - observer, and

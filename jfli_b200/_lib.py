@@ -120,6 +120,13 @@ _SIGNATURES = {
          c_float, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_int, c_int,
          c_void_p, c_int, *_DIMS, *_ERR],
     ),
+    "jfli_healpix_paint_tiled_adjoint": (
+        c_int,
+        [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float, c_float,
+         c_int, ctypes.POINTER(ctypes.c_byte), ctypes.POINTER(c_float), c_int, c_float, c_float, c_float, c_float,
+         c_float, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_int, c_int,
+         c_void_p, c_void_p, c_void_p, c_void_p, *_DIMS, *_ERR],
+    ),
     "jfli_lightcone_drift": (
         c_int,
         [c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_float, c_float, c_float, c_float, c_float, c_float,

@@ -677,16 +677,11 @@ int jfli_healpix_paint_rbf(void* stream, const float* disp, int absolute, const 
       errlen, "jfli_healpix_paint_rbf");
 }
 
-int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, const float* vel, const float* weights,
-                             float weight, float lx, float ly, float lz, float ox, float oy, float oz, int ntiles,
-                             const signed char* rotations, const float* shifts, int telephoto, float rmin, float rmax,
-                             float t, float gp_t, float dbound, const float* chi, const float* a_chi, int n_chi,
-                             const float* ga, const float* g, int n_g, const float* da, const float* dgfa, int n_d,
-                             int nside, int scheme, float* map, int accumulate, int nx, int ny, int nz, int batch,
-                             char* err, size_t errlen) {
-  CHECK_DIMS(nx, ny, nz, batch);
-  CHECK_PTR(disp);
-  CHECK_PTR(map);
+// Arguments of the replica painter and its adjoint (0 when valid).
+static int tiled_args_check(const float* vel, float lx, float ly, float lz, int ntiles, const signed char* rotations,
+                            const float* shifts, float t, float dbound, const float* chi, const float* a_chi,
+                            int n_chi, const float* ga, const float* g, int n_g, const float* da, const float* dgfa,
+                            int n_d, int nside, int scheme, char* err, size_t errlen) {
   CHECK_PTR(rotations);
   CHECK_PTR(shifts);
   if (nside < 1 || nside > 8192) return fail(err, errlen, JFLI_EINVAL, "nside %d outside [1, 8192]", nside);
@@ -723,6 +718,26 @@ int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, cons
     if (!(t > 0)) return fail(err, errlen, JFLI_EINVAL, "scale factor must be positive");
     if (!(dbound >= 0) || !isfinite(dbound)) return fail(err, errlen, JFLI_EINVAL, "drift bound must be finite, >= 0");
   }
+  if (nside < 1 || nside > 8192) return fail(err, errlen, JFLI_EINVAL, "nside %d outside [1, 8192]", nside);
+  if (scheme != JFLI_HEALPIX_NGP && scheme != JFLI_HEALPIX_BILINEAR)
+    return fail(err, errlen, JFLI_EUNSUPPORTED, "HEALPix scheme %d not supported (0 = ngp, 1 = bilinear)", scheme);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  return 0;
+}
+
+int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, const float* vel, const float* weights,
+                             float weight, float lx, float ly, float lz, float ox, float oy, float oz, int ntiles,
+                             const signed char* rotations, const float* shifts, int telephoto, float rmin, float rmax,
+                             float t, float gp_t, float dbound, const float* chi, const float* a_chi, int n_chi,
+                             const float* ga, const float* g, int n_g, const float* da, const float* dgfa, int n_d,
+                             int nside, int scheme, float* map, int accumulate, int nx, int ny, int nz, int batch,
+                             char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(map);
+  if (int rc = tiled_args_check(vel, lx, ly, lz, ntiles, rotations, shifts, t, dbound, chi, a_chi, n_chi, ga, g,
+                                n_g, da, dgfa, n_d, nside, scheme, err, errlen))
+    return rc;
   const MeshDims d{nx, ny, nz, batch};
   cudaStream_t s = (cudaStream_t)stream;
   if (!accumulate) {
@@ -736,6 +751,32 @@ int jfli_healpix_paint_tiled(void* stream, const float* disp, int absolute, cons
                                                shifts, telephoto, rmin, rmax, t, gp_t, dbound, tb, nside, scheme, map,
                                                s),
                      err, errlen, "jfli_healpix_paint_tiled");
+}
+
+int jfli_healpix_paint_tiled_adjoint(void* stream, const float* disp, int absolute, const float* vel,
+                                     const float* weights, float weight, float lx, float ly, float lz, float ox,
+                                     float oy, float oz, int ntiles, const signed char* rotations, const float* shifts,
+                                     int telephoto, float rmin, float rmax, float t, float gp_t, float dbound,
+                                     const float* chi, const float* a_chi, int n_chi, const float* ga, const float* g,
+                                     int n_g, const float* da, const float* dgfa, int n_d, int nside, int scheme,
+                                     const float* map_bar, float* disp_bar, float* vel_bar, float* weights_bar,
+                                     int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(map_bar);
+  CHECK_PTR(disp_bar);
+  if (int rc = tiled_args_check(vel, lx, ly, lz, ntiles, rotations, shifts, t, dbound, chi, a_chi, n_chi, ga, g,
+                                n_g, da, dgfa, n_d, nside, scheme, err, errlen))
+    return rc;
+  const MeshDims d{nx, ny, nz, batch};
+  const float box[3] = {lx, ly, lz};
+  const float obs[3] = {ox, oy, oz};
+  const jfli::DriftTables tb{chi, a_chi, n_chi, ga, g, n_g, da, dgfa, n_d};
+  return cuda_status(jfli::healpix_paint_tiled_adjoint(disp, absolute, vel, weights, weight, d, box, obs, ntiles,
+                                                       rotations, shifts, telephoto, rmin, rmax, t, gp_t, dbound, tb,
+                                                       nside, scheme, map_bar, disp_bar, vel ? vel_bar : nullptr,
+                                                       weights_bar, (cudaStream_t)stream),
+                     err, errlen, "jfli_healpix_paint_tiled_adjoint");
 }
 
 int jfli_replica_positions(void* stream, const float* disp, int absolute, const float* vel, float lx, float ly,

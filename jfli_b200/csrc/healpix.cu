@@ -559,6 +559,155 @@ __global__ void __launch_bounds__(256, 4)
   }
 }
 
+// Adjoint of k_healpix_paint_tiled (ngp or bilinear) for one shell's map cotangent
+// map_bar. Each painted copy q' = q + D(r) u (q = M c + s, u = M v, r = |q| onion or
+// |q - o| telephoto, D the light-cone drift factor of interpolated tables) passes back
+// g = dL/dq' from the painter (as k_healpix_paint_shells_adjoint), and
+//   dL/dq = g + D'(r) (u . g) dr/dq,   dL/dc += M^T dL/dq,   dL/dv += D M^T g,
+// D'(r) chaining the slopes of the tables' segments (a(chi), Gp(a) unless clipped,
+// dGfa(sqrt(t a))). The cull and the FP64 placement are the forward's; shell edges pass
+// nothing back. Accumulates into disp_bar, vel_bar and weights_bar (each may be null but
+// disp_bar).
+__global__ void k_healpix_paint_tiled_adjoint(const float* __restrict__ disp, int absolute,
+                                              const float* __restrict__ vel, const float* __restrict__ weights,
+                                              float weight, PGrid g, float3 box, float3 obs, TileSet ts,
+                                              int telephoto, float rmin, float rmax, float t, float gp_t,
+                                              float dbound, DriftTables tb, int nside, int scheme,
+                                              const double* __restrict__ theta_tab,
+                                              const float* __restrict__ map_bar, float* __restrict__ disp_bar,
+                                              float* __restrict__ vel_bar, float* __restrict__ weights_bar) {
+  const long long b = blockIdx.y;
+  const long long npix = 12LL * nside * nside;
+  disp += b * g.np * 3;
+  disp_bar += b * g.np * 3;
+  if (vel) vel += b * g.np * 3;
+  if (vel_bar) vel_bar += b * g.np * 3;
+  if (weights) weights += b * g.np;
+  if (weights_bar) weights_bar += b * g.np;
+  map_bar += b * npix;
+  const float nx = (float)g.nx, ny = (float)g.ny, nz = (float)g.nz;
+  float cm2 = 0.f;
+  if (vel) {
+    const float onorm = sqrtf(obs.x * obs.x + obs.y * obs.y + obs.z * obs.z);
+    const float cm = tb.chi[tb.n_chi - 1] * (1.f - 1e-5f) - 0.01f - (telephoto ? onorm : 0.f);
+    cm2 = cm > 0.f ? cm * cm * (1.f - 1e-6f) : -1.f;
+  }
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    const float d0 = disp[3 * p + 0], d1 = disp[3 * p + 1], d2 = disp[3 * p + 2];
+    int i = 0, j = 0, k = 0;
+    if (!absolute) particle_ijk(g, p, i, j, k);
+    const float c[3] = {((float)i + d0) / nx * box.x - obs.x, ((float)j + d1) / ny * box.y - obs.y,
+                        ((float)k + d2) / nz * box.z - obs.z};
+    float v[3] = {0.f, 0.f, 0.f}, vmag = 0.f;
+    if (vel) {
+      v[0] = vel[3 * p + 0];
+      v[1] = vel[3 * p + 1];
+      v[2] = vel[3 * p + 2];
+      vmag = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    }
+    const double wp = weights ? (double)weights[p] * (double)weight : (double)weight;
+    const float dv = dbound * vmag;
+    const float lo = (rmin - dv - 4e-3f) / (1.f + 4e-6f), hi = (rmax + dv + 4e-3f) / (1.f - 4e-6f);
+    const float lo2 = lo > 0.f ? lo * lo * (1.f - 1e-6f) : -1.f, hi2 = hi * hi * (1.f + 1e-6f);
+    double gc[3] = {0.0, 0.0, 0.0}, gvel[3] = {0.0, 0.0, 0.0}, gw = 0.0;
+    for (int tile = 0; tile < ts.n; ++tile) {
+      const signed char* M = ts.m[tile];
+      float q[3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        q[r] = (float)M[3 * r + 0] * c[0] + (float)M[3 * r + 1] * c[1] + (float)M[3 * r + 2] * c[2] + ts.shift[tile][r];
+      const float qn2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+      if ((!vel || qn2 <= cm2) && (qn2 <= lo2 || qn2 > hi2)) continue;
+      const double cd[3] = {((double)i + (double)d0) / nx * box.x - obs.x, ((double)j + (double)d1) / ny * box.y - obs.y,
+                            ((double)k + (double)d2) / nz * box.z - obs.z};
+      double qd[3], u[3] = {0.0, 0.0, 0.0}, dr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        qd[r] = (double)M[3 * r + 0] * cd[0] + (double)M[3 * r + 1] * cd[1] + (double)M[3 * r + 2] * cd[2] +
+                (double)ts.shift[tile][r];
+      double D = 0.0, dD = 0.0;
+      if (vel) {
+        double e[3] = {qd[0], qd[1], qd[2]};
+        if (telephoto) {
+          e[0] -= obs.x;
+          e[1] -= obs.y;
+          e[2] -= obs.z;
+        }
+        const double dist = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        float s_a, s_g, s_d;
+        const float at = interp_table_d((float)dist, tb.chi, tb.a_chi, tb.n_chi, s_a);
+        const float ac = sqrtf(t * at);
+        const float graw = interp_table_d(at, tb.ga, tb.g, tb.n_g, s_g);
+        const float gp_at = fminf(fmaxf(graw, 0.f), 1.f);
+        const float dgv = interp_table_d(ac, tb.da, tb.dgfa, tb.n_d, s_d);
+        const float drift = (gp_at - gp_t) / dgv;
+        D = (double)drift;
+        const double dgp = (graw > 0.f && graw < 1.f) ? (double)s_g : 0.0;
+        const double dac = ac > 0.f ? (double)t / (2.0 * (double)ac) : 0.0;
+        dD = (double)s_a * (dgp * dgv - ((double)gp_at - gp_t) * (double)s_d * dac) / ((double)dgv * dgv);
+        if (dist > 0.0) {
+#pragma unroll
+          for (int r = 0; r < 3; ++r) dr[r] = e[r] / dist;
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          u[r] = (double)M[3 * r + 0] * v[0] + (double)M[3 * r + 1] * v[1] + (double)M[3 * r + 2] * v[2];
+          qd[r] += (double)(drift * (float)u[r]);
+        }
+      }
+      const double rr = sqrt(qd[0] * qd[0] + qd[1] * qd[1] + qd[2] * qd[2]);
+      if (!(rr > (double)rmin && rr <= (double)rmax)) continue;
+      // the painter's adjoint at the painted vector qd
+      const double zc = qd[2] / rr, phi = atan2(qd[1], qd[0]);
+      long long pix[4] = {-1, -1, -1, -1};
+      double w[4] = {0.0, 0.0, 0.0, 0.0}, dth[4] = {0.0, 0.0, 0.0, 0.0}, dph[4] = {0.0, 0.0, 0.0, 0.0};
+      if (scheme == 0) {
+        pix[0] = ang2pix_ring(zc, phi, nside);
+        w[0] = 1.0;
+      } else {
+        interp_weights_grad(acos(fmin(1.0, fmax(-1.0, zc))), phi, nside, theta_tab, pix, w, dth, dph);
+      }
+      double g_th = 0.0, g_ph = 0.0, g_s = 0.0;
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq) {
+        if (pix[qq] < 0 || pix[qq] >= npix) continue;
+        const double m = (double)__ldg(map_bar + pix[qq]);
+        g_th += m * dth[qq];
+        g_ph += m * dph[qq];
+        g_s += m * w[qq];
+      }
+      gw += (double)weight * g_s;
+      if (scheme == 0) continue;
+      const double s2 = qd[0] * qd[0] + qd[1] * qd[1];
+      if (!(s2 > 0.0)) continue;
+      const double sxy = sqrt(s2), r2 = rr * rr;
+      double gq[3] = {wp * (g_th * qd[2] * qd[0] / (r2 * sxy) - g_ph * qd[1] / s2),
+                      wp * (g_th * qd[2] * qd[1] / (r2 * sxy) + g_ph * qd[0] / s2), wp * (-g_th * sxy / r2)};
+      if (vel) {
+        const double ug = u[0] * gq[0] + u[1] * gq[1] + u[2] * gq[2];
+        // dL/dv += D M^T g  (before g gains the drift's distance term)
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+          gvel[r] += D * ((double)M[0 * 3 + r] * gq[0] + (double)M[1 * 3 + r] * gq[1] + (double)M[2 * 3 + r] * gq[2]);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) gq[r] += dD * ug * dr[r];
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        gc[r] += (double)M[0 * 3 + r] * gq[0] + (double)M[1 * 3 + r] * gq[1] + (double)M[2 * 3 + r] * gq[2];
+    }
+    if (weights_bar) weights_bar[p] += (float)gw;
+    disp_bar[3 * p + 0] += (float)(gc[0] * box.x / nx);
+    disp_bar[3 * p + 1] += (float)(gc[1] * box.y / ny);
+    disp_bar[3 * p + 2] += (float)(gc[2] * box.z / nz);
+    if (vel && vel_bar) {
+      vel_bar[3 * p + 0] += (float)gvel[0];
+      vel_bar[3 * p + 1] += (float)gvel[1];
+      vel_bar[3 * p + 2] += (float)gvel[2];
+    }
+  }
+}
+
 // Positions (Mpc/h) of one rotated, shifted replica, drifted to the light cone when vel is
 // given, with the same conventions as k_healpix_paint_tiled (TelephotoInterp's flat planes
 // beyond the box paint these with the flat-sky painter, pm/interp.py:643-699).
@@ -748,6 +897,28 @@ cudaError_t healpix_paint_shells_adjoint(const float* disp, int absolute, const 
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+cudaError_t healpix_paint_tiled_adjoint(const float* disp, int absolute, const float* vel, const float* weights,
+                                        float weight, const MeshDims& d, const float* box, const float* observer,
+                                        int ntiles, const signed char* rotations, const float* shifts, int telephoto,
+                                        float rmin, float rmax, float t, float gp_t, float dbound,
+                                        const DriftTables& tb, int nside, int scheme, const float* map_bar,
+                                        float* disp_bar, float* vel_bar, float* weights_bar, cudaStream_t s) {
+  TileSet ts;
+  ts.n = ntiles;
+  for (int i = 0; i < ntiles; ++i) {
+    for (int e = 0; e < 9; ++e) ts.m[i][e] = rotations[9 * i + e];
+    for (int e = 0; e < 3; ++e) ts.shift[i][e] = shifts[3 * i + e];
+  }
+  const double* tab = ring_theta_table(nside);
+  if (!tab) return cudaErrorMemoryAllocation;
+  k_healpix_paint_tiled_adjoint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(
+      disp, absolute, vel, weights, weight, make_pgrid(d), make_float3(box[0], box[1], box[2]),
+      make_float3(observer[0], observer[1], observer[2]), ts, telephoto, rmin, rmax, t, gp_t, dbound, tb, nside, scheme,
+      tab, map_bar, disp_bar, vel_bar, weights_bar);
+  note_launch();
+  return cudaGetLastError();
 }
 
 cudaError_t healpix_paint_tiled(const float* disp, int absolute, const float* vel, const float* weights, float weight,

@@ -185,6 +185,14 @@ cudaError_t healpix_paint_tiled(const float* disp, int absolute, const float* ve
                                 const signed char* rotations, const float* shifts, int telephoto, float rmin,
                                 float rmax, float t, float gp_t, float dbound, const DriftTables& tb, int nside,
                                 int scheme, float* map, cudaStream_t s);
+// Adjoint of healpix_paint_tiled (one shell's map cotangent): accumulates into disp_bar and,
+// when non-null, vel_bar and weights_bar.
+cudaError_t healpix_paint_tiled_adjoint(const float* disp, int absolute, const float* vel, const float* weights,
+                                        float weight, const MeshDims& d, const float* box, const float* observer,
+                                        int ntiles, const signed char* rotations, const float* shifts, int telephoto,
+                                        float rmin, float rmax, float t, float gp_t, float dbound,
+                                        const DriftTables& tb, int nside, int scheme, const float* map_bar,
+                                        float* disp_bar, float* vel_bar, float* weights_bar, cudaStream_t s);
 
 // ---- flat.cu ----
 cudaError_t paint_flat(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d, int npx,

@@ -85,6 +85,23 @@ __device__ __forceinline__ float interp_table(float x, const float* xp, const fl
   return fp[i] + (x - xp[i]) * slope;
 }
 
+// interp_table with the slope of the segment it used (the derivative of the linear
+// interpolation, end segments extrapolated as in the value).
+__device__ __forceinline__ float interp_table_d(float x, const float* xp, const float* fp, int n, float& slope) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (xp[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  int i = lo - 1;
+  i = i < 0 ? 0 : (i > n - 2 ? n - 2 : i);
+  slope = (fp[i + 1] - fp[i]) / (xp[i + 1] - xp[i]);
+  return fp[i] + (x - xp[i]) * slope;
+}
+
 // Gaussian initial conditions (reference initial.py:175-182):
 // field_k *= sqrt(P(|k|) * M / V) * norm, |k| in h/Mpc. `zero_mode_one` reproduces the
 // k = 0 guard of infer/dist.py:68.

@@ -526,6 +526,65 @@ def drift_bound(tables, t: float, gp_t: float) -> float:
     return max(gp_t, 1.0 - gp_t) / den * 1.001 + 1e-6
 
 
+def _tiled_prep(pos, rotations, shifts, scheme, vel, t, cosmo, tables, dbound):
+    """(scheme code, int8 rotations (T, 9), float32 shifts (T, 3), drift tables, t, Gp(t),
+    drift bound) for the replica painter and its adjoint."""
+    from . import cosmology as cj
+
+    sch = {"ngp": _lib.JFLI_HEALPIX_NGP, "bilinear": _lib.JFLI_HEALPIX_BILINEAR}.get(scheme)
+    if sch is None:
+        raise NotImplementedError(f"spherical painting scheme {scheme!r} is not implemented (ngp, bilinear)")
+    rot = np.ascontiguousarray(np.rint(np.asarray(rotations, np.float64)).astype(np.int8).reshape(-1, 9))
+    sh = np.ascontiguousarray(np.asarray(shifts, np.float32).reshape(-1, 3))
+    if rot.shape[0] != sh.shape[0]:
+        raise ValueError(f"{rot.shape[0]} rotations for {sh.shape[0]} shifts")
+    tabs = (None,) * 6
+    t_arg = gp_t = 0.0
+    if vel is None:
+        return sch, rot, sh, tabs, t_arg, gp_t, 0.0
+    _check(vel, "vel")
+    if vel.shape != pos.shape:
+        raise ValueError("vel must have the shape of pos")
+    if t is None or cosmo is None:
+        raise ValueError("the light-cone drift needs the time t and the cosmology")
+    tabs = drift_tables(cosmo) if tables is None else tables
+    t_arg = float(t)
+    gp_t = float(cj.Gp(cosmo, t_arg))
+    if dbound is None:
+        dbound = drift_bound(tabs, t_arg, gp_t)
+    return sch, rot, sh, tabs, t_arg, gp_t, (dbound if math.isfinite(dbound) else 1e30)
+
+
+def healpix_paint_tiled_adjoint(pos: torch.Tensor, map_bar: torch.Tensor, nside: int, box_size, observer_mpc,
+                                rmin: float, rmax: float, rotations, shifts, *, absolute: bool = False,
+                                vel: torch.Tensor | None = None, t: float | None = None, cosmo=None,
+                                telephoto: bool = False, scheme: str = "bilinear",
+                                weights: torch.Tensor | None = None, weight: float = 1.0, tables=None,
+                                dbound: float | None = None, pos_bar: torch.Tensor | None = None,
+                                vel_bar: torch.Tensor | None = None,
+                                weights_bar: torch.Tensor | None = None) -> torch.Tensor:
+    """Adjoint of healpix_paint_tiled: accumulates into pos_bar (zeros when None, returned),
+    vel_bar and weights_bar (see jfli_healpix_paint_tiled_adjoint)."""
+    _check(pos, "pos")
+    _check(map_bar, "map_bar")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    sch, rot, sh, tabs, t_arg, gp_t, dbound = _tiled_prep(pos, rotations, shifts, scheme, vel, t, cosmo, tables, dbound)
+    if tuple(map_bar.shape) != (*lead, 12 * nside * nside) or not map_bar.is_contiguous():
+        raise ValueError("map_bar must be a contiguous map per particle set")
+    if pos_bar is None:
+        pos_bar = torch.zeros_like(pos)
+    lx, ly, lz = (float(v) for v in box_size)
+    ox, oy, oz = (float(v) for v in observer_mpc)
+    chi, a_chi, ga, g, da, dg = tabs
+    n = lambda x: int(x.numel()) if x is not None else 0
+    call("jfli_healpix_paint_tiled_adjoint", stream_ptr(), ptr(pos), int(absolute), ptr(vel), ptr(weights),
+         float(weight), lx, ly, lz, ox, oy, oz, int(rot.shape[0]), rot.ctypes.data_as(ctypes.POINTER(ctypes.c_byte)),
+         sh.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(bool(telephoto)), float(rmin), float(rmax), t_arg,
+         gp_t, float(dbound), ptr(chi), ptr(a_chi), n(chi), ptr(ga), ptr(g), n(ga), ptr(da), ptr(dg), n(da),
+         int(nside), sch, ptr(map_bar), ptr(pos_bar), ptr(vel_bar), ptr(weights_bar), nx, ny, nz, batch)
+    return pos_bar
+
+
 def healpix_paint_tiled(pos: torch.Tensor, nside: int, box_size, observer_mpc, rmin: float, rmax: float, rotations,
                         shifts, *, absolute: bool = False, vel: torch.Tensor | None = None, t: float | None = None,
                         cosmo=None, telephoto: bool = False, scheme: str = "bilinear",
@@ -535,38 +594,14 @@ def healpix_paint_tiled(pos: torch.Tensor, nside: int, box_size, observer_mpc, r
     jfli_healpix_paint_tiled). rotations (T, 3, 3) signed permutation matrices, shifts
     (T, 3) in Mpc/h; with `vel` the replicas are drifted to the light cone at time t.
     `dbound` replaces the computed drift bound (a larger one only skips fewer replicas)."""
-    from . import cosmology as cj
-
     _check(pos, "pos")
     (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
-    sch = {"ngp": _lib.JFLI_HEALPIX_NGP, "bilinear": _lib.JFLI_HEALPIX_BILINEAR}.get(scheme)
-    if sch is None:
-        raise NotImplementedError(f"spherical painting scheme {scheme!r} is not implemented (ngp, bilinear)")
-    rot = np.ascontiguousarray(np.rint(np.asarray(rotations, np.float64)).astype(np.int8).reshape(-1, 9))
-    sh = np.ascontiguousarray(np.asarray(shifts, np.float32).reshape(-1, 3))
-    if rot.shape[0] != sh.shape[0]:
-        raise ValueError(f"{rot.shape[0]} rotations for {sh.shape[0]} shifts")
+    sch, rot, sh, tabs, t_arg, gp_t, dbound = _tiled_prep(pos, rotations, shifts, scheme, vel, t, cosmo, tables, dbound)
     if out is None:
         out = torch.empty(*lead, 12 * nside * nside, dtype=torch.float32, device=pos.device)
         accumulate = False
     lx, ly, lz = (float(v) for v in box_size)
     ox, oy, oz = (float(v) for v in observer_mpc)
-    tabs = (None,) * 6
-    t_arg = gp_t = 0.0
-    if vel is None:
-        dbound = 0.0
-    if vel is not None:
-        _check(vel, "vel")
-        if vel.shape != pos.shape:
-            raise ValueError("vel must have the shape of pos")
-        if t is None or cosmo is None:
-            raise ValueError("the light-cone drift needs the time t and the cosmology")
-        tabs = drift_tables(cosmo) if tables is None else tables
-        t_arg = float(t)
-        gp_t = float(cj.Gp(cosmo, t_arg))
-        if dbound is None:
-            dbound = drift_bound(tabs, t_arg, gp_t)
-        dbound = dbound if math.isfinite(dbound) else 1e30
     chi, a_chi, ga, g, da, dg = tabs
     n = lambda x: int(x.numel()) if x is not None else 0
     call("jfli_healpix_paint_tiled", stream_ptr(), ptr(pos), int(absolute), ptr(vel), ptr(weights), float(weight),

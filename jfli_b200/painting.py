@@ -123,6 +123,39 @@ def paint_shell_tiled(field, vel, center: float, width: float, rotations, shifts
     vol = shell_volume_per_pixel(field.nside, rmin, rmax)
     scale = ws / vol if vol > 0 else ws
     v = vel.contiguous() if vel is not None else None
-    return ops.healpix_paint_tiled(field.array.contiguous(), field.nside, field.box_size, field.observer_position_mpc,
-                                   rmin, rmax, rotations, shifts, absolute=absolute, vel=v, t=t, cosmo=cosmo,
-                                   telephoto=telephoto, scheme=scheme, weights=w, weight=scale)
+    pos = field.array.contiguous()
+    kw = dict(absolute=absolute, t=t, cosmo=cosmo, telephoto=telephoto, scheme=scheme, weight=scale)
+    if torch.is_grad_enabled() and (pos.requires_grad or (v is not None and v.requires_grad)):
+        if pos.dim() != 4 or w is not None:
+            raise NotImplementedError("gradients of replica painting: one particle set, scalar weights")
+        geom = (field.nside, tuple(field.box_size), tuple(field.observer_position_mpc), rmin, rmax, rotations, shifts,
+                kw)
+        return PaintShellTiled.apply(pos, v, geom)
+    return ops.healpix_paint_tiled(pos, field.nside, field.box_size, field.observer_position_mpc, rmin, rmax,
+                                   rotations, shifts, vel=v, weights=w, **kw)
+
+
+class PaintShellTiled(torch.autograd.Function):
+    """One shell of rotated, shifted (and light-cone drifted) replicas as an autograd node:
+    forward jfli_healpix_paint_tiled, backward its adjoint (position and velocity
+    cotangents)."""
+
+    @staticmethod
+    def forward(ctx, pos, vel, geom):
+        nside, box, obs, rmin, rmax, rotations, shifts, kw = geom
+        ctx.geom = geom
+        ctx.has_v = vel is not None
+        ctx.save_for_backward(pos, vel) if vel is not None else ctx.save_for_backward(pos)
+        return ops.healpix_paint_tiled(pos.detach(), nside, box, obs, rmin, rmax, rotations, shifts,
+                                       vel=None if vel is None else vel.detach(), **kw)
+
+    @staticmethod
+    def backward(ctx, map_bar):
+        nside, box, obs, rmin, rmax, rotations, shifts, kw = ctx.geom
+        saved = ctx.saved_tensors
+        pos = saved[0].detach()
+        vel = saved[1].detach() if ctx.has_v else None
+        vel_bar = torch.zeros_like(vel) if vel is not None else None
+        pos_bar = ops.healpix_paint_tiled_adjoint(pos, map_bar.contiguous(), nside, box, obs, rmin, rmax, rotations,
+                                                  shifts, vel=vel, vel_bar=vel_bar, **kw)
+        return pos_bar, vel_bar, None
