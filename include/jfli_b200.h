@@ -126,6 +126,12 @@ size_t jfli_pgd_adjoint_workspace_bytes(int nx, int ny, int nz, int batch);
 int jfli_pgd_adjoint(void* stream, const float* disp, const float* u, float alpha, float kl, float ks, float* lam_x,
                      void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
                      size_t errlen);
+/* The same VJP for the PM force itself: lam_x += scale J^T u, J = dF/dx for F the CIC
+ * readout of the FD force mesh of the Poisson potential of the particles' own density at
+ * the relative positions disp (the force the KDK and KKD steps kick with, unscaled).
+ * Workspace: jfli_pgd_adjoint_workspace_bytes. */
+int jfli_force_adjoint(void* stream, const float* disp, const float* u, float scale, float* lam_x, void* workspace,
+                       size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
 /* forces[p] = scale * CIC readout of -grad_FD(pot) at the particle positions. */
 int jfli_readout_gradient(void* stream, const float* pos, int absolute, const float* pot, float scale, float* forces,
                           int nx, int ny, int nz, int batch, char* err, size_t errlen);

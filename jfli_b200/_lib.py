@@ -174,6 +174,8 @@ _SIGNATURES = {
     "jfli_pgd_adjoint_workspace_bytes": (c_size_t, _DIMS),
     "jfli_pgd_adjoint": (
         c_int, [c_void_p, c_void_p, c_void_p, c_float, c_float, c_float, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR]),
+    "jfli_force_adjoint": (
+        c_int, [c_void_p, c_void_p, c_void_p, c_float, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR]),
     "jfli_kkd_run_stored": (
         c_int,
         [c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_float), ctypes.POINTER(c_float), c_int, c_void_p, c_void_p,

@@ -168,9 +168,12 @@ size_t jfli_pgd_adjoint_workspace_bytes(int nx, int ny, int nz, int batch) {
   return spec_bytes(d) + 4 * mesh_bytes(d) + 2 * align256(sizeof(float) * 4 * (size_t)d.cells() * d.batch);
 }
 
-int jfli_pgd_adjoint(void* stream, const float* disp, const float* u, float alpha, float kl, float ks, float* lam_x,
-                     void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
-                     size_t errlen) {
+namespace {
+// lam_x += scale J^T u, J = dF/dx for F the CIC readout of the FD force mesh of the
+// particles' own density through the Poisson operator (pgd false) or the PGD filter.
+int force_vjp(void* stream, const float* disp, const float* u, float scale, bool pgd, float kl, float ks,
+              float* lam_x, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+              size_t errlen, const char* name) {
   CHECK_DIMS(nx, ny, nz, batch);
   CHECK_STENCIL(nx, ny, nz);
   CHECK_FFT(nx, ny, nz);
@@ -179,7 +182,7 @@ int jfli_pgd_adjoint(void* stream, const float* disp, const float* u, float alph
   CHECK_PTR(lam_x);
   CHECK_PTR(workspace);
   CHECK_ALIGN16(workspace);
-  if (!(kl >= 0.0f && ks > 0.0f)) return fail(err, errlen, JFLI_EINVAL, "PGD scales need kl >= 0 and ks > 0");
+  if (pgd && !(kl >= 0.0f && ks > 0.0f)) return fail(err, errlen, JFLI_EINVAL, "PGD scales need kl >= 0 and ks > 0");
   const MeshDims d{nx, ny, nz, batch};
   const size_t need = jfli_pgd_adjoint_workspace_bytes(nx, ny, nz, batch);
   if (workspace_bytes < need)
@@ -194,18 +197,36 @@ int jfli_pgd_adjoint(void* stream, const float* disp, const float* u, float alph
   float* force = (float*)(w + spec_bytes(d) + 4 * mesh_bytes(d));
   float* ubar = force + 4 * (size_t)d.cells() * d.batch;
   float* x = const_cast<float*>(disp);  // painted only: the pass writes no particle array
-  // the PGD force mesh at x, as PGDKernel.apply builds it
+  // the force mesh at x, as the forward builds it
   cudaError_t e = jfli::zero_floats(rho, d.cells() * batch, s);
   if (e == cudaSuccess) e = jfli::kick_drift_paint(x, x, nullptr, 0.f, 0.f, JFLI_STEP_PAINT, 1.0f, rho, d, s);
-  if (e == cudaSuccess) e = jfli::pgd_potential(rho, spec, pot, d, 1.0f, kl, ks, 1.0f, s);
+  if (e == cudaSuccess)
+    e = pgd ? jfli::pgd_potential(rho, spec, pot, d, 1.0f, kl, ks, 1.0f, s)
+            : jfli::poisson_potential(rho, spec, pot, d, 1.0f, 1.0f, s);
   if (e == cudaSuccess) e = jfli::force_mesh(pot, force, 1.0f, d, s);
-  // rho_bar = P_pgd(div paint(u)); lam_x += alpha grad R[rho_bar + u . F]
+  // rho_bar = P(div paint(u)); lam_x += scale grad R[rho_bar + u . F]
   if (e == cudaSuccess) e = cudaMemsetAsync(ubar, 0, sizeof(float) * 4 * (size_t)d.cells() * d.batch, s);
   if (e == cudaSuccess) e = jfli::paint_vec4(disp, u, ubar, d, s);
   if (e == cudaSuccess) e = jfli::divergence_fd(ubar, 1.0f, nullptr, 0.0f, 2, 0, div, d, s);
-  if (e == cudaSuccess) e = jfli::pgd_potential(div, spec, rho_bar, d, 0.0f, kl, ks, 1.0f, s);
-  if (e == cudaSuccess) e = jfli::adjoint_position(disp, u, rho_bar, force, alpha, lam_x, d, s);
-  return cuda_status(e, err, errlen, "jfli_pgd_adjoint");
+  if (e == cudaSuccess)
+    e = pgd ? jfli::pgd_potential(div, spec, rho_bar, d, 0.0f, kl, ks, 1.0f, s)
+            : jfli::poisson_potential(div, spec, rho_bar, d, 0.0f, 1.0f, s);
+  if (e == cudaSuccess) e = jfli::adjoint_position(disp, u, rho_bar, force, scale, lam_x, d, s);
+  return cuda_status(e, err, errlen, name);
+}
+}  // namespace
+
+int jfli_pgd_adjoint(void* stream, const float* disp, const float* u, float alpha, float kl, float ks, float* lam_x,
+                     void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err,
+                     size_t errlen) {
+  return force_vjp(stream, disp, u, alpha, true, kl, ks, lam_x, workspace, workspace_bytes, nx, ny, nz, batch, err,
+                   errlen, "jfli_pgd_adjoint");
+}
+
+int jfli_force_adjoint(void* stream, const float* disp, const float* u, float scale, float* lam_x, void* workspace,
+                       size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  return force_vjp(stream, disp, u, scale, false, 0.f, 1.f, lam_x, workspace, workspace_bytes, nx, ny, nz, batch, err,
+                   errlen, "jfli_force_adjoint");
 }
 
 int jfli_pgd_potential(void* stream, const float* rho, float rho_mean, float kl, float ks, float* pot, void* workspace,

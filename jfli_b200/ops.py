@@ -706,6 +706,18 @@ def _check_pots(pots: torch.Tensor, nsteps: int, disp: torch.Tensor, batch: int)
         raise ValueError(f"pots must hold {nsteps} potentials of the particle grid's mesh")
 
 
+def force_adjoint(disp: torch.Tensor, u: torch.Tensor, scale: float, lam_x: torch.Tensor) -> torch.Tensor:
+    """lam_x += scale J^T u for the PM force at the relative positions disp (in place;
+    jfli_force_adjoint)."""
+    for name, t in (("disp", disp), ("u", u), ("lam_x", lam_x)):
+        _check(t, name)
+    (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
+    ws = workspace(int(query("jfli_pgd_adjoint_workspace_bytes", nx, ny, nz, batch)), "force_adj", disp.device)
+    call("jfli_force_adjoint", stream_ptr(), ptr(disp), ptr(u), float(scale), ptr(lam_x), ptr(ws), ws.numel(), nx, ny,
+         nz, batch)
+    return lam_x
+
+
 def kkd_run(disp: torch.Tensor, vel: torch.Tensor, kicks, drifts, rho: torch.Tensor,
             pots: torch.Tensor | None = None) -> None:
     """The ReversibleDoubleKickDrift loop in one call (in place on disp, vel); rho receives

@@ -266,28 +266,45 @@ class ReversibleNBody(torch.autograd.Function):
 class ReversibleNBodyShells(torch.autograd.Function):
     """(dx, p) -> HEALPix shells painted at snapshot times along the KKD loop (S, npix).
 
-    The loop runs in segments: `segments[j]` steps, then shell j painted from the positions
-    there (shell j: rmin, rmax, scale, with the scheme and nside of `geom`). The backward
-    walks the segments in reverse: at each shell the painter's adjoint adds that shell's
-    cotangent to lambda_x at the reconstructed positions, then the segment's steps are
-    reversed (jfli_kkd_adjoint, over the potentials kept by the forward when they fit)."""
+    The loop runs in segments: `segments[j]` steps, then shell j painted from the state
+    there by `painters[j]`, a dict with rmin, rmax, scale and either kind "sphere" (the
+    particles as they are) or kind "tiled" (replicas `rot`, `shifts`, `telephoto`, drifted
+    to the light cone at time `t` with the velocities when `vel` is set; `kick` is the
+    kick the EfficientDriftDoubleKick loop applies before a velocity paint, so the painted
+    velocity is v + kick F(x) while the loop's state stays in the reversible form). The
+    backward walks the segments in reverse: at each shell the painter's adjoint adds its
+    cotangent to lambda_x (and lambda_v, with k J^T of it through the force for a kicked
+    paint) at the reconstructed state, then the segment's steps are reversed
+    (jfli_kkd_adjoint, over the potentials kept by the forward when they fit)."""
+
+    @staticmethod
+    def _painted_velocity(x, v, pt):
+        if not pt.get("vel"):
+            return None
+        if not pt.get("kick"):
+            return v
+        vp = v.clone()
+        rho = ops.paint_cic(x)
+        force = torch.empty(x.shape[:-1] + (4,), dtype=torch.float32, device=x.device)
+        ops.poisson_force(rho, 1.0, out=force, pot=torch.empty_like(rho))
+        ops.kick_drift_paint(x, vp, force, float(pt["kick"]), 0.0, JFLI_STEP_KICK)
+        return vp
 
     @staticmethod
     def forward(ctx, dx, p, tables: ForwardTables, segments, geom):
-        nside, box, obs, rmin, rmax, scale, scheme = geom
         x = dx.detach().contiguous().clone()
         v = p.detach().contiguous().clone()
         n_all = int(sum(segments))
         pots = potential_store(n_all, x) if any(ctx.needs_input_grad[:2]) else None
         rho = torch.empty(x.shape[:-1], dtype=torch.float32, device=x.device)
+        nside = geom["nside"]
         maps = torch.empty(len(segments), 12 * nside * nside, dtype=torch.float32, device=x.device)
         s0 = 0
         for j, c in enumerate(segments):
             if c > 0:
                 kkd_forward(x, v, tables.kicks[s0:s0 + c], tables.drifts[s0:s0 + c], rho,
                             pots=None if pots is None else pots[s0:s0 + c])
-            ops.healpix_paint_shells(x, nside, box, obs, rmin[j:j + 1], rmax[j:j + 1], scale[j:j + 1], scheme=scheme,
-                                     out=maps[j:j + 1])
+            _paint(x, ReversibleNBodyShells._painted_velocity(x, v, geom["painters"][j]), geom, j, maps[j:j + 1])
             s0 += c
         ctx.tables, ctx.segments, ctx.geom, ctx.pots = tables, list(segments), geom, pots
         ctx.save_for_backward(x, v)
@@ -295,7 +312,7 @@ class ReversibleNBodyShells(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, maps_bar):
-        nside, box, obs, rmin, rmax, scale, scheme = ctx.geom
+        geom = ctx.geom
         x, v = ctx.saved_tensors
         x = x.clone()
         v = v.clone()
@@ -305,8 +322,14 @@ class ReversibleNBodyShells(torch.autograd.Function):
         mb = maps_bar.contiguous()
         s1 = int(sum(ctx.segments))
         for j in range(len(ctx.segments) - 1, -1, -1):
-            ops.healpix_paint_shells_adjoint(x, mb[j:j + 1], nside, box, obs, rmin[j:j + 1], rmax[j:j + 1],
-                                             scale[j:j + 1], scheme=scheme, pos_bar=lam_x)
+            pt = geom["painters"][j]
+            vp = ReversibleNBodyShells._painted_velocity(x, v, pt)
+            vp_bar = torch.zeros_like(v) if vp is not None else None
+            _paint_adjoint(x, vp, geom, j, mb[j:j + 1], lam_x, vp_bar)
+            if vp_bar is not None:
+                lam_v += vp_bar
+                if pt.get("kick"):
+                    ops.force_adjoint(x, vp_bar, float(pt["kick"]), lam_x)
             c = ctx.segments[j]
             if c > 0:
                 s0 = s1 - c
@@ -315,6 +338,30 @@ class ReversibleNBodyShells(torch.autograd.Function):
                 s1 = s0
         ctx.pots = None
         return lam_x, lam_v, None, None, None
+
+
+def _paint(x, vp, geom, j, out):
+    pt = geom["painters"][j]
+    if pt["kind"] == "sphere":
+        ops.healpix_paint_shells(x, geom["nside"], geom["box"], geom["obs"], [pt["rmin"]], [pt["rmax"]], [pt["scale"]],
+                                 scheme=geom["scheme"], out=out)
+    else:
+        ops.healpix_paint_tiled(x, geom["nside"], geom["box"], geom["obs"], pt["rmin"], pt["rmax"], pt["rot"],
+                                pt["shifts"], vel=vp, t=pt.get("t"), cosmo=geom.get("cosmo"),
+                                telephoto=pt.get("telephoto", False), scheme=geom["scheme"], weight=pt["scale"],
+                                out=out[0])
+
+
+def _paint_adjoint(x, vp, geom, j, map_bar, lam_x, vp_bar):
+    pt = geom["painters"][j]
+    if pt["kind"] == "sphere":
+        ops.healpix_paint_shells_adjoint(x, map_bar, geom["nside"], geom["box"], geom["obs"], [pt["rmin"]],
+                                         [pt["rmax"]], [pt["scale"]], scheme=geom["scheme"], pos_bar=lam_x)
+    else:
+        ops.healpix_paint_tiled_adjoint(x, map_bar[0], geom["nside"], geom["box"], geom["obs"], pt["rmin"], pt["rmax"],
+                                        pt["rot"], pt["shifts"], vel=vp, t=pt.get("t"), cosmo=geom.get("cosmo"),
+                                        telephoto=pt.get("telephoto", False), scheme=geom["scheme"],
+                                        weight=pt["scale"], pos_bar=lam_x, vel_bar=vp_bar)
 
 
 class PowerSpectrum(torch.autograd.Function):

@@ -180,7 +180,7 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
     v' = v + k_i F(x), x' = x + d_i v', which is the reversible step with the kick array
     shifted by one; its last kick only touches the final velocities, not the density."""
     from .adjoint import ForwardTables, ReversibleNBody
-    from .interp import NoInterp
+    from .interp import DriftInterp, NoInterp, OnionTiler
 
     interp = solver.interp_kernel
     tgt = interp.painting.target if interp.painting is not None else "particles"
@@ -189,30 +189,34 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
     solver_ok = (efficient or isinstance(solver, ReversibleDoubleKickDrift)) and isinstance(solver.pgd_kernel,
                                                                                             NoCorrection)
     pt = interp.painting
-    shells_ok = (solver_ok and isinstance(interp, NoInterp) and tgt == "spherical" and pt.scheme in ("ngp", "bilinear")
-                 and pt.paint_nside is None and isinstance(pt.weights, (type(None), int, float))
-                 and bool(np.all(np.diff(ts_arr) > 0)))
+    shells_ok = (solver_ok and tgt == "spherical" and pt.scheme in ("ngp", "bilinear") and pt.paint_nside is None
+                 and isinstance(pt.weights, (type(None), int, float)) and bool(np.all(np.diff(ts_arr) > 0))
+                 and (isinstance(interp, NoInterp) or (isinstance(interp, (DriftInterp, OnionTiler))
+                                                       and dx.array.dim() == 4)))
     if not shells_ok and not (solver_ok and isinstance(interp, NoInterp) and tgt == "density" and ts_arr.size == 1
                               and _scalar_weight(interp.painting.weights) == 1.0):
         raise NotImplementedError(
             "gradients run through the reversible adjoint: ReversibleDoubleKickDrift or EfficientDriftDoubleKick "
-            "with NoCorrection and NoInterp, painting a density snapshot at one time or HEALPix shells (ngp or "
-            "bilinear) at increasing times")
+            "with NoCorrection, painting a density snapshot at one time (NoInterp) or HEALPix shells (ngp or "
+            "bilinear) at increasing times (NoInterp, DriftInterp or OnionTiler)")
     if dx.unit != PositionUnit.GRID_RELATIVE:
         raise NotImplementedError("differentiable integration takes GRID_RELATIVE displacements")
     steps = [(e[1], e[2]) for e in time_events(t0, ts, dt0, dtype) if e[0] == "step"]
+    paint_kicks = None
     if efficient:
         kicks, drifts = EfficientDriftDoubleKick.schedule_arrays(cosmo, [a for a, _ in steps], [b for _, b in steps],
                                                                  dt0)
-        kicks = np.concatenate([[EfficientDriftDoubleKick.init_kick(cosmo, t0, t0 + dt0)],
-                                np.asarray(kicks, np.float64)[:-1]])
+        # the kick pending at a snapshot after s steps: the initial half kick, then step s-1's
+        paint_kicks = np.concatenate([[EfficientDriftDoubleKick.init_kick(cosmo, t0, t0 + dt0)],
+                                      np.asarray(kicks, np.float64)])
+        kicks = paint_kicks[:-1]
     else:
         cs = [solver.step_coefficients(cosmo, a, b, dt0, t0) for a, b in steps]
         kicks, drifts = np.array([c.kick for c in cs]), np.array([c.drift for c in cs])
     tables = ForwardTables(ktab=None, ptab=None, lpt=None, kicks=np.asarray(kicks, np.float64),
                            drifts=np.asarray(drifts, np.float64))
     if shells_ok:
-        return _run_differentiable_shells(interp, dx, p, t0, ts, dt0, dtype, tables)
+        return _run_differentiable_shells(interp, dx, p, cosmo, t0, ts, dt0, dtype, tables, paint_kicks)
     rho = ReversibleNBody.apply(dx.array.contiguous(), p.array.contiguous(), None, tables)
     from ..fields import DensityField, FieldStatus
 
@@ -224,14 +228,19 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
     return RunResult(snapshots=[snap], disp=None, vel=None, steps=len(steps))
 
 
-def _run_differentiable_shells(interp, dx: ParticleField, p: ParticleField, t0: float, ts, dt0: float, dtype,
-                               tables) -> RunResult:
-    """NoInterp HEALPix shells along the loop as one autograd node (adjoint.ReversibleNBodyShells):
-    shell i is painted at the i-th snapshot time from the positions there, with the geometry
-    and normalisation of the fused loop's shells (NoInterp.paint -> paint_spherical)."""
+def _run_differentiable_shells(interp, dx: ParticleField, p: ParticleField, cosmo, t0: float, ts, dt0: float, dtype,
+                               tables, paint_kicks) -> RunResult:
+    """HEALPix shells along the loop as one autograd node (adjoint.ReversibleNBodyShells):
+    shell j is painted at the j-th snapshot time from the state there, with the geometry,
+    painter and normalisation of the fused loop's shells. NoInterp paints the particles as
+    they are (paint_spherical); DriftInterp, and OnionTiler inside the box, paint one
+    identity replica drifted to the light cone; OnionTiler beyond the box paints the 27
+    rotated replicas, drifted when drift_on_lightcone. Under EfficientDriftDoubleKick a
+    drifted shell is painted with the velocities after the pending kick, as the fused loop
+    applies it before a velocity-dependent paint (`paint_kicks[s]` after s steps)."""
     from ..painting import shell_volume_per_pixel
     from .adjoint import ReversibleNBodyShells
-    from .interp import _spherical_result
+    from .interp import DriftInterp, NoInterp, _spherical_result, tile_shifts
 
     events = time_events(t0, ts, dt0, dtype)
     segments, count = [], 0
@@ -242,18 +251,35 @@ def _run_differentiable_shells(interp, dx: ParticleField, p: ParticleField, t0: 
             segments.append(count)
             count = 0
     nshell = len(segments)
+    saves = [ev for ev in events if ev[0] == "save"]
     rc = np.asarray(interp.r_centers, np.float64)[:nshell]
     wd = np.asarray(interp.density_widths, np.float64)[:nshell]
     rmin, rmax = rc - wd / 2.0, rc + wd / 2.0
     ws = _scalar_weight(interp.painting.weights)
     vol = np.array([shell_volume_per_pixel(dx.nside, a, b) for a, b in zip(rmin, rmax)])
     scale = np.where(vol > 0, ws / np.where(vol > 0, vol, 1.0), ws)
-    geom = (int(dx.nside), tuple(dx.box_size), tuple(dx.observer_position_mpc), rmin, rmax, scale,
-            interp.painting.scheme)
+    drift = isinstance(interp, DriftInterp) or (not isinstance(interp, NoInterp) and interp.drift_on_lightcone)
+    rotations = interp.init().rotations if not isinstance(interp, (NoInterp, DriftInterp)) else None
+    painters, done = [], 0
+    for j in range(nshell):
+        done += segments[j]
+        pj = dict(rmin=float(rmin[j]), rmax=float(rmax[j]), scale=float(scale[j]))
+        beyond = rotations is not None and rmax[j] > interp.max_comoving_distance
+        if not drift and not beyond:
+            pj["kind"] = "sphere"
+        else:
+            pj.update(kind="tiled", t=float(saves[j][2]), vel=drift,
+                      kick=float(paint_kicks[done]) if (drift and paint_kicks is not None) else None)
+            if beyond:
+                pj.update(rot=rotations, shifts=tile_shifts(dx.observer_position, dx.box_size))
+            else:
+                pj.update(rot=np.eye(3)[None], shifts=np.zeros((1, 3)))
+        painters.append(pj)
+    geom = dict(nside=int(dx.nside), box=tuple(dx.box_size), obs=tuple(dx.observer_position_mpc),
+                scheme=interp.painting.scheme, cosmo=cosmo, painters=painters)
     maps = ReversibleNBodyShells.apply(dx.array.contiguous(), p.array.contiguous(), tables, segments, geom)
     template = dx.replace(array=dx.array.detach()).paint_spherical(center=rc[0], density_plane_width=wd[0],
                                                                    scheme=interp.painting.scheme)
-    saves = [ev for ev in events if ev[0] == "save"]
     snaps = [_spherical_result(template.replace(array=maps[j]), float(saves[j][2]), float(rc[j]), float(wd[j]))
              for j in range(nshell)]
     return RunResult(snapshots=snaps, disp=None, vel=None, steps=int(sum(segments)))

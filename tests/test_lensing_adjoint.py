@@ -320,3 +320,105 @@ def test_tiled_paint_adjoint_matches_oracle_fd():
           f"oracle central difference {fd:.6e}")
     assert _rel(float(loss), L0) < 1e-4
     assert _rel(g_dir, fd) < 1e-3
+
+
+@pytest.mark.parametrize("tiler,solver_name", [("onion", "edk"), ("drift", "edk"), ("onion", "kkd")])
+def test_nbody_drifted_shells_gradient_matches_oracle_fd(tiler, solver_name):
+    """nbody with light-cone-drifted HEALPix shells (OnionTiler: the shell inside the box from
+    the particles drifted to the light cone, the two beyond it from 27 rotated replicas;
+    DriftInterp: every shell from the drifted particles) on displacements and momenta that
+    require grad: the shells equal the fused loop's, and the directional derivative of a
+    linear loss of the shells matches central differences of an FP64 oracle loop (oracle/pm.py
+    forces, the solver's steps, oracle/healpix.py's replica painter at each snapshot with the
+    velocities there; under EfficientDriftDoubleKick those include the pending kick, which the
+    loop applies before a velocity-dependent paint).
+
+    The central differences take steps of 3e-7: at 1e-6 a particle of the nearest shell
+    crosses a kink of the bilinear weights along the velocity direction under
+    EfficientDriftDoubleKick (the difference moves by 7e-3 of the derivative; at 3e-7 it
+    agrees with the adjoint to 7e-6)."""
+    import jfli_b200 as jf
+    from jfli_b200 import cosmology as cj
+    from jfli_b200.painting import shell_volume_per_pixel
+    from jfli_b200.pm.integrate import time_events
+    from jfli_b200.pm.interp import get_all_47_symmetries, tile_shifts
+    from jfli_b200.pm.solvers import EfficientDriftDoubleKick as EDK
+
+    n, box, nside, t0, t1, dt0 = 32, 200.0, 16, 0.1, 1.0, 0.15
+    cosmo = jf.Planck18()
+    ic = jf.interpolate_initial_conditions(jf.white_noise(43, (n,) * 3), (n,) * 3, (box,) * 3, cosmo=cosmo,
+                                           nside=nside)
+    dx, p = jf.lpt(cosmo, ic, ts=t0, order=2)
+    x0, v0 = dx.array.detach().contiguous().clone(), p.array.detach().contiguous().clone()
+    rng = np.random.default_rng(44)
+    ridx = tuple(int(i) for i in rng.integers(0, 47, 27))
+    painting = jf.PaintingOptions(target="spherical")
+    interp = (jf.OnionTiler(painting=painting, rotation_indices=ridx) if tiler == "onion"
+              else jf.DriftInterp(painting=painting))
+    solver = (jf.EfficientDriftDoubleKick(interp_kernel=interp) if solver_name == "edk"
+              else jf.ReversibleDoubleKickDrift(interp_kernel=interp))
+    edges = np.array([170.0, 110.0, 60.0, 20.0])  # far -> near; the box holds a sphere of 100 Mpc/h
+    centres = 0.5 * (edges[1:] + edges[:-1])
+    kw = dict(t0=t0, t1=t1, dt0=dt0, solver=solver, ts=np.asarray(cj.a_of_chi(cosmo, centres), np.float64),
+              density_widths=edges[:-1] - edges[1:])
+    xg, vg = x0.clone().requires_grad_(True), v0.clone().requires_grad_(True)
+    lc = jf.nbody(cosmo, dx.replace(array=xg), p.replace(array=vg), **kw)
+    b = rng.standard_normal(tuple(lc.array.shape))
+    r = rng.standard_normal((n, n, n, 3))
+    s = rng.standard_normal((n, n, n, 3))
+    loss = (lc.array.double() * torch.as_tensor(b, device="cuda")).sum()
+    loss.backward()
+    g_dir = float(np.sum(xg.grad.cpu().numpy() * r) + np.sum(vg.grad.cpu().numpy() * s))
+    with torch.no_grad():
+        lc_f = jf.nbody(cosmo, dx.replace(array=x0), p.replace(array=v0), **kw)
+    e_fwd = float((lc.array.detach() - lc_f.array).norm() / lc_f.array.norm())
+
+    ts = np.asarray(lc.scale_factors, np.float64)[::-1]
+    rc = np.asarray(lc.comoving_centers, np.float64)[::-1]
+    wd = np.asarray(lc.density_width, np.float64)[::-1]
+    events = time_events(t0, ts, dt0)
+    steps = [(e[1], e[2]) for e in events if e[0] == "step"]
+    if solver_name == "edk":
+        kicks, drifts = EDK.schedule_arrays(cosmo, [q for q, _ in steps], [q for _, q in steps], dt0)
+        k_init = EDK.init_kick(cosmo, t0, t0 + dt0)
+    else:
+        cs = [solver.step_coefficients(cosmo, a, q, dt0, t0) for a, q in steps]
+        kicks, drifts = [c.kick for c in cs], [c.drift for c in cs]
+    obs = np.asarray(dx.observer_position_mpc, np.float64)
+    rot27 = get_all_47_symmetries()[list(ridx)]
+    sh27 = tile_shifts(dx.observer_position, dx.box_size)
+    fn = dict(a_of_chi=lambda q: cj.a_of_chi(cosmo, q), Gp=lambda a: cj.Gp(cosmo, a), dGfa=lambda a: cj.dGfa(cosmo, a))
+
+    def oracle_shells(x, v):
+        x, v = x.copy(), v.copy()
+        if solver_name == "edk":
+            v += opm.pm_forces(x, np.float64) * k_init
+        maps, si = [], 0
+        for ev in events:
+            if ev[0] == "step":
+                if solver_name == "edk":
+                    x += v * drifts[si]
+                    v += opm.pm_forces(x, np.float64) * kicks[si]
+                else:
+                    v += opm.pm_forces(x, np.float64) * kicks[si]
+                    x += v * drifts[si]
+                si += 1
+            else:
+                i = ev[1]
+                lo, hi = rc[i] - wd[i] / 2, rc[i] + wd[i] / 2
+                rot, sh = ((rot27, sh27) if (tiler == "onion" and hi > box / 2)
+                           else (np.eye(3)[None], np.zeros((1, 3))))
+                m = oh.paint_shell_tiled(x, v, (box,) * 3, obs, lo, hi, nside, rot, sh, t=float(ev[2]), **fn)
+                maps.append(m / shell_volume_per_pixel(nside, lo, hi))
+        return np.stack(maps[::-1])  # near -> far, as nbody returns them
+
+    x64, v64 = x0.cpu().numpy().astype(np.float64), v0.cpu().numpy().astype(np.float64)
+    eps = 3e-7
+    fd = (np.sum(b * oracle_shells(x64 + eps * r, v64 + eps * s))
+          - np.sum(b * oracle_shells(x64 - eps * r, v64 - eps * s))) / (2 * eps)
+    L0 = float(np.sum(b * oracle_shells(x64, v64)))
+    print(f"nbody {tiler} shells ({solver_name}): vs the fused loop {e_fwd:.2e}; loss GPU {float(loss.detach()):.8e} "
+          f"oracle {L0:.8e}; directional derivative {g_dir:.6e} vs oracle central difference {fd:.6e}")
+    assert e_fwd < 1e-5
+    assert _rel(float(loss.detach()), L0) < 1e-3
+    assert _rel(g_dir, fd) < 1e-3
