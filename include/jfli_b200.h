@@ -115,6 +115,17 @@ int jfli_poisson_potential(void* stream, const float* rho, float rho_mean, float
  * (kl, ks in radians per cell). Replaces pm/correction.py:170-189 (PGDKernel.apply). */
 int jfli_pgd_potential(void* stream, const float* rho, float rho_mean, float kl, float ks, float* pot, void* workspace,
                        size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* The reversible step's kick and SharpeningKernel's velocity boost as one potential:
+ * pot = irfft(rfft(rho - rho_mean) (-1/k^2) (kick + boost exp(-kl^2/k^2) exp(-k^4/ks^4))),
+ * so that the CIC readout of its force mesh with factor 1 is kick F + boost F_pgd at the
+ * same positions. Replaces ReversibleDoubleKickDrift.step's kick and
+ * SharpeningKernel.apply (pm/solvers.py:292-318, pm/correction.py:248-333; boost =
+ * alpha / the full drift factor) and EfficientDriftDoubleKick.step's boost and kick at the
+ * drifted positions (pm/solvers.py:174-195; boost = alpha / the bare drift factor).
+ * Workspace as jfli_pgd_potential. */
+int jfli_sharpen_potential(void* stream, const float* rho, float rho_mean, float kick, float boost, float kl, float ks,
+                           float* pot, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch,
+                           char* err, size_t errlen);
 /* Adjoint of the PGD correction x' = x + alpha F_pgd(x) (the `jfli_pgd` entries' `_bwd`;
  * F_pgd the CIC readout of the FD force mesh of jfli_pgd_potential's potential of the
  * particles' own density, reference pm/correction.py:157-202): lam_x += alpha J^T u with J
@@ -471,6 +482,20 @@ int jfli_kkd_run_stored(void* stream, float* disp, float* vel, const float* kick
 int jfli_kkd_adjoint_stored(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
                             const float* drifts, int nsteps, const float* pots, double* sens, void* workspace,
                             size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+
+/* The pair with SharpeningKernel (pm/correction.py:214-333 in pm/solvers.py:258-411): the
+ * force of step i is jfli_sharpen_potential's combined force with (kicks[i], boosts[i]),
+ * host arrays, boosts[i] = alpha / drift factor of step i, applied with factor 1; the reverse
+ * sweep un-drifts, takes the boost and the kick off together and solves the adjoint with the
+ * same (symmetric) combined operator. pots may be null (recompute) or as the stored pair.
+ * sens[i][b][0] is then dL/d(the combined force's factor), not dL/dk. Same workspace. */
+int jfli_kkd_run_sharpened(void* stream, float* disp, float* vel, const float* kicks, const float* drifts,
+                           const float* boosts, float kl, float ks, int nsteps, float* rho, float* pots, void* workspace,
+                           size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+int jfli_kkd_adjoint_sharpened(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
+                               const float* drifts, const float* boosts, float kl, float ks, int nsteps,
+                               const float* pots, double* sens, void* workspace, size_t workspace_bytes, int nx,
+                               int ny, int nz, int batch, char* err, size_t errlen);
 
 /* dL/dmesh of P(k): out = irfft(rfft(mesh) * weights[digitize(|k|, kedges)] / M), with
  * weights[b] = 2 (dL/dP_b) prod(L/N) / count_b for the kept bins and 0 for bin 0 and

@@ -186,6 +186,21 @@ _SIGNATURES = {
         [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_float), ctypes.POINTER(c_float), c_int,
          c_void_p, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
     ),
+    "jfli_kkd_run_sharpened": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_float), ctypes.POINTER(c_float), ctypes.POINTER(c_float),
+         c_float, c_float, c_int, c_void_p, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
+    ),
+    "jfli_kkd_adjoint_sharpened": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_float), ctypes.POINTER(c_float),
+         ctypes.POINTER(c_float), c_float, c_float, c_int, c_void_p, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
+    ),
+    "jfli_sharpen_potential": (
+        c_int,
+        [c_void_p, c_void_p, c_float, c_float, c_float, c_float, c_float, c_void_p, c_void_p, c_size_t, *_DIMS,
+         *_ERR],
+    ),
     "jfli_adjoint_unkick_paint": (
         c_int,
         [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_float, c_void_p, c_void_p, c_size_t,

@@ -1133,12 +1133,31 @@ KkdWs kkd_ws(void* w, const MeshDims& d) {
   return k;
 }
 
-// density of the current positions -> potential (into pot) -> force mesh (in ws.force)
+// SharpeningKernel in the reversible step: per-step velocity boost factors alpha / drift and
+// the PGD scales; boosts == nullptr is the plain step. With boosts, step i's force is the
+// combined one, kicks[i] F + boosts[i] F_pgd at the same positions, applied with factor 1.
+struct Sharpen {
+  const float* boosts = nullptr;
+  float kl = 0.f, ks = 1.f;
+};
+
+// The potential whose force kicks step i (the mean 1 of a painted density; 0 for the
+// divergence of a cotangent mesh, whose solve is the same symmetric operator).
+cudaError_t step_potential(const float* src, float2* spec, float* pot, const MeshDims& d, float mean,
+                           const float* kicks, int i, const Sharpen& sh, cudaStream_t s) {
+  if (sh.boosts) return jfli::mixed_pgd_potential(src, spec, pot, d, mean, sh.kl, sh.ks, kicks[i], sh.boosts[i], 1.0f, s);
+  return jfli::poisson_potential(src, spec, pot, d, mean, 1.0f, s);
+}
+
+// the factor the force mesh of step i is applied with
+float step_kick(const float* kicks, int i, const Sharpen& sh) { return sh.boosts ? 1.0f : kicks[i]; }
+
+// density of the current positions -> potential of step i (into pot) -> force mesh (in ws.force)
 cudaError_t kkd_force(float* disp, float* vel, float* rho, const KkdWs& w, float* pot, const MeshDims& d,
-                      cudaStream_t s) {
+                      cudaStream_t s, const float* kicks, int i, const Sharpen& sh) {
   cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)d.cells() * d.batch * sizeof(float), s);
   if (e == cudaSuccess) e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, 0.f, JFLI_STEP_PAINT, 1.0f, rho, d, s);
-  if (e == cudaSuccess) e = jfli::poisson_potential(rho, w.spec, pot, d, 1.0f, 1.0f, s);
+  if (e == cudaSuccess) e = step_potential(rho, w.spec, pot, d, 1.0f, kicks, i, sh, s);
   if (e == cudaSuccess) e = jfli::force_mesh(pot, w.force, 1.0f, d, s);
   return e;
 }
@@ -1147,7 +1166,7 @@ cudaError_t kkd_force(float* disp, float* vel, float* rho, const KkdWs& w, float
 // potential whose force kicks step i is written to pots[i] instead of the workspace.
 int kkd_run_impl(void* stream, float* disp, float* vel, const float* kicks, const float* drifts, int nsteps,
                  float* rho, float* pots, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch,
-                 char* err, size_t errlen, const char* name) {
+                 char* err, size_t errlen, const char* name, const Sharpen& sh = Sharpen()) {
   CHECK_DIMS(nx, ny, nz, batch);
   CHECK_STENCIL(nx, ny, nz);
   CHECK_FFT(nx, ny, nz);
@@ -1168,13 +1187,14 @@ int kkd_run_impl(void* stream, float* disp, float* vel, const float* kicks, cons
   auto pot_of = [&](int i) { return pots ? pots + (size_t)i * per : w.pot; };
   // rho is cleared right before each paint (zeroed lines still in L2 when the deposits come);
   // the last step's paint stays in rho (the density of the final positions)
-  cudaError_t e = kkd_force(disp, vel, rho, w, pot_of(0), d, s);
+  cudaError_t e = nsteps > 0 ? kkd_force(disp, vel, rho, w, pot_of(0), d, s, kicks, 0, sh)
+                             : kkd_force(disp, vel, rho, w, pot_of(0), d, s, kicks, 0, Sharpen());
   for (int i = 0; i < nsteps && e == cudaSuccess; ++i) {
     e = jfli::zero_floats(rho, d.cells() * batch, s);
     if (e == cudaSuccess)
-      e = jfli::kick_drift_paint(disp, vel, w.force, kicks[i], drifts[i], JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT,
-                                 1.0f, rho, d, s);
-    if (e == cudaSuccess && i + 1 < nsteps) e = jfli::poisson_potential(rho, w.spec, pot_of(i + 1), d, 1.0f, 1.0f, s);
+      e = jfli::kick_drift_paint(disp, vel, w.force, step_kick(kicks, i, sh), drifts[i],
+                                 JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT, 1.0f, rho, d, s);
+    if (e == cudaSuccess && i + 1 < nsteps) e = step_potential(rho, w.spec, pot_of(i + 1), d, 1.0f, kicks, i + 1, sh, s);
     if (e == cudaSuccess && i + 1 < nsteps) e = jfli::force_mesh(pot_of(i + 1), w.force, 1.0f, d, s);
   }
   return cuda_status(e, err, errlen, name);
@@ -1186,7 +1206,7 @@ int kkd_run_impl(void* stream, float* disp, float* vel, const float* kicks, cons
 int kkd_adjoint_impl(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
                      const float* drifts, int nsteps, const float* pots, double* sens, void* workspace,
                      size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen,
-                     const char* name) {
+                     const char* name, const Sharpen& sh = Sharpen()) {
   CHECK_DIMS(nx, ny, nz, batch);
   CHECK_STENCIL(nx, ny, nz);
   CHECK_FFT(nx, ny, nz);
@@ -1208,7 +1228,7 @@ int kkd_adjoint_impl(void* stream, float* disp, float* vel, float* lam_x, float*
   const size_t per = (size_t)d.cells() * batch;
   cudaError_t e = cudaSuccess;
   for (int i = nsteps - 1; i >= 0 && e == cudaSuccess; --i) {
-    const float k = kicks[i], dr = drifts[i];
+    const float k = step_kick(kicks, i, sh), dr = drifts[i];
     if (pots) {
       // the force mesh of step i from its stored potential; un-drift in the paint below
       e = jfli::force_mesh(pots + (size_t)i * per, w.force, 1.0f, d, s);
@@ -1217,17 +1237,18 @@ int kkd_adjoint_impl(void* stream, float* disp, float* vel, float* lam_x, float*
       e = jfli::zero_floats(w.rho, d.cells() * batch, s);
       if (e == cudaSuccess)
         e = jfli::kick_drift_paint(disp, vel, nullptr, 0.f, -dr, JFLI_STEP_DRIFT | JFLI_STEP_PAINT, 1.0f, w.rho, d, s);
-      if (e == cudaSuccess) e = jfli::poisson_potential(w.rho, w.spec, w.pot, d, 1.0f, 1.0f, s);
+      if (e == cudaSuccess) e = step_potential(w.rho, w.spec, w.pot, d, 1.0f, kicks, i, sh, s);
       if (e == cudaSuccess) e = jfli::force_mesh(w.pot, w.force, 1.0f, d, s);
     }
-    // un-kick, adjoint paint, dL/dk and dL/dd
+    // un-kick, adjoint paint, dL/dk and dL/dd (with sharpening, dL/d of the combined force's
+    // factor 1 in place of dL/dk)
     if (e == cudaSuccess)
       e = jfli::adjoint_unkick_paint(disp, vel, lam_x, lam_v, w.force, k, dr, w.ubar, w.partials, d, s, true,
                                      pots ? disp : nullptr);
     if (e == cudaSuccess) e = jfli::sum_adjoint_partials(w.partials, d, sens + 2ll * i * batch, s);
     // rho_bar = P(div ubar); lam_x += k grad R[rho_bar + lam_v . F]
     if (e == cudaSuccess) e = jfli::divergence_fd(w.ubar, 1.0f, nullptr, 0.0f, 2, 0, w.div, d, s);
-    if (e == cudaSuccess) e = jfli::poisson_potential(w.div, w.spec, w.rho_bar, d, 0.0f, 1.0f, s);
+    if (e == cudaSuccess) e = step_potential(w.div, w.spec, w.rho_bar, d, 0.0f, kicks, i, sh, s);
     if (e == cudaSuccess) e = jfli::adjoint_position(disp, lam_v, w.rho_bar, w.force, k, lam_x, d, s);
   }
   return cuda_status(e, err, errlen, name);
@@ -1266,6 +1287,51 @@ int jfli_kkd_adjoint_stored(void* stream, float* disp, float* vel, float* lam_x,
   CHECK_PTR(pots);
   return kkd_adjoint_impl(stream, disp, vel, lam_x, lam_v, kicks, drifts, nsteps, pots, sens, workspace,
                           workspace_bytes, nx, ny, nz, batch, err, errlen, "jfli_kkd_adjoint_stored");
+}
+
+int jfli_kkd_run_sharpened(void* stream, float* disp, float* vel, const float* kicks, const float* drifts,
+                           const float* boosts, float kl, float ks, int nsteps, float* rho, float* pots, void* workspace,
+                           size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_PTR(boosts);
+  if (!(kl >= 0.0f && ks > 0.0f)) return fail(err, errlen, JFLI_EINVAL, "PGD scales need kl >= 0 and ks > 0");
+  Sharpen sh;
+  sh.boosts = boosts;
+  sh.kl = kl;
+  sh.ks = ks;
+  return kkd_run_impl(stream, disp, vel, kicks, drifts, nsteps, rho, pots, workspace, workspace_bytes, nx, ny, nz,
+                      batch, err, errlen, "jfli_kkd_run_sharpened", sh);
+}
+
+int jfli_kkd_adjoint_sharpened(void* stream, float* disp, float* vel, float* lam_x, float* lam_v, const float* kicks,
+                               const float* drifts, const float* boosts, float kl, float ks, int nsteps,
+                               const float* pots, double* sens, void* workspace, size_t workspace_bytes, int nx,
+                               int ny, int nz, int batch, char* err, size_t errlen) {
+  CHECK_PTR(boosts);
+  if (!(kl >= 0.0f && ks > 0.0f)) return fail(err, errlen, JFLI_EINVAL, "PGD scales need kl >= 0 and ks > 0");
+  Sharpen sh;
+  sh.boosts = boosts;
+  sh.kl = kl;
+  sh.ks = ks;
+  return kkd_adjoint_impl(stream, disp, vel, lam_x, lam_v, kicks, drifts, nsteps, pots, sens, workspace,
+                          workspace_bytes, nx, ny, nz, batch, err, errlen, "jfli_kkd_adjoint_sharpened", sh);
+}
+
+int jfli_sharpen_potential(void* stream, const float* rho, float rho_mean, float kick, float boost, float kl, float ks,
+                           float* pot, void* workspace, size_t workspace_bytes, int nx, int ny, int nz, int batch,
+                           char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(rho);
+  CHECK_PTR(pot);
+  CHECK_PTR(workspace);
+  CHECK_ALIGN16(workspace);
+  if (!(kl >= 0.0f && ks > 0.0f)) return fail(err, errlen, JFLI_EINVAL, "PGD scales need kl >= 0 and ks > 0");
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < spec_bytes(d))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, spec_bytes(d));
+  return cuda_status(jfli::mixed_pgd_potential(rho, (float2*)workspace, pot, d, rho_mean, kl, ks, kick, boost, 1.0f,
+                                               (cudaStream_t)stream),
+                     err, errlen, "jfli_sharpen_potential");
 }
 
 // ---- adjoints --------------------------------------------------------------------

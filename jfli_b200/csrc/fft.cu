@@ -903,6 +903,11 @@ cudaError_t poisson_potential(const float* rho, float2* spec, float* pot, const 
 
 cudaError_t pgd_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean, float kl,
                           float ks, float scale, cudaStream_t s) {
+  return mixed_pgd_potential(rho, spec, pot, d, rho_mean, kl, ks, 0.f, 1.f, scale, s);
+}
+
+cudaError_t mixed_pgd_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean,
+                                float kl, float ks, float c0, float c1, float scale, cudaStream_t s) {
   PgdOp op;
   op.nx = d.nx;
   op.ny = d.ny;
@@ -910,6 +915,8 @@ cudaError_t pgd_potential(const float* rho, float2* spec, float* pot, const Mesh
   op.norm = scale / ((float)d.nx * (float)d.ny * (float)d.nz);
   op.kl2 = kl * kl;
   op.ks4 = ks * ks * ks * ks;
+  op.c0 = c0;
+  op.c1 = c1;
   return filter_chain(rho, spec, pot, d, rho_mean, op, s);
 }
 

@@ -29,6 +29,10 @@ cudaError_t poisson_potential(const float* rho, float2* spec, float* pot, const 
                               float scale, cudaStream_t s, float* clear = nullptr);
 cudaError_t pgd_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean, float kl,
                           float ks, float scale, cudaStream_t s);
+// pot_k = delta_k (-1/k^2) (c0 + c1 PGD filter) * scale: (0, 1) is pgd_potential, (kick, boost)
+// the reversible step's kick plus the sharpening boost as one potential.
+cudaError_t mixed_pgd_potential(const float* rho, float2* spec, float* pot, const MeshDims& d, float rho_mean,
+                                float kl, float ks, float c0, float c1, float scale, cudaStream_t s);
 // dptab != null: the tangent of the filter along a change dptab of the P(k) table.
 cudaError_t ic_filter(const float* noise, float2* spec, float* out, const MeshDims& d, const float* ktab,
                       const float* ptab, int ntab, const float* box, int zero_mode_one, cudaStream_t s,

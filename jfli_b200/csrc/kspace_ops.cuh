@@ -40,13 +40,18 @@ struct PoissonOp {
   __device__ void epilogue(float*, int, int, int) const {}
 };
 
-// PGD short-range potential (reference pm/correction.py:177-189):
-// pot_k = delta_k * (-1/k^2) * exp(-kl^2/k^2) * exp(-k^4/ks^4) * norm, k = 0 -> 0.
+// PGD short-range potential (reference pm/correction.py:177-189), optionally mixed with the
+// Poisson potential:
+// pot_k = delta_k * (-1/k^2) * (c0 + c1 exp(-kl^2/k^2) exp(-k^4/ks^4)) * norm, k = 0 -> 0.
+// (c0, c1) = (0, 1) is the PGD potential; (kick, boost) the combined potential whose force
+// is a reversible step's kick plus SharpeningKernel's velocity boost at the same positions
+// (reference pm/solvers.py:292-318, pm/correction.py:214-333).
 struct PgdOp {
   static constexpr bool kInverse = true;
   static constexpr bool kStore = true;
   int nx, ny, nz;
   float norm, kl2, ks4;
+  float c0 = 0.f, c1 = 1.f;
   static size_t smem_bytes(const PgdOp& op) { return sizeof(float) * op.nx; }
   __device__ void prologue(float* sm, int) const {
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
@@ -61,7 +66,7 @@ struct PgdOp {
     const float kk = sm[kx] + k1 * k1 + k2 * k2;
     if (kk == 0.f) return make_float2(0.f, 0.f);
     const float range = expf(-kl2 / kk) * expf(-(kk * kk) / ks4);
-    return cscale(v, (-1.f / kk) * range * norm);
+    return cscale(v, (-1.f / kk) * (c0 + c1 * range) * norm);
   }
   __device__ void epilogue(float*, int, int, int) const {}
 };

@@ -706,6 +706,19 @@ def _check_pots(pots: torch.Tensor, nsteps: int, disp: torch.Tensor, batch: int)
         raise ValueError(f"pots must hold {nsteps} potentials of the particle grid's mesh")
 
 
+def pgd_adjoint(disp: torch.Tensor, u: torch.Tensor, alpha: float, kl: float, ks: float,
+                lam_x: torch.Tensor) -> torch.Tensor:
+    """lam_x += alpha J_pgd^T u for the PGD force at the relative positions disp (in place;
+    jfli_pgd_adjoint with lam_x as its accumulator)."""
+    for name, t in (("disp", disp), ("u", u), ("lam_x", lam_x)):
+        _check(t, name)
+    (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
+    ws = workspace(int(query("jfli_pgd_adjoint_workspace_bytes", nx, ny, nz, batch)), "force_adj", disp.device)
+    call("jfli_pgd_adjoint", stream_ptr(), ptr(disp), ptr(u), float(alpha), float(kl), float(ks), ptr(lam_x),
+         ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return lam_x
+
+
 def force_adjoint(disp: torch.Tensor, u: torch.Tensor, scale: float, lam_x: torch.Tensor) -> torch.Tensor:
     """lam_x += scale J^T u for the PM force at the relative positions disp (in place;
     jfli_force_adjoint)."""
@@ -718,11 +731,22 @@ def force_adjoint(disp: torch.Tensor, u: torch.Tensor, scale: float, lam_x: torc
     return lam_x
 
 
+def _sharpen_args(sharpen, nsteps: int):
+    """(boost array, its float pointer, kl, ks) of a (boosts, kl, ks) sharpening triple."""
+    boosts, kl, ks = sharpen
+    b_arr, b_ptr = _host_floats(boosts)
+    if b_arr.size != nsteps:
+        raise ValueError(f"{b_arr.size} boost factors for {nsteps} steps")
+    return b_arr, b_ptr, float(kl), float(ks)
+
+
 def kkd_run(disp: torch.Tensor, vel: torch.Tensor, kicks, drifts, rho: torch.Tensor,
-            pots: torch.Tensor | None = None) -> None:
+            pots: torch.Tensor | None = None, sharpen=None) -> None:
     """The ReversibleDoubleKickDrift loop in one call (in place on disp, vel); rho receives
     the CIC density of the final positions. With `pots` (nsteps potentials, float32 on the
-    device) the potential of every step is kept there for kkd_adjoint."""
+    device) the potential of every step is kept there for kkd_adjoint. `sharpen` = (boosts,
+    kl, ks): SharpeningKernel's per-step boost factors and PGD scales
+    (jfli_kkd_run_sharpened)."""
     _check(disp, "disp")
     _check(vel, "vel")
     _check(rho, "rho")
@@ -735,6 +759,12 @@ def kkd_run(disp: torch.Tensor, vel: torch.Tensor, kicks, drifts, rho: torch.Ten
     ws = workspace(nb, "kkd", disp.device)
     if pots is not None:
         _check_pots(pots, int(k_arr.size), disp, batch)
+    if sharpen is not None:
+        b_arr, b_ptr, kl, ks = _sharpen_args(sharpen, k_arr.size)
+        call("jfli_kkd_run_sharpened", stream_ptr(), ptr(disp), ptr(vel), k_ptr, d_ptr, b_ptr, kl, ks,
+             int(k_arr.size), ptr(rho), ptr(pots), ptr(ws), ws.numel(), nx, ny, nz, batch)
+        return
+    if pots is not None:
         call("jfli_kkd_run_stored", stream_ptr(), ptr(disp), ptr(vel), k_ptr, d_ptr, int(k_arr.size), ptr(rho),
              ptr(pots), ptr(ws), ws.numel(), nx, ny, nz, batch)
         return
@@ -743,10 +773,12 @@ def kkd_run(disp: torch.Tensor, vel: torch.Tensor, kicks, drifts, rho: torch.Ten
 
 
 def kkd_adjoint(disp: torch.Tensor, vel: torch.Tensor, lam_x: torch.Tensor, lam_v: torch.Tensor, kicks,
-                drifts, pots: torch.Tensor | None = None) -> torch.Tensor:
+                drifts, pots: torch.Tensor | None = None, sharpen=None) -> torch.Tensor:
     """Reverse sweep of kkd_run in one call (in place on all four particle grids); returns
     the (nsteps, 2) FP64 (dL/dkick, dL/ddrift) on the device. `pots`: the potentials a
-    kkd_run with pots kept (the forces are then rebuilt from them, not recomputed)."""
+    kkd_run with pots kept (the forces are then rebuilt from them, not recomputed).
+    `sharpen` as for kkd_run (the first column is then dL/d of the combined force's
+    factor; jfli_kkd_adjoint_sharpened)."""
     for name, t in (("disp", disp), ("vel", vel), ("lam_x", lam_x), ("lam_v", lam_v)):
         _check(t, name)
     (nx, ny, nz), batch, _ = _mesh_dims(disp, True)
@@ -759,6 +791,11 @@ def kkd_adjoint(disp: torch.Tensor, vel: torch.Tensor, lam_x: torch.Tensor, lam_
     ws = workspace(nb, "kkd", disp.device)
     if pots is not None:
         _check_pots(pots, int(k_arr.size), disp, batch)
+    if sharpen is not None:
+        b_arr, b_ptr, kl, ks = _sharpen_args(sharpen, k_arr.size)
+        call("jfli_kkd_adjoint_sharpened", stream_ptr(), ptr(disp), ptr(vel), ptr(lam_x), ptr(lam_v), k_ptr, d_ptr,
+             b_ptr, kl, ks, int(k_arr.size), ptr(pots), ptr(sens), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    elif pots is not None:
         call("jfli_kkd_adjoint_stored", stream_ptr(), ptr(disp), ptr(vel), ptr(lam_x), ptr(lam_v), k_ptr, d_ptr,
              int(k_arr.size), ptr(pots), ptr(sens), ptr(ws), ws.numel(), nx, ny, nz, batch)
     else:

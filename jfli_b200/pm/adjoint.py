@@ -66,6 +66,14 @@ class ForwardTables:
     dlpt: np.ndarray | None = None
     dkicks: np.ndarray | None = None
     ddrifts: np.ndarray | None = None
+    sharpen: tuple | None = None  # SharpeningKernel: (per-step boost factors, kl, ks)
+
+    def sharpen_slice(self, s0: int, s1: int):
+        """The sharpening triple of steps s0..s1-1 (None without sharpening)."""
+        if self.sharpen is None:
+            return None
+        boosts, kl, ks = self.sharpen
+        return np.asarray(boosts, np.float64)[s0:s1], kl, ks
 
 
 def kkd_schedule(cosmo, t0: float, t1: float, dt0: float):
@@ -208,24 +216,25 @@ def potential_store(nsteps: int, x: torch.Tensor) -> torch.Tensor | None:
 
 
 def kkd_forward(x: torch.Tensor, v: torch.Tensor, kicks, drifts, rho: torch.Tensor, force: torch.Tensor | None = None,
-                pot: torch.Tensor | None = None, pots: torch.Tensor | None = None) -> None:
+                pot: torch.Tensor | None = None, pots: torch.Tensor | None = None, sharpen=None) -> None:
     """The ReversibleDoubleKickDrift loop in place: per step kick with the force at the
     current positions, drift, paint; rho ends as the CIC density of the final positions.
     One library call (`jfli_kkd_run`, or `jfli_kkd_run_stored` keeping every step's
     potential in `pots`); force and pot are accepted for callers that pass buffers and are
-    not used (the library keeps its own in its workspace)."""
-    ops.kkd_run(x, v, kicks, drifts, rho, pots=pots)
+    not used (the library keeps its own in its workspace). `sharpen` = (boosts, kl, ks) adds
+    SharpeningKernel's boost to each step's kick (jfli_kkd_run_sharpened)."""
+    ops.kkd_run(x, v, kicks, drifts, rho, pots=pots, sharpen=sharpen)
 
 
 def kkd_reverse_adjoint(x: torch.Tensor, v: torch.Tensor, lam_x: torch.Tensor, lam_v: torch.Tensor, kicks, drifts,
-                        pots: torch.Tensor | None = None):
+                        pots: torch.Tensor | None = None, sharpen=None):
     """Backward sweep of kkd_forward, in place on (x, v, lam_x, lam_v): on return (x, v) is
     the recomputed initial state and (lam_x, lam_v) the cotangent at it. Returns the FP64
     (dL/dkick_n, dL/ddrift_n) arrays. One library call (`jfli_kkd_adjoint`): per step
     un-drift + paint, force mesh, un-kick + adjoint paint, P(div), CIC-gradient gather;
     with the forward pass's `pots` (`jfli_kkd_adjoint_stored`) the force mesh comes from
     the stored potential and the un-drift is part of the un-kick."""
-    return ops.kkd_adjoint(x, v, lam_x, lam_v, kicks, drifts, pots=pots)
+    return ops.kkd_adjoint(x, v, lam_x, lam_v, kicks, drifts, pots=pots, sharpen=sharpen)
 
 
 class ReversibleNBody(torch.autograd.Function):
@@ -237,7 +246,7 @@ class ReversibleNBody(torch.autograd.Function):
         v = p.detach().contiguous().clone()
         rho = torch.empty(x.shape[:-1], dtype=torch.float32, device=x.device)
         pots = potential_store(len(tables.kicks), x) if any(ctx.needs_input_grad[:3]) else None
-        kkd_forward(x, v, tables.kicks, tables.drifts, rho, pots=pots)
+        kkd_forward(x, v, tables.kicks, tables.drifts, rho, pots=pots, sharpen=tables.sharpen)
         ctx.tables = tables
         ctx.omega_c = omega_c
         ctx.pots = pots
@@ -253,7 +262,10 @@ class ReversibleNBody(torch.autograd.Function):
         lam_x = torch.zeros_like(x)
         lam_v = torch.zeros_like(v)
         ops.adjoint_position(x, lam_x, rho_bar=grho.contiguous())  # adjoint of the final paint
-        sens = kkd_reverse_adjoint(x, v, lam_x, lam_v, t.kicks, t.drifts, pots=ctx.pots)
+        if ctx.needs_input_grad[2] and t.sharpen is not None:
+            raise NotImplementedError("d/dOmega_c of a run with SharpeningKernel: the sweep's sensitivities are "
+                                      "those of the combined kick and boost")
+        sens = kkd_reverse_adjoint(x, v, lam_x, lam_v, t.kicks, t.drifts, pots=ctx.pots, sharpen=t.sharpen)
         ctx.pots = None
         gom = None
         if ctx.needs_input_grad[2]:
@@ -278,13 +290,20 @@ class ReversibleNBodyShells(torch.autograd.Function):
     (jfli_kkd_adjoint, over the potentials kept by the forward when they fit)."""
 
     @staticmethod
-    def _painted_velocity(x, v, pt):
+    def _painted_velocity(x, v, pt, tables):
         if not pt.get("vel"):
             return None
         if not pt.get("kick"):
             return v
         vp = v.clone()
         rho = ops.paint_cic(x)
+        if pt.get("boost"):  # kick F + boost F_pgd, one combined force
+            from .correction import sharpen_potential
+
+            _, kl, ks = tables.sharpen
+            force = ops.force_mesh(sharpen_potential(rho, float(pt["kick"]), float(pt["boost"]), kl, ks, 1.0))
+            ops.kick_drift_paint(x, vp, force, 1.0, 0.0, JFLI_STEP_KICK)
+            return vp
         force = torch.empty(x.shape[:-1] + (4,), dtype=torch.float32, device=x.device)
         ops.poisson_force(rho, 1.0, out=force, pot=torch.empty_like(rho))
         ops.kick_drift_paint(x, vp, force, float(pt["kick"]), 0.0, JFLI_STEP_KICK)
@@ -303,8 +322,9 @@ class ReversibleNBodyShells(torch.autograd.Function):
         for j, c in enumerate(segments):
             if c > 0:
                 kkd_forward(x, v, tables.kicks[s0:s0 + c], tables.drifts[s0:s0 + c], rho,
-                            pots=None if pots is None else pots[s0:s0 + c])
-            _paint(x, ReversibleNBodyShells._painted_velocity(x, v, geom["painters"][j]), geom, j, maps[j:j + 1])
+                            pots=None if pots is None else pots[s0:s0 + c], sharpen=tables.sharpen_slice(s0, s0 + c))
+            _paint(x, ReversibleNBodyShells._painted_velocity(x, v, geom["painters"][j], tables), geom, j,
+                   maps[j:j + 1])
             s0 += c
         ctx.tables, ctx.segments, ctx.geom, ctx.pots = tables, list(segments), geom, pots
         ctx.save_for_backward(x, v)
@@ -323,18 +343,21 @@ class ReversibleNBodyShells(torch.autograd.Function):
         s1 = int(sum(ctx.segments))
         for j in range(len(ctx.segments) - 1, -1, -1):
             pt = geom["painters"][j]
-            vp = ReversibleNBodyShells._painted_velocity(x, v, pt)
+            vp = ReversibleNBodyShells._painted_velocity(x, v, pt, t)
             vp_bar = torch.zeros_like(v) if vp is not None else None
             _paint_adjoint(x, vp, geom, j, mb[j:j + 1], lam_x, vp_bar)
             if vp_bar is not None:
                 lam_v += vp_bar
                 if pt.get("kick"):
                     ops.force_adjoint(x, vp_bar, float(pt["kick"]), lam_x)
+                    if pt.get("boost"):  # the sharpening boost's share: boost J_pgd^T vp_bar
+                        _, kl, ks = t.sharpen
+                        ops.pgd_adjoint(x, vp_bar, float(pt["boost"]), kl, ks, lam_x)
             c = ctx.segments[j]
             if c > 0:
                 s0 = s1 - c
                 kkd_reverse_adjoint(x, v, lam_x, lam_v, t.kicks[s0:s1], t.drifts[s0:s1],
-                                    pots=None if pots is None else pots[s0:s1])
+                                    pots=None if pots is None else pots[s0:s1], sharpen=t.sharpen_slice(s0, s1))
                 s1 = s0
         ctx.pots = None
         return lam_x, lam_v, None, None, None

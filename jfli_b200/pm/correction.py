@@ -7,7 +7,7 @@ import dataclasses
 import torch
 
 from .. import ops
-from .._lib import JFLI_STEP_CORRECT, JFLI_STEP_PAINT
+from .._lib import JFLI_STEP_CORRECT, JFLI_STEP_KICK, JFLI_STEP_PAINT
 
 
 class AbstractCorrection:
@@ -65,17 +65,37 @@ class PGDKernel(AbstractCorrection):
 
 @dataclasses.dataclass(frozen=True)
 class SharpeningKernel(AbstractCorrection):
-    """Velocity sharpening (reference pm/correction.py:205-333); not on the B200 path."""
+    """Reversible PGD-style correction (reference pm/correction.py:214-333): a velocity boost
+    v += alpha F_pgd(x) / full_drift_factor at the positions the next drift starts from, so
+    that the drift adds alpha F_pgd(x) to x on top of v * drift; rewind takes the same boost
+    off at the un-drifted positions. F_pgd as for PGDKernel. The fused loops fold the boost
+    into the step's kick (one combined potential, sharpen_potential)."""
+
+    alpha: float = 0.2
+    kl: float = 0.3
+    ks: float = 1.0
 
     @property
     def reversible(self) -> bool:
         return True
 
+    def boost(self, full_drift_factor: float) -> float:
+        """The factor of F_pgd in the velocity boost."""
+        return float(self.alpha) / float(full_drift_factor)
+
+    def _boosted(self, pos, vel, factor):
+        x = pos.array.contiguous()
+        v = vel.array.contiguous().clone()
+        rho = ops.paint_cic(x)
+        force = ops.force_mesh(pgd_potential(rho, self.kl, self.ks, 1.0))
+        ops.kick_drift_paint(x, v, force, factor, 0.0, JFLI_STEP_KICK)
+        return pos, vel.replace(array=v)
+
     def apply(self, t, pos, vel, full_drift_factor):
-        raise NotImplementedError("SharpeningKernel is not on the B200 path")
+        return self._boosted(pos, vel, self.boost(full_drift_factor))
 
     def rewind(self, t, pos, vel, full_drift_factor):
-        raise NotImplementedError("SharpeningKernel is not on the B200 path")
+        return self._boosted(pos, vel, -self.boost(full_drift_factor))
 
 
 def pgd_correct(x: torch.Tensor, alpha: float, kl: float, ks: float) -> torch.Tensor:
@@ -125,4 +145,21 @@ def pgd_potential(rho: torch.Tensor, kl: float, ks: float, rho_mean: float = 1.0
     ws = ops.workspace(nb, "spec", rho.device)
     call("jfli_pgd_potential", stream_ptr(), ptr(rho), float(rho_mean), float(kl), float(ks), ptr(out), ptr(ws),
          ws.numel(), nx, ny, nz, batch)
+    return out
+
+
+def sharpen_potential(rho: torch.Tensor, kick: float, boost: float, kl: float, ks: float, rho_mean: float = 1.0,
+                      out: torch.Tensor | None = None) -> torch.Tensor:
+    """The potential whose force, applied with factor 1, is kick F + boost F_pgd at the
+    positions rho was painted from (jfli_sharpen_potential)."""
+    from .._lib import call, ptr, query, stream_ptr
+
+    (nx, ny, nz) = tuple(rho.shape[-3:])
+    batch = rho.numel() // (nx * ny * nz)
+    if out is None:
+        out = torch.empty_like(rho)
+    nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
+    ws = ops.workspace(nb, "spec", rho.device)
+    call("jfli_sharpen_potential", stream_ptr(), ptr(rho), float(rho_mean), float(kick), float(boost), float(kl),
+         float(ks), ptr(out), ptr(ws), ws.numel(), nx, ny, nz, batch)
     return out

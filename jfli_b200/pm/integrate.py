@@ -28,7 +28,7 @@ import torch
 from .. import ops
 from .._lib import JFLI_STEP_CLEAR, JFLI_STEP_CORRECT, JFLI_STEP_DRIFT, JFLI_STEP_KICK, JFLI_STEP_PAINT
 from ..fields import ParticleField, PositionUnit
-from .correction import NoCorrection, PGDKernel, pgd_potential
+from .correction import NoCorrection, PGDKernel, SharpeningKernel, pgd_potential, sharpen_potential
 from .solvers import (AbstractNBodySolver, EfficientDriftDoubleKick, NBodyState, ReversibleDoubleKickDrift,
                       StepCoefficients)
 
@@ -81,7 +81,8 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
     if not efficient and not isinstance(solver, ReversibleDoubleKickDrift):
         raise NotImplementedError(f"{type(solver).__name__} has no fused GPU schedule")
     pgd = solver.pgd_kernel if (efficient and isinstance(solver.pgd_kernel, PGDKernel)) else None
-    if not isinstance(solver.pgd_kernel, (NoCorrection, PGDKernel)):
+    sharpen = solver.pgd_kernel if isinstance(solver.pgd_kernel, SharpeningKernel) else None
+    if not isinstance(solver.pgd_kernel, (NoCorrection, PGDKernel, SharpeningKernel)):
         raise NotImplementedError(f"{type(solver.pgd_kernel).__name__} is not on the B200 path")
     interp = solver.interp_kernel
     if dx.unit != PositionUnit.GRID_RELATIVE:
@@ -103,6 +104,17 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
             kicks_all, drifts_all = EfficientDriftDoubleKick.schedule_arrays(cosmo, ta_all, tb_all, dt0)
         else:
             kicks_all, drifts_all = ReversibleDoubleKickDrift.schedule_arrays(cosmo, ta_all, tb_all, dt0, t0)
+        if sharpen is not None:
+            # the boost factor per step: alpha / the drift factor the reference hands to the
+            # correction (the bare one in the efficient step, the full one in the reversible)
+            fd = (EfficientDriftDoubleKick.bare_drift(cosmo, ta_all, tb_all) if efficient
+                  else np.asarray(drifts_all, np.float64))
+            boosts_all = float(sharpen.alpha) / np.asarray(fd, np.float64)
+
+    def sharpened_force(i):
+        """Force mesh of step i's kick plus its sharpening boost, from the density in rho."""
+        sharpen_potential(rho, float(kicks_all[i]), float(boosts_all[i]), sharpen.kl, sharpen.ks, 1.0, out=pot)
+        ops.force_mesh(pot, out=force)
 
     tgt = interp.painting.target if interp.painting is not None else "particles"
     w_snap = _scalar_weight(interp.painting.weights) if interp.painting is not None else 1.0
@@ -110,7 +122,10 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
 
     # force at the initial positions (every paint clears the density mesh right before it)
     ops.kick_drift_paint(x, v, None, 0.0, 0.0, JFLI_STEP_PAINT | JFLI_STEP_CLEAR, rho)
-    ops.poisson_force(rho, 1.0, out=force, pot=pot)
+    if sharpen is not None and not efficient and n_steps:
+        sharpened_force(0)
+    else:
+        ops.poisson_force(rho, 1.0, out=force, pot=pot)
     pending = EfficientDriftDoubleKick.init_kick(cosmo, t0, t0 + dt0) if efficient else None
     rho_is_current = True  # rho holds the paint of the current positions
 
@@ -135,13 +150,20 @@ def run_fused(solver: AbstractNBodySolver, dx: ParticleField, p: ParticleField, 
                                          JFLI_STEP_CORRECT | JFLI_STEP_PAINT | JFLI_STEP_CLEAR, rho)
                 else:
                     ops.kick_drift_paint(x, v, force, kick, c.drift, flags, rho)
-                ops.poisson_force(rho, 1.0, out=force, pot=pot)
-                pending = c.kick
+                if sharpen is not None:  # the boost and the kick at the drifted positions
+                    sharpened_force(step_i - 1)
+                    pending = 1.0
+                else:
+                    ops.poisson_force(rho, 1.0, out=force, pot=pot)
+                    pending = c.kick
             else:
-                ops.kick_drift_paint(x, v, force, c.kick, c.drift,
+                ops.kick_drift_paint(x, v, force, 1.0 if sharpen is not None else c.kick, c.drift,
                                      JFLI_STEP_KICK | JFLI_STEP_DRIFT | JFLI_STEP_PAINT | JFLI_STEP_CLEAR, rho)
                 if step_i < n_steps:
-                    ops.poisson_force(rho, 1.0, out=force, pot=pot)
+                    if sharpen is not None:
+                        sharpened_force(step_i)
+                    else:
+                        ops.poisson_force(rho, 1.0, out=force, pot=pot)
             rho_is_current = True
             state = NBodyState(interp_state=interp.advance(state.interp_state, tb), t_initial=t0)
         else:
@@ -186,8 +208,9 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
     tgt = interp.painting.target if interp.painting is not None else "particles"
     ts_arr = np.atleast_1d(np.asarray(ts))
     efficient = isinstance(solver, EfficientDriftDoubleKick)
-    solver_ok = (efficient or isinstance(solver, ReversibleDoubleKickDrift)) and isinstance(solver.pgd_kernel,
-                                                                                            NoCorrection)
+    solver_ok = (efficient or isinstance(solver, ReversibleDoubleKickDrift)) and isinstance(
+        solver.pgd_kernel, (NoCorrection, SharpeningKernel))
+    sharpen = solver.pgd_kernel if isinstance(solver.pgd_kernel, SharpeningKernel) else None
     pt = interp.painting
     shells_ok = (solver_ok and tgt == "spherical" and pt.scheme in ("ngp", "bilinear") and pt.paint_nside is None
                  and isinstance(pt.weights, (type(None), int, float)) and bool(np.all(np.diff(ts_arr) > 0))
@@ -197,26 +220,34 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
                               and _scalar_weight(interp.painting.weights) == 1.0):
         raise NotImplementedError(
             "gradients run through the reversible adjoint: ReversibleDoubleKickDrift or EfficientDriftDoubleKick "
-            "with NoCorrection, painting a density snapshot at one time (NoInterp) or HEALPix shells (ngp or "
+            "with NoCorrection or SharpeningKernel, painting a density snapshot at one time (NoInterp) or HEALPix shells (ngp or "
             "bilinear) at increasing times (NoInterp, DriftInterp or OnionTiler)")
     if dx.unit != PositionUnit.GRID_RELATIVE:
         raise NotImplementedError("differentiable integration takes GRID_RELATIVE displacements")
     steps = [(e[1], e[2]) for e in time_events(t0, ts, dt0, dtype) if e[0] == "step"]
-    paint_kicks = None
+    paint_kicks = paint_boosts = boosts = None
     if efficient:
-        kicks, drifts = EfficientDriftDoubleKick.schedule_arrays(cosmo, [a for a, _ in steps], [b for _, b in steps],
-                                                                 dt0)
+        ta, tb = [a for a, _ in steps], [b for _, b in steps]
+        kicks, drifts = EfficientDriftDoubleKick.schedule_arrays(cosmo, ta, tb, dt0)
         # the kick pending at a snapshot after s steps: the initial half kick, then step s-1's
         paint_kicks = np.concatenate([[EfficientDriftDoubleKick.init_kick(cosmo, t0, t0 + dt0)],
                                       np.asarray(kicks, np.float64)])
         kicks = paint_kicks[:-1]
+        if sharpen is not None:
+            # the boost rides with the kick it shares positions with (none on the initial half kick)
+            b = float(sharpen.alpha) / np.asarray(EfficientDriftDoubleKick.bare_drift(cosmo, ta, tb), np.float64)
+            paint_boosts = np.concatenate([[0.0], np.atleast_1d(b)])
+            boosts = paint_boosts[:-1]
     else:
         cs = [solver.step_coefficients(cosmo, a, b, dt0, t0) for a, b in steps]
         kicks, drifts = np.array([c.kick for c in cs]), np.array([c.drift for c in cs])
+        if sharpen is not None:
+            boosts = np.array([sharpen.boost(c.drift) for c in cs], np.float64)
     tables = ForwardTables(ktab=None, ptab=None, lpt=None, kicks=np.asarray(kicks, np.float64),
-                           drifts=np.asarray(drifts, np.float64))
+                           drifts=np.asarray(drifts, np.float64),
+                           sharpen=None if sharpen is None else (boosts, float(sharpen.kl), float(sharpen.ks)))
     if shells_ok:
-        return _run_differentiable_shells(interp, dx, p, cosmo, t0, ts, dt0, dtype, tables, paint_kicks)
+        return _run_differentiable_shells(interp, dx, p, cosmo, t0, ts, dt0, dtype, tables, paint_kicks, paint_boosts)
     rho = ReversibleNBody.apply(dx.array.contiguous(), p.array.contiguous(), None, tables)
     from ..fields import DensityField, FieldStatus
 
@@ -229,7 +260,7 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
 
 
 def _run_differentiable_shells(interp, dx: ParticleField, p: ParticleField, cosmo, t0: float, ts, dt0: float, dtype,
-                               tables, paint_kicks) -> RunResult:
+                               tables, paint_kicks, paint_boosts=None) -> RunResult:
     """HEALPix shells along the loop as one autograd node (adjoint.ReversibleNBodyShells):
     shell j is painted at the j-th snapshot time from the state there, with the geometry,
     painter and normalisation of the fused loop's shells. NoInterp paints the particles as
@@ -269,7 +300,8 @@ def _run_differentiable_shells(interp, dx: ParticleField, p: ParticleField, cosm
             pj["kind"] = "sphere"
         else:
             pj.update(kind="tiled", t=float(saves[j][2]), vel=drift,
-                      kick=float(paint_kicks[done]) if (drift and paint_kicks is not None) else None)
+                      kick=float(paint_kicks[done]) if (drift and paint_kicks is not None) else None,
+                      boost=float(paint_boosts[done]) if (drift and paint_boosts is not None) else None)
             if beyond:
                 pj.update(rot=rotations, shifts=tile_shifts(dx.observer_position, dx.box_size))
             else:

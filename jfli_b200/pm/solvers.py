@@ -22,7 +22,7 @@ from .. import cosmology as cj
 from .. import ops
 from .._lib import JFLI_STEP_DRIFT, JFLI_STEP_KICK
 from ..fields import PositionUnit
-from .correction import AbstractCorrection, NoCorrection, PGDKernel
+from .correction import AbstractCorrection, NoCorrection, PGDKernel, SharpeningKernel, sharpen_potential
 from .interp import AbstractInterp, InterpTilerState
 
 
@@ -36,6 +36,15 @@ def _force_mesh(x: torch.Tensor) -> torch.Tensor:
     """Force meshes (without 1.5 Omega_m) of the CIC density of relative positions x."""
     rho = ops.paint_cic(x)
     return ops.poisson_force(rho, rho_mean=1.0)
+
+
+def _step_force(x: torch.Tensor, kick: float, corr, boost: float = 0.0):
+    """(force mesh, factor) of a kick at relative positions x: kick F, or with a
+    SharpeningKernel the combined kick F + boost F_pgd as one force applied with factor 1."""
+    if isinstance(corr, SharpeningKernel):
+        rho = ops.paint_cic(x)
+        return ops.force_mesh(sharpen_potential(rho, kick, boost, corr.kl, corr.ks, 1.0)), 1.0
+    return _force_mesh(x), kick
 
 
 def _rel(field):
@@ -81,6 +90,14 @@ class EfficientDriftDoubleKick(AbstractNBodySolver):
         return float(1.5 * cosmo.Omega_m * kf / (ac**2 * cj.E(cosmo, ac)))
 
     @staticmethod
+    def bare_drift(cosmo, t0, t1):
+        """(Gp(t1) - Gp(t0)) / gp(sqrt(t0 t1)): the drift factor without its 1/(a^3 E)
+        prefactor, which the reference's step hands to the correction kernel
+        (pm/solvers.py:164-175). Scalars or arrays."""
+        t0t1 = np.sqrt(np.asarray(t0, np.float64) * np.asarray(t1, np.float64))
+        return (cj.Gp(cosmo, t1) - cj.Gp(cosmo, t0)) / cj.gp(cosmo, t0t1)
+
+    @staticmethod
     def step_coefficients(cosmo, t0, t1, dt, t_initial=None) -> StepCoefficients:
         t0t1 = math.sqrt(t0 * t1)
         ai, ac, af = t0, t0t1, t1
@@ -121,11 +138,17 @@ class EfficientDriftDoubleKick(AbstractNBodySolver):
         x = disp.array.contiguous().clone()
         v = velocities.array.contiguous().clone()
         ops.kick_drift_paint(x, v, None, 0.0, c.drift, JFLI_STEP_DRIFT)
-        xf, vf = self.pgd_kernel.apply(t1, disp.replace(array=x, scale_factors=t1), velocities.replace(array=v),
-                                       full_drift_factor=c.drift)
-        x = xf.array.contiguous()
-        force = _force_mesh(x)
-        ops.kick_drift_paint(x, v, force, c.kick, 0.0, JFLI_STEP_KICK)
+        if isinstance(self.pgd_kernel, SharpeningKernel):
+            # the boost and the kick act at the same (drifted) positions: one combined force
+            boost = self.pgd_kernel.boost(float(self.bare_drift(cosmo, t0, t1)))
+            xf = disp.replace(array=x, scale_factors=t1)
+            force, factor = _step_force(x, c.kick, self.pgd_kernel, boost)
+        else:
+            xf, vf = self.pgd_kernel.apply(t1, disp.replace(array=x, scale_factors=t1), velocities.replace(array=v),
+                                           full_drift_factor=c.drift)
+            x = xf.array.contiguous()
+            force, factor = _force_mesh(x), c.kick
+        ops.kick_drift_paint(x, v, force, factor, 0.0, JFLI_STEP_KICK)
         new_state = NBodyState(interp_state=self.interp_kernel.advance(state.interp_state, t1),
                                t_initial=state.t_initial)
         return xf.replace(array=x, scale_factors=t1), velocities.replace(array=v, scale_factors=t1), new_state
@@ -162,6 +185,10 @@ class ReversibleDoubleKickDrift(AbstractNBodySolver):
         drift = (cj.Gp(cosmo, t1s) - cj.Gp(cosmo, t0s)) / cj.gp(cosmo, af_2) / (af_2**3 * cj.E(cosmo, af_2))
         return kick, drift
 
+    def _boost(self, c: StepCoefficients) -> float:
+        """The sharpening boost factor of a step (alpha / its full drift factor), 0 without one."""
+        return self.pgd_kernel.boost(c.drift) if isinstance(self.pgd_kernel, SharpeningKernel) else 0.0
+
     def init(self, displacement, velocities, t0, t1, dt, cosmo):
         return displacement, velocities, NBodyState(interp_state=self.interp_kernel.init(), t_initial=t0)
 
@@ -170,14 +197,15 @@ class ReversibleDoubleKickDrift(AbstractNBodySolver):
             # The reference applies PGD here but then drifts from the uncorrected position,
             # so the correction has no effect on the trajectory (pm/solvers.py:314-318).
             pass
-        elif not isinstance(self.pgd_kernel, NoCorrection):
+        elif not isinstance(self.pgd_kernel, (NoCorrection, SharpeningKernel)):
             raise NotImplementedError(f"{type(self.pgd_kernel).__name__} is not on the B200 path")
         c = self.step_coefficients(cosmo, t0, t1, dt, state.t_initial)
         disp = _rel(displacement)
         x = disp.array.contiguous().clone()
         v = velocities.array.contiguous().clone()
-        force = _force_mesh(x)
-        ops.kick_drift_paint(x, v, force, c.kick, c.drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT)
+        # kick, then the sharpening boost at the same x (one combined force), then the drift
+        force, factor = _step_force(x, c.kick, self.pgd_kernel, self._boost(c))
+        ops.kick_drift_paint(x, v, force, factor, c.drift, JFLI_STEP_KICK | JFLI_STEP_DRIFT)
         new_state = NBodyState(interp_state=self.interp_kernel.advance(state.interp_state, t1),
                                t_initial=state.t_initial)
         return (disp.replace(array=x, scale_factors=t1), velocities.replace(array=v, scale_factors=math.sqrt(t0 * t1)),
@@ -189,8 +217,8 @@ class ReversibleDoubleKickDrift(AbstractNBodySolver):
         x = disp.array.contiguous().clone()
         v = velocities.array.contiguous().clone()
         ops.kick_drift_paint(x, v, None, 0.0, -c.drift, JFLI_STEP_DRIFT)
-        force = _force_mesh(x)
-        ops.kick_drift_paint(x, v, force, -c.kick, 0.0, JFLI_STEP_KICK)
+        force, factor = _step_force(x, c.kick, self.pgd_kernel, self._boost(c))
+        ops.kick_drift_paint(x, v, force, -factor, 0.0, JFLI_STEP_KICK)
         ts = self.interp_kernel.ts
         t1c = min(t1, float(ts[-1])) if ts is not None else t1
         prev = NBodyState(interp_state=self.interp_kernel.rewind(state.interp_state, t1c), t_initial=state.t_initial)

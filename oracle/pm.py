@@ -333,10 +333,18 @@ def pgd_correction(disp, alpha, kl, ks, dtype=np.float64):
     return disp + dtype(alpha) * f
 
 
-def kdk_run(dx, p, coeffs, dtype=np.float64, snapshot_after=None, pgd=None):
+def sharpening_boost(disp, alpha, kl, ks, drift_factor, dtype=np.float64):
+    """SharpeningKernel's velocity boost (reference pm/correction.py:293-333): the PGD
+    displacement alpha F_pgd(x) divided by the drift factor the step hands over."""
+    x = disp.astype(dtype)
+    return (pgd_correction(x, alpha, kl, ks, dtype) - x) / dtype(drift_factor)
+
+
+def kdk_run(dx, p, coeffs, dtype=np.float64, snapshot_after=None, pgd=None, sharpen=None):
     """FastPM KDK loop (EfficientDriftDoubleKick): coeffs = dict(init_kick, steps=[(kick, drift)]).
     pgd = (alpha, kl, ks) applies the PGD correction after each drift (reference
-    pm/solvers.py:165-178).
+    pm/solvers.py:165-178); sharpen = (alpha, kl, ks, bare drift factors) adds the
+    SharpeningKernel boost at the drifted positions before the kick (pm/solvers.py:174-195).
 
     Returns (x, v, snapshots) with snapshots = densities painted after the listed steps."""
     x = dx.astype(dtype).copy()
@@ -347,31 +355,40 @@ def kdk_run(dx, p, coeffs, dtype=np.float64, snapshot_after=None, pgd=None):
         x += v * dtype(drift)
         if pgd is not None:
             x = pgd_correction(x, *pgd, dtype=dtype)
+        if sharpen is not None:
+            v += sharpening_boost(x, *sharpen[:3], sharpen[3][n], dtype)
         v += pm_forces(x, dtype) * dtype(kick)
         if snapshot_after is not None and n in snapshot_after:
             snaps.append(cic_paint(x))
     return x, v, snaps
 
 
-def kkd_step(x, v, kick, drift, dtype=np.float64):
-    """One ReversibleDoubleKickDrift step: kick with the force at x, then drift."""
+def kkd_step(x, v, kick, drift, dtype=np.float64, sharpen=None):
+    """One ReversibleDoubleKickDrift step: kick with the force at x, then drift. sharpen =
+    (alpha, kl, ks) adds SharpeningKernel's boost at x between the kick and the drift, with
+    the step's full drift factor (reference pm/solvers.py:292-318)."""
     v = v + pm_forces(x, dtype) * dtype(kick)
+    if sharpen is not None:
+        v = v + sharpening_boost(x, *sharpen, drift, dtype)
     x = x + v * dtype(drift)
     return x, v
 
 
-def kkd_reverse(x, v, kick, drift, dtype=np.float64):
+def kkd_reverse(x, v, kick, drift, dtype=np.float64, sharpen=None):
+    """The inverse of kkd_step: un-drift, take the boost off at the recovered positions, un-kick."""
     x = x - v * dtype(drift)
+    if sharpen is not None:
+        v = v - sharpening_boost(x, *sharpen, drift, dtype)
     v = v - pm_forces(x, dtype) * dtype(kick)
     return x, v
 
 
-def kkd_run(dx, p, steps, dtype=np.float64, snapshot_after=None):
+def kkd_run(dx, p, steps, dtype=np.float64, snapshot_after=None, sharpen=None):
     x = dx.astype(dtype).copy()
     v = p.astype(dtype).copy()
     snaps = []
     for n, (kick, drift) in enumerate(steps):
-        x, v = kkd_step(x, v, kick, drift, dtype)
+        x, v = kkd_step(x, v, kick, drift, dtype, sharpen)
         if snapshot_after is not None and n in snapshot_after:
             snaps.append(cic_paint(x))
     return x, v, snaps

@@ -322,7 +322,8 @@ def test_tiled_paint_adjoint_matches_oracle_fd():
     assert _rel(g_dir, fd) < 1e-3
 
 
-@pytest.mark.parametrize("tiler,solver_name", [("onion", "edk"), ("drift", "edk"), ("onion", "kkd")])
+@pytest.mark.parametrize("tiler,solver_name", [("onion", "edk"), ("drift", "edk"), ("onion", "kkd"),
+                                               ("onion", "edk_sharp")])
 def test_nbody_drifted_shells_gradient_matches_oracle_fd(tiler, solver_name):
     """nbody with light-cone-drifted HEALPix shells (OnionTiler: the shell inside the box from
     the particles drifted to the light cone, the two beyond it from 27 rotated replicas;
@@ -331,7 +332,8 @@ def test_nbody_drifted_shells_gradient_matches_oracle_fd(tiler, solver_name):
     linear loss of the shells matches central differences of an FP64 oracle loop (oracle/pm.py
     forces, the solver's steps, oracle/healpix.py's replica painter at each snapshot with the
     velocities there; under EfficientDriftDoubleKick those include the pending kick, which the
-    loop applies before a velocity-dependent paint).
+    loop applies before a velocity-dependent paint; with SharpeningKernel, "edk_sharp", that
+    pending kick carries the sharpening boost, whose VJP adds boost J_pgd^T).
 
     The central differences take steps of 3e-7: at 1e-6 a particle of the nearest shell
     crosses a kink of the bilinear weights along the velocity direction under
@@ -355,8 +357,12 @@ def test_nbody_drifted_shells_gradient_matches_oracle_fd(tiler, solver_name):
     painting = jf.PaintingOptions(target="spherical")
     interp = (jf.OnionTiler(painting=painting, rotation_indices=ridx) if tiler == "onion"
               else jf.DriftInterp(painting=painting))
-    solver = (jf.EfficientDriftDoubleKick(interp_kernel=interp) if solver_name == "edk"
-              else jf.ReversibleDoubleKickDrift(interp_kernel=interp))
+    sharp = (0.03, 0.3, 1.0)  # SharpeningKernel(alpha, kl, ks) for "edk_sharp"
+    if solver_name == "kkd":
+        solver = jf.ReversibleDoubleKickDrift(interp_kernel=interp)
+    else:
+        solver = jf.EfficientDriftDoubleKick(interp_kernel=interp, pgd_kernel=jf.SharpeningKernel(*sharp)
+                                             if solver_name == "edk_sharp" else jf.NoCorrection())
     edges = np.array([170.0, 110.0, 60.0, 20.0])  # far -> near; the box holds a sphere of 100 Mpc/h
     centres = 0.5 * (edges[1:] + edges[:-1])
     kw = dict(t0=t0, t1=t1, dt0=dt0, solver=solver, ts=np.asarray(cj.a_of_chi(cosmo, centres), np.float64),
@@ -378,9 +384,10 @@ def test_nbody_drifted_shells_gradient_matches_oracle_fd(tiler, solver_name):
     wd = np.asarray(lc.density_width, np.float64)[::-1]
     events = time_events(t0, ts, dt0)
     steps = [(e[1], e[2]) for e in events if e[0] == "step"]
-    if solver_name == "edk":
+    if solver_name != "kkd":
         kicks, drifts = EDK.schedule_arrays(cosmo, [q for q, _ in steps], [q for _, q in steps], dt0)
         k_init = EDK.init_kick(cosmo, t0, t0 + dt0)
+        bare = np.atleast_1d(EDK.bare_drift(cosmo, [q for q, _ in steps], [q for _, q in steps]))
     else:
         cs = [solver.step_coefficients(cosmo, a, q, dt0, t0) for a, q in steps]
         kicks, drifts = [c.kick for c in cs], [c.drift for c in cs]
@@ -391,13 +398,15 @@ def test_nbody_drifted_shells_gradient_matches_oracle_fd(tiler, solver_name):
 
     def oracle_shells(x, v):
         x, v = x.copy(), v.copy()
-        if solver_name == "edk":
+        if solver_name != "kkd":
             v += opm.pm_forces(x, np.float64) * k_init
         maps, si = [], 0
         for ev in events:
             if ev[0] == "step":
-                if solver_name == "edk":
+                if solver_name != "kkd":
                     x += v * drifts[si]
+                    if solver_name == "edk_sharp":
+                        v += opm.sharpening_boost(x, *sharp, bare[si], np.float64)
                     v += opm.pm_forces(x, np.float64) * kicks[si]
                 else:
                     v += opm.pm_forces(x, np.float64) * kicks[si]
