@@ -276,11 +276,12 @@ class ReversibleNBody(torch.autograd.Function):
 
 
 class ReversibleNBodyShells(torch.autograd.Function):
-    """(dx, p) -> HEALPix shells painted at snapshot times along the KKD loop (S, npix).
+    """(dx, p) -> snapshots painted at their times along the KKD loop: HEALPix shells
+    (S, npix) or CIC densities (S, *mesh; geom["out_shape"] the mesh).
 
-    The loop runs in segments: `segments[j]` steps, then shell j painted from the state
-    there by `painters[j]`, a dict with rmin, rmax, scale and either kind "sphere" (the
-    particles as they are) or kind "tiled" (replicas `rot`, `shifts`, `telephoto`, drifted
+    The loop runs in segments: `segments[j]` steps, then snapshot j painted from the state
+    there by `painters[j]`, a dict with a scale and its kind: "density" (the CIC density
+    times scale), or, with rmin and rmax, "sphere" (the particles as they are) or "tiled" (replicas `rot`, `shifts`, `telephoto`, drifted
     to the light cone at time `t` with the velocities when `vel` is set; `kick` is the
     kick the EfficientDriftDoubleKick loop applies before a velocity paint, so the painted
     velocity is v + kick F(x) while the loop's state stays in the reversible form). The
@@ -316,8 +317,8 @@ class ReversibleNBodyShells(torch.autograd.Function):
         n_all = int(sum(segments))
         pots = potential_store(n_all, x) if any(ctx.needs_input_grad[:2]) else None
         rho = torch.empty(x.shape[:-1], dtype=torch.float32, device=x.device)
-        nside = geom["nside"]
-        maps = torch.empty(len(segments), 12 * nside * nside, dtype=torch.float32, device=x.device)
+        shape = geom.get("out_shape") or (12 * geom["nside"] ** 2,)
+        maps = torch.empty(len(segments), *shape, dtype=torch.float32, device=x.device)
         s0 = 0
         for j, c in enumerate(segments):
             if c > 0:
@@ -365,7 +366,9 @@ class ReversibleNBodyShells(torch.autograd.Function):
 
 def _paint(x, vp, geom, j, out):
     pt = geom["painters"][j]
-    if pt["kind"] == "sphere":
+    if pt["kind"] == "density":
+        ops.paint_cic(x, weight=pt["scale"], out=out[0])
+    elif pt["kind"] == "sphere":
         ops.healpix_paint_shells(x, geom["nside"], geom["box"], geom["obs"], [pt["rmin"]], [pt["rmax"]], [pt["scale"]],
                                  scheme=geom["scheme"], out=out)
     else:
@@ -377,7 +380,9 @@ def _paint(x, vp, geom, j, out):
 
 def _paint_adjoint(x, vp, geom, j, map_bar, lam_x, vp_bar):
     pt = geom["painters"][j]
-    if pt["kind"] == "sphere":
+    if pt["kind"] == "density":
+        ops.adjoint_position(x, lam_x, rho_bar=map_bar[0].contiguous(), scale=pt["scale"])
+    elif pt["kind"] == "sphere":
         ops.healpix_paint_shells_adjoint(x, map_bar, geom["nside"], geom["box"], geom["obs"], [pt["rmin"]],
                                          [pt["rmax"]], [pt["scale"]], scheme=geom["scheme"], pos_bar=lam_x)
     else:
@@ -411,6 +416,39 @@ class PowerSpectrum(torch.autograd.Function):
         w[1:-1] = torch.where(c > 0, 2.0 * gpk * ctx.vol / torch.where(c > 0, c, torch.ones_like(c)),
                               torch.zeros_like(c))
         return ops.power_adjoint(mesh, ke, w.float(), ctx.box), None, None
+
+
+class CrossPowerSpectrum(torch.autograd.Function):
+    """(mesh, mesh2) -> cross P(k) in the kept bins (FP64): the modulus of the binned sum of
+    F1 conj(F2) over the mode count, times prod(L/N) (reference _src/power/_compute.py:68-119
+    with mesh2). For real meshes the imaginary parts cancel between k and -k, so
+    d|S_b| = sign(Re S_b) d Re S_b, and d Re S_b / d mesh is the other mesh through the auto
+    spectrum's adjoint with half its weight (the auto spectrum's factor 2 comes from
+    |F|^2): dL/dmesh = power_adjoint(mesh2, w / 2), dL/dmesh2 = power_adjoint(mesh, w / 2)."""
+
+    @staticmethod
+    def forward(ctx, mesh, mesh2, kedges: np.ndarray, box):
+        from ..power import poles_sums
+
+        out, _ = poles_sums(mesh, mesh2, box, kedges, (0,), (0.0, 0.0, 1.0))
+        re, im, cnt = out[0, 0], out[0, 1], out[0, 2]
+        vol = float(np.prod(np.asarray(box, np.float64) / np.asarray(mesh.shape[-3:], np.float64)))
+        norm = torch.where(cnt > 0, cnt, torch.ones_like(cnt))
+        pk = (torch.sqrt(re**2 + im**2) / norm)[1:-1] * vol
+        ctx.save_for_backward(mesh, mesh2, _dev(kedges), cnt, torch.sign(re))
+        ctx.vol, ctx.box = vol, box
+        return pk
+
+    @staticmethod
+    def backward(ctx, gpk):
+        mesh, mesh2, ke, cnt, sgn = ctx.saved_tensors
+        w = torch.zeros(ke.numel() + 1, dtype=torch.float64, device=mesh.device)
+        c = cnt[1:-1]
+        w[1:-1] = torch.where(c > 0, gpk * ctx.vol * sgn[1:-1] / torch.where(c > 0, c, torch.ones_like(c)),
+                              torch.zeros_like(c))
+        g1 = ops.power_adjoint(mesh2, ke, w.float(), ctx.box) if ctx.needs_input_grad[0] else None
+        g2 = ops.power_adjoint(mesh, ke, w.float(), ctx.box) if ctx.needs_input_grad[1] else None
+        return g1, g2, None, None
 
 
 # ----------------------------------------------------------------------------- model

@@ -195,7 +195,8 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
     """The N-body loop as one autograd node whose backward is the reversible adjoint
     (pm/adjoint.py), for inputs that require gradients. The reference's equivalents are
     nbody(..., adjoint="reverse") and nbody(..., adjoint="checkpointed") under jax.grad
-    (pm/integrate.py:109-535). Covers one density snapshot without a correction kernel.
+    (pm/integrate.py:109-535). Covers density snapshots and HEALPix shells, with
+    NoCorrection or SharpeningKernel.
 
     EfficientDriftDoubleKick takes the same route: its fused step kicks with the pending
     factor (the initial half kick at step 0, step i-1's kick after that) and then drifts,
@@ -216,12 +217,13 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
                  and isinstance(pt.weights, (type(None), int, float)) and bool(np.all(np.diff(ts_arr) > 0))
                  and (isinstance(interp, NoInterp) or (isinstance(interp, (DriftInterp, OnionTiler))
                                                        and dx.array.dim() == 4)))
-    if not shells_ok and not (solver_ok and isinstance(interp, NoInterp) and tgt == "density" and ts_arr.size == 1
-                              and _scalar_weight(interp.painting.weights) == 1.0):
+    density_ok = (solver_ok and isinstance(interp, NoInterp) and tgt == "density"
+                  and isinstance(pt.weights, (type(None), int, float)) and bool(np.all(np.diff(ts_arr) > 0)))
+    if not shells_ok and not density_ok:
         raise NotImplementedError(
             "gradients run through the reversible adjoint: ReversibleDoubleKickDrift or EfficientDriftDoubleKick "
-            "with NoCorrection or SharpeningKernel, painting a density snapshot at one time (NoInterp) or HEALPix shells (ngp or "
-            "bilinear) at increasing times (NoInterp, DriftInterp or OnionTiler)")
+            "with NoCorrection or SharpeningKernel, painting density snapshots (NoInterp, scalar weights) or HEALPix "
+            "shells (ngp or bilinear; NoInterp, DriftInterp or OnionTiler) at increasing times")
     if dx.unit != PositionUnit.GRID_RELATIVE:
         raise NotImplementedError("differentiable integration takes GRID_RELATIVE displacements")
     steps = [(e[1], e[2]) for e in time_events(t0, ts, dt0, dtype) if e[0] == "step"]
@@ -248,6 +250,8 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
                            sharpen=None if sharpen is None else (boosts, float(sharpen.kl), float(sharpen.ks)))
     if shells_ok:
         return _run_differentiable_shells(interp, dx, p, cosmo, t0, ts, dt0, dtype, tables, paint_kicks, paint_boosts)
+    if ts_arr.size > 1 or _scalar_weight(interp.painting.weights) != 1.0:
+        return _run_differentiable_densities(interp, dx, p, t0, ts, dt0, dtype, tables)
     rho = ReversibleNBody.apply(dx.array.contiguous(), p.array.contiguous(), None, tables)
     from ..fields import DensityField, FieldStatus
 
@@ -257,6 +261,38 @@ def run_differentiable(solver, dx: ParticleField, p: ParticleField, cosmo, ts, t
     snap = snap.replace(scale_factors=t_target, comoving_centers=float(interp.r_centers[state.interp_state.shell_idx]),
                         density_width=float(interp.density_widths[state.interp_state.shell_idx]))
     return RunResult(snapshots=[snap], disp=None, vel=None, steps=len(steps))
+
+
+def _run_differentiable_densities(interp, dx: ParticleField, p: ParticleField, t0: float, ts, dt0: float, dtype,
+                                  tables) -> RunResult:
+    """Density snapshots at several times (or with a scalar weight) along the loop as one
+    autograd node (adjoint.ReversibleNBodyShells with density painters): snapshot j is the
+    CIC density of the positions at the j-th snapshot time times the weight, as the fused
+    loop paints it (NoInterp.paint -> ParticleField.paint); the backward adds each
+    snapshot's CIC gradient at the reconstructed positions before reversing the steps that
+    led there."""
+    from ..fields import DensityField, FieldStatus
+    from .adjoint import ReversibleNBodyShells
+
+    events = time_events(t0, ts, dt0, dtype)
+    segments, count = [], 0
+    for ev in events:
+        if ev[0] == "step":
+            count += 1
+        else:
+            segments.append(count)
+            count = 0
+    saves = [ev for ev in events if ev[0] == "save"]
+    w = float(_scalar_weight(interp.painting.weights))
+    geom = dict(painters=[dict(kind="density", scale=w)] * len(segments), out_shape=tuple(dx.array.shape[:-1]))
+    rhos = ReversibleNBodyShells.apply(dx.array.contiguous(), p.array.contiguous(), tables, segments, geom)
+    snaps = []
+    for j, ev in enumerate(saves):
+        t_j = float(ev[2])
+        snap = DensityField(array=rhos[j], **dx.replace(scale_factors=t_j)._meta_for_density(FieldStatus.DENSITY_FIELD))
+        snaps.append(snap.replace(scale_factors=t_j, comoving_centers=float(interp.r_centers[j]),
+                                  density_width=float(interp.density_widths[j])))
+    return RunResult(snapshots=snaps, disp=None, vel=None, steps=int(sum(segments)))
 
 
 def _run_differentiable_shells(interp, dx: ParticleField, p: ParticleField, cosmo, t0: float, ts, dt0: float, dtype,

@@ -45,11 +45,10 @@ def finalize(sums: torch.Tensor, mesh_shape, box_shape):
     return kavg, pk
 
 
-def power_poles(mesh: torch.Tensor, mesh2, box_shape, kedges, poles, los):
-    """Cross spectra and/or multipoles (reference _src/power/_compute.py:68-119): for each
-    multipole the sum over the full grid of (2l + 1) L_l(mu) F1 conj(F2) per bin, its real
-    part for an auto spectrum and its modulus for a cross spectrum, over the mode count,
-    bins 0 and nedges dropped, times prod(L/N). -> (kavg, pk (npoles, nbins) or (nbins,))."""
+def poles_sums(mesh: torch.Tensor, mesh2, box_shape, kedges, poles, los):
+    """The raw per-bin sums of jfli_power_poles: (batch, 2 npoles + 2, nedges + 1) FP64 --
+    Re and Im of sum (2l + 1) L_l(mu) F1 conj(F2) per multipole, then the mode count and the
+    sum of |k| -- and the number of multipoles."""
     mesh_shape = tuple(int(v) for v in mesh.shape[-3:])
     lead = tuple(mesh.shape[:-3])
     batch = int(np.prod(lead)) if lead else 1
@@ -66,6 +65,17 @@ def power_poles(mesh: torch.Tensor, mesh2, box_shape, kedges, poles, los):
     ops.call("jfli_power_poles", ops.stream_ptr(), ops.ptr(mesh), ops.ptr(mesh2), ops.ptr(edges), nedges,
              *(float(v) for v in box_shape), *(float(v) for v in lv), ells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
              nell, ops.ptr(out), ops.ptr(ws), ws.numel(), *mesh_shape, batch)
+    return out, nell
+
+
+def power_poles(mesh: torch.Tensor, mesh2, box_shape, kedges, poles, los):
+    """Cross spectra and/or multipoles (reference _src/power/_compute.py:68-119): for each
+    multipole the sum over the full grid of (2l + 1) L_l(mu) F1 conj(F2) per bin, its real
+    part for an auto spectrum and its modulus for a cross spectrum, over the mode count,
+    bins 0 and nedges dropped, times prod(L/N). -> (kavg, pk (npoles, nbins) or (nbins,))."""
+    mesh_shape = tuple(int(v) for v in mesh.shape[-3:])
+    lead = tuple(mesh.shape[:-3])
+    out, nell = poles_sums(mesh, mesh2, box_shape, kedges, poles, los)
     cnt = out[:, 2 * nell]
     norm = torch.where(cnt > 0, cnt, torch.ones_like(cnt))
     re, im = out[:, 0:2 * nell:2], out[:, 1:2 * nell:2]
@@ -91,8 +101,10 @@ def power(mesh, mesh2=None, *, box_shape, kedges=None, multipoles=0, los=(0.0, 0
         kedges = default_kedges(mesh_shape, box_shape)
     poles = tuple(multipoles) if isinstance(multipoles, (list, tuple)) else (multipoles,)
     if mesh2 is not None or poles != (0,):
-        if torch.is_grad_enabled() and mesh.requires_grad:
-            raise NotImplementedError("gradients of cross spectra and multipoles are not on the B200 path")
+        grad = torch.is_grad_enabled() and (mesh.requires_grad or (isinstance(mesh2, torch.Tensor)
+                                                                   and mesh2.requires_grad))
+        if grad and (poles != (0,) or mesh.dim() != 3):
+            raise NotImplementedError("gradients of multipoles and of batched cross spectra are not on the B200 path")
         m2 = None
         if mesh2 is not None:
             m2 = mesh2 if isinstance(mesh2, torch.Tensor) else torch.as_tensor(np.asarray(mesh2, np.float32),
@@ -101,6 +113,12 @@ def power(mesh, mesh2=None, *, box_shape, kedges=None, multipoles=0, los=(0.0, 0
             if m2.shape != mesh.shape:
                 raise ValueError("mesh2 must have the shape of mesh")
         # multipoles == 0 uses mu = 1 in the reference (no line of sight): L_0 = 1 either way
+        if grad:
+            from .pm.adjoint import CrossPowerSpectrum
+
+            with torch.no_grad():
+                kavg, _ = power_poles(mesh.contiguous(), m2, box_shape, kedges, poles, los)
+            return kavg, CrossPowerSpectrum.apply(mesh.contiguous(), m2, np.asarray(kedges, np.float64), box_shape)
         return power_poles(mesh.contiguous(), m2, box_shape, kedges, poles, los)
     if torch.is_grad_enabled() and mesh.requires_grad:
         # differentiable path: the adjoint kernel gives dL/dmesh (pm/adjoint.py)

@@ -517,3 +517,117 @@ def test_public_api_gradient_equals_forward_model():
     err = float(torch.linalg.norm(noise.grad - w2.grad) / torch.linalg.norm(w2.grad))
     print(f"public API vs forward_model_pk gradient rel L2 {err:.2e}")
     assert err < 1e-5
+
+
+@pytest.mark.parametrize("solver_name", ["kkd", "edk"])
+def test_density_snapshots_gradient_matches_oracle_fd(solver_name):
+    """nbody painting density snapshots at a = 0.4, 0.7 and 1 with weight 2 (the reference
+    differentiates any snapshot list, pm/integrate.py:109-145) on displacements and momenta
+    that require grad: the snapshots equal the fused loop's, and the directional derivative
+    of sum_j <a_j, rho_j> matches central differences of the FP64 oracle loop painting at
+    the same (clipped) snapshot times.
+
+    The painted densities are piecewise linear in the positions, with kinks where a
+    particle crosses a cell face. With this seed a step of 1e-5 cells crosses enough of them
+    that the oracle's central difference for the final snapshot is 1% below the slope
+    (1286.3 against 1301.7, 1300.9 and 1298.9 at steps 3e-6, 1e-6 and 3e-7, measured with
+    the oracle alone); the test takes steps of 3e-7, and the bound is 2e-3."""
+    import jfli_b200 as jf
+    from jfli_b200.pm.integrate import time_events
+    from jfli_b200.pm.solvers import EfficientDriftDoubleKick as EDK
+    from jfli_b200.pm.solvers import ReversibleDoubleKickDrift as KKD
+
+    n, box, t0, dt0, w = 32, 128.0, 0.1, 0.15, 2.0
+    ts = [0.4, 0.7, 1.0]
+    cosmo = jf.Planck18()
+    ic = jf.interpolate_initial_conditions(jf.white_noise(23, (n,) * 3), (n,) * 3, (box,) * 3, cosmo=cosmo)
+    dx, p = jf.lpt(cosmo, ic, ts=t0, order=2)
+    x0, v0 = dx.array.detach().contiguous().clone(), p.array.detach().contiguous().clone()
+    rng = np.random.default_rng(24)
+    a = rng.standard_normal((len(ts), n, n, n))
+    r = rng.standard_normal((n, n, n, 3))
+    s = rng.standard_normal((n, n, n, 3))
+    interp = jf.NoInterp(painting=jf.PaintingOptions(target="density", weights=w))
+    solver = (jf.ReversibleDoubleKickDrift(interp_kernel=interp) if solver_name == "kkd"
+              else jf.EfficientDriftDoubleKick(interp_kernel=interp))
+    kw = dict(t0=t0, t1=1.0, dt0=dt0, ts=np.asarray(ts), solver=solver)
+    xg, vg = x0.clone().requires_grad_(True), v0.clone().requires_grad_(True)
+    rho = jf.nbody(cosmo, dx.replace(array=xg), p.replace(array=vg), **kw)
+    loss = (rho.array.double() * torch.as_tensor(a, device="cuda")).sum()
+    loss.backward()
+    g_dir = float(np.sum(xg.grad.cpu().numpy() * r) + np.sum(vg.grad.cpu().numpy() * s))
+    with torch.no_grad():
+        rho_f = jf.nbody(cosmo, dx.replace(array=x0), p.replace(array=v0), **kw)
+    e_fwd = float((rho.array.detach() - rho_f.array).norm() / rho_f.array.norm())
+
+    ts_run = np.asarray(rho.scale_factors, np.float64)[::-1]  # ascending, as the loop meets them
+    events = time_events(t0, ts_run, dt0)
+    steps = [(e[1], e[2]) for e in events if e[0] == "step"]
+    after, count = set(), 0
+    for ev in events:
+        if ev[0] == "step":
+            count += 1
+        else:
+            after.add(count - 1)
+    if solver_name == "kkd":
+        cs = [KKD.step_coefficients(cosmo, q, u, dt0, t0) for q, u in steps]
+
+        def oracle_snaps(x, v):
+            return opm.kkd_run(x, v, [(c.kick, c.drift) for c in cs], np.float64, snapshot_after=after)[2]
+    else:
+        kicks, drifts = EDK.schedule_arrays(cosmo, [q for q, _ in steps], [q for _, q in steps], dt0)
+        coeffs = dict(init_kick=EDK.init_kick(cosmo, t0, t0 + dt0), steps=list(zip(kicks, drifts)))
+
+        def oracle_snaps(x, v):
+            return opm.kdk_run(x, v, coeffs, np.float64, snapshot_after=after)[2]
+
+    def oracle_loss(x, v):
+        snaps = np.stack(oracle_snaps(x, v)[::-1]) * w  # latest first, as nbody returns them
+        return float(np.sum(a * snaps))
+
+    x64, v64 = x0.cpu().numpy().astype(np.float64), v0.cpu().numpy().astype(np.float64)
+    eps = 3e-7
+    fd = (oracle_loss(x64 + eps * r, v64 + eps * s) - oracle_loss(x64 - eps * r, v64 - eps * s)) / (2 * eps)
+    L0 = oracle_loss(x64, v64)
+    print(f"{solver_name} density snapshots {len(ts)}: vs the fused loop {e_fwd:.2e}; loss GPU "
+          f"{float(loss.detach()):.8e} oracle {L0:.8e}; directional derivative {g_dir:.6e} vs oracle central "
+          f"difference {fd:.6e}")
+    assert tuple(rho.array.shape) == (len(ts), n, n, n)
+    assert e_fwd < 1e-5
+    assert _rel(float(loss.detach()), L0) < 1e-4
+    assert _rel(g_dir, fd) < 2e-3
+
+
+def test_cross_power_gradient_matches_oracle_fd():
+    """power(mesh, mesh2) with both meshes requiring grad: the cross spectrum equals the
+    FP64 oracle's (oracle/pm.py power_poles, the reference's _power with mesh2), and the
+    directional derivative of sum_b c_b P_b matches central differences of the oracle (the
+    spectrum is quadratic in the meshes, so steps of 1e-3 are exact up to rounding)."""
+    import jfli_b200 as jf
+
+    n, box = 32, (100.0, 100.0, 100.0)
+    rng = np.random.default_rng(31)
+    m1 = rng.standard_normal((n, n, n))
+    m2 = 0.6 * m1 + 0.8 * rng.standard_normal((n, n, n))  # correlated: no bin sum near zero
+    r1, r2 = rng.standard_normal((n, n, n)), rng.standard_normal((n, n, n))
+    kedges = np.linspace(0.05, 1.5, 12)
+    t1 = torch.as_tensor(m1, dtype=torch.float32, device="cuda").requires_grad_(True)
+    t2 = torch.as_tensor(m2, dtype=torch.float32, device="cuda").requires_grad_(True)
+    _, pk = jf.power(t1, t2, box_shape=box, kedges=kedges)
+    c = rng.standard_normal(pk.shape[-1])
+    loss = (pk * torch.as_tensor(c, device="cuda")).sum()
+    loss.backward()
+    g_dir = float(np.sum(t1.grad.cpu().numpy() * r1) + np.sum(t2.grad.cpu().numpy() * r2))
+    _, ref = opm.power_poles(m1, m2, box, kedges)
+    ref = np.asarray(ref).reshape(-1)
+    err = float(np.abs(pk.detach().cpu().numpy() - ref).max() / np.abs(ref).max())
+
+    def oracle_loss(a, b):
+        return float(np.sum(c * np.asarray(opm.power_poles(a, b, box, kedges)[1]).reshape(-1)))
+
+    eps = 1e-3
+    fd = (oracle_loss(m1 + eps * r1, m2 + eps * r2) - oracle_loss(m1 - eps * r1, m2 - eps * r2)) / (2 * eps)
+    print(f"cross P(k): vs the oracle {err:.2e}; directional derivative {g_dir:.8e} vs oracle central difference "
+          f"{fd:.8e}")
+    assert err < 1e-5
+    assert _rel(g_dir, fd) < 1e-4
