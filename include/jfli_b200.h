@@ -503,6 +503,18 @@ int jfli_kkd_adjoint_sharpened(void* stream, float* disp, float* vel, float* lam
 int jfli_power_spectrum_adjoint(void* stream, const float* mesh, const float* kedges, const float* weights,
                                 int nedges, float lx, float ly, float lz, float* out, void* workspace,
                                 size_t workspace_bytes, int nx, int ny, int nz, int batch, char* err, size_t errlen);
+/* The same for Legendre multipoles of an auto spectrum (the VJP of jfli_power_poles
+ * without mesh2; reference _src/power/_compute.py:68-119 with multipoles): out =
+ * irfft(rfft(mesh) * w(k) / M), w(k) the mean over the mode and its conjugate partner of
+ * sum_e weights[e][bin] (2 l_e + 1) L_l_e(mu), mu = (k . los) / |k| with los = (losx, losy,
+ * losz) normalised (the partner's frequencies negated except on Nyquist planes), weights
+ * nell x (nedges + 1) (2 dL/dP_e,b prod(L/N) / count_b, 0 outside the kept bins). ells:
+ * nell <= 8 values in [0, 16]; nedges + nell (nedges + 1) <= 4097. Workspace:
+ * jfli_poisson_workspace_bytes. */
+int jfli_power_poles_adjoint(void* stream, const float* mesh, const float* kedges, const float* weights, int nedges,
+                             const int* ells, int nell, float lx, float ly, float lz, float losx, float losy,
+                             float losz, float* out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
+                             int batch, char* err, size_t errlen);
 
 /* dL/d ic of jfli_lpt given dL/ddx (lam_x) and dL/dp (lam_v). Workspace:
  * jfli_lpt_adjoint_workspace_bytes. */

@@ -4,12 +4,14 @@
 // JFLI_E* codes with a message in `err`. Nothing throws across this boundary and
 // nothing synchronises the device except where documented.
 #include <atomic>
+#include <cmath>
 #include <cstdint>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 
 #include "../../include/jfli_b200.h"
+
 #include "internal.h"
 
 namespace jfli {
@@ -1398,6 +1400,37 @@ int jfli_adjoint_position(void* stream, const float* disp, const float* u, const
   const MeshDims d{nx, ny, nz, batch};
   return cuda_status(jfli::adjoint_position(disp, u, rho_bar, force, scale, lam_x, d, (cudaStream_t)stream), err,
                      errlen, "jfli_adjoint_position");
+}
+
+int jfli_power_poles_adjoint(void* stream, const float* mesh, const float* kedges, const float* weights, int nedges,
+                             const int* ells, int nell, float lx, float ly, float lz, float losx, float losy,
+                             float losz, float* out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
+                             int batch, char* err, size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_FFT(nx, ny, nz);
+  CHECK_PTR(mesh);
+  CHECK_PTR(kedges);
+  CHECK_PTR(weights);
+  CHECK_PTR(ells);
+  CHECK_PTR(out);
+  CHECK_PTR(workspace);
+  // 8: the multipole slots of the adjoint operator (kMaxAdjPoles)
+  if (nell < 1 || nell > 8) return fail(err, errlen, JFLI_EINVAL, "nell %d outside [1, 8]", nell);
+  if (nedges < 1 || nedges + nell * (nedges + 1) > 2 * 2048 + 1)
+    return fail(err, errlen, JFLI_EINVAL, "nedges %d with %d multipoles exceeds the weight table", nedges, nell);
+  for (int e = 0; e < nell; ++e)
+    if (ells[e] < 0 || ells[e] > 16) return fail(err, errlen, JFLI_EINVAL, "multipole %d outside [0, 16]", ells[e]);
+  if (!(lx > 0 && ly > 0 && lz > 0)) return fail(err, errlen, JFLI_EINVAL, "box sizes must be positive");
+  const double ln = std::sqrt((double)losx * losx + (double)losy * losy + (double)losz * losz);
+  if (!(ln > 0)) return fail(err, errlen, JFLI_EINVAL, "the line of sight must be nonzero");
+  const MeshDims d{nx, ny, nz, batch};
+  if (workspace_bytes < spec_bytes(d))
+    return fail(err, errlen, JFLI_EINVAL, "workspace too small: %zu < %zu bytes", workspace_bytes, spec_bytes(d));
+  const float box[3] = {lx, ly, lz};
+  const float los[3] = {(float)(losx / ln), (float)(losy / ln), (float)(losz / ln)};
+  return cuda_status(jfli::power_poles_adjoint(mesh, (float2*)workspace, out, d, kedges, weights, nedges, ells, nell,
+                                               box, los, (cudaStream_t)stream),
+                     err, errlen, "jfli_power_poles_adjoint");
 }
 
 int jfli_power_spectrum_adjoint(void* stream, const float* mesh, const float* kedges, const float* weights,

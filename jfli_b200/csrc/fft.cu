@@ -956,6 +956,28 @@ cudaError_t power_adjoint(const float* mesh, float2* spec, float* out, const Mes
   return filter_chain(mesh, spec, out, d, 0.0f, op, s);
 }
 
+cudaError_t power_poles_adjoint(const float* mesh, float2* spec, float* out, const MeshDims& d, const float* kedges,
+                                const float* weights, int nedges, const int* ells, int nell, const float* box,
+                                const float* los, cudaStream_t s) {
+  PkAdjOp op;
+  op.nx = d.nx;
+  op.ny = d.ny;
+  op.nz = d.nz;
+  op.kedges = kedges;
+  op.weights = weights;
+  op.nedges = nedges;
+  op.cx = (float)(2.0 * M_PI / (double)box[0]);
+  op.cy = (float)(2.0 * M_PI / (double)box[1]);
+  op.cz = (float)(2.0 * M_PI / (double)box[2]);
+  op.norm = 1.0f / ((float)d.nx * (float)d.ny * (float)d.nz);
+  op.nell = nell;
+  for (int e = 0; e < nell && e < kMaxAdjPoles; ++e) op.ells[e] = ells[e];
+  op.lx = los[0];
+  op.ly = los[1];
+  op.lz = los[2];
+  return filter_chain(mesh, spec, out, d, 0.0f, op, s);
+}
+
 cudaError_t power_partials(const float* mesh, float2* spec, double* partials, const MeshDims& d, const float* kedges,
                            int nedges, const float* box, float norm, cudaStream_t s) {
   cudaError_t e = launch_rfft_z(mesh, spec, d, 0.0f, s);

@@ -232,6 +232,30 @@ struct PkOp {
 // bin(k) = digitize(|k|, kedges) with the same |k| rounding as PkOp, so that the inverse
 // transform gives dL/dmesh = sum over bins of dL/dP_b * dP_b/dmesh when
 // weights[b] = 2 * dL/dP_b * prod(L/N) / count_b (0 for the dropped under/overflow bins).
+// L_l(mu) by the reference's recurrence, in FP32 (the multipole weights (2l + 1) L_l(mu) of
+// the reference's _power, _src/power/_compute.py:96-103)
+__device__ __forceinline__ float legendre_f32(int ell, float mu) {
+  if (ell == 0) return 1.f;
+  if (ell == 1) return mu;
+  float p0 = 1.f, p1 = mu;
+  for (int n = 2; n <= ell; ++n) {
+    const float pn = __fdiv_rn(__fsub_rn(__fmul_rn(__fmul_rn((float)(2 * n - 1), mu), p1), __fmul_rn((float)(n - 1), p0)),
+                               (float)n);
+    p0 = p1;
+    p1 = pn;
+  }
+  return p1;
+}
+
+constexpr int kMaxAdjPoles = 8;
+
+// Adjoint of the binned P(k) sums: out = irfft(rfft(mesh) * w(k) / M). Monopole (nell = 0):
+// w(k) = weights[bin(|k|)]. Multipoles of an auto spectrum (nell > 0): the mode's weight is
+// sum over the multipoles e of weights[e][bin] (2l_e + 1) L_l_e(mu), mu = (k . los) / |k|,
+// and w(k) its mean over the mode and its conjugate partner (a real mesh's gradient sees
+// only that Hermitian part). The partner's signed frequencies are the mode's negated, except
+// along an axis where the mode sits on the Nyquist plane (index n/2, frequency -n/2 for
+// both): there mu is not -mu, and odd multipoles of an auto spectrum do not vanish.
 struct PkAdjOp {
   static constexpr bool kInverse = true;
   static constexpr bool kStore = true;
@@ -241,10 +265,16 @@ struct PkAdjOp {
   int nedges;
   float cx, cy, cz;  // 2*pi / L_i
   float norm;        // 1 / M (inverse transform)
-  static size_t smem_bytes(const PkAdjOp& op) { return sizeof(float) * (2 * op.nedges + 1); }
+  int nell = 0;      // multipoles: weights holds nell x (nedges + 1)
+  int ells[kMaxAdjPoles] = {};
+  float lx = 0.f, ly = 0.f, lz = 1.f;  // unit line of sight
+  static size_t smem_bytes(const PkAdjOp& op) {
+    return sizeof(float) * (op.nedges + (op.nell > 0 ? op.nell : 1) * (op.nedges + 1));
+  }
   __device__ void prologue(float* sm, int) const {
+    const int nw = (nell > 0 ? nell : 1) * (nedges + 1);
     for (int i = threadIdx.x; i < nedges; i += blockDim.x) sm[i] = kedges[i];
-    for (int i = threadIdx.x; i <= nedges; i += blockDim.x) sm[nedges + i] = weights[i];
+    for (int i = threadIdx.x; i < nw; i += blockDim.x) sm[nedges + i] = weights[i];
     __syncthreads();
   }
   __device__ float2 apply(float2 v, int kx, int ky, int kz, float* sm, int) const {
@@ -260,7 +290,19 @@ struct PkAdjOp {
       else
         hi = mid;
     }
-    return cscale(v, sm[nedges + lo] * norm);
+    if (nell == 0) return cscale(v, sm[nedges + lo] * norm);
+    const float dot = __fadd_rn(__fadd_rn(__fmul_rn(ax, lx), __fmul_rn(ay, ly)), __fmul_rn(az, lz));
+    const float mu = kmag == 0.f ? 0.f : __fdiv_rn(dot, kmag);
+    const float px = 2 * kx == nx ? ax : -ax, py = 2 * ky == ny ? ay : -ay, pz = 2 * kz == nz ? az : -az;
+    const float dotp = __fadd_rn(__fadd_rn(__fmul_rn(px, lx), __fmul_rn(py, ly)), __fmul_rn(pz, lz));
+    const float mup = kmag == 0.f ? 0.f : __fdiv_rn(dotp, kmag);
+    float w = 0.f;
+    for (int e = 0; e < nell; ++e) {
+      const float f = (float)(2 * ells[e] + 1);
+      w += sm[nedges + e * (nedges + 1) + lo] *
+           (0.5f * (__fmul_rn(f, legendre_f32(ells[e], mu)) + __fmul_rn(f, legendre_f32(ells[e], mup))));
+    }
+    return cscale(v, w * norm);
   }
   __device__ void epilogue(float*, int, int, int) const {}
 };

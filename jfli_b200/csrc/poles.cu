@@ -25,19 +25,6 @@ struct PolesArgs {
   int ells[kMaxPoles];
 };
 
-__device__ __forceinline__ float legendre_f32(int ell, float mu) {
-  if (ell == 0) return 1.f;
-  if (ell == 1) return mu;
-  float p0 = 1.f, p1 = mu;
-  for (int n = 2; n <= ell; ++n) {
-    const float pn = __fdiv_rn(__fsub_rn(__fmul_rn(__fmul_rn((float)(2 * n - 1), mu), p1), __fmul_rn((float)(n - 1), p0)),
-                               (float)n);
-    p0 = p1;
-    p1 = pn;
-  }
-  return p1;
-}
-
 // adds mode (ix, iy, iz) with the value c = F1 conj F2 (norm applied) to the CTA's sums
 __device__ __forceinline__ void add_mode(const PolesArgs& a, int ix, int iy, int iz, double cre, double cim,
                                          const float* edges, double* sums) {

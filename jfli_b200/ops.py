@@ -822,6 +822,28 @@ def power_adjoint(mesh: torch.Tensor, kedges: torch.Tensor, weights: torch.Tenso
     return out
 
 
+def power_poles_adjoint(mesh: torch.Tensor, kedges: torch.Tensor, weights: torch.Tensor, ells, box_size,
+                        los=(0.0, 0.0, 1.0)) -> torch.Tensor:
+    """dL/dmesh of auto-spectrum multipole sums for per-multipole, per-bin weights
+    (nell, nedges + 1) = 2 dL/dP_l,b prod(L/N) / count_b (jfli_power_poles_adjoint)."""
+    _check(mesh, "mesh")
+    _check(kedges, "kedges")
+    _check(weights, "weights")
+    (nx, ny, nz), batch, lead = _mesh_dims(mesh, False)
+    ne = int(kedges.numel())
+    ell_arr = np.ascontiguousarray(np.asarray(ells, dtype=np.int32))
+    if weights.numel() != ell_arr.size * (ne + 1):
+        raise ValueError("weights must hold nedges + 1 entries per multipole")
+    out = torch.empty_like(mesh)
+    nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
+    ws = workspace(nb, "spec", mesh.device)
+    lx, ly, lz = (float(v) for v in box_size)
+    call("jfli_power_poles_adjoint", stream_ptr(), ptr(mesh), ptr(kedges), ptr(weights), ne,
+         ell_arr.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(ell_arr.size), lx, ly, lz,
+         *(float(v) for v in los), ptr(out), ptr(ws), ws.numel(), nx, ny, nz, batch)
+    return out
+
+
 def lpt_adjoint(ic: torch.Tensor, order: int, c1x: float, c2x: float, c1p: float, c2p: float, lam_x: torch.Tensor,
                 lam_v: torch.Tensor) -> torch.Tensor:
     """dL/d ic of lpt() given the cotangents of its displacement and momentum."""

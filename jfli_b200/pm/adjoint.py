@@ -418,6 +418,43 @@ class PowerSpectrum(torch.autograd.Function):
         return ops.power_adjoint(mesh, ke, w.float(), ctx.box), None, None
 
 
+class PowerPoles(torch.autograd.Function):
+    """mesh -> Legendre multipoles of its auto spectrum in the kept bins (FP64): for each l
+    the real part of the binned sum of (2l + 1) L_l(mu) |F|^2 over the mode count, times
+    prod(L/N) (reference _src/power/_compute.py:68-119 with multipoles). The gradient is the
+    auto spectrum's adjoint with each mode weighted by sum_l w_l[bin] (2l + 1) L_l(mu),
+    averaged with the mode's conjugate partner (jfli_power_poles_adjoint): odd multipoles
+    cancel between k and -k except on the grid's Nyquist planes, where the partner has the
+    same frequency -n/2."""
+
+    @staticmethod
+    def forward(ctx, mesh, kedges: np.ndarray, box, poles, los):
+        from ..power import poles_sums
+
+        out, nell = poles_sums(mesh, None, box, kedges, poles, los)
+        re, cnt = out[0, 0:2 * nell:2], out[0, 2 * nell]
+        vol = float(np.prod(np.asarray(box, np.float64) / np.asarray(mesh.shape[-3:], np.float64)))
+        norm = torch.where(cnt > 0, cnt, torch.ones_like(cnt))
+        pk = (re / norm[None, :])[:, 1:-1] * vol
+        ctx.save_for_backward(mesh, _dev(kedges), cnt)
+        ctx.vol, ctx.box, ctx.poles, ctx.los = vol, box, tuple(int(p) for p in poles), los
+        return pk[0] if nell == 1 else pk
+
+    @staticmethod
+    def backward(ctx, gpk):
+        mesh, ke, cnt = ctx.saved_tensors
+        g = gpk.reshape(len(ctx.poles), -1)
+        c = cnt[1:-1]
+        w = torch.zeros(len(ctx.poles), ke.numel() + 1, dtype=torch.float64, device=mesh.device)
+        for e in range(len(ctx.poles)):
+            w[e, 1:-1] = torch.where(c > 0, 2.0 * g[e] * ctx.vol / torch.where(c > 0, c, torch.ones_like(c)),
+                                     torch.zeros_like(c))
+        lv = np.asarray(ctx.los, np.float64)
+        out = ops.power_poles_adjoint(mesh, ke, w.float().contiguous(), list(ctx.poles), ctx.box,
+                                      tuple(lv / np.linalg.norm(lv)))
+        return out, None, None, None, None
+
+
 class CrossPowerSpectrum(torch.autograd.Function):
     """(mesh, mesh2) -> cross P(k) in the kept bins (FP64): the modulus of the binned sum of
     F1 conj(F2) over the mode count, times prod(L/N) (reference _src/power/_compute.py:68-119
