@@ -509,12 +509,16 @@ int jfli_power_spectrum_adjoint(void* stream, const float* mesh, const float* ke
  * sum_e weights[e][bin] (2 l_e + 1) L_l_e(mu), mu = (k . los) / |k| with los = (losx, losy,
  * losz) normalised (the partner's frequencies negated except on Nyquist planes), weights
  * nell x (nedges + 1) (2 dL/dP_e,b prod(L/N) / count_b, 0 outside the kept bins). ells:
- * nell <= 8 values in [0, 16]; nedges + nell (nedges + 1) <= 4097. Workspace:
+ * nell <= 8 values in [0, 16]. For the cross spectrum |S_e,b| of meshes 1 and 2 (mesh2),
+ * complex_weights = 1 and weights holds the real then the imaginary parts of c_e,b = u_e,b
+ * dL/dP_e,b prod(L/N) / count_b, u = S / |S|: called on mesh 2 with c it gives dL/dmesh1,
+ * on mesh 1 with conj(c) dL/dmesh2; the multiplier is then the Hermitian part of c w(k).
+ * nedges + (1 + complex_weights) nell (nedges + 1) <= 4097. Workspace:
  * jfli_poisson_workspace_bytes. */
 int jfli_power_poles_adjoint(void* stream, const float* mesh, const float* kedges, const float* weights, int nedges,
-                             const int* ells, int nell, float lx, float ly, float lz, float losx, float losy,
-                             float losz, float* out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
-                             int batch, char* err, size_t errlen);
+                             const int* ells, int nell, int complex_weights, float lx, float ly, float lz, float losx,
+                             float losy, float losz, float* out, void* workspace, size_t workspace_bytes, int nx,
+                             int ny, int nz, int batch, char* err, size_t errlen);
 
 /* dL/d ic of jfli_lpt given dL/ddx (lam_x) and dL/dp (lam_v). Workspace:
  * jfli_lpt_adjoint_workspace_bytes. */

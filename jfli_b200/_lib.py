@@ -188,8 +188,8 @@ _SIGNATURES = {
     ),
     "jfli_power_poles_adjoint": (
         c_int,
-        [c_void_p, c_void_p, c_void_p, c_void_p, c_int, ctypes.POINTER(c_int), c_int, c_float, c_float, c_float,
-         c_float, c_float, c_float, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
+        [c_void_p, c_void_p, c_void_p, c_void_p, c_int, ctypes.POINTER(c_int), c_int, c_int, c_float, c_float,
+         c_float, c_float, c_float, c_float, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
     ),
     "jfli_kkd_run_sharpened": (
         c_int,

@@ -1403,9 +1403,9 @@ int jfli_adjoint_position(void* stream, const float* disp, const float* u, const
 }
 
 int jfli_power_poles_adjoint(void* stream, const float* mesh, const float* kedges, const float* weights, int nedges,
-                             const int* ells, int nell, float lx, float ly, float lz, float losx, float losy,
-                             float losz, float* out, void* workspace, size_t workspace_bytes, int nx, int ny, int nz,
-                             int batch, char* err, size_t errlen) {
+                             const int* ells, int nell, int complex_weights, float lx, float ly, float lz,
+                             float losx, float losy, float losz, float* out, void* workspace, size_t workspace_bytes,
+                             int nx, int ny, int nz, int batch, char* err, size_t errlen) {
   CHECK_DIMS(nx, ny, nz, batch);
   CHECK_FFT(nx, ny, nz);
   CHECK_PTR(mesh);
@@ -1416,7 +1416,8 @@ int jfli_power_poles_adjoint(void* stream, const float* mesh, const float* kedge
   CHECK_PTR(workspace);
   // 8: the multipole slots of the adjoint operator (kMaxAdjPoles)
   if (nell < 1 || nell > 8) return fail(err, errlen, JFLI_EINVAL, "nell %d outside [1, 8]", nell);
-  if (nedges < 1 || nedges + nell * (nedges + 1) > 2 * 2048 + 1)
+  const int cplx = complex_weights ? 1 : 0;
+  if (nedges < 1 || nedges + (1 + cplx) * nell * (nedges + 1) > 2 * 2048 + 1)
     return fail(err, errlen, JFLI_EINVAL, "nedges %d with %d multipoles exceeds the weight table", nedges, nell);
   for (int e = 0; e < nell; ++e)
     if (ells[e] < 0 || ells[e] > 16) return fail(err, errlen, JFLI_EINVAL, "multipole %d outside [0, 16]", ells[e]);
@@ -1429,7 +1430,7 @@ int jfli_power_poles_adjoint(void* stream, const float* mesh, const float* kedge
   const float box[3] = {lx, ly, lz};
   const float los[3] = {(float)(losx / ln), (float)(losy / ln), (float)(losz / ln)};
   return cuda_status(jfli::power_poles_adjoint(mesh, (float2*)workspace, out, d, kedges, weights, nedges, ells, nell,
-                                               box, los, (cudaStream_t)stream),
+                                               box, los, cplx, (cudaStream_t)stream),
                      err, errlen, "jfli_power_poles_adjoint");
 }
 

@@ -958,7 +958,7 @@ cudaError_t power_adjoint(const float* mesh, float2* spec, float* out, const Mes
 
 cudaError_t power_poles_adjoint(const float* mesh, float2* spec, float* out, const MeshDims& d, const float* kedges,
                                 const float* weights, int nedges, const int* ells, int nell, const float* box,
-                                const float* los, cudaStream_t s) {
+                                const float* los, int cplx, cudaStream_t s) {
   PkAdjOp op;
   op.nx = d.nx;
   op.ny = d.ny;
@@ -971,6 +971,7 @@ cudaError_t power_poles_adjoint(const float* mesh, float2* spec, float* out, con
   op.cz = (float)(2.0 * M_PI / (double)box[2]);
   op.norm = 1.0f / ((float)d.nx * (float)d.ny * (float)d.nz);
   op.nell = nell;
+  op.cplx = cplx;
   for (int e = 0; e < nell && e < kMaxAdjPoles; ++e) op.ells[e] = ells[e];
   op.lx = los[0];
   op.ly = los[1];

@@ -39,11 +39,12 @@ cudaError_t ic_filter(const float* noise, float2* spec, float* out, const MeshDi
                       const float* dptab = nullptr);
 cudaError_t power_adjoint(const float* mesh, float2* spec, float* out, const MeshDims& d, const float* kedges,
                           const float* weights, int nedges, const float* box, cudaStream_t s);
-// The same for auto-spectrum multipoles: weights nell x (nedges + 1), even ells only, each
-// mode weighted by sum_e weights[e][bin] (2l_e + 1) L_l_e(mu), mu along the unit vector los.
+// The same for multipoles: weights nell x (nedges + 1) (with cplx, real then imaginary parts
+// of a complex factor per bin), each mode weighted by sum_e weights[e][bin] (2l_e + 1)
+// L_l_e(mu), mu along the unit vector los, averaged with its conjugate partner.
 cudaError_t power_poles_adjoint(const float* mesh, float2* spec, float* out, const MeshDims& d, const float* kedges,
                                 const float* weights, int nedges, const int* ells, int nell, const float* box,
-                                const float* los, cudaStream_t s);
+                                const float* los, int cplx, cudaStream_t s);
 cudaError_t power_partials(const float* mesh, float2* spec, double* partials, const MeshDims& d, const float* kedges,
                            int nedges, const float* box, float norm, cudaStream_t s);
 

@@ -256,6 +256,9 @@ constexpr int kMaxAdjPoles = 8;
 // only that Hermitian part). The partner's signed frequencies are the mode's negated, except
 // along an axis where the mode sits on the Nyquist plane (index n/2, frequency -n/2 for
 // both): there mu is not -mu, and odd multipoles of an auto spectrum do not vanish.
+// Cross spectra (cplx = 1): weights holds the real then the imaginary parts, nell x (nedges +
+// 1) each, of a complex per-bin factor c; the Hermitian part of c w(k) is the multiplier:
+// Re(c) (w(k) + w(partner)) / 2 + i Im(c) (w(k) - w(partner)) / 2.
 struct PkAdjOp {
   static constexpr bool kInverse = true;
   static constexpr bool kStore = true;
@@ -265,14 +268,15 @@ struct PkAdjOp {
   int nedges;
   float cx, cy, cz;  // 2*pi / L_i
   float norm;        // 1 / M (inverse transform)
-  int nell = 0;      // multipoles: weights holds nell x (nedges + 1)
+  int nell = 0;      // multipoles: weights holds nell x (nedges + 1) (twice that when cplx)
+  int cplx = 0;
   int ells[kMaxAdjPoles] = {};
   float lx = 0.f, ly = 0.f, lz = 1.f;  // unit line of sight
   static size_t smem_bytes(const PkAdjOp& op) {
-    return sizeof(float) * (op.nedges + (op.nell > 0 ? op.nell : 1) * (op.nedges + 1));
+    return sizeof(float) * (op.nedges + (op.cplx ? 2 : 1) * (op.nell > 0 ? op.nell : 1) * (op.nedges + 1));
   }
   __device__ void prologue(float* sm, int) const {
-    const int nw = (nell > 0 ? nell : 1) * (nedges + 1);
+    const int nw = (cplx ? 2 : 1) * (nell > 0 ? nell : 1) * (nedges + 1);
     for (int i = threadIdx.x; i < nedges; i += blockDim.x) sm[i] = kedges[i];
     for (int i = threadIdx.x; i < nw; i += blockDim.x) sm[nedges + i] = weights[i];
     __syncthreads();
@@ -296,13 +300,16 @@ struct PkAdjOp {
     const float px = 2 * kx == nx ? ax : -ax, py = 2 * ky == ny ? ay : -ay, pz = 2 * kz == nz ? az : -az;
     const float dotp = __fadd_rn(__fadd_rn(__fmul_rn(px, lx), __fmul_rn(py, ly)), __fmul_rn(pz, lz));
     const float mup = kmag == 0.f ? 0.f : __fdiv_rn(dotp, kmag);
-    float w = 0.f;
+    float w = 0.f, wo = 0.f;
+    const int im0 = nedges + nell * (nedges + 1);
     for (int e = 0; e < nell; ++e) {
       const float f = (float)(2 * ells[e] + 1);
-      w += sm[nedges + e * (nedges + 1) + lo] *
-           (0.5f * (__fmul_rn(f, legendre_f32(ells[e], mu)) + __fmul_rn(f, legendre_f32(ells[e], mup))));
+      const float a = __fmul_rn(f, legendre_f32(ells[e], mu)), b = __fmul_rn(f, legendre_f32(ells[e], mup));
+      w += sm[nedges + e * (nedges + 1) + lo] * (0.5f * (a + b));
+      if (cplx) wo += sm[im0 + e * (nedges + 1) + lo] * (0.5f * (a - b));
     }
-    return cscale(v, w * norm);
+    if (!cplx) return cscale(v, w * norm);
+    return make_float2((v.x * w - v.y * wo) * norm, (v.x * wo + v.y * w) * norm);
   }
   __device__ void epilogue(float*, int, int, int) const {}
 };

@@ -823,23 +823,24 @@ def power_adjoint(mesh: torch.Tensor, kedges: torch.Tensor, weights: torch.Tenso
 
 
 def power_poles_adjoint(mesh: torch.Tensor, kedges: torch.Tensor, weights: torch.Tensor, ells, box_size,
-                        los=(0.0, 0.0, 1.0)) -> torch.Tensor:
-    """dL/dmesh of auto-spectrum multipole sums for per-multipole, per-bin weights
-    (nell, nedges + 1) = 2 dL/dP_l,b prod(L/N) / count_b (jfli_power_poles_adjoint)."""
+                        los=(0.0, 0.0, 1.0), complex_weights: bool = False) -> torch.Tensor:
+    """dL/dmesh of multipole sums for per-multipole, per-bin weights (nell, nedges + 1) =
+    2 dL/dP_l,b prod(L/N) / count_b of an auto spectrum, or (2, nell, nedges + 1), the real
+    and imaginary parts of a cross spectrum's complex factors (jfli_power_poles_adjoint)."""
     _check(mesh, "mesh")
     _check(kedges, "kedges")
     _check(weights, "weights")
     (nx, ny, nz), batch, lead = _mesh_dims(mesh, False)
     ne = int(kedges.numel())
     ell_arr = np.ascontiguousarray(np.asarray(ells, dtype=np.int32))
-    if weights.numel() != ell_arr.size * (ne + 1):
-        raise ValueError("weights must hold nedges + 1 entries per multipole")
+    if weights.numel() != (2 if complex_weights else 1) * ell_arr.size * (ne + 1):
+        raise ValueError("weights must hold nedges + 1 entries per multipole (twice that for complex weights)")
     out = torch.empty_like(mesh)
     nb = query("jfli_poisson_workspace_bytes", nx, ny, nz, batch)
     ws = workspace(nb, "spec", mesh.device)
     lx, ly, lz = (float(v) for v in box_size)
     call("jfli_power_poles_adjoint", stream_ptr(), ptr(mesh), ptr(kedges), ptr(weights), ne,
-         ell_arr.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(ell_arr.size), lx, ly, lz,
+         ell_arr.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(ell_arr.size), int(bool(complex_weights)), lx, ly, lz,
          *(float(v) for v in los), ptr(out), ptr(ws), ws.numel(), nx, ny, nz, batch)
     return out
 

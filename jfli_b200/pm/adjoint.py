@@ -455,6 +455,49 @@ class PowerPoles(torch.autograd.Function):
         return out, None, None, None, None
 
 
+class CrossPoles(torch.autograd.Function):
+    """(mesh, mesh2) -> Legendre multipoles of the cross spectrum (FP64): |S_l,b| over the
+    mode count times prod(L/N), S_l,b the binned sum of (2l + 1) L_l(mu) F1 conj(F2)
+    (reference _src/power/_compute.py:68-119 with mesh2 and multipoles). With u = S / |S|,
+    dL/dmesh1 is the multipole adjoint on mesh2 with the complex factors c = u dL/dP
+    prod(L/N) / count, and dL/dmesh2 the same on mesh1 with conj(c)."""
+
+    @staticmethod
+    def forward(ctx, mesh, mesh2, kedges: np.ndarray, box, poles, los):
+        from ..power import poles_sums
+
+        out, nell = poles_sums(mesh, mesh2, box, kedges, poles, los)
+        re, im, cnt = out[0, 0:2 * nell:2], out[0, 1:2 * nell:2], out[0, 2 * nell]
+        mod = torch.sqrt(re**2 + im**2)
+        vol = float(np.prod(np.asarray(box, np.float64) / np.asarray(mesh.shape[-3:], np.float64)))
+        norm = torch.where(cnt > 0, cnt, torch.ones_like(cnt))
+        pk = (mod / norm[None, :])[:, 1:-1] * vol
+        safe = torch.where(mod > 0, mod, torch.ones_like(mod))
+        ure, uim = torch.where(mod > 0, re / safe, torch.zeros_like(re)), torch.where(mod > 0, im / safe,
+                                                                                       torch.zeros_like(im))
+        ctx.save_for_backward(mesh, mesh2, _dev(kedges), cnt, ure, uim)
+        ctx.vol, ctx.box, ctx.poles, ctx.los = vol, box, tuple(int(p) for p in poles), los
+        return pk[0] if nell == 1 else pk
+
+    @staticmethod
+    def backward(ctx, gpk):
+        mesh, mesh2, ke, cnt, ure, uim = ctx.saved_tensors
+        g = gpk.reshape(len(ctx.poles), -1)
+        c = cnt[1:-1]
+        s = torch.zeros(len(ctx.poles), ke.numel() + 1, dtype=torch.float64, device=mesh.device)
+        s[:, 1:-1] = torch.where(c > 0, g * ctx.vol / torch.where(c > 0, c, torch.ones_like(c)), torch.zeros_like(c))
+        lv = np.asarray(ctx.los, np.float64)
+        los = tuple(lv / np.linalg.norm(lv))
+
+        def adj(m, sign):
+            w = torch.stack([s * ure, sign * s * uim]).float().contiguous()
+            return ops.power_poles_adjoint(m, ke, w, list(ctx.poles), ctx.box, los, complex_weights=True)
+
+        g1 = adj(mesh2, 1.0) if ctx.needs_input_grad[0] else None
+        g2 = adj(mesh, -1.0) if ctx.needs_input_grad[1] else None
+        return g1, g2, None, None, None, None
+
+
 class CrossPowerSpectrum(torch.autograd.Function):
     """(mesh, mesh2) -> cross P(k) in the kept bins (FP64): the modulus of the binned sum of
     F1 conj(F2) over the mode count, times prod(L/N) (reference _src/power/_compute.py:68-119

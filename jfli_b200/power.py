@@ -103,9 +103,8 @@ def power(mesh, mesh2=None, *, box_shape, kedges=None, multipoles=0, los=(0.0, 0
     if mesh2 is not None or poles != (0,):
         grad = torch.is_grad_enabled() and (mesh.requires_grad or (isinstance(mesh2, torch.Tensor)
                                                                    and mesh2.requires_grad))
-        if grad and (mesh.dim() != 3 or (mesh2 is not None and poles != (0,))):
-            raise NotImplementedError("gradients of cross-spectrum multipoles and of batched spectra are not on the "
-                                      "B200 path")
+        if grad and mesh.dim() != 3:
+            raise NotImplementedError("gradients of batched spectra are not on the B200 path")
         m2 = None
         if mesh2 is not None:
             m2 = mesh2 if isinstance(mesh2, torch.Tensor) else torch.as_tensor(np.asarray(mesh2, np.float32),
@@ -120,6 +119,12 @@ def power(mesh, mesh2=None, *, box_shape, kedges=None, multipoles=0, los=(0.0, 0
             with torch.no_grad():
                 kavg, _ = power_poles(mesh.contiguous(), None, box_shape, kedges, poles, los)
             return kavg, PowerPoles.apply(mesh.contiguous(), np.asarray(kedges, np.float64), box_shape, poles, los)
+        if grad and poles != (0,):  # cross-spectrum multipoles
+            from .pm.adjoint import CrossPoles
+
+            with torch.no_grad():
+                kavg, _ = power_poles(mesh.contiguous(), m2, box_shape, kedges, poles, los)
+            return kavg, CrossPoles.apply(mesh.contiguous(), m2, np.asarray(kedges, np.float64), box_shape, poles, los)
         if grad:
             from .pm.adjoint import CrossPowerSpectrum
 
