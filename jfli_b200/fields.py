@@ -723,6 +723,14 @@ class ParticleField(AbstractField):
         w, ws = _weights_arg(weights)
         out = None
         acc = False
+        if torch.is_grad_enabled() and self.array.requires_grad:
+            if absolute or w is not None or mesh is not None:
+                raise NotImplementedError("gradients of CIC painting: relative displacements, a scalar weight, a new "
+                                          "mesh")
+            from .painting import CICPaint
+
+            dens = CICPaint.apply(self.array.contiguous(), ws)
+            return DensityField(array=dens, **self._meta_for_density(FieldStatus.DENSITY_FIELD))
         if mesh is not None:
             out = (mesh.array if isinstance(mesh, AbstractField) else mesh).clone().contiguous()
             acc = True
@@ -740,6 +748,8 @@ class ParticleField(AbstractField):
         """CIC interpolation of a mesh at the particle positions (reference fields/particles.py:182-229)."""
         absolute = self._grid_mode()
         mesh = density_mesh.array if isinstance(density_mesh, AbstractField) else density_mesh
+        if torch.is_grad_enabled() and (self.array.requires_grad or mesh.requires_grad):
+            raise NotImplementedError("gradients of the CIC readout are not on the B200 path")
         vals = ops.readout_cic(self.array.contiguous(), mesh.contiguous(), absolute=absolute)
         return DensityField(array=vals, **self._meta_for_density(self.status))
 
@@ -752,6 +762,8 @@ class ParticleField(AbstractField):
         snapshot of a batched (S, ...) input that fall in its z range."""
         if self.flatsky_npix is None:
             raise ValueError("ParticleField requires `flatsky_npix` for paint_2d.")
+        if torch.is_grad_enabled() and self.array.requires_grad:
+            raise NotImplementedError("gradients of flat-sky planes are not on the B200 path")
         field = self if self.unit != PositionUnit.MPC_H else self.to(PositionUnit.GRID_ABSOLUTE)
         absolute = field._grid_mode()
         centers = np.atleast_1d(np.asarray(center, dtype=np.float64))

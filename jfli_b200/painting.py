@@ -21,6 +21,26 @@ def shell_volume_per_pixel(nside: int, rmin: float, rmax: float) -> float:
     return (4.0 * math.pi / (12 * nside * nside)) * (rmax**3 - rmin**3) / 3.0
 
 
+class CICPaint(torch.autograd.Function):
+    """Relative displacements -> their CIC density times a scalar weight (ParticleField.paint,
+    reference fields/particles.py:119-178); the backward is the CIC gradient of the density
+    cotangent at the positions (jfli_adjoint_position), the adjoint of the deposit."""
+
+    @staticmethod
+    def forward(ctx, x, weight: float):
+        x = x.contiguous()
+        ctx.save_for_backward(x)
+        ctx.weight = float(weight)
+        return ops.paint_cic(x, weight=ctx.weight)
+
+    @staticmethod
+    def backward(ctx, g):
+        (x,) = ctx.saved_tensors
+        lam = torch.zeros_like(x)
+        ops.adjoint_position(x, lam, rho_bar=g.contiguous(), scale=ctx.weight)
+        return lam, None
+
+
 class PaintShells(torch.autograd.Function):
     """Shells of one particle set as an autograd node: forward jfli_healpix_paint_shells,
     backward its adjoint (position and per-particle weight cotangents; the shell edges are

@@ -455,6 +455,43 @@ class PowerPoles(torch.autograd.Function):
         return out, None, None, None, None
 
 
+class LPTLightcone(torch.autograd.Function):
+    """ic -> (dx, p, a) of light-cone-mode LPT (jfli_lpt_lightcone; reference pm/lpt.py:110-130
+    with utils.py:234-244): each particle at the scale factor a_p of its own light-cone
+    crossing, fixed by its Lagrangian position. The map is jfli_lpt's with per-particle
+    coefficients (c1x, c2x, c1p, c2p)(a_p), so its VJP is jfli_lpt_adjoint with the
+    cotangents weighted per particle, u1 = c1x lam_x + c1p c1x lam_v and u2 = c2x lam_x +
+    c2p c2x lam_v, passed as lam_x = u1, lam_v = u2 - u1 with unit coefficients (c1x = 1,
+    c1p = 0, c2x = c2p = 1). a passes no gradient."""
+
+    @staticmethod
+    def forward(ctx, ic, order: int, cosmo, box, observer):
+        dx, p, a = ops.lpt_lightcone(ic.contiguous(), order, cosmo, box, observer)
+        ctx.save_for_backward(ic.contiguous(), a)
+        ctx.order, ctx.cosmo = int(order), cosmo
+        ctx.mark_non_differentiable(a)
+        return dx, p, a
+
+    @staticmethod
+    def backward(ctx, gdx, gp, ga):
+        ic, a = ctx.saved_tensors
+        gdx = torch.zeros(a.shape + (3,), dtype=torch.float32, device=a.device) if gdx is None else gdx
+        gp = torch.zeros_like(gdx) if gp is None else gp
+        av = a.double().cpu().numpy()
+        c = ctx.cosmo
+        d1, f1 = cj.growth_factor(c, av), cj.growth_rate(c, av)
+        d2, f2 = cj.growth_factor_second(c, av), cj.growth_rate_second(c, av)
+        ea = cj.E(c, av)
+        coef = [torch.as_tensor(np.asarray(v, np.float64), device=a.device)[..., None]
+                for v in (d1, 3.0 / 7.0 * d2, av * av * f1 * ea, av * av * f2 * ea)]
+        c1x, c2x, c1p, c2p = coef
+        gx, gv = gdx.double(), gp.double()
+        u1 = c1x * gx + c1p * c1x * gv
+        u2 = c2x * gx + c2p * c2x * gv
+        out = ops.lpt_adjoint(ic, ctx.order, 1.0, 1.0, 0.0, 1.0, u1.float().contiguous(), (u2 - u1).float().contiguous())
+        return out, None, None, None, None
+
+
 class CrossPoles(torch.autograd.Function):
     """(mesh, mesh2) -> Legendre multipoles of the cross spectrum (FP64): |S_l,b| over the
     mode count times prod(L/N), S_l,b the binned sum of (2l + 1) L_l(mu) F1 conj(F2)

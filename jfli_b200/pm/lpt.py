@@ -134,8 +134,11 @@ def _lpt_lightcone(cosmo, initial_field, order, painting, r_centers, widths):
     per-particle scale factors, shape (..., nx, ny, nz, 1), as the reference's do."""
     ic = initial_field.array.contiguous()
     if torch.is_grad_enabled() and ic.requires_grad:
-        raise NotImplementedError("gradients through light-cone-mode LPT are not on the B200 path")
-    dx, p, a = ops.lpt_lightcone(ic, order, cosmo, initial_field.box_size, initial_field.observer_position_mpc)
+        from .adjoint import LPTLightcone
+
+        dx, p, a = LPTLightcone.apply(ic, order, cosmo, initial_field.box_size, initial_field.observer_position_mpc)
+    else:
+        dx, p, a = ops.lpt_lightcone(ic, order, cosmo, initial_field.box_size, initial_field.observer_position_mpc)
     a = a[..., None]
     dt = cj.distance_table(cosmo)
     chi = _device_interp(a, dt.a, dt.chi).clamp(0.0, 1e6).float()

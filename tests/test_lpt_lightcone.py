@@ -76,3 +76,59 @@ def test_lightcone_lpt_painted_shells_and_density(cosmo):
         assert ref.sum() > 0 and err < 2e-5
     dens, _ = jf.lpt(cosmo, ic, nb_shells=4, order=2, painting=jf.PaintingOptions(target="density"))
     assert rel_l2(dens.array.double().cpu().numpy(), opm.cic_paint(rdx)) < 1e-5
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_lightcone_lpt_gradient_matches_oracle_fd(cosmo, order):
+    """Light-cone-mode LPT on an initial field that requires grad (the per-particle
+    coefficients applied to the cotangents of jfli_lpt_adjoint): the directional derivative
+    of <r1, dx> + <r2, p> with respect to the initial field matches central differences of
+    the FP64 oracle (oracle/pm.py lpt_lightcone; linear or quadratic in the field, so steps
+    of 1e-3 are exact up to rounding)."""
+    n, L = 32, 300.0
+    ic, ic64 = _setup(cosmo, n, L)
+    rng = np.random.default_rng(40 + order)
+    r1, r2, s = rng.standard_normal((n, n, n, 3)), rng.standard_normal((n, n, n, 3)), rng.standard_normal((n, n, n))
+    icg = ic.array.detach().clone().requires_grad_(True)
+    dx, p = jf.lpt(cosmo, ic.replace(array=icg), nb_shells=4, order=order)
+    loss = (dx.array.double() * torch.as_tensor(r1, device="cuda")).sum() + \
+        (p.array.double() * torch.as_tensor(r2, device="cuda")).sum()
+    loss.backward()
+    g_dir = float(np.sum(icg.grad.cpu().numpy() * s))
+    obs = ic.observer_position_mpc
+
+    def oracle_loss(f):
+        rdx, rp, _ = opm.lpt_lightcone(f, order, (L, L, L), obs, lambda r: cj.a_of_chi(cosmo, r), _coefficients(cosmo))
+        return float(np.sum(r1 * rdx) + np.sum(r2 * rp))
+
+    eps = 1e-3
+    fd = (oracle_loss(ic64 + eps * s) - oracle_loss(ic64 - eps * s)) / (2 * eps)
+    print(f"light-cone LPT order {order}: directional derivative {g_dir:.8e} vs oracle central difference {fd:.8e}")
+    assert abs(g_dir - fd) / abs(fd) < 1e-4
+
+
+def test_lpt_density_gradient_matches_oracle_fd(cosmo):
+    """Snapshot LPT painted to a density (ParticleField.paint on displacements that require
+    grad: the CIC-paint node, whose backward is jfli_adjoint_position): the directional
+    derivative of <a, rho> with respect to the initial field matches central differences
+    of the FP64 oracle (LPT then CIC paint; steps of 1e-6 keep the particles inside their
+    cells)."""
+    n, L = 32, 300.0
+    ic, ic64 = _setup(cosmo, n, L)
+    rng = np.random.default_rng(44)
+    a, s = rng.standard_normal((n, n, n)), rng.standard_normal((n, n, n))
+    icg = ic.array.detach().clone().requires_grad_(True)
+    rho, _ = jf.lpt(cosmo, ic.replace(array=icg), ts=0.5, order=2, painting=jf.PaintingOptions(target="density"))
+    loss = (rho.array.double() * torch.as_tensor(a, device="cuda")).sum()
+    loss.backward()
+    g_dir = float(np.sum(icg.grad.cpu().numpy() * s))
+    c = lpt_coefficients(cosmo, 0.5)
+
+    def oracle_loss(f):
+        rdx, _ = opm.lpt(f, *c, order=2)
+        return float(np.sum(a * opm.cic_paint(rdx)))
+
+    eps = 1e-6
+    fd = (oracle_loss(ic64 + eps * s) - oracle_loss(ic64 - eps * s)) / (2 * eps)
+    print(f"LPT density: directional derivative {g_dir:.8e} vs oracle central difference {fd:.8e}")
+    assert abs(g_dir - fd) / abs(fd) < 1e-3
