@@ -749,7 +749,13 @@ class ParticleField(AbstractField):
         absolute = self._grid_mode()
         mesh = density_mesh.array if isinstance(density_mesh, AbstractField) else density_mesh
         if torch.is_grad_enabled() and (self.array.requires_grad or mesh.requires_grad):
-            raise NotImplementedError("gradients of the CIC readout are not on the B200 path")
+            if absolute or tuple(mesh.shape) != tuple(self.array.shape[:-1]):
+                raise NotImplementedError("gradients of the CIC readout: relative displacements, one mesh per "
+                                          "particle set")
+            from .painting import CICReadout
+
+            vals = CICReadout.apply(self.array, mesh)
+            return DensityField(array=vals, **self._meta_for_density(self.status))
         vals = ops.readout_cic(self.array.contiguous(), mesh.contiguous(), absolute=absolute)
         return DensityField(array=vals, **self._meta_for_density(self.status))
 

@@ -41,6 +41,36 @@ class CICPaint(torch.autograd.Function):
         return lam, None
 
 
+class CICReadout(torch.autograd.Function):
+    """(relative displacements, mesh) -> the mesh's CIC interpolation at the particles
+    (ParticleField.read_out, reference fields/particles.py:182-229). Backward: the mesh's
+    cotangent is the CIC paint of the output cotangent g as per-particle weights; the
+    positions' is g_p grad_x R_x[mesh], the u . F term of jfli_adjoint_position with the mesh
+    as the first lane of a float4 mesh and u = (g, 0, 0)."""
+
+    @staticmethod
+    def forward(ctx, x, mesh):
+        x, mesh = x.contiguous(), mesh.contiguous()
+        ctx.save_for_backward(x, mesh)
+        return ops.readout_cic(x, mesh)
+
+    @staticmethod
+    def backward(ctx, g):
+        x, mesh = ctx.saved_tensors
+        g = g.contiguous()
+        gx = gm = None
+        if ctx.needs_input_grad[1]:
+            gm = ops.paint_cic(x, weights=g)
+        if ctx.needs_input_grad[0]:
+            m4 = torch.zeros(tuple(mesh.shape) + (4,), dtype=torch.float32, device=mesh.device)
+            m4[..., 0] = mesh
+            u = torch.zeros_like(x)
+            u[..., 0] = g
+            gx = torch.zeros_like(x)
+            ops.adjoint_position(x, gx, u=u, force=m4)
+        return gx, gm
+
+
 class PaintShells(torch.autograd.Function):
     """Shells of one particle set as an autograd node: forward jfli_healpix_paint_shells,
     backward its adjoint (position and per-particle weight cotangents; the shell edges are
