@@ -332,6 +332,13 @@ int jfli_replica_positions(void* stream, const float* disp, int absolute, const 
 int jfli_paint_flat(void* stream, const float* disp, int absolute, const float* weights, float weight, float zlo,
                     float zhi, int npx, int npy, float* map, int accumulate, int nx, int ny, int nz, int batch,
                     char* err, size_t errlen);
+/* Adjoint of jfli_paint_flat with a scalar weight (the VJP of paint_2d; reference
+ * _src/fields/_painting.py:117-202): pos_bar[p] += the gradient in the particle's x and y
+ * (grid units) of <map_bar, plane>, the slab edges in z passing none. map_bar has the
+ * planes' shape (batch, npx, npy); pos_bar the particles'. */
+int jfli_paint_flat_adjoint(void* stream, const float* disp, int absolute, float weight, float zlo, float zhi, int npx,
+                            int npy, const float* map_bar, float* pos_bar, int nx, int ny, int nz, int batch, char* err,
+                            size_t errlen);
 
 /* Flat-sky angular power sums of maps [batch][npx][npy] (auto, or cross with map2):
  * Re(F1 conj F2) of the full 2D FFT grid binned by ell = |2 pi fftfreq(n, d)| with

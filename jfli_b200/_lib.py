@@ -186,6 +186,10 @@ _SIGNATURES = {
         [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_float), ctypes.POINTER(c_float), c_int,
          c_void_p, c_void_p, c_void_p, c_size_t, *_DIMS, *_ERR],
     ),
+    "jfli_paint_flat_adjoint": (
+        c_int,
+        [c_void_p, c_void_p, c_int, c_float, c_float, c_float, c_int, c_int, c_void_p, c_void_p, *_DIMS, *_ERR],
+    ),
     "jfli_power_poles_adjoint": (
         c_int,
         [c_void_p, c_void_p, c_void_p, c_void_p, c_int, ctypes.POINTER(c_int), c_int, c_int, c_float, c_float,

@@ -862,6 +862,21 @@ int jfli_paint_flat(void* stream, const float* disp, int absolute, const float* 
                      "jfli_paint_flat");
 }
 
+int jfli_paint_flat_adjoint(void* stream, const float* disp, int absolute, float weight, float zlo, float zhi, int npx,
+                            int npy, const float* map_bar, float* pos_bar, int nx, int ny, int nz, int batch, char* err,
+                            size_t errlen) {
+  CHECK_DIMS(nx, ny, nz, batch);
+  CHECK_PTR(disp);
+  CHECK_PTR(map_bar);
+  CHECK_PTR(pos_bar);
+  if (npx < 1 || npy < 1 || (long long)npx * npy > (1LL << 30))
+    return fail(err, errlen, JFLI_EINVAL, "flat-sky map (%d, %d) outside [1, 2^30] pixels", npx, npy);
+  const MeshDims d{nx, ny, nz, batch};
+  return cuda_status(jfli::paint_flat_adjoint(disp, absolute, weight, d, npx, npy, zlo, zhi, map_bar, pos_bar,
+                                              (cudaStream_t)stream),
+                     err, errlen, "jfli_paint_flat_adjoint");
+}
+
 static bool flat_fft_supported(int npx, int npy) {
   return npy % 2 == 0 && npy >= 4 && jfli::fft_axis_supported(npx) && jfli::fft_axis_supported(npy / 2);
 }

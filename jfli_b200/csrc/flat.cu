@@ -69,6 +69,66 @@ cudaError_t paint_flat(const float* disp, int absolute, const float* weights, fl
   return cudaGetLastError();
 }
 
+// Adjoint of k_paint_flat with a scalar weight: for the plane cotangent map_bar, each
+// particle in the slab adds weight * sum over its 4 cells of map_bar times the gradient of
+// the 2D CIC weights to its x and y (the scaling to the plane grid and the periodic wrap
+// have derivative s_x, s_y and 1; the slab edges pass no gradient), placed as the forward
+// places it.
+__global__ void k_paint_flat_adjoint(const float* __restrict__ disp, int absolute, float weight, PGrid g, float sx,
+                                     float sy, float zlo, float zhi, int npx, int npy,
+                                     const float* __restrict__ map_bar, float* __restrict__ pos_bar) {
+  const long long b = blockIdx.y;
+  disp += b * g.np * 3;
+  pos_bar += b * g.np * 3;
+  map_bar += b * (long long)npx * npy;
+  const float fnx = (float)npx, fny = (float)npy;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < g.np; p += gridDim.x * blockDim.x) {
+    float gx = disp[3 * p + 0], gy = disp[3 * p + 1], gz = disp[3 * p + 2];
+    if (!absolute) {
+      int i, j, k;
+      particle_ijk(g, p, i, j, k);
+      gx += (float)i;
+      gy += (float)j;
+      gz += (float)k;
+    }
+    if (!(gz > zlo && gz <= zhi)) continue;
+    float x = __fmul_rn(gx, sx), y = __fmul_rn(gy, sy);
+    x = fmodf(x, fnx);
+    y = fmodf(y, fny);
+    if (x < 0.f) x += fnx;
+    if (y < 0.f) y += fny;
+    const float fx0 = floorf(x), fy0 = floorf(y);
+    const float wx[2] = {1.f - fabsf(x - fx0), 1.f - fabsf(x - (fx0 + 1.f))};
+    const float wy[2] = {1.f - fabsf(y - fy0), 1.f - fabsf(y - (fy0 + 1.f))};
+    const float dx[2] = {-1.f, 1.f}, dy[2] = {-1.f, 1.f};  // d w / d x of the two cells
+    int ix0 = (int)fx0 % npx, iy0 = (int)fy0 % npy;
+    if (ix0 < 0) ix0 += npx;
+    if (iy0 < 0) iy0 += npy;
+    const int ix[2] = {ix0, ix0 + 1 == npx ? 0 : ix0 + 1};
+    const int iy[2] = {iy0, iy0 + 1 == npy ? 0 : iy0 + 1};
+    float ax = 0.f, ay = 0.f;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const float m = map_bar[(long long)ix[a] * npy + iy[c]];
+        ax += m * dx[a] * wy[c];
+        ay += m * wx[a] * dy[c];
+      }
+    pos_bar[3 * p + 0] += weight * sx * ax;
+    pos_bar[3 * p + 1] += weight * sy * ay;
+  }
+}
+
+cudaError_t paint_flat_adjoint(const float* disp, int absolute, float weight, const MeshDims& d, int npx, int npy,
+                               float zlo, float zhi, const float* map_bar, float* pos_bar, cudaStream_t s) {
+  const float sx = (float)((double)npx / d.nx), sy = (float)((double)npy / d.ny);
+  k_paint_flat_adjoint<<<particle_grid_dims(d.cells(), d.batch, 256, 16), 256, 0, s>>>(
+      disp, absolute, weight, make_pgrid(d), sx, sy, zlo, zhi, npx, npy, map_bar, pos_bar);
+  note_launch();
+  return cudaGetLastError();
+}
+
 constexpr int kFlatThreads = 256;
 
 __device__ __forceinline__ float ell_component(int i, int n, float dn) {

@@ -207,6 +207,9 @@ cudaError_t healpix_paint_tiled_adjoint(const float* disp, int absolute, const f
 // ---- flat.cu ----
 cudaError_t paint_flat(const float* disp, int absolute, const float* weights, float weight, const MeshDims& d, int npx,
                        int npy, float zlo, float zhi, float* map, cudaStream_t s);
+// Adjoint of paint_flat with a scalar weight: pos_bar[p] += d<map_bar, plane>/d(x, y) (in place).
+cudaError_t paint_flat_adjoint(const float* disp, int absolute, float weight, const MeshDims& d, int npx, int npy,
+                               float zlo, float zhi, const float* map_bar, float* pos_bar, cudaStream_t s);
 int flat_cl_ctas(int n0, int n1);
 cudaError_t flat_cl(const float* map1, const float* map2, int n0, int n1, int batch, float dn0, float dn1,
                     const float* edges, int nedges, float2* spec1, float2* spec2, double* partials, double* out,

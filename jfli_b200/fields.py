@@ -768,8 +768,11 @@ class ParticleField(AbstractField):
         snapshot of a batched (S, ...) input that fall in its z range."""
         if self.flatsky_npix is None:
             raise ValueError("ParticleField requires `flatsky_npix` for paint_2d.")
-        if torch.is_grad_enabled() and self.array.requires_grad:
-            raise NotImplementedError("gradients of flat-sky planes are not on the B200 path")
+        grad = torch.is_grad_enabled() and self.array.requires_grad
+        if grad and (self.unit != PositionUnit.GRID_RELATIVE or self.array.ndim != 4 or
+                     not isinstance(weights, (type(None), int, float))):
+            raise NotImplementedError("gradients of flat-sky planes: one set of relative displacements, a scalar "
+                                      "weight")
         field = self if self.unit != PositionUnit.MPC_H else self.to(PositionUnit.GRID_ABSOLUTE)
         absolute = field._grid_mode()
         centers = np.atleast_1d(np.asarray(center, dtype=np.float64))
@@ -792,6 +795,11 @@ class ParticleField(AbstractField):
         for c, wd in zip(centers, widths):
             cg, wg = c * nz / Lz, wd * nz / Lz  # grid units along z
             vol = (Lx / npx) * (Ly / npy) * wd
+            if grad:
+                from .painting import PaintFlat
+
+                maps.append(PaintFlat.apply(arr, (npx, npy), cg - wg / 2, cg + wg / 2, ws / vol if vol > 0 else ws))
+                continue
             m = None
             for src in srcs:
                 m = ops.paint_flat(src, (npx, npy), cg - wg / 2, cg + wg / 2, absolute=absolute, weights=w,

@@ -468,6 +468,21 @@ def replica_positions(pos: torch.Tensor, box_size, observer_mpc, rotation, shift
     return out
 
 
+def paint_flat_adjoint(pos: torch.Tensor, map_bar: torch.Tensor, zlo: float, zhi: float, *, absolute: bool = False,
+                       weight: float = 1.0, pos_bar: torch.Tensor | None = None) -> torch.Tensor:
+    """pos_bar += the gradient of <map_bar, paint_flat(pos, ...)> in the positions (zeros when
+    None; returned); scalar weight (jfli_paint_flat_adjoint)."""
+    _check(pos, "pos")
+    _check(map_bar, "map_bar")
+    (nx, ny, nz), batch, lead = _mesh_dims(pos, True)
+    npx, npy = (int(v) for v in map_bar.shape[-2:])
+    if pos_bar is None:
+        pos_bar = torch.zeros_like(pos)
+    call("jfli_paint_flat_adjoint", stream_ptr(), ptr(pos), int(absolute), float(weight), float(zlo), float(zhi), npx,
+         npy, ptr(map_bar), ptr(pos_bar), nx, ny, nz, batch)
+    return pos_bar
+
+
 def paint_flat(pos: torch.Tensor, npix, zlo: float, zhi: float, *, absolute: bool = False,
                weights: torch.Tensor | None = None, weight: float = 1.0, out: torch.Tensor | None = None,
                accumulate: bool = False) -> torch.Tensor:

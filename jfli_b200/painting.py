@@ -71,6 +71,24 @@ class CICReadout(torch.autograd.Function):
         return gx, gm
 
 
+class PaintFlat(torch.autograd.Function):
+    """Relative displacements -> one flat-sky plane (paint_2d's 2D CIC of the particles in a
+    z slab, scalar weight; reference _src/fields/_painting.py:117-202); the backward is
+    jfli_paint_flat_adjoint (the CIC weights' gradient in x and y; none at the slab edges)."""
+
+    @staticmethod
+    def forward(ctx, x, npix, zlo: float, zhi: float, weight: float):
+        x = x.contiguous()
+        ctx.save_for_backward(x)
+        ctx.zlo, ctx.zhi, ctx.weight = float(zlo), float(zhi), float(weight)
+        return ops.paint_flat(x, npix, zlo, zhi, weight=weight)
+
+    @staticmethod
+    def backward(ctx, g):
+        (x,) = ctx.saved_tensors
+        return ops.paint_flat_adjoint(x, g.contiguous(), ctx.zlo, ctx.zhi, weight=ctx.weight), None, None, None, None
+
+
 class PaintShells(torch.autograd.Function):
     """Shells of one particle set as an autograd node: forward jfli_healpix_paint_shells,
     backward its adjoint (position and per-particle weight cotangents; the shell edges are

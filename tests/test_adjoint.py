@@ -737,3 +737,46 @@ def test_cic_readout_gradient_matches_oracle_fd():
           f"{fd:.8e}")
     assert err < 1e-5
     assert _rel(g_dir, fd) < 1e-3
+
+
+def test_flat_plane_gradient_matches_oracle_fd():
+    """paint_2d of displacements that require grad (painting.PaintFlat, backward
+    jfli_paint_flat_adjoint): two planes, the directional derivative of sum <a_j, plane_j>
+    matches central differences of the FP64 oracle's flat painter (oracle/flat.py) with the
+    same pixel-volume normalisation (steps of 1e-6 cells keep particles in their pixels and
+    slabs)."""
+    from jfli_b200.fields import ParticleField, PositionUnit
+    from oracle import flat as ofl
+
+    n, L, npix = 32, 128.0, (48, 40)
+    rng = np.random.default_rng(61)
+    x = 0.8 * rng.standard_normal((n, n, n, 3))
+    centers, widths = np.array([40.0, 90.0]), np.array([30.0, 40.0])
+    a = rng.standard_normal((2,) + npix)
+    r = rng.standard_normal((n, n, n, 3))
+    xt = torch.as_tensor(x, dtype=torch.float32, device="cuda").requires_grad_(True)
+    f = ParticleField(array=xt, mesh_size=(n,) * 3, box_size=(L,) * 3, flatsky_npix=npix,
+                      unit=PositionUnit.GRID_RELATIVE)
+    planes = f.paint_2d(centers, widths)
+    loss = (planes.array.double() * torch.as_tensor(a, device="cuda")).sum()
+    loss.backward()
+    g_dir = float(np.sum(xt.grad.cpu().numpy() * r))
+    x32 = xt.detach().cpu().numpy().astype(np.float64)
+    grid = np.stack(np.meshgrid(*[np.arange(n, dtype=np.float64)] * 3, indexing="ij"), axis=-1)
+
+    def oracle_planes(xx):
+        out = []
+        for c, w in zip(centers, widths):
+            cg, wg = c * n / L, w * n / L
+            vol = (L / npix[0]) * (L / npix[1]) * w
+            out.append(ofl.paint_2d(grid + xx, npix, cg - wg / 2, cg + wg / 2, (n, n, n)) / vol)
+        return np.stack(out)
+
+    err = float(np.abs(planes.array.detach().cpu().numpy() - oracle_planes(x32)).max() /
+                np.abs(oracle_planes(x32)).max())
+    eps = 1e-6
+    fd = (np.sum(a * oracle_planes(x32 + eps * r)) - np.sum(a * oracle_planes(x32 - eps * r))) / (2 * eps)
+    print(f"flat planes: vs the oracle {err:.2e}; directional derivative {g_dir:.8e} vs oracle central difference "
+          f"{fd:.8e}")
+    assert err < 1e-5
+    assert _rel(g_dir, fd) < 1e-3
